@@ -1,0 +1,173 @@
+// extern "C" surface of the oracle for the Python test harness (ctypes).
+// Test infrastructure only (see flockref.hpp): loaded by tests/, by
+// __graft_entry__.smoke() and by bench.py's CPU-baseline / reference arm.
+#include "flockref.hpp"
+#include <chrono>
+#include <cstdio>
+
+using namespace flockref;
+
+extern "C" {
+
+int flockref_prove(uint32_t log2, uint64_t seed, uint8_t* out, size_t cap, size_t* out_len) {
+  try {
+    auto blocks = generate_compressions(log2, seed);
+    Bundle b = prove(blocks, (int)log2, "flock-bench-v0");
+    std::vector<uint8_t> bytes = serialize(b);
+    *out_len = bytes.size();
+    if (bytes.size() > cap) return 2;
+    memcpy(out, bytes.data(), bytes.size());
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
+void flockref_f128_mul(const uint64_t* a, const uint64_t* b, uint64_t* out) {
+  F128 r = F128(a[0], a[1]) * F128(b[0], b[1]);
+  out[0] = r.lo;
+  out[1] = r.hi;
+}
+void flockref_f128_inv(const uint64_t* a, uint64_t* out) {
+  F128 r = f128_inv(F128(a[0], a[1]));
+  out[0] = r.lo;
+  out[1] = r.hi;
+}
+void flockref_phi8_table(uint64_t* out512) {
+  const F128* t = phi8_table();
+  for (int i = 0; i < 256; i++) { out512[2 * i] = t[i].lo; out512[2 * i + 1] = t[i].hi; }
+}
+uint8_t flockref_gf8_mul(uint8_t a, uint8_t b) { return gf8_mul(a, b); }
+
+void flockref_blake3_hash(const uint8_t* d, size_t n, uint8_t* out32) { b3::hash(d, n, out32); }
+void flockref_blake3_xof(const uint8_t* d, size_t n, uint8_t* out, size_t olen) {
+  b3::Hasher h;
+  h.update(d, n);
+  h.finalize_xof(out, olen);
+}
+void flockref_blake3_leaf_cv(const uint8_t* d, size_t n, uint8_t* out32) { b3::leaf_cv(d, n, out32); }
+void flockref_blake3_parent_cv(const uint8_t* l, const uint8_t* r, uint8_t* out32) { b3::parent_cv(l, r, out32); }
+
+void flockref_generate_compressions(uint32_t log2, uint64_t seed, uint32_t* out25) {
+  auto v = generate_compressions(log2, seed);
+  for (size_t i = 0; i < v.size(); i++) {
+    uint32_t* o = out25 + 25 * i;
+    memcpy(o, v[i].cv, 32);
+    memcpy(o + 8, v[i].m, 64);
+    o[24] = (uint32_t)v[i].counter;
+  }
+}
+
+// z, a, b: 2^(14 + n_log - 7) F128 each (as u64 pairs)
+void flockref_witness(uint32_t log2, uint64_t seed, uint64_t* z, uint64_t* a, uint64_t* b) {
+  auto blocks = generate_compressions(log2, seed);
+  std::vector<F128> vz, va, vb;
+  generate_witness(blocks, (int)log2, vz, va, vb);
+  memcpy(z, vz.data(), vz.size() * 16);
+  memcpy(a, va.data(), va.size() * 16);
+  memcpy(b, vb.data(), vb.size() * 16);
+}
+
+// a_out, b_out = A0 z, B0 z for n_blocks blocks of packed z (matrix apply)
+void flockref_apply_matrices(const uint64_t* z, int n_blocks, uint64_t* a_out, uint64_t* b_out) {
+  const R1cs& rc = blake3_r1cs(3);
+  size_t n = (size_t)n_blocks * (K / 128);
+  std::vector<F128> vz(n), va, vb;
+  memcpy(vz.data(), z, n * 16);
+  apply_block_diag(rc.a0, vz, n_blocks, va);
+  apply_block_diag(rc.b0, vz, n_blocks, vb);
+  memcpy(a_out, va.data(), n * 16);
+  memcpy(b_out, vb.data(), n * 16);
+}
+
+void flockref_statement_digest(uint32_t n_log, uint8_t* out32) {
+  const R1cs& rc = blake3_r1cs((int)n_log);
+  memcpy(out32, rc.digest.data(), 32);
+}
+uint64_t flockref_matrix_nnz(int which) {
+  const R1cs& rc = blake3_r1cs(3);
+  return which == 0 ? rc.a0.col.size() : rc.b0.col.size();
+}
+// CSR export of A0 (which=0) / B0 (which=1): ptr[K+1], col[nnz]
+void flockref_matrix_csr(int which, uint32_t* ptr, uint16_t* col) {
+  const R1cs& rc = blake3_r1cs(3);
+  const SparseRows& s = which == 0 ? rc.a0 : rc.b0;
+  memcpy(ptr, s.ptr.data(), s.ptr.size() * 4);
+  memcpy(col, s.col.data(), s.col.size() * 2);
+}
+
+// RS encode: msg has n_pos positions x lanes (position-major); out 2^rate x larger
+void flockref_rs_encode(const uint64_t* msg, size_t n_pos, size_t lanes, int log_inv_rate, uint64_t* out) {
+  std::vector<F128> m(n_pos * lanes), cw;
+  memcpy(m.data(), msg, m.size() * 16);
+  rs_encode(m, lanes, log_inv_rate, cw);
+  memcpy(out, cw.data(), cw.size() * 16);
+}
+void flockref_ntt_twiddles(int dim, uint64_t* out) {
+  const AdditiveNtt& n = standard_ntt(dim);
+  memcpy(out, n.twiddles.data(), n.twiddles.size() * 16);
+}
+
+// Merkle: tree of 2n-1 nodes (32 B each)
+void flockref_merkle_tree(const uint8_t* data, size_t n_leaves, size_t leaf_size, uint8_t* tree_out) {
+  auto t = merkle_tree(data, n_leaves, leaf_size);
+  memcpy(tree_out, t.data(), t.size() * 32);
+}
+size_t flockref_merkle_multi_proof(const uint8_t* tree, size_t n_leaves, const uint64_t* pos, size_t npos,
+                                   uint8_t* out, size_t cap_nodes) {
+  std::vector<Hash> t(2 * n_leaves - 1);
+  memcpy(t.data(), tree, t.size() * 32);
+  std::vector<size_t> p(pos, pos + npos);
+  auto pr = merkle_multi_proof(t, n_leaves, p);
+  if (pr.size() <= cap_nodes) memcpy(out, pr.data(), pr.size() * 32);
+  return pr.size();
+}
+
+void flockref_build_eq(const uint64_t* r, int n, uint64_t* out) {
+  std::vector<F128> v(n);
+  memcpy(v.data(), r, n * 16);
+  auto e = build_eq(v);
+  memcpy(out, e.data(), e.size() * 16);
+}
+void flockref_lagrange(const uint64_t* z, int node_base, uint64_t* out64) {
+  auto w = lagrange_weights(K_SKIP, F128(z[0], z[1]), node_base);
+  memcpy(out64, w.data(), 64 * 16);
+}
+
+// Challenger script: domain, then ops; used to pin transcript framing.
+void* flockref_ch_new(const char* domain) { return new Challenger(domain); }
+void flockref_ch_free(void* c) { delete (Challenger*)c; }
+void flockref_ch_label(void* c, const char* l) { ((Challenger*)c)->observe_label(l); }
+void flockref_ch_observe(void* c, const uint64_t* v) { ((Challenger*)c)->observe_f128(F128(v[0], v[1])); }
+void flockref_ch_observe_slice(void* c, const uint64_t* v, size_t n) {
+  std::vector<F128> x(n);
+  memcpy(x.data(), v, n * 16);
+  ((Challenger*)c)->observe_f128_slice(x);
+}
+void flockref_ch_bytes(void* c, const uint8_t* d, size_t n) { ((Challenger*)c)->observe_bytes(d, n); }
+void flockref_ch_sample(void* c, uint64_t* out) {
+  F128 v = ((Challenger*)c)->sample_f128();
+  out[0] = v.lo;
+  out[1] = v.hi;
+}
+void flockref_ch_sample_vec(void* c, size_t n, uint64_t* out) {
+  auto v = ((Challenger*)c)->sample_f128_vec(n);
+  memcpy(out, v.data(), n * 16);
+}
+uint64_t flockref_ch_grind(void* c, uint32_t bits) { return ((Challenger*)c)->grind_pow(bits); }
+void flockref_ch_digest(void* c, uint8_t* out32) { ((Challenger*)c)->state_digest(out32); }
+int flockref_pow_ok(const uint8_t* digest, uint64_t nonce, uint32_t bits) { return pow_ok(digest, nonce, bits); }
+
+// Wall-clock seconds of one full oracle prove at log2 (for the CPU baseline).
+double flockref_time_prove(uint32_t log2, uint64_t seed, size_t* proof_len) {
+  auto blocks = generate_compressions(log2, seed);
+  blake3_r1cs((int)log2);
+  auto t0 = std::chrono::steady_clock::now();
+  Bundle b = prove(blocks, (int)log2, "flock-bench-v0");
+  std::vector<uint8_t> bytes = serialize(b);
+  auto t1 = std::chrono::steady_clock::now();
+  *proof_len = bytes.size();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+}  // extern "C"

@@ -1,0 +1,236 @@
+// flockref — CPU restatement of the Flock BLAKE3-compression prover.
+//
+// TEST INFRASTRUCTURE ONLY. This directory is the oracle that the CUDA
+// product is checked against: only tests/, __graft_entry__.smoke() and the
+// cpu_baseline / reference arm of bench.py may load or run it, and only as
+// the checker. The product library never links, loads or calls it.
+//
+// Parity pin: proofs produced by this restatement are accepted by the
+// reference's own prebuilt trusted verifier
+// (benchmark-tools/trusted/flock_benchmark_verifier, run as a program, never
+// inspected), which recomputes the pristine witness + commitment root and
+// replays the full transcript.  BLAKE3 primitives are pinned by the Python
+// `blake3` module (root hashes) and by the verifier's root recompute.
+//
+// Every function cites the reference file:line it restates (paths relative
+// to the reference project root).
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <array>
+
+namespace flockref {
+
+// ---------------------------------------------------------------------------
+// GF(2^128), GHASH polynomial x^128 + x^7 + x^2 + x + 1, lo = x^0..63.
+// crates/flock-core/src/field/gf2_128.rs:22-265, gf2_128/portable.rs.
+// ---------------------------------------------------------------------------
+struct F128 {
+  uint64_t lo = 0, hi = 0;
+  F128() = default;
+  constexpr F128(uint64_t l, uint64_t h) : lo(l), hi(h) {}
+  bool is_zero() const { return lo == 0 && hi == 0; }
+  bool operator==(const F128& o) const { return lo == o.lo && hi == o.hi; }
+  bool operator!=(const F128& o) const { return !(*this == o); }
+};
+static_assert(sizeof(F128) == 16, "F128 layout");
+inline F128 operator+(F128 a, F128 b) { return F128(a.lo ^ b.lo, a.hi ^ b.hi); }
+inline F128& operator+=(F128& a, F128 b) { a.lo ^= b.lo; a.hi ^= b.hi; return a; }
+F128 operator*(F128 a, F128 b);
+inline F128& operator*=(F128& a, F128 b) { a = a * b; return a; }
+F128 f128_inv(F128 a);
+inline const F128 ONE(1, 0);
+inline const F128 ZERO(0, 0);
+
+struct U256 { uint64_t r0 = 0, r1 = 0, r2 = 0, r3 = 0; };
+U256 mul_unreduced(F128 a, F128 b);
+F128 ghash_reduce(uint64_t r0, uint64_t r1, uint64_t r2, uint64_t r3);
+
+// GF(2^8) with the AES polynomial 0x11B.  field/gf2_8.rs:20-140.
+uint8_t gf8_mul(uint8_t a, uint8_t b);
+uint8_t gf8_inv(uint8_t a);
+// phi_8: GF(2^8) -> GF(2^128) field embedding.  field/phi8.rs:18-1050.
+F128 phi8(uint8_t v);
+const F128* phi8_table();
+
+// ---------------------------------------------------------------------------
+// BLAKE3 (spec restatement; crate blake3 1.8.6 semantics).
+// ---------------------------------------------------------------------------
+namespace b3 {
+extern const uint32_t IV[8];
+enum : uint32_t { CHUNK_START = 1, CHUNK_END = 2, PARENT = 4, ROOT = 8 };
+void compress(const uint32_t cv[8], const uint8_t block[64], uint64_t counter,
+              uint32_t block_len, uint32_t flags, uint32_t out[16]);
+// compress with block given as 16 little-endian words
+void compress_words(const uint32_t cv[8], const uint32_t m[16], uint64_t counter,
+                    uint32_t block_len, uint32_t flags, uint32_t out[16]);
+
+class Hasher {
+ public:
+  Hasher();
+  void update(const void* data, size_t len);
+  void finalize(uint8_t out32[32]) const;                // root hash
+  void finalize_xof(uint8_t* out, size_t len) const;     // root XOF
+  void finalize_non_root(uint8_t out32[32]) const;       // hazmat finalize_non_root
+ private:
+  struct Output { uint32_t cv[8]; uint8_t block[64]; uint32_t block_len; uint64_t counter; uint32_t flags; };
+  Output final_output() const;
+  void push_cv(const uint32_t cv[8], uint64_t total_chunks);
+  uint32_t chunk_cv_[8];
+  uint64_t chunk_counter_ = 0;
+  uint8_t buf_[64];
+  size_t buf_len_ = 0;
+  uint8_t blocks_compressed_ = 0;
+  std::vector<std::array<uint32_t, 8>> stack_;
+};
+void hash(const void* data, size_t len, uint8_t out32[32]);
+// non-root chaining value of a leaf of any length (merkle.rs:192-197)
+void leaf_cv(const void* data, size_t len, uint8_t out32[32]);
+// parent chaining value (merkle.rs:199-203)
+void parent_cv(const uint8_t l[32], const uint8_t r[32], uint8_t out32[32]);
+}  // namespace b3
+
+using Hash = std::array<uint8_t, 32>;
+
+// ---------------------------------------------------------------------------
+// Fiat-Shamir challenger over BLAKE3.  crates/flock-core/src/challenger.rs:170-380
+// ---------------------------------------------------------------------------
+class Challenger {
+ public:
+  explicit Challenger(const std::string& domain);
+  void observe_label(const std::string& label);
+  void observe_f128(F128 v);
+  void observe_f128_slice(const std::vector<F128>& v);
+  void observe_bytes(const void* data, size_t len);
+  F128 sample_f128();
+  std::vector<F128> sample_f128_vec(size_t n);
+  uint64_t grind_pow(uint32_t bits);           // smallest satisfying nonce
+  bool verify_pow(uint64_t nonce, uint32_t bits);
+  void state_digest(uint8_t out[32]) const;
+ private:
+  void absorb(const void* p, size_t n) { h_.update(p, n); }
+  b3::Hasher h_;
+};
+bool pow_ok(const uint8_t digest[32], uint64_t nonce, uint32_t bits);
+
+// ---------------------------------------------------------------------------
+// BLAKE3 compression R1CS.  crates/flock-prover/src/r1cs_hashes/blake3.rs
+// ---------------------------------------------------------------------------
+constexpr int K_LOG = 14;
+constexpr int K = 1 << K_LOG;
+constexpr int K_SKIP = 6;
+constexpr int Z_CONST_POS = 512;
+constexpr int USEFUL_BITS = 15409;
+
+struct Compression { uint32_t cv[8]; uint32_t m[16]; uint64_t counter; uint32_t block_len; uint32_t flags; };
+
+// benchmark-tools/common/src/lib.rs:25-37
+std::vector<Compression> generate_compressions(uint32_t log2, uint64_t seed);
+
+struct SparseRows { std::vector<uint32_t> ptr; std::vector<uint16_t> col; };  // CSR, K rows
+struct R1cs {
+  int m = 0, n_log = 0;
+  SparseRows a0, b0;
+  std::array<uint8_t, 32> digest{};
+};
+const R1cs& blake3_r1cs(int n_log);   // cached per n_log; matrices shared
+void build_matrices(SparseRows& a, SparseRows& b);
+// packed witness: z, a, b each 2^(m-7) F128 (bit r of word i = bit 128 i + r)
+void generate_witness(const std::vector<Compression>& blocks, int n_log,
+                      std::vector<F128>& z, std::vector<F128>& a, std::vector<F128>& b);
+void apply_block_diag(const SparseRows& m0, const std::vector<F128>& z, int n_blocks,
+                      std::vector<F128>& out);
+
+// ---------------------------------------------------------------------------
+// Additive NTT over F128 (novel basis, neighbours-last) and GF(2^8) NTT.
+// ntt/additive_ntt_f128.rs:54-141,2640-2800,4766-4800; ntt.rs:22-169
+// ---------------------------------------------------------------------------
+struct AdditiveNtt {
+  int dim = 0;
+  std::vector<std::vector<F128>> evals;
+  std::vector<F128> twiddles;  // layer l at offset 2^l - 1
+  explicit AdditiveNtt(int dim);
+  F128 twiddle(int layer, size_t block) const { return twiddles[((size_t)1 << layer) - 1 + block]; }
+  void forward_interleaved(std::vector<F128>& data, size_t num_ntts, int start_layer = 0) const;
+};
+const AdditiveNtt& standard_ntt(int dim);
+// RS encode: msg (n positions x lanes) -> codeword (n * 2^rate positions x lanes)
+void rs_encode(const std::vector<F128>& msg, size_t lanes, int log_inv_rate, std::vector<F128>& cw);
+
+struct Gf8Ntt {
+  int k; std::vector<uint8_t> tw;
+  Gf8Ntt(int k, uint8_t beta);
+  void forward(uint8_t* v) const;
+  void inverse(uint8_t* v) const;
+};
+
+// ---------------------------------------------------------------------------
+// Merkle (BLAKE3 leaf/parent CVs, flat 2n-1 layout).  merkle.rs:16-21,192-240,753-1072
+// ---------------------------------------------------------------------------
+std::vector<Hash> merkle_tree(const uint8_t* data, size_t n_leaves, size_t leaf_size);
+std::vector<Hash> merkle_multi_proof(const std::vector<Hash>& tree, size_t n_leaves,
+                                     std::vector<size_t> positions);
+
+// ---------------------------------------------------------------------------
+// Sub-protocol helpers
+// ---------------------------------------------------------------------------
+std::vector<F128> build_eq(const std::vector<F128>& r);       // index bit i <-> r[i]
+std::vector<F128> lagrange_weights(int k_skip, F128 z, int node_base);
+F128 interpolate_on_lambda(const std::vector<F128>& vals, F128 z);
+F128 interpolate_combined(const std::vector<F128>& vals, F128 z);
+std::array<F128, 3> small_challenges();
+std::array<F128, 4> medium_challenges();
+std::vector<F128> eval_sk_at_vks(int log_n);
+
+// ---------------------------------------------------------------------------
+// Proof structures (serde field order) and bincode-fixint serialization.
+// crates/flock-prover/src/proof_io.rs:40-232
+// ---------------------------------------------------------------------------
+struct SumcheckMsg { F128 u0, u2; };
+struct RecursiveProof { std::vector<std::vector<F128>> opened_rows; std::vector<Hash> merkle_proof; };
+struct FinalProof { std::vector<F128> yr; std::vector<std::vector<F128>> opened_rows; std::vector<Hash> merkle_proof; };
+struct LigeritoProof {
+  Hash initial_root{};
+  RecursiveProof initial_proof;
+  std::vector<Hash> recursive_roots;
+  std::vector<RecursiveProof> recursive_proofs;
+  FinalProof final_proof;
+  std::vector<SumcheckMsg> sumcheck_transcript;
+  std::vector<uint64_t> grinding_nonces;
+  std::vector<F128> ood_values;
+  std::vector<uint64_t> fold_grinding_nonces;
+};
+struct ZerocheckProof {
+  std::vector<F128> round1_ab, round1_c;
+  std::vector<std::pair<F128, F128>> rounds;
+  F128 final_a, final_b, final_c;
+};
+struct LincheckProof { std::vector<std::pair<F128, F128>> rounds; std::vector<F128> z_partial; };
+struct Bundle {
+  Hash root{};
+  uint64_t m = 0, log_inv_rate = 1, log_batch_size = 6;
+  uint32_t profile = 0, merkle_hash = 1;  // Fast, Blake3
+  ZerocheckProof zc;
+  LincheckProof lc;
+  std::vector<std::vector<F128>> s_hat_v;  // one per ring-switched claim
+  LigeritoProof lig;
+};
+std::vector<uint8_t> serialize(const Bundle& b);
+
+struct LigeritoConfig {
+  int initial_k = 6;
+  std::vector<int> log_inv_rates, recursive_ks, queries, grinding_bits, fold_grinding_bits, ood_samples;
+  int yr_log_n = 0;
+};
+const LigeritoConfig& ligerito_config(int m);
+
+// ---------------------------------------------------------------------------
+// Full prover.  crates/flock-prover/src/prover.rs:373-473 (generic path,
+// byte-identical to Blake3Setup::prove_fast).
+// ---------------------------------------------------------------------------
+Bundle prove(const std::vector<Compression>& blocks, int n_log, const std::string& domain);
+
+}  // namespace flockref
