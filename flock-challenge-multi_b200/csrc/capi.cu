@@ -1,0 +1,299 @@
+// extern "C" boundary of libflockgpu.so (declared in include/flock_gpu.h).
+// Status codes, never exceptions across the ABI; caller-owned buffers.
+#include "../../include/flock_gpu.h"
+#include "prover.hpp"
+#include <memory>
+#include <mutex>
+
+struct flock_ctx {
+  int device = 0;
+  uint64_t budget = 0;
+  cudaStream_t st = nullptr;
+  std::string err;
+  std::mutex mu;
+};
+struct flock_setup {
+  flock_ctx* ctx = nullptr;
+  std::unique_ptr<flock::Setup> s;
+};
+
+namespace {
+template <class F>
+int guard(flock_ctx* c, F&& f) {
+  try {
+    return f();
+  } catch (const CudaError& e) {
+    if (c) c->err = e.what();
+    return FLOCK_ERR_CUDA;
+  } catch (const std::exception& e) {
+    if (c) c->err = e.what();
+    return FLOCK_ERR_INTERNAL;
+  }
+}
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  explicit DevBuf(size_t n) { CK(cudaMalloc(&p, n * sizeof(T) + 16)); }
+  ~DevBuf() { if (p) cudaFree(p); }
+};
+__global__ void k_fill(uint64_t* p, size_t n, uint64_t seed) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  p[i] = z ^ (z >> 31);
+}
+__global__ void k_mul(const f128* a, const f128* b, size_t n, f128* out) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) st(out + i, fmul(ld(a + i), ld(b + i)));
+}
+}  // namespace
+
+extern "C" {
+
+int flock_ctx_create(int device, uint64_t hbm_budget_bytes, flock_ctx** out) {
+  if (!out) return FLOCK_ERR_ARG;
+  auto* c = new flock_ctx();
+  c->device = device;
+  c->budget = hbm_budget_bytes;
+  int rc = guard(c, [&] {
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) throw std::runtime_error("no such CUDA device");
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    return FLOCK_OK;
+  });
+  if (rc) {
+    *out = nullptr;
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return FLOCK_OK;
+}
+
+void flock_ctx_destroy(flock_ctx* c) {
+  if (!c) return;
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+const char* flock_last_error(flock_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int flock_setup_create(flock_ctx* c, uint32_t log2_n, int hash, int profile, flock_setup** out) {
+  if (!c || !out) return FLOCK_ERR_ARG;
+  if (log2_n < 8 || log2_n > 20 || hash != FLOCK_HASH_BLAKE3 || profile != FLOCK_PROFILE_FAST) {
+    c->err = "unsupported setup (log2 in 8..=20, BLAKE3 Merkle hash, fast profile)";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(c, [&] {
+    auto* s = new flock_setup();
+    s->ctx = c;
+    s->s.reset(new flock::Setup(c->device, log2_n));
+    *out = s;
+    return FLOCK_OK;
+  });
+}
+
+void flock_setup_destroy(flock_setup* s) { delete s; }
+
+static int emit(flock_ctx* c, const std::vector<uint8_t>& bytes, uint8_t* out, size_t cap, size_t* out_len) {
+  if (out_len) *out_len = bytes.size();
+  if (bytes.size() > cap || !out) {
+    c->err = "output buffer too small";
+    return FLOCK_ERR_CAPACITY;
+  }
+  memcpy(out, bytes.data(), bytes.size());
+  return FLOCK_OK;
+}
+
+int flock_prove_seed(flock_setup* s, uint64_t seed, const uint8_t* domain, size_t dlen, uint8_t* out, size_t cap,
+                     size_t* out_len) {
+  if (!s || (!domain && dlen)) return FLOCK_ERR_ARG;
+  return guard(s->ctx, [&] {
+    std::string d((const char*)domain, dlen);
+    return emit(s->ctx, s->s->prove(&seed, nullptr, 0, d), out, cap, out_len);
+  });
+}
+
+int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const uint8_t* domain, size_t dlen,
+                       uint8_t* out, size_t cap, size_t* out_len) {
+  if (!s || !blocks || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (n != ((size_t)1 << s->s->log2)) {
+    s->ctx->err = "expected exactly 2^log2 compressions";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(s->ctx, [&] {
+    if (!s->s->blocks_buf) CK(cudaMalloc(&s->s->blocks_buf, n * 25 * sizeof(uint32_t)));
+    CK(cudaMemcpyAsync(s->s->blocks_buf, blocks, n * 25 * sizeof(uint32_t), cudaMemcpyHostToDevice, s->s->st));
+    std::string d((const char*)domain, dlen);
+    return emit(s->ctx, s->s->prove(nullptr, s->s->blocks_buf, n, d), out, cap, out_len);
+  });
+}
+
+int flock_statement_digest(uint32_t m, uint8_t* out32) {
+  if (!out32 || m < 17 || m > 40) return FLOCK_ERR_ARG;
+  try {
+    auto d = flock::statement_digest((int)m);
+    memcpy(out32, d.data(), 32);
+    return FLOCK_OK;
+  } catch (...) {
+    return FLOCK_ERR_INTERNAL;
+  }
+}
+
+int flock_setup_phase_ms(flock_setup* s, double* ms, int n) {
+  if (!s || !ms) return 0;
+  double t[flock::Setup::kPhases];
+  s->s->phase_times(t);
+  int k = n < flock::Setup::kPhases ? n : flock::Setup::kPhases;
+  for (int i = 0; i < k; i++) ms[i] = t[i];
+  return k;
+}
+
+int flock_witness(flock_ctx* c, uint32_t log2, uint64_t seed, uint64_t* z, uint64_t* a, uint64_t* b) {
+  if (!c || !z || !a || !b || log2 > 24) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    uint32_t slots = 1u << (log2 < 3 ? 3 : log2);
+    size_t words = (size_t)slots * 128;
+    DevBuf<f128> dz(words), da(words), db(words);
+    launch_witness_seed(seed, log2, 1u << log2, slots, dz.p, da.p, db.p, c->st);
+    CK(cudaMemcpyAsync(z, dz.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(a, da.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(b, db.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+
+int flock_ntt_rs_encode(flock_ctx* c, const uint64_t* msg, uint32_t log_msg_pos, uint32_t lanes, uint32_t rate,
+                        uint64_t* out) {
+  if (!c || !msg || !out || lanes == 0 || (lanes & (lanes - 1)) || log_msg_pos + rate > 30 || rate < 1)
+    return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    size_t n = ((size_t)lanes) << log_msg_pos, nc = n << rate;
+    DevBuf<f128> dm(n), dc(nc);
+    CK(cudaMemcpyAsync(dm.p, msg, n * 16, cudaMemcpyHostToDevice, c->st));
+    ntt_rs_encode(dm.p, dc.p, (int)log_msg_pos, (int)lanes, (int)rate, c->st);
+    CK(cudaMemcpyAsync(out, dc.p, nc * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+
+int flock_merkle_tree(flock_ctx* c, const uint8_t* data, size_t n_leaves, size_t leaf_size, uint8_t* tree_out) {
+  if (!c || !data || !tree_out || n_leaves == 0 || (n_leaves & (n_leaves - 1)) || leaf_size == 0 ||
+      leaf_size > 1024 || (leaf_size % 16))
+    return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    DevBuf<uint8_t> dd(n_leaves * leaf_size);
+    DevBuf<uint32_t> dt(8 * (2 * n_leaves - 1));
+    CK(cudaMemcpyAsync(dd.p, data, n_leaves * leaf_size, cudaMemcpyHostToDevice, c->st));
+    merkle_build(dd.p, n_leaves, leaf_size, dt.p, c->st);
+    CK(cudaMemcpyAsync(tree_out, dt.p, (2 * n_leaves - 1) * 32, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+
+int flock_sumcheck_round(flock_ctx* c, const uint64_t* f, const uint64_t* b, size_t n, uint64_t* msg_out) {
+  if (!c || !f || !b || !msg_out || n < 2 || (n & (n - 1))) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    DevBuf<f128> df(n), db(n), dout(2);
+    CK(cudaMemcpyAsync(df.p, f, n * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(db.p, b, n * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemsetAsync(dout.p, 0, 32, c->st));
+    lig_msg(df.p, db.p, n / 2, dout.p, 148 * 4, c->st);
+    CK(cudaMemcpyAsync(msg_out, dout.p, 32, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+
+int flock_pow(flock_ctx* c, const uint8_t* digest32, uint32_t bits, uint64_t* nonce) {
+  if (!c || !digest32 || !nonce || bits > 40) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    DevBuf<unsigned long long> d(1);
+    unsigned long long* h = nullptr;
+    CK(cudaMallocHost(&h, 8));
+    *nonce = pow_search(digest32, bits, c->st, d.p, h);
+    cudaFreeHost(h);
+    return FLOCK_OK;
+  });
+}
+
+int flock_f128_mul(flock_ctx* c, const uint64_t* a, const uint64_t* b, size_t n, uint64_t* out) {
+  if (!c || !a || !b || !out) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    DevBuf<f128> da(n), db(n), dout(n);
+    CK(cudaMemcpyAsync(da.p, a, n * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(db.p, b, n * 16, cudaMemcpyHostToDevice, c->st));
+    k_mul<<<(unsigned)((n + 255) / 256), 256, 0, c->st>>>(da.p, db.p, n, dout.p);
+    CK(cudaMemcpyAsync(out, dout.p, n * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+
+}  // extern "C"
+
+template <class F>
+static double time_launches(cudaStream_t st, int iters, F&& f) {
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  f();
+  CK(cudaStreamSynchronize(st));
+  CK(cudaEventRecord(e0, st));
+  for (int i = 0; i < iters; i++) f();
+  CK(cudaEventRecord(e1, st));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms / iters;
+}
+
+extern "C" {
+
+int flock_bench_ntt(flock_ctx* c, uint32_t log_msg_pos, uint32_t lanes, uint32_t rate, int iters, double* ms) {
+  if (!c || !ms || iters < 1 || lanes == 0 || rate < 1) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    size_t n = ((size_t)lanes) << log_msg_pos, nc = n << rate;
+    DevBuf<f128> dm(n), dc(nc);
+    k_fill<<<(unsigned)((2 * n + 255) / 256), 256, 0, c->st>>>((uint64_t*)dm.p, 2 * n, 1);
+    *ms = time_launches(c->st, iters, [&] { ntt_rs_encode(dm.p, dc.p, (int)log_msg_pos, (int)lanes, (int)rate, c->st); });
+    return FLOCK_OK;
+  });
+}
+
+int flock_bench_merkle(flock_ctx* c, size_t n_leaves, size_t leaf_size, int iters, double* ms) {
+  if (!c || !ms || iters < 1 || leaf_size % 16 || leaf_size > 1024) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    DevBuf<uint8_t> dd(n_leaves * leaf_size);
+    DevBuf<uint32_t> dt(8 * (2 * n_leaves - 1));
+    size_t words = n_leaves * leaf_size / 8;
+    k_fill<<<(unsigned)((words + 255) / 256), 256, 0, c->st>>>((uint64_t*)dd.p, words, 2);
+    *ms = time_launches(c->st, iters, [&] { merkle_build(dd.p, n_leaves, leaf_size, dt.p, c->st); });
+    return FLOCK_OK;
+  });
+}
+
+int flock_bench_sumcheck(flock_ctx* c, size_t n, int iters, double* ms) {
+  if (!c || !ms || iters < 1 || n < 4) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    DevBuf<f128> df(n), db(n), fo(n / 2), bo(n / 2), dout(2);
+    k_fill<<<(unsigned)((2 * n + 255) / 256), 256, 0, c->st>>>((uint64_t*)df.p, 2 * n, 3);
+    k_fill<<<(unsigned)((2 * n + 255) / 256), 256, 0, c->st>>>((uint64_t*)db.p, 2 * n, 4);
+    f128 r = mk(0x1234567890abcdefull, 0x0fedcba987654321ull);
+    *ms = time_launches(c->st, iters, [&] {
+      lig_fold_msg(df.p, db.p, fo.p, bo.p, r, n / 4, true, dout.p, 148 * 4, c->st);
+    });
+    return FLOCK_OK;
+  });
+}
+
+}  // extern "C"

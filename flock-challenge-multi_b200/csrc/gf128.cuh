@@ -1,0 +1,124 @@
+// Device arithmetic in GF(2^128) (GHASH polynomial x^128 + x^7 + x^2 + x + 1,
+// lo = coefficients x^0..x^63) and GF(2^8) (AES polynomial 0x11B).
+//
+// Field semantics follow the reference's crates/flock-core/src/field/
+// gf2_128.rs:22-265 (mul, ghash_reduce) and gf2_8.rs:20-140.  The GPU has no
+// carry-less multiplier, so a 32x32 carry-less product is built from four
+// interleaved bit classes (bit positions i mod 4) and sixteen 32x32->64
+// integer multiplies: within one class pair at most 8 partial products land
+// on a bit position, so the integer carries never reach the next same-class
+// position and the parity of every class position is exact.  64x64 and
+// 128x128 products use Karatsuba on top of it.
+#pragma once
+#include <cstdint>
+
+struct __align__(16) f128 {
+  uint64_t lo, hi;
+};
+
+__host__ __device__ __forceinline__ f128 mk(uint64_t lo, uint64_t hi) { f128 r; r.lo = lo; r.hi = hi; return r; }
+__host__ __device__ __forceinline__ f128 fx(f128 a, f128 b) { return mk(a.lo ^ b.lo, a.hi ^ b.hi); }
+__host__ __device__ __forceinline__ bool fz(f128 a) { return (a.lo | a.hi) == 0; }
+
+__device__ __forceinline__ uint64_t clmul32(uint32_t x, uint32_t y) {
+  const uint32_t m0 = 0x11111111u, m1 = 0x22222222u, m2 = 0x44444444u, m3 = 0x88888888u;
+  uint32_t x0 = x & m0, x1 = x & m1, x2 = x & m2, x3 = x & m3;
+  uint32_t y0 = y & m0, y1 = y & m1, y2 = y & m2, y3 = y & m3;
+  uint64_t z0 = ((uint64_t)x0 * y0) ^ ((uint64_t)x1 * y3) ^ ((uint64_t)x2 * y2) ^ ((uint64_t)x3 * y1);
+  uint64_t z1 = ((uint64_t)x0 * y1) ^ ((uint64_t)x1 * y0) ^ ((uint64_t)x2 * y3) ^ ((uint64_t)x3 * y2);
+  uint64_t z2 = ((uint64_t)x0 * y2) ^ ((uint64_t)x1 * y1) ^ ((uint64_t)x2 * y0) ^ ((uint64_t)x3 * y3);
+  uint64_t z3 = ((uint64_t)x0 * y3) ^ ((uint64_t)x1 * y2) ^ ((uint64_t)x2 * y1) ^ ((uint64_t)x3 * y0);
+  return (z0 & 0x1111111111111111ull) | (z1 & 0x2222222222222222ull) |
+         (z2 & 0x4444444444444444ull) | (z3 & 0x8888888888888888ull);
+}
+
+// 64x64 -> 128 carry-less product (Karatsuba over clmul32)
+__device__ __forceinline__ void clmul64(uint64_t a, uint64_t b, uint64_t& lo, uint64_t& hi) {
+  uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+  uint64_t l = clmul32(a0, b0), h = clmul32(a1, b1);
+  uint64_t m = clmul32(a0 ^ a1, b0 ^ b1) ^ l ^ h;
+  lo = l ^ (m << 32);
+  hi = h ^ (m >> 32);
+}
+
+struct u256 { uint64_t r0, r1, r2, r3; };
+
+__device__ __forceinline__ u256 mul_wide(f128 a, f128 b) {
+  uint64_t l0, l1, h0, h1, m0, m1;
+  clmul64(a.lo, b.lo, l0, l1);
+  clmul64(a.hi, b.hi, h0, h1);
+  clmul64(a.lo ^ a.hi, b.lo ^ b.hi, m0, m1);
+  m0 ^= l0 ^ h0;
+  m1 ^= l1 ^ h1;
+  u256 u;
+  u.r0 = l0;
+  u.r1 = l1 ^ m0;
+  u.r2 = h0 ^ m1;
+  u.r3 = h1;
+  return u;
+}
+
+__host__ __device__ __forceinline__ f128 reduce256(uint64_t r0, uint64_t r1, uint64_t r2, uint64_t r3) {
+  uint64_t t_lo = r2 ^ (r2 << 1) ^ (r2 << 2) ^ (r2 << 7);
+  uint64_t t_hi = r3 ^ ((r3 << 1) | (r2 >> 63)) ^ ((r3 << 2) | (r2 >> 62)) ^ ((r3 << 7) | (r2 >> 57));
+  uint64_t ov = (r3 >> 63) ^ (r3 >> 62) ^ (r3 >> 57);
+  uint64_t corr = ov ^ (ov << 1) ^ (ov << 2) ^ (ov << 7);
+  return mk(r0 ^ t_lo ^ corr, r1 ^ t_hi);
+}
+
+__device__ __forceinline__ f128 reduce(u256 u) { return reduce256(u.r0, u.r1, u.r2, u.r3); }
+__device__ __forceinline__ f128 fmul(f128 a, f128 b) { return reduce(mul_wide(a, b)); }
+__device__ __forceinline__ void acc_wide(u256& acc, u256 v) { acc.r0 ^= v.r0; acc.r1 ^= v.r1; acc.r2 ^= v.r2; acc.r3 ^= v.r3; }
+__device__ __forceinline__ u256 zero256() { u256 u; u.r0 = u.r1 = u.r2 = u.r3 = 0; return u; }
+
+// multiply by x^k (0 <= k < 64) with reduction
+__host__ __device__ __forceinline__ f128 mul_xk(f128 a, int k) {
+  if (k == 0) return a;
+  uint64_t r0 = a.lo << k, r1 = (a.hi << k) | (a.lo >> (64 - k)), r2 = a.hi >> (64 - k);
+  return reduce256(r0, r1, r2, 0);
+}
+
+__device__ __forceinline__ f128 ld(const f128* p) {
+  ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p);
+  return mk(v.x, v.y);
+}
+__device__ __forceinline__ f128 ldg(const f128* p) {
+  ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p));
+  return mk(v.x, v.y);
+}
+__device__ __forceinline__ void st(f128* p, f128 v) {
+  *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(v.lo, v.hi);
+}
+
+// ---- warp / block XOR reductions ----
+__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
+  return __shfl_xor_sync(0xffffffffu, v, m);
+}
+__device__ __forceinline__ f128 warp_xor(f128 v) {
+#pragma unroll
+  for (int m = 16; m; m >>= 1) { v.lo ^= shfl_xor64(v.lo, m); v.hi ^= shfl_xor64(v.hi, m); }
+  return v;
+}
+__device__ __forceinline__ u256 warp_xor(u256 v) {
+#pragma unroll
+  for (int m = 16; m; m >>= 1) {
+    v.r0 ^= shfl_xor64(v.r0, m); v.r1 ^= shfl_xor64(v.r1, m);
+    v.r2 ^= shfl_xor64(v.r2, m); v.r3 ^= shfl_xor64(v.r3, m);
+  }
+  return v;
+}
+// XOR into a global 128-bit slot (order-independent => deterministic)
+__device__ __forceinline__ void atomic_xor128(f128* p, f128 v) {
+  if (v.lo) atomicXor(reinterpret_cast<unsigned long long*>(&p->lo), (unsigned long long)v.lo);
+  if (v.hi) atomicXor(reinterpret_cast<unsigned long long*>(&p->hi), (unsigned long long)v.hi);
+}
+
+// ---- GF(2^8) ----
+__host__ __device__ __forceinline__ uint8_t gf8_mul_slow(uint8_t a, uint8_t b) {
+  uint32_t acc = 0;
+  for (int i = 0; i < 8; i++)
+    if ((a >> i) & 1) acc ^= (uint32_t)b << i;
+  for (int i = 14; i >= 8; i--)
+    if ((acc >> i) & 1) acc ^= 0x11Bu << (i - 8);
+  return (uint8_t)acc;
+}

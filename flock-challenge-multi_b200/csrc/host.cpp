@@ -1,0 +1,547 @@
+// Host-side support of the B200 prover (see host.hpp).
+//  * GF(2^128)/GF(2^8): crates/flock-core/src/field/gf2_128.rs:22-265,
+//    gf2_8.rs:20-140, phi8.rs:18-1050 (carried as the images of the eight
+//    basis bytes and expanded by linearity).
+//  * BLAKE3: published specification (the reference uses the blake3 crate
+//    1.8.6 for its transcript, challenger.rs:189-307).
+//  * Transcript framing: challenger.rs:170-380 (op/kind tags, LE lengths,
+//    lo||hi F128 encoding, XOF squeeze re-absorbed).
+//  * R1CS: crates/flock-prover/src/r1cs_hashes/blake3.rs:198-262 (layout),
+//    :456-640 (build_matrices, Option-D cascade) and
+//    crates/flock-core/src/r1cs.rs:334-385 (statement digest).
+//  * Wire format: crates/flock-prover/src/proof_io.rs:40-215 (bincode 1.3
+//    fixint; enum = u32 variant index; Vec = u64 length).
+#include "host.hpp"
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <wmmintrin.h>
+#include <emmintrin.h>
+
+namespace flock {
+
+// ---------------------------------------------------------------- field --
+static inline void hclmul(uint64_t a, uint64_t b, uint64_t& lo, uint64_t& hi) {
+  __m128i r = _mm_clmulepi64_si128(_mm_set_epi64x(0, (long long)a), _mm_set_epi64x(0, (long long)b), 0);
+  lo = (uint64_t)_mm_cvtsi128_si64(r);
+  hi = (uint64_t)_mm_cvtsi128_si64(_mm_unpackhi_epi64(r, r));
+}
+
+f128 hmul(f128 a, f128 b) {
+  uint64_t l0, l1, h0, h1, m0, m1;
+  hclmul(a.lo, b.lo, l0, l1);
+  hclmul(a.hi, b.hi, h0, h1);
+  hclmul(a.lo ^ a.hi, b.lo ^ b.hi, m0, m1);
+  m0 ^= l0 ^ h0;
+  m1 ^= l1 ^ h1;
+  return reduce256(l0, l1 ^ m0, h0 ^ m1, h1);
+}
+
+f128 hinv(f128 a) {  // a^(2^128 - 2)
+  f128 r = hone(), s = hmul(a, a);
+  for (int i = 1; i < 128; i++) {
+    r = hmul(r, s);
+    s = hmul(s, s);
+  }
+  return r;
+}
+
+static const f128 kPhiBasis[8] = {
+    {0x0000000000000001ull, 0x0000000000000000ull}, {0x6b8330483c2e9849ull, 0x0dcb364640a222feull},
+    {0x7573da4a5f7710edull, 0x3d5bd35c94646a24ull}, {0x41a12db1f974f3acull, 0x6d58c4e181f9199full},
+    {0x5e2f716f4ede412full, 0xa72ec17764d7ced5ull}, {0x5cb10fbabcf00118ull, 0x4d52354a3a3d8c86ull},
+    {0x95ed1f57f3632d4dull, 0x553e92e8bc0ae9a7ull}, {0x512625b1f09fa87eull, 0x93252331bf042b11ull}};
+
+static std::array<f128, 256> phi_expand() {
+  std::array<f128, 256> t;
+  for (int v = 0; v < 256; v++) {
+    f128 acc = mk(0, 0);
+    for (int b = 0; b < 8; b++)
+      if (v & (1 << b)) acc = fx(acc, kPhiBasis[b]);
+    t[v] = acc;
+  }
+  return t;
+}
+static const std::array<f128, 256> kPhiArr = phi_expand();
+const f128* phi8_table() { return kPhiArr.data(); }
+
+std::vector<f128> heq(const std::vector<f128>& r) {
+  std::vector<f128> t((size_t)1 << r.size());
+  t[0] = hone();
+  for (size_t i = 0; i < r.size(); i++) {
+    size_t len = (size_t)1 << i;
+    for (size_t x = 0; x < len; x++) {
+      f128 h = hmul(t[x], r[i]);
+      t[x + len] = h;
+      t[x] = fx(t[x], h);
+    }
+  }
+  return t;
+}
+
+std::vector<f128> hlagrange(f128 z, int base) {
+  // L_i(z) = prod_{j != i} (z + s_j) / (s_i + s_j),  s_j = phi8(base + j)
+  std::vector<f128> w(64);
+  const auto& P = kPhiArr;
+  for (int i = 0; i < 64; i++) {
+    f128 num = hone(), den = hone();
+    for (int j = 0; j < 64; j++) {
+      if (j == i) continue;
+      num = hmul(num, fx(z, P[base + j]));
+      den = hmul(den, fx(P[base + i], P[base + j]));
+    }
+    w[i] = hmul(num, hinv(den));
+  }
+  return w;
+}
+
+uint8_t hgf8_mul(uint8_t a, uint8_t b) { return gf8_mul_slow(a, b); }
+
+// --------------------------------------------------------------- BLAKE3 --
+static const uint32_t kIV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
+                                0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
+static inline uint32_t ror(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+
+void b3_compress(const uint32_t cv[8], const uint32_t m[16], uint64_t ctr, uint32_t blen, uint32_t flags,
+                 uint32_t out[16]) {
+  static const uint8_t P[16] = {2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8};
+  static const uint8_t G[8][4] = {{0, 4, 8, 12}, {1, 5, 9, 13}, {2, 6, 10, 14}, {3, 7, 11, 15},
+                                  {0, 5, 10, 15}, {1, 6, 11, 12}, {2, 7, 8, 13}, {3, 4, 9, 14}};
+  uint32_t s[16], w[16];
+  memcpy(s, cv, 32);
+  memcpy(s + 8, kIV, 16);
+  s[12] = (uint32_t)ctr;
+  s[13] = (uint32_t)(ctr >> 32);
+  s[14] = blen;
+  s[15] = flags;
+  memcpy(w, m, 64);
+  for (int r = 0; r < 7; r++) {
+    for (int g = 0; g < 8; g++) {
+      uint32_t &a = s[G[g][0]], &b = s[G[g][1]], &c = s[G[g][2]], &d = s[G[g][3]];
+      a += b + w[2 * g];     d = ror(d ^ a, 16);
+      c += d;                b = ror(b ^ c, 12);
+      a += b + w[2 * g + 1]; d = ror(d ^ a, 8);
+      c += d;                b = ror(b ^ c, 7);
+    }
+    uint32_t t[16];
+    for (int i = 0; i < 16; i++) t[i] = w[P[i]];
+    memcpy(w, t, 64);
+  }
+  for (int i = 0; i < 8; i++) {
+    out[i] = s[i] ^ s[i + 8];
+    out[i + 8] = s[i + 8] ^ cv[i];
+  }
+}
+
+static void le_words(const uint8_t* b, uint32_t w[16]) {
+  for (int i = 0; i < 16; i++) w[i] = (uint32_t)b[4 * i] | (uint32_t)b[4 * i + 1] << 8 | (uint32_t)b[4 * i + 2] << 16 | (uint32_t)b[4 * i + 3] << 24;
+}
+
+B3::B3() { memcpy(cv_, kIV, 32); }
+
+void B3::chunk_done() {
+  uint32_t w[16], out[16];
+  le_words(buf_, w);
+  b3_compress(cv_, w, chunk_, 64, 2 /*CHUNK_END*/, out);
+  std::array<uint32_t, 8> cv;
+  memcpy(cv.data(), out, 32);
+  uint64_t total = ++chunk_;
+  while (!(total & 1)) {
+    uint32_t blk[16];
+    memcpy(blk, stack_.back().data(), 32);
+    memcpy(blk + 8, cv.data(), 32);
+    stack_.pop_back();
+    b3_compress(kIV, blk, 0, 64, 4 /*PARENT*/, out);
+    memcpy(cv.data(), out, 32);
+    total >>= 1;
+  }
+  stack_.push_back(cv);
+  memcpy(cv_, kIV, 32);
+  nblk_ = 0;
+  blen_ = 0;
+}
+
+void B3::update(const void* p, size_t n) {
+  const uint8_t* d = (const uint8_t*)p;
+  while (n) {
+    if (blen_ == 64) {
+      if (nblk_ == 15) {
+        chunk_done();
+      } else {
+        uint32_t w[16], out[16];
+        le_words(buf_, w);
+        b3_compress(cv_, w, chunk_, 64, nblk_ == 0 ? 1u : 0u, out);
+        memcpy(cv_, out, 32);
+        nblk_++;
+        blen_ = 0;
+      }
+    }
+    size_t take = std::min(n, 64 - blen_);
+    memcpy(buf_ + blen_, d, take);
+    blen_ += take;
+    d += take;
+    n -= take;
+  }
+}
+
+void B3::xof(uint8_t* out, size_t n) const {
+  uint32_t cv[8], w[16], o[16];
+  uint8_t blk[64] = {0};
+  memcpy(cv, cv_, 32);
+  memcpy(blk, buf_, blen_);
+  uint32_t blen = (uint32_t)blen_, flags = 2u | (nblk_ == 0 ? 1u : 0u);
+  uint64_t ctr = chunk_;
+  for (size_t i = stack_.size(); i-- > 0;) {
+    le_words(blk, w);
+    b3_compress(cv, w, ctr, blen, flags, o);
+    uint32_t pw[16];
+    memcpy(pw, stack_[i].data(), 32);
+    memcpy(pw + 8, o, 32);
+    for (int k = 0; k < 16; k++)
+      for (int j = 0; j < 4; j++) blk[4 * k + j] = (uint8_t)(pw[k] >> (8 * j));
+    memcpy(cv, kIV, 32);
+    blen = 64;
+    ctr = 0;
+    flags = 4;
+  }
+  le_words(blk, w);
+  for (uint64_t c = 0; n; c++) {
+    b3_compress(cv, w, c, blen, flags | 8u /*ROOT*/, o);
+    size_t take = std::min<size_t>(n, 64);
+    for (size_t k = 0; k < take; k++) out[k] = (uint8_t)(o[k / 4] >> (8 * (k % 4)));
+    out += take;
+    n -= take;
+  }
+}
+
+// ----------------------------------------------------------- transcript --
+static void le64(uint64_t v, uint8_t* b) { for (int i = 0; i < 8; i++) b[i] = (uint8_t)(v >> (8 * i)); }
+
+Transcript::Transcript(const std::string& domain) {
+  uint8_t op = 1, n[8];
+  le64(domain.size(), n);
+  put(&op, 1);
+  put(n, 8);
+  put(domain.data(), domain.size());
+}
+void Transcript::label(const char* s) {
+  uint8_t op = 2, n[8];
+  size_t len = strlen(s);
+  le64(len, n);
+  put(&op, 1);
+  put(n, 8);
+  put(s, len);
+}
+void Transcript::f128v(f128 v) {
+  uint8_t b[18] = {3, 1};
+  le64(v.lo, b + 2);
+  le64(v.hi, b + 10);
+  put(b, 18);
+}
+void Transcript::f128s(const f128* v, size_t n) {
+  std::vector<uint8_t> b(10 + 16 * n);
+  b[0] = 3;
+  b[1] = 2;
+  le64(n, &b[2]);
+  for (size_t i = 0; i < n; i++) {
+    le64(v[i].lo, &b[10 + 16 * i]);
+    le64(v[i].hi, &b[18 + 16 * i]);
+  }
+  put(b.data(), b.size());
+}
+void Transcript::bytes(const void* p, size_t n) {
+  uint8_t h[9] = {5};
+  le64(n, h + 1);
+  put(h, 9);
+  put(p, n);
+}
+static f128 from_le(const uint8_t* b) {
+  uint64_t lo = 0, hi = 0;
+  for (int i = 0; i < 8; i++) { lo |= (uint64_t)b[i] << (8 * i); hi |= (uint64_t)b[8 + i] << (8 * i); }
+  return mk(lo, hi);
+}
+f128 Transcript::sample() {
+  uint8_t t[2] = {4, 1}, buf[16];
+  put(t, 2);
+  h_.xof(buf, 16);
+  put(buf, 16);
+  return from_le(buf);
+}
+std::vector<f128> Transcript::sample_vec(size_t n) {
+  uint8_t t[10] = {4, 2};
+  le64(n, t + 2);
+  put(t, 10);
+  std::vector<uint8_t> buf(16 * n);
+  if (n) h_.xof(buf.data(), buf.size());
+  put(buf.data(), buf.size());
+  std::vector<f128> v(n);
+  for (size_t i = 0; i < n; i++) v[i] = from_le(&buf[16 * i]);
+  return v;
+}
+
+// ------------------------------------------------------------------ R1CS --
+namespace {
+using Set = std::vector<uint16_t>;  // sorted, square-free slot set
+Set sdiff(const Set& a, const Set& b) {
+  Set out;
+  out.reserve(a.size() + b.size());
+  std::set_symmetric_difference(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(out));
+  return out;
+}
+Set prefix(int base, int n) {  // {base, ..., base + n - 1}
+  Set s(n);
+  for (int j = 0; j < n; j++) s[j] = (uint16_t)(base + j);
+  return s;
+}
+struct SymWord {
+  std::array<Set, 32> b;
+  static SymWord slots(int base) { SymWord w; for (int i = 0; i < 32; i++) w.b[i] = {(uint16_t)(base + i)}; return w; }
+  static SymWord konst(uint32_t v) { SymWord w; for (int i = 0; i < 32; i++) if (v >> i & 1) w.b[i] = {(uint16_t)kZConst}; return w; }
+  SymWord operator^(const SymWord& o) const { SymWord w; for (int i = 0; i < 32; i++) w.b[i] = sdiff(b[i], o.b[i]); return w; }
+  SymWord rotr(int n) const { SymWord w; for (int i = 0; i < 32; i++) w.b[i] = b[(i + n) & 31]; return w; }
+};
+const int kLanes[8][4] = {{0, 4, 8, 12}, {1, 5, 9, 13}, {2, 6, 10, 14}, {3, 7, 11, 15},
+                          {0, 5, 10, 15}, {1, 6, 11, 12}, {2, 7, 8, 13}, {3, 4, 9, 14}};
+const int kPerm[16] = {2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8};
+constexpr int CV0 = 0, OUTLO = 256, MSG = 513, TLO = 1025, THI = 1057, BLEN = 1089, FLG = 1121, GS = 1153, OUTHI = 15153;
+
+// one 32-bit ADD: rows for its 31 carry slots; returns the sum word
+SymWord add(std::vector<Set>& A, std::vector<Set>& B, const SymWord& x, const SymWord& y, int cb) {
+  SymWord s;
+  for (int i = 0; i < 32; i++) {
+    Set cin = prefix(cb, i);
+    if (i < 31) {
+      A[cb + i] = sdiff(x.b[i], cin);
+      B[cb + i] = sdiff(y.b[i], cin);
+    }
+    s.b[i] = sdiff(sdiff(x.b[i], y.b[i]), cin);
+  }
+  return s;
+}
+
+void to_csr(const std::vector<Set>& rows, std::vector<uint32_t>& ptr, std::vector<uint16_t>& col) {
+  ptr.assign(rows.size() + 1, 0);
+  for (size_t r = 0; r < rows.size(); r++) ptr[r + 1] = ptr[r] + (uint32_t)rows[r].size();
+  col.resize(ptr.back());
+  for (size_t r = 0; r < rows.size(); r++) std::copy(rows[r].begin(), rows[r].end(), col.begin() + ptr[r]);
+}
+void to_csc(const std::vector<uint32_t>& ptr, const std::vector<uint16_t>& col,
+            std::vector<uint32_t>& cptr, std::vector<uint16_t>& crow) {
+  cptr.assign(kK + 1, 0);
+  for (uint16_t c : col) cptr[c + 1]++;
+  for (int c = 0; c < kK; c++) cptr[c + 1] += cptr[c];
+  crow.resize(col.size());
+  std::vector<uint32_t> fill(cptr.begin(), cptr.end() - 1);
+  for (int r = 0; r < kK; r++)
+    for (uint32_t j = ptr[r]; j < ptr[r + 1]; j++) crow[fill[col[j]]++] = (uint16_t)r;
+}
+
+Statement build() {
+  std::vector<Set> A(kK), B(kK);
+  const Set one = {(uint16_t)kZConst};
+  A[kZConst] = one;
+  B[kZConst] = one;
+  auto ident_rows = [&](int base, int n) {
+    for (int j = 0; j < n; j++) { A[base + j] = {(uint16_t)(base + j)}; B[base + j] = one; }
+  };
+  ident_rows(CV0, 256);
+  ident_rows(MSG, 512);
+  ident_rows(TLO, 128);  // counter lo/hi, block_len, flags are contiguous
+  std::array<SymWord, 16> st;
+  for (int w = 0; w < 8; w++) st[w] = SymWord::slots(CV0 + 32 * w);
+  for (int i = 0; i < 4; i++) st[8 + i] = SymWord::konst(kIV[i]);
+  st[12] = SymWord::slots(TLO);
+  st[13] = SymWord::slots(THI);
+  st[14] = SymWord::slots(BLEN);
+  st[15] = SymWord::slots(FLG);
+  int perm[16];
+  for (int i = 0; i < 16; i++) perm[i] = i;
+  for (int r = 0; r < 7; r++) {
+    for (int gi = 0; gi < 8; gi++) {
+      int g = 8 * r + gi, base = GS + 250 * g;
+      const int* L = kLanes[gi];
+      SymWord mx = SymWord::slots(MSG + 32 * perm[2 * gi]), my = SymWord::slots(MSG + 32 * perm[2 * gi + 1]);
+      SymWord a1 = add(A, B, add(A, B, st[L[0]], st[L[1]], base), mx, base + 31);
+      SymWord d1 = (st[L[3]] ^ a1).rotr(16);
+      SymWord c1 = add(A, B, st[L[2]], d1, base + 62);
+      SymWord b1 = (st[L[1]] ^ c1).rotr(12);
+      SymWord a2 = add(A, B, add(A, B, a1, b1, base + 93), my, base + 124);
+      SymWord d2 = (d1 ^ a2).rotr(8);
+      SymWord c2 = add(A, B, c1, d2, base + 155);
+      SymWord bn = (b1 ^ c2).rotr(7);
+      for (int i = 0; i < 32; i++) {
+        A[base + 186 + i] = bn.b[i];
+        B[base + 186 + i] = one;
+        A[base + 218 + i] = d2.b[i];
+        B[base + 218 + i] = one;
+      }
+      st[L[0]] = a2;
+      st[L[1]] = SymWord::slots(base + 186);
+      st[L[2]] = c2;
+      st[L[3]] = SymWord::slots(base + 218);
+    }
+    int next[16];
+    for (int i = 0; i < 16; i++) next[i] = perm[kPerm[i]];
+    memcpy(perm, next, sizeof(perm));
+  }
+  for (int w = 0; w < 8; w++) {
+    SymWord lo = st[w] ^ st[w + 8], hi = st[w + 8] ^ SymWord::slots(CV0 + 32 * w);
+    for (int i = 0; i < 32; i++) {
+      A[OUTLO + 32 * w + i] = lo.b[i];
+      B[OUTLO + 32 * w + i] = one;
+      A[OUTHI + 32 * w + i] = hi.b[i];
+      B[OUTHI + 32 * w + i] = one;
+    }
+  }
+  Statement s;
+  to_csr(A, s.a_ptr, s.a_col);
+  to_csr(B, s.b_ptr, s.b_col);
+  to_csc(s.a_ptr, s.a_col, s.at_ptr, s.at_row);
+  to_csc(s.b_ptr, s.b_col, s.bt_ptr, s.bt_row);
+  return s;
+}
+
+void put_u64(B3& h, uint64_t v) { uint8_t b[8]; le64(v, b); h.update(b, 8); }
+void put_matrix(B3& h, const std::vector<uint32_t>* ptr, const std::vector<uint16_t>* col) {
+  put_u64(h, kK);
+  put_u64(h, kK);
+  std::vector<uint8_t> buf;
+  for (int r = 0; r < kK; r++) {
+    uint32_t s = ptr ? (*ptr)[r] : (uint32_t)r, e = ptr ? (*ptr)[r + 1] : (uint32_t)r + 1;
+    buf.assign(8 * (e - s + 1), 0);
+    le64(e - s, buf.data());
+    for (uint32_t j = s; j < e; j++) le64(ptr ? (*col)[j] : (uint64_t)r, &buf[8 * (1 + j - s)]);
+    h.update(buf.data(), buf.size());
+  }
+}
+}  // namespace
+
+const Statement& blake3_statement() {
+  static std::once_flag once;
+  static std::unique_ptr<Statement> s;
+  std::call_once(once, [] { s.reset(new Statement(build())); });
+  return *s;
+}
+
+std::array<uint8_t, 32> statement_digest(int m) {
+  static std::mutex mu;
+  static std::map<int, std::array<uint8_t, 32>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(m);
+  if (it != cache.end()) return it->second;
+  const Statement& st = blake3_statement();
+  B3 h;
+  h.update("flock-r1cs-stmt-v1", 18);
+  put_u64(h, (uint64_t)m);
+  put_u64(h, kKLog);
+  put_u64(h, kKSkip);
+  uint8_t row_major = 0;
+  h.update(&row_major, 1);
+  put_matrix(h, &st.a_ptr, &st.a_col);
+  put_matrix(h, &st.b_ptr, &st.b_col);
+  put_matrix(h, nullptr, nullptr);  // C = I
+  std::array<uint8_t, 32> d;
+  h.digest(d.data());
+  cache[m] = d;
+  return d;
+}
+
+// ----------------------------------------------------------------- ladder --
+namespace {
+struct Row { int rate, k, q, g, fg, ood; };
+struct Levels {
+  std::vector<Row> rows;
+  int yr;
+};
+struct Entry {
+  int m;
+  Levels lv;
+};
+const std::vector<Entry>& entries() {
+  static const std::vector<Entry> e = {
+#include "ligerito_configs.inc"
+  };
+  return e;
+}
+}  // namespace
+
+const Ladder* ladder_for(int m) {
+  static std::mutex mu;
+  static std::map<int, Ladder> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(m);
+  if (it != cache.end()) return &it->second;
+  for (const Entry& e : entries()) {
+    if (e.m != m) continue;
+    Ladder l;
+    const std::vector<Row>& rows = e.lv.rows;
+    l.initial_k = rows[0].k;
+    l.yr_log_n = e.lv.yr;
+    for (size_t i = 0; i < rows.size(); i++) {
+      l.rate.push_back(rows[i].rate);
+      if (i) l.ks.push_back(rows[i].k);
+      l.queries.push_back(rows[i].q);
+      l.grind.push_back(rows[i].g);
+      l.fold_grind.push_back(rows[i].fg);
+      l.ood.push_back(rows[i].ood);
+    }
+    return &(cache[m] = l);
+  }
+  return nullptr;
+}
+
+// ---------------------------------------------------------------- encode --
+namespace {
+struct Enc {
+  std::vector<uint8_t> o;
+  void u32(uint32_t v) { for (int i = 0; i < 4; i++) o.push_back((uint8_t)(v >> (8 * i))); }
+  void u64(uint64_t v) { for (int i = 0; i < 8; i++) o.push_back((uint8_t)(v >> (8 * i))); }
+  void f(f128 v) { u64(v.lo); u64(v.hi); }
+  void h(const H32& v) { o.insert(o.end(), v.begin(), v.end()); }
+  void fs(const std::vector<f128>& v) { u64(v.size()); for (auto& x : v) f(x); }
+  void hs(const std::vector<H32>& v) { u64(v.size()); for (auto& x : v) h(x); }
+  void pairs(const std::vector<std::pair<f128, f128>>& v) { u64(v.size()); for (auto& x : v) { f(x.first); f(x.second); } }
+  void open(const Opening& p) { u64(p.rows.size()); for (auto& r : p.rows) fs(r); hs(p.proof); }
+};
+}  // namespace
+
+std::vector<uint8_t> encode(const Proof& p) {
+  Enc e;
+  e.o.reserve(512 * 1024);
+  for (char c : std::string("FLOCK")) e.o.push_back((uint8_t)c);
+  e.o.push_back(4);
+  e.o.push_back(2);
+  e.h(p.root);
+  e.u64(p.m);
+  e.u64(1);  // log_inv_rate
+  e.u64(6);  // log_batch_size
+  e.u32(0);  // profile Fast
+  e.u32(1);  // merkle hash Blake3
+  e.fs(p.r1_ab);
+  e.fs(p.r1_c);
+  e.pairs(p.zc_rounds);
+  e.f(p.fa);
+  e.f(p.fb);
+  e.f(p.fc);
+  e.pairs(p.lc_rounds);
+  e.fs(p.z_partial);
+  e.u64(p.s_hat_v.size());
+  for (auto& s : p.s_hat_v) e.fs(s);
+  e.h(p.lig_root);
+  e.open(p.initial);
+  e.hs(p.roots);
+  e.u64(p.levels.size());
+  for (auto& l : p.levels) e.open(l);
+  e.fs(p.yr);
+  e.open(p.final_open);
+  e.pairs(p.sc_msgs);
+  e.u64(p.grind_nonces.size());
+  for (auto v : p.grind_nonces) e.u64(v);
+  e.fs(p.ood);
+  e.u64(p.fold_nonces.size());
+  for (auto v : p.fold_nonces) e.u64(v);
+  return e.o;
+}
+
+}  // namespace flock

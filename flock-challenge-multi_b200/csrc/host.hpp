@@ -1,0 +1,102 @@
+// Host-side support of the B200 prover: field ops on small vectors, the
+// BLAKE3 Fiat-Shamir transcript, the BLAKE3-compression R1CS statement, the
+// Ligerito ladder configs and the FLOCK wire format.  Everything here is
+// O(transcript) work between GPU phases; all O(witness) work is on the GPU.
+#pragma once
+#include <array>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "gf128.cuh"
+
+namespace flock {
+
+// ---- GF(2^128) on the host (PCLMULQDQ); gf2_128.rs:22-265 semantics ----
+f128 hmul(f128 a, f128 b);
+f128 hinv(f128 a);
+inline f128 hadd(f128 a, f128 b) { return fx(a, b); }
+const f128* phi8_table();              // field/phi8.rs:18-1050 (basis-expanded)
+inline const f128 hone() { return mk(1, 0); }
+std::vector<f128> heq(const std::vector<f128>& r);           // eq table, bit i <-> r[i]
+std::vector<f128> hlagrange(f128 z, int node_base);           // 64 weights over phi8 nodes
+uint8_t hgf8_mul(uint8_t a, uint8_t b);
+
+// ---- BLAKE3 hasher (incremental, root / XOF) ----
+class B3 {
+ public:
+  B3();
+  void update(const void* p, size_t n);
+  void xof(uint8_t* out, size_t n) const;
+  void digest(uint8_t out[32]) const { xof(out, 32); }
+ private:
+  void chunk_done();
+  uint32_t cv_[8];
+  uint64_t chunk_ = 0;
+  uint8_t buf_[64];
+  size_t blen_ = 0;
+  int nblk_ = 0;
+  std::vector<std::array<uint32_t, 8>> stack_;
+};
+void b3_compress(const uint32_t cv[8], const uint32_t m[16], uint64_t ctr, uint32_t blen, uint32_t flags, uint32_t out[16]);
+
+// ---- Fiat-Shamir transcript (challenger.rs:170-600) ----
+class Transcript {
+ public:
+  explicit Transcript(const std::string& domain);
+  void label(const char* s);
+  void f128v(f128 v);
+  void f128s(const f128* v, size_t n);
+  void bytes(const void* p, size_t n);
+  f128 sample();
+  std::vector<f128> sample_vec(size_t n);
+  void state_digest(uint8_t out[32]) const { h_.digest(out); }
+  void nonce(uint64_t n) { uint8_t b[8]; for (int i = 0; i < 8; i++) b[i] = (uint8_t)(n >> (8 * i)); bytes(b, 8); }
+ private:
+  void put(const void* p, size_t n) { h_.update(p, n); }
+  B3 h_;
+};
+
+// ---- R1CS statement for 2^n_log BLAKE3 compressions ----
+constexpr int kKLog = 14, kK = 1 << kKLog, kKSkip = 6, kZConst = 512, kUseful = 15409;
+struct Statement {
+  std::vector<uint32_t> a_ptr, b_ptr;    // CSR rows
+  std::vector<uint16_t> a_col, b_col;
+  std::vector<uint32_t> at_ptr, bt_ptr;  // CSC (column -> rows)
+  std::vector<uint16_t> at_row, bt_row;
+};
+const Statement& blake3_statement();     // matrices (built once per process)
+std::array<uint8_t, 32> statement_digest(int m);
+
+// ---- Ligerito fast ladder (configs/ligerito/m*_fast.toml) ----
+struct Ladder {
+  int initial_k = 6, yr_log_n = 0;
+  std::vector<int> rate, ks, queries, grind, fold_grind, ood;  // per level
+};
+const Ladder* ladder_for(int m);
+
+// ---- proof object + FLOCK v4 bincode-fixint writer (proof_io.rs:40-215) ----
+using H32 = std::array<uint8_t, 32>;
+struct Opening { std::vector<std::vector<f128>> rows; std::vector<H32> proof; };
+struct Proof {
+  H32 root{};
+  uint64_t m = 0;
+  std::vector<f128> r1_ab, r1_c;
+  std::vector<std::pair<f128, f128>> zc_rounds;
+  f128 fa{}, fb{}, fc{};
+  std::vector<std::pair<f128, f128>> lc_rounds;
+  std::vector<f128> z_partial;
+  std::vector<std::vector<f128>> s_hat_v;
+  H32 lig_root{};
+  Opening initial;
+  std::vector<H32> roots;
+  std::vector<Opening> levels;
+  std::vector<f128> yr;
+  Opening final_open;
+  std::vector<std::pair<f128, f128>> sc_msgs;
+  std::vector<uint64_t> grind_nonces, fold_nonces;
+  std::vector<f128> ood;
+};
+std::vector<uint8_t> encode(const Proof& p);
+
+}  // namespace flock

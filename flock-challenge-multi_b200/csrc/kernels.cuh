@@ -1,0 +1,61 @@
+// Launch wrappers of the prover's device kernels (K0..K9).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include "gf128.cuh"
+#include "blake3.cuh"
+
+constexpr int kK_ = 16384;  // bits per compression block (2^14)
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+#define CK(x)                                                                                   \
+  do {                                                                                          \
+    cudaError_t e_ = (x);                                                                       \
+    if (e_ != cudaSuccess)                                                                      \
+      throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_) + " @" + __FILE__ + ":" + \
+                      std::to_string(__LINE__));                                                \
+  } while (0)
+
+// K0
+void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
+                         f128* b, cudaStream_t s);
+void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a, f128* b,
+                           cudaStream_t s);
+// K1
+void ntt_rs_encode(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, cudaStream_t s);
+void ntt_forward(f128* data, int log_d, int lanes, int start_layer, cudaStream_t s);
+void ntt_transposed_encode(f128* e, f128* out, int log_msg, int log_inv_rate, cudaStream_t s);
+// K2 / K9
+void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, cudaStream_t s);
+__global__ void k_gather_nodes(const uint32_t* tree, const uint64_t* idx, size_t n, uint32_t* out);
+__global__ void k_gather_rows(const f128* cw, const uint64_t* pos, size_t n, int lanes, f128* out);
+uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, unsigned long long* d_found,
+                    unsigned long long* h_found);
+// K3..K8
+void eq_split(const f128* lo, const f128* hi, int s_bits, size_t n, f128* out, cudaStream_t s);
+void axpy(f128* out, const f128* x, f128 beta, size_t n, cudaStream_t s);
+void inner(const f128* f, const f128* g, size_t n, f128* out, int grid, cudaStream_t s);
+size_t round1_tables_size();
+void zc_round1(const f128* a, const f128* b, const f128* c, const void* tabs, const f128* eqc, size_t n_blocks,
+               f128* out, int grid, cudaStream_t s);
+void zc_msg0(const f128* a, const f128* b, const f128* lag, const f128* elo, const f128* ehi, int es, size_t n_pairs,
+             f128* out, int grid, cudaStream_t s);
+void zc_fold_msg(bool from_packed, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag,
+                 f128 rho, const f128* elo, const f128* ehi, int es, size_t n_pairs_out, bool emit, f128* out,
+                 int grid, cudaStream_t s);
+void fold_pair_final(const f128* a_in, const f128* b_in, f128 rho, f128* out, cudaStream_t s);
+void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
+             const f128* eq, f128 alpha, f128 beta, int pin, f128* comb, cudaStream_t s);
+void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, f128* zv, cudaStream_t s);
+void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s);
+void ring_shat(const f128* z, const f128* eq, size_t n, f128* out, int grid, cudaStream_t s);
+void ring_bcombined(const f128* eq0, const f128* eq1, const f128* tabs, size_t n, f128* out, int grid, cudaStream_t s);
+void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int grid, cudaStream_t s);
+void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size_t n_pairs_out, bool emit, f128* out,
+                  int grid, cudaStream_t s);

@@ -1,0 +1,154 @@
+// K2: BLAKE3 Merkle trees (leaves, parent levels, multi-proof gathers) and
+// K9: proof-of-work nonce search.
+//
+// Tree semantics: crates/flock-core/src/merkle.rs — flat 2n-1 layout
+// (:16-21), leaf = non-root BLAKE3 chaining value of the leaf bytes (one
+// chunk: blocks chained from the IV, CHUNK_START on the first, CHUNK_END on
+// the last, counter 0, no ROOT; :192-197), parent = compress(IV, l||r,
+// counter 0, 64, PARENT) (:199-203).  PoW: crates/flock-core/src/
+// challenger.rs:384-475,549-600 — the smallest nonce n such that the root
+// BLAKE3 hash of (state_digest || n_le || 0^24) has `bits` leading zero bits.
+#include "kernels.cuh"
+
+// one thread per leaf; leaf_size <= 1024 (a single BLAKE3 chunk)
+__global__ void k_merkle_leaves(const uint8_t* __restrict__ data, size_t leaf_size, size_t n_leaves,
+                                uint32_t* __restrict__ tree) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_leaves) return;
+  const uint8_t* p = data + i * leaf_size;
+  uint32_t cv[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) cv[k] = b3d::kIV[k];
+  size_t nblk = leaf_size == 0 ? 1 : (leaf_size + 63) / 64;
+  for (size_t blk = 0; blk < nblk; blk++) {
+    uint32_t m[16];
+    size_t off = blk * 64, len = leaf_size - off < 64 ? leaf_size - off : 64;
+    if (len == 64 && (((uintptr_t)(p + off)) & 15) == 0) {
+      const uint4* q = reinterpret_cast<const uint4*>(p + off);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        uint4 v = q[k];
+        m[4 * k] = v.x; m[4 * k + 1] = v.y; m[4 * k + 2] = v.z; m[4 * k + 3] = v.w;
+      }
+    } else {
+      uint8_t b[64];
+      for (int k = 0; k < 64; k++) b[k] = (size_t)k < len ? p[off + k] : 0;
+      for (int k = 0; k < 16; k++)
+        m[k] = (uint32_t)b[4 * k] | (uint32_t)b[4 * k + 1] << 8 | (uint32_t)b[4 * k + 2] << 16 | (uint32_t)b[4 * k + 3] << 24;
+    }
+    uint32_t flags = (blk == 0 ? b3d::CHUNK_START : 0) | (blk + 1 == nblk ? b3d::CHUNK_END : 0);
+    b3d::compress(cv, m, 0, (uint32_t)len, flags, cv);
+  }
+  uint4* o = reinterpret_cast<uint4*>(tree + 8 * i);
+  o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+  o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
+}
+
+__global__ void k_merkle_parents(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, size_t n_out) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_out) return;
+  const uint4* q = reinterpret_cast<const uint4*>(in + 16 * i);
+  uint32_t m[16];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    uint4 v = q[k];
+    m[4 * k] = v.x; m[4 * k + 1] = v.y; m[4 * k + 2] = v.z; m[4 * k + 3] = v.w;
+  }
+  uint32_t cv[8];
+  b3d::compress(b3d::kIV, m, 0, 64, b3d::PARENT, cv);
+  uint4* o = reinterpret_cast<uint4*>(out + 8 * i);
+  o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+  o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
+}
+
+// upper levels of a tree inside one CTA (levels of at most 1024 nodes); each
+// level is read back from global memory after the barrier that published it
+__global__ void k_merkle_top(uint32_t* tree, size_t level_start, size_t level_len) {
+  int t = threadIdx.x;
+  size_t len = level_len, start = level_start;
+  while (len > 1) {
+    size_t n = len >> 1;
+    for (size_t i = t; i < n; i += blockDim.x) {
+      uint32_t m[16], cv[8];
+      for (int k = 0; k < 16; k++) m[k] = tree[(start + 2 * i) * 8 + k];
+      b3d::compress(b3d::kIV, m, 0, 64, b3d::PARENT, cv);
+      for (int k = 0; k < 8; k++) tree[(start + len + i) * 8 + k] = cv[k];
+    }
+    __syncthreads();
+    start += len;
+    len = n;
+  }
+}
+
+void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, cudaStream_t s) {
+  k_merkle_leaves<<<(unsigned)((n_leaves + 127) / 128), 128, 0, s>>>((const uint8_t*)data, leaf_size, n_leaves, tree);
+  size_t start = 0, len = n_leaves;
+  while (len > 1024) {
+    size_t n = len >> 1;
+    k_merkle_parents<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(tree + 8 * start, tree + 8 * (start + len), n);
+    start += len;
+    len = n;
+  }
+  if (len > 1) k_merkle_top<<<1, 512, 0, s>>>(tree, start, len);
+}
+
+__global__ void k_gather_nodes(const uint32_t* __restrict__ tree, const uint64_t* __restrict__ idx, size_t n,
+                               uint32_t* __restrict__ out) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int k = 0; k < 8; k++) out[8 * i + k] = tree[idx[i] * 8 + k];
+}
+
+__global__ void k_gather_rows(const f128* __restrict__ cw, const uint64_t* __restrict__ pos, size_t n, int lanes,
+                              f128* __restrict__ out) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * lanes) return;
+  size_t q = i / lanes, l = i % lanes;
+  st(out + i, ld(cw + pos[q] * lanes + l));
+}
+
+__global__ void k_scatter(f128* __restrict__ dst, const uint64_t* __restrict__ pos, const f128* __restrict__ vals,
+                          size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) st(dst + pos[i], ld(vals + i));
+}
+namespace flock {
+void scatter(f128* dst, const uint64_t* pos, const f128* vals, size_t n, cudaStream_t s) {
+  if (n) k_scatter<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(dst, pos, vals, n);
+}
+}  // namespace flock
+
+// ---------------------------------------------------------------- PoW --
+__global__ void k_pow(uint4 d0, uint4 d1, uint32_t bits, uint64_t start, uint64_t count,
+                      unsigned long long* __restrict__ found) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint64_t n = start + i;
+  if (n >= *found) return;
+  uint32_t m[16] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w, (uint32_t)n, (uint32_t)(n >> 32), 0, 0, 0, 0, 0, 0};
+  uint32_t h[8];
+  b3d::compress(b3d::kIV, m, 0, 64, b3d::CHUNK_START | b3d::CHUNK_END | b3d::ROOT, h);
+  // leading zero bits of the 32-byte hash (byte order = LE words)
+  uint32_t full = bits >> 3, extra = bits & 7;
+  bool ok = true;
+  for (uint32_t k = 0; k < full && ok; k++) ok = ((h[k >> 2] >> (8 * (k & 3))) & 0xFF) == 0;
+  if (ok && extra) ok = ((((h[full >> 2] >> (8 * (full & 3))) & 0xFF) >> (8 - extra)) == 0);
+  if (ok) atomicMin(found, (unsigned long long)n);
+}
+
+uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, unsigned long long* d_found,
+                    unsigned long long* h_found) {
+  if (bits == 0) return 0;
+  uint4 d0, d1;
+  memcpy(&d0, digest, 16);
+  memcpy(&d1, digest + 16, 16);
+  const uint64_t chunk = 1ull << 22;
+  for (uint64_t start = 0;; start += chunk) {
+    *h_found = ~0ull;
+    CK(cudaMemcpyAsync(d_found, h_found, 8, cudaMemcpyHostToDevice, s));
+    k_pow<<<(unsigned)(chunk / 256), 256, 0, s>>>(d0, d1, bits, start, chunk, d_found);
+    CK(cudaMemcpyAsync(h_found, d_found, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (*h_found != ~0ull) return *h_found;
+  }
+}

@@ -1,0 +1,605 @@
+// Host orchestration of the B200 prover: one proof = witness -> commit ->
+// bind -> zerocheck -> lincheck -> ring switch + combine -> Ligerito open ->
+// FLOCK bytes.  All O(witness) work runs in the kernels of K0..K9 on one
+// stream; the host keeps the Fiat-Shamir transcript and exchanges only
+// round messages, challenges, roots and opened rows with the device.
+//
+// Transcript order mirrors the reference verifier, which is its
+// specification: crates/flock-core/src/verifier.rs:134-232 (bind, zerocheck,
+// lincheck, claims), zerocheck.rs:1642-1797, lincheck.rs:5880-6050,
+// pcs.rs:1861-1990, pcs/ring_switch.rs:4783-4811 and
+// pcs/ligerito.rs:11321-11834; prover-side values follow
+// crates/flock-prover/src/prover.rs:373-473 and pcs/ligerito.rs:8894-9100.
+#include "prover.hpp"
+#include <algorithm>
+#include <chrono>
+#include <set>
+
+namespace flock {
+
+namespace {
+template <class T>
+T* dalloc(size_t n) {
+  T* p = nullptr;
+  CK(cudaMalloc(&p, n * sizeof(T) + 256));
+  return p;
+}
+
+std::vector<f128> small_consts() {  // phi8(0xF7), phi8(0x53), phi8(0xB5)
+  const f128* P = phi8_table();
+  return {P[0xF7], P[0x53], P[0xB5]};
+}
+std::vector<f128> medium_consts() {  // gamma^(2^i) / (1 + gamma^(2^i))
+  std::vector<f128> v;
+  for (int sh : {1, 2, 4, 8}) {
+    f128 g = mk(1ull << sh, 0);
+    v.push_back(hmul(g, hinv(fx(hone(), g))));
+  }
+  return v;
+}
+size_t ceil_log2(size_t n) {
+  if (n <= 1) return 0;
+  size_t v = n - 1, l = 0;
+  while (v) { l++; v >>= 1; }
+  return l;
+}
+}  // namespace
+
+// ---------------------------------------------------------------- setup --
+Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
+  CK(cudaSetDevice(device));
+  n_log = std::max<int>(3, (int)log2);
+  m = kKLog + n_log;
+  lad = ladder_for(m);
+  if (!lad) throw std::runtime_error("no Ligerito configuration for this size (m = " + std::to_string(m) + ")");
+  n_words = (size_t)1 << (m - 7);
+  digest = statement_digest(m);
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  z = dalloc<f128>(n_words);
+  a = dalloc<f128>(n_words);
+  b = dalloc<f128>(n_words);
+  cw0 = dalloc<f128>(2 * n_words);
+  n_leaves0 = (size_t)1 << (m - 12);
+  tree0 = dalloc<uint32_t>(8 * (2 * n_leaves0 - 1));
+  for (int i = 0; i < 4; i++) pp[i] = dalloc<f128>(n_words);
+  eqbuf[0] = dalloc<f128>(n_words);
+  eqbuf[1] = dalloc<f128>(n_words);
+  // recursive Ligero levels
+  int n_cur = m - 7 - lad->initial_k;
+  for (size_t i = 0; i < lad->ks.size(); i++) {
+    Level L;
+    L.lanes = 1 << lad->ks[i];
+    L.log_msg_pos = n_cur - lad->ks[i];
+    L.rate = lad->rate[i + 1];
+    L.positions = (size_t)1 << (L.log_msg_pos + L.rate);
+    L.cw = dalloc<f128>(L.positions * L.lanes);
+    L.tree = dalloc<uint32_t>(8 * (2 * L.positions - 1));
+    levels.push_back(L);
+    n_cur -= lad->ks[i];
+  }
+  induce_buf = dalloc<f128>((size_t)1 << (m - 7 - lad->initial_k + lad->rate[0]));
+  out = dalloc<f128>(512);
+  tabs_r1 = dalloc<uint8_t>(round1_tables_size());
+  lag = dalloc<f128>(8 * 256);
+  elo = dalloc<f128>(1 << 13);
+  ehi = dalloc<f128>(1 << 16);
+  comb = dalloc<f128>(kK);
+  zv = dalloc<f128>(kK);
+  eq_inner = dalloc<f128>(kK);
+  bc_tabs = dalloc<f128>(2 * 16 * 256);
+  idx = dalloc<uint64_t>(1 << 16);
+  gather = dalloc<f128>(1 << 16);
+  d_found = dalloc<unsigned long long>(1);
+  CK(cudaMallocHost(&h_found, 8));
+  CK(cudaMallocHost(&h_out, 512 * sizeof(f128)));
+  CK(cudaMallocHost(&h_stage, (size_t)1 << 20));
+  const Statement& S = blake3_statement();
+  at_ptr = dalloc<uint32_t>(S.at_ptr.size());
+  bt_ptr = dalloc<uint32_t>(S.bt_ptr.size());
+  at_row = dalloc<uint16_t>(S.at_row.size());
+  bt_row = dalloc<uint16_t>(S.bt_row.size());
+  CK(cudaMemcpy(at_ptr, S.at_ptr.data(), S.at_ptr.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(bt_ptr, S.bt_ptr.data(), S.bt_ptr.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(at_row, S.at_row.data(), S.at_row.size() * 2, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(bt_row, S.bt_row.data(), S.bt_row.size() * 2, cudaMemcpyHostToDevice));
+  build_round1_tables();
+  int dev_sms = 0;
+  CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
+  sms = dev_sms;
+  for (int i = 0; i < kPhases + 1; i++) CK(cudaEventCreate(&ev[i]));
+}
+
+Setup::~Setup() {
+  cudaStreamSynchronize(st);
+  void* ptrs[] = {z, a, b, cw0, tree0, pp[0], pp[1], pp[2], pp[3], eqbuf[0], eqbuf[1], induce_buf, out, blocks_buf,
+                  tabs_r1, lag, elo, ehi, comb, zv, eq_inner, bc_tabs, idx, gather, d_found, at_ptr, bt_ptr,
+                  at_row, bt_row};
+  for (void* p : ptrs) cudaFree(p);
+  for (auto& L : levels) { cudaFree(L.cw); cudaFree(L.tree); }
+  cudaFreeHost(h_found);
+  cudaFreeHost(h_out);
+  cudaFreeHost(h_stage);
+  for (int i = 0; i < kPhases + 1; i++) cudaEventDestroy(ev[i]);
+  cudaStreamDestroy(st);
+}
+
+// Round-1 constant tables: the GF(2^8) S -> Lambda extension matrix (Lagrange
+// basis of the nodes 0..63 evaluated at 64..127), log/exp tables, phi8 and
+// the small-eq weights g(xs) with eq(r[6..9], xs) = phi8(g(xs)).
+void Setup::build_round1_tables() {
+  std::vector<uint8_t> host(round1_tables_size(), 0);
+  uint8_t(*lde)[256][64] = reinterpret_cast<uint8_t(*)[256][64]>(host.data());
+  uint8_t* exp_ = host.data() + 8 * 256 * 64;
+  uint8_t* log_ = exp_ + 512;
+  f128* phi = reinterpret_cast<f128*>(log_ + 256);
+  uint8_t* g_log = reinterpret_cast<uint8_t*>(phi + 256);
+  // generator 3 of GF(2^8)*
+  uint8_t x = 1;
+  for (int i = 0; i < 255; i++) {
+    exp_[i] = x;
+    log_[x] = (uint8_t)i;
+    x = hgf8_mul(x, 3);
+  }
+  for (int i = 255; i < 512; i++) exp_[i] = exp_[i - 255];
+  auto ginv = [&](uint8_t v) { return exp_[(255 - log_[v]) % 255]; };
+  uint8_t M[64][64];  // M[l][s] = L_s(64 + l) over nodes 0..63 in GF(2^8)
+  for (int l = 0; l < 64; l++) {
+    uint8_t pt = (uint8_t)(64 + l);
+    for (int s = 0; s < 64; s++) {
+      uint8_t num = 1, den = 1;
+      for (int j = 0; j < 64; j++) {
+        if (j == s) continue;
+        num = hgf8_mul(num, pt ^ (uint8_t)j);
+        den = hgf8_mul(den, (uint8_t)s ^ (uint8_t)j);
+      }
+      M[l][s] = hgf8_mul(num, ginv(den));
+    }
+  }
+  for (int k = 0; k < 8; k++)
+    for (int v = 0; v < 256; v++)
+      for (int l = 0; l < 64; l++) {
+        uint8_t acc = 0;
+        for (int j = 0; j < 8; j++)
+          if ((v >> j) & 1) acc ^= M[l][8 * k + j];
+        lde[k][v][l] = acc;
+      }
+  for (int v = 0; v < 256; v++) phi[v] = phi8_table()[v];
+  const uint8_t sc[3] = {0xF7, 0x53, 0xB5};
+  for (int xs = 0; xs < 8; xs++) {
+    uint8_t g = 1;
+    for (int i = 0; i < 3; i++) g = hgf8_mul(g, ((xs >> i) & 1) ? sc[i] : (uint8_t)(1 ^ sc[i]));
+    g_log[xs] = g ? log_[g] : 0xFF;
+  }
+  CK(cudaMemcpy(tabs_r1, host.data(), host.size(), cudaMemcpyHostToDevice));
+}
+
+// eq table of r into dev (length 2^|r|), as lo (<= 12 vars) x hi on the device
+void Setup::eq_table(const std::vector<f128>& r, f128* dev) {
+  size_t n = r.size();
+  int s = (int)std::min<size_t>(n, 12);
+  std::vector<f128> lo = heq(std::vector<f128>(r.begin(), r.begin() + s));
+  std::vector<f128> hi = heq(std::vector<f128>(r.begin() + s, r.end()));
+  put_eq_split(lo, hi);
+  eq_split(elo, ehi, s, (size_t)1 << n, dev, st);
+}
+
+void Setup::put_eq_split(const std::vector<f128>& lo, const std::vector<f128>& hi) {
+  if (hi.size() > (1u << 16) || lo.size() > (1u << 13)) throw std::runtime_error("eq split too large");
+  CK(cudaMemcpyAsync(elo, lo.data(), lo.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ehi, hi.data(), hi.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
+  // host vectors must stay alive until the copies complete
+  CK(cudaStreamSynchronize(st));
+}
+
+void Setup::fetch(const f128* dev, size_t n, f128* host) {
+  CK(cudaMemcpyAsync(host, dev, n * sizeof(f128), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+}
+
+uint64_t Setup::grind(Transcript& tr, uint32_t bits) {
+  uint64_t nonce = 0;
+  if (bits) {
+    uint8_t d[32];
+    tr.state_digest(d);
+    nonce = pow_search(d, bits, st, d_found, h_found);
+  }
+  tr.nonce(nonce);
+  return nonce;
+}
+
+std::vector<size_t> Setup::sample_queries(Transcript& tr, size_t block_len, size_t count) {
+  std::vector<size_t> q;
+  std::set<size_t> seen;
+  while (q.size() < count) {
+    size_t v = (size_t)(tr.sample().lo % block_len);
+    if (seen.insert(v).second) q.push_back(v);
+  }
+  std::sort(q.begin(), q.end());
+  return q;
+}
+
+// Opened rows + Merkle multi-proof (merkle.rs:1074-1120 index order).
+Opening Setup::open(const f128* cw, const uint32_t* tree, size_t n_leaves, int lanes, const std::vector<size_t>& q) {
+  Opening o;
+  std::vector<uint64_t> pos(q.begin(), q.end());
+  CK(cudaMemcpyAsync(idx, pos.data(), pos.size() * 8, cudaMemcpyHostToDevice, st));
+  size_t nr = q.size() * lanes;
+  k_gather_rows<<<(unsigned)((nr + 255) / 256), 256, 0, st>>>(cw, idx, q.size(), lanes, gather);
+  std::vector<f128> rows(nr);
+  fetch(gather, nr, rows.data());
+  for (size_t i = 0; i < q.size(); i++) o.rows.emplace_back(rows.begin() + i * lanes, rows.begin() + (i + 1) * lanes);
+  // sibling indices of the multi-proof
+  std::vector<uint64_t> sib;
+  std::vector<size_t> act(q);
+  size_t ls = 0, ll = n_leaves;
+  while (ll > 1) {
+    size_t w = 0, i = 0;
+    while (i < act.size()) {
+      size_t p = act[i];
+      if (i + 1 < act.size() && act[i + 1] == (p ^ 1)) i += 2;
+      else { sib.push_back(ls + (p ^ 1)); i += 1; }
+      act[w++] = p >> 1;
+    }
+    act.resize(w);
+    ls += ll;
+    ll >>= 1;
+  }
+  if (!sib.empty()) {
+    CK(cudaMemcpyAsync(idx, sib.data(), sib.size() * 8, cudaMemcpyHostToDevice, st));
+    k_gather_nodes<<<(unsigned)((sib.size() + 127) / 128), 128, 0, st>>>(tree, idx, sib.size(),
+                                                                         reinterpret_cast<uint32_t*>(gather));
+    o.proof.resize(sib.size());
+    CK(cudaMemcpyAsync(o.proof.data(), gather, sib.size() * 32, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  return o;
+}
+
+H32 Setup::root_of(const uint32_t* tree, size_t n_leaves) {
+  H32 r;
+  CK(cudaMemcpyAsync(r.data(), tree + 8 * (2 * n_leaves - 2), 32, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return r;
+}
+
+void Setup::mark(int phase) {
+  if (phase >= 0 && phase <= kPhases) CK(cudaEventRecord(ev[phase], st));
+}
+
+// -------------------------------------------------------------- prove --
+std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
+                                  const std::string& domain) {
+  Proof P;
+  P.m = (uint64_t)m;
+  const int G = sms * 4;
+  const uint32_t n_slots = 1u << n_log;
+  mark(0);
+  // ---- K0 witness
+  if (seed) launch_witness_seed(*seed, log2, 1u << log2, n_slots, z, a, b, st);
+  else launch_witness_blocks(blocks_dev, (uint32_t)n_blocks, n_slots, z, a, b, st);
+  CK(cudaGetLastError());
+  mark(1);
+  // ---- K1 + K2 commit: 64 interleaved lanes, rate 1/2, 1 KiB leaves
+  ntt_rs_encode(z, cw0, m - 13, 64, 1, st);
+  merkle_build(cw0, n_leaves0, 64 * 16, tree0, st);
+  P.root = root_of(tree0, n_leaves0);
+  mark(2);
+
+  Transcript tr(domain);
+  tr.label("flock-r1cs-v0");
+  tr.bytes(digest.data(), 32);
+  tr.bytes(P.root.data(), 32);
+
+  // ---- zerocheck
+  tr.label("flock-zerocheck-v0");
+  std::vector<f128> r = tr.sample_vec(6);
+  std::vector<f128> r_outer = tr.sample_vec(m - 13);
+  for (f128 v : small_consts()) r.push_back(v);
+  std::vector<f128> med = medium_consts();
+  for (f128 v : med) r.push_back(v);
+  r.insert(r.end(), r_outer.begin(), r_outer.end());
+  {
+    f128 C = hone();
+    for (f128 bm : med) C = hmul(C, fx(hone(), bm));
+    std::vector<f128> rh(r.begin() + 13, r.end());
+    int s = (int)std::min<size_t>(rh.size(), 12);
+    std::vector<f128> lo = heq(std::vector<f128>(rh.begin(), rh.begin() + s));
+    std::vector<f128> hi = heq(std::vector<f128>(rh.begin() + s, rh.end()));
+    for (auto& v : hi) v = hmul(v, C);
+    put_eq_split(lo, hi);
+    eq_split(elo, ehi, s, (size_t)1 << rh.size(), scratch_eq(), st);
+    CK(cudaMemsetAsync(out, 0, 128 * sizeof(f128), st));
+    size_t n_blocks128 = (size_t)1 << (m - 13);
+    zc_round1(a, b, z, tabs_r1, scratch_eq(), n_blocks128, out, sms, st);
+    fetch(out, 128, h_out);
+    P.r1_ab.assign(h_out, h_out + 64);
+    P.r1_c.assign(h_out + 64, h_out + 128);
+  }
+  mark(3);
+  tr.f128s(P.r1_ab.data(), 64);
+  tr.f128s(P.r1_c.data(), 64);
+  f128 zc_z = tr.sample();
+  {
+    std::vector<f128> L = hlagrange(zc_z, 0);
+    std::vector<f128> lagt(8 * 256);
+    for (int k = 0; k < 8; k++)
+      for (int v = 0; v < 256; v++) {
+        f128 acc = mk(0, 0);
+        for (int j = 0; j < 8; j++)
+          if ((v >> j) & 1) acc = fx(acc, L[8 * k + j]);
+        lagt[k * 256 + v] = acc;
+      }
+    CK(cudaMemcpyAsync(lag, lagt.data(), lagt.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
+    std::vector<f128> LL = hlagrange(zc_z, 64);
+    f128 ce = mk(0, 0);
+    for (int i = 0; i < 64; i++) ce = fx(ce, hmul(LL[i], P.r1_c[i]));
+    P.fc = ce;
+    CK(cudaStreamSynchronize(st));
+  }
+  const int n_mlv = m - 6;
+  std::vector<f128> rhos;
+  auto set_eq = [&](int from) -> int {  // eq over r[from..m) as lo x hi; returns lo bits
+    std::vector<f128> rs(r.begin() + from, r.end());
+    int s = (int)std::min<size_t>(rs.size(), 12);
+    put_eq_split(heq(std::vector<f128>(rs.begin(), rs.begin() + s)), heq(std::vector<f128>(rs.begin() + s, rs.end())));
+    return s;
+  };
+  {
+    int es = set_eq(7);
+    CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
+    zc_msg0(a, b, lag, elo, ehi, es, n_words, out, G, st);
+    fetch(out, 2, h_out);
+  }
+  f128* av = pp[0];
+  f128* bv = pp[1];
+  f128* av2 = pp[2];
+  f128* bv2 = pp[3];
+  for (int i = 0; i < n_mlv; i++) {
+    P.zc_rounds.push_back({h_out[0], h_out[1]});
+    tr.f128v(h_out[0]);
+    tr.f128v(h_out[1]);
+    f128 rho = tr.sample();
+    rhos.push_back(rho);
+    if (i < n_mlv - 1) {
+      int es = set_eq(8 + i);
+      size_t n_pairs_out = (size_t)1 << (n_mlv - i - 2);
+      CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
+      if (i == 0) zc_fold_msg(true, a, b, av, bv, lag, rho, elo, ehi, es, n_pairs_out, true, out, G, st);
+      else {
+        zc_fold_msg(false, av, bv, av2, bv2, lag, rho, elo, ehi, es, n_pairs_out, true, out, G, st);
+        std::swap(av, av2);
+        std::swap(bv, bv2);
+      }
+      fetch(out, 2, h_out);
+    } else {
+      fold_pair_final(av, bv, rho, out, st);
+      fetch(out, 2, h_out);
+      P.fa = h_out[0];
+      P.fb = h_out[1];
+    }
+  }
+  tr.f128v(P.fa);
+  tr.f128v(P.fb);
+  mark(4);
+
+  // ---- lincheck
+  const int ir = kKLog - kKSkip;
+  std::vector<f128> x_inner(rhos.begin(), rhos.begin() + ir), x_outer(rhos.begin() + ir, rhos.end());
+  tr.label("flock-lincheck-v0");
+  f128 alpha = tr.sample();
+  f128 beta = tr.sample();
+  {
+    std::vector<f128> L = hlagrange(zc_z, 0), er = heq(x_inner), ei(kK);
+    for (size_t k = 0; k < er.size(); k++)
+      for (int s = 0; s < 64; s++) ei[s + 64 * k] = hmul(L[s], er[k]);
+    CK(cudaMemcpyAsync(eq_inner, ei.data(), kK * sizeof(f128), cudaMemcpyHostToDevice, st));
+    lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, kZConst, comb, st);
+    eq_table(x_outer, scratch_eq());
+    CK(cudaMemsetAsync(zv, 0, kK * sizeof(f128), st));
+    lc_zvec(z, scratch_eq(), (size_t)1 << (m - kKLog), zv, st);
+    CK(cudaStreamSynchronize(st));
+  }
+  std::vector<f128> rr;
+  int len = kK;
+  lc_round(comb, zv, len, false, mk(0, 0), true, out, st);
+  for (int k = 0; k < ir; k++) {
+    fetch(out, 2, h_out);
+    P.lc_rounds.push_back({h_out[0], h_out[1]});
+    tr.f128v(h_out[0]);
+    tr.f128v(h_out[1]);
+    f128 rk = tr.sample();
+    rr.push_back(rk);
+    len >>= 1;
+    lc_round(comb, zv, len, true, rk, k + 1 < ir, out, st);
+  }
+  P.z_partial.resize(64);
+  fetch(zv, 64, P.z_partial.data());
+  tr.f128s(P.z_partial.data(), 64);
+  f128 r_skip2 = tr.sample();
+  std::vector<f128> r_inner_rest(rr.rbegin(), rr.rend());
+  (void)r_skip2;
+  mark(5);
+
+  // ---- PCS open: ring switches + combine
+  tr.label("flock-pcs-open-batch-v0");
+  std::vector<f128> x_ab = r_inner_rest;
+  x_ab.insert(x_ab.end(), x_outer.begin(), x_outer.end());
+  std::vector<f128> x_c(r.begin() + 6, r.end());
+  std::vector<f128> eqdd[2];
+  f128 claim[2];
+  for (int k = 0; k < 2; k++) {
+    const std::vector<f128>& xf = k == 0 ? x_ab : x_c;
+    tr.label("flock-ring-switch-v0");
+    eq_table(std::vector<f128>(xf.begin() + 1, xf.end()), eqbuf[k]);
+    CK(cudaMemsetAsync(out, 0, 128 * sizeof(f128), st));
+    ring_shat(z, eqbuf[k], n_words, out, sms * 8, st);
+    std::vector<f128> sv(128);
+    fetch(out, 128, sv.data());
+    P.s_hat_v.push_back(sv);
+    tr.f128s(sv.data(), 128);
+    std::vector<f128> rdp = tr.sample_vec(7);
+    eqdd[k] = heq(rdp);
+    // s_hat_u[b] bit i = bit b of s_hat_v[i];  claim = sum_b s_hat_u[b] eq''[b]
+    f128 c = mk(0, 0);
+    for (int bb = 0; bb < 128; bb++) {
+      f128 u = mk(0, 0);
+      for (int i = 0; i < 128; i++) {
+        uint64_t bit = bb < 64 ? (sv[i].lo >> bb) & 1 : (sv[i].hi >> (bb - 64)) & 1;
+        if (bit) { if (i < 64) u.lo |= 1ull << i; else u.hi |= 1ull << (i - 64); }
+      }
+      c = fx(c, hmul(u, eqdd[k][bb]));
+    }
+    claim[k] = c;
+  }
+  f128 gam[2] = {tr.sample(), tr.sample()};
+  f128 target = fx(hmul(gam[0], claim[0]), hmul(gam[1], claim[1]));
+  {
+    std::vector<f128> T(2 * 16 * 256);
+    for (int k = 0; k < 2; k++) {
+      std::vector<f128> sc(128);
+      for (int bb = 0; bb < 128; bb++) sc[bb] = hmul(gam[k], eqdd[k][bb]);
+      for (int byte = 0; byte < 16; byte++)
+        for (int v = 0; v < 256; v++) {
+          f128 acc = mk(0, 0);
+          for (int j = 0; j < 8; j++)
+            if ((v >> j) & 1) acc = fx(acc, sc[8 * byte + j]);
+          T[(size_t)k * 4096 + byte * 256 + v] = acc;
+        }
+    }
+    CK(cudaMemcpyAsync(bc_tabs, T.data(), T.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
+    ring_bcombined(eqbuf[0], eqbuf[1], bc_tabs, n_words, pp[1], sms * 2, st);
+    CK(cudaStreamSynchronize(st));
+  }
+  mark(6);
+
+  // ---- Ligerito
+  const Ladder& Ld = *lad;
+  tr.label("flock-ligerito-basis-v0");
+  tr.f128v(target);
+  tr.bytes(P.root.data(), 32);
+  P.lig_root = P.root;
+  f128* f = z;       // current f, b
+  f128* bb = pp[1];
+  f128* fo = pp[2];
+  f128* bo = pp[3];
+  size_t flen = n_words;
+  auto push_msg = [&]() {
+    fetch(out, 2, h_out);
+    P.sc_msgs.push_back({h_out[0], h_out[1]});
+    tr.f128v(h_out[0]);
+    tr.f128v(h_out[1]);
+  };
+  CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
+  lig_msg(f, bb, flen / 2, out, G, st);
+  push_msg();
+  auto fold_round = [&](int bits) -> f128 {
+    if (bits > 0) P.fold_nonces.push_back(grind(tr, (uint32_t)bits));
+    f128 rch = tr.sample();
+    CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
+    lig_fold_msg(f, bb, fo, bo, rch, flen / 4, true, out, G, st);
+    // after the first fold f lives in the ping-pong pair (pp[0], pp[2]) / (pp[1], pp[3])
+    if (f == z) { f = fo; fo = pp[0]; }
+    else std::swap(f, fo);
+    std::swap(bb, bo);
+    flen /= 2;
+    push_msg();
+    return rch;
+  };
+  auto introduce = [&](const f128* bnew) {
+    CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
+    lig_msg(f, bnew, flen / 2, out, G, st);
+    push_msg();
+    f128 be = tr.sample();
+    axpy(bb, bnew, be, flen, st);
+  };
+  int n_cur = m - 7;
+  auto do_ood = [&](int count) {
+    for (int s = 0; s < count; s++) {
+      std::vector<f128> zp = tr.sample_vec((size_t)n_cur);
+      f128* eqz = scratch_eq();
+      eq_table(zp, eqz);
+      CK(cudaMemsetAsync(out, 0, sizeof(f128), st));
+      inner(f, eqz, flen, out, G, st);
+      f128 y;
+      fetch(out, 1, &y);
+      P.ood.push_back(y);
+      tr.f128v(y);
+      introduce(eqz);
+    }
+  };
+  // induced basis of a queried level: transposed RS encoding of the
+  // alpha-weighted query indicator, restricted to the message (n_cur vars)
+  auto induce = [&](const std::vector<size_t>& q, const std::vector<f128>& alpha_v, int rate) {
+    std::vector<f128> eqa = heq(alpha_v);
+    size_t dlen = (size_t)1 << (n_cur + rate);
+    CK(cudaMemsetAsync(induce_buf, 0, dlen * sizeof(f128), st));
+    std::vector<uint64_t> qp(q.begin(), q.end());
+    CK(cudaMemcpyAsync(idx, qp.data(), qp.size() * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(gather, eqa.data(), q.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
+    scatter(induce_buf, idx, gather, q.size(), st);
+    f128* bind = scratch_eq();
+    ntt_transposed_encode(induce_buf, bind, n_cur, rate, st);
+    CK(cudaStreamSynchronize(st));
+    introduce(bind);
+  };
+
+  std::vector<f128> lane_rs;
+  for (int j = 0; j < Ld.initial_k; j++) lane_rs.push_back(fold_round(std::max(0, Ld.fold_grind[0] - j)));
+  n_cur -= Ld.initial_k;
+  mark(7);
+  // level 1 commit
+  auto commit = [&](Level& L) {
+    ntt_rs_encode(f, L.cw, L.log_msg_pos, L.lanes, L.rate, st);
+    merkle_build(L.cw, L.positions, (size_t)L.lanes * 16, L.tree, st);
+    H32 rt = root_of(L.tree, L.positions);
+    P.roots.push_back(rt);
+    tr.bytes(rt.data(), 32);
+  };
+  commit(levels[0]);
+  do_ood(Ld.ood.size() > 1 ? Ld.ood[1] : 0);
+  P.grind_nonces.push_back(grind(tr, (uint32_t)Ld.grind[0]));
+  {
+    std::vector<size_t> q0 = sample_queries(tr, n_leaves0, (size_t)Ld.queries[0]);
+    std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[0]));
+    P.initial = open(cw0, tree0, n_leaves0, 64, q0);
+    induce(q0, al, Ld.rate[0]);
+  }
+  const int rsteps = (int)Ld.ks.size();
+  for (int i = 0; i < rsteps; i++) {
+    for (int j = 0; j < Ld.ks[i]; j++) fold_round(std::max(0, Ld.fold_grind[i + 1] - j));
+    n_cur -= Ld.ks[i];
+    Level& prev = levels[i];
+    if (i == rsteps - 1) {
+      P.yr.resize(flen);
+      fetch(f, flen, P.yr.data());
+      for (f128 v : P.yr) tr.f128v(v);
+      P.grind_nonces.push_back(grind(tr, (uint32_t)Ld.grind[i + 1]));
+      std::vector<size_t> ql = sample_queries(tr, prev.positions, (size_t)Ld.queries[i + 1]);
+      tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
+      P.final_open = open(prev.cw, prev.tree, prev.positions, prev.lanes, ql);
+      tr.sample();
+      break;
+    }
+    commit(levels[i + 1]);
+    do_ood((i + 2) < (int)Ld.ood.size() ? Ld.ood[i + 2] : 0);
+    P.grind_nonces.push_back(grind(tr, (uint32_t)Ld.grind[i + 1]));
+    std::vector<size_t> qi = sample_queries(tr, prev.positions, (size_t)Ld.queries[i + 1]);
+    std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
+    P.levels.push_back(open(prev.cw, prev.tree, prev.positions, prev.lanes, qi));
+    induce(qi, al, prev.rate);
+  }
+  mark(8);
+  CK(cudaStreamSynchronize(st));
+  std::vector<uint8_t> bytes = encode(P);
+  return bytes;
+}
+
+void Setup::phase_times(double* ms) const {
+  for (int i = 0; i < kPhases; i++) {
+    float t = 0;
+    if (cudaEventElapsedTime(&t, ev[i], ev[i + 1]) != cudaSuccess) t = -1;
+    ms[i] = t;
+  }
+}
+
+}  // namespace flock

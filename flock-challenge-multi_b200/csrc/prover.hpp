@@ -1,0 +1,73 @@
+// One prover setup per (device, size): device buffers sized for 2^log2
+// compressions, the statement (CSC matrices on the device), constant tables
+// and the proof entry point.
+#pragma once
+#include <string>
+#include <vector>
+#include "host.hpp"
+#include "kernels.cuh"
+
+namespace flock {
+
+void scatter(f128* dst, const uint64_t* pos, const f128* vals, size_t n, cudaStream_t s);
+
+struct Level {
+  int lanes = 0, log_msg_pos = 0, rate = 0;
+  size_t positions = 0;
+  f128* cw = nullptr;
+  uint32_t* tree = nullptr;
+};
+
+class Setup {
+ public:
+  static constexpr int kPhases = 8;  // witness, commit, round1, zc rounds, lincheck, ring switch, L0 folds, levels
+  Setup(int device, uint32_t log2);
+  ~Setup();
+  Setup(const Setup&) = delete;
+  Setup& operator=(const Setup&) = delete;
+
+  // seed != nullptr: inputs generated on the device from the benchmark
+  // generator; otherwise blocks_dev holds n_blocks x 25 u32 on the device.
+  std::vector<uint8_t> prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
+                             const std::string& domain);
+  void phase_times(double* ms) const;
+
+  uint32_t log2 = 0;
+  int n_log = 0, m = 0, sms = 0;
+  size_t n_words = 0, n_leaves0 = 0;
+  cudaStream_t st = nullptr;
+  uint32_t* blocks_buf = nullptr;  // device staging for caller-provided compressions
+
+ private:
+  void build_round1_tables();
+  void eq_table(const std::vector<f128>& r, f128* dev);
+  void put_eq_split(const std::vector<f128>& lo, const std::vector<f128>& hi);
+  void fetch(const f128* dev, size_t n, f128* host);
+  uint64_t grind(Transcript& tr, uint32_t bits);
+  std::vector<size_t> sample_queries(Transcript& tr, size_t block_len, size_t count);
+  Opening open(const f128* cw, const uint32_t* tree, size_t n_leaves, int lanes, const std::vector<size_t>& q);
+  H32 root_of(const uint32_t* tree, size_t n_leaves);
+  void mark(int phase);
+  f128* scratch_eq() { return eqbuf[0]; }
+
+  const Ladder* lad = nullptr;
+  std::array<uint8_t, 32> digest{};
+  f128 *z = nullptr, *a = nullptr, *b = nullptr, *cw0 = nullptr;
+  uint32_t* tree0 = nullptr;
+  f128* pp[4] = {nullptr, nullptr, nullptr, nullptr};
+  f128* eqbuf[2] = {nullptr, nullptr};
+  std::vector<Level> levels;
+  f128 *induce_buf = nullptr, *out = nullptr, *lag = nullptr, *elo = nullptr, *ehi = nullptr;
+  f128 *comb = nullptr, *zv = nullptr, *eq_inner = nullptr, *bc_tabs = nullptr, *gather = nullptr;
+  uint8_t* tabs_r1 = nullptr;
+  uint64_t* idx = nullptr;
+  unsigned long long* d_found = nullptr;
+  unsigned long long* h_found = nullptr;
+  f128* h_out = nullptr;
+  uint8_t* h_stage = nullptr;
+  uint32_t *at_ptr = nullptr, *bt_ptr = nullptr;
+  uint16_t *at_row = nullptr, *bt_row = nullptr;
+  cudaEvent_t ev[kPhases + 1] = {};
+};
+
+}  // namespace flock

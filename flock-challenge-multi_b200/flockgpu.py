@@ -1,0 +1,204 @@
+"""Python binding of libflockgpu.so (the B200 Flock prover's C ABI).
+
+The C ABI (include/flock_gpu.h) is the product boundary; this module is a
+thin ctypes mirror of it, shaped like the reference worker's use of
+`Blake3Setup::new` + `prove_fast` + `to_bytes`
+(benchmark-tools/worker/src/main.rs:24-47).  There is no CPU fallback: if
+the shared library or a CUDA device is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libflockgpu.so"
+DOMAIN = b"flock-bench-v0"
+MAX_PROOF_BYTES = 500_000
+
+# every symbol include/flock_gpu.h declares
+EXPORTS = (
+    "flock_ctx_create", "flock_ctx_destroy", "flock_last_error", "flock_setup_create",
+    "flock_setup_destroy", "flock_prove_seed", "flock_prove_blocks", "flock_setup_phase_ms",
+    "flock_witness", "flock_ntt_rs_encode", "flock_merkle_tree", "flock_sumcheck_round",
+    "flock_pow", "flock_f128_mul", "flock_statement_digest", "flock_bench_ntt",
+    "flock_bench_merkle", "flock_bench_sumcheck",
+)
+PHASES = ("witness", "commit", "zerocheck_round1", "zerocheck_rounds", "lincheck",
+          "ring_switch_combine", "ligerito_l0_folds", "ligerito_levels")
+
+_lib = None
+
+
+class FlockError(RuntimeError):
+    pass
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FlockError(f"{LIB_PATH} is not built (run `make -C {HERE}`); there is no CPU fallback")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        vp, u32, u64, sz, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_int
+        lib.flock_last_error.restype = ctypes.c_char_p
+        lib.flock_last_error.argtypes = [vp]
+        lib.flock_ctx_create.argtypes = [i32, u64, ctypes.POINTER(vp)]
+        lib.flock_ctx_destroy.argtypes = [vp]
+        lib.flock_setup_create.argtypes = [vp, u32, i32, i32, ctypes.POINTER(vp)]
+        lib.flock_setup_destroy.argtypes = [vp]
+        lib.flock_prove_seed.argtypes = [vp, u64, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        lib.flock_prove_blocks.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        lib.flock_setup_phase_ms.argtypes = [vp, vp, i32]
+        lib.flock_witness.argtypes = [vp, u32, u64, vp, vp, vp]
+        lib.flock_ntt_rs_encode.argtypes = [vp, vp, u32, u32, u32, vp]
+        lib.flock_merkle_tree.argtypes = [vp, vp, sz, sz, vp]
+        lib.flock_sumcheck_round.argtypes = [vp, vp, vp, sz, vp]
+        lib.flock_pow.argtypes = [vp, vp, u32, ctypes.POINTER(u64)]
+        lib.flock_f128_mul.argtypes = [vp, vp, vp, sz, vp]
+        lib.flock_statement_digest.argtypes = [u32, vp]
+        lib.flock_bench_ntt.argtypes = [vp, u32, u32, u32, i32, ctypes.POINTER(ctypes.c_double)]
+        lib.flock_bench_merkle.argtypes = [vp, sz, sz, i32, ctypes.POINTER(ctypes.c_double)]
+        lib.flock_bench_sumcheck.argtypes = [vp, sz, i32, ctypes.POINTER(ctypes.c_double)]
+        _lib = lib
+    return _lib
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def statement_digest(m: int) -> bytes:
+    out = np.zeros(32, np.uint8)
+    if load().flock_statement_digest(m, _ptr(out)):
+        raise FlockError("statement digest failed")
+    return out.tobytes()
+
+
+class Context:
+    """One CUDA device (reference: the process-wide rayon pool + allocator)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 150 << 30):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        rc = self.lib.flock_ctx_create(device, hbm_budget_bytes, ctypes.byref(h))
+        if rc:
+            raise FlockError(f"flock_ctx_create failed ({rc}): no usable CUDA device {device}")
+        self.h = h
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc:
+            raise FlockError(f"{what} failed ({rc}): {self.lib.flock_last_error(self.h).decode()}")
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.flock_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- kernel-level entry points (host arrays in, host arrays out) ----
+    def witness(self, log2: int, seed: int):
+        words = (1 << max(log2, 3)) * 128
+        z, a, b = (np.zeros(2 * words, np.uint64) for _ in range(3))
+        self._check(self.lib.flock_witness(self.h, log2, seed, _ptr(z), _ptr(a), _ptr(b)), "witness")
+        return z, a, b
+
+    def ntt_rs_encode(self, msg: np.ndarray, log_msg_pos: int, lanes: int, log_inv_rate: int) -> np.ndarray:
+        msg = np.ascontiguousarray(msg, np.uint64)
+        assert msg.size == 2 * (lanes << log_msg_pos)
+        out = np.zeros(msg.size << log_inv_rate, np.uint64)
+        self._check(self.lib.flock_ntt_rs_encode(self.h, _ptr(msg), log_msg_pos, lanes, log_inv_rate, _ptr(out)),
+                    "ntt_rs_encode")
+        return out
+
+    def merkle_tree(self, data: np.ndarray, n_leaves: int, leaf_size: int) -> np.ndarray:
+        data = np.ascontiguousarray(data, np.uint8)
+        out = np.zeros((2 * n_leaves - 1) * 32, np.uint8)
+        self._check(self.lib.flock_merkle_tree(self.h, _ptr(data), n_leaves, leaf_size, _ptr(out)), "merkle_tree")
+        return out
+
+    def sumcheck_round(self, f: np.ndarray, b: np.ndarray) -> np.ndarray:
+        f = np.ascontiguousarray(f, np.uint64)
+        b = np.ascontiguousarray(b, np.uint64)
+        out = np.zeros(4, np.uint64)
+        self._check(self.lib.flock_sumcheck_round(self.h, _ptr(f), _ptr(b), f.size // 2, _ptr(out)), "sumcheck_round")
+        return out
+
+    def pow(self, digest: bytes, bits: int) -> int:
+        d = np.frombuffer(digest, np.uint8).copy()
+        n = ctypes.c_uint64()
+        self._check(self.lib.flock_pow(self.h, _ptr(d), bits, ctypes.byref(n)), "pow")
+        return n.value
+
+    def f128_mul(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(a, np.uint64)
+        b = np.ascontiguousarray(b, np.uint64)
+        out = np.zeros_like(a)
+        self._check(self.lib.flock_f128_mul(self.h, _ptr(a), _ptr(b), a.size // 2, _ptr(out)), "f128_mul")
+        return out
+
+    def bench_ntt(self, log_msg_pos: int, lanes: int, rate: int, iters: int = 5) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.flock_bench_ntt(self.h, log_msg_pos, lanes, rate, iters, ctypes.byref(ms)), "bench_ntt")
+        return ms.value
+
+    def bench_merkle(self, n_leaves: int, leaf_size: int, iters: int = 5) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.flock_bench_merkle(self.h, n_leaves, leaf_size, iters, ctypes.byref(ms)), "bench_merkle")
+        return ms.value
+
+    def bench_sumcheck(self, n: int, iters: int = 5) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.flock_bench_sumcheck(self.h, n, iters, ctypes.byref(ms)), "bench_sumcheck")
+        return ms.value
+
+
+class Prover:
+    """`Blake3Setup` for 2^log2 compressions with BLAKE3 Merkle hashing
+    (crates/flock-prover/src/r1cs_hashes/blake3.rs:4656-5170)."""
+
+    def __init__(self, ctx: Context, log2: int):
+        self.ctx, self.log2 = ctx, log2
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.flock_setup_create(ctx.h, log2, 1, 0, ctypes.byref(h)), "setup_create")
+        self.h = h
+        self._buf = np.zeros(MAX_PROOF_BYTES * 2, np.uint8)
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.flock_setup_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def prove_seed(self, seed: int, domain: bytes = DOMAIN) -> bytes:
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_prove_seed(self.h, seed, domain, len(domain), _ptr(self._buf), self._buf.size,
+                                           ctypes.byref(n))
+        self.ctx._check(rc, "prove_seed")
+        return self._buf[: n.value].tobytes()
+
+    def prove_blocks(self, blocks: np.ndarray, domain: bytes = DOMAIN) -> bytes:
+        blocks = np.ascontiguousarray(blocks, np.uint32).reshape(-1, 25)
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_prove_blocks(self.h, _ptr(blocks), blocks.shape[0], domain, len(domain),
+                                             _ptr(self._buf), self._buf.size, ctypes.byref(n))
+        self.ctx._check(rc, "prove_blocks")
+        return self._buf[: n.value].tobytes()
+
+    def phase_ms(self) -> dict:
+        out = np.zeros(len(PHASES), np.float64)
+        k = self.ctx.lib.flock_setup_phase_ms(self.h, _ptr(out), len(PHASES))
+        return dict(zip(PHASES[:k], out[:k].tolist()))

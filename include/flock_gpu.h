@@ -1,0 +1,93 @@
+/* C ABI of the B200 Flock prover (libflockgpu.so).
+ *
+ * The library is the drop-in replacement for the reference's proving entry
+ * point; a Rust (or any FFI) host binds these symbols.  All functions return
+ * 0 on success and a nonzero status otherwise (never unwind across the ABI);
+ * flock_last_error() describes the last failure of a context.  Output buffers
+ * are caller-owned.  One context per device; a setup is used by one thread at
+ * a time.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *  - flock_setup_create  <- Blake3Setup::new(n_blocks) + pcs_params.merkle_hash
+ *                           = Blake3 (crates/flock-prover/src/r1cs_hashes/
+ *                           blake3.rs:4706-4780, benchmark-tools/worker/src/
+ *                           main.rs:24-25)
+ *  - flock_prove_seed    <- generate_compressions(log2, seed) + prove_fast +
+ *                           R1csProofBundleLigerito::to_bytes
+ *                           (benchmark-tools/worker/src/main.rs:42-47,
+ *                           blake3.rs:4846, proof_io.rs:165)
+ *  - flock_prove_blocks  <- Blake3Setup::prove_fast(&blocks, &mut FsChallenger)
+ *                           + to_bytes (blake3.rs:4846-4990)
+ *  - flock_ntt_rs_encode <- AdditiveNttF128::standard(d) + rs_encode_interleaved
+ *                           (crates/flock-core/src/ntt/additive_ntt_f128.rs:
+ *                           2661-2670, 2785)
+ *  - flock_merkle_tree   <- merkle::merkle_tree (crates/flock-core/src/merkle.rs:753)
+ *  - flock_sumcheck_round<- ligerito round_msg_lsb (crates/flock-core/src/pcs/
+ *                           ligerito.rs:4958) and zerocheck round_pair_naive
+ *                           (zerocheck/multilinear.rs:616)
+ *  - flock_witness       <- generate_witness_with_ab_packed_and_lincheck
+ *                           (blake3.rs:4617) for the inputs of
+ *                           generate_compressions (benchmark-tools/common/src/lib.rs:25)
+ *  - flock_pow           <- FsChallenger::grind_pow (crates/flock-core/src/challenger.rs:384)
+ *  - flock_f128_mul      <- F128 * F128 (crates/flock-core/src/field/gf2_128.rs:140-165)
+ */
+#ifndef FLOCK_GPU_H
+#define FLOCK_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct flock_ctx flock_ctx;
+typedef struct flock_setup flock_setup;
+
+enum { FLOCK_OK = 0, FLOCK_ERR_ARG = 1, FLOCK_ERR_CUDA = 2, FLOCK_ERR_CAPACITY = 3, FLOCK_ERR_INTERNAL = 4 };
+enum { FLOCK_HASH_BLAKE3 = 1 };
+enum { FLOCK_PROFILE_FAST = 0 };
+
+int flock_ctx_create(int device, uint64_t hbm_budget_bytes, flock_ctx** out);
+void flock_ctx_destroy(flock_ctx* ctx);
+const char* flock_last_error(flock_ctx* ctx);
+
+/* Untimed setup for 2^log2_n compressions (8 <= log2_n <= 20). */
+int flock_setup_create(flock_ctx* ctx, uint32_t log2_n, int hash, int profile, flock_setup** out);
+void flock_setup_destroy(flock_setup* s);
+
+/* One proof; inputs generated on the GPU from `seed` exactly as the
+ * benchmark generator does.  Writes the FLOCK v4 bundle bytes. */
+int flock_prove_seed(flock_setup* s, uint64_t seed, const uint8_t* domain, size_t dlen, uint8_t* out, size_t cap,
+                     size_t* out_len);
+/* One proof over caller compressions: n x 25 u32 (cv[8], m[16], counter),
+ * block_len 64, flags 11, n == 2^log2_n. */
+int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const uint8_t* domain, size_t dlen,
+                       uint8_t* out, size_t cap, size_t* out_len);
+/* Device milliseconds of the last proof's phases (witness, commit, zerocheck
+ * round 1, zerocheck rounds, lincheck, ring switch + combine, Ligerito L0
+ * folds, Ligerito levels).  Returns the number written. */
+int flock_setup_phase_ms(flock_setup* s, double* ms, int n);
+
+/* Kernel-level entry points (host buffers). */
+int flock_witness(flock_ctx* ctx, uint32_t log2, uint64_t seed, uint64_t* z, uint64_t* a, uint64_t* b);
+int flock_ntt_rs_encode(flock_ctx* ctx, const uint64_t* msg, uint32_t log_msg_pos, uint32_t lanes,
+                        uint32_t log_inv_rate, uint64_t* out);
+int flock_merkle_tree(flock_ctx* ctx, const uint8_t* data, size_t n_leaves, size_t leaf_size, uint8_t* tree_out);
+int flock_sumcheck_round(flock_ctx* ctx, const uint64_t* f, const uint64_t* b, size_t n, uint64_t* msg_out);
+int flock_pow(flock_ctx* ctx, const uint8_t* digest32, uint32_t bits, uint64_t* nonce);
+int flock_f128_mul(flock_ctx* ctx, const uint64_t* a, const uint64_t* b, size_t n, uint64_t* out);
+/* BLAKE3 digest of the R1CS statement for m = 14 + log2 (host only; replaces
+ * BlockR1cs::statement_digest, crates/flock-core/src/r1cs.rs:334). */
+int flock_statement_digest(uint32_t m, uint8_t* out32);
+
+/* Device-resident timing of kernel microbenchmarks (inputs generated on the
+ * device, CUDA events on the launching stream; milliseconds per launch). */
+int flock_bench_ntt(flock_ctx* ctx, uint32_t log_msg_pos, uint32_t lanes, uint32_t log_inv_rate, int iters,
+                    double* ms);
+int flock_bench_merkle(flock_ctx* ctx, size_t n_leaves, size_t leaf_size, int iters, double* ms);
+int flock_bench_sumcheck(flock_ctx* ctx, size_t n, int iters, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

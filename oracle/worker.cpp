@@ -12,8 +12,10 @@
 using namespace flockref;
 
 int main(int argc, char** argv) {
-  if (argc != 4) {
-    fprintf(stderr, "usage: flockref_worker LOG2 READY_PATH PROOF_PATH\n");
+  // optional 4th argument: a directory where (seed, proof) pairs are recorded
+  // before publication, so a fixture script can pin verifier-accepted bytes
+  if (argc != 4 && argc != 5) {
+    fprintf(stderr, "usage: flockref_worker LOG2 READY_PATH PROOF_PATH [RECORD_DIR]\n");
     return 2;
   }
   int log2 = atoi(argv[1]);
@@ -30,6 +32,14 @@ int main(int argc, char** argv) {
   auto blocks = generate_compressions((uint32_t)log2, seed);
   Bundle b = prove(blocks, log2, "flock-bench-v0");
   std::vector<uint8_t> bytes = serialize(b);
+  if (argc == 5) {
+    std::string rec = std::string(argv[4]) + "/proof_" + std::to_string(log2) + "_" + std::to_string(seed) + ".bin";
+    FILE* rfp = fopen(rec.c_str(), "wb");
+    if (rfp) {
+      fwrite(bytes.data(), 1, bytes.size(), rfp);
+      fclose(rfp);
+    }
+  }
   std::string tmp = std::string(argv[3]) + ".tmp";
   FILE* pf = fopen(tmp.c_str(), "wb");
   if (!pf) return 1;

@@ -1,0 +1,84 @@
+"""Generate the golden fixtures used by the test-suite.
+
+1. phi8_table.json — the reference's PHI_8_TABLE (crates/flock-core/src/field/
+   phi8.rs:18-1050), parsed as data from the reference source.
+2. verified_proofs.json — (log2, seed, sha256, size) of oracle proofs that the
+   reference's own prebuilt trusted verifier accepted: the oracle worker is
+   driven by benchmark-tools/trusted/flock_benchmark_verifier (run as a
+   program; it draws the seed, recomputes the pristine witness and commitment
+   root and replays the full verifier) and records every (seed, proof) it
+   published.  Only proofs of trials the verifier reported `verified=true`
+   are kept.
+3. witness_digests.json — sha256 of the oracle's packed (z, a, b) for small
+   cases, so the device witness kernel is pinned without the oracle.
+
+Usage (needs the reference checkout and a built oracle):
+    python tests/golden/make_golden.py /root/reference
+"""
+import hashlib
+import json
+import re
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+
+
+def phi8(ref: Path) -> None:
+    src = (ref / "crates/flock-core/src/field/phi8.rs").read_text()
+    body = src[src.index("PHI_8_TABLE"):src.index("];")]
+    vals = re.findall(r"lo:\s*0x([0-9a-fA-F]+),\s*hi:\s*0x([0-9a-fA-F]+)", body)
+    assert len(vals) == 256
+    (HERE / "phi8_table.json").write_text(json.dumps([[lo, hi] for lo, hi in vals]))
+
+
+def verified_proofs(ref: Path) -> None:
+    verifier = ref / "benchmark-tools/trusted/flock_benchmark_verifier"
+    worker = REPO / "oracle/_build/flockref_worker"
+    out = []
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        rec = td / "rec"
+        rec.mkdir()
+        wrapper = td / "worker.sh"
+        wrapper.write_text(f'#!/bin/sh\nexec "{worker}" "$@" "{rec}"\n')
+        wrapper.chmod(0o755)
+        for log2, runs in ((8, 3), (9, 2), (10, 2)):
+            scratch = td / f"s{log2}"
+            score = td / f"score{log2}.json"
+            r = subprocess.run([str(verifier), str(wrapper), str(scratch), str(score), str(td / f"sum{log2}.md"),
+                                str(log2), "1", "0", str(runs)], capture_output=True, text=True, timeout=1800)
+            assert r.returncode == 0, r.stderr
+            metrics = json.loads(score.read_text())["metrics"]
+            assert metrics["verified"] is True and metrics["measured_runs"] == runs
+            for p in sorted(rec.glob(f"proof_{log2}_*.bin")):
+                seed = int(p.stem.split("_")[2])
+                data = p.read_bytes()
+                out.append({"log2": log2, "seed": seed, "sha256": hashlib.sha256(data).hexdigest(),
+                            "size": len(data), "verified_by": "reference trusted verifier"})
+    (HERE / "verified_proofs.json").write_text(json.dumps(out, indent=1))
+
+
+def witness_digests() -> None:
+    import ctypes
+    import numpy as np
+    lib = ctypes.CDLL(str(REPO / "oracle/_build/libflockref.so"))
+    rows = []
+    for log2, seed in ((3, 7), (4, 1), (5, 0x00C0FFEEBEEFD15C)):
+        words = (1 << log2) * 128
+        z, a, b = (np.zeros(2 * words, np.uint64) for _ in range(3))
+        lib.flockref_witness(ctypes.c_uint32(log2), ctypes.c_uint64(seed), ctypes.c_void_p(z.ctypes.data),
+                             ctypes.c_void_p(a.ctypes.data), ctypes.c_void_p(b.ctypes.data))
+        rows.append({"log2": log2, "seed": seed, "z": hashlib.sha256(z.tobytes()).hexdigest(),
+                     "a": hashlib.sha256(a.tobytes()).hexdigest(), "b": hashlib.sha256(b.tobytes()).hexdigest()})
+    (HERE / "witness_digests.json").write_text(json.dumps(rows, indent=1))
+
+
+if __name__ == "__main__":
+    ref = Path(sys.argv[1])
+    phi8(ref)
+    witness_digests()
+    verified_proofs(ref)

@@ -1,0 +1,163 @@
+"""ctypes access to the oracle (oracle/_build/libflockref.so) for the tests.
+
+The oracle is test infrastructure: a CPU restatement of the reference prover
+whose proofs the reference's trusted verifier accepts.  Only the tests,
+__graft_entry__.smoke() and bench.py's CPU-baseline / reference arm load it.
+"""
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+LIB = Path(__file__).resolve().parents[1] / "oracle/_build/libflockref.so"
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Oracle:
+    def __init__(self):
+        L = ctypes.CDLL(str(LIB))
+        vp, u32, u64, sz, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_int
+        L.flockref_prove.argtypes = [u32, u64, vp, sz, ctypes.POINTER(sz)]
+        L.flockref_f128_mul.argtypes = [vp, vp, vp]
+        L.flockref_f128_inv.argtypes = [vp, vp]
+        L.flockref_phi8_table.argtypes = [vp]
+        L.flockref_gf8_mul.argtypes = [ctypes.c_uint8, ctypes.c_uint8]
+        L.flockref_gf8_mul.restype = ctypes.c_uint8
+        L.flockref_blake3_hash.argtypes = [ctypes.c_char_p, sz, vp]
+        L.flockref_blake3_xof.argtypes = [ctypes.c_char_p, sz, vp, sz]
+        L.flockref_blake3_leaf_cv.argtypes = [ctypes.c_char_p, sz, vp]
+        L.flockref_blake3_parent_cv.argtypes = [ctypes.c_char_p, ctypes.c_char_p, vp]
+        L.flockref_generate_compressions.argtypes = [u32, u64, vp]
+        L.flockref_witness.argtypes = [u32, u64, vp, vp, vp]
+        L.flockref_apply_matrices.argtypes = [vp, i32, vp, vp]
+        L.flockref_statement_digest.argtypes = [u32, vp]
+        L.flockref_matrix_nnz.argtypes = [i32]
+        L.flockref_matrix_nnz.restype = u64
+        L.flockref_rs_encode.argtypes = [vp, sz, sz, i32, vp]
+        L.flockref_ntt_twiddles.argtypes = [i32, vp]
+        L.flockref_merkle_tree.argtypes = [vp, sz, sz, vp]
+        L.flockref_merkle_multi_proof.argtypes = [vp, sz, vp, sz, vp, sz]
+        L.flockref_merkle_multi_proof.restype = sz
+        L.flockref_build_eq.argtypes = [vp, i32, vp]
+        L.flockref_lagrange.argtypes = [vp, i32, vp]
+        L.flockref_ch_new.argtypes = [ctypes.c_char_p]
+        L.flockref_ch_new.restype = vp
+        L.flockref_ch_free.argtypes = [vp]
+        L.flockref_ch_label.argtypes = [vp, ctypes.c_char_p]
+        L.flockref_ch_observe.argtypes = [vp, vp]
+        L.flockref_ch_observe_slice.argtypes = [vp, vp, sz]
+        L.flockref_ch_bytes.argtypes = [vp, ctypes.c_char_p, sz]
+        L.flockref_ch_sample.argtypes = [vp, vp]
+        L.flockref_ch_sample_vec.argtypes = [vp, sz, vp]
+        L.flockref_ch_grind.argtypes = [vp, u32]
+        L.flockref_ch_grind.restype = u64
+        L.flockref_ch_digest.argtypes = [vp, vp]
+        L.flockref_pow_ok.argtypes = [vp, u64, u32]
+        L.flockref_time_prove.argtypes = [u32, u64, ctypes.POINTER(sz)]
+        L.flockref_time_prove.restype = ctypes.c_double
+        self.L = L
+
+    def prove(self, log2: int, seed: int) -> bytes:
+        buf = np.zeros(1 << 20, np.uint8)
+        n = ctypes.c_size_t()
+        rc = self.L.flockref_prove(log2, seed, _p(buf), buf.size, ctypes.byref(n))
+        assert rc == 0, rc
+        return buf[: n.value].tobytes()
+
+    def f128_mul(self, a, b):
+        a = np.ascontiguousarray(a, np.uint64)
+        b = np.ascontiguousarray(b, np.uint64)
+        out = np.zeros_like(a)
+        for i in range(a.size // 2):
+            self.L.flockref_f128_mul(ctypes.c_void_p(a.ctypes.data + 16 * i), ctypes.c_void_p(b.ctypes.data + 16 * i),
+                                     ctypes.c_void_p(out.ctypes.data + 16 * i))
+        return out
+
+    def phi8_table(self):
+        out = np.zeros(512, np.uint64)
+        self.L.flockref_phi8_table(_p(out))
+        return out.reshape(256, 2)
+
+    def blake3(self, data: bytes) -> bytes:
+        out = ctypes.create_string_buffer(32)
+        self.L.flockref_blake3_hash(data, len(data), out)
+        return out.raw
+
+    def xof(self, data: bytes, n: int) -> bytes:
+        out = ctypes.create_string_buffer(n)
+        self.L.flockref_blake3_xof(data, len(data), out, n)
+        return out.raw
+
+    def leaf_cv(self, data: bytes) -> bytes:
+        out = ctypes.create_string_buffer(32)
+        self.L.flockref_blake3_leaf_cv(data, len(data), out)
+        return out.raw
+
+    def parent_cv(self, l: bytes, r: bytes) -> bytes:
+        out = ctypes.create_string_buffer(32)
+        self.L.flockref_blake3_parent_cv(l, r, out)
+        return out.raw
+
+    def compressions(self, log2: int, seed: int) -> np.ndarray:
+        out = np.zeros(25 << log2, np.uint32)
+        self.L.flockref_generate_compressions(log2, seed, _p(out))
+        return out.reshape(-1, 25)
+
+    def witness(self, log2: int, seed: int):
+        words = (1 << max(log2, 3)) * 128
+        z, a, b = (np.zeros(2 * words, np.uint64) for _ in range(3))
+        self.L.flockref_witness(log2, seed, _p(z), _p(a), _p(b))
+        return z, a, b
+
+    def apply_matrices(self, z: np.ndarray, n_blocks: int):
+        a = np.zeros(n_blocks * 256, np.uint64)
+        b = np.zeros(n_blocks * 256, np.uint64)
+        self.L.flockref_apply_matrices(_p(np.ascontiguousarray(z[: n_blocks * 256])), n_blocks, _p(a), _p(b))
+        return a, b
+
+    def statement_digest(self, n_log: int) -> bytes:
+        out = np.zeros(32, np.uint8)
+        self.L.flockref_statement_digest(n_log, _p(out))
+        return out.tobytes()
+
+    def rs_encode(self, msg: np.ndarray, n_pos: int, lanes: int, rate: int) -> np.ndarray:
+        msg = np.ascontiguousarray(msg, np.uint64)
+        out = np.zeros(msg.size << rate, np.uint64)
+        self.L.flockref_rs_encode(_p(msg), n_pos, lanes, rate, _p(out))
+        return out
+
+    def merkle_tree(self, data: np.ndarray, n_leaves: int, leaf_size: int) -> np.ndarray:
+        data = np.ascontiguousarray(data, np.uint8)
+        out = np.zeros((2 * n_leaves - 1) * 32, np.uint8)
+        self.L.flockref_merkle_tree(_p(data), n_leaves, leaf_size, _p(out))
+        return out
+
+    def build_eq(self, r: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(r, np.uint64)
+        n = r.size // 2
+        out = np.zeros(2 << n, np.uint64)
+        self.L.flockref_build_eq(_p(r), n, _p(out))
+        return out
+
+    def lagrange(self, z: np.ndarray, node_base: int) -> np.ndarray:
+        z = np.ascontiguousarray(z, np.uint64)
+        out = np.zeros(128, np.uint64)
+        self.L.flockref_lagrange(_p(z), node_base, _p(out))
+        return out
+
+    def grind(self, domain: bytes, label: bytes, bits: int) -> tuple:
+        c = self.L.flockref_ch_new(domain)
+        self.L.flockref_ch_label(c, label)
+        d = np.zeros(32, np.uint8)
+        self.L.flockref_ch_digest(c, _p(d))
+        n = self.L.flockref_ch_grind(c, bits)
+        self.L.flockref_ch_free(c)
+        return d.tobytes(), n
+
+    def time_prove(self, log2: int, seed: int) -> tuple:
+        n = ctypes.c_size_t()
+        s = self.L.flockref_time_prove(log2, seed, ctypes.byref(n))
+        return s, n.value

@@ -1,0 +1,133 @@
+"""GPU parity: every kernel entry point and the full prover against the oracle
+(bit-exact; the path is pure binary-field / integer arithmetic), plus the
+golden proofs the reference's trusted verifier accepted."""
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def rng_u64(seed, n):
+    return np.random.default_rng(seed).integers(0, 2**64, n, dtype=np.uint64)
+
+
+def test_f128_mul(gpu_ctx, oracle):
+    a, b = rng_u64(1, 2 * 512), rng_u64(2, 2 * 512)
+    a[:8] = 0
+    b[8:16] = np.uint64(2**64 - 1)
+    assert np.array_equal(gpu_ctx.f128_mul(a, b), oracle.f128_mul(a, b))
+
+
+@pytest.mark.parametrize("log2,seed", [(3, 7), (4, 1), (6, 0x00C0FFEEBEEFD15C), (8, 12345)])
+def test_witness(gpu_ctx, oracle, log2, seed):
+    gz, ga, gb = gpu_ctx.witness(log2, seed)
+    oz, oa, ob = oracle.witness(log2, seed)
+    assert np.array_equal(gz, oz)
+    assert np.array_equal(ga, oa)
+    assert np.array_equal(gb, ob)
+
+
+def test_witness_golden(gpu_ctx):
+    for row in json.loads((GOLD / "witness_digests.json").read_text()):
+        z, a, b = gpu_ctx.witness(row["log2"], row["seed"])
+        assert hashlib.sha256(z.tobytes()).hexdigest() == row["z"]
+        assert hashlib.sha256(a.tobytes()).hexdigest() == row["a"]
+        assert hashlib.sha256(b.tobytes()).hexdigest() == row["b"]
+
+
+@pytest.mark.parametrize("lanes,log_pos,rate", [(1, 3, 1), (1, 12, 2), (2, 9, 1), (4, 10, 2), (8, 13, 3),
+                                                 (64, 8, 1), (64, 11, 1), (16, 12, 4), (256, 6, 1)])
+def test_ntt_rs_encode(gpu_ctx, oracle, lanes, log_pos, rate):
+    msg = rng_u64(lanes * 31 + log_pos, 2 * (lanes << log_pos))
+    got = gpu_ctx.ntt_rs_encode(msg, log_pos, lanes, rate)
+    want = oracle.rs_encode(msg, 1 << log_pos, lanes, rate)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("n_leaves,leaf_size", [(1, 64), (2, 32), (16, 48), (1024, 128), (4096, 1024), (2048, 512)])
+def test_merkle_tree(gpu_ctx, oracle, n_leaves, leaf_size):
+    data = np.random.default_rng(n_leaves + leaf_size).integers(0, 256, n_leaves * leaf_size, dtype=np.uint8)
+    assert np.array_equal(gpu_ctx.merkle_tree(data, n_leaves, leaf_size), oracle.merkle_tree(data, n_leaves, leaf_size))
+
+
+def test_sumcheck_round(gpu_ctx, oracle):
+    n = 64
+    f, b = rng_u64(5, 2 * n), rng_u64(6, 2 * n)
+    F, B = f.reshape(-1, 2), b.reshape(-1, 2)
+    u0 = np.bitwise_xor.reduce(oracle.f128_mul(F[0::2].reshape(-1), B[0::2].reshape(-1)).reshape(-1, 2), axis=0)
+    u2 = np.bitwise_xor.reduce(
+        oracle.f128_mul((F[0::2] ^ F[1::2]).reshape(-1), (B[0::2] ^ B[1::2]).reshape(-1)).reshape(-1, 2), axis=0)
+    got = gpu_ctx.sumcheck_round(f, b)
+    assert list(got) == [u0[0], u0[1], u2[0], u2[1]]
+
+
+@pytest.mark.parametrize("bits", [1, 6, 12])
+def test_pow_smallest_nonce(gpu_ctx, oracle, bits):
+    digest, nonce = oracle.grind(b"flock-bench-v0", b"gpu-pow-%d" % bits, bits)
+    assert gpu_ctx.pow(digest, bits) == nonce
+
+
+@pytest.fixture(scope="module")
+def prover8(gpu_ctx):
+    import flockgpu
+    p = flockgpu.Prover(gpu_ctx, 8)
+    yield p
+    p.close()
+
+
+def test_proof_matches_verifier_accepted_golden(prover8):
+    rows = [r for r in json.loads((GOLD / "verified_proofs.json").read_text()) if r["log2"] == 8]
+    for r in rows:
+        p = prover8.prove_seed(r["seed"])
+        assert len(p) == r["size"] and hashlib.sha256(p).hexdigest() == r["sha256"]
+
+
+def test_proof_matches_oracle_log2_8(prover8, oracle):
+    import proofparse
+    for seed in (1, 0x00C0FFEEBEEFD15C):
+        g, o = prover8.prove_seed(seed), oracle.prove(8, seed)
+        assert proofparse.first_difference(g, o) is None
+        assert g == o
+
+
+def test_prove_blocks_equals_prove_seed(prover8, oracle):
+    blocks = oracle.compressions(8, 77)
+    assert prover8.prove_blocks(blocks) == prover8.prove_seed(77)
+
+
+@pytest.mark.parametrize("log2", [9, 10, 12])
+def test_proof_matches_oracle_larger(gpu_ctx, oracle, log2):
+    import flockgpu
+    import proofparse
+    p = flockgpu.Prover(gpu_ctx, log2)
+    try:
+        g = p.prove_seed(2024 + log2)
+        o = oracle.prove(log2, 2024 + log2)
+        assert proofparse.first_difference(g, o) is None
+        assert g == o
+        assert len(g) <= flockgpu.MAX_PROOF_BYTES
+    finally:
+        p.close()
+
+
+def test_golden_larger(gpu_ctx):
+    import flockgpu
+    rows = [r for r in json.loads((GOLD / "verified_proofs.json").read_text()) if r["log2"] in (9, 10)]
+    for log2 in sorted({r["log2"] for r in rows}):
+        p = flockgpu.Prover(gpu_ctx, log2)
+        try:
+            for r in [r for r in rows if r["log2"] == log2]:
+                assert hashlib.sha256(p.prove_seed(r["seed"])).hexdigest() == r["sha256"]
+        finally:
+            p.close()
+
+
+def test_phase_times_reported(prover8):
+    prover8.prove_seed(5)
+    ph = prover8.phase_ms()
+    assert len(ph) == 8 and all(v >= 0 for v in ph.values())
