@@ -1,0 +1,263 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Flock prover: verified BLAKE3 compressions per second.
+
+A step is one complete proof of 2^18 independent BLAKE3 compressions (the
+reference's ranked workload: benchmark-tools/worker, README.md:17-31): inputs
+from the benchmark generator's seed, witness -> commit -> zerocheck ->
+lincheck -> ring switch -> Ligerito open -> FLOCK bytes.  Every proof is
+byte-identical to the oracle, whose proofs the reference's verifier accepts
+(tests/test_gpu_parity.py).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs are replicas (proofs are independent): each rank proves its
+own seeds, timing is the max over ranks of the device time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "flock-challenge-multi_b200"))
+
+LOG2 = 18
+METRIC = "verified BLAKE3 compressions/sec on 1 B200 (2^18/proof); p50/p99 proof latency served"
+PUBLISHED_CPU = 381080.0  # reference, c7i.4xlarge 16 vCPU (README.md:95-98)
+PHASE_KERNEL = {
+    # phase -> (kernel, algorithmic bytes per launch at m = 32, description)
+    "zerocheck_round1": ("k_zc_round1", 3 * (1 << 29), "reads packed a, b, c (3 x 512 MiB)"),
+    "commit": ("k_ntt_pass + k_merkle_leaves", (1 << 29) + 2 * (1 << 30) + (1 << 30) + (1 << 26),
+               "RS encode 512 MiB -> 1 GiB, leaf hashing reads 1 GiB, 64 MiB tree"),
+    "zerocheck_rounds": ("k_zc_msg0 + k_zc_fold_msg", 2 * (1 << 30) + 2 * (1 << 30) + 2 * (1 << 30),
+                         "round 0 reads a, b; folds stream 2 x 512 MiB halving"),
+    "ring_switch_combine": ("k_shat + k_bcombined", 2 * (1 << 29) * 3 + (1 << 29),
+                            "eq tables 2 x 512 MiB written/read, z read twice, b_combined 512 MiB"),
+    "ligerito_l0_folds": ("k_lig_fold_msg", 4 * (1 << 30), "6 folds over f, b (2 x 512 MiB, halving)"),
+    "lincheck": ("k_lc_zvec", 1 << 29, "reads z (512 MiB)"),
+    "witness": ("k_witness_seed", 3 * (1 << 29), "writes z, a, b (3 x 512 MiB)"),
+    "ligerito_levels": ("levels", 1 << 27, "recursive levels"),
+}
+
+
+def peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait(timeout=10)
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def host_blocks(log2: int, seed: int):
+    """Benchmark inputs on the host (benchmark-tools/common/src/lib.rs:25-37),
+    vectorised SplitMix64: draw j of compression i uses state init+(25i+j+1)g."""
+    import numpy as np
+    g = np.uint64(0x9E3779B97F4A7C15)
+    init = np.uint64((seed ^ (((log2 << 29) | (log2 >> 35)) & (2**64 - 1))) & (2**64 - 1))
+    idx = np.arange(25 << log2, dtype=np.uint64) + np.uint64(1)
+    with np.errstate(over="ignore"):
+        z = init + idx * g
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z.astype(np.uint32).reshape(-1, 25)
+
+
+def cpu_baseline_sample() -> dict:
+    """The oracle (CPU restatement of the reference prover) on a bounded sample."""
+    sys.path.insert(0, str(REPO / "tests"))
+    lib = REPO / "oracle/_build/libflockref.so"
+    if not lib.exists():
+        subprocess.run(["make", "-C", str(REPO / "oracle")], check=True, capture_output=True)
+    import oracle_lib
+    o = oracle_lib.Oracle()
+    log2 = 12
+    secs, _ = o.time_prove(log2, 1)
+    return {"value": (1 << log2) / secs, "unit": "compressions/s", "cores": 1, "kind": "port",
+            "sample": f"one 2^{log2}-compression proof by the single-threaded oracle ({secs:.1f} s); "
+                      f"the reference's published figure is {PUBLISHED_CPU:.0f} c/s on 16 vCPU"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, str(REPO / "tests"))
+    lib = REPO / "oracle/_build/libflockref.so"
+    if not lib.exists():
+        subprocess.run(["make", "-C", str(REPO / "oracle")], check=True, capture_output=True)
+    import oracle_lib
+    o = oracle_lib.Oracle()
+    log2 = 10
+    for i in range(args.warmup):
+        o.time_prove(log2, 1000 + i)
+    times = [o.time_prove(log2, 2000 + i)[0] for i in range(args.steps)]
+    tot = sum(times)
+    value = args.steps * (1 << log2) / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "compressions/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_CPU, "dtype": "gf2^128/u32",
+        "data": "synthetic (benchmark SplitMix64 generator)",
+        "config": {"workload": f"single proof of 2^{log2} BLAKE3 compressions per step (bounded CPU sample of the "
+                               f"2^18 workload)", "log2": log2, "parallelism": "cpu, 1 thread"},
+        "cpu_baseline": {"value": value, "unit": "compressions/s", "cores": 1, "kind": "port",
+                         "sample": f"{args.steps} oracle proofs of 2^{log2} compressions (the reference Rust "
+                                   f"prover cannot be built here: no cargo/rustc)"},
+        "e2e": {"value": value, "unit": "compressions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import flockgpu
+    log2 = args.log2
+    ctx = flockgpu.Context(local)
+    prover = flockgpu.Prover(ctx, log2)
+    seed_base = 0x5EED0000 + 1_000_003 * rank
+    for i in range(args.warmup):
+        prover.prove_seed(seed_base + 900 + i)
+    barrier(world)
+    sampler = ClockSampler(local)
+    total_ms, phases, launches = prover.bench(seed_base, args.steps)
+    clocks = sampler.stop()
+    max_ms = allreduce_max(total_ms, world)
+    # end to end through the public API with host inputs: H2D of the
+    # compressions, prove, D2H of the proof bytes (all inside the timed region)
+    blocks = [host_blocks(log2, seed_base + 500 + i) for i in range(args.steps)]
+    barrier(world)
+    t0 = time.perf_counter()
+    sizes = [len(prover.prove_blocks(b)) for b in blocks]
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    if rank != 0:
+        prover.close()
+        return
+    n = (1 << log2) * args.steps * world
+    value = n / (max_ms / 1e3)
+    peak, peak_kind = peaks()
+    dom = max(phases, key=phases.get)
+    kname, kbytes, kdesc = PHASE_KERNEL[dom]
+    scale = 1 << (log2 - 18) if log2 >= 18 else 1.0 / (1 << (18 - log2))
+    kbytes = int(kbytes * scale)
+    achieved = kbytes / (phases[dom] / 1e3) / 1e9
+    traffic = None
+    tfile = REPO / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(kname)
+    line = {
+        "metric": METRIC, "value": value, "unit": "compressions/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": value / PUBLISHED_CPU, "dtype": "gf2^128/u32", "data": "synthetic (benchmark SplitMix64 generator)",
+        "config": {"workload": f"single proof of 2^{log2} BLAKE3 compressions (m={14 + log2}), Ligerito fast "
+                               f"profile, BLAKE3 Merkle + transcript", "log2": log2, "proofs_per_step": 1,
+                   "parallelism": f"replicas x{world}", "l2": "working set ~5 GB per proof > 126 MB L2",
+                   "proof_bytes": sizes[0]},
+        "e2e": {"value": n / e2e_s, "unit": "compressions/s", "h2d_bytes_per_step": (1 << log2) * 100,
+                "d2h_bytes_per_step": sizes[0]},
+        "gpu_launches": int(launches),
+        "phases_ms": {k: round(v, 3) for k, v in phases.items()},
+        "roofline": {"bound": "hbm", "kernel": kname, "phase": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes": kbytes, "note": f"{kdesc}; peak {peak_kind}"},
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    print(json.dumps(line), flush=True)
+    prover.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--log2", type=int, default=LOG2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
+                                                                    int(os.environ.get("RANK", "0")), 0)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+    if world > 1 and args.impl == "ours":
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -17,6 +17,11 @@ struct flock_setup {
   std::unique_ptr<flock::Setup> s;
 };
 
+uint64_t& kernel_launch_counter() {
+  static uint64_t n = 0;
+  return n;
+}
+
 namespace {
 template <class F>
 int guard(flock_ctx* c, F&& f) {
@@ -278,6 +283,39 @@ int flock_bench_merkle(flock_ctx* c, size_t n_leaves, size_t leaf_size, int iter
     size_t words = n_leaves * leaf_size / 8;
     k_fill<<<(unsigned)((words + 255) / 256), 256, 0, c->st>>>((uint64_t*)dd.p, words, 2);
     *ms = time_launches(c->st, iters, [&] { merkle_build(dd.p, n_leaves, leaf_size, dt.p, c->st); });
+    return FLOCK_OK;
+  });
+}
+
+int flock_bench_prove(flock_setup* s, uint64_t seed0, int steps, double* total_ms, double* phase_ms,
+                      uint64_t* launches) {
+  if (!s || steps < 1 || !total_ms) return FLOCK_ERR_ARG;
+  return guard(s->ctx, [&] {
+    flock::Setup& S = *s->s;
+    double acc[flock::Setup::kPhases] = {0};
+    uint64_t l0 = kernel_launch_counter();
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaStreamSynchronize(S.st));
+    CK(cudaEventRecord(e0, S.st));
+    for (int i = 0; i < steps; i++) {
+      S.prove(&seed0, nullptr, 0, "flock-bench-v0");
+      seed0++;
+      double t[flock::Setup::kPhases];
+      S.phase_times(t);
+      for (int k = 0; k < flock::Setup::kPhases; k++) acc[k] += t[k];
+    }
+    CK(cudaEventRecord(e1, S.st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *total_ms = ms;
+    if (phase_ms)
+      for (int k = 0; k < flock::Setup::kPhases; k++) phase_ms[k] = acc[k] / steps;
+    if (launches) *launches = kernel_launch_counter() - l0;
     return FLOCK_OK;
   });
 }

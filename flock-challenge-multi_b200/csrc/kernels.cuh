@@ -11,6 +11,11 @@
 
 constexpr int kK_ = 16384;  // bits per compression block (2^14)
 
+// Number of this library's kernel launches issued by this process (reported
+// by the benchmark; every launch wrapper adds its launches here).
+uint64_t& kernel_launch_counter();
+inline void count_launch(uint64_t n = 1) { kernel_launch_counter() += n; }
+
 struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& s) : std::runtime_error(s) {}
 };

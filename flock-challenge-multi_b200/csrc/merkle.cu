@@ -81,15 +81,15 @@ __global__ void k_merkle_top(uint32_t* tree, size_t level_start, size_t level_le
 }
 
 void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, cudaStream_t s) {
-  k_merkle_leaves<<<(unsigned)((n_leaves + 127) / 128), 128, 0, s>>>((const uint8_t*)data, leaf_size, n_leaves, tree);
+  count_launch(); k_merkle_leaves<<<(unsigned)((n_leaves + 127) / 128), 128, 0, s>>>((const uint8_t*)data, leaf_size, n_leaves, tree);
   size_t start = 0, len = n_leaves;
   while (len > 1024) {
     size_t n = len >> 1;
-    k_merkle_parents<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(tree + 8 * start, tree + 8 * (start + len), n);
+    count_launch(); k_merkle_parents<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(tree + 8 * start, tree + 8 * (start + len), n);
     start += len;
     len = n;
   }
-  if (len > 1) k_merkle_top<<<1, 512, 0, s>>>(tree, start, len);
+  if (len > 1) count_launch(), k_merkle_top<<<1, 512, 0, s>>>(tree, start, len);
 }
 
 __global__ void k_gather_nodes(const uint32_t* __restrict__ tree, const uint64_t* __restrict__ idx, size_t n,
@@ -114,7 +114,7 @@ __global__ void k_scatter(f128* __restrict__ dst, const uint64_t* __restrict__ p
 }
 namespace flock {
 void scatter(f128* dst, const uint64_t* pos, const f128* vals, size_t n, cudaStream_t s) {
-  if (n) k_scatter<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(dst, pos, vals, n);
+  if (n) count_launch(), k_scatter<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(dst, pos, vals, n);
 }
 }  // namespace flock
 
@@ -146,7 +146,7 @@ uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, uns
   for (uint64_t start = 0;; start += chunk) {
     *h_found = ~0ull;
     CK(cudaMemcpyAsync(d_found, h_found, 8, cudaMemcpyHostToDevice, s));
-    k_pow<<<(unsigned)(chunk / 256), 256, 0, s>>>(d0, d1, bits, start, chunk, d_found);
+    count_launch(); k_pow<<<(unsigned)(chunk / 256), 256, 0, s>>>(d0, d1, bits, start, chunk, d_found);
     CK(cudaMemcpyAsync(h_found, d_found, 8, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (*h_found != ~0ull) return *h_found;

@@ -165,10 +165,10 @@ void run_passes(f128* data, int log_d, int lanes, int layer_begin, bool transpos
     int threads = std::min(512, std::max(32, (LG << pr.second) / 2));
     if (transpose) {
       CK(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_ntt_pass<true><<<(unsigned)tiles, threads, smem, s>>>(a);
+      count_launch(); k_ntt_pass<true><<<(unsigned)tiles, threads, smem, s>>>(a);
     } else {
       CK(cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_ntt_pass<false><<<(unsigned)tiles, threads, smem, s>>>(a);
+      count_launch(); k_ntt_pass<false><<<(unsigned)tiles, threads, smem, s>>>(a);
     }
   }
 }
@@ -176,7 +176,7 @@ void run_passes(f128* data, int log_d, int lanes, int layer_begin, bool transpos
 
 void ntt_rs_encode(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, cudaStream_t s) {
   size_t msg_len = ((size_t)lanes) << log_msg_pos;
-  k_replicate<<<(unsigned)((msg_len + 255) / 256), 256, 0, s>>>(msg, cw, msg_len, 1 << log_inv_rate);
+  count_launch(); k_replicate<<<(unsigned)((msg_len + 255) / 256), 256, 0, s>>>(msg, cw, msg_len, 1 << log_inv_rate);
   run_passes(cw, log_msg_pos + log_inv_rate, lanes, log_inv_rate, false, s);
 }
 
@@ -189,5 +189,5 @@ void ntt_forward(f128* data, int log_d, int lanes, int start_layer, cudaStream_t
 void ntt_transposed_encode(f128* e, f128* out, int log_msg, int log_inv_rate, cudaStream_t s) {
   run_passes(e, log_msg + log_inv_rate, 1, log_inv_rate, true, s);
   size_t len = (size_t)1 << log_msg;
-  k_fold_copies<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(e, out, len, 1 << log_inv_rate);
+  count_launch(); k_fold_copies<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(e, out, len, 1 << log_inv_rate);
 }

@@ -224,7 +224,7 @@ Opening Setup::open(const f128* cw, const uint32_t* tree, size_t n_leaves, int l
   std::vector<uint64_t> pos(q.begin(), q.end());
   CK(cudaMemcpyAsync(idx, pos.data(), pos.size() * 8, cudaMemcpyHostToDevice, st));
   size_t nr = q.size() * lanes;
-  k_gather_rows<<<(unsigned)((nr + 255) / 256), 256, 0, st>>>(cw, idx, q.size(), lanes, gather);
+  count_launch(); k_gather_rows<<<(unsigned)((nr + 255) / 256), 256, 0, st>>>(cw, idx, q.size(), lanes, gather);
   std::vector<f128> rows(nr);
   fetch(gather, nr, rows.data());
   for (size_t i = 0; i < q.size(); i++) o.rows.emplace_back(rows.begin() + i * lanes, rows.begin() + (i + 1) * lanes);
@@ -246,7 +246,7 @@ Opening Setup::open(const f128* cw, const uint32_t* tree, size_t n_leaves, int l
   }
   if (!sib.empty()) {
     CK(cudaMemcpyAsync(idx, sib.data(), sib.size() * 8, cudaMemcpyHostToDevice, st));
-    k_gather_nodes<<<(unsigned)((sib.size() + 127) / 128), 128, 0, st>>>(tree, idx, sib.size(),
+    count_launch(); k_gather_nodes<<<(unsigned)((sib.size() + 127) / 128), 128, 0, st>>>(tree, idx, sib.size(),
                                                                          reinterpret_cast<uint32_t*>(gather));
     o.proof.resize(sib.size());
     CK(cudaMemcpyAsync(o.proof.data(), gather, sib.size() * 32, cudaMemcpyDeviceToHost, st));

@@ -152,7 +152,7 @@ void zc_round1(const f128* a, const f128* b, const f128* c, const void* tabs, co
                f128* out, int grid, cudaStream_t s) {
   size_t smem = sizeof(Round1Tables) + 2 * 256 * 64;
   CK(cudaFuncSetAttribute(k_zc_round1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_zc_round1<<<grid, 256, smem, s>>>((const uint64_t*)a, (const uint64_t*)b, (const uint64_t*)c,
+  count_launch(); k_zc_round1<<<grid, 256, smem, s>>>((const uint64_t*)a, (const uint64_t*)b, (const uint64_t*)c,
                                       (const Round1Tables*)tabs, eqc, n_blocks, out);
 }
 size_t round1_tables_size() { return sizeof(Round1Tables); }
@@ -240,18 +240,19 @@ __global__ void k_fold_pair_final(const f128* a_in, const f128* b_in, f128 rho, 
 
 void zc_msg0(const f128* a, const f128* b, const f128* lag, const f128* elo, const f128* ehi, int es, size_t n_pairs,
              f128* out, int grid, cudaStream_t s) {
-  k_zc_msg0<<<grid, 256, 0, s>>>(a, b, lag, elo, ehi, es, n_pairs, out);
+  count_launch(); k_zc_msg0<<<grid, 256, 0, s>>>(a, b, lag, elo, ehi, es, n_pairs, out);
 }
 void zc_fold_msg(bool from_packed, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag,
                  f128 rho, const f128* elo, const f128* ehi, int es, size_t n_pairs_out, bool emit, f128* out,
                  int grid, cudaStream_t s) {
+  count_launch();
   if (from_packed)
     k_zc_fold_msg<true><<<grid, 256, 0, s>>>(a_in, b_in, a_out, b_out, lag, rho, elo, ehi, es, n_pairs_out, emit, out);
   else
     k_zc_fold_msg<false><<<grid, 256, 0, s>>>(a_in, b_in, a_out, b_out, lag, rho, elo, ehi, es, n_pairs_out, emit, out);
 }
 void fold_pair_final(const f128* a_in, const f128* b_in, f128 rho, f128* out, cudaStream_t s) {
-  k_fold_pair_final<<<1, 32, 0, s>>>(a_in, b_in, rho, out);
+  count_launch(); k_fold_pair_final<<<1, 32, 0, s>>>(a_in, b_in, rho, out);
 }
 
 // ------------------------------------------------------------------ K6 --
@@ -323,15 +324,15 @@ __global__ void __launch_bounds__(512) k_lc_round(f128* comb, f128* zv, int len,
 
 void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
              const f128* eq, f128 alpha, f128 beta, int pin, f128* comb, cudaStream_t s) {
-  k_lc_comb<<<kK_ / 128, 128, 0, s>>>(at_ptr, at_row, bt_ptr, bt_row, eq, alpha, beta, pin, comb);
+  count_launch(); k_lc_comb<<<kK_ / 128, 128, 0, s>>>(at_ptr, at_row, bt_ptr, bt_row, eq, alpha, beta, pin, comb);
 }
 void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, f128* zv, cudaStream_t s) {
   int chunk = 256;
   dim3 grid(2048 / 128, (unsigned)((n_outer + chunk - 1) / chunk));
-  k_lc_zvec<<<grid, 128, 0, s>>>((const uint8_t*)z, eqo, n_outer, chunk, zv);
+  count_launch(); k_lc_zvec<<<grid, 128, 0, s>>>((const uint8_t*)z, eqo, n_outer, chunk, zv);
 }
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s) {
-  k_lc_round<<<1, 512, 0, s>>>(comb, zv, len, fold, r, emit, out);
+  count_launch(); k_lc_round<<<1, 512, 0, s>>>(comb, zv, len, fold, r, emit, out);
 }
 
 // ------------------------------------------------------------------ K7 --
@@ -383,12 +384,12 @@ __global__ void __launch_bounds__(256) k_bcombined(const f128* __restrict__ eq0,
 }
 
 void ring_shat(const f128* z, const f128* eq, size_t n, f128* out, int grid, cudaStream_t s) {
-  k_shat<<<grid, 256, 0, s>>>(z, eq, n, out);
+  count_launch(); k_shat<<<grid, 256, 0, s>>>(z, eq, n, out);
 }
 void ring_bcombined(const f128* eq0, const f128* eq1, const f128* tabs, size_t n, f128* out, int grid, cudaStream_t s) {
   size_t smem = 2 * 16 * 256 * sizeof(f128);
   CK(cudaFuncSetAttribute(k_bcombined, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_bcombined<<<grid, 256, smem, s>>>(eq0, eq1, tabs, n, out);
+  count_launch(); k_bcombined<<<grid, 256, smem, s>>>(eq0, eq1, tabs, n, out);
 }
 
 // ------------------------------------------------------------------ K8 --
@@ -429,18 +430,18 @@ __global__ void __launch_bounds__(256) k_lig_fold_msg(const f128* __restrict__ f
 }
 
 void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int grid, cudaStream_t s) {
-  k_lig_msg<<<grid, 256, 0, s>>>(f, b, n_pairs, out);
+  count_launch(); k_lig_msg<<<grid, 256, 0, s>>>(f, b, n_pairs, out);
 }
 void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size_t n_pairs_out, bool emit, f128* out,
                   int grid, cudaStream_t s) {
-  k_lig_fold_msg<<<grid, 256, 0, s>>>(f, b, fo, bo, r, n_pairs_out, emit, out);
+  count_launch(); k_lig_fold_msg<<<grid, 256, 0, s>>>(f, b, fo, bo, r, n_pairs_out, emit, out);
 }
 void eq_split(const f128* lo, const f128* hi, int s_bits, size_t n, f128* out, cudaStream_t s) {
-  k_eq_split<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(lo, hi, s_bits, n, out);
+  count_launch(); k_eq_split<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(lo, hi, s_bits, n, out);
 }
 void axpy(f128* out, const f128* x, f128 beta, size_t n, cudaStream_t s) {
-  k_axpy<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, x, beta, n);
+  count_launch(); k_axpy<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, x, beta, n);
 }
 void inner(const f128* f, const f128* g, size_t n, f128* out, int grid, cudaStream_t s) {
-  k_inner<<<grid, 256, 0, s>>>(f, g, n, out);
+  count_launch(); k_inner<<<grid, 256, 0, s>>>(f, g, n, out);
 }

@@ -176,9 +176,9 @@ __global__ void k_witness_blocks(const uint32_t* __restrict__ blocks, uint32_t n
 
 void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
                          f128* b, cudaStream_t s) {
-  k_witness_seed<<<(n_slots + 127) / 128, 128, 0, s>>>(seed, log2, n_blocks, n_slots, z, a, b);
+  count_launch(); k_witness_seed<<<(n_slots + 127) / 128, 128, 0, s>>>(seed, log2, n_blocks, n_slots, z, a, b);
 }
 void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a, f128* b,
                            cudaStream_t s) {
-  k_witness_blocks<<<(n_slots + 127) / 128, 128, 0, s>>>(blocks, n_blocks, n_slots, z, a, b);
+  count_launch(); k_witness_blocks<<<(n_slots + 127) / 128, 128, 0, s>>>(blocks, n_blocks, n_slots, z, a, b);
 }

@@ -25,7 +25,7 @@ EXPORTS = (
     "flock_setup_destroy", "flock_prove_seed", "flock_prove_blocks", "flock_setup_phase_ms",
     "flock_witness", "flock_ntt_rs_encode", "flock_merkle_tree", "flock_sumcheck_round",
     "flock_pow", "flock_f128_mul", "flock_statement_digest", "flock_bench_ntt",
-    "flock_bench_merkle", "flock_bench_sumcheck",
+    "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove",
 )
 PHASES = ("witness", "commit", "zerocheck_round1", "zerocheck_rounds", "lincheck",
           "ring_switch_combine", "ligerito_l0_folds", "ligerito_levels")
@@ -63,6 +63,8 @@ def load() -> ctypes.CDLL:
         lib.flock_bench_ntt.argtypes = [vp, u32, u32, u32, i32, ctypes.POINTER(ctypes.c_double)]
         lib.flock_bench_merkle.argtypes = [vp, sz, sz, i32, ctypes.POINTER(ctypes.c_double)]
         lib.flock_bench_sumcheck.argtypes = [vp, sz, i32, ctypes.POINTER(ctypes.c_double)]
+        lib.flock_bench_prove.argtypes = [vp, u64, i32, ctypes.POINTER(ctypes.c_double), vp,
+                                          ctypes.POINTER(u64)]
         _lib = lib
     return _lib
 
@@ -197,6 +199,15 @@ class Prover:
                                              _ptr(self._buf), self._buf.size, ctypes.byref(n))
         self.ctx._check(rc, "prove_blocks")
         return self._buf[: n.value].tobytes()
+
+    def bench(self, seed0: int, steps: int):
+        """(total device ms of `steps` proofs, mean per-phase ms, kernel launches)."""
+        total = ctypes.c_double()
+        ph = np.zeros(len(PHASES), np.float64)
+        n = ctypes.c_uint64()
+        self.ctx._check(self.ctx.lib.flock_bench_prove(self.h, seed0, steps, ctypes.byref(total), _ptr(ph),
+                                                       ctypes.byref(n)), "bench_prove")
+        return total.value, dict(zip(PHASES, ph.tolist())), n.value
 
     def phase_ms(self) -> dict:
         out = np.zeros(len(PHASES), np.float64)

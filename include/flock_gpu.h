@@ -86,6 +86,11 @@ int flock_bench_ntt(flock_ctx* ctx, uint32_t log_msg_pos, uint32_t lanes, uint32
                     double* ms);
 int flock_bench_merkle(flock_ctx* ctx, size_t n_leaves, size_t leaf_size, int iters, double* ms);
 int flock_bench_sumcheck(flock_ctx* ctx, size_t n, int iters, double* ms);
+/* `steps` back-to-back proofs (seeds seed0, seed0+1, ...) timed with CUDA
+ * events on the setup's stream; also the mean per-phase device times and the
+ * number of this library's kernel launches inside the timed region. */
+int flock_bench_prove(flock_setup* s, uint64_t seed0, int steps, double* total_ms, double* phase_ms,
+                      uint64_t* launches);
 
 #ifdef __cplusplus
 }
