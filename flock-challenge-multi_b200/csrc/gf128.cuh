@@ -113,6 +113,40 @@ __device__ __forceinline__ void atomic_xor128(f128* p, f128 v) {
   if (v.hi) atomicXor(reinterpret_cast<unsigned long long*>(&p->hi), (unsigned long long)v.hi);
 }
 
+// ---- multiplication by a constant through an 8-bit window table ----
+// T[p][v] = E * v(x) * x^(8p): E * y = XOR over the 16 bytes y_p of T[p][y_p].
+// Built cooperatively by a CTA (8 doubling levels); 64 KiB of shared memory.
+struct MulTab8 {
+  f128 t[16][256];
+};
+__device__ __forceinline__ void multab_build(MulTab8* T, f128 E) {
+  for (int i = threadIdx.x; i < 16 * 8; i += blockDim.x) {
+    int p = i >> 3, j = i & 7;
+    f128 v = E;
+    for (int q = 0; q < p; q++) v = mul_xk(v, 8);
+    T->t[p][1 << j] = mul_xk(v, j);
+    if (j == 0) T->t[p][0] = mk(0, 0);
+  }
+  __syncthreads();
+  for (int lvl = 1; lvl < 8; lvl++) {
+    int base = 1 << lvl, cnt = base - 1;  // entries base+1 .. 2*base-1
+    for (int i = threadIdx.x; i < 16 * cnt; i += blockDim.x) {
+      int p = i / cnt, w = 1 + i % cnt;
+      T->t[p][base + w] = fx(T->t[p][w], T->t[p][base]);
+    }
+    __syncthreads();
+  }
+}
+__device__ __forceinline__ f128 multab_mul(const MulTab8* T, f128 y) {
+  f128 acc = mk(0, 0);
+#pragma unroll
+  for (int p = 0; p < 8; p++) {
+    acc = fx(acc, T->t[p][(y.lo >> (8 * p)) & 0xFF]);
+    acc = fx(acc, T->t[8 + p][(y.hi >> (8 * p)) & 0xFF]);
+  }
+  return acc;
+}
+
 // ---- GF(2^8) ----
 __host__ __device__ __forceinline__ uint8_t gf8_mul_slow(uint8_t a, uint8_t b) {
   uint32_t acc = 0;

@@ -47,20 +47,20 @@ void eq_split(const f128* lo, const f128* hi, int s_bits, size_t n, f128* out, c
 void axpy(f128* out, const f128* x, f128 beta, size_t n, cudaStream_t s);
 void inner(const f128* f, const f128* g, size_t n, f128* out, int grid, cudaStream_t s);
 size_t round1_tables_size();
+void build_round1_tables_host(const uint8_t M[64][64], const f128* phi8, void* dst);
 void zc_round1(const f128* a, const f128* b, const f128* c, const void* tabs, const f128* eqc, size_t n_blocks,
                f128* out, int grid, cudaStream_t s);
-void zc_msg0(const f128* a, const f128* b, const f128* lag, const f128* elo, const f128* ehi, int es, size_t n_pairs,
-             f128* out, int grid, cudaStream_t s);
-void zc_fold_msg(bool from_packed, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag,
-                 f128 rho, const f128* elo, const f128* ehi, int es, size_t n_pairs_out, bool emit, f128* out,
-                 int grid, cudaStream_t s);
+void zc_round(bool packed, bool fold, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag,
+              f128 rho, size_t n_pairs, int ns, int nm, const int* shift, const f128* K, const f128* elo,
+              const f128* ehi, int es, f128* out, int grid, cudaStream_t s);
 void fold_pair_final(const f128* a_in, const f128* b_in, f128 rho, f128* out, cudaStream_t s);
 void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
              const f128* eq, f128 alpha, f128 beta, int pin, f128* comb, cudaStream_t s);
 void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, f128* zv, cudaStream_t s);
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s);
-void ring_shat(const f128* z, const f128* eq, size_t n, f128* out, int grid, cudaStream_t s);
-void ring_bcombined(const f128* eq0, const f128* eq1, const f128* tabs, size_t n, f128* out, int grid, cudaStream_t s);
+void ring_shat_ab(const f128* zv_pre, const f128* eqt, f128* out, cudaStream_t s);
+void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, const f128* ehi1, const f128* L0,
+                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int grid, cudaStream_t s);
 void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int grid, cudaStream_t s);
 void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size_t n_pairs_out, bool emit, f128* out,
                   int grid, cudaStream_t s);

@@ -63,7 +63,6 @@ Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
   tree0 = dalloc<uint32_t>(8 * (2 * n_leaves0 - 1));
   for (int i = 0; i < 4; i++) pp[i] = dalloc<f128>(n_words);
   eqbuf[0] = dalloc<f128>(n_words);
-  eqbuf[1] = dalloc<f128>(n_words);
   // recursive Ligero levels
   int n_cur = m - 7 - lad->initial_k;
   for (size_t i = 0; i < lad->ks.size(); i++) {
@@ -85,6 +84,7 @@ Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
   ehi = dalloc<f128>(1 << 16);
   comb = dalloc<f128>(kK);
   zv = dalloc<f128>(kK);
+  zv_pre = dalloc<f128>(kK);
   eq_inner = dalloc<f128>(kK);
   bc_tabs = dalloc<f128>(2 * 16 * 256);
   idx = dalloc<uint64_t>(1 << 16);
@@ -111,7 +111,7 @@ Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
 
 Setup::~Setup() {
   cudaStreamSynchronize(st);
-  void* ptrs[] = {z, a, b, cw0, tree0, pp[0], pp[1], pp[2], pp[3], eqbuf[0], eqbuf[1], induce_buf, out, blocks_buf,
+  void* ptrs[] = {z, a, b, cw0, tree0, pp[0], pp[1], pp[2], pp[3], eqbuf[0], zv_pre, induce_buf, out, blocks_buf,
                   tabs_r1, lag, elo, ehi, comb, zv, eq_inner, bc_tabs, idx, gather, d_found, at_ptr, bt_ptr,
                   at_row, bt_row};
   for (void* p : ptrs) cudaFree(p);
@@ -128,13 +128,8 @@ Setup::~Setup() {
 // the small-eq weights g(xs) with eq(r[6..9], xs) = phi8(g(xs)).
 void Setup::build_round1_tables() {
   std::vector<uint8_t> host(round1_tables_size(), 0);
-  uint8_t(*lde)[256][64] = reinterpret_cast<uint8_t(*)[256][64]>(host.data());
-  uint8_t* exp_ = host.data() + 8 * 256 * 64;
-  uint8_t* log_ = exp_ + 512;
-  f128* phi = reinterpret_cast<f128*>(log_ + 256);
-  uint8_t* g_log = reinterpret_cast<uint8_t*>(phi + 256);
-  // generator 3 of GF(2^8)*
-  uint8_t x = 1;
+  uint8_t exp_[512], log_[256];
+  uint8_t x = 1;  // generator 3 of GF(2^8)*
   for (int i = 0; i < 255; i++) {
     exp_[i] = x;
     log_[x] = (uint8_t)i;
@@ -142,7 +137,7 @@ void Setup::build_round1_tables() {
   }
   for (int i = 255; i < 512; i++) exp_[i] = exp_[i - 255];
   auto ginv = [&](uint8_t v) { return exp_[(255 - log_[v]) % 255]; };
-  uint8_t M[64][64];  // M[l][s] = L_s(64 + l) over nodes 0..63 in GF(2^8)
+  uint8_t(&M)[64][64] = lde_m;  // M[l][s] = L_s(64 + l) over nodes 0..63 in GF(2^8)
   for (int l = 0; l < 64; l++) {
     uint8_t pt = (uint8_t)(64 + l);
     for (int s = 0; s < 64; s++) {
@@ -155,21 +150,7 @@ void Setup::build_round1_tables() {
       M[l][s] = hgf8_mul(num, ginv(den));
     }
   }
-  for (int k = 0; k < 8; k++)
-    for (int v = 0; v < 256; v++)
-      for (int l = 0; l < 64; l++) {
-        uint8_t acc = 0;
-        for (int j = 0; j < 8; j++)
-          if ((v >> j) & 1) acc ^= M[l][8 * k + j];
-        lde[k][v][l] = acc;
-      }
-  for (int v = 0; v < 256; v++) phi[v] = phi8_table()[v];
-  const uint8_t sc[3] = {0xF7, 0x53, 0xB5};
-  for (int xs = 0; xs < 8; xs++) {
-    uint8_t g = 1;
-    for (int i = 0; i < 3; i++) g = hgf8_mul(g, ((xs >> i) & 1) ? sc[i] : (uint8_t)(1 ^ sc[i]));
-    g_log[xs] = g ? log_[g] : 0xFF;
-  }
+  build_round1_tables_host(M, phi8_table(), host.data());
   CK(cudaMemcpy(tabs_r1, host.data(), host.size(), cudaMemcpyHostToDevice));
 }
 
@@ -308,12 +289,21 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     for (auto& v : hi) v = hmul(v, C);
     put_eq_split(lo, hi);
     eq_split(elo, ehi, s, (size_t)1 << rh.size(), scratch_eq(), st);
-    CK(cudaMemsetAsync(out, 0, 128 * sizeof(f128), st));
+    CK(cudaMemsetAsync(out, 0, 192 * sizeof(f128), st));
     size_t n_blocks128 = (size_t)1 << (m - 13);
     zc_round1(a, b, z, tabs_r1, scratch_eq(), n_blocks128, out, sms, st);
-    fetch(out, 128, h_out);
+    fetch(out, 192, h_out);
     P.r1_ab.assign(h_out, h_out + 64);
-    P.r1_c.assign(h_out + 64, h_out + 128);
+    // c-claim ring-switch statistic (suffix r[7..m]) and, from it, the
+    // extract-c message: S_s = (1 + r6) sv[s] + r6 sv[64 + s];
+    // P_C(l) = sum_s phi8(M[l][s]) S_s
+    s_hat_v_c.assign(h_out + 64, h_out + 192);
+    P.r1_c.assign(64, mk(0, 0));
+    for (int s = 0; s < 64; s++) {
+      f128 S = fx(hmul(fx(hone(), r[6]), s_hat_v_c[s]), hmul(r[6], s_hat_v_c[64 + s]));
+      for (int l = 0; l < 64; l++)
+        if (lde_m[l][s]) P.r1_c[l] = fx(P.r1_c[l], hmul(phi8_table()[lde_m[l][s]], S));
+    }
   }
   mark(3);
   tr.f128s(P.r1_ab.data(), 64);
@@ -338,18 +328,43 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   }
   const int n_mlv = m - 6;
   std::vector<f128> rhos;
-  auto set_eq = [&](int from) -> int {  // eq over r[from..m) as lo x hi; returns lo bits
-    std::vector<f128> rs(r.begin() + from, r.end());
-    int s = (int)std::min<size_t>(rs.size(), 12);
-    put_eq_split(heq(std::vector<f128>(rs.begin(), rs.begin() + s)), heq(std::vector<f128>(rs.begin() + s, rs.end())));
-    return s;
-  };
-  {
-    int es = set_eq(7);
+  // Message of round k weights pair j by eq(r[7+k..m], j).  Its low bits sit
+  // on the fixed small (phi8) and medium (x^(2^t) / (1 + x^(2^t))) challenges:
+  // the kernel needs ns, nm, the medium shifts, K[js] = phi8(g(js)), and eq
+  // over the random suffix (scaled by the medium constant C).
+  auto run_round = [&](int k, bool packed, bool fold, const f128* ain, const f128* bin, f128* aout, f128* bout,
+                       f128 rho, size_t n_pairs) {
+    const int st0 = 7 + k;
+    const int ns = std::max(0, 9 - st0);
+    const int med0 = std::max(st0, 9);
+    const int nm = med0 <= 13 ? 13 - med0 : 0;
+    int shift[4] = {0, 0, 0, 0};
+    f128 C = hone();
+    for (int t = 0; t < nm; t++) {
+      shift[t] = 1 << (med0 + t - 9);
+      C = hmul(C, fx(hone(), r[med0 + t]));
+    }
+    const uint8_t sc[3] = {0xF7, 0x53, 0xB5};  // r[6], r[7], r[8] = phi8(sc)
+    f128 K[4] = {};
+    for (int js = 0; js < (1 << ns); js++) {
+      uint8_t g = 1;
+      for (int t = 0; t < ns; t++) {
+        uint8_t s8 = sc[st0 - 6 + t];
+        g = hgf8_mul(g, ((js >> t) & 1) ? s8 : (uint8_t)(1 ^ s8));
+      }
+      K[js] = phi8_table()[g];
+    }
+    std::vector<f128> rs(r.begin() + std::max(st0, 13), r.end());
+    int es = (int)std::min<size_t>(rs.size(), 12);
+    std::vector<f128> lo = heq(std::vector<f128>(rs.begin(), rs.begin() + es));
+    std::vector<f128> hi = heq(std::vector<f128>(rs.begin() + es, rs.end()));
+    for (auto& v : hi) v = hmul(v, C);
+    put_eq_split(lo, hi);
     CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-    zc_msg0(a, b, lag, elo, ehi, es, n_words, out, G, st);
+    zc_round(packed, fold, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, shift, K, elo, ehi, es, out, G, st);
     fetch(out, 2, h_out);
-  }
+  };
+  run_round(0, true, false, a, b, nullptr, nullptr, mk(0, 0), n_words);
   f128* av = pp[0];
   f128* bv = pp[1];
   f128* av2 = pp[2];
@@ -361,16 +376,13 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     f128 rho = tr.sample();
     rhos.push_back(rho);
     if (i < n_mlv - 1) {
-      int es = set_eq(8 + i);
       size_t n_pairs_out = (size_t)1 << (n_mlv - i - 2);
-      CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-      if (i == 0) zc_fold_msg(true, a, b, av, bv, lag, rho, elo, ehi, es, n_pairs_out, true, out, G, st);
+      if (i == 0) run_round(1, true, true, a, b, av, bv, rho, n_pairs_out);
       else {
-        zc_fold_msg(false, av, bv, av2, bv2, lag, rho, elo, ehi, es, n_pairs_out, true, out, G, st);
+        run_round(i + 1, false, true, av, bv, av2, bv2, rho, n_pairs_out);
         std::swap(av, av2);
         std::swap(bv, bv2);
       }
-      fetch(out, 2, h_out);
     } else {
       fold_pair_final(av, bv, rho, out, st);
       fetch(out, 2, h_out);
@@ -397,6 +409,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     eq_table(x_outer, scratch_eq());
     CK(cudaMemsetAsync(zv, 0, kK * sizeof(f128), st));
     lc_zvec(z, scratch_eq(), (size_t)1 << (m - kKLog), zv, st);
+    // pre-sumcheck z_vec: the ab-claim's ring-switch statistic is read from it
+    CK(cudaMemcpyAsync(zv_pre, zv, kK * sizeof(f128), cudaMemcpyDeviceToDevice, st));
     CK(cudaStreamSynchronize(st));
   }
   std::vector<f128> rr;
@@ -427,15 +441,18 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   std::vector<f128> x_c(r.begin() + 6, r.end());
   std::vector<f128> eqdd[2];
   f128 claim[2];
-  for (int k = 0; k < 2; k++) {
-    const std::vector<f128>& xf = k == 0 ? x_ab : x_c;
-    tr.label("flock-ring-switch-v0");
-    eq_table(std::vector<f128>(xf.begin() + 1, xf.end()), eqbuf[k]);
-    CK(cudaMemsetAsync(out, 0, 128 * sizeof(f128), st));
-    ring_shat(z, eqbuf[k], n_words, out, sms * 8, st);
+  {
+    std::vector<f128> eqt = heq(std::vector<f128>(r_inner_rest.begin() + 1, r_inner_rest.end()));
+    CK(cudaMemcpyAsync(eq_inner, eqt.data(), eqt.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
+    ring_shat_ab(zv_pre, eq_inner, out, st);
     std::vector<f128> sv(128);
     fetch(out, 128, sv.data());
     P.s_hat_v.push_back(sv);
+    P.s_hat_v.push_back(s_hat_v_c);
+  }
+  for (int k = 0; k < 2; k++) {
+    tr.label("flock-ring-switch-v0");
+    const std::vector<f128>& sv = P.s_hat_v[k];
     tr.f128s(sv.data(), 128);
     std::vector<f128> rdp = tr.sample_vec(7);
     eqdd[k] = heq(rdp);
@@ -467,7 +484,22 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
         }
     }
     CK(cudaMemcpyAsync(bc_tabs, T.data(), T.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
-    ring_bcombined(eqbuf[0], eqbuf[1], bc_tabs, n_words, pp[1], sms * 2, st);
+    // eq(suffix_k, i) = lo_k(i mod 2^12) * hi_k(i >> 12), both tables on the device
+    std::vector<f128> lo[2], hi[2];
+    int lo_bits = (int)std::min<size_t>(x_ab.size() - 1, 12);
+    for (int k = 0; k < 2; k++) {
+      const std::vector<f128>& xf = k == 0 ? x_ab : x_c;
+      lo[k] = heq(std::vector<f128>(xf.begin() + 1, xf.begin() + 1 + lo_bits));
+      hi[k] = heq(std::vector<f128>(xf.begin() + 1 + lo_bits, xf.end()));
+    }
+    f128* d = eqbuf[0];  // [lo0 | hi0 | lo1 | hi1]
+    size_t nlo = lo[0].size(), nhi = hi[0].size();
+    CK(cudaMemcpyAsync(d, lo[0].data(), nlo * sizeof(f128), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d + nlo, hi[0].data(), nhi * sizeof(f128), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d + nlo + nhi, lo[1].data(), nlo * sizeof(f128), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d + 2 * nlo + nhi, hi[1].data(), nhi * sizeof(f128), cudaMemcpyHostToDevice, st));
+    ring_bcombined_ct(d, d + nlo, d + nlo + nhi, d + 2 * nlo + nhi, bc_tabs, bc_tabs + 4096, lo_bits, nhi, pp[1],
+                      sms, st);
     CK(cudaStreamSynchronize(st));
   }
   mark(6);

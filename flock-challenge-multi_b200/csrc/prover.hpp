@@ -50,6 +50,7 @@ class Setup {
   void mark(int phase);
   f128* scratch_eq() { return eqbuf[0]; }
 
+  uint8_t lde_m[64][64] = {};  // GF(2^8) extension S -> Lambda (Lagrange basis)
   const Ladder* lad = nullptr;
   std::array<uint8_t, 32> digest{};
   f128 *z = nullptr, *a = nullptr, *b = nullptr, *cw0 = nullptr;
@@ -58,7 +59,8 @@ class Setup {
   f128* eqbuf[2] = {nullptr, nullptr};
   std::vector<Level> levels;
   f128 *induce_buf = nullptr, *out = nullptr, *lag = nullptr, *elo = nullptr, *ehi = nullptr;
-  f128 *comb = nullptr, *zv = nullptr, *eq_inner = nullptr, *bc_tabs = nullptr, *gather = nullptr;
+  f128 *comb = nullptr, *zv = nullptr, *zv_pre = nullptr, *eq_inner = nullptr, *bc_tabs = nullptr, *gather = nullptr;
+  std::vector<f128> s_hat_v_c;  // c-claim ring-switch statistic, captured by zerocheck round 1
   uint8_t* tabs_r1 = nullptr;
   uint64_t* idx = nullptr;
   unsigned long long* d_found = nullptr;

@@ -1,0 +1,86 @@
+// K7: ring switch (DP24 with phi8 weights) — crates/flock-core/src/pcs/
+// ring_switch.rs.  Per claim k with suffix point x_k[1..] (25 coordinates at
+// m = 32):  s_hat_v[r] = sum_i eq(suffix, i) bit_r(z_i)  (:1594-1640), and the
+// transparent rs_eq_ind[i] = sum_b bit_b(eq(suffix, i)) eq''[b]  (:1952-2087).
+// The open combines them: b_combined = sum_k gamma_k rs_eq_ind_k (pcs.rs:778-1290).
+//
+//  * s_hat_v of the ab-claim: its suffix is (r_inner_rest[1..8], x_outer), so
+//    it is a 128 x 128 contraction of the lincheck's pre-sumcheck z_vec
+//    (z_vec[c] = sum_o eq(x_outer, o) z[c + 2^14 o]):
+//      s_hat_v[r] = sum_t eq(r_inner_rest[1..], t) z_vec[128 t + r]
+//    (the reference's s_hat_v_from_z_vec, ring_switch.rs:1273).  The c-claim's
+//    statistic is captured by zerocheck round 1 (round1.cu).
+//  * b_combined: with eq(suffix, i) = eq_lo(i_lo) * eq_hi(i_hi), the map
+//    u -> gamma_k L_k(u * eq_hi(i_hi)) is GF(2)-linear; per 2^12-element
+//    chunk it is tabulated once (128 columns, then byte-window doubling) and
+//    applied to eq_lo with 16 lookups per claim — no general products.
+#include "kernels.cuh"
+
+__global__ void k_shat_from_zvec(const f128* __restrict__ zv, const f128* __restrict__ eqt, f128* __restrict__ out) {
+  int r = threadIdx.x;  // 128 threads
+  u256 acc = zero256();
+  for (int t = 0; t < 128; t++) acc_wide(acc, mul_wide(ldg(eqt + t), ldg(zv + 128 * t + r)));
+  out[r] = reduce(acc);
+}
+
+namespace {
+__device__ __forceinline__ f128 apply_tab(const f128* T, f128 y) {  // T = [16][256] global
+  f128 acc = mk(0, 0);
+#pragma unroll
+  for (int p = 0; p < 8; p++) {
+    acc = fx(acc, ldg(T + p * 256 + ((y.lo >> (8 * p)) & 0xFF)));
+    acc = fx(acc, ldg(T + (8 + p) * 256 + ((y.hi >> (8 * p)) & 0xFF)));
+  }
+  return acc;
+}
+}  // namespace
+
+// out[chunk * 2^lo_bits + i_lo] = gamma0 L0(eq_lo0[i_lo] eq_hi0[chunk]) + gamma1 L1(...)
+// Lk: [16][256] byte tables of gamma_k eq''_k (global)
+__global__ void __launch_bounds__(512) k_bcombined_ct(const f128* __restrict__ elo0, const f128* __restrict__ ehi0,
+                                                      const f128* __restrict__ elo1, const f128* __restrict__ ehi1,
+                                                      const f128* __restrict__ L0, const f128* __restrict__ L1,
+                                                      int lo_bits, size_t n_chunks, f128* __restrict__ out) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  MulTab8* C0 = reinterpret_cast<MulTab8*>(sm);
+  MulTab8* C1 = C0 + 1;
+  const size_t chunk_len = (size_t)1 << lo_bits;
+  for (size_t ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
+    const f128 E0 = ldg(ehi0 + ch), E1 = ldg(ehi1 + ch);
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+      int k = i >> 7, j = i & 127;
+      f128 y = k ? E1 : E0;
+      for (int left = j; left > 0; left -= 32) y = mul_xk(y, left < 32 ? left : 32);
+      MulTab8* C = k ? C1 : C0;
+      C->t[j >> 3][1 << (j & 7)] = apply_tab(k ? L1 : L0, y);
+      if ((j & 7) == 0) C->t[j >> 3][0] = mk(0, 0);
+    }
+    __syncthreads();
+    for (int lvl = 1; lvl < 8; lvl++) {
+      int base = 1 << lvl, cnt = base - 1;
+      for (int i = threadIdx.x; i < 2 * 16 * cnt; i += blockDim.x) {
+        int k = i / (16 * cnt), rem = i % (16 * cnt), p = rem / cnt, w = 1 + rem % cnt;
+        MulTab8* C = k ? C1 : C0;
+        C->t[p][base + w] = fx(C->t[p][w], C->t[p][base]);
+      }
+      __syncthreads();
+    }
+    for (size_t i = threadIdx.x; i < chunk_len; i += blockDim.x)
+      st(out + ch * chunk_len + i, fx(multab_mul(C0, ldg(elo0 + i)), multab_mul(C1, ldg(elo1 + i))));
+    __syncthreads();
+  }
+}
+
+void ring_shat_ab(const f128* zv_pre, const f128* eqt, f128* out, cudaStream_t s) {
+  count_launch();
+  k_shat_from_zvec<<<1, 128, 0, s>>>(zv_pre, eqt, out);
+}
+
+void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, const f128* ehi1, const f128* L0,
+                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int grid, cudaStream_t s) {
+  size_t smem = 2 * sizeof(MulTab8);
+  CK(cudaFuncSetAttribute(k_bcombined_ct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  count_launch();
+  k_bcombined_ct<<<(unsigned)std::min<size_t>(n_chunks, (size_t)grid), 512, smem, s>>>(elo0, ehi0, elo1, ehi1, L0, L1,
+                                                                                      lo_bits, n_chunks, out);
+}
