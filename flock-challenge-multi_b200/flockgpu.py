@@ -25,7 +25,7 @@ EXPORTS = (
     "flock_setup_destroy", "flock_prove_seed", "flock_prove_blocks", "flock_setup_phase_ms",
     "flock_witness", "flock_ntt_rs_encode", "flock_merkle_tree", "flock_sumcheck_round",
     "flock_pow", "flock_f128_mul", "flock_statement_digest", "flock_bench_ntt",
-    "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove",
+    "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove", "flock_merkle_root_noalloc",
 )
 PHASES = ("witness", "commit", "zerocheck_round1", "zerocheck_rounds", "lincheck",
           "ring_switch_combine", "ligerito_l0_folds", "ligerito_levels")
@@ -65,6 +65,7 @@ def load() -> ctypes.CDLL:
         lib.flock_bench_sumcheck.argtypes = [vp, sz, i32, ctypes.POINTER(ctypes.c_double)]
         lib.flock_bench_prove.argtypes = [vp, u64, i32, ctypes.POINTER(ctypes.c_double), vp,
                                           ctypes.POINTER(u64)]
+        lib.flock_merkle_root_noalloc.argtypes = [vp, sz, sz, vp, vp]
         _lib = lib
     return _lib
 

@@ -92,6 +92,21 @@ int flock_bench_sumcheck(flock_ctx* ctx, size_t n, int iters, double* ms);
 int flock_bench_prove(flock_setup* s, uint64_t seed0, int steps, double* total_ms, double* phase_ms,
                       uint64_t* launches);
 
+/* Merkle root of leaves already in device memory, for callers that may not
+ * allocate device memory when they need the root (inside a stream capture,
+ * fixed-memory hosts, plugins whose buffers are all owned by an outer
+ * framework).  No counterpart in the reference: it exists only for such
+ * callers.  `leaves` (n_leaves x leaf_size bytes) and `root_out` (32 bytes)
+ * are device pointers; the work is queued on `stream` (a cudaStream_t, NULL
+ * for the default stream) and the call returns without waiting.  The tree is
+ * built in one fixed device array that holds at most 2^15 leaves (2 MiB, kept
+ * by every GPU that loads the library until exit); more leaves return
+ * FLOCK_ERR_CAPACITY.  Same leaf rules and same root as flock_merkle_tree.
+ * The first call on a device looks the array's address up; make it before
+ * any stream capture begins.  Calls share the array, so calls whose work
+ * overlaps on the GPU race: serialise them. */
+int flock_merkle_root_noalloc(const void* leaves, size_t n_leaves, size_t leaf_size, void* root_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
