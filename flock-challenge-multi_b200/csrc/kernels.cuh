@@ -50,9 +50,9 @@ size_t round1_tables_size();
 void build_round1_tables_host(const uint8_t M[64][64], const f128* phi8, void* dst);
 void zc_round1(const f128* a, const f128* b, const f128* c, const void* tabs, const f128* eqc, size_t n_blocks,
                f128* out, int grid, cudaStream_t s);
-void zc_round(bool packed, bool fold, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag,
-              f128 rho, size_t n_pairs, int ns, int nm, const int* shift, const f128* K, const f128* elo,
-              const f128* ehi, int es, f128* out, int grid, cudaStream_t s);
+void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag, f128 rho,
+              size_t n_pairs, int ns, int nm, int msh, const f128* elo, const f128* ehi, int es, f128* out, int grid,
+              cudaStream_t s);
 void fold_pair_final(const f128* a_in, const f128* b_in, f128 rho, f128* out, cudaStream_t s);
 void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
              const f128* eq, f128 alpha, f128 beta, int pin, f128* comb, cudaStream_t s);

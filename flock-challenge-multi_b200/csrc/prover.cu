@@ -77,7 +77,7 @@ Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
     n_cur -= lad->ks[i];
   }
   induce_buf = dalloc<f128>((size_t)1 << (m - 7 - lad->initial_k + lad->rate[0]));
-  out = dalloc<f128>(512);
+  out = dalloc<f128>(1024);
   tabs_r1 = dalloc<uint8_t>(round1_tables_size());
   lag = dalloc<f128>(8 * 256);
   elo = dalloc<f128>(1 << 13);
@@ -91,7 +91,7 @@ Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
   gather = dalloc<f128>(1 << 16);
   d_found = dalloc<unsigned long long>(1);
   CK(cudaMallocHost(&h_found, 8));
-  CK(cudaMallocHost(&h_out, 512 * sizeof(f128)));
+  CK(cudaMallocHost(&h_out, 1024 * sizeof(f128)));
   CK(cudaMallocHost(&h_stage, (size_t)1 << 20));
   const Statement& S = blake3_statement();
   at_ptr = dalloc<uint32_t>(S.at_ptr.size());
@@ -289,15 +289,29 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     for (auto& v : hi) v = hmul(v, C);
     put_eq_split(lo, hi);
     eq_split(elo, ehi, s, (size_t)1 << rh.size(), scratch_eq(), st);
-    CK(cudaMemsetAsync(out, 0, 192 * sizeof(f128), st));
+    CK(cudaMemsetAsync(out, 0, 1024 * sizeof(f128), st));
     size_t n_blocks128 = (size_t)1 << (m - 13);
     zc_round1(a, b, z, tabs_r1, scratch_eq(), n_blocks128, out, sms, st);
-    fetch(out, 192, h_out);
-    P.r1_ab.assign(h_out, h_out + 64);
-    // c-claim ring-switch statistic (suffix r[7..m]) and, from it, the
+    fetch(out, 1024, h_out);
+    // P_AB(l) = sum_k phi8(e_k) H(l, k)
+    const f128* phi8 = phi8_table();
+    P.r1_ab.assign(64, mk(0, 0));
+    for (int l = 0; l < 64; l++)
+      for (int k = 0; k < 8; k++) P.r1_ab[l] = fx(P.r1_ab[l], hmul(phi8[1 << k], h_out[l * 8 + k]));
+    // c-claim ring-switch statistic (suffix r[7..m]):
+    // sv[s + 64 h] = sum_j phi8(g2(j)) H_C(s, h, j), g2(j) = eq(r[7..9], j)
+    // over GF(2^8) with the small constants 0x53, 0xB5
+    s_hat_v_c.assign(128, mk(0, 0));
+    for (int j = 0; j < 4; j++) {
+      uint8_t g2 = 1;
+      g2 = hgf8_mul(g2, (j & 1) ? 0x53 : (uint8_t)(1 ^ 0x53));
+      g2 = hgf8_mul(g2, (j & 2) ? 0xB5 : (uint8_t)(1 ^ 0xB5));
+      for (int h = 0; h < 2; h++)
+        for (int s = 0; s < 64; s++)
+          s_hat_v_c[64 * h + s] = fx(s_hat_v_c[64 * h + s], hmul(phi8[g2], h_out[512 + s * 8 + 4 * h + j]));
+    }
     // extract-c message: S_s = (1 + r6) sv[s] + r6 sv[64 + s];
     // P_C(l) = sum_s phi8(M[l][s]) S_s
-    s_hat_v_c.assign(h_out + 64, h_out + 192);
     P.r1_c.assign(64, mk(0, 0));
     for (int s = 0; s < 64; s++) {
       f128 S = fx(hmul(fx(hone(), r[6]), s_hat_v_c[s]), hmul(r[6], s_hat_v_c[64 + s]));
@@ -330,20 +344,17 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   std::vector<f128> rhos;
   // Message of round k weights pair j by eq(r[7+k..m], j).  Its low bits sit
   // on the fixed small (phi8) and medium (x^(2^t) / (1 + x^(2^t))) challenges:
-  // the kernel needs ns, nm, the medium shifts, K[js] = phi8(g(js)), and eq
-  // over the random suffix (scaled by the medium constant C).
-  auto run_round = [&](int k, bool packed, bool fold, const f128* ain, const f128* bin, f128* aout, f128* bout,
-                       f128 rho, size_t n_pairs) {
+  // the kernel needs ns, nm, the medium shift, and eq over the random suffix
+  // (scaled by the medium constant C); it returns per-js sums that are
+  // weighted here by K[js] = phi8(g(js)).
+  auto run_round = [&](int k, int mode, const f128* ain, const f128* bin, f128* aout, f128* bout, f128 rho,
+                       size_t n_pairs) {
     const int st0 = 7 + k;
     const int ns = std::max(0, 9 - st0);
     const int med0 = std::max(st0, 9);
     const int nm = med0 <= 13 ? 13 - med0 : 0;
-    int shift[4] = {0, 0, 0, 0};
     f128 C = hone();
-    for (int t = 0; t < nm; t++) {
-      shift[t] = 1 << (med0 + t - 9);
-      C = hmul(C, fx(hone(), r[med0 + t]));
-    }
+    for (int t = 0; t < nm; t++) C = hmul(C, fx(hone(), r[med0 + t]));
     const uint8_t sc[3] = {0xF7, 0x53, 0xB5};  // r[6], r[7], r[8] = phi8(sc)
     f128 K[4] = {};
     for (int js = 0; js < (1 << ns); js++) {
@@ -360,11 +371,18 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     std::vector<f128> hi = heq(std::vector<f128>(rs.begin() + es, rs.end()));
     for (auto& v : hi) v = hmul(v, C);
     put_eq_split(lo, hi);
-    CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-    zc_round(packed, fold, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, shift, K, elo, ehi, es, out, G, st);
-    fetch(out, 2, h_out);
+    CK(cudaMemsetAsync(out, 0, 8 * sizeof(f128), st));
+    zc_round(mode, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, med0 - 9, elo, ehi, es, out, G, st);
+    fetch(out, 8, h_out);
+    f128 g1 = mk(0, 0), gi = mk(0, 0);
+    for (int js = 0; js < (1 << ns); js++) {
+      g1 = fx(g1, ns ? hmul(K[js], h_out[2 * js]) : h_out[2 * js]);
+      gi = fx(gi, ns ? hmul(K[js], h_out[2 * js + 1]) : h_out[2 * js + 1]);
+    }
+    h_out[0] = g1;
+    h_out[1] = gi;
   };
-  run_round(0, true, false, a, b, nullptr, nullptr, mk(0, 0), n_words);
+  run_round(0, 0, a, b, nullptr, nullptr, mk(0, 0), n_words);
   f128* av = pp[0];
   f128* bv = pp[1];
   f128* av2 = pp[2];
@@ -377,9 +395,9 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     rhos.push_back(rho);
     if (i < n_mlv - 1) {
       size_t n_pairs_out = (size_t)1 << (n_mlv - i - 2);
-      if (i == 0) run_round(1, true, true, a, b, av, bv, rho, n_pairs_out);
+      if (i == 0) run_round(1, 1, a, b, av, bv, rho, n_pairs_out);
       else {
-        run_round(i + 1, false, true, av, bv, av2, bv2, rho, n_pairs_out);
+        run_round(i + 1, 2, av, bv, av2, bv2, rho, n_pairs_out);
         std::swap(av, av2);
         std::swap(bv, bv2);
       }

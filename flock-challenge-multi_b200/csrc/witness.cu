@@ -25,23 +25,58 @@ __device__ __forceinline__ uint32_t splitmix(uint64_t state) {
   return (uint32_t)(z ^ (z >> 31));
 }
 
+// Words are staged per thread in shared memory, 16 per stream, and written
+// out by the whole warp once every lane has filled a 16-word block: the
+// layout of the 2^14-bit block is data-independent, so all lanes reach the
+// same word at the same time, and the warp stores each thread's 128-byte
+// run with 16 consecutive lanes (two full lines per store instruction).
+constexpr int kWThreads = 128;
+constexpr int kStride = 17;  // words per staged thread row (16 + 1 pad)
+constexpr size_t kWitnessSmem = (size_t)3 * kWThreads * kStride * sizeof(uint64_t);
+
+struct Stage {
+  uint64_t* sm;      // [stream][thread][kStride] for this CTA
+  uint64_t* out[3];  // z, a, b of compression i0 (the warp's first)
+  int lane, warp;
+  uint32_t valid;    // lanes whose compression slot exists
+};
+
+// store words [lo, hi) of block blk of the warp's 32 compressions
+__device__ __forceinline__ void flush(const Stage& S, int blk, int lo, int hi) {
+  __syncwarp();
+#pragma unroll
+  for (int st = 0; st < 3; st++) {
+    const uint64_t* src = S.sm + ((size_t)st * kWThreads + S.warp * 32) * kStride;
+    for (int idx = S.lane; idx < 32 * 16; idx += 32) {
+      const int t = idx >> 4, w = idx & 15;
+      if (w >= lo && w < hi && ((S.valid >> t) & 1))
+        S.out[st][(size_t)t * 256 + blk * 16 + w] = src[t * kStride + w];
+    }
+  }
+  __syncwarp();
+}
+
 struct RowStream {
-  uint64_t* z;
-  uint64_t* a;
-  uint64_t* b;
+  const Stage& S;
+  uint64_t* z;  // this thread's staged rows (stride kWThreads * kStride between streams)
   uint64_t zw = 0, aw = 0, bw = 0;
   int fill = 0;  // bits pending in the accumulators
   int word = 8;  // next u64 index to write (bit 512 starts word 8)
+  __device__ __forceinline__ void emit(uint64_t zv, uint64_t av, uint64_t bv) {
+    const int w = word & 15;
+    z[w] = zv;
+    z[kWThreads * kStride + w] = av;
+    z[2 * kWThreads * kStride + w] = bv;
+    if (w == 15) flush(S, word >> 4, word < 16 ? 8 : 0, 16);
+    word++;
+  }
   __device__ __forceinline__ void put(int n, uint32_t zv, uint32_t av, uint32_t bv) {
     zw |= (uint64_t)zv << fill;
     aw |= (uint64_t)av << fill;
     bw |= (uint64_t)bv << fill;
     int nf = fill + n;
     if (nf >= 64) {
-      z[word] = zw;
-      a[word] = aw;
-      b[word] = bw;
-      word++;
+      emit(zw, aw, bw);
       int used = 64 - fill;  // bits of this field already consumed
       zw = used < 32 ? (uint64_t)(zv >> used) : 0;
       aw = used < 32 ? (uint64_t)(av >> used) : 0;
@@ -62,8 +97,9 @@ struct RowStream {
 __device__ __forceinline__ uint32_t rr(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
 
 __device__ void compression_witness(const uint32_t cv[8], const uint32_t m_in[16], uint32_t tlo, uint32_t thi,
-                                    uint32_t blen, uint32_t flags, uint64_t* z, uint64_t* a, uint64_t* b) {
-  RowStream s{z, a, b};
+                                    uint32_t blen, uint32_t flags, const Stage& S) {
+  uint64_t* row = S.sm + (size_t)threadIdx.x * kStride;
+  RowStream s{S, row};
   s.put(1, 1, 1, 1);  // constant wire at bit 512
   uint32_t m[16];
 #pragma unroll
@@ -110,25 +146,41 @@ __device__ void compression_witness(const uint32_t cv[8], const uint32_t m_in[16
     lo[w] = v[w] ^ v[w + 8];
     s.ident(v[w + 8] ^ cv[w]);  // out_hi at 15153 + 32 w
   }
-  // bit 15409 reached: flush the partial word, then zero padding to 16384
+  // bit 15409 reached: the partial word, then zero padding to 16384
   s.put(0, 0, 0, 0);
-  z[s.word] = s.zw; a[s.word] = s.aw; b[s.word] = s.bw;
-  for (int w = s.word + 1; w < 256; w++) { z[w] = 0; a[w] = 0; b[w] = 0; }
+  s.emit(s.zw, s.aw, s.bw);
+  while (s.word < 256) s.emit(0, 0, 0);
   // prefix: cv (bits 0..255) and out_lo (256..511), rows (v, v, 1)
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     uint64_t c = (uint64_t)cv[2 * k] | ((uint64_t)cv[2 * k + 1] << 32);
     uint64_t o = (uint64_t)lo[2 * k] | ((uint64_t)lo[2 * k + 1] << 32);
-    z[k] = c; a[k] = c; b[k] = ~0ull;
-    z[4 + k] = o; a[4 + k] = o; b[4 + k] = ~0ull;
+    row[k] = c; row[kWThreads * kStride + k] = c; row[2 * kWThreads * kStride + k] = ~0ull;
+    row[4 + k] = o; row[kWThreads * kStride + 4 + k] = o; row[2 * kWThreads * kStride + 4 + k] = ~0ull;
   }
+  flush(S, 0, 0, 8);
+}
+
+__device__ __forceinline__ Stage make_stage(uint64_t* sm, f128* z, f128* a, f128* b, uint32_t n_slots) {
+  Stage S;
+  S.sm = sm;
+  S.lane = threadIdx.x & 31;
+  S.warp = threadIdx.x >> 5;
+  const uint32_t i0 = blockIdx.x * kWThreads + S.warp * 32;
+  S.out[0] = reinterpret_cast<uint64_t*>(z) + (size_t)i0 * 256;
+  S.out[1] = reinterpret_cast<uint64_t*>(a) + (size_t)i0 * 256;
+  S.out[2] = reinterpret_cast<uint64_t*>(b) + (size_t)i0 * 256;
+  S.valid = i0 >= n_slots ? 0u : (n_slots - i0 >= 32 ? 0xffffffffu : (1u << (n_slots - i0)) - 1u);
+  return S;
 }
 }  // namespace
 
-__global__ void k_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32_t n_slots,
-                               f128* __restrict__ z, f128* __restrict__ a, f128* __restrict__ b) {
+__global__ void __launch_bounds__(kWThreads, 4) k_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks,
+                                                           uint32_t n_slots, f128* __restrict__ z,
+                                                           f128* __restrict__ a, f128* __restrict__ b) {
+  extern __shared__ uint64_t wsm[];
+  const Stage S = make_stage(wsm, z, a, b, n_slots);
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_slots) return;
   uint32_t cv[8], m[16], ctr = 0, blen = 0, flags = 0;
   if (i < n_blocks) {
     uint64_t init = seed ^ (((uint64_t)log2 << 29) | ((uint64_t)log2 >> 35));
@@ -147,17 +199,17 @@ __global__ void k_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, 
 #pragma unroll
     for (int w = 0; w < 16; w++) m[w] = 0;
   }
-  size_t off = (size_t)i * 256;
-  compression_witness(cv, m, ctr, 0, blen, flags, reinterpret_cast<uint64_t*>(z) + off,
-                      reinterpret_cast<uint64_t*>(a) + off, reinterpret_cast<uint64_t*>(b) + off);
+  compression_witness(cv, m, ctr, 0, blen, flags, S);
 }
 
 // blocks: 25 u32 per compression (cv[8], m[16], counter_lo); counter_hi = 0,
 // block_len = 64, flags = 11 as in the benchmark generator.
-__global__ void k_witness_blocks(const uint32_t* __restrict__ blocks, uint32_t n_blocks, uint32_t n_slots,
-                                 f128* __restrict__ z, f128* __restrict__ a, f128* __restrict__ b) {
+__global__ void __launch_bounds__(kWThreads, 4) k_witness_blocks(const uint32_t* __restrict__ blocks, uint32_t n_blocks,
+                                                             uint32_t n_slots, f128* __restrict__ z,
+                                                             f128* __restrict__ a, f128* __restrict__ b) {
+  extern __shared__ uint64_t wsm[];
+  const Stage S = make_stage(wsm, z, a, b, n_slots);
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_slots) return;
   uint32_t cv[8] = {0}, m[16] = {0}, ctr = 0, blen = 0, flags = 0;
   if (i < n_blocks) {
     const uint32_t* p = blocks + (size_t)25 * i;
@@ -169,16 +221,20 @@ __global__ void k_witness_blocks(const uint32_t* __restrict__ blocks, uint32_t n
     blen = 64;
     flags = 11;
   }
-  size_t off = (size_t)i * 256;
-  compression_witness(cv, m, ctr, 0, blen, flags, reinterpret_cast<uint64_t*>(z) + off,
-                      reinterpret_cast<uint64_t*>(a) + off, reinterpret_cast<uint64_t*>(b) + off);
+  compression_witness(cv, m, ctr, 0, blen, flags, S);
 }
 
 void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
                          f128* b, cudaStream_t s) {
-  count_launch(); k_witness_seed<<<(n_slots + 127) / 128, 128, 0, s>>>(seed, log2, n_blocks, n_slots, z, a, b);
+  CK(cudaFuncSetAttribute(k_witness_seed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWitnessSmem));
+  count_launch();
+  k_witness_seed<<<(n_slots + kWThreads - 1) / kWThreads, kWThreads, kWitnessSmem, s>>>(seed, log2, n_blocks, n_slots,
+                                                                                     z, a, b);
 }
 void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a, f128* b,
                            cudaStream_t s) {
-  count_launch(); k_witness_blocks<<<(n_slots + 127) / 128, 128, 0, s>>>(blocks, n_blocks, n_slots, z, a, b);
+  CK(cudaFuncSetAttribute(k_witness_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWitnessSmem));
+  count_launch();
+  k_witness_blocks<<<(n_slots + kWThreads - 1) / kWThreads, kWThreads, kWitnessSmem, s>>>(blocks, n_blocks, n_slots,
+                                                                                       z, a, b);
 }
