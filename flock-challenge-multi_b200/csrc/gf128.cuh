@@ -147,6 +147,60 @@ __device__ __forceinline__ f128 multab_mul(const MulTab8* T, f128 y) {
   return acc;
 }
 
+// ---- products by a factor reused across many products ----
+// The factor's side of the Karatsuba tree (its nine 32-bit operands) is
+// split into the four bit classes once; each product then masks only its
+// own operand.
+struct ClassY {
+  uint32_t c0, c1, c2, c3;
+};
+__device__ __forceinline__ ClassY classes_of(uint32_t y) {
+  ClassY r;
+  r.c0 = y & 0x11111111u;
+  r.c1 = y & 0x22222222u;
+  r.c2 = y & 0x44444444u;
+  r.c3 = y & 0x88888888u;
+  return r;
+}
+__device__ __forceinline__ uint64_t clmul32_c(uint32_t x, const ClassY& y) {
+  const uint32_t x0 = x & 0x11111111u, x1 = x & 0x22222222u, x2 = x & 0x44444444u, x3 = x & 0x88888888u;
+  uint64_t z0 = ((uint64_t)x0 * y.c0) ^ ((uint64_t)x1 * y.c3) ^ ((uint64_t)x2 * y.c2) ^ ((uint64_t)x3 * y.c1);
+  uint64_t z1 = ((uint64_t)x0 * y.c1) ^ ((uint64_t)x1 * y.c0) ^ ((uint64_t)x2 * y.c3) ^ ((uint64_t)x3 * y.c2);
+  uint64_t z2 = ((uint64_t)x0 * y.c2) ^ ((uint64_t)x1 * y.c1) ^ ((uint64_t)x2 * y.c0) ^ ((uint64_t)x3 * y.c3);
+  uint64_t z3 = ((uint64_t)x0 * y.c3) ^ ((uint64_t)x1 * y.c2) ^ ((uint64_t)x2 * y.c1) ^ ((uint64_t)x3 * y.c0);
+  return (z0 & 0x1111111111111111ull) | (z1 & 0x2222222222222222ull) | (z2 & 0x4444444444444444ull) |
+         (z3 & 0x8888888888888888ull);
+}
+struct MulConst {
+  ClassY k[9];  // (t0, t1, t0^t1), (t2, t3, t2^t3), (s0, s1, s0^s1), s = lo ^ hi
+};
+__device__ __forceinline__ MulConst mulconst(f128 t) {
+  const uint32_t w0 = (uint32_t)t.lo, w1 = (uint32_t)(t.lo >> 32), w2 = (uint32_t)t.hi, w3 = (uint32_t)(t.hi >> 32);
+  const uint32_t s0 = w0 ^ w2, s1 = w1 ^ w3;
+  MulConst M;
+  M.k[0] = classes_of(w0); M.k[1] = classes_of(w1); M.k[2] = classes_of(w0 ^ w1);
+  M.k[3] = classes_of(w2); M.k[4] = classes_of(w3); M.k[5] = classes_of(w2 ^ w3);
+  M.k[6] = classes_of(s0); M.k[7] = classes_of(s1); M.k[8] = classes_of(s0 ^ s1);
+  return M;
+}
+__device__ __forceinline__ void clmul64_c(uint64_t a, const ClassY* y, uint64_t& lo, uint64_t& hi) {
+  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+  const uint64_t l = clmul32_c(a0, y[0]), h = clmul32_c(a1, y[1]);
+  const uint64_t m = clmul32_c(a0 ^ a1, y[2]) ^ l ^ h;
+  lo = l ^ (m << 32);
+  hi = h ^ (m >> 32);
+}
+// a * t for the t that M was built from (same result as fmul(a, t))
+__device__ __forceinline__ f128 fmul_c(f128 a, const MulConst& M) {
+  uint64_t l0, l1, h0, h1, m0, m1;
+  clmul64_c(a.lo, &M.k[0], l0, l1);
+  clmul64_c(a.hi, &M.k[3], h0, h1);
+  clmul64_c(a.lo ^ a.hi, &M.k[6], m0, m1);
+  m0 ^= l0 ^ h0;
+  m1 ^= l1 ^ h1;
+  return reduce256(l0, l1 ^ m0, h0 ^ m1, h1);
+}
+
 // ---- GF(2^8) ----
 __host__ __device__ __forceinline__ uint8_t gf8_mul_slow(uint8_t a, uint8_t b) {
   uint32_t acc = 0;

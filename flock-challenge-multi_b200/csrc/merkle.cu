@@ -142,7 +142,9 @@ uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, uns
   uint4 d0, d1;
   memcpy(&d0, digest, 16);
   memcpy(&d1, digest + 16, 16);
-  const uint64_t chunk = 1ull << 22;
+  // the smallest valid nonce is expected near 2^bits: scan ranges of twice
+  // that (at least 2^16, at most 2^22) in increasing order
+  const uint64_t chunk = 1ull << (bits + 1 < 16 ? 16 : bits + 1 > 22 ? 22 : bits + 1);
   for (uint64_t start = 0;; start += chunk) {
     *h_found = ~0ull;
     CK(cudaMemcpyAsync(d_found, h_found, 8, cudaMemcpyHostToDevice, s));

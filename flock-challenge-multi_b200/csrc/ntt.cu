@@ -66,26 +66,60 @@ __global__ void __launch_bounds__(512) k_ntt_pass(PassArgs p) {
     tw[k] = twiddle(p.ev, l0 + s, (hi << s) | blk);
   }
   __syncthreads();
-  const int pairs = n_el >> 1;
+  // A thread owns one position pair and `per` of its LG lanes (all of them
+  // once the tile has as many position pairs as threads): the twiddle's
+  // operand split is built once and reused for every lane.  Lanes are
+  // visited in an order rotated by the thread index so that the 8 threads
+  // of a quarter warp read 8 different 16-byte bank groups.
+  const int n_pp = 1 << (R - 1);
+  const int per = min(LG, max(1, (n_pp * LG) / (int)blockDim.x));
+  const int tpp = LG / per;  // threads per position pair
   for (int stg = 0; stg < R; stg++) {
     const int s = TRANSPOSE ? R - 1 - stg : stg;
     const int hb = R - 1 - s;                // local pair bit
-    for (int q = threadIdx.x; q < pairs; q += blockDim.x) {
-      int lane = q & (LG - 1);
-      int pq = q >> p.lg_shift;
-      int top = ((pq >> hb) << (hb + 1)) | (pq & ((1 << hb) - 1));
-      int bot = top | (1 << hb);
-      f128 t = tw[(1 << s) - 1 + (top >> (hb + 1))];
-      f128 u = tile[(top << p.lg_shift) | lane], v = tile[(bot << p.lg_shift) | lane];
-      if (!TRANSPOSE) {
-        u = fx(u, fmul(v, t));
-        v = fx(v, u);
+    for (int w = threadIdx.x; w < n_pp * tpp; w += blockDim.x) {
+      const int pq = w / tpp, lane0 = (w % tpp) * per;
+      const int top = ((pq >> hb) << (hb + 1)) | (pq & ((1 << hb) - 1));
+      const int bot = top | (1 << hb);
+      const MulConst M = mulconst(tw[(1 << s) - 1 + (top >> (hb + 1))]);
+      // lane order rotated by the position pair: lane0 + rot covers all 8
+      // bank groups over 8 consecutive threads for every `per`
+      auto bfly = [&](int lane) {
+        f128 u = tile[(top << p.lg_shift) | lane], v = tile[(bot << p.lg_shift) | lane];
+        if (!TRANSPOSE) {
+          u = fx(u, fmul_c(v, M));
+          v = fx(v, u);
+        } else {
+          u = fx(u, v);
+          v = fx(v, fmul_c(u, M));
+        }
+        tile[(top << p.lg_shift) | lane] = u;
+        tile[(bot << p.lg_shift) | lane] = v;
+      };
+      if (per == 1) {
+        bfly(lane0);
       } else {
-        u = fx(u, v);
-        v = fx(v, fmul(u, t));
+        for (int k = 0; k < per; k += 2) {  // two independent butterflies per step
+          const int l0 = lane0 + ((k + pq) & (per - 1)), l1 = lane0 + ((k + 1 + pq) & (per - 1));
+          f128 u0 = tile[(top << p.lg_shift) | l0], v0 = tile[(bot << p.lg_shift) | l0];
+          f128 u1 = tile[(top << p.lg_shift) | l1], v1 = tile[(bot << p.lg_shift) | l1];
+          if (!TRANSPOSE) {
+            u0 = fx(u0, fmul_c(v0, M));
+            u1 = fx(u1, fmul_c(v1, M));
+            v0 = fx(v0, u0);
+            v1 = fx(v1, u1);
+          } else {
+            u0 = fx(u0, v0);
+            u1 = fx(u1, v1);
+            v0 = fx(v0, fmul_c(u0, M));
+            v1 = fx(v1, fmul_c(u1, M));
+          }
+          tile[(top << p.lg_shift) | l0] = u0;
+          tile[(bot << p.lg_shift) | l0] = v0;
+          tile[(top << p.lg_shift) | l1] = u1;
+          tile[(bot << p.lg_shift) | l1] = v1;
+        }
       }
-      tile[(top << p.lg_shift) | lane] = u;
-      tile[(bot << p.lg_shift) | lane] = v;
     }
     __syncthreads();
   }

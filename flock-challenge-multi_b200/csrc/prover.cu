@@ -344,16 +344,25 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   std::vector<f128> rhos;
   // Message of round k weights pair j by eq(r[7+k..m], j).  Its low bits sit
   // on the fixed small (phi8) and medium (x^(2^t) / (1 + x^(2^t))) challenges:
-  // the kernel needs ns, nm, the medium shift, and eq over the random suffix
-  // (scaled by the medium constant C); it returns per-js sums that are
-  // weighted here by K[js] = phi8(g(js)).
+  // the kernel needs ns, nm, the medium shift, and eq over the random suffix;
+  // it returns per-js sums that are weighted here by
+  // K[js] = phi8(g(js)) * C_round / C_full.
+  // The eq over the random suffix stays on the device: rounds 0..6 share
+  // eq(r[13..m]) (the round-1 table, which carries the medium factor C of
+  // all four medium bits); from round 7 on, each round's table is the
+  // previous one with its lowest variable summed out.
+  f128 C_full = hone();
+  for (f128 bm : medium_consts()) C_full = hmul(C_full, fx(hone(), bm));
+  const f128 C_inv = hinv(C_full);
+  const f128* etab = scratch_eq();
+  size_t etab_len = (size_t)1 << (m - 13), etab_off = etab_len;
   auto run_round = [&](int k, int mode, const f128* ain, const f128* bin, f128* aout, f128* bout, f128 rho,
                        size_t n_pairs) {
     const int st0 = 7 + k;
     const int ns = std::max(0, 9 - st0);
     const int med0 = std::max(st0, 9);
     const int nm = med0 <= 13 ? 13 - med0 : 0;
-    f128 C = hone();
+    f128 C = C_inv;
     for (int t = 0; t < nm; t++) C = hmul(C, fx(hone(), r[med0 + t]));
     const uint8_t sc[3] = {0xF7, 0x53, 0xB5};  // r[6], r[7], r[8] = phi8(sc)
     f128 K[4] = {};
@@ -363,21 +372,22 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
         uint8_t s8 = sc[st0 - 6 + t];
         g = hgf8_mul(g, ((js >> t) & 1) ? s8 : (uint8_t)(1 ^ s8));
       }
-      K[js] = phi8_table()[g];
+      K[js] = hmul(phi8_table()[g], C);
     }
-    std::vector<f128> rs(r.begin() + std::max(st0, 13), r.end());
-    int es = (int)std::min<size_t>(rs.size(), 12);
-    std::vector<f128> lo = heq(std::vector<f128>(rs.begin(), rs.begin() + es));
-    std::vector<f128> hi = heq(std::vector<f128>(rs.begin() + es, rs.end()));
-    for (auto& v : hi) v = hmul(v, C);
-    put_eq_split(lo, hi);
+    if (st0 > 13) {  // drop r[st0 - 1]
+      f128* nxt = scratch_eq() + etab_off;
+      eq_halve(etab, nxt, etab_len / 2, st);
+      etab = nxt;
+      etab_len /= 2;
+      etab_off += etab_len;
+    }
     CK(cudaMemsetAsync(out, 0, 8 * sizeof(f128), st));
-    zc_round(mode, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, med0 - 9, elo, ehi, es, out, G, st);
+    zc_round(mode, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, med0 - 9, etab, out, G, st);
     fetch(out, 8, h_out);
     f128 g1 = mk(0, 0), gi = mk(0, 0);
     for (int js = 0; js < (1 << ns); js++) {
-      g1 = fx(g1, ns ? hmul(K[js], h_out[2 * js]) : h_out[2 * js]);
-      gi = fx(gi, ns ? hmul(K[js], h_out[2 * js + 1]) : h_out[2 * js + 1]);
+      g1 = fx(g1, hmul(K[js], h_out[2 * js]));
+      gi = fx(gi, hmul(K[js], h_out[2 * js + 1]));
     }
     h_out[0] = g1;
     h_out[1] = gi;

@@ -95,24 +95,82 @@ __global__ void k_lc_comb(const uint32_t* __restrict__ at_ptr, const uint16_t* _
   st(comb + c, v);
 }
 
-// z_vec: thread (byte position cb, o-chunk) accumulates 8 columns
-__global__ void __launch_bounds__(128) k_lc_zvec(const uint8_t* __restrict__ z, const f128* __restrict__ eqo,
+// z_vec[i] = XOR over compressions o of eq(x_outer, o) where bit i of o's
+// 2^14-bit block is set (lincheck.rs:2423 partial_fold_packed_z_block_major).
+// A CTA owns 4096 bit positions (one quarter of the block) and a run of
+// compressions; a thread owns 16 positions (one u16 of each block).  For
+// every 8 compressions the CTA builds the 256 subset sums of their eq
+// weights; a thread transposes its 8 u16 words into 16 bytes (bit k of byte
+// p = bit p of compression k) and XORs in one table entry per position.
+namespace {
+constexpr int kZvGroups = 8;  // 8-compression tables built per barrier pair
+
+__device__ __forceinline__ uint64_t transpose8x8(uint64_t x) {
+  uint64_t t;
+  t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+  x = x ^ t ^ (t << 7);
+  t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+  x = x ^ t ^ (t << 14);
+  t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+  x = x ^ t ^ (t << 28);
+  return x;
+}
+}  // namespace
+
+__global__ void __launch_bounds__(256) k_lc_zvec(const uint16_t* __restrict__ z, const f128* __restrict__ eqo,
                                                  size_t n_outer, int chunk, f128* __restrict__ zv) {
-  int cb = blockIdx.x * blockDim.x + threadIdx.x;  // 0..2047
-  size_t o0 = (size_t)blockIdx.y * chunk, o1 = o0 + chunk < n_outer ? o0 + chunk : n_outer;
-  f128 acc[8];
+  __shared__ __align__(16) f128 T[kZvGroups][256];
+  const int col = blockIdx.x;  // quarter of the 2^14-bit block
+  const int t = threadIdx.x;
+  const size_t o0 = (size_t)blockIdx.y * chunk;
+  const size_t o1 = o0 + chunk < n_outer ? o0 + chunk : n_outer;
+  f128 acc[16];
 #pragma unroll
-  for (int k = 0; k < 8; k++) acc[k] = mk(0, 0);
-  for (size_t o = o0; o < o1; o++) {
-    uint32_t byte = z[o * 2048 + cb];
-    if (!byte) continue;
-    f128 e = ldg(eqo + o);
+  for (int p = 0; p < 16; p++) acc[p] = mk(0, 0);
+  for (size_t ob = o0; ob < o1; ob += 8 * kZvGroups) {
+    __syncthreads();
+    // entry v of table g: XOR of eq(o) over the set bits k of v, o = ob + 8g + k
+#pragma unroll 1
+    for (int g = 0; g < kZvGroups; g++) {
+      f128 v = mk(0, 0);
 #pragma unroll
-    for (int k = 0; k < 8; k++)
-      if ((byte >> k) & 1) acc[k] = fx(acc[k], e);
+      for (int k = 0; k < 8; k++) {
+        const size_t o = ob + 8 * g + k;
+        if (((t >> k) & 1) && o < o1) v = fx(v, ldg(eqo + o));
+      }
+      st(&T[g][t], v);
+    }
+    __syncthreads();
+    // the next group's words are loaded while the current one is folded in
+    uint32_t r[8], rn[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) r[k] = ob + k < o1 ? z[(ob + k) * 1024 + col * 256 + t] : 0u;
+#pragma unroll 1
+    for (int g = 0; g < kZvGroups; g++) {
+      const size_t og = ob + 8 * g;
+      if (og >= o1) break;
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const size_t o = og + 8 + k;
+        rn[k] = (g + 1 < kZvGroups && o < o1) ? z[o * 1024 + col * 256 + t] : 0u;
+      }
+      const uint32_t t01 = __byte_perm(r[0], r[1], 0x5140), t23 = __byte_perm(r[2], r[3], 0x5140);
+      const uint32_t t45 = __byte_perm(r[4], r[5], 0x5140), t67 = __byte_perm(r[6], r[7], 0x5140);
+      const uint64_t lo = transpose8x8((uint64_t)__byte_perm(t01, t23, 0x5410) |
+                                       ((uint64_t)__byte_perm(t45, t67, 0x5410) << 32));
+      const uint64_t hi = transpose8x8((uint64_t)__byte_perm(t01, t23, 0x7632) |
+                                       ((uint64_t)__byte_perm(t45, t67, 0x7632) << 32));
+#pragma unroll
+      for (int p = 0; p < 8; p++) {
+        acc[p] = fx(acc[p], ld(&T[g][(lo >> (8 * p)) & 0xFF]));
+        acc[8 + p] = fx(acc[8 + p], ld(&T[g][(hi >> (8 * p)) & 0xFF]));
+      }
+#pragma unroll
+      for (int k = 0; k < 8; k++) r[k] = rn[k];
+    }
   }
 #pragma unroll
-  for (int k = 0; k < 8; k++) atomic_xor128(zv + 8 * cb + k, acc[k]);
+  for (int p = 0; p < 16; p++) atomic_xor128(zv + col * 4096 + 16 * t + p, acc[p]);
 }
 
 // One CTA: optionally bind the top variable at r (fold), then emit (q(1), q(inf)).
@@ -153,9 +211,9 @@ void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_
   count_launch(); k_lc_comb<<<kK_ / 128, 128, 0, s>>>(at_ptr, at_row, bt_ptr, bt_row, eq, alpha, beta, pin, comb);
 }
 void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, f128* zv, cudaStream_t s) {
-  int chunk = 256;
-  dim3 grid(2048 / 128, (unsigned)((n_outer + chunk - 1) / chunk));
-  count_launch(); k_lc_zvec<<<grid, 128, 0, s>>>((const uint8_t*)z, eqo, n_outer, chunk, zv);
+  const int chunk = 1024;  // compressions per CTA (a multiple of 64)
+  dim3 grid(4, (unsigned)((n_outer + chunk - 1) / chunk));
+  count_launch(); k_lc_zvec<<<grid, 256, 0, s>>>((const uint16_t*)z, eqo, n_outer, chunk, zv);
 }
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s) {
   count_launch(); k_lc_round<<<1, 512, 0, s>>>(comb, zv, len, fold, r, emit, out);

@@ -14,18 +14,20 @@
 //  * round 1 folds the packed rows at rho while it reads them:
 //    a'(i) = a^(2i) + rho (a^(2i) + a^(2i+1)) = Lag(row 2i) + rhoLag(row 2i ^
 //    row 2i+1), with rhoLag = rho * Lag built in shared memory by each CTA;
-//  * later rounds fold the previous round's vectors at rho with one product
-//    per element.
+//  * later rounds fold the previous round's vectors at rho through a
+//    CTA-resident 8-bit window table of rho (16 lookups per product: the
+//    shared-memory pipe takes the folds, the integer pipe the messages).
 // The folded vectors are written for the next round.
 //
 // The eq weights exploit the fixed inner challenges of the zerocheck
 // (univariate_skip_optimized.rs:136-233): the low `ns` bits js of j sit on
 // phi8 subfield constants (weight phi8(g(js))) and the next `nm` bits jm on
 // the medium constants (weight C * x^(jm << msh)); the rest is the random
-// suffix, eq(.) = elo x ehi.  A lane owns one js and one group (all bits
-// above js and jm): it sums its 2^nm pairs with shifts, multiplies once by
-// e(group), and keeps the result per js.  The products by phi8(g(js)) are
-// left to the host: out[2 js] = T1(js), out[2 js + 1] = Tinf(js).
+// suffix, whose eq table etab (indexed by group) stays on the device.  A
+// lane owns one js and one group (all bits above js and jm): it sums its
+// 2^nm pairs with shifts, multiplies once by etab[group], and keeps the
+// result per js.  The products by phi8(g(js)) and by the round's constant
+// factor are left to the host: out[2 js] = T1(js), out[2 js + 1] = Tinf(js).
 #include "kernels.cuh"
 
 namespace {
@@ -38,9 +40,7 @@ struct ZcArgs {
   f128 rho;
   size_t n_pairs;   // pairs of the message round
   int ns, nm, msh;
-  const f128* elo;  // eq over the random suffix (x C), indexed by group
-  const f128* ehi;
-  int es;
+  const f128* etab;  // eq over the random suffix, indexed by group
   f128* out;
 };
 
@@ -74,6 +74,7 @@ template <int MODE>
 __global__ void __launch_bounds__(256, 2) k_zc_round(ZcArgs A) {
   extern __shared__ __align__(16) uint8_t smraw[];
   f128* lag = reinterpret_cast<f128*>(smraw);
+  MulTab8* rt = reinterpret_cast<MulTab8*>(smraw);
   if (MODE < 2) {
     for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) {
       f128 v = ldg(A.lag + i);
@@ -81,6 +82,8 @@ __global__ void __launch_bounds__(256, 2) k_zc_round(ZcArgs A) {
       if (MODE == 1) st(lag + 2048 + i, fmul(A.rho, v));
     }
     __syncthreads();
+  } else {
+    multab_build(rt, A.rho);
   }
   const int lane = threadIdx.x & 31;
   const int ns = A.ns, nm = A.nm, gb = ns + nm;
@@ -124,10 +127,10 @@ __global__ void __launch_bounds__(256, 2) k_zc_round(ZcArgs A) {
             av[k] = mk(x.x, x.y);
             bv[k] = mk(y.x, y.y);
           }
-          a0 = fx(av[0], fmul(A.rho, fx(av[0], av[1])));
-          a1 = fx(av[2], fmul(A.rho, fx(av[2], av[3])));
-          b0 = fx(bv[0], fmul(A.rho, fx(bv[0], bv[1])));
-          b1 = fx(bv[2], fmul(A.rho, fx(bv[2], bv[3])));
+          a0 = fx(av[0], multab_mul(rt, fx(av[0], av[1])));
+          a1 = fx(av[2], multab_mul(rt, fx(av[2], av[3])));
+          b0 = fx(bv[0], multab_mul(rt, fx(bv[0], bv[1])));
+          b1 = fx(bv[2], multab_mul(rt, fx(bv[2], bv[3])));
         }
         st(A.a_out + 2 * j, a0);
         st(A.a_out + 2 * j + 1, a1);
@@ -140,7 +143,7 @@ __global__ void __launch_bounds__(256, 2) k_zc_round(ZcArgs A) {
       acc_shl(s1, fmul(a1, b1), sh);
       acc_shl(si, fmul(ad, bd), sh);
     }
-    const f128 e = fmul(ldg(A.elo + (grp & ((1ull << A.es) - 1))), ldg(A.ehi + (grp >> A.es)));
+    const f128 e = ldg(A.etab + grp);
     T1 = fx(T1, fmul(reduce256(s1.w0, s1.w1, s1.w2, 0), e));
     Ti = fx(Ti, fmul(reduce256(si.w0, si.w1, si.w2, 0), e));
   }
@@ -167,15 +170,14 @@ __global__ void __launch_bounds__(256, 2) k_zc_round(ZcArgs A) {
 // One zerocheck round launch: out[2 js + {0, 1}] ^= (T1, Tinf)(js) for js < 2^ns.
 // mode 0: packed message round, 1: packed fold + message, 2: fold + message.
 void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag, f128 rho,
-              size_t n_pairs, int ns, int nm, int msh, const f128* elo, const f128* ehi, int es, f128* out, int grid,
-              cudaStream_t s) {
+              size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int grid, cudaStream_t s) {
   if (ns < 0 || ns > 2 || nm < 0 || nm > 4 || msh < 0 || (nm > 0 && (((1 << nm) - 1) << msh) >= 64))
     throw CudaError("zc_round: bad eq structure");
   ZcArgs A;
   A.a_in = a_in; A.b_in = b_in; A.a_out = a_out; A.b_out = b_out; A.lag = lag; A.rho = rho;
   A.n_pairs = n_pairs; A.ns = ns; A.nm = nm; A.msh = msh;
-  A.elo = elo; A.ehi = ehi; A.es = es; A.out = out;
-  const size_t smem = mode == 0 ? 2048 * sizeof(f128) : mode == 1 ? 4096 * sizeof(f128) : 0;
+  A.etab = etab; A.out = out;
+  const size_t smem = mode == 0 ? 2048 * sizeof(f128) : mode == 1 ? 4096 * sizeof(f128) : sizeof(MulTab8);
   const size_t lanes = (n_pairs + ((size_t)1 << nm) - 1) >> nm;
   const int g = (int)std::max<size_t>(1, std::min<size_t>((size_t)grid, (lanes + 255) / 256));
   count_launch();
@@ -186,6 +188,19 @@ void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b
     CK(cudaFuncSetAttribute(k_zc_round<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_zc_round<1><<<g, 256, smem, s>>>(A);
   } else {
-    k_zc_round<2><<<g, 256, 0, s>>>(A);
+    CK(cudaFuncSetAttribute(k_zc_round<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_zc_round<2><<<g, 256, smem, s>>>(A);
   }
+}
+
+__global__ void k_eq_halve(const f128* __restrict__ in, f128* __restrict__ out, size_t n_out) {
+  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n_out) st(out + j, fx(ldg(in + 2 * j), ldg(in + 2 * j + 1)));
+}
+
+// out[j] = in[2j] + in[2j+1]: eq over r[t+1..] from eq over r[t..] (the
+// dropped variable's two weights sum to one)
+void eq_halve(const f128* in, f128* out, size_t n_out, cudaStream_t s) {
+  count_launch();
+  k_eq_halve<<<(unsigned)((n_out + 255) / 256), 256, 0, s>>>(in, out, n_out);
 }
