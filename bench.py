@@ -30,18 +30,25 @@ LOG2 = 18
 METRIC = "verified BLAKE3 compressions/sec on 1 B200 (2^18/proof); p50/p99 proof latency served"
 PUBLISHED_CPU = 381080.0  # reference, c7i.4xlarge 16 vCPU (README.md:95-98)
 PHASE_KERNEL = {
-    # phase -> (kernel, algorithmic bytes per launch at m = 32, description)
-    "zerocheck_round1": ("k_zc_round1", 3 * (1 << 29), "reads packed a, b, c (3 x 512 MiB)"),
-    "commit": ("k_ntt_pass + k_merkle_leaves", (1 << 29) + 2 * (1 << 30) + (1 << 30) + (1 << 26),
-               "RS encode 512 MiB -> 1 GiB, leaf hashing reads 1 GiB, 64 MiB tree"),
-    "zerocheck_rounds": ("k_zc_msg0 + k_zc_fold_msg", 2 * (1 << 30) + 2 * (1 << 30) + 2 * (1 << 30),
-                         "round 0 reads a, b; folds stream 2 x 512 MiB halving"),
-    "ring_switch_combine": ("k_shat + k_bcombined", 2 * (1 << 29) * 3 + (1 << 29),
-                            "eq tables 2 x 512 MiB written/read, z read twice, b_combined 512 MiB"),
-    "ligerito_l0_folds": ("k_lig_fold_msg", 4 * (1 << 30), "6 folds over f, b (2 x 512 MiB, halving)"),
-    "lincheck": ("k_lc_zvec", 1 << 29, "reads z (512 MiB)"),
-    "witness": ("k_witness_seed", 3 * (1 << 29), "writes z, a, b (3 x 512 MiB)"),
-    "ligerito_levels": ("levels", 1 << 27, "recursive levels"),
+    # phase -> (kernel, algorithmic bytes per proof at m = 32, launches per proof, description)
+    "rs_encode": ("k_ntt_pass", 2 * 2 * (1 << 30), 2,
+                  "two passes (10 + 9 of the 19 butterfly layers), each reads and writes the 1 GiB codeword"),
+    "merkle_commit": ("k_merkle_leaves", (1 << 30) + (1 << 25), 1, "reads the 1 GiB codeword, writes 32 MiB of leaf CVs"),
+    "zerocheck_round1": ("k_zc_round1_ab", 2 * (1 << 29), 1, "reads packed a, b (2 x 512 MiB)"),
+    "zerocheck_rounds": ("k_zc_round", 2 * (1 << 29) + 4 * (1 << 29) + 3 * (1 << 29), 26,
+                         "round 0 reads a, b; round 1 reads a, b, writes the folded pair; then halving"),
+    "ring_switch_combine": ("k_bcombined_ct", 1 << 29, 1, "writes b_combined (512 MiB)"),
+    "ligerito_l0_folds": ("k_lig_fold_msg", 4 * (1 << 29), 6, "6 folds over f, b (2 x 512 MiB, halving)"),
+    "lincheck": ("k_lc_zvec", 1 << 29, 1, "reads z (512 MiB)"),
+    "witness": ("k_witness_seed", 3 * (1 << 29), 1, "writes z, a, b (3 x 512 MiB)"),
+    "ligerito_levels": ("levels", 1 << 27, 1, "recursive levels"),
+}
+
+
+# kernels whose bound is the integer pipe rather than HBM (ncu captures under profiles/)
+INT_NOTES = {
+    "k_ntt_pass": "6.4e8 GF(2^128) products per proof; ALU pipe ~51%, FMA pipe ~40% busy (ncu, "
+                  "profiles/k_ntt_pass_2p16.md)",
 }
 
 
@@ -208,9 +215,10 @@ def run_ours(args, world, rank, local):
     value = n / (max_ms / 1e3)
     peak, peak_kind = peaks()
     dom = max(phases, key=phases.get)
-    kname, kbytes, kdesc = PHASE_KERNEL[dom]
+    kname, kbytes, klaunches, kdesc = PHASE_KERNEL[dom]
     scale = 1 << (log2 - 18) if log2 >= 18 else 1.0 / (1 << (18 - log2))
     kbytes = int(kbytes * scale)
+    # the phase's events bracket only its own launches on the prover stream
     achieved = kbytes / (phases[dom] / 1e3) / 1e9
     traffic = None
     tfile = REPO / "profiles" / "traffic.json"
@@ -229,8 +237,11 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(launches),
         "phases_ms": {k: round(v, 3) for k, v in phases.items()},
         "roofline": {"bound": "hbm", "kernel": kname, "phase": dom, "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                     "algorithmic_bytes": kbytes, "note": f"{kdesc}; peak {peak_kind}"},
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": (traffic * scale / klaunches) if traffic else None,
+                     "algorithmic_bytes": kbytes // klaunches, "launches": klaunches,
+                     "note": f"{kdesc}; per launch; peak {peak_kind}" +
+                             ("; integer-pipe bound: " + INT_NOTES[kname] if kname in INT_NOTES else "")},
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:

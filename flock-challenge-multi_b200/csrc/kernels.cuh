@@ -45,6 +45,8 @@ uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, uns
 // K3..K8
 void eq_split(const f128* lo, const f128* hi, int s_bits, size_t n, f128* out, cudaStream_t s);
 void axpy(f128* out, const f128* x, f128 beta, size_t n, cudaStream_t s);
+void eq_build(const f128* r, int n, f128 scale, f128* out, cudaStream_t s);
+void outer64(const f128* L, const f128* e, size_t n_e, f128* out, cudaStream_t s);
 void inner(const f128* f, const f128* g, size_t n, f128* out, int grid, cudaStream_t s);
 size_t round1_tables_size();
 void build_round1_tables_host(const uint8_t M[64][64], const f128* phi8, void* dst);

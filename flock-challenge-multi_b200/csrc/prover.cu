@@ -158,18 +158,9 @@ void Setup::build_round1_tables() {
 void Setup::eq_table(const std::vector<f128>& r, f128* dev) {
   size_t n = r.size();
   int s = (int)std::min<size_t>(n, 12);
-  std::vector<f128> lo = heq(std::vector<f128>(r.begin(), r.begin() + s));
-  std::vector<f128> hi = heq(std::vector<f128>(r.begin() + s, r.end()));
-  put_eq_split(lo, hi);
+  eq_build(r.data(), s, hone(), elo, st);
+  eq_build(r.data() + s, (int)n - s, hone(), ehi, st);
   eq_split(elo, ehi, s, (size_t)1 << n, dev, st);
-}
-
-void Setup::put_eq_split(const std::vector<f128>& lo, const std::vector<f128>& hi) {
-  if (hi.size() > (1u << 16) || lo.size() > (1u << 13)) throw std::runtime_error("eq split too large");
-  CK(cudaMemcpyAsync(elo, lo.data(), lo.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(ehi, hi.data(), hi.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
-  // host vectors must stay alive until the copies complete
-  CK(cudaStreamSynchronize(st));
 }
 
 void Setup::fetch(const f128* dev, size_t n, f128* host) {
@@ -262,9 +253,10 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   mark(1);
   // ---- K1 + K2 commit: 64 interleaved lanes, rate 1/2, 1 KiB leaves
   ntt_rs_encode(z, cw0, m - 13, 64, 1, st);
+  mark(2);
   merkle_build(cw0, n_leaves0, 64 * 16, tree0, st);
   P.root = root_of(tree0, n_leaves0);
-  mark(2);
+  mark(3);
 
   Transcript tr(domain);
   tr.label("flock-r1cs-v0");
@@ -284,10 +276,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     for (f128 bm : med) C = hmul(C, fx(hone(), bm));
     std::vector<f128> rh(r.begin() + 13, r.end());
     int s = (int)std::min<size_t>(rh.size(), 12);
-    std::vector<f128> lo = heq(std::vector<f128>(rh.begin(), rh.begin() + s));
-    std::vector<f128> hi = heq(std::vector<f128>(rh.begin() + s, rh.end()));
-    for (auto& v : hi) v = hmul(v, C);
-    put_eq_split(lo, hi);
+    eq_build(rh.data(), s, hone(), elo, st);
+    eq_build(rh.data() + s, (int)rh.size() - s, C, ehi, st);
     eq_split(elo, ehi, s, (size_t)1 << rh.size(), scratch_eq(), st);
     CK(cudaMemsetAsync(out, 0, 1024 * sizeof(f128), st));
     size_t n_blocks128 = (size_t)1 << (m - 13);
@@ -319,7 +309,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
         if (lde_m[l][s]) P.r1_c[l] = fx(P.r1_c[l], hmul(phi8_table()[lde_m[l][s]], S));
     }
   }
-  mark(3);
+  mark(4);
   tr.f128s(P.r1_ab.data(), 64);
   tr.f128s(P.r1_c.data(), 64);
   f128 zc_z = tr.sample();
@@ -420,7 +410,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   }
   tr.f128v(P.fa);
   tr.f128v(P.fb);
-  mark(4);
+  mark(5);
 
   // ---- lincheck
   const int ir = kKLog - kKSkip;
@@ -429,10 +419,10 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   f128 alpha = tr.sample();
   f128 beta = tr.sample();
   {
-    std::vector<f128> L = hlagrange(zc_z, 0), er = heq(x_inner), ei(kK);
-    for (size_t k = 0; k < er.size(); k++)
-      for (int s = 0; s < 64; s++) ei[s + 64 * k] = hmul(L[s], er[k]);
-    CK(cudaMemcpyAsync(eq_inner, ei.data(), kK * sizeof(f128), cudaMemcpyHostToDevice, st));
+    // eq_inner[s + 64 k] = L_s(z) eq(x_inner, k)
+    std::vector<f128> L = hlagrange(zc_z, 0);
+    eq_build(x_inner.data(), (int)x_inner.size(), hone(), zv_pre, st);
+    outer64(L.data(), zv_pre, (size_t)1 << x_inner.size(), eq_inner, st);
     lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, kZConst, comb, st);
     eq_table(x_outer, scratch_eq());
     CK(cudaMemsetAsync(zv, 0, kK * sizeof(f128), st));
@@ -460,7 +450,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   f128 r_skip2 = tr.sample();
   std::vector<f128> r_inner_rest(rr.rbegin(), rr.rend());
   (void)r_skip2;
-  mark(5);
+  mark(6);
 
   // ---- PCS open: ring switches + combine
   tr.label("flock-pcs-open-batch-v0");
@@ -513,24 +503,21 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     }
     CK(cudaMemcpyAsync(bc_tabs, T.data(), T.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
     // eq(suffix_k, i) = lo_k(i mod 2^12) * hi_k(i >> 12), both tables on the device
-    std::vector<f128> lo[2], hi[2];
     int lo_bits = (int)std::min<size_t>(x_ab.size() - 1, 12);
+    const int hi_bits = (int)x_ab.size() - 1 - lo_bits;
+    f128* d = eqbuf[0];  // [lo0 | hi0 | lo1 | hi1]
+    const size_t nlo = (size_t)1 << lo_bits, nhi = (size_t)1 << hi_bits;
     for (int k = 0; k < 2; k++) {
       const std::vector<f128>& xf = k == 0 ? x_ab : x_c;
-      lo[k] = heq(std::vector<f128>(xf.begin() + 1, xf.begin() + 1 + lo_bits));
-      hi[k] = heq(std::vector<f128>(xf.begin() + 1 + lo_bits, xf.end()));
+      f128* base = d + k * (nlo + nhi);
+      eq_build(xf.data() + 1, lo_bits, hone(), base, st);
+      eq_build(xf.data() + 1 + lo_bits, hi_bits, hone(), base + nlo, st);
     }
-    f128* d = eqbuf[0];  // [lo0 | hi0 | lo1 | hi1]
-    size_t nlo = lo[0].size(), nhi = hi[0].size();
-    CK(cudaMemcpyAsync(d, lo[0].data(), nlo * sizeof(f128), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(d + nlo, hi[0].data(), nhi * sizeof(f128), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(d + nlo + nhi, lo[1].data(), nlo * sizeof(f128), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(d + 2 * nlo + nhi, hi[1].data(), nhi * sizeof(f128), cudaMemcpyHostToDevice, st));
     ring_bcombined_ct(d, d + nlo, d + nlo + nhi, d + 2 * nlo + nhi, bc_tabs, bc_tabs + 4096, lo_bits, nhi, pp[1],
                       sms, st);
     CK(cudaStreamSynchronize(st));
   }
-  mark(6);
+  mark(7);
 
   // ---- Ligerito
   const Ladder& Ld = *lad;
@@ -606,7 +593,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   std::vector<f128> lane_rs;
   for (int j = 0; j < Ld.initial_k; j++) lane_rs.push_back(fold_round(std::max(0, Ld.fold_grind[0] - j)));
   n_cur -= Ld.initial_k;
-  mark(7);
+  mark(8);
   // level 1 commit
   auto commit = [&](Level& L) {
     ntt_rs_encode(f, L.cw, L.log_msg_pos, L.lanes, L.rate, st);
@@ -648,7 +635,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     P.levels.push_back(open(prev.cw, prev.tree, prev.positions, prev.lanes, qi));
     induce(qi, al, prev.rate);
   }
-  mark(8);
+  mark(9);
   CK(cudaStreamSynchronize(st));
   std::vector<uint8_t> bytes = encode(P);
   return bytes;

@@ -20,7 +20,8 @@ struct Level {
 
 class Setup {
  public:
-  static constexpr int kPhases = 8;  // witness, commit, round1, zc rounds, lincheck, ring switch, L0 folds, levels
+  static constexpr int kPhases = 9;  // witness, RS encode, Merkle commit, round1, zc rounds, lincheck,
+                                     // ring switch, L0 folds, levels
   Setup(int device, uint32_t log2);
   ~Setup();
   Setup(const Setup&) = delete;
@@ -41,7 +42,6 @@ class Setup {
  private:
   void build_round1_tables();
   void eq_table(const std::vector<f128>& r, f128* dev);
-  void put_eq_split(const std::vector<f128>& lo, const std::vector<f128>& hi);
   void fetch(const f128* dev, size_t n, f128* host);
   uint64_t grind(Transcript& tr, uint32_t bits);
   std::vector<size_t> sample_queries(Transcript& tr, size_t block_len, size_t count);

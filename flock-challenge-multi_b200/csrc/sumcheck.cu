@@ -52,6 +52,32 @@ __global__ void k_eq_split(const f128* __restrict__ lo, const f128* __restrict__
   st(out + i, fmul(ldg(lo + (i & ((1ull << s) - 1))), ldg(hi + (i >> s))));
 }
 
+// eq tables built on the device: out[i] = scale * prod_j (bit j of i ? r_j : 1 + r_j)
+// (the same values as the doubling construction of eq(r, .), field products
+// being exact)
+struct EqVec {
+  f128 r[24];
+  f128 scale;
+  int n;
+};
+__global__ void k_eq_build(EqVec E, f128* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ((size_t)1 << E.n)) return;
+  f128 v = E.scale;
+  for (int j = 0; j < E.n; j++) v = fmul(v, ((i >> j) & 1) ? E.r[j] : fx(E.r[j], mk(1, 0)));
+  st(out + i, v);
+}
+
+// out[s + 64 k] = L[s] * e[k]
+struct Vec64 {
+  f128 v[64];
+};
+__global__ void k_outer64(Vec64 L, const f128* __restrict__ e, size_t n_e, f128* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 64 * n_e) return;
+  st(out + i, fmul(L.v[i & 63], ldg(e + (i >> 6))));
+}
+
 // out[i] += beta * x[i]
 __global__ void k_axpy(f128* __restrict__ out, const f128* __restrict__ x, f128 beta, size_t n) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -279,6 +305,22 @@ void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size
 }
 void eq_split(const f128* lo, const f128* hi, int s_bits, size_t n, f128* out, cudaStream_t s) {
   count_launch(); k_eq_split<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(lo, hi, s_bits, n, out);
+}
+void eq_build(const f128* r, int n, f128 scale, f128* out, cudaStream_t s) {
+  if (n < 0 || n > 24) throw CudaError("eq_build: at most 24 variables");
+  EqVec E;
+  for (int j = 0; j < n; j++) E.r[j] = r[j];
+  E.scale = scale;
+  E.n = n;
+  const size_t len = (size_t)1 << n;
+  count_launch();
+  k_eq_build<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(E, out);
+}
+void outer64(const f128* L, const f128* e, size_t n_e, f128* out, cudaStream_t s) {
+  Vec64 V;
+  for (int j = 0; j < 64; j++) V.v[j] = L[j];
+  count_launch();
+  k_outer64<<<(unsigned)((64 * n_e + 255) / 256), 256, 0, s>>>(V, e, n_e, out);
 }
 void axpy(f128* out, const f128* x, f128 beta, size_t n, cudaStream_t s) {
   count_launch(); k_axpy<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, x, beta, n);

@@ -27,7 +27,7 @@ EXPORTS = (
     "flock_pow", "flock_f128_mul", "flock_statement_digest", "flock_bench_ntt",
     "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove", "flock_merkle_root_noalloc",
 )
-PHASES = ("witness", "commit", "zerocheck_round1", "zerocheck_rounds", "lincheck",
+PHASES = ("witness", "rs_encode", "merkle_commit", "zerocheck_round1", "zerocheck_rounds", "lincheck",
           "ring_switch_combine", "ligerito_l0_folds", "ligerito_levels")
 
 _lib = None

@@ -63,9 +63,9 @@ int flock_prove_seed(flock_setup* s, uint64_t seed, const uint8_t* domain, size_
  * block_len 64, flags 11, n == 2^log2_n. */
 int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const uint8_t* domain, size_t dlen,
                        uint8_t* out, size_t cap, size_t* out_len);
-/* Device milliseconds of the last proof's phases (witness, commit, zerocheck
- * round 1, zerocheck rounds, lincheck, ring switch + combine, Ligerito L0
- * folds, Ligerito levels).  Returns the number written. */
+/* Device milliseconds of the last proof's phases (witness, RS encode, Merkle
+ * commit, zerocheck round 1, zerocheck rounds, lincheck, ring switch +
+ * combine, Ligerito L0 folds, Ligerito levels).  Returns the number written. */
 int flock_setup_phase_ms(flock_setup* s, double* ms, int n);
 
 /* Kernel-level entry points (host buffers). */

@@ -130,4 +130,5 @@ def test_golden_larger(gpu_ctx):
 def test_phase_times_reported(prover8):
     prover8.prove_seed(5)
     ph = prover8.phase_ms()
-    assert len(ph) == 8 and all(v >= 0 for v in ph.values())
+    import flockgpu
+    assert list(ph) == list(flockgpu.PHASES) and all(v >= 0 for v in ph.values())
