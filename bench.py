@@ -15,7 +15,9 @@ own seeds, timing is the max over ranks of the device time.
 """
 import argparse
 import json
+import multiprocessing as mp
 import os
+import random
 import statistics
 import subprocess
 import sys
@@ -28,7 +30,8 @@ sys.path.insert(0, str(REPO / "flock-challenge-multi_b200"))
 
 LOG2 = 18
 METRIC = "verified BLAKE3 compressions/sec on 1 B200 (2^18/proof); p50/p99 proof latency served"
-PUBLISHED_CPU = 381080.0  # reference, c7i.4xlarge 16 vCPU (README.md:95-98)
+PUBLISHED_CPU = 381080.0
+SERVE_SLOTS = 4  # reference, c7i.4xlarge 16 vCPU (README.md:95-98)
 PHASE_KERNEL = {
     # phase -> (kernel, algorithmic bytes per proof at m = 32, launches per proof, description)
     "rs_encode": ("k_ntt_pass", 2 * 2 * (1 << 30), 2,
@@ -129,18 +132,9 @@ def barrier(world: int) -> None:
 
 
 def host_blocks(log2: int, seed: int):
-    """Benchmark inputs on the host (benchmark-tools/common/src/lib.rs:25-37),
-    vectorised SplitMix64: draw j of compression i uses state init+(25i+j+1)g."""
-    import numpy as np
-    g = np.uint64(0x9E3779B97F4A7C15)
-    init = np.uint64((seed ^ (((log2 << 29) | (log2 >> 35)) & (2**64 - 1))) & (2**64 - 1))
-    idx = np.arange(25 << log2, dtype=np.uint64) + np.uint64(1)
-    with np.errstate(over="ignore"):
-        z = init + idx * g
-        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
-        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
-        z = z ^ (z >> np.uint64(31))
-    return z.astype(np.uint32).reshape(-1, 25)
+    """Benchmark inputs on the host (the library's generate_compressions)."""
+    import flockgpu
+    return flockgpu.generate_compressions(log2, seed)
 
 
 def cpu_baseline_sample() -> dict:
@@ -166,26 +160,136 @@ def run_reference(args, world, rank):
     if not lib.exists():
         subprocess.run(["make", "-C", str(REPO / "oracle")], check=True, capture_output=True)
     import oracle_lib
-    o = oracle_lib.Oracle()
     log2 = 10
-    for i in range(args.warmup):
-        o.time_prove(log2, 1000 + i)
-    times = [o.time_prove(log2, 2000 + i)[0] for i in range(args.steps)]
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    # one single-threaded oracle proof per host core, run concurrently: a step is
+    # `cores` proofs of 2^10 compressions (a bounded sample of the 2^18 workload)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_oracle_proof, [(log2, 1000 + i) for i in range(cores)] * max(args.warmup, 1))
+        times = []
+        for i in range(args.steps):
+            t0 = time.perf_counter()
+            pool.map(_oracle_proof, [(log2, 2000 + 97 * i + c) for c in range(cores)])
+            times.append(time.perf_counter() - t0)
     tot = sum(times)
-    value = args.steps * (1 << log2) / tot
+    value = args.steps * cores * (1 << log2) / tot
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "compressions/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_CPU, "dtype": "gf2^128/u32",
         "data": "synthetic (benchmark SplitMix64 generator)",
-        "config": {"workload": f"single proof of 2^{log2} BLAKE3 compressions per step (bounded CPU sample of the "
-                               f"2^18 workload)", "log2": log2, "parallelism": "cpu, 1 thread"},
-        "cpu_baseline": {"value": value, "unit": "compressions/s", "cores": 1, "kind": "port",
-                         "sample": f"{args.steps} oracle proofs of 2^{log2} compressions (the reference Rust "
-                                   f"prover cannot be built here: no cargo/rustc)"},
+        "config": {"workload": f"{cores} concurrent proofs of 2^{log2} BLAKE3 compressions per step (bounded CPU "
+                               f"sample of the 2^18 workload)", "log2": log2,
+                   "parallelism": f"cpu, {cores} processes x 1 thread"},
+        "cpu_baseline": {"value": value, "unit": "compressions/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} steps of {cores} concurrent oracle proofs of 2^{log2} compressions "
+                                   f"(the reference Rust prover cannot be built here: no cargo/rustc)"},
         "e2e": {"value": value, "unit": "compressions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def _oracle_proof(job):
+    log2, seed = job
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle_lib
+    return oracle_lib.Oracle().time_prove(log2, seed)[0]
+
+
+def splitmix64(seed: int):
+    """The benchmark's SplitMix64 stream (benchmark-tools/common/src/lib.rs)."""
+    state = seed & (2**64 - 1)
+    while True:
+        state = (state + 0x9E3779B97F4A7C15) & (2**64 - 1)
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & (2**64 - 1)
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & (2**64 - 1)
+        yield z ^ (z >> 31)
+
+
+def job_mix(n: int, lo: int, hi: int, seed: int):
+    """n jobs, log2 log-uniform over [lo, hi] (log2 = lo + floor(u (hi - lo + 1))), own seeds."""
+    g = splitmix64(seed)
+    return [(lo + (next(g) * (hi - lo + 1) >> 64), next(g)) for _ in range(n)]
+
+
+def plain_seconds(ctx, jobs):
+    """Wall time of the jobs proved one at a time through the plain entry point
+    (setups made beforehand, untimed)."""
+    import flockgpu
+    provers = {l: flockgpu.Prover(ctx, l) for l in sorted({l for l, _ in jobs})}
+    try:
+        for l, p in provers.items():
+            p.prove_seed(1)  # warm
+        t0 = time.perf_counter()
+        for l, s in jobs:
+            provers[l].prove_seed(s)
+        return time.perf_counter() - t0
+    finally:
+        for p in provers.values():
+            p.close()
+
+
+def served_run(ctx, jobs, rate=None):
+    """Submit the jobs (all at once, or Poisson arrivals at `rate` jobs/s) and
+    collect them; returns (wall seconds, latencies in ms)."""
+    rng = random.Random(7)
+    t0 = time.perf_counter()
+    tickets, when = [], 0.0
+    for l, s in jobs:
+        if rate:
+            when += rng.expovariate(rate)
+            dt = t0 + when - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+        tickets.append(ctx.submit(l, s))
+    lat = [ctx.poll(t)["latency_ms"] for t in tickets]
+    return time.perf_counter() - t0, lat
+
+
+def pct(v, q):
+    v = sorted(v)
+    k = (len(v) - 1) * q
+    i = int(k)
+    return v[i] + (v[min(i + 1, len(v) - 1)] - v[i]) * (k - i)
+
+
+def serving_report(device: int, full: bool):
+    """Batched (64 uneven jobs, 2^12..2^18, all at once) and served (Poisson
+    arrivals, p50/p99) against the plain one-proof-at-a-time form."""
+    import flockgpu
+    out = {}
+    ctx = flockgpu.Context(device, hbm_budget_bytes=150 << 30)
+    try:
+        ctx.serve_start(SERVE_SLOTS)
+        jobs = job_mix(64, 12, 18, 3)
+        n = sum(1 << l for l, _ in jobs)
+        served_run(ctx, jobs)  # warm: setups of every size cached
+        wall, lat = served_run(ctx, jobs)
+        plain = plain_seconds(ctx, jobs)
+        out["batched"] = {"jobs": len(jobs), "log2_range": [12, 18], "compressions": n,
+                          "value": n / wall, "unit": "compressions/s", "plain_value": n / plain,
+                          "speedup_vs_plain": plain / wall, "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
+                          "slots": SERVE_SLOTS}
+        lo, hi = (10, 20) if full else (10, 18)
+        jobs = job_mix(48 if not full else 96, lo, hi, 4)
+        n = sum(1 << l for l, _ in jobs)
+        served_run(ctx, jobs)  # warm
+        plain = plain_seconds(ctx, jobs)
+        cap = len(jobs) / plain  # plain capacity in jobs/s for this size mix
+        rates = [0.25, 0.5, 1.0, 2.0] if full else [1.0]
+        out["served"] = []
+        for f in rates:
+            wall, lat = served_run(ctx, jobs, rate=f * cap)
+            out["served"].append({"arrival_rate_x_plain_capacity": f, "jobs": len(jobs), "log2_range": [lo, hi],
+                                  "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
+                                  "sustained_value": n / wall, "plain_value": n / plain,
+                                  "unit": "compressions/s", "slots": SERVE_SLOTS,
+                                  "hbm_budget_gb": 150})
+    finally:
+        ctx.close()
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -246,6 +350,9 @@ def run_ours(args, world, rank, local):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
+    if world == 1 and not args.no_serve:
+        prover.close()
+        line.update(serving_report(local, full=False))
     print(json.dumps(line), flush=True)
     prover.close()
 
@@ -258,9 +365,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--log2", type=int, default=LOG2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the batched / served measurements")
+    ap.add_argument("--serve", action="store_true",
+                    help="only the batched + served report: 64 uneven jobs, then Poisson arrivals at 4 rates")
     args = ap.parse_args()
     world, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                     int(os.environ.get("RANK", "0")), 0)
+    if args.serve:
+        if rank == 0:
+            print(json.dumps({"metric": "served/batched proof throughput and latency", **serving_report(0, True)}),
+                  flush=True)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
     else:

@@ -2,6 +2,8 @@
 // Status codes, never exceptions across the ABI; caller-owned buffers.
 #include "../../include/flock_gpu.h"
 #include "prover.hpp"
+#include "serve.hpp"
+#include <atomic>
 #include <memory>
 #include <mutex>
 
@@ -11,14 +13,15 @@ struct flock_ctx {
   cudaStream_t st = nullptr;
   std::string err;
   std::mutex mu;
+  std::unique_ptr<flock::Server> server;
 };
 struct flock_setup {
   flock_ctx* ctx = nullptr;
   std::unique_ptr<flock::Setup> s;
 };
 
-uint64_t& kernel_launch_counter() {
-  static uint64_t n = 0;
+std::atomic<uint64_t>& kernel_launch_counter() {
+  static std::atomic<uint64_t> n{0};
   return n;
 }
 
@@ -81,6 +84,7 @@ int flock_ctx_create(int device, uint64_t hbm_budget_bytes, flock_ctx** out) {
 
 void flock_ctx_destroy(flock_ctx* c) {
   if (!c) return;
+  c->server.reset();  // joins the serving threads, frees their setups
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -135,6 +139,76 @@ int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const u
     CK(cudaMemcpyAsync(s->s->blocks_buf, blocks, n * 25 * sizeof(uint32_t), cudaMemcpyHostToDevice, s->s->st));
     std::string d((const char*)domain, dlen);
     return emit(s->ctx, s->s->prove(nullptr, s->s->blocks_buf, n, d), out, cap, out_len);
+  });
+}
+
+int flock_serve_start(flock_ctx* c, int slots) {
+  if (!c || slots < 1 || slots > 64) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (c->server) {
+      c->err = "serving already started";
+      return FLOCK_ERR_ARG;
+    }
+    uint64_t budget = c->budget;
+    if (!budget) {  // default: the device's free memory less 4 GiB of headroom
+      size_t free_b = 0, total_b = 0;
+      CK(cudaSetDevice(c->device));
+      CK(cudaMemGetInfo(&free_b, &total_b));
+      budget = free_b > ((size_t)4 << 30) ? free_b - ((size_t)4 << 30) : free_b / 2;
+    }
+    c->server.reset(new flock::Server(c->device, budget, slots));
+    return FLOCK_OK;
+  });
+}
+
+int flock_submit(flock_ctx* c, const flock_job* job, uint64_t* ticket) {
+  if (!c || !job || !ticket || (!job->domain && job->dlen)) return FLOCK_ERR_ARG;
+  if (job->log2_n < 8 || job->log2_n > 20) {
+    c->err = "unsupported job size (log2 in 8..=20)";
+    return FLOCK_ERR_ARG;
+  }
+  if (!c->server) {
+    int rc = flock_serve_start(c, 4);
+    if (rc && !c->server) return rc;
+  }
+  return guard(c, [&] {
+    std::string d((const char*)job->domain, job->dlen);
+    *ticket = c->server->submit(job->log2_n, job->seed, job->blocks, d);
+    return FLOCK_OK;
+  });
+}
+
+int flock_poll(flock_ctx* c, uint64_t ticket, flock_result* res, int timeout_ms) {
+  if (!c || !res) return FLOCK_ERR_ARG;
+  if (!c->server) {
+    c->err = "serving not started";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(c, [&] {
+    const size_t len = c->server->peek_len(ticket);
+    if (len && (len > res->cap || !res->out)) {  // keep the result: the caller retries with room
+      res->out_len = len;
+      c->err = "output buffer too small";
+      return FLOCK_ERR_CAPACITY;
+    }
+    flock::JobResult r;
+    if (!c->server->wait(ticket, timeout_ms, &r)) return FLOCK_ERR_TIMEOUT;
+    res->status = r.status;
+    res->queue_ms = r.queue_ms;
+    res->run_ms = r.run_ms;
+    res->latency_ms = r.latency_ms;
+    res->out_len = r.bytes.size();
+    if (r.status != FLOCK_OK) {
+      c->err = r.error;
+      return FLOCK_OK;
+    }
+    if (r.bytes.size() > res->cap || !res->out) {
+      c->err = "output buffer too small (the proof was dropped)";
+      return FLOCK_ERR_CAPACITY;
+    }
+    memcpy(res->out, r.bytes.data(), r.bytes.size());
+    return FLOCK_OK;
   });
 }
 

@@ -1,6 +1,7 @@
 // Launch wrappers of the prover's device kernels (K0..K9).
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -13,8 +14,8 @@ constexpr int kK_ = 16384;  // bits per compression block (2^14)
 
 // Number of this library's kernel launches issued by this process (reported
 // by the benchmark; every launch wrapper adds its launches here).
-uint64_t& kernel_launch_counter();
-inline void count_launch(uint64_t n = 1) { kernel_launch_counter() += n; }
+std::atomic<uint64_t>& kernel_launch_counter();
+inline void count_launch(uint64_t n = 1) { kernel_launch_counter().fetch_add(n, std::memory_order_relaxed); }
 
 struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& s) : std::runtime_error(s) {}

@@ -18,10 +18,12 @@
 namespace flock {
 
 namespace {
+thread_local size_t t_alloc_bytes = 0;  // device bytes allocated by this thread's setups
 template <class T>
 T* dalloc(size_t n) {
   T* p = nullptr;
   CK(cudaMalloc(&p, n * sizeof(T) + 256));
+  t_alloc_bytes += n * sizeof(T) + 256;
   return p;
 }
 
@@ -46,8 +48,17 @@ size_t ceil_log2(size_t n) {
 }  // namespace
 
 // ---------------------------------------------------------------- setup --
+size_t Setup::estimate_bytes(uint32_t log2) {
+  const size_t n_words = (size_t)1 << (kKLog + std::max<int>(3, (int)log2) - 7);
+  // z, a, b, 4 fold buffers, eq scratch, the rate-1/2 codeword (2x), its tree
+  // (1/16 of a word per word), the Ligero levels and query basis (< 1/8),
+  // blocks staging (25 u32 per compression), statement and small tables
+  return n_words * 16 * 10 + n_words * 2 + n_words * 2 + (n_words / 128) * 100 + ((size_t)96 << 20);
+}
+
 Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
   CK(cudaSetDevice(device));
+  const size_t bytes0 = t_alloc_bytes;
   n_log = std::max<int>(3, (int)log2);
   m = kKLog + n_log;
   lad = ladder_for(m);
@@ -107,6 +118,7 @@ Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
   CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
   sms = dev_sms;
   for (int i = 0; i < kPhases + 1; i++) CK(cudaEventCreate(&ev[i]));
+  device_bytes = t_alloc_bytes - bytes0;
 }
 
 Setup::~Setup() {

@@ -32,6 +32,10 @@ class Setup {
   std::vector<uint8_t> prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
                              const std::string& domain);
   void phase_times(double* ms) const;
+  // device bytes a setup for 2^log2 compressions holds (an upper estimate,
+  // used for admission before allocating)
+  static size_t estimate_bytes(uint32_t log2);
+  size_t device_bytes = 0;  // allocated by the constructor
 
   uint32_t log2 = 0;
   int n_log = 0, m = 0, sms = 0;

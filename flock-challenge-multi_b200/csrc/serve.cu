@@ -1,0 +1,177 @@
+// Serving scheduler (see serve.hpp).  Host code only: every proof runs through
+// Setup::prove on the setup's own stream.
+#include "serve.hpp"
+#include "../../include/flock_gpu.h"
+
+namespace flock {
+
+Server::Server(int device, uint64_t budget, int slots) : device_(device), budget_(budget) {
+  if (slots < 1 || slots > 64) throw std::runtime_error("serving slots must be in 1..64");
+  for (int i = 0; i < slots; i++) workers_.emplace_back([this] { worker(); });
+}
+
+Server::~Server() {
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    stop_ = true;
+  }
+  cv_jobs_.notify_all();
+  cv_mem_.notify_all();
+  for (auto& t : workers_) t.join();
+  idle_.clear();  // frees the cached setups
+}
+
+uint64_t Server::submit(uint32_t log2, uint64_t seed, const uint32_t* blocks, const std::string& domain) {
+  Job j;
+  j.log2 = log2;
+  j.seed = seed;
+  j.domain = domain;
+  if (blocks) {
+    j.has_blocks = true;
+    j.blocks.assign(blocks, blocks + ((size_t)25 << log2));
+  }
+  j.submitted = Clock::now();
+  uint64_t t;
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (stop_) throw std::runtime_error("server stopped");
+    t = j.ticket = next_ticket_++;
+    queue_.push_back(std::move(j));
+  }
+  cv_jobs_.notify_one();
+  return t;
+}
+
+bool Server::wait(uint64_t ticket, int timeout_ms, JobResult* out) {
+  std::unique_lock<std::mutex> lk(mu_);
+  auto ready = [&] { return done_.count(ticket) > 0; };
+  if (timeout_ms < 0) cv_done_.wait(lk, ready);
+  else if (!cv_done_.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return false;
+  *out = std::move(done_[ticket]);
+  done_.erase(ticket);
+  return true;
+}
+
+size_t Server::peek_len(uint64_t ticket) {
+  std::lock_guard<std::mutex> lk(mu_);
+  auto it = done_.find(ticket);
+  return it == done_.end() ? 0 : it->second.bytes.size();
+}
+
+uint64_t Server::cached_bytes() {
+  std::lock_guard<std::mutex> lk(mu_);
+  return bytes_;
+}
+
+// Called with the lock held; may drop it while constructing a setup.
+std::unique_ptr<Setup> Server::acquire(uint32_t log2, std::unique_lock<std::mutex>& lk) {
+  for (;;) {
+    if (stop_) return nullptr;
+    auto it = idle_.find(log2);
+    if (it != idle_.end() && !it->second.empty()) {
+      std::unique_ptr<Setup> s = std::move(it->second.back().setup);
+      it->second.pop_back();
+      busy_++;
+      return s;
+    }
+    const uint64_t need = Setup::estimate_bytes(log2);
+    // evict idle setups of other sizes, least recently used first, until it fits
+    while (bytes_ + need > budget_) {
+      uint32_t victim = 0;
+      size_t vi = 0;
+      uint64_t oldest = UINT64_MAX;
+      for (auto& kv : idle_)
+        for (size_t i = 0; i < kv.second.size(); i++)
+          if (kv.second[i].last_use < oldest) {
+            oldest = kv.second[i].last_use;
+            victim = kv.first;
+            vi = i;
+          }
+      if (oldest == UINT64_MAX) break;  // nothing idle to evict
+      auto& vec = idle_[victim];
+      bytes_ -= vec[vi].setup->device_bytes;
+      vec.erase(vec.begin() + (long)vi);  // frees the device buffers
+    }
+    if (bytes_ + need <= budget_) {
+      bytes_ += need;  // reserved while constructing, corrected afterwards
+      lk.unlock();
+      std::unique_ptr<Setup> s;
+      std::string err;
+      try {
+        s.reset(new Setup(device_, log2));
+      } catch (const std::exception& e) {
+        err = e.what();
+      }
+      lk.lock();
+      bytes_ -= need;
+      if (!s) throw std::runtime_error("setup for 2^" + std::to_string(log2) + " failed: " + err);
+      bytes_ += s->device_bytes;
+      busy_++;
+      return s;
+    }
+    if (busy_ == 0)  // nothing in flight will ever free memory for this job
+      throw std::runtime_error("a 2^" + std::to_string(log2) + " proof does not fit the HBM budget");
+    // every byte is held by proofs in flight: wait for one to finish
+    cv_mem_.wait(lk);
+  }
+}
+
+void Server::release(std::unique_ptr<Setup> s) {
+  const uint32_t log2 = s->log2;
+  busy_--;
+  idle_[log2].push_back(Cached{std::move(s), ++use_clock_});
+  cv_mem_.notify_all();
+}
+
+void Server::worker() {
+  cudaSetDevice(device_);
+  std::unique_lock<std::mutex> lk(mu_);
+  for (;;) {
+    cv_jobs_.wait(lk, [&] { return stop_ || !queue_.empty(); });
+    if (stop_) return;
+    Job job = std::move(queue_.front());
+    queue_.pop_front();
+    JobResult r;
+    std::unique_ptr<Setup> s;
+    try {
+      s = acquire(job.log2, lk);
+    } catch (const std::exception& e) {
+      r.status = FLOCK_ERR_CAPACITY;
+      r.error = e.what();
+    }
+    if (stop_ && !s) return;
+    const auto t_run = Clock::now();
+    if (s) {
+      lk.unlock();
+      try {
+        if (job.has_blocks) {
+          const size_t n = (size_t)1 << job.log2;
+          if (!s->blocks_buf) CK(cudaMalloc(&s->blocks_buf, n * 25 * sizeof(uint32_t)));
+          CK(cudaMemcpyAsync(s->blocks_buf, job.blocks.data(), n * 25 * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             s->st));
+          r.bytes = s->prove(nullptr, s->blocks_buf, n, job.domain);
+        } else {
+          r.bytes = s->prove(&job.seed, nullptr, 0, job.domain);
+        }
+        r.status = FLOCK_OK;
+      } catch (const CudaError& e) {
+        r.status = FLOCK_ERR_CUDA;
+        r.error = e.what();
+      } catch (const std::exception& e) {
+        r.status = FLOCK_ERR_INTERNAL;
+        r.error = e.what();
+      }
+      lk.lock();
+      release(std::move(s));
+    }
+    const auto t_end = Clock::now();
+    auto ms = [](Clock::duration d) { return std::chrono::duration<double, std::milli>(d).count(); };
+    r.queue_ms = ms(t_run - job.submitted);
+    r.run_ms = ms(t_end - t_run);
+    r.latency_ms = ms(t_end - job.submitted);
+    done_[job.ticket] = std::move(r);
+    cv_done_.notify_all();
+  }
+}
+
+}  // namespace flock

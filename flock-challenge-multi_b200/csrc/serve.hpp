@@ -1,0 +1,87 @@
+// Serving scheduler: continuous batching of proof jobs of different sizes on
+// one GPU.  Jobs are admitted in arrival order as proof slots and device
+// memory free up: each slot is a host thread that drives one proof at a time
+// on its own CUDA stream, so the kernels of up to `slots` proofs overlap on
+// the device and fill each other's host round-trip gaps (the Fiat-Shamir
+// transcript stays on the host).  Setups (device buffers + tables for one
+// size) are cached per size and reused; admission keeps the bytes of all
+// cached setups within the HBM budget, evicting idle setups of other sizes
+// (least recently used first) when a new size needs room.
+#pragma once
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <list>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+#include "prover.hpp"
+
+namespace flock {
+
+struct JobResult {
+  int status = 0;  // FLOCK_* status of the proof
+  std::string error;
+  std::vector<uint8_t> bytes;
+  double queue_ms = 0, run_ms = 0, latency_ms = 0;
+};
+
+class Server {
+ public:
+  // budget: device bytes all cached setups may hold; slots: proofs in flight
+  Server(int device, uint64_t budget, int slots);
+  ~Server();
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
+
+  // blocks == nullptr: inputs generated on the device from `seed`; otherwise
+  // 2^log2 x 25 u32, copied here (the caller may free them on return)
+  uint64_t submit(uint32_t log2, uint64_t seed, const uint32_t* blocks, const std::string& domain);
+  // true once the job finished (its result is moved out and forgotten)
+  bool wait(uint64_t ticket, int timeout_ms, JobResult* out);
+  // the job's proof length if finished, else 0 (leaves the result in place)
+  size_t peek_len(uint64_t ticket);
+
+  int slots() const { return (int)workers_.size(); }
+  uint64_t budget() const { return budget_; }
+  uint64_t cached_bytes();
+
+ private:
+  using Clock = std::chrono::steady_clock;
+  struct Job {
+    uint64_t ticket = 0;
+    uint32_t log2 = 0;
+    uint64_t seed = 0;
+    bool has_blocks = false;
+    std::vector<uint32_t> blocks;
+    std::string domain;
+    Clock::time_point submitted;
+  };
+  struct Cached {
+    std::unique_ptr<Setup> setup;
+    uint64_t last_use = 0;
+  };
+
+  void worker();
+  std::unique_ptr<Setup> acquire(uint32_t log2, std::unique_lock<std::mutex>& lk);
+  void release(std::unique_ptr<Setup> s);
+
+  int device_;
+  uint64_t budget_;
+  std::mutex mu_;
+  std::condition_variable cv_jobs_, cv_done_, cv_mem_;
+  std::deque<Job> queue_;
+  std::map<uint64_t, JobResult> done_;
+  std::map<uint32_t, std::vector<Cached>> idle_;  // cached setups not in use, by size
+  uint64_t bytes_ = 0;                            // device bytes of all setups (idle + busy)
+  int busy_ = 0;                                  // setups held by proofs in flight
+  uint64_t next_ticket_ = 1, use_clock_ = 0;
+  bool stop_ = false;
+  std::vector<std::thread> workers_;
+};
+
+}  // namespace flock

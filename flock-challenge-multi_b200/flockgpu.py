@@ -26,7 +26,21 @@ EXPORTS = (
     "flock_witness", "flock_ntt_rs_encode", "flock_merkle_tree", "flock_sumcheck_round",
     "flock_pow", "flock_f128_mul", "flock_statement_digest", "flock_bench_ntt",
     "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove", "flock_merkle_root_noalloc",
+    "flock_serve_start", "flock_submit", "flock_poll",
 )
+FLOCK_ERR_CAPACITY = 3
+FLOCK_ERR_TIMEOUT = 5
+
+
+class FlockJob(ctypes.Structure):
+    _fields_ = [("log2_n", ctypes.c_uint32), ("seed", ctypes.c_uint64), ("blocks", ctypes.c_void_p),
+                ("domain", ctypes.c_char_p), ("dlen", ctypes.c_size_t)]
+
+
+class FlockResult(ctypes.Structure):
+    _fields_ = [("out", ctypes.c_void_p), ("cap", ctypes.c_size_t), ("out_len", ctypes.c_size_t),
+                ("status", ctypes.c_int), ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double)]
 PHASES = ("witness", "rs_encode", "merkle_commit", "zerocheck_round1", "zerocheck_rounds", "lincheck",
           "ring_switch_combine", "ligerito_l0_folds", "ligerito_levels")
 
@@ -66,12 +80,31 @@ def load() -> ctypes.CDLL:
         lib.flock_bench_prove.argtypes = [vp, u64, i32, ctypes.POINTER(ctypes.c_double), vp,
                                           ctypes.POINTER(u64)]
         lib.flock_merkle_root_noalloc.argtypes = [vp, sz, sz, vp, vp]
+        lib.flock_serve_start.argtypes = [vp, i32]
+        lib.flock_submit.argtypes = [vp, ctypes.POINTER(FlockJob), ctypes.POINTER(u64)]
+        lib.flock_poll.argtypes = [vp, u64, ctypes.POINTER(FlockResult), i32]
         _lib = lib
     return _lib
 
 
 def _ptr(a: np.ndarray) -> ctypes.c_void_p:
     return ctypes.c_void_p(a.ctypes.data)
+
+
+def generate_compressions(log2: int, seed: int) -> np.ndarray:
+    """The benchmark inputs on the host, (2^log2, 25) u32: cv[8], m[16],
+    counter (benchmark-tools/common/src/lib.rs:25-37 generate_compressions).
+    SplitMix64 with state init = seed ^ rotl(log2, 29); draw j of compression
+    i uses state init + (25 i + j + 1) * gamma (seed_pipe.rs:114-146)."""
+    g = np.uint64(0x9E3779B97F4A7C15)
+    init = np.uint64((seed ^ (((log2 << 29) | (log2 >> 35)) & (2**64 - 1))) & (2**64 - 1))
+    idx = np.arange(25 << log2, dtype=np.uint64) + np.uint64(1)
+    with np.errstate(over="ignore"):
+        z = init + idx * g
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z.astype(np.uint32).reshape(-1, 25)
 
 
 def statement_digest(m: int) -> bytes:
@@ -106,6 +139,35 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    # ---- serving (continuous batching of proof jobs) ----
+    def serve_start(self, slots: int = 4) -> None:
+        self._check(self.lib.flock_serve_start(self.h, slots), "serve_start")
+
+    def submit(self, log2: int, seed: int = 0, blocks=None, domain: bytes = None) -> int:
+        """Queue one proof; returns its ticket.  blocks: (2^log2, 25) u32 or None."""
+        domain = DOMAIN if domain is None else domain
+        job = FlockJob(log2, seed, None, domain, len(domain))
+        if blocks is not None:
+            blocks = np.ascontiguousarray(blocks, np.uint32).reshape(-1, 25)
+            job.blocks = blocks.ctypes.data  # copied by the library before submit returns
+        t = ctypes.c_uint64()
+        self._check(self.lib.flock_submit(self.h, ctypes.byref(job), ctypes.byref(t)), "submit")
+        return t.value
+
+    def poll(self, ticket: int, timeout_ms: int = -1):
+        """None while the job runs (after timeout_ms), else a dict with the proof
+        bytes, its status and the queue / run / end-to-end latencies in ms."""
+        buf = np.zeros(MAX_PROOF_BYTES * 2, np.uint8)
+        res = FlockResult(buf.ctypes.data, buf.size, 0, 0, 0.0, 0.0, 0.0)
+        rc = self.lib.flock_poll(self.h, ticket, ctypes.byref(res), timeout_ms)
+        if rc == FLOCK_ERR_TIMEOUT:
+            return None
+        self._check(rc, "poll")
+        if res.status:
+            raise FlockError(f"job {ticket} failed ({res.status}): {self.lib.flock_last_error(self.h).decode()}")
+        return {"bytes": buf[: res.out_len].tobytes(), "queue_ms": res.queue_ms, "run_ms": res.run_ms,
+                "latency_ms": res.latency_ms}
 
     # ---- kernel-level entry points (host arrays in, host arrays out) ----
     def witness(self, log2: int, seed: int):

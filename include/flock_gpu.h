@@ -43,7 +43,14 @@ extern "C" {
 typedef struct flock_ctx flock_ctx;
 typedef struct flock_setup flock_setup;
 
-enum { FLOCK_OK = 0, FLOCK_ERR_ARG = 1, FLOCK_ERR_CUDA = 2, FLOCK_ERR_CAPACITY = 3, FLOCK_ERR_INTERNAL = 4 };
+enum {
+  FLOCK_OK = 0,
+  FLOCK_ERR_ARG = 1,
+  FLOCK_ERR_CUDA = 2,
+  FLOCK_ERR_CAPACITY = 3,
+  FLOCK_ERR_INTERNAL = 4,
+  FLOCK_ERR_TIMEOUT = 5
+};
 enum { FLOCK_HASH_BLAKE3 = 1 };
 enum { FLOCK_PROFILE_FAST = 0 };
 
@@ -91,6 +98,42 @@ int flock_bench_sumcheck(flock_ctx* ctx, size_t n, int iters, double* ms);
  * number of this library's kernel launches inside the timed region. */
 int flock_bench_prove(flock_setup* s, uint64_t seed0, int steps, double* total_ms, double* phase_ms,
                       uint64_t* launches);
+
+/* Serving: continuous batching of proof jobs of different sizes on the
+ * context's device.  Jobs run in arrival order as proof slots and device
+ * memory free up; the kernels of up to `slots` proofs overlap on the GPU.
+ * Per-size setups are cached and reused within the HBM budget given to
+ * flock_ctx_create (0: the free device memory less 4 GiB), evicting idle
+ * setups of other sizes when a new size needs room.  The result of a job is
+ * byte-identical to flock_prove_seed / flock_prove_blocks of the same inputs.
+ * No counterpart in the reference, which proves one request at a time
+ * (benchmark-tools/worker/src/main.rs); this is the served form of the same
+ * prove entry point. */
+typedef struct flock_job {
+  uint32_t log2_n;         /* 8..20 */
+  uint64_t seed;           /* inputs from the benchmark generator when blocks == NULL */
+  const uint32_t* blocks;  /* or 2^log2_n x 25 u32 compressions (copied at submit) */
+  const uint8_t* domain;
+  size_t dlen;
+} flock_job;
+typedef struct flock_result {
+  uint8_t* out;       /* caller buffer for the proof bytes */
+  size_t cap;
+  size_t out_len;     /* proof length (also set when the buffer is too small) */
+  int status;         /* status of the proof itself */
+  double queue_ms;    /* submit -> start */
+  double run_ms;      /* start -> proof bytes ready */
+  double latency_ms;  /* submit -> proof bytes ready */
+} flock_result;
+/* Start serving with `slots` proofs in flight (optional: the first submit
+ * starts it with 4). */
+int flock_serve_start(flock_ctx* ctx, int slots);
+int flock_submit(flock_ctx* ctx, const flock_job* job, uint64_t* ticket);
+/* FLOCK_OK once the job finished (then res->status is the proof's status),
+ * FLOCK_ERR_TIMEOUT if it did not finish within timeout_ms (< 0: wait), or
+ * FLOCK_ERR_CAPACITY with res->out_len set when res->cap is too small (the
+ * result is kept for a retry). */
+int flock_poll(flock_ctx* ctx, uint64_t ticket, flock_result* res, int timeout_ms);
 
 /* Merkle root of leaves already in device memory, for callers that may not
  * allocate device memory when they need the root (inside a stream capture,
