@@ -14,8 +14,10 @@
 // tile = 2^R positions (one per combination of the pass's pair bits, the
 // other position bits fixed) x LG consecutive lanes, staged in shared
 // memory (LG lanes of one position are contiguous: 16*LG-byte coalesced
-// rows).  The tile's 2^R - 1 twiddles are derived once into shared memory
-// from the per-layer basis values (XOR of at most d values each).
+// rows); LG is chosen so that two CTAs fit an SM.  The tile's 2^R - 1
+// twiddles are derived once into shared memory from the per-layer basis
+// values (XOR of at most d values each); block 0 of every layer has the zero
+// twiddle and needs no product.
 #include "kernels.cuh"
 #include <algorithm>
 #include <map>
@@ -40,7 +42,7 @@ __device__ __forceinline__ f128 twiddle(const f128* ev, int l, uint64_t b) {
 }
 
 template <bool TRANSPOSE>
-__global__ void __launch_bounds__(512) k_ntt_pass(PassArgs p) {
+__global__ void __launch_bounds__(256, 2) k_ntt_pass(PassArgs p) {
   extern __shared__ f128 smem[];
   const int R = p.R, LG = 1 << p.lg_shift;
   f128* tile = smem;                       // [2^R][LG]
@@ -74,6 +76,7 @@ __global__ void __launch_bounds__(512) k_ntt_pass(PassArgs p) {
   const int n_pp = 1 << (R - 1);
   const int per = min(LG, max(1, (n_pp * LG) / (int)blockDim.x));
   const int tpp = LG / per;  // threads per position pair
+  const int rs = 3 - p.lg_shift;  // rotate by pq >> rs: distinct bank groups per quarter warp
   for (int stg = 0; stg < R; stg++) {
     const int s = TRANSPOSE ? R - 1 - stg : stg;
     const int hb = R - 1 - s;                // local pair bit
@@ -81,7 +84,17 @@ __global__ void __launch_bounds__(512) k_ntt_pass(PassArgs p) {
       const int pq = w / tpp, lane0 = (w % tpp) * per;
       const int top = ((pq >> hb) << (hb + 1)) | (pq & ((1 << hb) - 1));
       const int bot = top | (1 << hb);
-      const MulConst M = mulconst(tw[(1 << s) - 1 + (top >> (hb + 1))]);
+      const f128 tv = tw[(1 << s) - 1 + (top >> (hb + 1))];
+      if (fz(tv)) {  // block 0 of every layer: the twiddle is the empty sum
+        for (int k = 0; k < per; k++) {
+          const int lane = lane0 + ((k + (pq >> rs)) & (per - 1));
+          const int it = (top << p.lg_shift) | lane, ib = (bot << p.lg_shift) | lane;
+          if (!TRANSPOSE) tile[ib] = fx(tile[ib], tile[it]);
+          else tile[it] = fx(tile[it], tile[ib]);
+        }
+        continue;
+      }
+      const MulConst M = mulconst(tv);
       // lane order rotated by the position pair: lane0 + rot covers all 8
       // bank groups over 8 consecutive threads for every `per`
       auto bfly = [&](int lane) {
@@ -100,7 +113,7 @@ __global__ void __launch_bounds__(512) k_ntt_pass(PassArgs p) {
         bfly(lane0);
       } else {
         for (int k = 0; k < per; k += 2) {  // two independent butterflies per step
-          const int l0 = lane0 + ((k + pq) & (per - 1)), l1 = lane0 + ((k + 1 + pq) & (per - 1));
+          const int l0 = lane0 + ((k + (pq >> rs)) & (per - 1)), l1 = lane0 + ((k + 1 + (pq >> rs)) & (per - 1));
           f128 u0 = tile[(top << p.lg_shift) | l0], v0 = tile[(bot << p.lg_shift) | l0];
           f128 u1 = tile[(top << p.lg_shift) | l1], v1 = tile[(bot << p.lg_shift) | l1];
           if (!TRANSPOSE) {
@@ -192,11 +205,18 @@ void run_passes(f128* data, int log_d, int lanes, int layer_begin, bool transpos
   }
   if (transpose) std::reverse(passes.begin(), passes.end());
   for (auto& pr : passes) {
-    PassArgs a{data, ev, log_d, lanes, lg_shift, pr.first, pr.second};
-    int LG = 1 << lg_shift;
-    size_t smem = ((size_t)LG << pr.second) * sizeof(f128) + ((1 << pr.second) - 1) * sizeof(f128);
-    uint64_t tiles = ((uint64_t)1 << (log_d - pr.second)) * (uint64_t)(lanes >> lg_shift);
-    int threads = std::min(512, std::max(32, (LG << pr.second) / 2));
+    // lanes per tile: as many as fit two CTAs per SM (<= 112 KiB of tile +
+    // twiddles each), so one CTA's stage barriers overlap the other's work
+    int lgs = lg_shift;
+    auto tile_bytes = [&](int sh) {
+      return ((size_t)(1 << sh) << pr.second) * sizeof(f128) + ((1 << pr.second) - 1) * sizeof(f128);
+    };
+    while (lgs > 0 && tile_bytes(lgs) > ((size_t)112 << 10)) lgs--;
+    PassArgs a{data, ev, log_d, lanes, lgs, pr.first, pr.second};
+    int LG = 1 << lgs;
+    size_t smem = tile_bytes(lgs);
+    uint64_t tiles = ((uint64_t)1 << (log_d - pr.second)) * (uint64_t)(lanes >> lgs);
+    int threads = std::min(256, std::max(32, (LG << pr.second) / 2));
     if (transpose) {
       CK(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       count_launch(); k_ntt_pass<true><<<(unsigned)tiles, threads, smem, s>>>(a);
