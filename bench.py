@@ -102,6 +102,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def dist_backend() -> str:
+    """nccl between GPU ranks; FLOCK_DIST_BACKEND=gloo runs the same plumbing on CPU."""
+    return os.environ.get("FLOCK_DIST_BACKEND", "nccl")
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -110,8 +115,9 @@ def dist_setup():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if dist_backend() == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(dist_backend(), timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
@@ -120,7 +126,7 @@ def allreduce_max(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -129,6 +135,18 @@ def barrier(world: int) -> None:
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def rank_seed_base(rank: int) -> int:
+    """Every replica proves its own inputs (distinct seeds per rank)."""
+    return 0x5EED0000 + 1_000_003 * rank
+
+
+def aggregate(local_ms: float, world: int, log2: int, steps: int):
+    """Whole-job throughput of `world` replicas: all ranks' compressions over
+    the slowest rank's device time.  Returns (value, max_ms)."""
+    max_ms = allreduce_max(local_ms, world)
+    return (1 << log2) * steps * world / (max_ms / 1e3), max_ms
 
 
 def host_blocks(log2: int, seed: int):
@@ -297,14 +315,14 @@ def run_ours(args, world, rank, local):
     log2 = args.log2
     ctx = flockgpu.Context(local)
     prover = flockgpu.Prover(ctx, log2)
-    seed_base = 0x5EED0000 + 1_000_003 * rank
+    seed_base = rank_seed_base(rank)
     for i in range(args.warmup):
         prover.prove_seed(seed_base + 900 + i)
     barrier(world)
     sampler = ClockSampler(local)
     total_ms, phases, launches = prover.bench(seed_base, args.steps)
     clocks = sampler.stop()
-    max_ms = allreduce_max(total_ms, world)
+    value, max_ms = aggregate(total_ms, world, log2, args.steps)
     # end to end through the public API with host inputs: H2D of the
     # compressions, prove, D2H of the proof bytes (all inside the timed region)
     blocks = [host_blocks(log2, seed_base + 500 + i) for i in range(args.steps)]
@@ -316,7 +334,6 @@ def run_ours(args, world, rank, local):
         prover.close()
         return
     n = (1 << log2) * args.steps * world
-    value = n / (max_ms / 1e3)
     peak, peak_kind = peaks()
     dom = max(phases, key=phases.get)
     kname, kbytes, klaunches, kdesc = PHASE_KERNEL[dom]
