@@ -310,6 +310,74 @@ def serving_report(device: int, full: bool):
     return out
 
 
+# Integer-pipe ceiling of the GF(2^128) product as built here: 144 IMAD.WIDE
+# (9 Karatsuba 32x32 carry-less products of 16 each) at 32 per SM per clock,
+# the FMA pipe's rate; the ~300 ALU operations at 64 per SM per clock bind at
+# the same rate.  148 SMs at the measured maximum SM clock.
+def int_product_peak() -> float:
+    mhz = 1965.0
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        mhz = float(json.loads(p.read_text()).get("sm_max_mhz", mhz))
+    return 148 * mhz * 1e6 * 32 / 144
+
+
+def kernel_report(device: int) -> list:
+    """Kernel microbenchmarks (additive NTT / RS encode, Merkle trees, degree-2
+    and degree-3 sumcheck rounds) on device-resident seeded inputs, CUDA-event
+    timed on the launching stream; each size is above the 126 MB L2 or is
+    reported as L2-resident."""
+    import flockgpu
+    ctx = flockgpu.Context(device)
+    hbm, kind = peaks()
+    ipk = int_product_peak()
+    rows = []
+    try:
+        for log_msg, cols in [(16, 1), (16, 64), (16, 256), (20, 1), (20, 16), (20, 64), (24, 1), (24, 4)]:
+            for rate in (1, 2):
+                if log_msg + cols.bit_length() - 1 + rate > 27:
+                    continue
+                ms = ctx.bench_ntt(log_msg, cols, rate, iters=5)
+                n_cw = (1 << (log_msg + rate)) * cols
+                prods = cols * (n_cw // cols // 2) * log_msg  # layers rate..log_d-1, one product per pair
+                byts = 16 * cols * (1 << log_msg) + 16 * n_cw  # algorithmic: read the message, write the codeword
+                rows.append({"kernel": "ntt_rs_encode", "log_msg": log_msg, "columns": cols, "rate": f"1/{1 << rate}",
+                             "ms": ms, "gf_products_per_s": prods / (ms / 1e3),
+                             "int_frac": prods / (ms / 1e3) / ipk, "gbs": byts / (ms / 1e3) / 1e9,
+                             "hbm_frac": byts / (ms / 1e3) / 1e9 / hbm, "l2_resident": 16 * n_cw < (126 << 20)})
+        for log_l in (16, 19, 22):
+            for size in (32, 64, 128, 256, 512, 1024):
+                if (size << log_l) > (4 << 30):
+                    continue
+                ms = ctx.bench_merkle(1 << log_l, size, iters=5)
+                comps = (1 << log_l) * ((size + 63) // 64) + (1 << log_l) - 1
+                byts = (size << log_l) + 32 * ((2 << log_l) - 1)
+                rows.append({"kernel": "merkle_tree", "leaves": 1 << log_l, "leaf_bytes": size, "ms": ms,
+                             "blake3_compressions_per_s": comps / (ms / 1e3), "gbs": byts / (ms / 1e3) / 1e9,
+                             "hbm_frac": byts / (ms / 1e3) / 1e9 / hbm, "l2_resident": byts < (126 << 20)})
+        for log_n in (16, 20, 24):
+            n = 1 << log_n
+            ms = ctx.bench_sumcheck(n, iters=5)
+            byts = 16 * (2 * n + n)  # read f, b; write the folded halves
+            prods = 3 * (n // 2)      # fold: 1 per output value (n / 2); message: 2 per output pair
+            rows.append({"kernel": "sumcheck_deg2_fold_round", "n": n, "ms": ms, "gbs": byts / (ms / 1e3) / 1e9,
+                         "hbm_frac": byts / (ms / 1e3) / 1e9 / hbm, "gf_products_per_s": prods / (ms / 1e3),
+                         "int_frac": prods / (ms / 1e3) / ipk, "l2_resident": 16 * 2 * n < (126 << 20)})
+            ms = ctx.bench_sumcheck3(n, iters=5)
+            byts = 16 * (2 * n + n + n // 4)  # read a, b, e; write the folded halves
+            prods = 2 * n                     # fold: 1 per output value (n / 2); message: 4 per output pair
+            rows.append({"kernel": "sumcheck_deg3_fold_round", "n": n, "ms": ms, "gbs": byts / (ms / 1e3) / 1e9,
+                         "hbm_frac": byts / (ms / 1e3) / 1e9 / hbm, "gf_products_per_s": prods / (ms / 1e3),
+                         "int_frac": prods / (ms / 1e3) / ipk, "l2_resident": 16 * 2 * n < (126 << 20)})
+    finally:
+        ctx.close()
+    for r in rows:
+        r["hbm_peak_gbs"] = hbm
+        r["peak_kind"] = kind
+        r["int_product_peak_per_s"] = ipk
+    return rows
+
+
 def run_ours(args, world, rank, local):
     import flockgpu
     log2 = args.log2
@@ -383,11 +451,18 @@ def main():
     ap.add_argument("--log2", type=int, default=LOG2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the batched / served measurements")
+    ap.add_argument("--kernels", action="store_true",
+                    help="only the kernel microbenchmarks (NTT / Merkle / sumcheck sweeps), one JSON line each")
     ap.add_argument("--serve", action="store_true",
                     help="only the batched + served report: 64 uneven jobs, then Poisson arrivals at 4 rates")
     args = ap.parse_args()
     world, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                     int(os.environ.get("RANK", "0")), 0)
+    if args.kernels:
+        if rank == 0:
+            for row in kernel_report(0):
+                print(json.dumps(row), flush=True)
+        return
     if args.serve:
         if rank == 0:
             print(json.dumps({"metric": "served/batched proof throughput and latency", **serving_report(0, True)}),

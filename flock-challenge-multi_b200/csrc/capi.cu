@@ -262,6 +262,42 @@ int flock_ntt_rs_encode(flock_ctx* c, const uint64_t* msg, uint32_t log_msg_pos,
   });
 }
 
+int flock_ntt_rs_encode_plan(flock_ctx* c, const uint64_t* msg, uint32_t log_msg_pos, uint32_t lanes,
+                             uint32_t rate, uint32_t plan_index, uint64_t* out) {
+  if (!c || !msg || !out || lanes == 0 || (lanes & (lanes - 1)) || log_msg_pos + rate > 30 || rate < 1)
+    return FLOCK_ERR_ARG;
+  if (plan_index >= ntt_plan_count((int)(log_msg_pos + rate), (int)lanes, (int)rate)) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    size_t n = ((size_t)lanes) << log_msg_pos, nc = n << rate;
+    DevBuf<f128> dm(n), dc(nc);
+    CK(cudaMemcpyAsync(dm.p, msg, n * 16, cudaMemcpyHostToDevice, c->st));
+    ntt_rs_encode_plan(dm.p, dc.p, (int)log_msg_pos, (int)lanes, (int)rate, plan_index, c->st);
+    CK(cudaMemcpyAsync(out, dc.p, nc * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+
+int flock_ntt_autotune(flock_ctx* c, uint32_t log_msg_pos, uint32_t lanes, uint32_t rate, double* best_ms,
+                       char* desc, size_t desc_cap) {
+  if (!c || lanes == 0 || (lanes & (lanes - 1)) || log_msg_pos + rate > 30 || rate < 1) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    const int log_d = (int)(log_msg_pos + rate);
+    NttPlan plan = ntt_plan(log_d, (int)lanes, (int)rate);
+    double ms = -1;
+    {
+      DevBuf<f128> dc(((size_t)lanes) << log_d);
+      plan = ntt_autotune(dc.p, log_d, (int)lanes, (int)rate, c->st, &ms);
+    }
+    if (best_ms) *best_ms = ms;
+    if (desc && desc_cap) {
+      std::string d = ntt_plan_desc(plan);
+      std::snprintf(desc, desc_cap, "%s", d.c_str());
+    }
+    return FLOCK_OK;
+  });
+}
+
 int flock_merkle_tree(flock_ctx* c, const uint8_t* data, size_t n_leaves, size_t leaf_size, uint8_t* tree_out) {
   if (!c || !data || !tree_out || n_leaves == 0 || (n_leaves & (n_leaves - 1)) || leaf_size == 0 ||
       leaf_size > 1024 || (leaf_size % 16))
@@ -286,6 +322,30 @@ int flock_sumcheck_round(flock_ctx* c, const uint64_t* f, const uint64_t* b, siz
     CK(cudaMemsetAsync(dout.p, 0, 32, c->st));
     lig_msg(df.p, db.p, n / 2, dout.p, 148 * 4, c->st);
     CK(cudaMemcpyAsync(msg_out, dout.p, 32, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+
+int flock_sumcheck_round3(flock_ctx* c, const uint64_t* e, const uint64_t* a, const uint64_t* b, size_t n,
+                          const uint64_t* rho, uint64_t* a_out, uint64_t* b_out, uint64_t* msg_out) {
+  const size_t min_n = rho ? 4 : 2;
+  if (!c || !e || !a || !b || !msg_out || n < min_n || (n & (n - 1)) || (rho && (!a_out || !b_out)))
+    return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    const size_t n_pairs = rho ? n / 4 : n / 2;
+    DevBuf<f128> da(n), db(n), de(n_pairs), dao(n / 2), dbo(n / 2), dout(2);
+    CK(cudaMemcpyAsync(da.p, a, n * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(db.p, b, n * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(de.p, e, n_pairs * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemsetAsync(dout.p, 0, 32, c->st));
+    f128 r = rho ? mk(rho[0], rho[1]) : mk(0, 0);
+    sc3_round(da.p, db.p, de.p, dao.p, dbo.p, rho ? &r : nullptr, n_pairs, dout.p, 148 * 4, c->st);
+    CK(cudaMemcpyAsync(msg_out, dout.p, 32, cudaMemcpyDeviceToHost, c->st));
+    if (rho) {
+      CK(cudaMemcpyAsync(a_out, dao.p, n / 2 * 16, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaMemcpyAsync(b_out, dbo.p, n / 2 * 16, cudaMemcpyDeviceToHost, c->st));
+    }
     CK(cudaStreamSynchronize(c->st));
     return FLOCK_OK;
   });
@@ -343,6 +403,7 @@ int flock_bench_ntt(flock_ctx* c, uint32_t log_msg_pos, uint32_t lanes, uint32_t
   return guard(c, [&] {
     size_t n = ((size_t)lanes) << log_msg_pos, nc = n << rate;
     DevBuf<f128> dm(n), dc(nc);
+    ntt_autotune(dc.p, (int)(log_msg_pos + rate), (int)lanes, (int)rate, c->st);
     k_fill<<<(unsigned)((2 * n + 255) / 256), 256, 0, c->st>>>((uint64_t*)dm.p, 2 * n, 1);
     *ms = time_launches(c->st, iters, [&] { ntt_rs_encode(dm.p, dc.p, (int)log_msg_pos, (int)lanes, (int)rate, c->st); });
     return FLOCK_OK;
@@ -404,6 +465,19 @@ int flock_bench_sumcheck(flock_ctx* c, size_t n, int iters, double* ms) {
     *ms = time_launches(c->st, iters, [&] {
       lig_fold_msg(df.p, db.p, fo.p, bo.p, r, n / 4, true, dout.p, 148 * 4, c->st);
     });
+    return FLOCK_OK;
+  });
+}
+
+int flock_bench_sumcheck3(flock_ctx* c, size_t n, int iters, double* ms) {
+  if (!c || !ms || iters < 1 || n < 4 || (n & (n - 1))) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    DevBuf<f128> da(n), db(n), de(n / 4), dao(n / 2), dbo(n / 2), dout(2);
+    k_fill<<<(unsigned)((2 * n + 255) / 256), 256, 0, c->st>>>((uint64_t*)da.p, 2 * n, 5);
+    k_fill<<<(unsigned)((2 * n + 255) / 256), 256, 0, c->st>>>((uint64_t*)db.p, 2 * n, 6);
+    k_fill<<<(unsigned)((n / 2 + 255) / 256), 256, 0, c->st>>>((uint64_t*)de.p, n / 2, 7);
+    f128 r = mk(0x1234567890abcdefull, 0x0fedcba987654321ull);
+    *ms = time_launches(c->st, iters, [&] { sc3_round(da.p, db.p, de.p, dao.p, dbo.p, &r, n / 4, dout.p, 148 * 4, c->st); });
     return FLOCK_OK;
   });
 }

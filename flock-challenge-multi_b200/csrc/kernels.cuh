@@ -7,6 +7,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <vector>
 #include "gf128.cuh"
 #include "blake3.cuh"
 
@@ -15,7 +16,16 @@ constexpr int kK_ = 16384;  // bits per compression block (2^14)
 // Number of this library's kernel launches issued by this process (reported
 // by the benchmark; every launch wrapper adds its launches here).
 std::atomic<uint64_t>& kernel_launch_counter();
-inline void count_launch(uint64_t n = 1) { kernel_launch_counter().fetch_add(n, std::memory_order_relaxed); }
+// Launches issued by the calling thread (a graph capture counts the kernel
+// nodes it records from this).
+inline uint64_t& thread_launch_counter() {
+  static thread_local uint64_t n = 0;
+  return n;
+}
+inline void count_launch(uint64_t n = 1) {
+  kernel_launch_counter().fetch_add(n, std::memory_order_relaxed);
+  thread_launch_counter() += n;
+}
 
 struct CudaError : std::runtime_error {
   explicit CudaError(const std::string& s) : std::runtime_error(s) {}
@@ -34,6 +44,22 @@ void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32
 void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a, f128* b,
                            cudaStream_t s);
 // K1
+// NTT pass plans: the passes (first layer l0, layer count R, 2^lgs lanes per
+// tile, threads per CTA) that cover layers layer_begin..log_d-1.
+struct NttPass {
+  int l0, R, lgs, threads;
+};
+using NttPlan = std::vector<NttPass>;
+// Times the candidate plans of a shape on `scratch` (lanes << log_d values,
+// overwritten), keeps the fastest for this device and returns it; later
+// encodes of the shape use it (untuned shapes use the default split).
+NttPlan ntt_autotune(f128* scratch, int log_d, int lanes, int layer_begin, cudaStream_t s, double* best_ms = nullptr);
+NttPlan ntt_plan(int log_d, int lanes, int layer_begin);
+std::string ntt_plan_desc(const NttPlan& plan);
+// every candidate plan of a shape, for parity tests of the tiling
+size_t ntt_plan_count(int log_d, int lanes, int layer_begin);
+void ntt_rs_encode_plan(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, size_t plan_idx,
+                        cudaStream_t s);
 void ntt_rs_encode(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, cudaStream_t s);
 void ntt_forward(f128* data, int log_d, int lanes, int start_layer, cudaStream_t s);
 void ntt_transposed_encode(f128* e, f128* out, int log_msg, int log_inv_rate, cudaStream_t s);
@@ -67,3 +93,5 @@ void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, con
 void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int grid, cudaStream_t s);
 void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size_t n_pairs_out, bool emit, f128* out,
                   int grid, cudaStream_t s);
+void sc3_round(const f128* a, const f128* b, const f128* e, f128* ao, f128* bo, const f128* rho, size_t n_pairs,
+               f128* out, int grid, cudaStream_t s);

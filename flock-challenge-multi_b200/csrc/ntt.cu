@@ -22,11 +22,12 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 #include "host.hpp"
 
 namespace {
-constexpr int kMaxR = 10;
+constexpr int kMaxR = 10;  // layers per pass in the default split (the tuner also tries 11)
 
 struct PassArgs {
   f128* data;
@@ -189,44 +190,259 @@ const f128* device_evals(int dim) {
   return d;
 }
 
-void run_passes(f128* data, int log_d, int lanes, int layer_begin, bool transpose, cudaStream_t s) {
-  const f128* ev = device_evals(log_d);
-  int lg_shift = 0;
-  while ((1 << (lg_shift + 1)) <= lanes && lg_shift < 3) lg_shift++;
-  int n_layers = log_d - layer_begin;
-  if (n_layers <= 0) return;
-  int n_pass = (n_layers + kMaxR - 1) / kMaxR;
-  std::vector<std::pair<int, int>> passes;  // (l0, R)
-  int l = layer_begin;
+// ---------------------------------------------------------------- plans --
+// A plan is the list of passes (first layer, layer count R, lanes per tile
+// 2^lgs, threads per CTA) that covers layers layer_begin..log_d-1.  The
+// autotuner times candidate splits of the layers and, for each pass, the
+// tile widths and CTA sizes that fit one or two CTAs per SM, and keeps the
+// fastest combination per (device, log_d, lanes, layer_begin).
+
+size_t pass_smem(int lgs, int R) { return ((size_t)(1 << lgs) << R) * sizeof(f128) + ((1 << R) - 1) * sizeof(f128); }
+constexpr size_t kSmem2 = (size_t)112 << 10;  // two CTAs per SM
+constexpr size_t kSmem1 = (size_t)200 << 10;  // one CTA per SM
+
+int max_lgs(int lanes) {
+  int g = 0;
+  while ((1 << (g + 1)) <= lanes && g < 3) g++;
+  return g;
+}
+
+std::vector<std::pair<int, int>> balanced_split(int begin, int n_layers, int n_pass) {
+  std::vector<std::pair<int, int>> v;
+  int l = begin;
   for (int i = 0; i < n_pass; i++) {
-    int R = (n_layers - (l - layer_begin) + (n_pass - i) - 1) / (n_pass - i);
-    passes.push_back({l, R});
+    int R = (n_layers - (l - begin) + (n_pass - i) - 1) / (n_pass - i);
+    v.push_back({l, R});
     l += R;
   }
-  if (transpose) std::reverse(passes.begin(), passes.end());
-  for (auto& pr : passes) {
-    // lanes per tile: as many as fit two CTAs per SM (<= 112 KiB of tile +
-    // twiddles each), so one CTA's stage barriers overlap the other's work
-    int lgs = lg_shift;
-    auto tile_bytes = [&](int sh) {
-      return ((size_t)(1 << sh) << pr.second) * sizeof(f128) + ((1 << pr.second) - 1) * sizeof(f128);
-    };
-    while (lgs > 0 && tile_bytes(lgs) > ((size_t)112 << 10)) lgs--;
-    PassArgs a{data, ev, log_d, lanes, lgs, pr.first, pr.second};
-    int LG = 1 << lgs;
-    size_t smem = tile_bytes(lgs);
-    uint64_t tiles = ((uint64_t)1 << (log_d - pr.second)) * (uint64_t)(lanes >> lgs);
-    int threads = std::min(256, std::max(32, (LG << pr.second) / 2));
-    if (transpose) {
-      CK(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      count_launch(); k_ntt_pass<true><<<(unsigned)tiles, threads, smem, s>>>(a);
-    } else {
-      CK(cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      count_launch(); k_ntt_pass<false><<<(unsigned)tiles, threads, smem, s>>>(a);
+  return v;
+}
+
+// layer splits to try: the balanced split into the fewest passes of <= 10
+// layers, its mirror, a split with one 11-layer pass, and one more pass
+std::vector<std::vector<std::pair<int, int>>> candidate_splits(int begin, int n_layers) {
+  std::vector<std::vector<std::pair<int, int>>> out;
+  auto add = [&](std::vector<std::pair<int, int>> v) {
+    for (auto& x : out)
+      if (x == v) return;
+    for (auto& pr : v)
+      if (pr.second < 1 || pr.second > kMaxR + 1) return;
+    out.push_back(v);
+  };
+  const int p0 = (n_layers + kMaxR - 1) / kMaxR;
+  auto bal = balanced_split(begin, n_layers, p0);
+  add(bal);
+  if (p0 >= 2) {  // mirror: the larger passes last
+    std::vector<int> Rs;
+    for (auto& pr : bal) Rs.push_back(pr.second);
+    std::reverse(Rs.begin(), Rs.end());
+    std::vector<std::pair<int, int>> v;
+    int l = begin;
+    for (int R : Rs) { v.push_back({l, R}); l += R; }
+    add(v);
+  }
+  if (n_layers == kMaxR + 1) add({{begin, n_layers}});
+  if (p0 == 2 && n_layers > 11) {
+    add({{begin, 11}, {begin + 11, n_layers - 11}});
+    add({{begin, n_layers - 11}, {begin + n_layers - 11, 11}});
+  }
+  if (n_layers >= p0 + 1) add(balanced_split(begin, n_layers, p0 + 1));
+  return out;
+}
+
+// per-pass launch shapes to try: (lgs, threads)
+std::vector<std::pair<int, int>> candidate_shapes(int lanes, int R) {
+  std::vector<std::pair<int, int>> out;
+  const int top = max_lgs(lanes);
+  int g2 = top;
+  while (g2 > 0 && pass_smem(g2, R) > kSmem2) g2--;
+  int g1 = top;
+  while (g1 > 0 && pass_smem(g1, R) > kSmem1) g1--;
+  std::vector<int> gs = {g2};
+  if (g2 > 0) gs.push_back(g2 - 1);
+  if (g1 > g2) gs.push_back(g1);
+  for (int g : gs) {
+    if (pass_smem(g, R) > kSmem1) continue;
+    const int work = ((1 << g) << R) / 2;  // butterflies per stage
+    for (int t : {128, 256}) {
+      if (t > std::max(32, work)) continue;
+      out.push_back({g, t});
     }
+    if (out.empty() || out.back().first != g) out.push_back({g, std::min(256, std::max(32, work))});
+  }
+  return out;
+}
+
+void launch_pass(const NttPass& ps, f128* data, const f128* ev, int log_d, int lanes, bool transpose,
+                 cudaStream_t s) {
+  PassArgs a{data, ev, log_d, lanes, ps.lgs, ps.l0, ps.R};
+  const size_t smem = pass_smem(ps.lgs, ps.R);
+  const uint64_t tiles = ((uint64_t)1 << (log_d - ps.R)) * (uint64_t)(lanes >> ps.lgs);
+  if (transpose) {
+    CK(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    count_launch(); k_ntt_pass<true><<<(unsigned)tiles, ps.threads, smem, s>>>(a);
+  } else {
+    CK(cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    count_launch(); k_ntt_pass<false><<<(unsigned)tiles, ps.threads, smem, s>>>(a);
   }
 }
+
+NttPlan default_plan(int log_d, int lanes, int layer_begin) {
+  NttPlan plan;
+  const int n_layers = log_d - layer_begin;
+  if (n_layers <= 0) return plan;
+  for (auto& pr : balanced_split(layer_begin, n_layers, (n_layers + kMaxR - 1) / kMaxR)) {
+    int g = max_lgs(lanes);
+    while (g > 0 && pass_smem(g, pr.second) > kSmem2) g--;
+    plan.push_back({pr.first, pr.second, g, std::min(256, std::max(32, ((1 << g) << pr.second) / 2))});
+  }
+  return plan;
+}
+
+// every plan the tuner may pick: each candidate split with each launch shape
+// applied to all of its passes (for parity tests of the tiling)
+std::vector<NttPlan> all_plans(int log_d, int lanes, int layer_begin) {
+  std::vector<NttPlan> out;
+  const int n_layers = log_d - layer_begin;
+  if (n_layers <= 0) return {NttPlan{}};
+  for (auto& split : candidate_splits(layer_begin, n_layers)) {
+    size_t n_shapes = 0;
+    for (auto& pr : split) n_shapes = std::max(n_shapes, candidate_shapes(lanes, pr.second).size());
+    for (size_t k = 0; k < n_shapes; k++) {
+      NttPlan plan;
+      for (auto& pr : split) {
+        auto sh = candidate_shapes(lanes, pr.second);
+        auto& c = sh[std::min(k, sh.size() - 1)];
+        plan.push_back({pr.first, pr.second, c.first, c.second});
+      }
+      out.push_back(plan);
+    }
+  }
+  return out;
+}
+
+struct PlanKey {
+  int device, log_d, lanes, begin;
+  bool operator<(const PlanKey& o) const {
+    return std::tie(device, log_d, lanes, begin) < std::tie(o.device, o.log_d, o.lanes, o.begin);
+  }
+};
+std::mutex g_plan_mu;
+std::map<PlanKey, NttPlan>& tuned_plans() {
+  static std::map<PlanKey, NttPlan> m;
+  return m;
+}
+
+NttPlan plan_for(int log_d, int lanes, int layer_begin) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  auto it = tuned_plans().find({dev, log_d, lanes, layer_begin});
+  return it != tuned_plans().end() ? it->second : default_plan(log_d, lanes, layer_begin);
+}
+
+void run_plan(const NttPlan& plan, f128* data, int log_d, int lanes, bool transpose, cudaStream_t s) {
+  if (plan.empty()) return;
+  const f128* ev = device_evals(log_d);
+  if (transpose)
+    for (auto it = plan.rbegin(); it != plan.rend(); ++it) launch_pass(*it, data, ev, log_d, lanes, true, s);
+  else
+    for (auto& ps : plan) launch_pass(ps, data, ev, log_d, lanes, false, s);
+}
+
+void run_passes(f128* data, int log_d, int lanes, int layer_begin, bool transpose, cudaStream_t s) {
+  run_plan(plan_for(log_d, lanes, layer_begin), data, log_d, lanes, transpose, s);
+}
 }  // namespace
+
+NttPlan ntt_autotune(f128* scratch, int log_d, int lanes, int layer_begin, cudaStream_t s, double* best_ms) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  const PlanKey key{dev, log_d, lanes, layer_begin};
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = tuned_plans().find(key);
+    if (it != tuned_plans().end()) {
+      if (best_ms) *best_ms = -1;
+      return it->second;
+    }
+  }
+  const int n_layers = log_d - layer_begin;
+  if (n_layers <= 0) return {};
+  const f128* ev = device_evals(log_d);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  // one warm launch, then the best of two timed launches (CUDA events on
+  // the launching stream); the scratch contents do not affect the timing
+  auto time_pass = [&](const NttPass& ps) {
+    launch_pass(ps, scratch, ev, log_d, lanes, false, s);
+    float best = 1e30f;
+    for (int r = 0; r < 2; r++) {
+      CK(cudaEventRecord(e0, s));
+      launch_pass(ps, scratch, ev, log_d, lanes, false, s);
+      CK(cudaEventRecord(e1, s));
+      CK(cudaEventSynchronize(e1));
+      float t = 0;
+      CK(cudaEventElapsedTime(&t, e0, e1));
+      best = std::min(best, t);
+    }
+    return (double)best;
+  };
+  std::map<std::pair<int, int>, std::pair<NttPass, double>> best_pass;  // (l0, R) -> fastest shape
+  NttPlan best_plan;
+  double best_total = 1e300;
+  for (auto& split : candidate_splits(layer_begin, n_layers)) {
+    NttPlan plan;
+    double total = 0;
+    for (auto& pr : split) {
+      auto it = best_pass.find(pr);
+      if (it == best_pass.end()) {
+        NttPass bp{};
+        double bt = 1e300;
+        for (auto& sh : candidate_shapes(lanes, pr.second)) {
+          const NttPass ps{pr.first, pr.second, sh.first, sh.second};
+          const double t = time_pass(ps);
+          if (t < bt) { bt = t; bp = ps; }
+        }
+        it = best_pass.emplace(pr, std::make_pair(bp, bt)).first;
+      }
+      plan.push_back(it->second.first);
+      total += it->second.second;
+    }
+    if (total < best_total) { best_total = total; best_plan = plan; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  tuned_plans()[key] = best_plan;
+  if (best_ms) *best_ms = best_total;
+  return best_plan;
+}
+
+NttPlan ntt_plan(int log_d, int lanes, int layer_begin) { return plan_for(log_d, lanes, layer_begin); }
+
+std::string ntt_plan_desc(const NttPlan& plan) {
+  std::string d;
+  for (auto& ps : plan) {
+    if (!d.empty()) d += " + ";
+    d += "R" + std::to_string(ps.R) + "@l" + std::to_string(ps.l0) + " x" + std::to_string(1 << ps.lgs) +
+         " lanes/" + std::to_string(ps.threads) + "t";
+  }
+  return d;
+}
+
+size_t ntt_plan_count(int log_d, int lanes, int layer_begin) { return all_plans(log_d, lanes, layer_begin).size(); }
+
+void ntt_rs_encode_plan(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, size_t plan_idx,
+                        cudaStream_t s) {
+  const int log_d = log_msg_pos + log_inv_rate;
+  auto plans = all_plans(log_d, lanes, log_inv_rate);
+  if (plan_idx >= plans.size()) throw std::out_of_range("ntt plan index");
+  size_t msg_len = ((size_t)lanes) << log_msg_pos;
+  count_launch(); k_replicate<<<(unsigned)((msg_len + 255) / 256), 256, 0, s>>>(msg, cw, msg_len, 1 << log_inv_rate);
+  run_plan(plans[plan_idx], cw, log_d, lanes, false, s);
+}
 
 void ntt_rs_encode(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, cudaStream_t s) {
   size_t msg_len = ((size_t)lanes) << log_msg_pos;

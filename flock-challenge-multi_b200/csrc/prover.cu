@@ -118,7 +118,58 @@ Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
   CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
   sms = dev_sms;
   for (int i = 0; i < kPhases + 1; i++) CK(cudaEventCreate(&ev[i]));
+  tune_ntt_plans();
+  capture_commit();
   device_bytes = t_alloc_bytes - bytes0;
+}
+
+// Tune the pass plans of every NTT shape a proof of this size runs, on this
+// setup's own buffers before they hold data: the commitment (64 lanes, rate
+// 1/2), each Ligero level, and the transposed encodes of the query-basis
+// induction (one lane).
+void Setup::tune_ntt_plans() {
+  ntt_autotune(cw0, m - 12, 64, 1, st);
+  for (auto& L : levels) ntt_autotune(L.cw, L.log_msg_pos + L.rate, L.lanes, L.rate, st);
+  int n = m - 7 - lad->initial_k;
+  ntt_autotune(induce_buf, n + lad->rate[0], 1, lad->rate[0], st);
+  for (size_t i = 0; i + 1 < lad->ks.size(); i++) {
+    n -= lad->ks[i];
+    ntt_autotune(induce_buf, n + levels[i].rate, 1, levels[i].rate, st);
+  }
+  CK(cudaStreamSynchronize(st));
+}
+
+namespace {
+// Capture the launches `body` issues on `st` into an executable graph;
+// returns the graph and the number of kernel launches it holds.
+template <class F>
+cudaGraphExec_t capture(cudaStream_t st, uint64_t* launches, F&& body) {
+  const uint64_t l0 = thread_launch_counter();
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaGraph_t g = nullptr;
+  try {
+    body();
+  } catch (...) {
+    cudaStreamEndCapture(st, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  CK(cudaStreamEndCapture(st, &g));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  CK(e);
+  // the capture counted its kernel nodes; they run once per replay
+  *launches = thread_launch_counter() - l0;
+  kernel_launch_counter().fetch_sub(*launches, std::memory_order_relaxed);
+  thread_launch_counter() = l0;
+  return exec;
+}
+}  // namespace
+
+void Setup::capture_commit() {
+  commit_graph[0] = capture(st, &commit_launches[0], [&] { ntt_rs_encode(z, cw0, m - 13, 64, 1, st); });
+  commit_graph[1] = capture(st, &commit_launches[1], [&] { merkle_build(cw0, n_leaves0, 64 * 16, tree0, st); });
 }
 
 Setup::~Setup() {
@@ -131,6 +182,8 @@ Setup::~Setup() {
   cudaFreeHost(h_found);
   cudaFreeHost(h_out);
   cudaFreeHost(h_stage);
+  for (auto g : commit_graph)
+    if (g) cudaGraphExecDestroy(g);
   for (int i = 0; i < kPhases + 1; i++) cudaEventDestroy(ev[i]);
   cudaStreamDestroy(st);
 }
@@ -263,10 +316,13 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   else launch_witness_blocks(blocks_dev, (uint32_t)n_blocks, n_slots, z, a, b, st);
   CK(cudaGetLastError());
   mark(1);
-  // ---- K1 + K2 commit: 64 interleaved lanes, rate 1/2, 1 KiB leaves
-  ntt_rs_encode(z, cw0, m - 13, 64, 1, st);
+  // ---- K1 + K2 commit: 64 interleaved lanes, rate 1/2, 1 KiB leaves (two
+  // captured graphs, the phase event between them)
+  CK(cudaGraphLaunch(commit_graph[0], st));
+  count_launch(commit_launches[0]);
   mark(2);
-  merkle_build(cw0, n_leaves0, 64 * 16, tree0, st);
+  CK(cudaGraphLaunch(commit_graph[1], st));
+  count_launch(commit_launches[1]);
   P.root = root_of(tree0, n_leaves0);
   mark(3);
 

@@ -74,6 +74,13 @@ class Setup {
   uint32_t *at_ptr = nullptr, *bt_ptr = nullptr;
   uint16_t *at_row = nullptr, *bt_row = nullptr;
   cudaEvent_t ev[kPhases + 1] = {};
+  // The commitment's RS encode (z -> cw0) and Merkle tree (cw0 -> tree0) on
+  // fixed buffers, each captured once as a CUDA graph (after the NTT plans
+  // are tuned) and replayed by every proof.
+  cudaGraphExec_t commit_graph[2] = {nullptr, nullptr};
+  uint64_t commit_launches[2] = {0, 0};
+  void tune_ntt_plans();
+  void capture_commit();
 };
 
 }  // namespace flock

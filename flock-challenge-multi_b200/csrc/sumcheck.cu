@@ -108,17 +108,27 @@ void fold_pair_final(const f128* a_in, const f128* b_in, f128 rho, f128* out, cu
 }
 
 // ------------------------------------------------------------------ K6 --
-__global__ void k_lc_comb(const uint32_t* __restrict__ at_ptr, const uint16_t* __restrict__ at_row,
-                          const uint32_t* __restrict__ bt_ptr, const uint16_t* __restrict__ bt_row,
-                          const f128* __restrict__ eq, f128 alpha, f128 beta, int pin, f128* __restrict__ comb) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
+// comb[c] = alpha * (A^T eq)[c] + (B^T eq)[c] (+ beta at the pinned column):
+// one warp per column, its lanes striding over the column's nonzeros
+// (CSC row indices) and XOR-reducing by shuffles.
+__global__ void __launch_bounds__(256) k_lc_comb(const uint32_t* __restrict__ at_ptr,
+                                                 const uint16_t* __restrict__ at_row,
+                                                 const uint32_t* __restrict__ bt_ptr,
+                                                 const uint16_t* __restrict__ bt_row, const f128* __restrict__ eq,
+                                                 f128 alpha, f128 beta, int pin, f128* __restrict__ comb) {
+  const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
   if (c >= kK_) return;
   f128 sa = mk(0, 0), sb = mk(0, 0);
-  for (uint32_t j = at_ptr[c]; j < at_ptr[c + 1]; j++) sa = fx(sa, ldg(eq + at_row[j]));
-  for (uint32_t j = bt_ptr[c]; j < bt_ptr[c + 1]; j++) sb = fx(sb, ldg(eq + bt_row[j]));
-  f128 v = fx(fmul(alpha, sa), sb);
-  if (c == pin) v = fx(v, beta);
-  st(comb + c, v);
+  for (uint32_t j = at_ptr[c] + lane; j < at_ptr[c + 1]; j += 32) sa = fx(sa, ldg(eq + at_row[j]));
+  for (uint32_t j = bt_ptr[c] + lane; j < bt_ptr[c + 1]; j += 32) sb = fx(sb, ldg(eq + bt_row[j]));
+  sa = warp_xor(sa);
+  sb = warp_xor(sb);
+  if (lane == 0) {
+    f128 v = fx(fmul(alpha, sa), sb);
+    if (c == pin) v = fx(v, beta);
+    st(comb + c, v);
+  }
 }
 
 // z_vec[i] = XOR over compressions o of eq(x_outer, o) where bit i of o's
@@ -234,7 +244,7 @@ __global__ void __launch_bounds__(512) k_lc_round(f128* comb, f128* zv, int len,
 
 void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
              const f128* eq, f128 alpha, f128 beta, int pin, f128* comb, cudaStream_t s) {
-  count_launch(); k_lc_comb<<<kK_ / 128, 128, 0, s>>>(at_ptr, at_row, bt_ptr, bt_row, eq, alpha, beta, pin, comb);
+  count_launch(); k_lc_comb<<<kK_ * 32 / 256, 256, 0, s>>>(at_ptr, at_row, bt_ptr, bt_row, eq, alpha, beta, pin, comb);
 }
 void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, f128* zv, cudaStream_t s) {
   const int chunk = 1024;  // compressions per CTA (a multiple of 64)
@@ -287,6 +297,53 @@ __global__ void __launch_bounds__(256) k_lig_fold_msg(const f128* __restrict__ f
     block_xor_out(reduce(u0), out);
     block_xor_out(reduce(u2), out + 1);
   }
+}
+
+// Degree-3 sumcheck round over plain F128 vectors (the zerocheck round of
+// zerocheck/multilinear.rs:616-657 in its unstructured form): for the pairs
+// (a0, a1) = (a[2j], a[2j+1]), (b0, b1) likewise and eq weight e[j],
+//   G(1) = sum_j e[j] a1 b1,  G(inf) = sum_j e[j] (a0 + a1)(b0 + b1),
+// optionally after folding the previous round's pairs at rho (LSB binding,
+// a' = a0 + rho (a0 + a1); multilinear.rs:3194-3219).  The eq product is
+// accumulated unreduced; rho's operand split is built once per thread.
+template <bool FOLD>
+__global__ void __launch_bounds__(256) k_sc3_round(const f128* __restrict__ a, const f128* __restrict__ b,
+                                                   const f128* __restrict__ e, f128* __restrict__ ao,
+                                                   f128* __restrict__ bo, f128 rho, size_t n_pairs,
+                                                   f128* __restrict__ out) {
+  const MulConst R = mulconst(rho);
+  u256 g1 = zero256(), gi = zero256();
+  for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < n_pairs; j += (size_t)gridDim.x * blockDim.x) {
+    f128 a0, a1, b0, b1;
+    if (FOLD) {
+      f128 av[4], bv[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) { av[k] = ld(a + 4 * j + k); bv[k] = ld(b + 4 * j + k); }
+      a0 = fx(av[0], fmul_c(fx(av[0], av[1]), R));
+      a1 = fx(av[2], fmul_c(fx(av[2], av[3]), R));
+      b0 = fx(bv[0], fmul_c(fx(bv[0], bv[1]), R));
+      b1 = fx(bv[2], fmul_c(fx(bv[2], bv[3]), R));
+      st(ao + 2 * j, a0); st(ao + 2 * j + 1, a1);
+      st(bo + 2 * j, b0); st(bo + 2 * j + 1, b1);
+    } else {
+      a0 = ld(a + 2 * j); a1 = ld(a + 2 * j + 1);
+      b0 = ld(b + 2 * j); b1 = ld(b + 2 * j + 1);
+    }
+    const f128 w = ld(e + j);
+    acc_wide(g1, mul_wide(w, fmul(a1, b1)));
+    acc_wide(gi, mul_wide(w, fmul(fx(a0, a1), fx(b0, b1))));
+  }
+  block_xor_out(reduce(g1), out);
+  block_xor_out(reduce(gi), out + 1);
+}
+
+void sc3_round(const f128* a, const f128* b, const f128* e, f128* ao, f128* bo, const f128* rho, size_t n_pairs,
+               f128* out, int grid, cudaStream_t s) {
+  count_launch();
+  if (rho)
+    k_sc3_round<true><<<grid, 256, 0, s>>>(a, b, e, ao, bo, *rho, n_pairs, out);
+  else
+    k_sc3_round<false><<<grid, 256, 0, s>>>(a, b, e, ao, bo, mk(0, 0), n_pairs, out);
 }
 
 void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int grid, cudaStream_t s) {

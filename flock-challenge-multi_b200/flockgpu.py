@@ -26,7 +26,8 @@ EXPORTS = (
     "flock_witness", "flock_ntt_rs_encode", "flock_merkle_tree", "flock_sumcheck_round",
     "flock_pow", "flock_f128_mul", "flock_statement_digest", "flock_bench_ntt",
     "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove", "flock_merkle_root_noalloc",
-    "flock_serve_start", "flock_submit", "flock_poll",
+    "flock_serve_start", "flock_submit", "flock_poll", "flock_sumcheck_round3", "flock_bench_sumcheck3",
+    "flock_ntt_autotune", "flock_ntt_rs_encode_plan",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -69,8 +70,12 @@ def load() -> ctypes.CDLL:
         lib.flock_setup_phase_ms.argtypes = [vp, vp, i32]
         lib.flock_witness.argtypes = [vp, u32, u64, vp, vp, vp]
         lib.flock_ntt_rs_encode.argtypes = [vp, vp, u32, u32, u32, vp]
+        lib.flock_ntt_rs_encode_plan.argtypes = [vp, vp, u32, u32, u32, u32, vp]
+        lib.flock_ntt_autotune.argtypes = [vp, u32, u32, u32, ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, sz]
         lib.flock_merkle_tree.argtypes = [vp, vp, sz, sz, vp]
         lib.flock_sumcheck_round.argtypes = [vp, vp, vp, sz, vp]
+        lib.flock_sumcheck_round3.argtypes = [vp, vp, vp, vp, sz, vp, vp, vp, vp]
+        lib.flock_bench_sumcheck3.argtypes = [vp, sz, i32, ctypes.POINTER(ctypes.c_double)]
         lib.flock_pow.argtypes = [vp, vp, u32, ctypes.POINTER(u64)]
         lib.flock_f128_mul.argtypes = [vp, vp, vp, sz, vp]
         lib.flock_statement_digest.argtypes = [u32, vp]
@@ -184,6 +189,24 @@ class Context:
                     "ntt_rs_encode")
         return out
 
+    def ntt_rs_encode_plan(self, msg: np.ndarray, log_msg_pos: int, lanes: int, log_inv_rate: int, plan: int):
+        """The encode with candidate pass plan `plan`; None past the last plan."""
+        msg = np.ascontiguousarray(msg, np.uint64)
+        out = np.zeros(msg.size << log_inv_rate, np.uint64)
+        rc = self.lib.flock_ntt_rs_encode_plan(self.h, _ptr(msg), log_msg_pos, lanes, log_inv_rate, plan, _ptr(out))
+        if rc == 1:
+            return None
+        self._check(rc, "ntt_rs_encode_plan")
+        return out
+
+    def ntt_autotune(self, log_msg_pos: int, lanes: int, log_inv_rate: int):
+        """(best plan ms or -1 if already tuned, plan description)."""
+        ms = ctypes.c_double()
+        d = ctypes.create_string_buffer(256)
+        self._check(self.lib.flock_ntt_autotune(self.h, log_msg_pos, lanes, log_inv_rate, ctypes.byref(ms), d, 256),
+                    "ntt_autotune")
+        return ms.value, d.value.decode()
+
     def merkle_tree(self, data: np.ndarray, n_leaves: int, leaf_size: int) -> np.ndarray:
         data = np.ascontiguousarray(data, np.uint8)
         out = np.zeros((2 * n_leaves - 1) * 32, np.uint8)
@@ -196,6 +219,19 @@ class Context:
         out = np.zeros(4, np.uint64)
         self._check(self.lib.flock_sumcheck_round(self.h, _ptr(f), _ptr(b), f.size // 2, _ptr(out)), "sumcheck_round")
         return out
+
+    def sumcheck_round3(self, e: np.ndarray, a: np.ndarray, b: np.ndarray, rho=None):
+        """Degree-3 round: (G(1), G(inf)) as 4 u64, after an optional fold of
+        a, b at rho ((lo, hi)); returns (msg, a_folded, b_folded)."""
+        e, a, b = (np.ascontiguousarray(x, np.uint64) for x in (e, a, b))
+        n = a.size // 2
+        out = np.zeros(4, np.uint64)
+        ao, bo = np.zeros(n, np.uint64), np.zeros(n, np.uint64)
+        r = None if rho is None else np.array(rho, np.uint64)
+        self._check(self.lib.flock_sumcheck_round3(self.h, _ptr(e), _ptr(a), _ptr(b), n,
+                                                   None if r is None else _ptr(r), _ptr(ao), _ptr(bo), _ptr(out)),
+                    "sumcheck_round3")
+        return (out, None, None) if rho is None else (out, ao, bo)
 
     def pow(self, digest: bytes, bits: int) -> int:
         d = np.frombuffer(digest, np.uint8).copy()
@@ -223,6 +259,12 @@ class Context:
     def bench_sumcheck(self, n: int, iters: int = 5) -> float:
         ms = ctypes.c_double()
         self._check(self.lib.flock_bench_sumcheck(self.h, n, iters, ctypes.byref(ms)), "bench_sumcheck")
+        return ms.value
+
+
+    def bench_sumcheck3(self, n: int, iters: int = 5) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.flock_bench_sumcheck3(self.h, n, iters, ctypes.byref(ms)), "bench_sumcheck3")
         return ms.value
 
 

@@ -80,7 +80,31 @@ int flock_witness(flock_ctx* ctx, uint32_t log2, uint64_t seed, uint64_t* z, uin
 int flock_ntt_rs_encode(flock_ctx* ctx, const uint64_t* msg, uint32_t log_msg_pos, uint32_t lanes,
                         uint32_t log_inv_rate, uint64_t* out);
 int flock_merkle_tree(flock_ctx* ctx, const uint8_t* data, size_t n_leaves, size_t leaf_size, uint8_t* tree_out);
+/* NTT pass plans.  A plan splits the butterfly layers into passes over
+ * shared-memory tiles (layers per pass, lanes per tile, threads per CTA);
+ * flock_ntt_autotune times the candidate plans of a shape on this device and
+ * keeps the fastest for every later encode of that shape in this process
+ * (setups tune their own shapes when created).  desc receives a short
+ * description of the chosen plan.  flock_ntt_rs_encode_plan runs candidate
+ * plan `plan_index` (FLOCK_ERR_ARG past the last one); every plan gives the
+ * same codeword.  No counterpart in the reference, whose CPU NTT has a fixed
+ * schedule (crates/flock-core/src/ntt/additive_ntt_f128.rs:2785-2940). */
+int flock_ntt_autotune(flock_ctx* ctx, uint32_t log_msg_pos, uint32_t lanes, uint32_t log_inv_rate, double* best_ms,
+                       char* desc, size_t desc_cap);
+int flock_ntt_rs_encode_plan(flock_ctx* ctx, const uint64_t* msg, uint32_t log_msg_pos, uint32_t lanes,
+                             uint32_t log_inv_rate, uint32_t plan_index, uint64_t* out);
+
 int flock_sumcheck_round(flock_ctx* ctx, const uint64_t* f, const uint64_t* b, size_t n, uint64_t* msg_out);
+/* Degree-3 (zerocheck-style) round over plain F128 vectors: msg_out =
+ * (G(1), G(inf)) with G(1) = sum_j e[j] a[2j+1] b[2j+1] and
+ * G(inf) = sum_j e[j] (a[2j] + a[2j+1]) (b[2j] + b[2j+1]).  With rho != NULL
+ * a and b (n values each) are first folded at rho into a_out, b_out (n/2
+ * values: x'[j] = x[2j] + rho (x[2j] + x[2j+1])) and the message is taken
+ * over the folded pairs (e: n/4 values); otherwise e has n/2 values.
+ * Replaces round_pair_naive + fold_in_place_pair (crates/flock-core/src/
+ * zerocheck/multilinear.rs:616-657, 3194-3219). */
+int flock_sumcheck_round3(flock_ctx* ctx, const uint64_t* e, const uint64_t* a, const uint64_t* b, size_t n,
+                          const uint64_t* rho, uint64_t* a_out, uint64_t* b_out, uint64_t* msg_out);
 int flock_pow(flock_ctx* ctx, const uint8_t* digest32, uint32_t bits, uint64_t* nonce);
 int flock_f128_mul(flock_ctx* ctx, const uint64_t* a, const uint64_t* b, size_t n, uint64_t* out);
 /* BLAKE3 digest of the R1CS statement for m = 14 + log2 (host only; replaces
@@ -93,6 +117,8 @@ int flock_bench_ntt(flock_ctx* ctx, uint32_t log_msg_pos, uint32_t lanes, uint32
                     double* ms);
 int flock_bench_merkle(flock_ctx* ctx, size_t n_leaves, size_t leaf_size, int iters, double* ms);
 int flock_bench_sumcheck(flock_ctx* ctx, size_t n, int iters, double* ms);
+/* fused fold + degree-3 message of flock_sumcheck_round3 over n values */
+int flock_bench_sumcheck3(flock_ctx* ctx, size_t n, int iters, double* ms);
 /* `steps` back-to-back proofs (seeds seed0, seed0+1, ...) timed with CUDA
  * events on the setup's stream; also the mean per-phase device times and the
  * number of this library's kernel launches inside the timed region. */

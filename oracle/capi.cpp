@@ -28,6 +28,14 @@ void flockref_f128_mul(const uint64_t* a, const uint64_t* b, uint64_t* out) {
   out[0] = r.lo;
   out[1] = r.hi;
 }
+// element-wise products of n F128 values ({lo, hi} pairs)
+void flockref_f128_mul_n(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* out) {
+  for (size_t i = 0; i < n; i++) {
+    F128 r = F128(a[2 * i], a[2 * i + 1]) * F128(b[2 * i], b[2 * i + 1]);
+    out[2 * i] = r.lo;
+    out[2 * i + 1] = r.hi;
+  }
+}
 void flockref_f128_inv(const uint64_t* a, uint64_t* out) {
   F128 r = f128_inv(F128(a[0], a[1]));
   out[0] = r.lo;

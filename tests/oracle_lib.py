@@ -22,6 +22,7 @@ class Oracle:
         vp, u32, u64, sz, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_int
         L.flockref_prove.argtypes = [u32, u64, vp, sz, ctypes.POINTER(sz)]
         L.flockref_f128_mul.argtypes = [vp, vp, vp]
+        L.flockref_f128_mul_n.argtypes = [vp, vp, sz, vp]
         L.flockref_f128_inv.argtypes = [vp, vp]
         L.flockref_phi8_table.argtypes = [vp]
         L.flockref_gf8_mul.argtypes = [ctypes.c_uint8, ctypes.c_uint8]
@@ -71,9 +72,7 @@ class Oracle:
         a = np.ascontiguousarray(a, np.uint64)
         b = np.ascontiguousarray(b, np.uint64)
         out = np.zeros_like(a)
-        for i in range(a.size // 2):
-            self.L.flockref_f128_mul(ctypes.c_void_p(a.ctypes.data + 16 * i), ctypes.c_void_p(b.ctypes.data + 16 * i),
-                                     ctypes.c_void_p(out.ctypes.data + 16 * i))
+        self.L.flockref_f128_mul_n(_p(a), _p(b), a.size // 2, _p(out))
         return out
 
     def phi8_table(self):

@@ -49,6 +49,23 @@ def test_ntt_rs_encode(gpu_ctx, oracle, lanes, log_pos, rate):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("lanes,log_pos,rate", [(64, 10, 1), (1, 16, 2), (8, 13, 3), (256, 6, 1), (4, 19, 1)])
+def test_ntt_every_plan(gpu_ctx, oracle, lanes, log_pos, rate):
+    """Every pass plan the autotuner may pick gives the oracle's codeword."""
+    msg = rng_u64(lanes * 7 + log_pos, 2 * (lanes << log_pos))
+    want = oracle.rs_encode(msg, 1 << log_pos, lanes, rate)
+    k = 0
+    while True:
+        got = gpu_ctx.ntt_rs_encode_plan(msg, log_pos, lanes, rate, k)
+        if got is None:
+            break
+        assert np.array_equal(got, want), f"plan {k}"
+        k += 1
+    assert k >= 2
+    ms, desc = gpu_ctx.ntt_autotune(log_pos, lanes, rate)
+    assert desc and np.array_equal(gpu_ctx.ntt_rs_encode(msg, log_pos, lanes, rate), want)
+
+
 @pytest.mark.parametrize("n_leaves,leaf_size", [(1, 64), (2, 32), (16, 48), (1024, 128), (4096, 1024), (2048, 512)])
 def test_merkle_tree(gpu_ctx, oracle, n_leaves, leaf_size):
     data = np.random.default_rng(n_leaves + leaf_size).integers(0, 256, n_leaves * leaf_size, dtype=np.uint8)
@@ -64,6 +81,56 @@ def test_sumcheck_round(gpu_ctx, oracle):
         oracle.f128_mul((F[0::2] ^ F[1::2]).reshape(-1), (B[0::2] ^ B[1::2]).reshape(-1)).reshape(-1, 2), axis=0)
     got = gpu_ctx.sumcheck_round(f, b)
     assert list(got) == [u0[0], u0[1], u2[0], u2[1]]
+
+
+def _xor_rows(v):
+    return np.bitwise_xor.reduce(v.reshape(-1, 2), axis=0)
+
+
+@pytest.mark.parametrize("log_n", [1, 6, 16])
+def test_sumcheck_round_deg2_sizes(gpu_ctx, oracle, log_n):
+    n = 1 << log_n
+    f, b = rng_u64(50 + log_n, 2 * n), rng_u64(60 + log_n, 2 * n)
+    F, B = f.reshape(-1, 2), b.reshape(-1, 2)
+    u0 = _xor_rows(oracle.f128_mul(F[0::2].reshape(-1), B[0::2].reshape(-1)))
+    u2 = _xor_rows(oracle.f128_mul((F[0::2] ^ F[1::2]).reshape(-1), (B[0::2] ^ B[1::2]).reshape(-1)))
+    assert list(gpu_ctx.sumcheck_round(f, b)) == [u0[0], u0[1], u2[0], u2[1]]
+
+
+def _deg3_expect(oracle, e, a, b):
+    A, B = a.reshape(-1, 2), b.reshape(-1, 2)
+    a0, a1, b0, b1 = A[0::2].reshape(-1), A[1::2].reshape(-1), B[0::2].reshape(-1), B[1::2].reshape(-1)
+    g1 = _xor_rows(oracle.f128_mul(e, oracle.f128_mul(a1, b1)))
+    gi = _xor_rows(oracle.f128_mul(e, oracle.f128_mul(a0 ^ a1, b0 ^ b1)))
+    return [g1[0], g1[1], gi[0], gi[1]]
+
+
+def _fold(oracle, x, rho):
+    X = x.reshape(-1, 2)
+    x0, x1 = X[0::2].reshape(-1), X[1::2].reshape(-1)
+    r = np.tile(np.array(rho, np.uint64), x0.size // 2)
+    return x0 ^ oracle.f128_mul(r, x0 ^ x1)
+
+
+@pytest.mark.parametrize("log_n", [1, 5, 16])
+def test_sumcheck_round_deg3(gpu_ctx, oracle, log_n):
+    """Zerocheck-style round (eq * a * b) over plain F128 vectors."""
+    n = 1 << log_n
+    a, b, e = rng_u64(70 + log_n, 2 * n), rng_u64(80 + log_n, 2 * n), rng_u64(90 + log_n, n)
+    msg, _, _ = gpu_ctx.sumcheck_round3(e, a, b)
+    assert list(msg) == _deg3_expect(oracle, e, a, b)
+
+
+@pytest.mark.parametrize("log_n", [2, 7, 16])
+def test_sumcheck_fold_round_deg3(gpu_ctx, oracle, log_n):
+    """Fold at rho, then the degree-3 message over the folded pairs."""
+    n = 1 << log_n
+    a, b, e = rng_u64(100 + log_n, 2 * n), rng_u64(110 + log_n, 2 * n), rng_u64(120 + log_n, n // 2)
+    rho = (0x0123456789ABCDEF, 0xFEDCBA9876543210)
+    msg, ao, bo = gpu_ctx.sumcheck_round3(e, a, b, rho)
+    fa, fb = _fold(oracle, a, rho), _fold(oracle, b, rho)
+    assert np.array_equal(ao, fa) and np.array_equal(bo, fb)
+    assert list(msg) == _deg3_expect(oracle, e, fa, fb)
 
 
 @pytest.mark.parametrize("bits", [1, 6, 12])
