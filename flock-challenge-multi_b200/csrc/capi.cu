@@ -212,6 +212,51 @@ int flock_poll(flock_ctx* c, uint64_t ticket, flock_result* res, int timeout_ms)
   });
 }
 
+int flock_prove_batch(flock_ctx* c, const flock_job* jobs, size_t n, flock_result* results, int threads) {
+  if (!c || (n && (!jobs || !results)) || threads < 1 || threads > 64) return FLOCK_ERR_ARG;
+  for (size_t i = 0; i < n; i++)
+    if (jobs[i].log2_n < 8 || jobs[i].log2_n > 20 || (!jobs[i].domain && jobs[i].dlen)) {
+      c->err = "unsupported job (log2 in 8..=20)";
+      return FLOCK_ERR_ARG;
+    }
+  if (!c->server) {
+    int rc = flock_serve_start(c, 4);
+    if (rc && !c->server) return rc;
+  }
+  return guard(c, [&] {
+    std::vector<flock::Server::BatchItem> items(n);
+    for (size_t i = 0; i < n; i++) {
+      items[i].log2 = jobs[i].log2_n;
+      items[i].seed = jobs[i].seed;
+      items[i].blocks = jobs[i].blocks;
+      items[i].domain.assign((const char*)jobs[i].domain, jobs[i].dlen);
+    }
+    std::vector<flock::JobResult> rs = c->server->prove_batch(items, threads);
+    int rc = FLOCK_OK;
+    for (size_t i = 0; i < n; i++) {
+      flock_result& o = results[i];
+      const flock::JobResult& r = rs[i];
+      o.status = r.status;
+      o.queue_ms = r.queue_ms;
+      o.run_ms = r.run_ms;
+      o.latency_ms = r.latency_ms;
+      o.out_len = r.bytes.size();
+      if (r.status != FLOCK_OK) {
+        c->err = r.error;
+        continue;
+      }
+      if (r.bytes.size() > o.cap || !o.out) {
+        o.status = FLOCK_ERR_CAPACITY;
+        c->err = "output buffer too small";
+        rc = FLOCK_ERR_CAPACITY;
+        continue;
+      }
+      memcpy(o.out, r.bytes.data(), r.bytes.size());
+    }
+    return rc;
+  });
+}
+
 int flock_statement_digest(uint32_t m, uint8_t* out32) {
   if (!out32 || m < 17 || m > 40) return FLOCK_ERR_ARG;
   try {

@@ -55,6 +55,7 @@ using NttPlan = std::vector<NttPass>;
 // encodes of the shape use it (untuned shapes use the default split).
 NttPlan ntt_autotune(f128* scratch, int log_d, int lanes, int layer_begin, cudaStream_t s, double* best_ms = nullptr);
 NttPlan ntt_plan(int log_d, int lanes, int layer_begin);
+const f128* ntt_evals(int log_d);  // device table of the per-layer basis values
 std::string ntt_plan_desc(const NttPlan& plan);
 // every candidate plan of a shape, for parity tests of the tiling
 size_t ntt_plan_count(int log_d, int lanes, int layer_begin);
@@ -63,6 +64,37 @@ void ntt_rs_encode_plan(const f128* msg, f128* cw, int log_msg_pos, int lanes, i
 void ntt_rs_encode(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, cudaStream_t s);
 void ntt_forward(f128* data, int log_d, int lanes, int start_layer, cudaStream_t s);
 void ntt_transposed_encode(f128* e, f128* out, int log_msg, int log_inv_rate, cudaStream_t s);
+// Fused multi-proof commit (serving / batching): one entry per proof of a
+// device-resident job table; every launch of the commit covers all jobs, a
+// thread block finding its job by binary search over the per-launch first
+// indices (jobs that take no part in a launch have an empty range).
+struct BatchJob {
+  uint64_t seed;  // witness inputs from the benchmark generator
+  uint32_t log2, n_blocks, n_slots;
+  f128 *z, *a, *b;
+  uint64_t wcta0;  // first CTA of this job in the witness launch
+  f128* cw;        // RS codeword: 64 lanes, rate 1/2, 2^log_d positions
+  const f128* ev;  // per-layer basis values of the NTT of dimension log_d
+  int log_d;
+  uint64_t msg_len, rep0;  // message values; first element in the replicate launch
+  int n_pass;
+  NttPass pass[3];
+  uint64_t tile0[3];  // first tile of this job in the launch of pass p
+  uint32_t* tree;     // Merkle tree over 2^log_d leaves of 1 KiB
+  uint64_t n_leaves, leaf0;
+  uint64_t par0[24];  // first node of this job in the launch of parent level k
+  uint64_t top_start, top_len;  // the level the per-job top kernel starts from
+};
+uint32_t witness_ctas(uint32_t n_slots);
+void launch_witness_seed_batch(const BatchJob* jobs, int n_jobs, uint32_t total_ctas, cudaStream_t s);
+void ntt_replicate_batch(const BatchJob* jobs, int n_jobs, uint64_t total, cudaStream_t s);
+size_t ntt_pass_batch_smem(const NttPass& p);
+void ntt_pass_batch(const BatchJob* jobs, int n_jobs, int pass, uint64_t total_tiles, size_t smem, int grid,
+                    cudaStream_t s);
+void merkle_leaves_batch(const BatchJob* jobs, int n_jobs, uint64_t total, cudaStream_t s);
+void merkle_parents_batch(const BatchJob* jobs, int n_jobs, int level, uint64_t total, cudaStream_t s);
+void merkle_top_batch(const BatchJob* jobs, int n_jobs, cudaStream_t s);
+
 // K2 / K9
 void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, cudaStream_t s);
 __global__ void k_gather_nodes(const uint32_t* tree, const uint64_t* idx, size_t n, uint32_t* out);

@@ -10,12 +10,10 @@
 // BLAKE3 hash of (state_digest || n_le || 0^24) has `bits` leading zero bits.
 #include "kernels.cuh"
 
-// one thread per leaf; leaf_size <= 1024 (a single BLAKE3 chunk)
-__global__ void k_merkle_leaves(const uint8_t* __restrict__ data, size_t leaf_size, size_t n_leaves,
-                                uint32_t* __restrict__ tree) {
-  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_leaves) return;
-  const uint8_t* p = data + i * leaf_size;
+namespace {
+// non-root chaining value of one leaf of leaf_size <= 1024 bytes (a single
+// BLAKE3 chunk) into out (8 words)
+__device__ __forceinline__ void leaf_cv(const uint8_t* __restrict__ p, size_t leaf_size, uint32_t* __restrict__ out) {
   uint32_t cv[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) cv[k] = b3d::kIV[k];
@@ -39,15 +37,14 @@ __global__ void k_merkle_leaves(const uint8_t* __restrict__ data, size_t leaf_si
     uint32_t flags = (blk == 0 ? b3d::CHUNK_START : 0) | (blk + 1 == nblk ? b3d::CHUNK_END : 0);
     b3d::compress(cv, m, 0, (uint32_t)len, flags, cv);
   }
-  uint4* o = reinterpret_cast<uint4*>(tree + 8 * i);
+  uint4* o = reinterpret_cast<uint4*>(out);
   o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
   o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
 }
 
-__global__ void k_merkle_parents(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, size_t n_out) {
-  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_out) return;
-  const uint4* q = reinterpret_cast<const uint4*>(in + 16 * i);
+// parent CV of the two child CVs at in (16 words) into out (8 words)
+__device__ __forceinline__ void parent_cv(const uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
+  const uint4* q = reinterpret_cast<const uint4*>(in);
   uint32_t m[16];
 #pragma unroll
   for (int k = 0; k < 4; k++) {
@@ -56,14 +53,15 @@ __global__ void k_merkle_parents(const uint32_t* __restrict__ in, uint32_t* __re
   }
   uint32_t cv[8];
   b3d::compress(b3d::kIV, m, 0, 64, b3d::PARENT, cv);
-  uint4* o = reinterpret_cast<uint4*>(out + 8 * i);
+  uint4* o = reinterpret_cast<uint4*>(out);
   o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
   o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
 }
 
-// upper levels of a tree inside one CTA (levels of at most 1024 nodes); each
-// level is read back from global memory after the barrier that published it
-__global__ void k_merkle_top(uint32_t* tree, size_t level_start, size_t level_len) {
+// upper levels of one tree inside one CTA (levels of at most 1024 nodes);
+// each level is read back from global memory after the barrier that
+// published it
+__device__ __forceinline__ void tree_top(uint32_t* tree, size_t level_start, size_t level_len) {
   int t = threadIdx.x;
   size_t len = level_len, start = level_start;
   while (len > 1) {
@@ -78,6 +76,75 @@ __global__ void k_merkle_top(uint32_t* tree, size_t level_start, size_t level_le
     start += len;
     len = n;
   }
+}
+
+// the job of global index i of a batched launch: the last job whose first
+// index (at member offset `field`) is <= i
+template <class F>
+__device__ __forceinline__ int find_job(const BatchJob* __restrict__ jobs, int n_jobs, uint64_t i, F first) {
+  int lo = 0, hi = n_jobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first(jobs[mid]) <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+}  // namespace
+
+// one thread per leaf
+__global__ void k_merkle_leaves(const uint8_t* __restrict__ data, size_t leaf_size, size_t n_leaves,
+                                uint32_t* __restrict__ tree) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_leaves) return;
+  leaf_cv(data + i * leaf_size, leaf_size, tree + 8 * i);
+}
+
+// the 1 KiB-leaf trees of every job of a batch (leaves, then one parent
+// level for all jobs per launch, then one CTA per job for its top levels)
+__global__ void k_merkle_leaves_batch(const BatchJob* __restrict__ jobs, int n_jobs, uint64_t total) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const BatchJob& J = jobs[find_job(jobs, n_jobs, i, [](const BatchJob& b) { return b.leaf0; })];
+  const uint64_t k = i - J.leaf0;
+  leaf_cv(reinterpret_cast<const uint8_t*>(J.cw) + k * 1024, 1024, J.tree + 8 * k);
+}
+__global__ void k_merkle_parents_batch(const BatchJob* __restrict__ jobs, int n_jobs, int level, uint64_t total) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const BatchJob& J = jobs[find_job(jobs, n_jobs, i, [level](const BatchJob& b) { return b.par0[level]; })];
+  const uint64_t k = i - J.par0[level];
+  // level `level` starts after the leaves and the levels below it
+  uint64_t start = 0, len = J.n_leaves;
+  for (int l = 1; l < level; l++) { start += len; len >>= 1; }
+  parent_cv(J.tree + 8 * (start + 2 * k), J.tree + 8 * (start + len + k));
+}
+__global__ void k_merkle_top_batch(const BatchJob* __restrict__ jobs) {
+  const BatchJob& J = jobs[blockIdx.x];
+  tree_top(J.tree, J.top_start, J.top_len);
+}
+
+__global__ void k_merkle_parents(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, size_t n_out) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_out) return;
+  parent_cv(in + 16 * i, out + 8 * i);
+}
+
+__global__ void k_merkle_top(uint32_t* tree, size_t level_start, size_t level_len) {
+  tree_top(tree, level_start, level_len);
+}
+
+void merkle_leaves_batch(const BatchJob* jobs, int n_jobs, uint64_t total, cudaStream_t s) {
+  count_launch();
+  k_merkle_leaves_batch<<<(unsigned)((total + 127) / 128), 128, 0, s>>>(jobs, n_jobs, total);
+}
+void merkle_parents_batch(const BatchJob* jobs, int n_jobs, int level, uint64_t total, cudaStream_t s) {
+  count_launch();
+  k_merkle_parents_batch<<<(unsigned)((total + 127) / 128), 128, 0, s>>>(jobs, n_jobs, level, total);
+}
+void merkle_top_batch(const BatchJob* jobs, int n_jobs, cudaStream_t s) {
+  count_launch();
+  k_merkle_top_batch<<<n_jobs, 512, 0, s>>>(jobs);
 }
 
 void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, cudaStream_t s) {

@@ -42,16 +42,15 @@ __device__ __forceinline__ f128 twiddle(const f128* ev, int l, uint64_t b) {
   return t;
 }
 
+// One tile of a pass (tile index t_id), staged through the CTA's shared memory.
 template <bool TRANSPOSE>
-__global__ void __launch_bounds__(256, 2) k_ntt_pass(PassArgs p) {
-  extern __shared__ f128 smem[];
+__device__ __forceinline__ void ntt_tile(const PassArgs& p, uint64_t t_id, f128* smem) {
   const int R = p.R, LG = 1 << p.lg_shift;
   f128* tile = smem;                       // [2^R][LG]
   f128* tw = smem + ((size_t)LG << R);     // [2^R - 1] : stage s block k at (1<<s)-1+k
   const int log_d = p.log_d, l0 = p.l0;
   const int lo_bits = log_d - l0 - R;      // position bits below the pair bits
   const int groups = p.lanes >> p.lg_shift;
-  uint64_t t_id = blockIdx.x;
   const int grp = (int)(t_id % groups);
   t_id /= groups;
   const uint64_t lo = t_id & ((1ull << lo_bits) - 1);
@@ -142,6 +141,48 @@ __global__ void __launch_bounds__(256, 2) k_ntt_pass(PassArgs p) {
     uint64_t pos = (hi << (log_d - l0)) | (pl << lo_bits) | lo;
     st(p.data + pos * p.lanes + ((size_t)grp << p.lg_shift) + (e & (LG - 1)), tile[e]);
   }
+}
+
+template <bool TRANSPOSE>
+__global__ void __launch_bounds__(256, 2) k_ntt_pass(PassArgs p) {
+  extern __shared__ f128 smem[];
+  ntt_tile<TRANSPOSE>(p, blockIdx.x, smem);
+}
+
+// Pass `pass` of every job of a batch: a persistent grid strides over the
+// tiles of all jobs (each job's tiles numbered from its tile0[pass]).
+__global__ void __launch_bounds__(256, 2) k_ntt_pass_batch(const BatchJob* __restrict__ jobs, int n_jobs, int pass,
+                                                           uint64_t total_tiles) {
+  extern __shared__ f128 smem[];
+  for (uint64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].tile0[pass] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchJob& J = jobs[lo];
+    const NttPass& ps = J.pass[pass];
+    const PassArgs a{J.cw, J.ev, J.log_d, 64, ps.lgs, ps.l0, ps.R};
+    __syncthreads();  // the previous tile's stores have read the shared tile
+    ntt_tile<false>(a, t - J.tile0[pass], smem);
+  }
+}
+
+__global__ void k_replicate_batch(const BatchJob* __restrict__ jobs, int n_jobs, uint64_t total) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  int lo = 0, hi = n_jobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].rep0 <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  const BatchJob& J = jobs[lo];
+  const uint64_t k = i - J.rep0;  // rate 1/2: the message and one copy
+  const f128 v = ld(J.z + k);
+  st(J.cw + k, v);
+  st(J.cw + J.msg_len + k, v);
 }
 
 __global__ void k_replicate(const f128* __restrict__ msg, f128* __restrict__ cw, size_t msg_len, int copies) {
@@ -355,6 +396,19 @@ void run_passes(f128* data, int log_d, int lanes, int layer_begin, bool transpos
 }
 }  // namespace
 
+void ntt_replicate_batch(const BatchJob* jobs, int n_jobs, uint64_t total, cudaStream_t s) {
+  count_launch();
+  k_replicate_batch<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(jobs, n_jobs, total);
+}
+size_t ntt_pass_batch_smem(const NttPass& p) { return pass_smem(p.lgs, p.R); }
+void ntt_pass_batch(const BatchJob* jobs, int n_jobs, int pass, uint64_t total_tiles, size_t smem, int grid,
+                    cudaStream_t s) {
+  CK(cudaFuncSetAttribute(k_ntt_pass_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  count_launch();
+  k_ntt_pass_batch<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)grid, total_tiles)), 256, smem, s>>>(
+      jobs, n_jobs, pass, total_tiles);
+}
+
 NttPlan ntt_autotune(f128* scratch, int log_d, int lanes, int layer_begin, cudaStream_t s, double* best_ms) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
@@ -421,6 +475,7 @@ NttPlan ntt_autotune(f128* scratch, int log_d, int lanes, int layer_begin, cudaS
 }
 
 NttPlan ntt_plan(int log_d, int lanes, int layer_begin) { return plan_for(log_d, lanes, layer_begin); }
+const f128* ntt_evals(int log_d) { return device_evals(log_d); }
 
 std::string ntt_plan_desc(const NttPlan& plan) {
   std::string d;

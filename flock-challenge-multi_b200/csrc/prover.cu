@@ -172,6 +172,104 @@ void Setup::capture_commit() {
   commit_graph[1] = capture(st, &commit_launches[1], [&] { merkle_build(cw0, n_leaves0, 64 * 16, tree0, st); });
 }
 
+// Fused witness + RS encode + Merkle commit of several seeded proofs: every
+// stage is one launch over all jobs (persistent NTT passes over the tiles of
+// every job, one parent level of every tree per launch), captured as one
+// CUDA graph and replayed on `st`.  The setups' streams wait for it; each
+// proof then continues with Setup::prove(..., committed = true).
+void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds, cudaStream_t st) {
+  const int n = (int)setups.size();
+  if (n == 0) return;
+  if ((int)seeds.size() != n) throw std::runtime_error("batch_commit: one seed per setup");
+  std::vector<BatchJob> J(n);
+  uint64_t wcta = 0, rep = 0, leaves = 0, tiles[3] = {0, 0, 0}, par[24] = {0};
+  size_t smem = 0;
+  int max_pass = 0, max_level = 0;
+  for (int i = 0; i < n; i++) {
+    Setup& S = *setups[i];
+    BatchJob& b = J[i];
+    b = BatchJob{};
+    b.seed = seeds[i];
+    b.log2 = S.log2;
+    b.n_blocks = 1u << S.log2;
+    b.n_slots = 1u << S.n_log;
+    b.z = S.z; b.a = S.a; b.b = S.b;
+    b.wcta0 = wcta;
+    wcta += witness_ctas(b.n_slots);
+    b.cw = S.cw0;
+    b.log_d = S.m - 12;
+    b.ev = ntt_evals(b.log_d);
+    b.msg_len = S.n_words;
+    b.rep0 = rep;
+    rep += b.msg_len;
+    const NttPlan plan = ntt_plan(b.log_d, 64, 1);
+    if (plan.size() > 3) throw std::runtime_error("batch_commit: more than three NTT passes");
+    b.n_pass = (int)plan.size();
+    max_pass = std::max(max_pass, b.n_pass);
+    for (int p = 0; p < 3; p++) {
+      b.tile0[p] = tiles[p];
+      if (p < b.n_pass) {
+        b.pass[p] = plan[p];
+        tiles[p] += ((uint64_t)1 << (b.log_d - plan[p].R)) * (uint64_t)(64 >> plan[p].lgs);
+        smem = std::max(smem, ntt_pass_batch_smem(plan[p]));
+      }
+    }
+    b.tree = S.tree0;
+    b.n_leaves = S.n_leaves0;
+    b.leaf0 = leaves;
+    leaves += b.n_leaves;
+    uint64_t start = 0, len = b.n_leaves;
+    int level = 0;
+    for (int l = 0; l < 24; l++) b.par0[l] = par[l];
+    while (len > 1024) {
+      level++;
+      if (level >= 24) throw std::runtime_error("batch_commit: tree too deep");
+      b.par0[level] = par[level];
+      par[level] += len >> 1;
+      start += len;
+      len >>= 1;
+    }
+    max_level = std::max(max_level, level);
+    b.top_start = start;
+    b.top_len = len;
+  }
+  // empty ranges for the jobs after the last one that takes part in a launch
+  for (int i = 0; i < n; i++)
+    for (int l = 0; l < 24; l++) J[i].par0[l] = std::min<uint64_t>(J[i].par0[l], par[l]);
+  BatchJob* dj = nullptr;
+  CK(cudaMalloc(&dj, n * sizeof(BatchJob)));
+  try {
+    CK(cudaMemcpyAsync(dj, J.data(), n * sizeof(BatchJob), cudaMemcpyHostToDevice, st));
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    uint64_t launches = 0;
+    cudaGraphExec_t g = capture(st, &launches, [&] {
+      launch_witness_seed_batch(dj, n, (uint32_t)wcta, st);
+      ntt_replicate_batch(dj, n, rep, st);
+      for (int p = 0; p < max_pass; p++) ntt_pass_batch(dj, n, p, tiles[p], smem, 2 * sms, st);
+      merkle_leaves_batch(dj, n, leaves, st);
+      for (int l = 1; l <= max_level; l++) merkle_parents_batch(dj, n, l, par[l], st);
+      merkle_top_batch(dj, n, st);
+    });
+    const cudaError_t e = cudaGraphLaunch(g, st);
+    count_launch(launches);
+    cudaEvent_t done;
+    CK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    CK(cudaEventRecord(done, st));
+    for (Setup* S : setups) CK(cudaStreamWaitEvent(S->st, done, 0));
+    CK(e);
+    CK(cudaStreamSynchronize(st));
+    cudaEventDestroy(done);
+    cudaGraphExecDestroy(g);
+  } catch (...) {
+    cudaStreamSynchronize(st);
+    cudaFree(dj);
+    throw;
+  }
+  cudaFree(dj);
+}
+
 Setup::~Setup() {
   cudaStreamSynchronize(st);
   void* ptrs[] = {z, a, b, cw0, tree0, pp[0], pp[1], pp[2], pp[3], eqbuf[0], zv_pre, induce_buf, out, blocks_buf,
@@ -305,24 +403,31 @@ void Setup::mark(int phase) {
 
 // -------------------------------------------------------------- prove --
 std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
-                                  const std::string& domain) {
+                                  const std::string& domain, bool committed) {
   Proof P;
   P.m = (uint64_t)m;
   const int G = sms * 4;
   const uint32_t n_slots = 1u << n_log;
   mark(0);
-  // ---- K0 witness
-  if (seed) launch_witness_seed(*seed, log2, 1u << log2, n_slots, z, a, b, st);
-  else launch_witness_blocks(blocks_dev, (uint32_t)n_blocks, n_slots, z, a, b, st);
-  CK(cudaGetLastError());
+  if (!committed) {
+    // ---- K0 witness
+    if (seed) launch_witness_seed(*seed, log2, 1u << log2, n_slots, z, a, b, st);
+    else launch_witness_blocks(blocks_dev, (uint32_t)n_blocks, n_slots, z, a, b, st);
+    CK(cudaGetLastError());
+  }
   mark(1);
   // ---- K1 + K2 commit: 64 interleaved lanes, rate 1/2, 1 KiB leaves (two
-  // captured graphs, the phase event between them)
-  CK(cudaGraphLaunch(commit_graph[0], st));
-  count_launch(commit_launches[0]);
+  // captured graphs, the phase event between them); a batch commit
+  // (batch_commit) has already filled z, a, b, the codeword and the tree
+  if (!committed) {
+    CK(cudaGraphLaunch(commit_graph[0], st));
+    count_launch(commit_launches[0]);
+  }
   mark(2);
-  CK(cudaGraphLaunch(commit_graph[1], st));
-  count_launch(commit_launches[1]);
+  if (!committed) {
+    CK(cudaGraphLaunch(commit_graph[1], st));
+    count_launch(commit_launches[1]);
+  }
   P.root = root_of(tree0, n_leaves0);
   mark(3);
 

@@ -10,6 +10,10 @@
 namespace flock {
 
 void scatter(f128* dst, const uint64_t* pos, const f128* vals, size_t n, cudaStream_t s);
+class Setup;
+// Fused witness + commit of several seeded proofs (one graph of batched
+// launches on st); each setup's stream waits for it.
+void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds, cudaStream_t st);
 
 struct Level {
   int lanes = 0, log_msg_pos = 0, rate = 0;
@@ -29,14 +33,16 @@ class Setup {
 
   // seed != nullptr: inputs generated on the device from the benchmark
   // generator; otherwise blocks_dev holds n_blocks x 25 u32 on the device.
+  // committed: the witness, codeword and tree were filled by batch_commit
   std::vector<uint8_t> prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
-                             const std::string& domain);
+                             const std::string& domain, bool committed = false);
   void phase_times(double* ms) const;
   // device bytes a setup for 2^log2 compressions holds (an upper estimate,
   // used for admission before allocating)
   static size_t estimate_bytes(uint32_t log2);
   size_t device_bytes = 0;  // allocated by the constructor
 
+  friend void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds, cudaStream_t st);
   uint32_t log2 = 0;
   int n_log = 0, m = 0, sms = 0;
   size_t n_words = 0, n_leaves0 = 0;

@@ -2,6 +2,7 @@
 // Setup::prove on the setup's own stream.
 #include "serve.hpp"
 #include "../../include/flock_gpu.h"
+#include <atomic>
 
 namespace flock {
 
@@ -18,7 +19,96 @@ Server::~Server() {
   cv_jobs_.notify_all();
   cv_mem_.notify_all();
   for (auto& t : workers_) t.join();
+  std::lock_guard<std::mutex> bl(batch_mu_);
   idle_.clear();  // frees the cached setups
+  if (batch_st_) cudaStreamDestroy(batch_st_);
+}
+
+std::vector<JobResult> Server::prove_batch(const std::vector<BatchItem>& jobs, int threads) {
+  std::lock_guard<std::mutex> bl(batch_mu_);
+  cudaSetDevice(device_);
+  if (!batch_st_) CK(cudaStreamCreateWithFlags(&batch_st_, cudaStreamNonBlocking));
+  if (threads < 1) threads = 1;
+  auto ms = [](Clock::duration d) { return std::chrono::duration<double, std::milli>(d).count(); };
+  const auto t0 = Clock::now();
+  std::vector<JobResult> res(jobs.size());
+  size_t next = 0;
+  while (next < jobs.size()) {
+    // admit a wave: as many jobs, in order, as fit the budget now
+    std::vector<std::pair<size_t, std::unique_ptr<Setup>>> wave;
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      while (next < jobs.size()) {
+        std::unique_ptr<Setup> s;
+        try {
+          s = acquire(jobs[next].log2, lk, wave.empty());
+        } catch (const std::exception& e) {
+          res[next].status = FLOCK_ERR_CAPACITY;
+          res[next].error = e.what();
+          next++;
+          continue;
+        }
+        if (!s) break;
+        wave.emplace_back(next++, std::move(s));
+      }
+    }
+    if (wave.empty()) continue;
+    const auto t_run = Clock::now();
+    std::string commit_err;
+    std::vector<bool> committed(wave.size(), false);
+    {
+      std::vector<Setup*> ss;
+      std::vector<uint64_t> seeds;
+      for (auto& w : wave)
+        if (!jobs[w.first].blocks) {
+          ss.push_back(w.second.get());
+          seeds.push_back(jobs[w.first].seed);
+        }
+      try {
+        batch_commit(ss, seeds, batch_st_);
+        for (size_t i = 0; i < wave.size(); i++) committed[i] = !jobs[wave[i].first].blocks;
+      } catch (const std::exception& e) {
+        commit_err = e.what();
+      }
+    }
+    std::atomic<size_t> k{0};
+    auto run = [&] {
+      cudaSetDevice(device_);
+      for (size_t i; (i = k.fetch_add(1)) < wave.size();) {
+        const BatchItem& job = jobs[wave[i].first];
+        Setup& S = *wave[i].second;
+        JobResult& r = res[wave[i].first];
+        try {
+          if (!commit_err.empty() && !job.blocks) throw std::runtime_error("batch commit: " + commit_err);
+          if (job.blocks) {
+            const size_t n = (size_t)1 << job.log2;
+            if (!S.blocks_buf) CK(cudaMalloc(&S.blocks_buf, n * 25 * sizeof(uint32_t)));
+            CK(cudaMemcpyAsync(S.blocks_buf, job.blocks, n * 25 * sizeof(uint32_t), cudaMemcpyHostToDevice, S.st));
+            r.bytes = S.prove(nullptr, S.blocks_buf, n, job.domain);
+          } else {
+            r.bytes = S.prove(&job.seed, nullptr, 0, job.domain, committed[i]);
+          }
+          r.status = FLOCK_OK;
+        } catch (const CudaError& e) {
+          r.status = FLOCK_ERR_CUDA;
+          r.error = e.what();
+        } catch (const std::exception& e) {
+          r.status = FLOCK_ERR_INTERNAL;
+          r.error = e.what();
+        }
+        const auto t_end = Clock::now();
+        r.queue_ms = ms(t_run - t0);
+        r.run_ms = ms(t_end - t_run);
+        r.latency_ms = ms(t_end - t0);
+      }
+    };
+    std::vector<std::thread> th;
+    for (int t = 0; t < threads && t < (int)wave.size(); t++) th.emplace_back(run);
+    for (auto& t : th) t.join();
+    std::lock_guard<std::mutex> lk(mu_);
+    for (auto& w : wave) release(std::move(w.second));
+  }
+  return res;
 }
 
 uint64_t Server::submit(uint32_t log2, uint64_t seed, const uint32_t* blocks, const std::string& domain) {
@@ -64,7 +154,7 @@ uint64_t Server::cached_bytes() {
 }
 
 // Called with the lock held; may drop it while constructing a setup.
-std::unique_ptr<Setup> Server::acquire(uint32_t log2, std::unique_lock<std::mutex>& lk) {
+std::unique_ptr<Setup> Server::acquire(uint32_t log2, std::unique_lock<std::mutex>& lk, bool wait) {
   for (;;) {
     if (stop_) return nullptr;
     auto it = idle_.find(log2);
@@ -111,6 +201,7 @@ std::unique_ptr<Setup> Server::acquire(uint32_t log2, std::unique_lock<std::mute
     }
     if (busy_ == 0)  // nothing in flight will ever free memory for this job
       throw std::runtime_error("a 2^" + std::to_string(log2) + " proof does not fit the HBM budget");
+    if (!wait) return nullptr;
     // every byte is held by proofs in flight: wait for one to finish
     cv_mem_.wait(lk);
   }

@@ -46,6 +46,18 @@ class Server {
   // the job's proof length if finished, else 0 (leaves the result in place)
   size_t peek_len(uint64_t ticket);
 
+  // Batched form: prove `jobs` together, in waves of as many jobs as fit the
+  // HBM budget; the seeded jobs of a wave share one fused witness + commit
+  // graph (batch_commit), then the remaining phases of every proof of the
+  // wave run concurrently on `threads` host threads, one stream each.
+  struct BatchItem {
+    uint32_t log2 = 0;
+    uint64_t seed = 0;
+    const uint32_t* blocks = nullptr;  // or 2^log2 x 25 u32 on the host
+    std::string domain;
+  };
+  std::vector<JobResult> prove_batch(const std::vector<BatchItem>& jobs, int threads);
+
   int slots() const { return (int)workers_.size(); }
   uint64_t budget() const { return budget_; }
   uint64_t cached_bytes();
@@ -67,7 +79,8 @@ class Server {
   };
 
   void worker();
-  std::unique_ptr<Setup> acquire(uint32_t log2, std::unique_lock<std::mutex>& lk);
+  // wait: block until memory frees up (else return nullptr when it does not fit now)
+  std::unique_ptr<Setup> acquire(uint32_t log2, std::unique_lock<std::mutex>& lk, bool wait = true);
   void release(std::unique_ptr<Setup> s);
 
   int device_;
@@ -82,6 +95,8 @@ class Server {
   uint64_t next_ticket_ = 1, use_clock_ = 0;
   bool stop_ = false;
   std::vector<std::thread> workers_;
+  std::mutex batch_mu_;  // one batch at a time
+  cudaStream_t batch_st_ = nullptr;
 };
 
 }  // namespace flock

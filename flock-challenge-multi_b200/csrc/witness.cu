@@ -161,12 +161,12 @@ __device__ void compression_witness(const uint32_t cv[8], const uint32_t m_in[16
   flush(S, 0, 0, 8);
 }
 
-__device__ __forceinline__ Stage make_stage(uint64_t* sm, f128* z, f128* a, f128* b, uint32_t n_slots) {
+__device__ __forceinline__ Stage make_stage(uint64_t* sm, f128* z, f128* a, f128* b, uint32_t n_slots, uint32_t cta) {
   Stage S;
   S.sm = sm;
   S.lane = threadIdx.x & 31;
   S.warp = threadIdx.x >> 5;
-  const uint32_t i0 = blockIdx.x * kWThreads + S.warp * 32;
+  const uint32_t i0 = cta * kWThreads + S.warp * 32;
   S.out[0] = reinterpret_cast<uint64_t*>(z) + (size_t)i0 * 256;
   S.out[1] = reinterpret_cast<uint64_t*>(a) + (size_t)i0 * 256;
   S.out[2] = reinterpret_cast<uint64_t*>(b) + (size_t)i0 * 256;
@@ -175,12 +175,12 @@ __device__ __forceinline__ Stage make_stage(uint64_t* sm, f128* z, f128* a, f128
 }
 }  // namespace
 
-__global__ void __launch_bounds__(kWThreads, 4) k_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks,
-                                                           uint32_t n_slots, f128* __restrict__ z,
-                                                           f128* __restrict__ a, f128* __restrict__ b) {
-  extern __shared__ uint64_t wsm[];
-  const Stage S = make_stage(wsm, z, a, b, n_slots);
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+// CTA `cta` of the witness of 2^log2 seeded compressions (n_slots >= n_blocks
+// slots; padding slots hold the all-zero compression, blake3.rs:4631-4636)
+__device__ __forceinline__ void witness_seed_cta(uint64_t* sm, uint64_t seed, uint32_t log2, uint32_t n_blocks,
+                                                 uint32_t n_slots, f128* z, f128* a, f128* b, uint32_t cta) {
+  const Stage S = make_stage(sm, z, a, b, n_slots, cta);
+  uint32_t i = cta * kWThreads + threadIdx.x;
   uint32_t cv[8], m[16], ctr = 0, blen = 0, flags = 0;
   if (i < n_blocks) {
     uint64_t init = seed ^ (((uint64_t)log2 << 29) | ((uint64_t)log2 >> 35));
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kWThreads, 4) k_witness_seed(uint64_t seed, ui
     ctr = splitmix(st);
     blen = 64;
     flags = 11;
-  } else {  // padding slot: the all-zero compression (blake3.rs:4631-4636)
+  } else {
 #pragma unroll
     for (int w = 0; w < 8; w++) cv[w] = 0;
 #pragma unroll
@@ -202,13 +202,35 @@ __global__ void __launch_bounds__(kWThreads, 4) k_witness_seed(uint64_t seed, ui
   compression_witness(cv, m, ctr, 0, blen, flags, S);
 }
 
+__global__ void __launch_bounds__(kWThreads, 4) k_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks,
+                                                           uint32_t n_slots, f128* __restrict__ z,
+                                                           f128* __restrict__ a, f128* __restrict__ b) {
+  extern __shared__ uint64_t wsm[];
+  witness_seed_cta(wsm, seed, log2, n_blocks, n_slots, z, a, b, blockIdx.x);
+}
+
+// The witnesses of a batch of proofs in one launch: CTA c belongs to the job
+// j with jobs[j].wcta0 <= c < jobs[j + 1].wcta0.
+__global__ void __launch_bounds__(kWThreads, 4) k_witness_seed_batch(const BatchJob* __restrict__ jobs, int n_jobs) {
+  extern __shared__ uint64_t wsm[];
+  const uint32_t c = blockIdx.x;
+  int lo = 0, hi = n_jobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].wcta0 <= c) lo = mid;
+    else hi = mid - 1;
+  }
+  const BatchJob& J = jobs[lo];
+  witness_seed_cta(wsm, J.seed, J.log2, J.n_blocks, J.n_slots, J.z, J.a, J.b, c - (uint32_t)J.wcta0);
+}
+
 // blocks: 25 u32 per compression (cv[8], m[16], counter_lo); counter_hi = 0,
 // block_len = 64, flags = 11 as in the benchmark generator.
 __global__ void __launch_bounds__(kWThreads, 4) k_witness_blocks(const uint32_t* __restrict__ blocks, uint32_t n_blocks,
                                                              uint32_t n_slots, f128* __restrict__ z,
                                                              f128* __restrict__ a, f128* __restrict__ b) {
   extern __shared__ uint64_t wsm[];
-  const Stage S = make_stage(wsm, z, a, b, n_slots);
+  const Stage S = make_stage(wsm, z, a, b, n_slots, blockIdx.x);
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t cv[8] = {0}, m[16] = {0}, ctr = 0, blen = 0, flags = 0;
   if (i < n_blocks) {
@@ -237,4 +259,11 @@ void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n
   count_launch();
   k_witness_blocks<<<(n_slots + kWThreads - 1) / kWThreads, kWThreads, kWitnessSmem, s>>>(blocks, n_blocks, n_slots,
                                                                                        z, a, b);
+}
+
+uint32_t witness_ctas(uint32_t n_slots) { return (n_slots + kWThreads - 1) / kWThreads; }
+void launch_witness_seed_batch(const BatchJob* jobs, int n_jobs, uint32_t total_ctas, cudaStream_t s) {
+  CK(cudaFuncSetAttribute(k_witness_seed_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWitnessSmem));
+  count_launch();
+  k_witness_seed_batch<<<total_ctas, kWThreads, kWitnessSmem, s>>>(jobs, n_jobs);
 }

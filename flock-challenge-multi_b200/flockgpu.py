@@ -27,7 +27,7 @@ EXPORTS = (
     "flock_pow", "flock_f128_mul", "flock_statement_digest", "flock_bench_ntt",
     "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove", "flock_merkle_root_noalloc",
     "flock_serve_start", "flock_submit", "flock_poll", "flock_sumcheck_round3", "flock_bench_sumcheck3",
-    "flock_ntt_autotune", "flock_ntt_rs_encode_plan",
+    "flock_ntt_autotune", "flock_ntt_rs_encode_plan", "flock_prove_batch",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -88,6 +88,7 @@ def load() -> ctypes.CDLL:
         lib.flock_serve_start.argtypes = [vp, i32]
         lib.flock_submit.argtypes = [vp, ctypes.POINTER(FlockJob), ctypes.POINTER(u64)]
         lib.flock_poll.argtypes = [vp, u64, ctypes.POINTER(FlockResult), i32]
+        lib.flock_prove_batch.argtypes = [vp, ctypes.POINTER(FlockJob), sz, ctypes.POINTER(FlockResult), i32]
         _lib = lib
     return _lib
 
@@ -173,6 +174,33 @@ class Context:
             raise FlockError(f"job {ticket} failed ({res.status}): {self.lib.flock_last_error(self.h).decode()}")
         return {"bytes": buf[: res.out_len].tobytes(), "queue_ms": res.queue_ms, "run_ms": res.run_ms,
                 "latency_ms": res.latency_ms}
+
+    def prove_batch(self, jobs, threads: int = 8):
+        """Prove [(log2, seed or (2^log2, 25) u32 blocks), ...] as one batch;
+        returns a list of dicts like poll()'s."""
+        n = len(jobs)
+        keep = []
+        cj = (FlockJob * max(n, 1))()
+        bufs = [np.zeros(MAX_PROOF_BYTES * 2, np.uint8) for _ in range(n)]
+        cr = (FlockResult * max(n, 1))()
+        for i, (log2, inp) in enumerate(jobs):
+            cj[i] = FlockJob(log2, 0, None, DOMAIN, len(DOMAIN))
+            if isinstance(inp, np.ndarray):
+                blk = np.ascontiguousarray(inp, np.uint32).reshape(-1, 25)
+                keep.append(blk)
+                cj[i].blocks = blk.ctypes.data
+            else:
+                cj[i].seed = inp
+            cr[i] = FlockResult(bufs[i].ctypes.data, bufs[i].size, 0, 0, 0.0, 0.0, 0.0)
+        self._check(self.lib.flock_prove_batch(self.h, cj, n, cr, threads), "prove_batch")
+        out = []
+        for i in range(n):
+            if cr[i].status:
+                raise FlockError(f"batch job {i} failed ({cr[i].status}): "
+                                 f"{self.lib.flock_last_error(self.h).decode()}")
+            out.append({"bytes": bufs[i][: cr[i].out_len].tobytes(), "queue_ms": cr[i].queue_ms,
+                        "run_ms": cr[i].run_ms, "latency_ms": cr[i].latency_ms})
+        return out
 
     # ---- kernel-level entry points (host arrays in, host arrays out) ----
     def witness(self, log2: int, seed: int):

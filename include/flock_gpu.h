@@ -161,6 +161,21 @@ int flock_submit(flock_ctx* ctx, const flock_job* job, uint64_t* ticket);
  * result is kept for a retry). */
 int flock_poll(flock_ctx* ctx, uint64_t ticket, flock_result* res, int timeout_ms);
 
+/* Batched form of the same prove entry point: proves jobs[0..n) together and
+ * returns when all are done (results[i] as flock_poll fills it; the call
+ * returns FLOCK_ERR_CAPACITY if an output buffer was too small, otherwise
+ * FLOCK_OK with each proof's own status in results[i].status).  Jobs are
+ * admitted in order, in waves of as many as fit the context's HBM budget.
+ * The witnesses, RS encodes and Merkle trees of a wave's seeded jobs run as
+ * one CUDA graph of fused launches over all of its jobs (one persistent NTT
+ * pass kernel over the tiles of every job, one tree level of every job per
+ * launch); the remaining phases of each proof then run concurrently on
+ * `threads` host threads, one CUDA stream each.  Every result is
+ * byte-identical to flock_prove_seed / flock_prove_blocks of the same job.
+ * No counterpart in the reference, which proves one job per worker process
+ * (benchmark-tools/worker/src/main.rs). */
+int flock_prove_batch(flock_ctx* ctx, const flock_job* jobs, size_t n, flock_result* results, int threads);
+
 /* Merkle root of leaves already in device memory, for callers that may not
  * allocate device memory when they need the root (inside a stream capture,
  * fixed-memory hosts, plugins whose buffers are all owned by an outer

@@ -85,3 +85,39 @@ def test_poll_timeout_returns_none():
         assert ctx.poll(t1)["bytes"] and ctx.poll(t2)["bytes"]
     finally:
         ctx.close()
+
+
+def test_batch_matches_plain_proofs():
+    """Batched form: one fused witness + commit graph over uneven jobs, then the
+    rest of every proof concurrently; each proof equals the plain one."""
+    import flockgpu
+    jobs = [(8, 41), (12, 42), (9, 43), (10, 44), (8, 45), (11, 46), (9, 47)]
+    ctx = flockgpu.Context(0)
+    try:
+        want = _alone(ctx, jobs)
+        for threads in (1, 4):
+            got = ctx.prove_batch(jobs, threads=threads)
+            for (l, s), r in zip(jobs, got):
+                assert hashlib.sha256(r["bytes"]).hexdigest() == want[(l, s)], (l, s, threads)
+                assert r["latency_ms"] >= r["run_ms"] > 0
+    finally:
+        ctx.close()
+
+
+def test_batch_mixes_blocks_and_waves():
+    """Jobs given as host compressions take the per-proof commit inside the
+    batch; a budget that holds two small setups splits the batch into waves."""
+    import flockgpu
+    jobs = [(9, 51), (8, 52), (9, 53), (8, 54)]
+    ref = flockgpu.Context(0)
+    try:
+        want = _alone(ref, jobs)
+    finally:
+        ref.close()
+    ctx = flockgpu.Context(0, hbm_budget_bytes=230 << 20)
+    try:
+        items = [(l, flockgpu.generate_compressions(l, s)) if i % 2 else (l, s) for i, (l, s) in enumerate(jobs)]
+        got = ctx.prove_batch(items, threads=2)
+        assert [hashlib.sha256(r["bytes"]).hexdigest() for r in got] == [want[j] for j in jobs]
+    finally:
+        ctx.close()
