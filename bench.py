@@ -25,6 +25,8 @@ import tempfile
 import time
 from pathlib import Path
 
+import numpy as np
+
 REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO / "flock-challenge-multi_b200"))
 
@@ -403,9 +405,15 @@ def run_ours(args, world, rank, local):
     total_ms, phases, launches = prover.bench(seed_base, args.steps)
     clocks = sampler.stop()
     value, max_ms = aggregate(total_ms, world, log2, args.steps)
-    # end to end through the public API with host inputs: H2D of the
-    # compressions, prove, D2H of the proof bytes (all inside the timed region)
-    blocks = [host_blocks(log2, seed_base + 500 + i) for i in range(args.steps)]
+    # end to end through the public API with host inputs in pinned memory: H2D
+    # of the compressions, prove, D2H of the proof bytes (all inside the timed
+    # region)
+    pinned = []
+    for i in range(args.steps):
+        pa = flockgpu.PinnedArray((1 << log2, 25), np.uint32)
+        pa.array[:] = host_blocks(log2, seed_base + 500 + i)
+        pinned.append(pa)
+    blocks = [pa.array for pa in pinned]
     barrier(world)
     t0 = time.perf_counter()
     sizes = [len(prover.prove_blocks(b)) for b in blocks]

@@ -142,6 +142,15 @@ int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const u
   });
 }
 
+int flock_host_alloc(size_t bytes, void** out) {
+  if (!out || bytes == 0) return FLOCK_ERR_ARG;
+  *out = nullptr;
+  return cudaMallocHost(out, bytes) == cudaSuccess ? FLOCK_OK : FLOCK_ERR_CUDA;
+}
+void flock_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
 int flock_serve_start(flock_ctx* c, int slots) {
   if (!c || slots < 1 || slots > 64) return FLOCK_ERR_ARG;
   return guard(c, [&] {

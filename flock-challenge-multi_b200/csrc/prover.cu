@@ -13,6 +13,8 @@
 #include "prover.hpp"
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
+#include <cstring>
 #include <set>
 
 namespace flock {
@@ -167,7 +169,12 @@ cudaGraphExec_t capture(cudaStream_t st, uint64_t* launches, F&& body) {
 }
 }  // namespace
 
+// FLOCK_COMMIT_GRAPHS=0 launches the same kernels directly (for profilers
+// that replay kernels one at a time: ncu's replay of these graph nodes failed
+// to launch on this driver).
 void Setup::capture_commit() {
+  const char* env = getenv("FLOCK_COMMIT_GRAPHS");
+  if (env && strcmp(env, "0") == 0) return;
   commit_graph[0] = capture(st, &commit_launches[0], [&] { ntt_rs_encode(z, cw0, m - 13, 64, 1, st); });
   commit_graph[1] = capture(st, &commit_launches[1], [&] { merkle_build(cw0, n_leaves0, 64 * 16, tree0, st); });
 }
@@ -353,18 +360,13 @@ std::vector<size_t> Setup::sample_queries(Transcript& tr, size_t block_len, size
   return q;
 }
 
-// Opened rows + Merkle multi-proof (merkle.rs:1074-1120 index order).
+// Opened rows + Merkle multi-proof (merkle.rs:1074-1120 index order).  The
+// sibling indices depend only on the queries, so both gathers are issued
+// together and read back with one synchronisation.
 Opening Setup::open(const f128* cw, const uint32_t* tree, size_t n_leaves, int lanes, const std::vector<size_t>& q) {
   Opening o;
-  std::vector<uint64_t> pos(q.begin(), q.end());
-  CK(cudaMemcpyAsync(idx, pos.data(), pos.size() * 8, cudaMemcpyHostToDevice, st));
-  size_t nr = q.size() * lanes;
-  count_launch(); k_gather_rows<<<(unsigned)((nr + 255) / 256), 256, 0, st>>>(cw, idx, q.size(), lanes, gather);
-  std::vector<f128> rows(nr);
-  fetch(gather, nr, rows.data());
-  for (size_t i = 0; i < q.size(); i++) o.rows.emplace_back(rows.begin() + i * lanes, rows.begin() + (i + 1) * lanes);
-  // sibling indices of the multi-proof
-  std::vector<uint64_t> sib;
+  std::vector<uint64_t> ids(q.begin(), q.end());
+  // sibling indices of the multi-proof, after the query positions
   std::vector<size_t> act(q);
   size_t ls = 0, ll = n_leaves;
   while (ll > 1) {
@@ -372,21 +374,28 @@ Opening Setup::open(const f128* cw, const uint32_t* tree, size_t n_leaves, int l
     while (i < act.size()) {
       size_t p = act[i];
       if (i + 1 < act.size() && act[i + 1] == (p ^ 1)) i += 2;
-      else { sib.push_back(ls + (p ^ 1)); i += 1; }
+      else { ids.push_back(ls + (p ^ 1)); i += 1; }
       act[w++] = p >> 1;
     }
     act.resize(w);
     ls += ll;
     ll >>= 1;
   }
-  if (!sib.empty()) {
-    CK(cudaMemcpyAsync(idx, sib.data(), sib.size() * 8, cudaMemcpyHostToDevice, st));
-    count_launch(); k_gather_nodes<<<(unsigned)((sib.size() + 127) / 128), 128, 0, st>>>(tree, idx, sib.size(),
-                                                                         reinterpret_cast<uint32_t*>(gather));
-    o.proof.resize(sib.size());
-    CK(cudaMemcpyAsync(o.proof.data(), gather, sib.size() * 32, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+  const size_t nq = q.size(), ns = ids.size() - nq, nr = nq * lanes;
+  if (ids.size() > ((size_t)1 << 16) || nr + 2 * ns > ((size_t)1 << 16))
+    throw std::runtime_error("opening larger than the gather buffers");
+  CK(cudaMemcpyAsync(idx, ids.data(), ids.size() * 8, cudaMemcpyHostToDevice, st));
+  count_launch(); k_gather_rows<<<(unsigned)((nr + 255) / 256), 256, 0, st>>>(cw, idx, nq, lanes, gather);
+  uint32_t* nodes = reinterpret_cast<uint32_t*>(gather + nr);  // 32 B per node = 2 f128
+  if (ns) {
+    count_launch(); k_gather_nodes<<<(unsigned)((ns + 127) / 128), 128, 0, st>>>(tree, idx + nq, ns, nodes);
   }
+  std::vector<f128> rows(nr);
+  o.proof.resize(ns);
+  CK(cudaMemcpyAsync(rows.data(), gather, nr * sizeof(f128), cudaMemcpyDeviceToHost, st));
+  if (ns) CK(cudaMemcpyAsync(o.proof.data(), nodes, ns * 32, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < nq; i++) o.rows.emplace_back(rows.begin() + i * lanes, rows.begin() + (i + 1) * lanes);
   return o;
 }
 
@@ -402,6 +411,10 @@ void Setup::mark(int phase) {
 }
 
 // -------------------------------------------------------------- prove --
+// Host buffers handed to cudaMemcpyAsync here are either pinned (h_out,
+// h_found, h_stage) and read only after a synchronisation, or pageable, which
+// the runtime stages before the call returns: the stream needs no
+// synchronisation except where the transcript reads a device value.
 std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
                                   const std::string& domain, bool committed) {
   Proof P;
@@ -420,13 +433,21 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   // captured graphs, the phase event between them); a batch commit
   // (batch_commit) has already filled z, a, b, the codeword and the tree
   if (!committed) {
-    CK(cudaGraphLaunch(commit_graph[0], st));
-    count_launch(commit_launches[0]);
+    if (commit_graph[0]) {
+      CK(cudaGraphLaunch(commit_graph[0], st));
+      count_launch(commit_launches[0]);
+    } else {
+      ntt_rs_encode(z, cw0, m - 13, 64, 1, st);
+    }
   }
   mark(2);
   if (!committed) {
-    CK(cudaGraphLaunch(commit_graph[1], st));
-    count_launch(commit_launches[1]);
+    if (commit_graph[1]) {
+      CK(cudaGraphLaunch(commit_graph[1], st));
+      count_launch(commit_launches[1]);
+    } else {
+      merkle_build(cw0, n_leaves0, 64 * 16, tree0, st);
+    }
   }
   P.root = root_of(tree0, n_leaves0);
   mark(3);
@@ -501,7 +522,6 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     f128 ce = mk(0, 0);
     for (int i = 0; i < 64; i++) ce = fx(ce, hmul(LL[i], P.r1_c[i]));
     P.fc = ce;
-    CK(cudaStreamSynchronize(st));
   }
   const int n_mlv = m - 6;
   std::vector<f128> rhos;
@@ -602,7 +622,6 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     lc_zvec(z, scratch_eq(), (size_t)1 << (m - kKLog), zv, st);
     // pre-sumcheck z_vec: the ab-claim's ring-switch statistic is read from it
     CK(cudaMemcpyAsync(zv_pre, zv, kK * sizeof(f128), cudaMemcpyDeviceToDevice, st));
-    CK(cudaStreamSynchronize(st));
   }
   std::vector<f128> rr;
   int len = kK;
@@ -675,9 +694,13 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
         }
     }
     CK(cudaMemcpyAsync(bc_tabs, T.data(), T.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
-    // eq(suffix_k, i) = lo_k(i mod 2^12) * hi_k(i >> 12), both tables on the device
-    int lo_bits = (int)std::min<size_t>(x_ab.size() - 1, 12);
-    const int hi_bits = (int)x_ab.size() - 1 - lo_bits;
+    // eq(suffix_k, i) = lo_k(i mod 2^lo_bits) * hi_k(i >> lo_bits), both tables
+    // on the device; chunks of up to 2^14 values (each CTA builds its two
+    // product tables once per chunk), as long as the four tables fit eqbuf
+    const int n_vars = (int)x_ab.size() - 1;
+    int lo_bits = std::min(n_vars, 14);
+    while (lo_bits > 0 && 2 * ((1ull << lo_bits) + (1ull << (n_vars - lo_bits))) > n_words) lo_bits--;
+    const int hi_bits = n_vars - lo_bits;
     f128* d = eqbuf[0];  // [lo0 | hi0 | lo1 | hi1]
     const size_t nlo = (size_t)1 << lo_bits, nhi = (size_t)1 << hi_bits;
     for (int k = 0; k < 2; k++) {
@@ -688,7 +711,6 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     }
     ring_bcombined_ct(d, d + nlo, d + nlo + nhi, d + 2 * nlo + nhi, bc_tabs, bc_tabs + 4096, lo_bits, nhi, pp[1],
                       sms, st);
-    CK(cudaStreamSynchronize(st));
   }
   mark(7);
 
@@ -759,7 +781,6 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     scatter(induce_buf, idx, gather, q.size(), st);
     f128* bind = scratch_eq();
     ntt_transposed_encode(induce_buf, bind, n_cur, rate, st);
-    CK(cudaStreamSynchronize(st));
     introduce(bind);
   };
 

@@ -27,7 +27,8 @@ EXPORTS = (
     "flock_pow", "flock_f128_mul", "flock_statement_digest", "flock_bench_ntt",
     "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove", "flock_merkle_root_noalloc",
     "flock_serve_start", "flock_submit", "flock_poll", "flock_sumcheck_round3", "flock_bench_sumcheck3",
-    "flock_ntt_autotune", "flock_ntt_rs_encode_plan", "flock_prove_batch",
+    "flock_ntt_autotune", "flock_ntt_rs_encode_plan", "flock_prove_batch", "flock_host_alloc",
+    "flock_host_free",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -88,6 +89,8 @@ def load() -> ctypes.CDLL:
         lib.flock_serve_start.argtypes = [vp, i32]
         lib.flock_submit.argtypes = [vp, ctypes.POINTER(FlockJob), ctypes.POINTER(u64)]
         lib.flock_poll.argtypes = [vp, u64, ctypes.POINTER(FlockResult), i32]
+        lib.flock_host_alloc.argtypes = [sz, ctypes.POINTER(vp)]
+        lib.flock_host_free.argtypes = [vp]
         lib.flock_prove_batch.argtypes = [vp, ctypes.POINTER(FlockJob), sz, ctypes.POINTER(FlockResult), i32]
         _lib = lib
     return _lib
@@ -111,6 +114,26 @@ def generate_compressions(log2: int, seed: int) -> np.ndarray:
         z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         z = z ^ (z >> np.uint64(31))
     return z.astype(np.uint32).reshape(-1, 25)
+
+
+class PinnedArray:
+    """A numpy array over page-locked host memory (flock_host_alloc); the
+    memory is freed when this object is."""
+
+    def __init__(self, shape, dtype):
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        p = ctypes.c_void_p()
+        if load().flock_host_alloc(n, ctypes.byref(p)):
+            raise FlockError("flock_host_alloc failed")
+        self._p = p
+        buf = (ctypes.c_uint8 * n).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            self.array = None
+            load().flock_host_free(self._p)
+            self._p = None
 
 
 def statement_digest(m: int) -> bytes:

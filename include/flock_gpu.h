@@ -70,6 +70,12 @@ int flock_prove_seed(flock_setup* s, uint64_t seed, const uint8_t* domain, size_
  * block_len 64, flags 11, n == 2^log2_n. */
 int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const uint8_t* domain, size_t dlen,
                        uint8_t* out, size_t cap, size_t* out_len);
+/* Page-locked host memory for inputs and outputs: flock_prove_blocks copies
+ * compressions from such a buffer at the full host-to-device rate (a
+ * pageable buffer is staged by the CUDA runtime first).  No counterpart in
+ * the reference, whose prover reads host memory directly. */
+int flock_host_alloc(size_t bytes, void** out);
+void flock_host_free(void* p);
 /* Device milliseconds of the last proof's phases (witness, RS encode, Merkle
  * commit, zerocheck round 1, zerocheck rounds, lincheck, ring switch +
  * combine, Ligerito L0 folds, Ligerito levels).  Returns the number written. */

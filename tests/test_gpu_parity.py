@@ -167,6 +167,13 @@ def test_prove_blocks_equals_prove_seed(prover8, oracle):
     assert prover8.prove_blocks(blocks) == prover8.prove_seed(77)
 
 
+def test_prove_blocks_from_pinned_memory(prover8):
+    import flockgpu
+    pa = flockgpu.PinnedArray((1 << 8, 25), np.uint32)
+    pa.array[:] = flockgpu.generate_compressions(8, 78)
+    assert prover8.prove_blocks(pa.array) == prover8.prove_seed(78)
+
+
 @pytest.mark.parametrize("log2", [9, 10, 12])
 def test_proof_matches_oracle_larger(gpu_ctx, oracle, log2):
     import flockgpu
