@@ -6,6 +6,8 @@
 // 1,2,4,...,128 (verbatim table entries 1,2,4,...,128) and expanded by
 // linearity; tests pin the expansion against all 256 reference entries.
 #include "flockref.hpp"
+#include <cstdlib>
+#include <thread>
 #if defined(__PCLMUL__)
 #include <wmmintrin.h>
 #include <emmintrin.h>
@@ -116,5 +118,29 @@ static const std::array<F128, 256> PHI8 = make_phi8();
 
 F128 phi8(uint8_t v) { return PHI8[v]; }
 const F128* phi8_table() { return PHI8.data(); }
+
+
+int par_threads() {
+  static const int n = [] {
+    const char* e = std::getenv("FLOCKREF_THREADS");
+    int v = e ? std::atoi(e) : 1;
+    return v < 1 ? 1 : v > 256 ? 256 : v;
+  }();
+  return n;
+}
+
+void par_for(size_t n, const std::function<void(size_t, size_t, int)>& f) {
+  const int t = par_threads();
+  if (t == 1 || n < 2) {
+    f(0, n, 0);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int i = 0; i < t; i++) {
+    const size_t b = n * i / t, e = n * (i + 1) / t;
+    th.emplace_back([&f, b, e, i] { f(b, e, i); });
+  }
+  for (auto& x : th) x.join();
+}
 
 }  // namespace flockref

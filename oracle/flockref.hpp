@@ -21,8 +21,16 @@
 #include <string>
 #include <vector>
 #include <array>
+#include <functional>
 
 namespace flockref {
+
+// Parallel loops: FLOCKREF_THREADS host threads (default 1, the
+// single-threaded restatement that the CPU baseline times).  Field sums are
+// XORs, so a reduction's result does not depend on how a range is split.
+int par_threads();
+// f(begin, end, slice) over par_threads() contiguous slices of [0, n)
+void par_for(size_t n, const std::function<void(size_t, size_t, int)>& f);
 
 // ---------------------------------------------------------------------------
 // GF(2^128), GHASH polynomial x^128 + x^7 + x^2 + x + 1, lo = x^0..63.

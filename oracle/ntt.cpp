@@ -48,11 +48,13 @@ void AdditiveNtt::forward_interleaved(std::vector<F128>& data, size_t num_ntts, 
   for (int layer = start_layer; layer < log_d; layer++) {
     size_t num_blocks = (size_t)1 << layer;
     size_t half = (size_t)1 << (log_d - layer - 1);
-#pragma omp parallel for schedule(static) if (num_blocks * half * num_ntts > 4096)
-    for (long long blk = 0; blk < (long long)num_blocks; blk++) {
-      F128 t = twiddle(layer, (size_t)blk);
-      size_t start = (size_t)blk * 2 * half * num_ntts;
-      for (size_t row = 0; row < half; row++) {
+    par_for(num_blocks * half, [&](size_t i0, size_t i1, int) {
+      size_t blk_t = ~(size_t)0;
+      F128 t;
+      for (size_t i = i0; i < i1; i++) {
+        const size_t blk = i / half, row = i % half;
+        if (blk != blk_t) { t = twiddle(layer, blk); blk_t = blk; }
+        size_t start = blk * 2 * half * num_ntts;
         size_t top = start + row * num_ntts, bot = top + half * num_ntts;
         for (size_t lane = 0; lane < num_ntts; lane++) {
           F128 v = data[bot + lane];
@@ -61,7 +63,7 @@ void AdditiveNtt::forward_interleaved(std::vector<F128>& data, size_t num_ntts, 
           data[bot + lane] = v + u;
         }
       }
-    }
+    });
   }
 }
 
@@ -136,14 +138,16 @@ void Gf8Ntt::inverse(uint8_t* v) const { ifft_rec(v, (size_t)1 << k, tw.data(), 
 // ---- Merkle ----
 std::vector<Hash> merkle_tree(const uint8_t* data, size_t n_leaves, size_t leaf_size) {
   std::vector<Hash> tree(2 * n_leaves - 1);
-#pragma omp parallel for schedule(static)
-  for (long long i = 0; i < (long long)n_leaves; i++) b3::leaf_cv(data + (size_t)i * leaf_size, leaf_size, tree[i].data());
+  par_for(n_leaves, [&](size_t i0, size_t i1, int) {
+    for (size_t i = i0; i < i1; i++) b3::leaf_cv(data + i * leaf_size, leaf_size, tree[i].data());
+  });
   size_t rs = 0, rl = n_leaves;
   while (rl > 1) {
     size_t nl = rl >> 1;
-#pragma omp parallel for schedule(static) if (nl > 1024)
-    for (long long j = 0; j < (long long)nl; j++)
-      b3::parent_cv(tree[rs + 2 * j].data(), tree[rs + 2 * j + 1].data(), tree[rs + rl + j].data());
+    par_for(nl, [&](size_t j0, size_t j1, int) {
+      for (size_t j = j0; j < j1; j++)
+        b3::parent_cv(tree[rs + 2 * j].data(), tree[rs + 2 * j + 1].data(), tree[rs + rl + j].data());
+    });
     rs += rl;
     rl = nl;
   }

@@ -184,11 +184,11 @@ static ZerocheckProof zerocheck_prove(const std::vector<F128>& a, const std::vec
   auto tabs = lde_byte_tables();
   // S[l][k] = sum over rows whose extended GF(2^8) value at lambda_l has bit k.
   std::vector<F128> sab(64 * 8, ZERO), sc(64 * 8, ZERO);
-#pragma omp parallel
-  {
-    std::vector<F128> lab(64 * 8, ZERO), lc(64 * 8, ZERO);
-#pragma omp for schedule(static)
-    for (long long x = 0; x < (long long)n_rows; x++) {
+  std::vector<std::vector<F128>> plab(par_threads(), std::vector<F128>(512, ZERO)), plc = plab;
+  par_for(n_rows, [&](size_t x0, size_t x1, int ti) {
+    std::vector<F128>& lab = plab[ti];
+    std::vector<F128>& lc = plc[ti];
+    for (size_t x = x0; x < x1; x++) {
       const F128& wa = a[x >> 1];
       const F128& wb = b[x >> 1];
       const F128& wc = c[x >> 1];
@@ -206,9 +206,9 @@ static ZerocheckProof zerocheck_prove(const std::vector<F128>& a, const std::vec
         }
       }
     }
-#pragma omp critical
-    for (int i = 0; i < 512; i++) { sab[i] += lab[i]; sc[i] += lc[i]; }
-  }
+  });
+  for (size_t ti = 0; ti < plab.size(); ti++)
+    for (int i = 0; i < 512; i++) { sab[i] += plab[ti][i]; sc[i] += plc[ti][i]; }
   pf.round1_ab.assign(64, ZERO);
   pf.round1_c.assign(64, ZERO);
   for (int l = 0; l < 64; l++)
@@ -223,19 +223,20 @@ static ZerocheckProof zerocheck_prove(const std::vector<F128>& a, const std::vec
   // fold a, b at z over the skip variables: hat(x) = sum_s L_s(z) bit(s, x)
   std::vector<F128> L = lagrange_weights(K_SKIP, z, 0);
   std::vector<F128> fa(n_rows), fb(n_rows);
-#pragma omp parallel for schedule(static)
-  for (long long x = 0; x < (long long)n_rows; x++) {
-    const F128& wa = a[x >> 1];
-    const F128& wb = b[x >> 1];
-    uint64_t ra = (x & 1) ? wa.hi : wa.lo, rb = (x & 1) ? wb.hi : wb.lo;
-    F128 sa = ZERO, sb = ZERO;
-    for (int s = 0; s < 64; s++) {
-      if ((ra >> s) & 1) sa += L[s];
-      if ((rb >> s) & 1) sb += L[s];
+  par_for(n_rows, [&](size_t x0, size_t x1, int) {
+    for (size_t x = x0; x < x1; x++) {
+      const F128& wa = a[x >> 1];
+      const F128& wb = b[x >> 1];
+      uint64_t ra = (x & 1) ? wa.hi : wa.lo, rb = (x & 1) ? wb.hi : wb.lo;
+      F128 sa = ZERO, sb = ZERO;
+      for (int s = 0; s < 64; s++) {
+        if ((ra >> s) & 1) sa += L[s];
+        if ((rb >> s) & 1) sb += L[s];
+      }
+      fa[x] = sa;
+      fb[x] = sb;
     }
-    fa[x] = sa;
-    fb[x] = sb;
-  }
+  });
   F128 c_eval = interpolate_on_lambda(pf.round1_c, z);
 
   int n_mlv = m - K_SKIP;
@@ -245,29 +246,30 @@ static ZerocheckProof zerocheck_prove(const std::vector<F128>& a, const std::vec
     std::vector<F128> e = build_eq(rem);
     size_t half = fa.size() / 2;
     F128 g1 = ZERO, ginf = ZERO;
-#pragma omp parallel
-    {
+    std::vector<F128> p1(par_threads(), ZERO), pinf(par_threads(), ZERO);
+    par_for(half, [&](size_t j0, size_t j1, int ti) {
       F128 l1 = ZERO, linf = ZERO;
-#pragma omp for schedule(static)
-      for (long long j = 0; j < (long long)half; j++) {
+      for (size_t j = j0; j < j1; j++) {
         F128 a0 = fa[2 * j], a1 = fa[2 * j + 1], b0 = fb[2 * j], b1 = fb[2 * j + 1];
         l1 += e[j] * (a1 * b1);
         linf += e[j] * ((a0 + a1) * (b0 + b1));
       }
-#pragma omp critical
-      { g1 += l1; ginf += linf; }
-    }
+      p1[ti] = l1;
+      pinf[ti] = linf;
+    });
+    for (size_t ti = 0; ti < p1.size(); ti++) { g1 += p1[ti]; ginf += pinf[ti]; }
     pf.rounds.push_back({g1, ginf});
     ch.observe_f128(g1);
     ch.observe_f128(ginf);
     F128 rho = ch.sample_f128();
     rhos.push_back(rho);
     std::vector<F128> na(half), nb(half);
-#pragma omp parallel for schedule(static) if (half > 4096)
-    for (long long j = 0; j < (long long)half; j++) {
-      na[j] = fa[2 * j] + rho * (fa[2 * j] + fa[2 * j + 1]);
-      nb[j] = fb[2 * j] + rho * (fb[2 * j] + fb[2 * j + 1]);
-    }
+    par_for(half, [&](size_t j0, size_t j1, int) {
+      for (size_t j = j0; j < j1; j++) {
+        na[j] = fa[2 * j] + rho * (fa[2 * j] + fa[2 * j + 1]);
+        nb[j] = fb[2 * j] + rho * (fb[2 * j] + fb[2 * j + 1]);
+      }
+    });
     fa.swap(na);
     fb.swap(nb);
   }
@@ -314,13 +316,14 @@ static LincheckProof lincheck_prove(const std::vector<F128>& zp, int m, const R1
   std::vector<F128> eqo = build_eq(x_outer);
   std::vector<F128> zv(K, ZERO);
   size_t n_outer = eqo.size();
-#pragma omp parallel for schedule(static)
-  for (int cidx = 0; cidx < K; cidx++) {
-    F128 acc = ZERO;
-    for (size_t o = 0; o < n_outer; o++)
-      if (bit_of(zp, (size_t)cidx + ((size_t)o << K_LOG))) acc += eqo[o];
-    zv[cidx] = acc;
-  }
+  par_for(K, [&](size_t c0, size_t c1, int) {
+    for (size_t cidx = c0; cidx < c1; cidx++) {
+      F128 acc = ZERO;
+      for (size_t o = 0; o < n_outer; o++)
+        if (bit_of(zp, cidx + (o << K_LOG))) acc += eqo[o];
+      zv[cidx] = acc;
+    }
+  });
   std::vector<F128> rr;
   for (int round = 0; round < K_LOG - K_SKIP; round++) {
     size_t half = comb.size() / 2;
@@ -359,18 +362,18 @@ static LincheckProof lincheck_prove(const std::vector<F128>& zp, int m, const R1
 static void round_msg(const std::vector<F128>& f, const std::vector<F128>& b, SumcheckMsg& msg) {
   size_t half = f.size() / 2;
   F128 u0 = ZERO, u2 = ZERO;
-#pragma omp parallel
-  {
+  std::vector<F128> p0(par_threads(), ZERO), p2(par_threads(), ZERO);
+  par_for(half, [&](size_t j0, size_t j1, int ti) {
     F128 l0 = ZERO, l2 = ZERO;
-#pragma omp for schedule(static)
-    for (long long j = 0; j < (long long)half; j++) {
+    for (size_t j = j0; j < j1; j++) {
       F128 f0 = f[2 * j], f1 = f[2 * j + 1], b0 = b[2 * j], b1 = b[2 * j + 1];
       l0 += f0 * b0;
       l2 += (f0 + f1) * (b0 + b1);
     }
-#pragma omp critical
-    { u0 += l0; u2 += l2; }
-  }
+    p0[ti] = l0;
+    p2[ti] = l2;
+  });
+  for (size_t ti = 0; ti < p0.size(); ti++) { u0 += p0[ti]; u2 += p2[ti]; }
   msg.u0 = u0;
   msg.u2 = u2;
 }
@@ -378,8 +381,9 @@ static void round_msg(const std::vector<F128>& f, const std::vector<F128>& b, Su
 static void fold_lsb(std::vector<F128>& v, F128 r) {
   size_t half = v.size() / 2;
   std::vector<F128> n(half);
-#pragma omp parallel for schedule(static) if (half > 4096)
-  for (long long j = 0; j < (long long)half; j++) n[j] = v[2 * j] + r * (v[2 * j] + v[2 * j + 1]);
+  par_for(half, [&](size_t j0, size_t j1, int) {
+    for (size_t j = j0; j < j1; j++) n[j] = v[2 * j] + r * (v[2 * j] + v[2 * j + 1]);
+  });
   v.swap(n);
 }
 
@@ -564,19 +568,18 @@ static void ring_switch(const std::vector<F128>& zp, const std::vector<F128>& x_
   std::vector<F128> suffix(x_full.begin() + 1, x_full.end());
   std::vector<F128> eqs = build_eq(suffix);
   s_hat_v.assign(128, ZERO);
-#pragma omp parallel
-  {
-    std::vector<F128> loc(128, ZERO);
-#pragma omp for schedule(static)
-    for (long long i = 0; i < (long long)zp.size(); i++) {
+  std::vector<std::vector<F128>> ploc(par_threads(), std::vector<F128>(128, ZERO));
+  par_for(zp.size(), [&](size_t i0, size_t i1, int ti) {
+    std::vector<F128>& loc = ploc[ti];
+    for (size_t i = i0; i < i1; i++) {
       for (int r = 0; r < 64; r++) {
         if ((zp[i].lo >> r) & 1) loc[r] += eqs[i];
         if ((zp[i].hi >> r) & 1) loc[64 + r] += eqs[i];
       }
     }
-#pragma omp critical
+  });
+  for (auto& loc : ploc)
     for (int r = 0; r < 128; r++) s_hat_v[r] += loc[r];
-  }
   ch.observe_f128_slice(s_hat_v);
   std::vector<F128> rdp = ch.sample_f128_vec(7);
   std::vector<F128> eqd = build_eq(rdp);
@@ -593,15 +596,16 @@ static void ring_switch(const std::vector<F128>& zp, const std::vector<F128>& x_
   claim = ZERO;
   for (int bb = 0; bb < 128; bb++) claim += u[bb] * eqd[bb];
   rs_eq_ind.assign(eqs.size(), ZERO);
-#pragma omp parallel for schedule(static)
-  for (long long i = 0; i < (long long)eqs.size(); i++) {
-    F128 acc = ZERO;
-    for (int bb = 0; bb < 64; bb++) {
-      if ((eqs[i].lo >> bb) & 1) acc += eqd[bb];
-      if ((eqs[i].hi >> bb) & 1) acc += eqd[64 + bb];
+  par_for(eqs.size(), [&](size_t i0, size_t i1, int) {
+    for (size_t i = i0; i < i1; i++) {
+      F128 acc = ZERO;
+      for (int bb = 0; bb < 64; bb++) {
+        if ((eqs[i].lo >> bb) & 1) acc += eqd[bb];
+        if ((eqs[i].hi >> bb) & 1) acc += eqd[64 + bb];
+      }
+      rs_eq_ind[i] = acc;
     }
-    rs_eq_ind[i] = acc;
-  }
+  });
 }
 
 // --------------------------------------------------------------------------
@@ -744,8 +748,9 @@ Bundle prove(const std::vector<Compression>& blocks, int n_log, const std::strin
   F128 g0 = ch.sample_f128(), g1 = ch.sample_f128();
   F128 target = g0 * c0 + g1 * c1;
   std::vector<F128> bc(rs0.size());
-#pragma omp parallel for schedule(static)
-  for (long long i = 0; i < (long long)bc.size(); i++) bc[i] = g0 * rs0[i] + g1 * rs1[i];
+  par_for(bc.size(), [&](size_t i0, size_t i1, int) {
+    for (size_t i = i0; i < i1; i++) bc[i] = g0 * rs0[i] + g1 * rs1[i];
+  });
   bd.lig = ligerito_prove(cfg, z, bc, target, l0, ch);
   return bd;
 }

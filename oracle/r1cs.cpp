@@ -342,11 +342,12 @@ void generate_witness(const std::vector<Compression>& blocks, int n_log,
   b.assign(n_total * per, ZERO);
   // padding slots hold the all-zero compression (blake3.rs:4631-4636)
   Compression pad{};
-#pragma omp parallel for schedule(static)
-  for (long long o = 0; o < (long long)n_total; o++) {
-    const Compression& c = (size_t)o < blocks.size() ? blocks[o] : pad;
-    block_witness(c, (uint64_t*)&z[o * per], (uint64_t*)&a[o * per], (uint64_t*)&b[o * per]);
-  }
+  par_for(n_total, [&](size_t o0, size_t o1, int) {
+    for (size_t o = o0; o < o1; o++) {
+      const Compression& c = o < blocks.size() ? blocks[o] : pad;
+      block_witness(c, (uint64_t*)&z[o * per], (uint64_t*)&a[o * per], (uint64_t*)&b[o * per]);
+    }
+  });
 }
 
 void apply_block_diag(const SparseRows& m0, const std::vector<F128>& z, int n_blocks,

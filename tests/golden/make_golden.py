@@ -12,8 +12,12 @@
 3. witness_digests.json — sha256 of the oracle's packed (z, a, b) for small
    cases, so the device witness kernel is pinned without the oracle.
 
+4. verified_proofs_large.json (--large) — the same for 2^14, 2^16 and 2^18
+   compressions (one trial each), so the GPU prover is pinned at the
+   benchmark's full size.
+
 Usage (needs the reference checkout and a built oracle):
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py /root/reference [--large]
 """
 import hashlib
 import json
@@ -35,7 +39,8 @@ def phi8(ref: Path) -> None:
     (HERE / "phi8_table.json").write_text(json.dumps([[lo, hi] for lo, hi in vals]))
 
 
-def verified_proofs(ref: Path) -> None:
+def verified_proofs(ref: Path, sizes=((8, 3), (9, 2), (10, 2)), name="verified_proofs.json",
+                    threads=1) -> None:
     verifier = ref / "benchmark-tools/trusted/flock_benchmark_verifier"
     worker = REPO / "oracle/_build/flockref_worker"
     out = []
@@ -44,13 +49,16 @@ def verified_proofs(ref: Path) -> None:
         rec = td / "rec"
         rec.mkdir()
         wrapper = td / "worker.sh"
-        wrapper.write_text(f'#!/bin/sh\nexec "{worker}" "$@" "{rec}"\n')
+        # the harness passes the worker no environment of ours: the wrapper
+        # sets the oracle's thread count
+        wrapper.write_text(f'#!/bin/sh\nFLOCKREF_THREADS={threads} exec "{worker}" "$@" "{rec}"\n')
         wrapper.chmod(0o755)
-        for log2, runs in ((8, 3), (9, 2), (10, 2)):
+        for log2, runs in sizes:
             scratch = td / f"s{log2}"
             score = td / f"score{log2}.json"
             r = subprocess.run([str(verifier), str(wrapper), str(scratch), str(score), str(td / f"sum{log2}.md"),
-                                str(log2), "1", "0", str(runs)], capture_output=True, text=True, timeout=1800)
+                                str(log2), str(threads), "0", str(runs)], capture_output=True, text=True,
+                               timeout=3600)
             assert r.returncode == 0, r.stderr
             metrics = json.loads(score.read_text())["metrics"]
             assert metrics["verified"] is True and metrics["measured_runs"] == runs
@@ -59,7 +67,9 @@ def verified_proofs(ref: Path) -> None:
                 data = p.read_bytes()
                 out.append({"log2": log2, "seed": seed, "sha256": hashlib.sha256(data).hexdigest(),
                             "size": len(data), "verified_by": "reference trusted verifier"})
-    (HERE / "verified_proofs.json").write_text(json.dumps(out, indent=1))
+            for p in rec.glob(f"proof_{log2}_*.bin"):
+                p.unlink()
+            (HERE / name).write_text(json.dumps(out, indent=1))  # after every size
 
 
 def witness_digests() -> None:
@@ -79,6 +89,11 @@ def witness_digests() -> None:
 
 if __name__ == "__main__":
     ref = Path(sys.argv[1])
-    phi8(ref)
-    witness_digests()
-    verified_proofs(ref)
+    if "--large" in sys.argv:
+        # full-size cases (the benchmark's 2^18 among them), one trial each:
+        # the single-threaded oracle takes minutes per proof
+        verified_proofs(ref, sizes=((14, 1), (16, 1), (18, 1)), name="verified_proofs_large.json", threads=8)
+    else:
+        phi8(ref)
+        witness_digests()
+        verified_proofs(ref)

@@ -201,6 +201,22 @@ def test_golden_larger(gpu_ctx):
             p.close()
 
 
+@pytest.mark.parametrize("log2", [14, 16, 18])
+def test_golden_full_size(gpu_ctx, log2):
+    """Bit-identity at the benchmark's full size: oracle proofs of 2^14, 2^16
+    and 2^18 compressions that the reference's trusted verifier accepted."""
+    import flockgpu
+    rows = [r for r in json.loads((GOLD / "verified_proofs_large.json").read_text()) if r["log2"] == log2]
+    assert rows
+    p = flockgpu.Prover(gpu_ctx, log2)
+    try:
+        for r in rows:
+            proof = p.prove_seed(r["seed"])
+            assert len(proof) == r["size"] and hashlib.sha256(proof).hexdigest() == r["sha256"]
+    finally:
+        p.close()
+
+
 def test_phase_times_reported(prover8):
     prover8.prove_seed(5)
     ph = prover8.phase_ms()
