@@ -625,6 +625,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   }
   std::vector<f128> rr;
   int len = kK;
+  // the round kernel adds its message atomically: clear it before each round
+  CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
   lc_round(comb, zv, len, false, mk(0, 0), true, out, st);
   for (int k = 0; k < ir; k++) {
     fetch(out, 2, h_out);
@@ -634,6 +636,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     f128 rk = tr.sample();
     rr.push_back(rk);
     len >>= 1;
+    if (k + 1 < ir) CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
     lc_round(comb, zv, len, true, rk, k + 1 < ir, out, st);
   }
   P.z_partial.resize(64);

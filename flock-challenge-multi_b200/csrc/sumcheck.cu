@@ -26,6 +26,7 @@
 //  K8 Ligerito:         round messages u0 = sum f0 b0, u2 = sum (f0+f1)(b0+b1) and
 //                       LSB folds (pcs/ligerito.rs:4923-5020, 8894-9100).
 #include "kernels.cuh"
+#include <algorithm>
 
 namespace {
 __device__ __forceinline__ void block_xor_out(f128 v, f128* out) {
@@ -209,37 +210,39 @@ __global__ void __launch_bounds__(256) k_lc_zvec(const uint16_t* __restrict__ z,
   for (int p = 0; p < 16; p++) atomic_xor128(zv + col * 4096 + 16 * t + p, acc[p]);
 }
 
-// One CTA: optionally bind the top variable at r (fold), then emit (q(1), q(inf)).
-__global__ void __launch_bounds__(512) k_lc_round(f128* comb, f128* zv, int len, int do_fold, f128 r, int emit,
-                                                   f128* out) {
-  int t = threadIdx.x;
-  if (do_fold) {
-    int half = len;  // len is the length after folding
-    for (int i = t; i < half; i += blockDim.x) {
-      f128 c0 = comb[i], c1 = comb[i + half], z0 = zv[i], z1 = zv[i + half];
-      comb[i] = fx(c0, fmul(r, fx(c1, c0)));
-      zv[i] = fx(z0, fmul(r, fx(z1, z0)));
+// One lincheck round (top binding): with do_fold, fold comb and zv (2 len
+// values each) at r into their first len values; with emit, add the
+// message over the (folded) pairs (i, i + len/2) into out[0..2):
+// q1 = sum c1 z1, qinf = sum (c0 + c1)(z0 + z1).  Thread i < len/2 owns
+// outputs i and i + len/2 and reads exactly the four inputs that fold into
+// them, so the grid needs no synchronisation; the message is XOR-reduced per
+// CTA and added atomically (out must be zero).
+__global__ void __launch_bounds__(256) k_lc_round(f128* comb, f128* zv, int len, int do_fold, f128 r, int emit,
+                                                  f128* out) {
+  const int h = len >> 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  f128 q1 = mk(0, 0), qi = mk(0, 0);
+  if (i < h) {
+    f128 c0 = comb[i], c1 = comb[i + h], z0 = zv[i], z1 = zv[i + h];
+    if (do_fold) {
+      const f128 c0h = comb[i + len], c1h = comb[i + h + len], z0h = zv[i + len], z1h = zv[i + h + len];
+      c0 = fx(c0, fmul(r, fx(c0h, c0)));
+      c1 = fx(c1, fmul(r, fx(c1h, c1)));
+      z0 = fx(z0, fmul(r, fx(z0h, z0)));
+      z1 = fx(z1, fmul(r, fx(z1h, z1)));
+      comb[i] = c0;
+      comb[i + h] = c1;
+      zv[i] = z0;
+      zv[i + h] = z1;
     }
-    __syncthreads();
+    if (emit) {
+      q1 = fmul(c1, z1);
+      qi = fmul(fx(c0, c1), fx(z0, z1));
+    }
   }
   if (!emit) return;
-  int half = len >> 1;
-  u256 q1 = zero256(), qi = zero256();
-  for (int i = t; i < half; i += blockDim.x) {
-    f128 c0 = comb[i], c1 = comb[i + half], z0 = zv[i], z1 = zv[i + half];
-    acc_wide(q1, mul_wide(c1, z1));
-    acc_wide(qi, mul_wide(fx(c0, c1), fx(z0, z1)));
-  }
-  __shared__ f128 red[2][32];
-  f128 a = warp_xor(reduce(q1)), bq = warp_xor(reduce(qi));
-  if ((t & 31) == 0) { red[0][t >> 5] = a; red[1][t >> 5] = bq; }
-  __syncthreads();
-  if (t == 0) {
-    f128 x = mk(0, 0), y = mk(0, 0);
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { x = fx(x, red[0][w]); y = fx(y, red[1][w]); }
-    out[0] = x;
-    out[1] = y;
-  }
+  block_xor_out(q1, out);
+  block_xor_out(qi, out + 1);
 }
 
 void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
@@ -252,7 +255,9 @@ void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, f128* zv, cudaStrea
   count_launch(); k_lc_zvec<<<grid, 256, 0, s>>>((const uint16_t*)z, eqo, n_outer, chunk, zv);
 }
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s) {
-  count_launch(); k_lc_round<<<1, 512, 0, s>>>(comb, zv, len, fold, r, emit, out);
+  const int threads = std::max(1, len / 2);
+  count_launch();
+  k_lc_round<<<(threads + 255) / 256, 256, 0, s>>>(comb, zv, len, fold, r, emit, out);
 }
 
 // ------------------------------------------------------------------ K7 --
