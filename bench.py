@@ -286,8 +286,15 @@ def serving_report(device: int, full: bool):
     out = {}
     ctx = flockgpu.Context(device, hbm_budget_bytes=150 << 30)
     try:
+        lo, hi = (10, 20) if full else (10, 18)
+        batch_jobs = job_mix(64, 12, 18, 3)
+        serve_jobs = job_mix(48 if not full else 96, lo, hi, 4)
+        # the plain one-at-a-time times first, before the serving cache holds
+        # its setups (the plain provers' memory is outside that budget)
+        plain_batch = plain_seconds(ctx, batch_jobs)
+        plain_serve = plain_seconds(ctx, serve_jobs)
         ctx.serve_start(SERVE_SLOTS)
-        jobs = job_mix(64, 12, 18, 3)
+        jobs = batch_jobs
         n = sum(1 << l for l, _ in jobs)
         ctx.prove_batch(jobs, threads=BATCH_THREADS)  # warm: setups of every size cached
         t0 = time.perf_counter()
@@ -295,7 +302,7 @@ def serving_report(device: int, full: bool):
         wall = time.perf_counter() - t0
         lat = [r["latency_ms"] for r in res]
         cwall, clat = served_run(ctx, jobs)  # the same jobs through the continuous-batching queue
-        plain = plain_seconds(ctx, jobs)
+        plain = plain_batch
         out["batched"] = {"jobs": len(jobs), "log2_range": [12, 18], "compressions": n,
                           "value": n / wall, "unit": "compressions/s", "plain_value": n / plain,
                           "speedup_vs_plain": plain / wall, "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
@@ -304,11 +311,10 @@ def serving_report(device: int, full: bool):
                                   "remaining phases on concurrent streams",
                           "continuous": {"value": n / cwall, "p50_ms": pct(clat, 0.5), "p99_ms": pct(clat, 0.99),
                                          "slots": SERVE_SLOTS}}
-        lo, hi = (10, 20) if full else (10, 18)
-        jobs = job_mix(48 if not full else 96, lo, hi, 4)
+        jobs = serve_jobs
         n = sum(1 << l for l, _ in jobs)
         served_run(ctx, jobs)  # warm
-        plain = plain_seconds(ctx, jobs)
+        plain = plain_serve
         cap = len(jobs) / plain  # plain capacity in jobs/s for this size mix
         rates = [0.25, 0.5, 1.0, 2.0] if full else [1.0]
         out["served"] = []
@@ -478,6 +484,9 @@ def main():
     ap.add_argument("--log2", type=int, default=LOG2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the batched / served measurements")
+    ap.add_argument("--ntt-case", default=None, metavar="LOG_MSG,LANES,RATE,PLAN",
+                    help="one RS encode with candidate pass plan PLAN (no autotuning launches): the case that "
+                         "the NTT's ncu captures profile")
     ap.add_argument("--kernels", action="store_true",
                     help="only the kernel microbenchmarks (NTT / Merkle / sumcheck sweeps), one JSON line each")
     ap.add_argument("--serve", action="store_true",
@@ -485,6 +494,17 @@ def main():
     args = ap.parse_args()
     world, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                     int(os.environ.get("RANK", "0")), 0)
+    if args.ntt_case:
+        import flockgpu
+        log_msg, lanes, rate, plan = (int(x) for x in args.ntt_case.split(","))
+        ctx = flockgpu.Context(0)
+        msg = np.random.default_rng(1).integers(0, 2**64, 2 * (lanes << log_msg), dtype=np.uint64)
+        out = ctx.ntt_rs_encode_plan(msg, log_msg, lanes, rate, plan)
+        ctx.close()
+        if out is None:
+            raise SystemExit(f"no candidate plan {plan} for this shape")
+        print(json.dumps({"ntt_case": args.ntt_case, "codeword_values": int(out.size // 2)}))
+        return
     if args.kernels:
         if rank == 0:
             for row in kernel_report(0):

@@ -319,11 +319,14 @@ void launch_pass(const NttPass& ps, f128* data, const f128* ev, int log_d, int l
   PassArgs a{data, ev, log_d, lanes, ps.lgs, ps.l0, ps.R};
   const size_t smem = pass_smem(ps.lgs, ps.R);
   const uint64_t tiles = ((uint64_t)1 << (log_d - ps.R)) * (uint64_t)(lanes >> ps.lgs);
+  // The attribute is the same upper bound for every launch: it is global to
+  // the kernel, so a per-launch size set by one host thread could undercut
+  // another thread's launch of a larger tile.
   if (transpose) {
-    CK(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem1));
     count_launch(); k_ntt_pass<true><<<(unsigned)tiles, ps.threads, smem, s>>>(a);
   } else {
-    CK(cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem1));
     count_launch(); k_ntt_pass<false><<<(unsigned)tiles, ps.threads, smem, s>>>(a);
   }
 }
@@ -403,7 +406,8 @@ void ntt_replicate_batch(const BatchJob* jobs, int n_jobs, uint64_t total, cudaS
 size_t ntt_pass_batch_smem(const NttPass& p) { return pass_smem(p.lgs, p.R); }
 void ntt_pass_batch(const BatchJob* jobs, int n_jobs, int pass, uint64_t total_tiles, size_t smem, int grid,
                     cudaStream_t s) {
-  CK(cudaFuncSetAttribute(k_ntt_pass_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem > kSmem1) throw CudaError("ntt_pass_batch: tile larger than the shared-memory bound");
+  CK(cudaFuncSetAttribute(k_ntt_pass_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem1));
   count_launch();
   k_ntt_pass_batch<<<(unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)grid, total_tiles)), 256, smem, s>>>(
       jobs, n_jobs, pass, total_tiles);
