@@ -279,7 +279,7 @@ def pct(v, q):
     return v[i] + (v[min(i + 1, len(v) - 1)] - v[i]) * (k - i)
 
 
-def serving_report(device: int, full: bool):
+def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: int = BATCH_THREADS):
     """Batched (64 uneven jobs, 2^12..2^18, all at once) and served (Poisson
     arrivals, p50/p99) against the plain one-proof-at-a-time form."""
     import flockgpu
@@ -293,12 +293,12 @@ def serving_report(device: int, full: bool):
         # its setups (the plain provers' memory is outside that budget)
         plain_batch = plain_seconds(ctx, batch_jobs)
         plain_serve = plain_seconds(ctx, serve_jobs)
-        ctx.serve_start(SERVE_SLOTS)
+        ctx.serve_start(slots)
         jobs = batch_jobs
         n = sum(1 << l for l, _ in jobs)
-        ctx.prove_batch(jobs, threads=BATCH_THREADS)  # warm: setups of every size cached
+        ctx.prove_batch(jobs, threads=threads)  # warm: setups of every size cached
         t0 = time.perf_counter()
-        res = ctx.prove_batch(jobs, threads=BATCH_THREADS)
+        res = ctx.prove_batch(jobs, threads=threads)
         wall = time.perf_counter() - t0
         lat = [r["latency_ms"] for r in res]
         cwall, clat = served_run(ctx, jobs)  # the same jobs through the continuous-batching queue
@@ -306,11 +306,11 @@ def serving_report(device: int, full: bool):
         out["batched"] = {"jobs": len(jobs), "log2_range": [12, 18], "compressions": n,
                           "value": n / wall, "unit": "compressions/s", "plain_value": n / plain,
                           "speedup_vs_plain": plain / wall, "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
-                          "threads": BATCH_THREADS,
+                          "threads": threads,
                           "form": "flock_prove_batch: fused witness + commit graph over all jobs, then the "
                                   "remaining phases on concurrent streams",
                           "continuous": {"value": n / cwall, "p50_ms": pct(clat, 0.5), "p99_ms": pct(clat, 0.99),
-                                         "slots": SERVE_SLOTS}}
+                                         "slots": slots}}
         jobs = serve_jobs
         n = sum(1 << l for l, _ in jobs)
         served_run(ctx, jobs)  # warm
@@ -323,7 +323,7 @@ def serving_report(device: int, full: bool):
             out["served"].append({"arrival_rate_x_plain_capacity": f, "jobs": len(jobs), "log2_range": [lo, hi],
                                   "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
                                   "sustained_value": n / wall, "plain_value": n / plain,
-                                  "unit": "compressions/s", "slots": SERVE_SLOTS,
+                                  "unit": "compressions/s", "slots": slots,
                                   "hbm_budget_gb": 150})
     finally:
         ctx.close()
@@ -489,6 +489,8 @@ def main():
                          "the NTT's ncu captures profile")
     ap.add_argument("--kernels", action="store_true",
                     help="only the kernel microbenchmarks (NTT / Merkle / sumcheck sweeps), one JSON line each")
+    ap.add_argument("--slots", type=int, default=SERVE_SLOTS, help="serving: proofs in flight")
+    ap.add_argument("--batch-threads", type=int, default=BATCH_THREADS, help="batched form: host threads")
     ap.add_argument("--serve", action="store_true",
                     help="only the batched + served report: 64 uneven jobs, then Poisson arrivals at 4 rates")
     args = ap.parse_args()
@@ -512,7 +514,8 @@ def main():
         return
     if args.serve:
         if rank == 0:
-            print(json.dumps({"metric": "served/batched proof throughput and latency", **serving_report(0, True)}),
+            print(json.dumps({"metric": "served/batched proof throughput and latency",
+                              **serving_report(0, True, args.slots, args.batch_threads)}),
                   flush=True)
         return
     if args.impl == "reference":
