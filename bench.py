@@ -307,8 +307,8 @@ def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: i
                           "value": n / wall, "unit": "compressions/s", "plain_value": n / plain,
                           "speedup_vs_plain": plain / wall, "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
                           "threads": threads,
-                          "form": "flock_prove_batch: fused witness + commit graph over all jobs, then the "
-                                  "remaining phases on concurrent streams",
+                          "form": "flock_prove_batch: fused witness + commit graphs over groups of 8 jobs, "
+                                  "each overlapping the earlier groups' remaining phases on concurrent streams",
                           "continuous": {"value": n / cwall, "p50_ms": pct(clat, 0.5), "p99_ms": pct(clat, 0.99),
                                          "slots": slots}}
         jobs = serve_jobs

@@ -182,11 +182,14 @@ void Setup::capture_commit() {
 // Fused witness + RS encode + Merkle commit of several seeded proofs: every
 // stage is one launch over all jobs (persistent NTT passes over the tiles of
 // every job, one parent level of every tree per launch), captured as one
-// CUDA graph and replayed on `st`.  The setups' streams wait for it; each
-// proof then continues with Setup::prove(..., committed = true).
-void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds, cudaStream_t st) {
+// CUDA graph and launched on `st`.  The setups' streams wait for it; each
+// proof then continues with Setup::prove(..., committed = true).  The call
+// returns once the work is queued; release the handle after `st` finished.
+BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds,
+                               cudaStream_t st) {
+  BatchCommit h;
   const int n = (int)setups.size();
-  if (n == 0) return;
+  if (n == 0) return h;
   if ((int)seeds.size() != n) throw std::runtime_error("batch_commit: one seed per setup");
   std::vector<BatchJob> J(n);
   uint64_t wcta = 0, rep = 0, leaves = 0, tiles[3] = {0, 0, 0}, par[24] = {0};
@@ -245,6 +248,7 @@ void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>
     for (int l = 0; l < 24; l++) J[i].par0[l] = std::min<uint64_t>(J[i].par0[l], par[l]);
   BatchJob* dj = nullptr;
   CK(cudaMalloc(&dj, n * sizeof(BatchJob)));
+  h.jobs = dj;
   try {
     CK(cudaMemcpyAsync(dj, J.data(), n * sizeof(BatchJob), cudaMemcpyHostToDevice, st));
     int dev = 0, sms = 0;
@@ -259,22 +263,32 @@ void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>
       for (int l = 1; l <= max_level; l++) merkle_parents_batch(dj, n, l, par[l], st);
       merkle_top_batch(dj, n, st);
     });
-    const cudaError_t e = cudaGraphLaunch(g, st);
+    h.graph = g;
+    CK(cudaGraphLaunch(g, st));
     count_launch(launches);
-    cudaEvent_t done;
-    CK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-    CK(cudaEventRecord(done, st));
-    for (Setup* S : setups) CK(cudaStreamWaitEvent(S->st, done, 0));
-    CK(e);
-    CK(cudaStreamSynchronize(st));
-    cudaEventDestroy(done);
-    cudaGraphExecDestroy(g);
+    CK(cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming));
+    CK(cudaEventRecord(h.done, st));
+    for (Setup* S : setups) CK(cudaStreamWaitEvent(S->st, h.done, 0));
   } catch (...) {
     cudaStreamSynchronize(st);
-    cudaFree(dj);
+    batch_commit_release(h);
     throw;
   }
-  cudaFree(dj);
+  return h;
+}
+
+void batch_commit_release(BatchCommit& h) {
+  if (h.done) cudaEventDestroy(h.done);
+  if (h.graph) cudaGraphExecDestroy(h.graph);
+  if (h.jobs) cudaFree(h.jobs);
+  h = BatchCommit{};
+}
+
+void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds, cudaStream_t st) {
+  BatchCommit h = batch_commit_async(setups, seeds, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  batch_commit_release(h);
+  CK(e);
 }
 
 Setup::~Setup() {

@@ -12,7 +12,17 @@ namespace flock {
 void scatter(f128* dst, const uint64_t* pos, const f128* vals, size_t n, cudaStream_t s);
 class Setup;
 // Fused witness + commit of several seeded proofs (one graph of batched
-// launches on st); each setup's stream waits for it.
+// launches on st); each setup's stream waits for it.  batch_commit waits for
+// the commit; batch_commit_async only queues it and returns the resources to
+// release (batch_commit_release) once st has finished.
+struct BatchCommit {
+  BatchJob* jobs = nullptr;  // device job table
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t done = nullptr;
+};
+BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds,
+                               cudaStream_t st);
+void batch_commit_release(BatchCommit& h);
 void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds, cudaStream_t st);
 
 struct Level {
@@ -42,7 +52,8 @@ class Setup {
   static size_t estimate_bytes(uint32_t log2);
   size_t device_bytes = 0;  // allocated by the constructor
 
-  friend void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds, cudaStream_t st);
+  friend BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds,
+                                        cudaStream_t st);
   uint32_t log2 = 0;
   int n_log = 0, m = 0, sms = 0;
   size_t n_words = 0, n_leaves0 = 0;

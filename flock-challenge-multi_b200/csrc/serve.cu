@@ -54,39 +54,42 @@ std::vector<JobResult> Server::prove_batch(const std::vector<BatchItem>& jobs, i
     }
     if (wave.empty()) continue;
     const auto t_run = Clock::now();
-    std::string commit_err;
-    std::vector<bool> committed(wave.size(), false);
-    {
-      std::vector<Setup*> ss;
-      std::vector<uint64_t> seeds;
-      for (auto& w : wave)
-        if (!jobs[w.first].blocks) {
-          ss.push_back(w.second.get());
-          seeds.push_back(jobs[w.first].seed);
-        }
-      try {
-        batch_commit(ss, seeds, batch_st_);
-        for (size_t i = 0; i < wave.size(); i++) committed[i] = !jobs[wave[i].first].blocks;
-      } catch (const std::exception& e) {
-        commit_err = e.what();
-      }
+    // The seeded jobs' fused commits are queued in groups, in order, on the
+    // batch stream; a job's remaining phases start (on its own stream, after
+    // its group's commit) as soon as its group is queued, so the commit of
+    // one group overlaps the transcript phases of the earlier ones.
+    constexpr size_t kGroup = 8;
+    const size_t nw = wave.size();
+    std::unique_ptr<std::atomic<int>[]> ready(new std::atomic<int>[nw]);  // 0 wait, 1 go, 2 commit failed
+    std::vector<std::string> commit_err(nw);
+    std::vector<size_t> seeded;
+    for (size_t i = 0; i < nw; i++) {
+      const bool blocks = jobs[wave[i].first].blocks != nullptr;
+      ready[i].store(blocks ? 1 : 0);
+      if (!blocks) seeded.push_back(i);
     }
+    std::mutex rmu;
+    std::condition_variable rcv;
     std::atomic<size_t> k{0};
     auto run = [&] {
       cudaSetDevice(device_);
-      for (size_t i; (i = k.fetch_add(1)) < wave.size();) {
+      for (size_t i; (i = k.fetch_add(1)) < nw;) {
+        {
+          std::unique_lock<std::mutex> rl(rmu);
+          rcv.wait(rl, [&] { return ready[i].load() != 0; });
+        }
         const BatchItem& job = jobs[wave[i].first];
         Setup& S = *wave[i].second;
         JobResult& r = res[wave[i].first];
         try {
-          if (!commit_err.empty() && !job.blocks) throw std::runtime_error("batch commit: " + commit_err);
+          if (ready[i].load() == 2) throw std::runtime_error("batch commit: " + commit_err[i]);
           if (job.blocks) {
             const size_t n = (size_t)1 << job.log2;
             if (!S.blocks_buf) CK(cudaMalloc(&S.blocks_buf, n * 25 * sizeof(uint32_t)));
             CK(cudaMemcpyAsync(S.blocks_buf, job.blocks, n * 25 * sizeof(uint32_t), cudaMemcpyHostToDevice, S.st));
             r.bytes = S.prove(nullptr, S.blocks_buf, n, job.domain);
           } else {
-            r.bytes = S.prove(&job.seed, nullptr, 0, job.domain, committed[i]);
+            r.bytes = S.prove(&job.seed, nullptr, 0, job.domain, true);
           }
           r.status = FLOCK_OK;
         } catch (const CudaError& e) {
@@ -103,8 +106,32 @@ std::vector<JobResult> Server::prove_batch(const std::vector<BatchItem>& jobs, i
       }
     };
     std::vector<std::thread> th;
-    for (int t = 0; t < threads && t < (int)wave.size(); t++) th.emplace_back(run);
+    for (int t = 0; t < threads && t < (int)nw; t++) th.emplace_back(run);
+    std::vector<BatchCommit> handles;
+    for (size_t g0 = 0; g0 < seeded.size(); g0 += kGroup) {
+      const size_t g1 = std::min(seeded.size(), g0 + kGroup);
+      std::vector<Setup*> ss;
+      std::vector<uint64_t> seeds;
+      for (size_t j = g0; j < g1; j++) {
+        ss.push_back(wave[seeded[j]].second.get());
+        seeds.push_back(jobs[wave[seeded[j]].first].seed);
+      }
+      int state = 1;
+      try {
+        handles.push_back(batch_commit_async(ss, seeds, batch_st_));
+      } catch (const std::exception& e) {
+        state = 2;
+        for (size_t j = g0; j < g1; j++) commit_err[seeded[j]] = e.what();
+      }
+      {
+        std::lock_guard<std::mutex> rl(rmu);
+        for (size_t j = g0; j < g1; j++) ready[seeded[j]].store(state);
+      }
+      rcv.notify_all();
+    }
     for (auto& t : th) t.join();
+    cudaStreamSynchronize(batch_st_);
+    for (auto& h : handles) batch_commit_release(h);
     std::lock_guard<std::mutex> lk(mu_);
     for (auto& w : wave) release(std::move(w.second));
   }
