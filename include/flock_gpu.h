@@ -172,11 +172,12 @@ int flock_poll(flock_ctx* ctx, uint64_t ticket, flock_result* res, int timeout_m
  * returns FLOCK_ERR_CAPACITY if an output buffer was too small, otherwise
  * FLOCK_OK with each proof's own status in results[i].status).  Jobs are
  * admitted in order, in waves of as many as fit the context's HBM budget.
- * The witnesses, RS encodes and Merkle trees of a wave's seeded jobs run as
- * one CUDA graph of fused launches over all of its jobs (one persistent NTT
- * pass kernel over the tiles of every job, one tree level of every job per
- * launch); the remaining phases of each proof then run concurrently on
- * `threads` host threads, one CUDA stream each.  Every result is
+ * The witnesses, RS encodes and Merkle trees of a wave's seeded jobs run in
+ * groups of 8 jobs, each group as one CUDA graph of fused launches over its
+ * jobs (one persistent NTT pass kernel over the tiles of every job, one tree
+ * level of every job per launch); the remaining phases of each proof run
+ * concurrently on `threads` host threads, one CUDA stream each, starting as
+ * soon as the proof's group is queued.  Every result is
  * byte-identical to flock_prove_seed / flock_prove_blocks of the same job.
  * No counterpart in the reference, which proves one job per worker process
  * (benchmark-tools/worker/src/main.rs). */
