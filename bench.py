@@ -398,6 +398,35 @@ def kernel_report(device: int) -> list:
     return rows
 
 
+def chain_report(prover, log2: int, steps: int = 5) -> dict:
+    """The BLAKE3 hash-chain statement (Blake3Setup::prove_chain) on the same
+    setup: the flock_chain CLI's honest chain of 2^log2 compressions, proved
+    end to end through flock_prove_chain from pinned host records (H2D of the
+    records, prove, D2H of the bundle), timed on the host clock; the device
+    time is the sum of the proof's phase events.  The region fold and the
+    shift sumcheck fall in the ring-switch phase."""
+    import flockgpu
+    recs = flockgpu.PinnedArray((1 << log2, 28), np.uint32)
+    recs.array[:] = flockgpu.chain_blocks(0x5EED, 1 << log2)
+    for _ in range(2):
+        prover.prove_chain(recs.array)
+    wall, dev = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        size = len(prover.prove_chain(recs.array))
+        wall.append(time.perf_counter() - t0)
+        ph = prover.phase_ms()
+        dev.append(sum(ph.values()))
+    n = 1 << log2
+    e2e = pct(wall, 0.5)
+    dms = pct(dev, 0.5)
+    return {"chain": {"statement": f"hash chain of 2^{log2} BLAKE3 compressions (cv_(i+1) = out_lo(compress(cv_i)))",
+                      "log2": log2, "proofs": steps, "e2e_ms_median": e2e * 1e3,
+                      "e2e_compressions_per_s": n / e2e, "device_ms_median": dms,
+                      "device_compressions_per_s": n / (dms / 1e3), "proof_bytes": size,
+                      "h2d_bytes_per_proof": n * 112, "phases_ms": {k: round(v, 3) for k, v in ph.items()}}}
+
+
 def run_ours(args, world, rank, local):
     import flockgpu
     log2 = args.log2
@@ -466,6 +495,8 @@ def run_ours(args, world, rank, local):
                                         "frac": rate / int_product_peak(),
                                         "peak_def": "148 SMs x max SM clock x 32 IMAD.WIDE per SM per clock / "
                                                     "144 IMAD.WIDE per product"}
+    if world == 1 and not args.no_chain:
+        line.update(chain_report(prover, log2))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     if world == 1 and not args.no_serve:
@@ -484,6 +515,7 @@ def main():
     ap.add_argument("--log2", type=int, default=LOG2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the batched / served measurements")
+    ap.add_argument("--no-chain", action="store_true", help="skip the hash-chain measurement")
     ap.add_argument("--ntt-case", default=None, metavar="LOG_MSG,LANES,RATE,PLAN",
                     help="one RS encode with candidate pass plan PLAN (no autotuning launches): the case that "
                          "the NTT's ncu captures profile")

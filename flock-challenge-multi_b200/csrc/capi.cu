@@ -142,6 +142,54 @@ int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const u
   });
 }
 
+int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const uint8_t* domain, size_t dlen,
+                      uint8_t* out, size_t cap, size_t* out_len) {
+  if (!s || !records || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (n != ((size_t)1 << s->s->log2)) {
+    s->ctx->err = "a chain fills every slot: expected exactly 2^log2 compressions";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(s->ctx, [&] {
+    flock::ChainEnds ends;
+    memcpy(ends.cv0, records, sizeof(ends.cv0));
+    const uint32_t* last = records + 28 * (n - 1);
+    uint32_t st16[16];
+    flock::b3_compress(last, last + 8, (uint64_t)last[24] | (uint64_t)last[25] << 32, last[26], last[27], st16);
+    memcpy(ends.cv_last, st16, sizeof(ends.cv_last));
+    if (!s->s->records_buf) CK(cudaMalloc(&s->s->records_buf, n * 28 * sizeof(uint32_t)));
+    CK(cudaMemcpyAsync(s->s->records_buf, records, n * 28 * sizeof(uint32_t), cudaMemcpyHostToDevice, s->s->st));
+    std::string d((const char*)domain, dlen);
+    return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d, false, &ends), out, cap, out_len);
+  });
+}
+
+int flock_chain_blocks(uint64_t seed, const uint32_t* initial_cv, size_t steps, uint32_t* records) {
+  if (!records && steps) return FLOCK_ERR_ARG;
+  static const uint32_t kIV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
+                                  0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
+  uint32_t cv[8];
+  memcpy(cv, initial_cv ? initial_cv : kIV, sizeof(cv));
+  uint64_t x = seed;
+  for (size_t i = 0; i < steps; i++) {
+    uint32_t* r = records + 28 * i;
+    memcpy(r, cv, 32);
+    for (int w = 0; w < 16; w++) {
+      x += 0x9E3779B97F4A7C15ull;
+      uint64_t z = x;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      r[8 + w] = (uint32_t)(z ^ (z >> 31));
+    }
+    r[24] = r[25] = 0;  // counter
+    r[26] = 64;         // block_len
+    r[27] = 0;          // flags
+    uint32_t st16[16];
+    flock::b3_compress(r, r + 8, 0, 64, 0, st16);
+    memcpy(cv, st16, 32);
+  }
+  return FLOCK_OK;
+}
+
 int flock_host_alloc(size_t bytes, void** out) {
   if (!out || bytes == 0) return FLOCK_ERR_ARG;
   *out = nullptr;

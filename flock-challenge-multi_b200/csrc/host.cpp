@@ -511,7 +511,11 @@ std::vector<uint8_t> encode(const Proof& p) {
   e.o.reserve(512 * 1024);
   for (char c : std::string("FLOCK")) e.o.push_back((uint8_t)c);
   e.o.push_back(4);
-  e.o.push_back(2);
+  // R1csProofBundleLigerito (flavor 2) or ChainProofBundleLigerito (flavor 3:
+  // hash_kind first, the shift proof after the lincheck, the endpoints last;
+  // proof_io.rs:144-157, chain_common.rs:247-253)
+  e.o.push_back(p.chain ? 3 : 2);
+  if (p.chain) e.u32(0);  // HashKind::Blake3
   e.h(p.root);
   e.u64(p.m);
   e.u64(1);  // log_inv_rate
@@ -526,6 +530,10 @@ std::vector<uint8_t> encode(const Proof& p) {
   e.f(p.fc);
   e.pairs(p.lc_rounds);
   e.fs(p.z_partial);
+  if (p.chain) {
+    e.pairs(p.shift_rounds);
+    e.f(p.g_at_point);
+  }
   e.u64(p.s_hat_v.size());
   for (auto& s : p.s_hat_v) e.fs(s);
   e.h(p.lig_root);
@@ -541,6 +549,13 @@ std::vector<uint8_t> encode(const Proof& p) {
   e.fs(p.ood);
   e.u64(p.fold_nonces.size());
   for (auto v : p.fold_nonces) e.u64(v);
+  if (p.chain) {
+    // Vec<bool>: u64 length, one byte per bit (bit 32 w + b = bit b of word w)
+    for (const uint32_t* cv : {p.cv0, p.cv_last}) {
+      e.u64(256);
+      for (int i = 0; i < 256; i++) e.o.push_back((uint8_t)((cv[i / 32] >> (i % 32)) & 1));
+    }
+  }
   return e.o;
 }
 

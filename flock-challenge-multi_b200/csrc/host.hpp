@@ -96,6 +96,11 @@ struct Proof {
   std::vector<std::pair<f128, f128>> sc_msgs;
   std::vector<uint64_t> grind_nonces, fold_nonces;
   std::vector<f128> ood;
+  // hash-chain bundle (flavor 3): the shift argument and public endpoints
+  bool chain = false;
+  std::vector<std::pair<f128, f128>> shift_rounds;
+  f128 g_at_point{};
+  uint32_t cv0[8] = {}, cv_last[8] = {};
 };
 std::vector<uint8_t> encode(const Proof& p);
 

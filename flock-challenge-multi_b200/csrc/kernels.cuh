@@ -41,8 +41,10 @@ struct CudaError : std::runtime_error {
 // K0
 void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
                          f128* b, cudaStream_t s);
+// records: 28 u32 per compression (cv, m, counter u64, block_len, flags);
+// otherwise 25 (cv, m, counter_lo of the benchmark generator)
 void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a, f128* b,
-                           cudaStream_t s);
+                           cudaStream_t s, bool records = false);
 // K1
 // NTT pass plans: the passes (first layer l0, layer count R, 2^lgs lanes per
 // tile, threads per CTA) that cover layers layer_begin..log_d-1.
@@ -125,5 +127,9 @@ void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, con
 void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int grid, cudaStream_t s);
 void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size_t n_pairs_out, bool emit, f128* out,
                   int grid, cudaStream_t s);
+// hash chain: region fold of every instance's cv / out_lo words (g = [In | Out],
+// 2 n_inst values) and the packed-direct claim's scatter into b_combined
+void chain_fold(const f128* z, size_t n_inst, f128 e0, f128 e1, f128* g, cudaStream_t s);
+void chain_scatter(f128* bc, const f128* eq_inst, size_t n_inst, const f128 c[4], cudaStream_t s);
 void sc3_round(const f128* a, const f128* b, const f128* e, f128* ao, f128* bo, const f128* rho, size_t n_pairs,
                f128* out, int grid, cudaStream_t s);

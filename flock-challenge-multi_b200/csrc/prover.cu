@@ -54,8 +54,9 @@ size_t Setup::estimate_bytes(uint32_t log2) {
   const size_t n_words = (size_t)1 << (kKLog + std::max<int>(3, (int)log2) - 7);
   // z, a, b, 4 fold buffers, eq scratch, the rate-1/2 codeword (2x), its tree
   // (1/16 of a word per word), the Ligero levels and query basis (< 1/8),
-  // blocks staging (25 u32 per compression), statement and small tables
-  return n_words * 16 * 10 + n_words * 2 + n_words * 2 + (n_words / 128) * 100 + ((size_t)96 << 20);
+  // blocks staging (25 u32 per compression) and chain records (28 u32),
+  // statement and small tables
+  return n_words * 16 * 10 + n_words * 2 + n_words * 2 + (n_words / 128) * 212 + ((size_t)96 << 20);
 }
 
 Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
@@ -293,7 +294,7 @@ void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>
 
 Setup::~Setup() {
   cudaStreamSynchronize(st);
-  void* ptrs[] = {z, a, b, cw0, tree0, pp[0], pp[1], pp[2], pp[3], eqbuf[0], zv_pre, induce_buf, out, blocks_buf,
+  void* ptrs[] = {z, a, b, cw0, tree0, pp[0], pp[1], pp[2], pp[3], eqbuf[0], zv_pre, induce_buf, out, blocks_buf, records_buf,
                   tabs_r1, lag, elo, ehi, comb, zv, eq_inner, bc_tabs, idx, gather, d_found, at_ptr, bt_ptr,
                   at_row, bt_row};
   for (void* p : ptrs) cudaFree(p);
@@ -430,7 +431,7 @@ void Setup::mark(int phase) {
 // the runtime stages before the call returns: the stream needs no
 // synchronisation except where the transcript reads a device value.
 std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
-                                  const std::string& domain, bool committed) {
+                                  const std::string& domain, bool committed, const ChainEnds* chain) {
   Proof P;
   P.m = (uint64_t)m;
   const int G = sms * 4;
@@ -439,7 +440,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   if (!committed) {
     // ---- K0 witness
     if (seed) launch_witness_seed(*seed, log2, 1u << log2, n_slots, z, a, b, st);
-    else launch_witness_blocks(blocks_dev, (uint32_t)n_blocks, n_slots, z, a, b, st);
+    else launch_witness_blocks(blocks_dev, (uint32_t)n_blocks, n_slots, z, a, b, st, chain != nullptr);
     CK(cudaGetLastError());
   }
   mark(1);
@@ -661,6 +662,59 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   (void)r_skip2;
   mark(6);
 
+  // ---- hash chain (chain_common.rs:318-324): tau_pos folds each instance's
+  // input cv and output out_lo to one value (g = [In | Out]); the shift
+  // sumcheck (chain.rs:155-236) over W(y, s0) g(y, s0), s0 the high
+  // variable, runs on the lincheck's round kernel (same message and
+  // top-variable fold) and leaves one packed-direct claim z(point) = value,
+  // point = [tau_pos, s0*, 0^5, tau'].  pp[2], pp[3] are free until the
+  // Ligerito folds.
+  std::vector<f128> pd_point;
+  f128 pd_value = mk(0, 0);
+  if (chain) {
+    P.chain = true;
+    memcpy(P.cv0, chain->cv0, sizeof(P.cv0));
+    memcpy(P.cv_last, chain->cv_last, sizeof(P.cv_last));
+    const size_t N = n_slots;
+    const f128 tau_pos = tr.sample_vec(1)[0];
+    f128* g = pp[2];
+    f128* w = pp[3];
+    chain_fold(z, N, fx(hone(), tau_pos), tau_pos, g, st);
+    const std::vector<f128> tau = tr.sample_vec((size_t)n_log);
+    const f128 alpha = tr.sample();
+    // W(y, 0) = eq(tau, y - 1) for y >= 1, W(0, 0) = alpha; W(y, 1) = eq(tau, y)
+    eq_table(tau, w + N);
+    CK(cudaMemcpyAsync(w + 1, w + N, (N - 1) * sizeof(f128), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(w, &alpha, sizeof(f128), cudaMemcpyHostToDevice, st));
+    int len = (int)(2 * N);
+    CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
+    lc_round(w, g, len, false, mk(0, 0), true, out, st);
+    std::vector<f128> rs;
+    for (int k = 0; k <= n_log; k++) {
+      // the last message is over g[0], g[1]; the final fold happens here
+      if (k == n_log) CK(cudaMemcpyAsync(h_out + 2, g, 2 * sizeof(f128), cudaMemcpyDeviceToHost, st));
+      fetch(out, 2, h_out);
+      P.shift_rounds.push_back({h_out[0], h_out[1]});
+      tr.f128v(h_out[0]);
+      tr.f128v(h_out[1]);
+      const f128 rk = tr.sample();
+      rs.push_back(rk);
+      if (k < n_log) {
+        len >>= 1;
+        CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
+        lc_round(w, g, len, true, rk, true, out, st);
+      } else {
+        pd_value = fx(h_out[2], hmul(rk, fx(h_out[3], h_out[2])));
+      }
+    }
+    P.g_at_point = pd_value;
+    // round k bound variable n_log - k; variable n_log is s0
+    pd_point.assign(7 + (size_t)n_log, mk(0, 0));
+    pd_point[0] = tau_pos;
+    pd_point[1] = rs[0];
+    for (int k = 1; k <= n_log; k++) pd_point[7 + (size_t)(n_log - k)] = rs[k];
+  }
+
   // ---- PCS open: ring switches + combine
   tr.label("flock-pcs-open-batch-v0");
   std::vector<f128> x_ab = r_inner_rest;
@@ -697,6 +751,14 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   }
   f128 gam[2] = {tr.sample(), tr.sample()};
   f128 target = fx(hmul(gam[0], claim[0]), hmul(gam[1], claim[1]));
+  // the packed-direct claim after the ring-switched ones (pcs.rs:844-872)
+  f128 gpd = mk(0, 0);
+  if (chain) {
+    tr.label("flock-pcs-packed-direct-v0");
+    tr.f128v(pd_value);
+    gpd = tr.sample();
+    target = fx(target, hmul(gpd, pd_value));
+  }
   {
     std::vector<f128> T(2 * 16 * 256);
     for (int k = 0; k < 2; k++) {
@@ -728,6 +790,16 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     }
     ring_bcombined_ct(d, d + nlo, d + nlo + nhi, d + 2 * nlo + nhi, bc_tabs, bc_tabs + 4096, lo_bits, nhi, pp[1],
                       sms, st);
+  }
+  if (chain) {
+    // b_combined += gpd eq(point): words w = 0..3 of block i get
+    // gpd eq(tau_pos, w & 1) eq(s0*, w >> 1) eq(tau', i) (pcs.rs:1236-1248)
+    const f128 tp = pd_point[0], s0 = pd_point[1];
+    const f128 ep[2] = {fx(hone(), tp), tp}, es[2] = {fx(hone(), s0), s0};
+    f128 c[4];
+    for (int wd = 0; wd < 4; wd++) c[wd] = hmul(gpd, hmul(ep[wd & 1], es[wd >> 1]));
+    eq_table(std::vector<f128>(pd_point.begin() + 7, pd_point.end()), scratch_eq());
+    chain_scatter(pp[1], scratch_eq(), n_slots, c, st);
   }
   mark(7);
 

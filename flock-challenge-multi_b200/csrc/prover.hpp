@@ -25,6 +25,12 @@ BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vec
 void batch_commit_release(BatchCommit& h);
 void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds, cudaStream_t st);
 
+// Public endpoints of a hash chain: the input cv of the first compression and
+// the output cv (out_lo) of the last.
+struct ChainEnds {
+  uint32_t cv0[8], cv_last[8];
+};
+
 struct Level {
   int lanes = 0, log_msg_pos = 0, rate = 0;
   size_t positions = 0;
@@ -43,9 +49,12 @@ class Setup {
 
   // seed != nullptr: inputs generated on the device from the benchmark
   // generator; otherwise blocks_dev holds n_blocks x 25 u32 on the device.
-  // committed: the witness, codeword and tree were filled by batch_commit
+  // committed: the witness, codeword and tree were filled by batch_commit.
+  // chain != nullptr: a hash-chain proof (Blake3Setup::prove_chain,
+  // blake3.rs:5195-5215) whose bundle carries these endpoints; blocks_dev
+  // then holds 2^log2 records of 28 u32 (cv, m, counter u64, block_len, flags).
   std::vector<uint8_t> prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
-                             const std::string& domain, bool committed = false);
+                             const std::string& domain, bool committed = false, const ChainEnds* chain = nullptr);
   void phase_times(double* ms) const;
   // device bytes a setup for 2^log2 compressions holds (an upper estimate,
   // used for admission before allocating)
@@ -59,6 +68,7 @@ class Setup {
   size_t n_words = 0, n_leaves0 = 0;
   cudaStream_t st = nullptr;
   uint32_t* blocks_buf = nullptr;  // device staging for caller-provided compressions
+  uint32_t* records_buf = nullptr;  // device staging for a hash chain's compression records
 
  private:
   void build_round1_tables();

@@ -224,26 +224,35 @@ __global__ void __launch_bounds__(kWThreads, 4) k_witness_seed_batch(const Batch
   witness_seed_cta(wsm, J.seed, J.log2, J.n_blocks, J.n_slots, J.z, J.a, J.b, c - (uint32_t)J.wcta0);
 }
 
-// blocks: 25 u32 per compression (cv[8], m[16], counter_lo); counter_hi = 0,
-// block_len = 64, flags = 11 as in the benchmark generator.
+// blocks: REC u32 per compression.  REC = 25: cv[8], m[16], counter_lo, with
+// counter_hi = 0, block_len = 64, flags = 11 as in the benchmark generator.
+// REC = 28: the full record cv[8], m[16], counter (u64), block_len, flags
+// (Compression, blake3.rs:1861).
+template <int REC>
 __global__ void __launch_bounds__(kWThreads, 4) k_witness_blocks(const uint32_t* __restrict__ blocks, uint32_t n_blocks,
                                                              uint32_t n_slots, f128* __restrict__ z,
                                                              f128* __restrict__ a, f128* __restrict__ b) {
   extern __shared__ uint64_t wsm[];
   const Stage S = make_stage(wsm, z, a, b, n_slots, blockIdx.x);
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t cv[8] = {0}, m[16] = {0}, ctr = 0, blen = 0, flags = 0;
+  uint32_t cv[8] = {0}, m[16] = {0}, ctr = 0, ctr_hi = 0, blen = 0, flags = 0;
   if (i < n_blocks) {
-    const uint32_t* p = blocks + (size_t)25 * i;
+    const uint32_t* p = blocks + (size_t)REC * i;
 #pragma unroll
     for (int w = 0; w < 8; w++) cv[w] = p[w];
 #pragma unroll
     for (int w = 0; w < 16; w++) m[w] = p[8 + w];
     ctr = p[24];
-    blen = 64;
-    flags = 11;
+    if (REC == 28) {
+      ctr_hi = p[25];
+      blen = p[26];
+      flags = p[27];
+    } else {
+      blen = 64;
+      flags = 11;
+    }
   }
-  compression_witness(cv, m, ctr, 0, blen, flags, S);
+  compression_witness(cv, m, ctr, ctr_hi, blen, flags, S);
 }
 
 void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
@@ -254,11 +263,11 @@ void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32
                                                                                      z, a, b);
 }
 void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a, f128* b,
-                           cudaStream_t s) {
-  CK(cudaFuncSetAttribute(k_witness_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWitnessSmem));
+                           cudaStream_t s, bool records) {
+  auto kern = records ? k_witness_blocks<28> : k_witness_blocks<25>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWitnessSmem));
   count_launch();
-  k_witness_blocks<<<(n_slots + kWThreads - 1) / kWThreads, kWThreads, kWitnessSmem, s>>>(blocks, n_blocks, n_slots,
-                                                                                       z, a, b);
+  kern<<<(n_slots + kWThreads - 1) / kWThreads, kWThreads, kWitnessSmem, s>>>(blocks, n_blocks, n_slots, z, a, b);
 }
 
 uint32_t witness_ctas(uint32_t n_slots) { return (n_slots + kWThreads - 1) / kWThreads; }

@@ -28,7 +28,7 @@ EXPORTS = (
     "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove", "flock_merkle_root_noalloc",
     "flock_serve_start", "flock_submit", "flock_poll", "flock_sumcheck_round3", "flock_bench_sumcheck3",
     "flock_ntt_autotune", "flock_ntt_rs_encode_plan", "flock_prove_batch", "flock_host_alloc",
-    "flock_host_free",
+    "flock_host_free", "flock_prove_chain", "flock_chain_blocks",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -92,6 +92,8 @@ def load() -> ctypes.CDLL:
         lib.flock_host_alloc.argtypes = [sz, ctypes.POINTER(vp)]
         lib.flock_host_free.argtypes = [vp]
         lib.flock_prove_batch.argtypes = [vp, ctypes.POINTER(FlockJob), sz, ctypes.POINTER(FlockResult), i32]
+        lib.flock_prove_chain.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        lib.flock_chain_blocks.argtypes = [u64, vp, sz, vp]
         _lib = lib
     return _lib
 
@@ -114,6 +116,21 @@ def generate_compressions(log2: int, seed: int) -> np.ndarray:
         z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         z = z ^ (z >> np.uint64(31))
     return z.astype(np.uint32).reshape(-1, 25)
+
+
+CHAIN_DOMAIN = b"flock_chain-cli"
+
+
+def chain_blocks(seed: int, steps: int, initial_cv=None) -> np.ndarray:
+    """The flock_chain CLI's honest BLAKE3 chain, (steps, 28) u32 records
+    cv[8], m[16], counter lo/hi, block_len, flags
+    (crates/flock-prover/src/bin/flock_chain.rs:178-193, 236-260)."""
+    out = np.zeros((steps, 28), np.uint32)
+    cv = None if initial_cv is None else np.ascontiguousarray(initial_cv, np.uint32)
+    rc = load().flock_chain_blocks(seed, None if cv is None else _ptr(cv), steps, _ptr(out))
+    if rc:
+        raise FlockError(f"chain_blocks failed ({rc})")
+    return out
 
 
 class PinnedArray:
@@ -354,6 +371,16 @@ class Prover:
         rc = self.ctx.lib.flock_prove_blocks(self.h, _ptr(blocks), blocks.shape[0], domain, len(domain),
                                              _ptr(self._buf), self._buf.size, ctypes.byref(n))
         self.ctx._check(rc, "prove_blocks")
+        return self._buf[: n.value].tobytes()
+
+    def prove_chain(self, records: np.ndarray, domain: bytes = CHAIN_DOMAIN) -> bytes:
+        """A hash-chain proof (Blake3Setup::prove_chain, blake3.rs:5195) over
+        (2^log2, 28) u32 compression records; FLOCK v4 chain bundle bytes."""
+        records = np.ascontiguousarray(records, np.uint32).reshape(-1, 28)
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_prove_chain(self.h, _ptr(records), records.shape[0], domain, len(domain),
+                                            _ptr(self._buf), self._buf.size, ctypes.byref(n))
+        self.ctx._check(rc, "prove_chain")
         return self._buf[: n.value].tobytes()
 
     def bench(self, seed0: int, steps: int):

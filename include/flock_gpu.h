@@ -18,6 +18,13 @@
  *                           blake3.rs:4846, proof_io.rs:165)
  *  - flock_prove_blocks  <- Blake3Setup::prove_fast(&blocks, &mut FsChallenger)
  *                           + to_bytes (blake3.rs:4846-4990)
+ *  - flock_prove_chain   <- Blake3Setup::prove_chain(&blocks, &mut FsChallenger)
+ *                           + ChainProofBundleLigerito::to_bytes (blake3.rs:
+ *                           5195-5215, r1cs_hashes/chain_common.rs:287-350,
+ *                           proof_io.rs:144-157, 943-950)
+ *  - flock_chain_blocks  <- the flock_chain CLI's honest BLAKE3 chain
+ *                           (crates/flock-prover/src/bin/flock_chain.rs:178-193,
+ *                           236-260)
  *  - flock_ntt_rs_encode <- AdditiveNttF128::standard(d) + rs_encode_interleaved
  *                           (crates/flock-core/src/ntt/additive_ntt_f128.rs:
  *                           2661-2670, 2785)
@@ -70,6 +77,21 @@ int flock_prove_seed(flock_setup* s, uint64_t seed, const uint8_t* domain, size_
  * block_len 64, flags 11, n == 2^log2_n. */
 int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const uint8_t* domain, size_t dlen,
                        uint8_t* out, size_t cap, size_t* out_len);
+/* One hash-chain proof: the 2^log2_n compressions form a chain
+ * x_{i+1} = out_lo(compress(x_i)) with public endpoints.  records: n x 28
+ * u32, each cv[8], m[16], counter (u64, little endian), block_len, flags
+ * (Compression, blake3.rs:1861); n == 2^log2_n (a chain fills every slot).
+ * The bundle (FLOCK v4, flavor 3) carries the endpoints records[0].cv and
+ * out_lo(compress(records[n - 1])).  The prover does not check the links: a
+ * broken chain gives a proof that the reference's verify_chain rejects. */
+int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const uint8_t* domain, size_t dlen,
+                      uint8_t* out, size_t cap, size_t* out_len);
+/* The flock_chain CLI's honest chain of `steps` records: record i has
+ * cv = x_i (x_0 = initial_cv, or the BLAKE3 IV when NULL), 16 message words
+ * from SplitMix64(seed) (low 32 bits of each draw), counter 0, block_len 64,
+ * flags 0; x_{i+1} = out_lo(compress(record i)).  Runs on the host (each link
+ * needs the previous output). */
+int flock_chain_blocks(uint64_t seed, const uint32_t* initial_cv, size_t steps, uint32_t* records);
 /* Page-locked host memory for inputs and outputs: flock_prove_blocks copies
  * compressions from such a buffer at the full host-to-device rate (a
  * pageable buffer is staged by the CUDA runtime first).  No counterpart in

@@ -23,6 +23,38 @@ int flockref_prove(uint32_t log2, uint64_t seed, uint8_t* out, size_t cap, size_
   }
 }
 
+// Hash chains.  A compression record is 28 u32: cv[8], m[16], counter (u64,
+// little endian), block_len, flags -- the layout of flockref::Compression.
+static_assert(sizeof(Compression) == 112, "compression record");
+
+void flockref_chain_blocks(uint64_t seed, const uint32_t* initial_cv, size_t steps, uint32_t* out28) {
+  std::vector<Compression> v = chain_blocks(seed, initial_cv ? initial_cv : b3::IV, steps);
+  memcpy(out28, v.data(), v.size() * sizeof(Compression));
+}
+
+// prove_chain over 2^log2 given compressions.  `check` receives 1 when the
+// shift argument verifies from the bundle's public endpoints and the batched
+// open's claim identity holds.  A non-null `cv_last` replaces the public
+// output endpoint (written to the bundle and used by that check).
+int flockref_prove_chain_blocks(const uint32_t* blocks28, uint32_t log2, const uint8_t* domain, size_t dlen,
+                                const uint32_t* cv_last, uint8_t* out, size_t cap, size_t* out_len, int* check) {
+  try {
+    std::vector<Compression> blocks((size_t)1 << log2);
+    memcpy(blocks.data(), blocks28, blocks.size() * sizeof(Compression));
+    std::string d((const char*)domain, dlen);
+    bool ok = false;
+    ChainBundle cb = prove_chain(blocks, (int)log2, d, &ok, cv_last);
+    if (check) *check = ok ? 1 : 0;
+    std::vector<uint8_t> bytes = serialize_chain(cb);
+    *out_len = bytes.size();
+    if (bytes.size() > cap) return 2;
+    memcpy(out, bytes.data(), bytes.size());
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
 void flockref_f128_mul(const uint64_t* a, const uint64_t* b, uint64_t* out) {
   F128 r = F128(a[0], a[1]) * F128(b[0], b[1]);
   out[0] = r.lo;

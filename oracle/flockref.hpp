@@ -241,4 +241,51 @@ const LigeritoConfig& ligerito_config(int m);
 // ---------------------------------------------------------------------------
 Bundle prove(const std::vector<Compression>& blocks, int n_log, const std::string& domain);
 
+// A packed-MLE evaluation claim z_packed(point) = value, opened directly in
+// the batched open beside the ring-switched claims (pcs.rs:57-95).
+struct DirectClaim { std::vector<F128> point; F128 value; };
+// Runs after the lincheck on the prover's transcript, with the packed z.
+using CoreHook = std::function<std::vector<DirectClaim>(Challenger&, const std::vector<F128>&)>;
+Bundle prove_with(const std::vector<Compression>& blocks, int n_log, const std::string& domain,
+                  const CoreHook& after_core);
+// sum_j bc[j] * z[j] == target (the batched open's claim)
+bool open_identity(const std::vector<F128>& z, const std::vector<F128>& bc, F128 target);
+// that identity, as checked by the last prove_with with a hook on this thread
+bool& last_open_identity_ok();
+
+// ---------------------------------------------------------------------------
+// BLAKE3 hash chain.  crates/flock-prover/src/chain.rs (shift argument),
+// r1cs_hashes/chain_common.rs (region fold, claim point, generic prover),
+// r1cs_hashes/blake3.rs:5150-5240 (CHAIN_LAYOUT, prove_chain),
+// bin/flock_chain.rs:178-193, 236-260 (the CLI's chain inputs).
+// ---------------------------------------------------------------------------
+struct ShiftProof { std::vector<std::pair<F128, F128>> rounds; F128 g_at_point; };
+struct ChainClaims { std::vector<F128> instance_point; F128 sel0; F128 value; };
+struct ChainBundle {
+  Bundle core;
+  ShiftProof shift;
+  uint32_t cv0[8], cv_last[8];
+};
+// out_lo of a compression: words 0..7 of the output state
+void compress_cv(const Compression& c, uint32_t out[8]);
+// the CLI's honest chain: cv_{i+1} = out_lo(compress(cv_i, m_i, 0, 64, 0)),
+// m_i = 16 SplitMix64 draws (low 32 bits) from `seed`
+std::vector<Compression> chain_blocks(uint64_t seed, const uint32_t initial_cv[8], size_t steps);
+F128 shift_mle(const std::vector<F128>& a, const std::vector<F128>& b);
+F128 eq_eval(const std::vector<F128>& a, const std::vector<F128>& b);
+ShiftProof shift_prove(const std::vector<F128>& in, const std::vector<F128>& out, Challenger& ch,
+                       ChainClaims& claims);
+// false on a malformed proof or a failed final check
+bool shift_verify(const ShiftProof& pf, F128 x0_r, F128 xlast_r, size_t n, Challenger& ch, ChainClaims& claims);
+// tau_pos-MLE of a public 256-bit chaining value over its two packed positions
+F128 fold_public_cv(const uint32_t cv[8], F128 tau_pos);
+// prove_chain; when `check` is non-null it receives the prover-side checks:
+// the shift argument verified from the public endpoints on a copy of the
+// transcript, and the batched open's claim identity.  `claimed_cv_last`, when
+// given, is the public output endpoint put in the bundle and checked against
+// (by default the output of the last compression).
+ChainBundle prove_chain(const std::vector<Compression>& blocks, int n_log, const std::string& domain,
+                        bool* check = nullptr, const uint32_t* claimed_cv_last = nullptr);
+std::vector<uint8_t> serialize_chain(const ChainBundle& cb);
+
 }  // namespace flockref

@@ -661,12 +661,16 @@ struct W {
 };
 }  // namespace
 
-std::vector<uint8_t> serialize(const Bundle& bd) {
-  W w;
+static void put_header(W& w, uint8_t flavor) {
   const char* magic = "FLOCK";
   for (int i = 0; i < 5; i++) w.u8((uint8_t)magic[i]);
   w.u8(4);  // VERSION
-  w.u8(2);  // flavor: R1CS Ligerito
+  w.u8(flavor);
+}
+
+// Commitment, ZerocheckProof, LincheckProof (the fields a compression bundle
+// and a chain bundle share, in this order)
+static void put_core(W& w, const Bundle& bd) {
   // Commitment { root, params { m, log_inv_rate, log_batch_size, profile, merkle_hash } }
   w.h(bd.root);
   w.u64(bd.m);
@@ -684,7 +688,10 @@ std::vector<uint8_t> serialize(const Bundle& bd) {
   // LincheckProof
   w.pairs(bd.lc.rounds);
   w.fv(bd.lc.z_partial);
-  // BatchOpeningProofLigerito { ring_switches: Vec<{s_hat_v}>, ligerito }
+}
+
+// BatchOpeningProofLigerito { ring_switches: Vec<{s_hat_v}>, ligerito }
+static void put_open(W& w, const Bundle& bd) {
   w.u64(bd.s_hat_v.size());
   for (auto& s : bd.s_hat_v) w.fv(s);
   const LigeritoProof& L = bd.lig;
@@ -702,13 +709,47 @@ std::vector<uint8_t> serialize(const Bundle& bd) {
   w.u64v(L.grinding_nonces);
   w.fv(L.ood_values);
   w.u64v(L.fold_grinding_nonces);
+}
+
+std::vector<uint8_t> serialize(const Bundle& bd) {
+  W w;
+  put_header(w, 2);  // flavor: R1CS Ligerito
+  put_core(w, bd);
+  put_open(w, bd);
+  return w.out;
+}
+
+// ChainProofBundleLigerito { hash_kind, commitment, proof { zerocheck,
+// lincheck, shift { rounds, g_at_point }, pcs_open }, cv_0_phys, cv_last_phys }
+// (proof_io.rs:144-157, 943-950; chain_common.rs:247-253; chain.rs:103-112);
+// Vec<bool> is a u64 length and one byte per bool.
+std::vector<uint8_t> serialize_chain(const ChainBundle& cb) {
+  W w;
+  put_header(w, 3);  // flavor: chain Ligerito
+  w.u32(0);          // HashKind::Blake3
+  put_core(w, cb.core);
+  w.pairs(cb.shift.rounds);
+  w.f(cb.shift.g_at_point);
+  put_open(w, cb.core);
+  for (const uint32_t* cv : {cb.cv0, cb.cv_last}) {
+    w.u64(256);
+    for (int i = 0; i < 256; i++) w.u8((uint8_t)((cv[i / 32] >> (i % 32)) & 1));
+  }
   return w.out;
 }
 
 // --------------------------------------------------------------------------
-// Full prove (prover.rs:373-473)
+// Full prove (prover.rs:373-473).  `after_core` (may be empty) runs between
+// the lincheck and the batched open, on the same transcript, and returns the
+// packed-direct claims the open batches with the two ring-switched ones
+// (pcs.rs:130-290; claim combine pcs.rs:844-872, 1236-1248): each claim's
+// value is observed under its label, one gamma is sampled per claim after
+// the ring-switch gammas, the target gains gamma * value and b_combined
+// gains gamma * eq(point), scattered over the point's nonzero coordinates
+// (ring_switch.rs:2600-2617 build_eq_sparse, :2565-2571 scatter_idx).
 // --------------------------------------------------------------------------
-Bundle prove(const std::vector<Compression>& blocks, int n_log, const std::string& domain) {
+Bundle prove_with(const std::vector<Compression>& blocks, int n_log, const std::string& domain,
+                  const CoreHook& after_core) {
   const R1cs& rc = blake3_r1cs(n_log);
   int m = rc.m;
   const LigeritoConfig& cfg = ligerito_config(m);
@@ -734,6 +775,9 @@ Bundle prove(const std::vector<Compression>& blocks, int n_log, const std::strin
   LcClaim lc;
   bd.lc = lincheck_prove(z, m, rc, zc.z, x_inner, x_outer, ch, lc);
 
+  std::vector<DirectClaim> direct;
+  if (after_core) direct = after_core(ch, z);
+
   // claims: ab at (r_inner_skip, r_inner_rest ++ x_outer); c at (z, r_rest)
   std::vector<F128> xab = lc.r_inner_rest;
   xab.insert(xab.end(), x_outer.begin(), x_outer.end());
@@ -751,8 +795,53 @@ Bundle prove(const std::vector<Compression>& blocks, int n_log, const std::strin
   par_for(bc.size(), [&](size_t i0, size_t i1, int) {
     for (size_t i = i0; i < i1; i++) bc[i] = g0 * rs0[i] + g1 * rs1[i];
   });
+  for (const DirectClaim& d : direct) {
+    ch.observe_label("flock-pcs-packed-direct-v0");
+    ch.observe_f128(d.value);
+  }
+  std::vector<F128> gd;
+  for (size_t k = 0; k < direct.size(); k++) gd.push_back(ch.sample_f128());
+  for (size_t k = 0; k < direct.size(); k++) {
+    const DirectClaim& d = direct[k];
+    if (d.point.size() != (size_t)(m - 7)) throw std::runtime_error("packed-direct point length");
+    target += gd[k] * d.value;
+    std::vector<size_t> live;
+    std::vector<F128> live_coords;
+    for (size_t i = 0; i < d.point.size(); i++)
+      if (!d.point[i].is_zero()) { live.push_back(i); live_coords.push_back(d.point[i]); }
+    std::vector<F128> t = build_eq(live_coords);
+    for (size_t c = 0; c < t.size(); c++) {
+      size_t idx = 0;
+      for (size_t j = 0; j < live.size(); j++) idx |= ((c >> j) & 1) << live[j];
+      bc[idx] += gd[k] * t[c];
+    }
+  }
+  if (after_core) last_open_identity_ok() = open_identity(z, bc, target);
   bd.lig = ligerito_prove(cfg, z, bc, target, l0, ch);
   return bd;
+}
+
+Bundle prove(const std::vector<Compression>& blocks, int n_log, const std::string& domain) {
+  return prove_with(blocks, n_log, domain, CoreHook());
+}
+
+// sum_j b_combined[j] * z_packed[j] == target: the batched open's claim, which
+// the Ligerito sumcheck then proves (pcs.rs:130-290)
+bool open_identity(const std::vector<F128>& z, const std::vector<F128>& bc, F128 target) {
+  std::vector<F128> part(par_threads(), ZERO);
+  par_for(z.size(), [&](size_t i0, size_t i1, int ti) {
+    F128 acc = ZERO;
+    for (size_t i = i0; i < i1; i++) acc += bc[i] * z[i];
+    part[ti] = acc;
+  });
+  F128 s = ZERO;
+  for (const F128& p : part) s += p;
+  return s == target;
+}
+
+bool& last_open_identity_ok() {
+  static thread_local bool ok = false;
+  return ok;
 }
 
 }  // namespace flockref

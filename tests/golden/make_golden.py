@@ -16,8 +16,17 @@
    compressions (one trial each), so the GPU prover is pinned at the
    benchmark's full size.
 
+5. chain_proofs.json (--chain) — sha256 of the oracle's BLAKE3 hash-chain
+   bundles (Blake3Setup::prove_chain) over the flock_chain CLI's honest
+   chains at 2^14, 2^16 and 2^18 compressions.  The reference's trusted
+   verifier checks only the compression statement, so these are pinned by
+   the oracle's own checks, recorded per entry: the shift argument verified
+   from the public endpoints (chain.rs:238-300) and the batched open's claim
+   identity sum_j b_combined[j] z[j] = target.  Needs no reference checkout.
+
 Usage (needs the reference checkout and a built oracle):
     python tests/golden/make_golden.py /root/reference [--large]
+    python tests/golden/make_golden.py --chain
 """
 import hashlib
 import json
@@ -87,7 +96,29 @@ def witness_digests() -> None:
     (HERE / "witness_digests.json").write_text(json.dumps(rows, indent=1))
 
 
+def chain_proofs(sizes=(14, 16, 18), threads=8) -> None:
+    import os
+    os.environ["FLOCKREF_THREADS"] = str(threads)
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle_lib
+    orc = oracle_lib.Oracle()
+    out = []
+    for log2 in sizes:
+        seed = 0x5EED0000 + log2
+        records = orc.chain_blocks(seed, 1 << log2)
+        data, ok = orc.prove_chain(records, b"flock_chain-cli")
+        assert ok, log2
+        out.append({"log2": log2, "seed": seed, "initial_cv": "blake3 IV", "domain": "flock_chain-cli",
+                    "sha256": hashlib.sha256(data).hexdigest(), "size": len(data),
+                    "checked_by": "oracle: shift argument verified from the public endpoints; "
+                                  "batched-open claim identity"})
+        (HERE / "chain_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
+
+
 if __name__ == "__main__":
+    if "--chain" in sys.argv:
+        chain_proofs()
+        sys.exit(0)
     ref = Path(sys.argv[1])
     if "--large" in sys.argv:
         # full-size cases (the benchmark's 2^18 among them), one trial each:

@@ -57,6 +57,9 @@ class Oracle:
         L.flockref_ch_grind.restype = u64
         L.flockref_ch_digest.argtypes = [vp, vp]
         L.flockref_pow_ok.argtypes = [vp, u64, u32]
+        L.flockref_chain_blocks.argtypes = [u64, vp, sz, vp]
+        L.flockref_prove_chain_blocks.argtypes = [vp, u32, ctypes.c_char_p, sz, vp, vp, sz, ctypes.POINTER(sz),
+                                                  ctypes.POINTER(ctypes.c_int)]
         L.flockref_time_prove.argtypes = [u32, u64, ctypes.POINTER(sz)]
         L.flockref_time_prove.restype = ctypes.c_double
         self.L = L
@@ -67,6 +70,28 @@ class Oracle:
         rc = self.L.flockref_prove(log2, seed, _p(buf), buf.size, ctypes.byref(n))
         assert rc == 0, rc
         return buf[: n.value].tobytes()
+
+    def chain_blocks(self, seed: int, steps: int, initial_cv=None) -> np.ndarray:
+        """(steps, 28) u32 records of the flock_chain CLI's honest chain."""
+        out = np.zeros((steps, 28), np.uint32)
+        cv = None if initial_cv is None else _p(np.ascontiguousarray(initial_cv, np.uint32))
+        self.L.flockref_chain_blocks(seed, cv, steps, _p(out))
+        return out
+
+    def prove_chain(self, records: np.ndarray, domain: bytes, cv_last=None) -> tuple:
+        """(chain bundle bytes, check): check is True when the shift argument
+        verifies from the bundle's public endpoints and the batched open's
+        claim identity holds."""
+        records = np.ascontiguousarray(records, np.uint32)
+        log2 = records.shape[0].bit_length() - 1
+        buf = np.zeros(1 << 21, np.uint8)
+        n = ctypes.c_size_t()
+        chk = ctypes.c_int(-1)
+        cvl = None if cv_last is None else _p(np.ascontiguousarray(cv_last, np.uint32))
+        rc = self.L.flockref_prove_chain_blocks(_p(records), log2, domain, len(domain), cvl, _p(buf), buf.size,
+                                                ctypes.byref(n), ctypes.byref(chk))
+        assert rc == 0, rc
+        return buf[: n.value].tobytes(), chk.value == 1
 
     def f128_mul(self, a, b):
         a = np.ascontiguousarray(a, np.uint64)
