@@ -427,6 +427,26 @@ def chain_report(prover, log2: int, steps: int = 5) -> dict:
                       "h2d_bytes_per_proof": n * 112, "phases_ms": {k: round(v, 3) for k, v in ph.items()}}}
 
 
+def verify_report(prover, log2: int, reps: int = 3) -> dict:
+    """The verifier behind flock_verify on this setup: one compression proof
+    and one chain proof of 2^log2 compressions, host wall clock per call
+    (median of `reps`); the lincheck's matrix combination runs on the GPU."""
+    import flockgpu
+    proof = prover.prove_seed(0x7E57)
+    chain = prover.prove_chain(flockgpu.chain_blocks(0x7E57, 1 << log2))
+    out = {}
+    for name, b, dom in (("compression", proof, flockgpu.DOMAIN), ("chain", chain, flockgpu.CHAIN_DOMAIN)):
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            why = prover.verify(b, dom)
+            ts.append(time.perf_counter() - t0)
+            if why:
+                raise SystemExit(f"verify_report: {name} proof rejected: {why}")
+        out[f"{name}_ms"] = pct(ts, 0.5) * 1e3
+    return {"verify": {"log2": log2, **out, "threads": 1}}
+
+
 def run_ours(args, world, rank, local):
     import flockgpu
     log2 = args.log2
@@ -497,6 +517,7 @@ def run_ours(args, world, rank, local):
                                                     "144 IMAD.WIDE per product"}
     if world == 1 and not args.no_chain:
         line.update(chain_report(prover, log2))
+        line.update(verify_report(prover, log2))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     if world == 1 and not args.no_serve:

@@ -163,6 +163,27 @@ int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const u
   });
 }
 
+int flock_verify(flock_setup* s, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen) {
+  if (!s || !bytes || (!domain && dlen)) return FLOCK_ERR_ARG;
+  return guard(s->ctx, [&] {
+    const std::string why = s->s->verify(bytes, len, std::string((const char*)domain, dlen));
+    if (why.empty()) return (int)FLOCK_OK;
+    s->ctx->err = "verify: " + why;
+    return (int)FLOCK_ERR_VERIFY;
+  });
+}
+
+int flock_serve_verify(flock_ctx* c, int on) {
+  if (!c) return FLOCK_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (!c->server) {
+    c->err = "serving not started";
+    return FLOCK_ERR_ARG;
+  }
+  c->server->set_verify(on != 0);
+  return FLOCK_OK;
+}
+
 int flock_chain_blocks(uint64_t seed, const uint32_t* initial_cv, size_t steps, uint32_t* records) {
   if (!records && steps) return FLOCK_ERR_ARG;
   static const uint32_t kIV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,

@@ -13,6 +13,7 @@
 //    fixint; enum = u32 variant index; Vec = u64 length).
 #include "host.hpp"
 #include <algorithm>
+#include <set>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -489,6 +490,38 @@ const Ladder* ladder_for(int m) {
     return &(cache[m] = l);
   }
   return nullptr;
+}
+
+std::vector<size_t> sample_distinct_queries(Transcript& tr, size_t block_len, size_t count) {
+  std::vector<size_t> q;
+  std::set<size_t> seen;
+  while (q.size() < count) {
+    size_t v = (size_t)(tr.sample().lo % block_len);
+    if (seen.insert(v).second) q.push_back(v);
+  }
+  std::sort(q.begin(), q.end());
+  return q;
+}
+
+size_t ceil_log2(size_t n) {
+  if (n <= 1) return 0;
+  size_t v = n - 1, l = 0;
+  while (v) { l++; v >>= 1; }
+  return l;
+}
+
+std::vector<f128> small_consts() {
+  const f128* P = phi8_table();
+  return {P[0xF7], P[0x53], P[0xB5]};
+}
+
+std::vector<f128> medium_consts() {
+  std::vector<f128> v;
+  for (int sh : {1, 2, 4, 8}) {
+    f128 g = mk(1ull << sh, 0);
+    v.push_back(hmul(g, hinv(fx(hone(), g))));
+  }
+  return v;
 }
 
 // ---------------------------------------------------------------- encode --

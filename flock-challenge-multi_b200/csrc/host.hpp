@@ -57,6 +57,16 @@ class Transcript {
   B3 h_;
 };
 
+// Ligerito query positions: `count` distinct values sample().lo % block_len,
+// first occurrences kept, sorted (pcs/ligerito.rs:9665-9718)
+std::vector<size_t> sample_distinct_queries(Transcript& tr, size_t block_len, size_t count);
+size_t ceil_log2(size_t n);
+// the zerocheck's fixed inner challenges (univariate_skip_optimized.rs:198-215):
+// phi8(0xF7), phi8(0x53), phi8(0xB5) and gamma^(2^i) / (1 + gamma^(2^i)),
+// gamma = x, i = 1, 2, 4, 8 as shifts
+std::vector<f128> small_consts();
+std::vector<f128> medium_consts();
+
 // ---- R1CS statement for 2^n_log BLAKE3 compressions ----
 constexpr int kKLog = 14, kK = 1 << kKLog, kKSkip = 6, kZConst = 512, kUseful = 15409;
 struct Statement {

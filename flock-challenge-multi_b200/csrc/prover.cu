@@ -29,24 +29,6 @@ T* dalloc(size_t n) {
   return p;
 }
 
-std::vector<f128> small_consts() {  // phi8(0xF7), phi8(0x53), phi8(0xB5)
-  const f128* P = phi8_table();
-  return {P[0xF7], P[0x53], P[0xB5]};
-}
-std::vector<f128> medium_consts() {  // gamma^(2^i) / (1 + gamma^(2^i))
-  std::vector<f128> v;
-  for (int sh : {1, 2, 4, 8}) {
-    f128 g = mk(1ull << sh, 0);
-    v.push_back(hmul(g, hinv(fx(hone(), g))));
-  }
-  return v;
-}
-size_t ceil_log2(size_t n) {
-  if (n <= 1) return 0;
-  size_t v = n - 1, l = 0;
-  while (v) { l++; v >>= 1; }
-  return l;
-}
 }  // namespace
 
 // ---------------------------------------------------------------- setup --
@@ -365,14 +347,7 @@ uint64_t Setup::grind(Transcript& tr, uint32_t bits) {
 }
 
 std::vector<size_t> Setup::sample_queries(Transcript& tr, size_t block_len, size_t count) {
-  std::vector<size_t> q;
-  std::set<size_t> seen;
-  while (q.size() < count) {
-    size_t v = (size_t)(tr.sample().lo % block_len);
-    if (seen.insert(v).second) q.push_back(v);
-  }
-  std::sort(q.begin(), q.end());
-  return q;
+  return sample_distinct_queries(tr, block_len, count);
 }
 
 // Opened rows + Merkle multi-proof (merkle.rs:1074-1120 index order).  The

@@ -2,6 +2,7 @@
 // compressions, the statement (CSC matrices on the device), constant tables
 // and the proof entry point.
 #pragma once
+#include <functional>
 #include <string>
 #include <vector>
 #include "host.hpp"
@@ -31,6 +32,17 @@ struct ChainEnds {
   uint32_t cv0[8], cv_last[8];
 };
 
+// What the verifier needs of a statement: its size, digest, and the
+// lincheck's matrix combination alpha A^T eq + B^T eq (+ beta at the constant
+// column) for eq = L(z_skip) (x) eq(x_inner) (lincheck.rs:5940-5960).
+struct VerifyStatement {
+  int m = 0;
+  std::array<uint8_t, 32> digest{};
+  std::function<std::vector<f128>(f128 z_skip, const std::vector<f128>& x_inner, f128 alpha, f128 beta)> comb;
+};
+// "" when the bundle verifies, otherwise the name of the failed check
+std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& domain, const VerifyStatement& V);
+
 struct Level {
   int lanes = 0, log_msg_pos = 0, rate = 0;
   size_t positions = 0;
@@ -55,6 +67,11 @@ class Setup {
   // then holds 2^log2 records of 28 u32 (cv, m, counter u64, block_len, flags).
   std::vector<uint8_t> prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
                              const std::string& domain, bool committed = false, const ChainEnds* chain = nullptr);
+  // Replays and checks a FLOCK v4 bundle of this statement size (compression
+  // or hash chain; a chain's public endpoints are the bundle's); "" when it
+  // verifies, otherwise the name of the failed check.  Uses this setup's
+  // device statement and stream.
+  std::string verify(const uint8_t* bytes, size_t len, const std::string& domain);
   void phase_times(double* ms) const;
   // device bytes a setup for 2^log2 compressions holds (an upper estimate,
   // used for admission before allocating)

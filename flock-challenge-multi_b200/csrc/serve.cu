@@ -24,6 +24,15 @@ Server::~Server() {
   if (batch_st_) cudaStreamDestroy(batch_st_);
 }
 
+void Server::self_check(Setup& s, const std::string& domain, JobResult& r) {
+  if (!verify_) return;
+  const std::string why = s.verify(r.bytes.data(), r.bytes.size(), domain);
+  if (!why.empty()) {
+    r.status = FLOCK_ERR_VERIFY;
+    r.error = "self-check failed: " + why;
+  }
+}
+
 std::vector<JobResult> Server::prove_batch(const std::vector<BatchItem>& jobs, int threads) {
   std::lock_guard<std::mutex> bl(batch_mu_);
   cudaSetDevice(device_);
@@ -92,6 +101,7 @@ std::vector<JobResult> Server::prove_batch(const std::vector<BatchItem>& jobs, i
             r.bytes = S.prove(&job.seed, nullptr, 0, job.domain, true);
           }
           r.status = FLOCK_OK;
+          self_check(S, job.domain, r);
         } catch (const CudaError& e) {
           r.status = FLOCK_ERR_CUDA;
           r.error = e.what();
@@ -272,6 +282,7 @@ void Server::worker() {
           r.bytes = s->prove(&job.seed, nullptr, 0, job.domain);
         }
         r.status = FLOCK_OK;
+        self_check(*s, job.domain, r);
       } catch (const CudaError& e) {
         r.status = FLOCK_ERR_CUDA;
         r.error = e.what();

@@ -8,6 +8,7 @@
 // cached setups within the HBM budget, evicting idle setups of other sizes
 // (least recently used first) when a new size needs room.
 #pragma once
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdint>
@@ -58,6 +59,9 @@ class Server {
   };
   std::vector<JobResult> prove_batch(const std::vector<BatchItem>& jobs, int threads);
 
+  // self-check: verify every proof on its own setup before returning it; a
+  // proof that fails gets FLOCK_ERR_VERIFY and the failed check's name
+  void set_verify(bool on) { verify_ = on; }
   int slots() const { return (int)workers_.size(); }
   uint64_t budget() const { return budget_; }
   uint64_t cached_bytes();
@@ -79,6 +83,7 @@ class Server {
   };
 
   void worker();
+  void self_check(Setup& s, const std::string& domain, JobResult& r);
   // wait: block until memory frees up (else return nullptr when it does not fit now)
   std::unique_ptr<Setup> acquire(uint32_t log2, std::unique_lock<std::mutex>& lk, bool wait = true);
   void release(std::unique_ptr<Setup> s);
@@ -94,6 +99,7 @@ class Server {
   int busy_ = 0;                                  // setups held by proofs in flight
   uint64_t next_ticket_ = 1, use_clock_ = 0;
   bool stop_ = false;
+  std::atomic<bool> verify_{false};
   std::vector<std::thread> workers_;
   std::mutex batch_mu_;  // one batch at a time
   cudaStream_t batch_st_ = nullptr;

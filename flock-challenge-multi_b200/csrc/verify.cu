@@ -1,0 +1,768 @@
+// Verifier of FLOCK v4 bundles for the self-checking prover: the compression
+// statement (Blake3Setup::verify -> verifier::verify_ligerito,
+// crates/flock-core/src/verifier.rs:95-232) and the hash-chain statement
+// (Blake3Setup::verify_chain, r1cs_hashes/blake3.rs:5217-5240 ->
+// chain_common.rs:355-420).  It replays the transcript and checks, in the
+// reference verifier's order:
+//  * the zerocheck rounds and its final product (zerocheck.rs:1642-1797);
+//  * the lincheck rounds against the folded matrix combination
+//    (lincheck.rs:5876-6050) -- the one O(statement) step, which runs on
+//    this setup's device copy of the block matrices with the prover's own
+//    comb kernel (k_lc_comb);
+//  * for chains, the shift argument from the public endpoints
+//    (chain.rs:238-300);
+//  * each ring switch's claim (ring_switch.rs:4783-4811), the batched open's
+//    target (pcs.rs:1861-1990) and the Ligerito proof
+//    (pcs/ligerito.rs:11321-11834): proof-of-work nonces, Merkle
+//    multi-proofs of every opened row (merkle.rs:1122-1190), the induced
+//    sums, and the final inner product against the residual basis, whose
+//    ring-switch part is evaluated in the 128 x 128 tensor algebra
+//    (pcs/tensor_algebra.rs, ring_switch.rs:4864-4935).
+#include "prover.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+namespace flock {
+namespace {
+
+const uint32_t kB3IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
+                           0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
+
+// ---------------------------------------------------------------- decode --
+struct Rd {
+  const uint8_t* p;
+  size_t n, i = 0;
+  bool bad = false;
+  bool need(size_t k) {
+    if (bad || n - i < k) bad = true;
+    return !bad;
+  }
+  uint64_t u64() {
+    if (!need(8)) return 0;
+    uint64_t v = 0;
+    for (int k = 0; k < 8; k++) v |= (uint64_t)p[i + k] << (8 * k);
+    i += 8;
+    return v;
+  }
+  uint32_t u32() {
+    if (!need(4)) return 0;
+    uint32_t v = 0;
+    for (int k = 0; k < 4; k++) v |= (uint32_t)p[i + k] << (8 * k);
+    i += 4;
+    return v;
+  }
+  f128 f() {
+    uint64_t lo = u64(), hi = u64();
+    return mk(lo, hi);
+  }
+  H32 h() {
+    H32 v{};
+    if (need(32)) { memcpy(v.data(), p + i, 32); i += 32; }
+    return v;
+  }
+  // a length prefix, bounded by what the remaining bytes can hold
+  size_t len(size_t elem_bytes) {
+    uint64_t v = u64();
+    if (bad || v > (n - i) / elem_bytes) { bad = true; return 0; }
+    return (size_t)v;
+  }
+  std::vector<f128> fs() {
+    std::vector<f128> v(len(16));
+    for (auto& x : v) x = f();
+    return v;
+  }
+  std::vector<H32> hs() {
+    std::vector<H32> v(len(32));
+    for (auto& x : v) x = h();
+    return v;
+  }
+  std::vector<std::pair<f128, f128>> pairs() {
+    std::vector<std::pair<f128, f128>> v(len(32));
+    for (auto& x : v) { x.first = f(); x.second = f(); }
+    return v;
+  }
+  std::vector<uint64_t> u64s() {
+    std::vector<uint64_t> v(len(8));
+    for (auto& x : v) x = u64();
+    return v;
+  }
+  Opening open() {
+    Opening o;
+    o.rows.resize(len(8));
+    for (auto& r : o.rows) r = fs();
+    o.proof = hs();
+    return o;
+  }
+  bool bits256(uint32_t cv[8]) {
+    if (u64() != 256 || !need(256)) return false;
+    memset(cv, 0, 32);
+    for (int b = 0; b < 256; b++) {
+      uint8_t v = p[i + b];
+      if (v > 1) return false;
+      cv[b / 32] |= (uint32_t)v << (b % 32);
+    }
+    i += 256;
+    return true;
+  }
+};
+
+// FLOCK v4 R1csProofBundleLigerito (flavor 2) or ChainProofBundleLigerito
+// (flavor 3), the inverse of encode()
+bool decode(const uint8_t* bytes, size_t n, Proof& P, std::string& why) {
+  Rd r{bytes, n};
+  if (n < 7 || memcmp(bytes, "FLOCK", 5) != 0) return why = "bad magic", false;
+  if (bytes[5] != 4) return why = "unsupported version", false;
+  if (bytes[6] != 2 && bytes[6] != 3) return why = "unknown flavor", false;
+  r.i = 7;
+  P.chain = bytes[6] == 3;
+  if (P.chain && r.u32() != 0) return why = "hash kind is not BLAKE3", false;
+  P.root = r.h();
+  P.m = r.u64();
+  if (r.u64() != 1 || r.u64() != 6 || r.u32() != 0 || r.u32() != 1)
+    return why = "PCS parameters are not (rate 1/2, batch 2^6, Fast, BLAKE3)", false;
+  P.r1_ab = r.fs();
+  P.r1_c = r.fs();
+  P.zc_rounds = r.pairs();
+  P.fa = r.f();
+  P.fb = r.f();
+  P.fc = r.f();
+  P.lc_rounds = r.pairs();
+  P.z_partial = r.fs();
+  if (P.chain) {
+    P.shift_rounds = r.pairs();
+    P.g_at_point = r.f();
+  }
+  P.s_hat_v.resize(r.len(8));
+  for (auto& v : P.s_hat_v) v = r.fs();
+  P.lig_root = r.h();
+  P.initial = r.open();
+  P.roots = r.hs();
+  P.levels.resize(r.len(16));
+  for (auto& l : P.levels) l = r.open();
+  P.yr = r.fs();
+  P.final_open = r.open();
+  P.sc_msgs = r.pairs();
+  P.grind_nonces = r.u64s();
+  P.ood = r.fs();
+  P.fold_nonces = r.u64s();
+  if (P.chain && (!r.bits256(P.cv0) || !r.bits256(P.cv_last))) return why = "chain endpoints", false;
+  if (r.bad) return why = "truncated", false;
+  if (r.i != n) return why = "trailing bytes", false;
+  return true;
+}
+
+// ----------------------------------------------------------- field utils --
+bool feq(f128 a, f128 b) { return a.lo == b.lo && a.hi == b.hi; }
+f128 ip(const f128* a, const f128* b, size_t n) {
+  f128 s = mk(0, 0);
+  for (size_t i = 0; i < n; i++) s = fx(s, hmul(a[i], b[i]));
+  return s;
+}
+f128 eq_eval(const f128* a, const f128* b, size_t n) {
+  f128 acc = hone();
+  for (size_t i = 0; i < n; i++) acc = hmul(acc, fx(hone(), fx(a[i], b[i])));
+  return acc;
+}
+// eq(pt, y) for a boolean y given by its bits
+f128 eq_binary(const f128* pt, size_t n, uint64_t y) {
+  f128 acc = hone();
+  for (size_t j = 0; j < n; j++) acc = hmul(acc, (y >> j) & 1 ? pt[j] : fx(hone(), pt[j]));
+  return acc;
+}
+// Lagrange interpolation at z from the 64 values on the Lambda nodes, over
+// Lambda alone (interpolate_at_z_on_lambda) and over S u Lambda with zeros on
+// S (interpolate_at_z_combined), zerocheck/multilinear.rs:410-535
+f128 interp_lambda(const std::vector<f128>& v, f128 z) {
+  std::vector<f128> w = hlagrange(z, 64);
+  return ip(w.data(), v.data(), 64);
+}
+f128 interp_combined(const std::vector<f128>& v, f128 z) {
+  const f128* P = phi8_table();
+  f128 acc = mk(0, 0);
+  for (int i = 0; i < 64; i++) {
+    const int node = 64 + i;
+    f128 num = hone(), den = hone();
+    for (int j = 0; j < 128; j++) {
+      if (j == node) continue;
+      num = hmul(num, fx(z, P[j]));
+      den = hmul(den, fx(P[node], P[j]));
+    }
+    acc = fx(acc, hmul(hmul(num, hinv(den)), v[i]));
+  }
+  return acc;
+}
+// ----------------------------------------------------- tensor algebra --
+// An element of F128 (x) F128 as 128 rows; transpose swaps the two factors
+// (bit j of row i <-> bit i of row j), pcs/tensor_algebra.rs.
+struct TA {
+  f128 e[128];
+};
+void ta_transpose(TA& t) {
+  uint64_t lo[128], hi[128];
+  for (int j = 0; j < 128; j++) {
+    uint64_t l = 0, h = 0;
+    const int w = j >> 6, b = j & 63;
+    for (int i = 0; i < 64; i++) l |= (((w ? t.e[i].hi : t.e[i].lo) >> b) & 1) << i;
+    for (int i = 64; i < 128; i++) h |= (((w ? t.e[i].hi : t.e[i].lo) >> b) & 1) << (i - 64);
+    lo[j] = l;
+    hi[j] = h;
+  }
+  for (int j = 0; j < 128; j++) t.e[j] = mk(lo[j], hi[j]);
+}
+void ta_scale(TA& t, f128 s) {
+  for (auto& x : t.e) x = hmul(x, s);
+}
+f128 ta_fold_vertical(TA t, const std::vector<f128>& c) {
+  ta_transpose(t);
+  return ip(t.e, c.data(), 128);
+}
+// eval_rs_eq_prefix: start at 1 (vertical); per coordinate
+// t += t * z (vertical) + t * q (horizontal)
+TA rs_eq_prefix(const f128* zv, const f128* q, size_t n) {
+  TA t;
+  for (auto& x : t.e) x = mk(0, 0);
+  t.e[0] = hone();
+  for (size_t i = 0; i < n; i++) {
+    TA v = t, h = t;
+    ta_scale(v, zv[i]);
+    ta_transpose(h);
+    ta_scale(h, q[i]);
+    ta_transpose(h);
+    for (int k = 0; k < 128; k++) t.e[k] = fx(t.e[k], fx(v.e[k], h.e[k]));
+  }
+  return t;
+}
+
+// ------------------------------------------------------- BLAKE3 Merkle --
+H32 cv_bytes(const uint32_t w[8]) {
+  H32 h;
+  for (int i = 0; i < 8; i++)
+    for (int k = 0; k < 4; k++) h[4 * i + k] = (uint8_t)(w[i] >> (8 * k));
+  return h;
+}
+// non-root chaining value of a leaf of at most one chunk (merkle.rs:192-197)
+H32 leaf_cv(const uint8_t* d, size_t len) {
+  uint32_t cv[8], out[16], m[16];
+  memcpy(cv, kB3IV, 32);
+  const size_t nb = std::max<size_t>(1, (len + 63) / 64);
+  for (size_t b = 0; b < nb; b++) {
+    uint8_t blk[64] = {0};
+    const size_t off = 64 * b, bl = std::min<size_t>(64, len - off);
+    memcpy(blk, d + off, bl);
+    for (int i = 0; i < 16; i++) m[i] = (uint32_t)blk[4 * i] | (uint32_t)blk[4 * i + 1] << 8 |
+                                       (uint32_t)blk[4 * i + 2] << 16 | (uint32_t)blk[4 * i + 3] << 24;
+    const uint32_t flags = (b == 0 ? 1u : 0u) | (b + 1 == nb ? 2u : 0u);
+    b3_compress(cv, m, 0, (uint32_t)bl, flags, out);
+    memcpy(cv, out, 32);
+  }
+  return cv_bytes(cv);
+}
+H32 parent_cv(const H32& l, const H32& r) {
+  uint32_t m[16], out[16];
+  for (int i = 0; i < 8; i++) {
+    m[i] = (uint32_t)l[4 * i] | (uint32_t)l[4 * i + 1] << 8 | (uint32_t)l[4 * i + 2] << 16 | (uint32_t)l[4 * i + 3] << 24;
+    m[8 + i] = (uint32_t)r[4 * i] | (uint32_t)r[4 * i + 1] << 8 | (uint32_t)r[4 * i + 2] << 16 |
+               (uint32_t)r[4 * i + 3] << 24;
+  }
+  b3_compress(kB3IV, m, 0, 64, 4 /*PARENT*/, out);
+  return cv_bytes(out);
+}
+// verify_merkle_multi_proof (merkle.rs:1122-1190)
+bool merkle_multi_verify(const H32& root, size_t n_leaves, const std::vector<size_t>& pos,
+                         const std::vector<H32>& leaves, const std::vector<H32>& proof) {
+  if (n_leaves == 0 || (n_leaves & (n_leaves - 1)) || pos.size() != leaves.size()) return false;
+  if (pos.empty()) return proof.empty();
+  for (size_t i = 0; i < pos.size(); i++)
+    if (pos[i] >= n_leaves || (i && pos[i - 1] >= pos[i])) return false;
+  if (n_leaves == 1) return proof.empty() && leaves[0] == root;
+  std::vector<std::pair<size_t, H32>> act;
+  for (size_t i = 0; i < pos.size(); i++) act.push_back({pos[i], leaves[i]});
+  size_t pi = 0;
+  for (size_t ll = n_leaves; ll > 1; ll >>= 1) {
+    std::vector<std::pair<size_t, H32>> nx;
+    for (size_t i = 0; i < act.size();) {
+      const size_t p = act[i].first;
+      H32 l, r;
+      if (i + 1 < act.size() && act[i + 1].first == (p ^ 1)) {
+        l = act[i].second;
+        r = act[i + 1].second;
+        i += 2;
+      } else {
+        if (pi >= proof.size()) return false;
+        const H32& sib = proof[pi++];
+        if (p & 1) { l = sib; r = act[i].second; }
+        else { l = act[i].second; r = sib; }
+        i += 1;
+      }
+      nx.push_back({p >> 1, parent_cv(l, r)});
+    }
+    act.swap(nx);
+  }
+  return pi == proof.size() && act.size() == 1 && act[0].second == root;
+}
+// verify_level_opens (pcs/ligerito.rs:12441-12468): rows of `lanes` values
+bool level_opens_ok(const H32& root, size_t block_len, const std::vector<size_t>& q, const Opening& o,
+                    size_t lanes) {
+  if (q.size() != o.rows.size()) return false;
+  std::vector<H32> leaves;
+  for (const auto& row : o.rows) {
+    if (row.size() != lanes || lanes * 16 > 1024) return false;
+    leaves.push_back(leaf_cv(reinterpret_cast<const uint8_t*>(row.data()), lanes * 16));
+  }
+  return merkle_multi_verify(root, block_len, q, leaves, o.proof);
+}
+
+// ---------------------------------------------------- transcript checks --
+// FsChallenger::verify_pow (challenger.rs:502-545): the BLAKE3 hash of
+// state digest || nonce (LE) || 0^24 has `bits` leading zero bits (bits = 0:
+// the nonce is 0); the nonce is observed either way
+bool pow_ok(Transcript& tr, uint64_t nonce, uint32_t bits) {
+  bool ok = true;
+  if (bits == 0) {
+    ok = nonce == 0;
+  } else {
+    uint8_t pre[64] = {0}, h[32];
+    tr.state_digest(pre);
+    for (int i = 0; i < 8; i++) pre[32 + i] = (uint8_t)(nonce >> (8 * i));
+    B3 b;
+    b.update(pre, 64);
+    b.digest(h);
+    for (uint32_t k = 0; k < bits && ok; k++) ok = ((h[k / 8] >> (7 - k % 8)) & 1) == 0;
+  }
+  tr.nonce(nonce);
+  return ok;
+}
+
+// A Ligerito round's quadratic from its message (u0, u2) and running claim
+// (pcs/ligerito.rs:4929-4958)
+struct Quad {
+  f128 c, b, a;
+  static Quad from(std::pair<f128, f128> msg, f128 claim) { return {msg.first, fx(claim, msg.second), msg.second}; }
+  f128 eval(f128 r) const { return fx(c, fx(hmul(r, b), hmul(hmul(r, r), a))); }
+  static Quad fold(const Quad& p, const Quad& q, f128 al) {
+    return {fx(p.c, hmul(al, q.c)), fx(p.b, hmul(al, q.b)), fx(p.a, hmul(al, q.a))};
+  }
+};
+
+// s_{k+1}(x) = s_k(x)^2 + s_k(v_k) s_k(x); the subspace polynomials at the
+// basis points (pcs/ligerito.rs:1186-1210)
+f128 next_s(f128 s, f128 root) { return fx(hmul(s, s), hmul(root, s)); }
+std::vector<f128> eval_sk_at_vks(int log_n) {
+  std::vector<f128> sks((size_t)log_n + 1, mk(0, 0));
+  sks[0] = hone();
+  if (log_n == 0) return sks;
+  std::vector<f128> layer;
+  for (int i = 1; i <= log_n; i++) layer.push_back(mk(1ull << i, 0));
+  int cur = log_n;
+  for (int i = 0; i < log_n; i++) {
+    for (int j = 0; j < cur; j++) {
+      f128 v = next_s(layer[j], sks[i]);
+      if (j == 0) sks[i + 1] = v;
+      else layer[j - 1] = v;
+    }
+    cur--;
+  }
+  return sks;
+}
+// induce_sumcheck_enforced_sum (pcs/ligerito.rs:1310-1335)
+f128 enforced_sum(const Opening& o, const std::vector<f128>& v, const std::vector<size_t>& q,
+                  const std::vector<f128>& alpha) {
+  std::vector<f128> eq = heq(v), aw = heq(alpha);
+  f128 s = mk(0, 0);
+  for (size_t i = 0; i < o.rows.size(); i++) s = fx(s, hmul(aw[i], ip(o.rows[i].data(), eq.data(), eq.size())));
+  return s;
+}
+// induce_sumcheck_evaluate_at_residual (pcs/ligerito.rs:1346-1435)
+std::vector<f128> induce_residual(int log_msg_cols, const std::vector<size_t>& q, const std::vector<f128>& alpha,
+                                  const f128* ris, int prefix_len, int yr_log_n) {
+  std::vector<f128> sks = eval_sk_at_vks(log_msg_cols), inv(sks.size());
+  for (size_t i = 0; i < sks.size(); i++) inv[i] = (sks[i].lo | sks[i].hi) ? hinv(sks[i]) : mk(0, 0);
+  std::vector<f128> aw = heq(alpha);
+  std::vector<f128> out((size_t)1 << yr_log_n, mk(0, 0));
+  for (size_t i = 0; i < q.size(); i++) {
+    std::vector<f128> sx((size_t)log_msg_cols);
+    if (log_msg_cols > 0) {
+      sx[0] = mk((uint64_t)q[i], 0);
+      for (int k = 1; k < log_msg_cols; k++) sx[k] = next_s(sx[k - 1], sks[k - 1]);
+      for (int k = 0; k < log_msg_cols; k++) sx[k] = hmul(sx[k], inv[k]);
+    }
+    f128 pre = hone();
+    for (int k = 0; k < prefix_len; k++) pre = hmul(pre, fx(hone(), hmul(ris[k], fx(hone(), sx[k]))));
+    const f128 w = hmul(aw[i], pre);
+    for (size_t y = 0; y < out.size(); y++) {
+      f128 suf = hone();
+      for (int j = 0; j < yr_log_n; j++)
+        if ((y >> j) & 1) suf = hmul(suf, sx[(size_t)prefix_len + j]);
+      out[y] = fx(out[y], hmul(w, suf));
+    }
+  }
+  return out;
+}
+
+// shift_mle (chain.rs:75-100)
+f128 shift_mle(const std::vector<f128>& a, const std::vector<f128>& b) {
+  const size_t n = a.size();
+  std::vector<f128> pre(n + 1, hone()), suf(n + 1, hone());
+  for (size_t j = 0; j < n; j++) pre[j + 1] = hmul(pre[j], hmul(a[j], fx(hone(), b[j])));
+  for (size_t j = n; j-- > 0;) suf[j] = hmul(suf[j + 1], fx(hone(), fx(a[j], b[j])));
+  f128 acc = mk(0, 0);
+  for (size_t j = 0; j < n; j++) acc = fx(acc, hmul(hmul(pre[j], hmul(fx(hone(), a[j]), b[j])), suf[j + 1]));
+  return acc;
+}
+// tau_pos-MLE of a public chaining value over its two packed positions
+// (fold_public_phys, chain_common.rs:84-118)
+f128 fold_cv(const uint32_t cv[8], f128 tp) {
+  const f128 p0 = mk((uint64_t)cv[0] | (uint64_t)cv[1] << 32, (uint64_t)cv[2] | (uint64_t)cv[3] << 32);
+  const f128 p1 = mk((uint64_t)cv[4] | (uint64_t)cv[5] << 32, (uint64_t)cv[6] | (uint64_t)cv[7] << 32);
+  return fx(hmul(fx(hone(), tp), p0), hmul(tp, p1));
+}
+
+struct RsClaim {
+  f128 z_skip, value;
+  std::vector<f128> x;  // x_inner_rest ++ x_outer
+};
+
+}  // namespace
+
+// ------------------------------------------------------------- verify --
+std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& domain, const VerifyStatement& V) {
+  Proof P;
+  std::string why;
+  if (!decode(bytes, len, P, why)) return "malformed bundle: " + why;
+  const int m = V.m, n_log = V.m - kKLog;
+  if (P.m != (uint64_t)m) return "bundle is for another statement size";
+  const Ladder* lad = ladder_for(m);
+  if (!lad) return "no Ligerito configuration for this size";
+  const Ladder& Ld = *lad;
+  Transcript tr(domain);
+  tr.label("flock-r1cs-v0");
+  tr.bytes(V.digest.data(), 32);
+  tr.bytes(P.root.data(), 32);
+
+  // ---- zerocheck
+  const int ks = kKSkip, n_mlv = m - kKSkip;
+  if (P.r1_ab.size() != 64 || P.r1_c.size() != 64 || P.zc_rounds.size() != (size_t)n_mlv)
+    return "zerocheck: malformed";
+  tr.label("flock-zerocheck-v0");
+  std::vector<f128> r = tr.sample_vec(ks), r_outer = tr.sample_vec((size_t)(m - ks - 7));
+  for (f128 v : small_consts()) r.push_back(v);
+  for (f128 v : medium_consts()) r.push_back(v);
+  r.insert(r.end(), r_outer.begin(), r_outer.end());
+  tr.f128s(P.r1_ab.data(), 64);
+  tr.f128s(P.r1_c.data(), 64);
+  const f128 zz = tr.sample();
+  const f128 pc = interp_lambda(P.r1_c, zz);
+  if (!feq(pc, P.fc)) return "zerocheck: c evaluation";
+  std::vector<f128> comb_l(64);
+  for (int i = 0; i < 64; i++) comb_l[i] = fx(P.r1_ab[i], P.r1_c[i]);
+  f128 run = fx(interp_combined(comb_l, zz), pc);
+  std::vector<f128> rhos;
+  for (int i = 0; i < n_mlv; i++) {
+    const f128 req = r[(size_t)(ks + i)], g1 = P.zc_rounds[i].first, gi = P.zc_rounds[i].second;
+    const f128 g0 = hmul(fx(run, hmul(req, g1)), hinv(fx(hone(), req)));
+    tr.f128v(g1);
+    tr.f128v(gi);
+    const f128 rho = tr.sample();
+    rhos.push_back(rho);
+    const f128 opr = fx(hone(), rho);
+    run = fx(fx(hmul(g0, opr), hmul(g1, rho)), hmul(gi, hmul(rho, opr)));
+  }
+  if (!feq(run, hmul(P.fa, P.fb))) return "zerocheck: final product";
+  tr.f128v(P.fa);
+  tr.f128v(P.fb);
+
+  // ---- lincheck: comb = alpha A^T eq + B^T eq (+ beta at the constant
+  // column) over the block's 2^14 columns, built on the device
+  const int ir = kKLog - kKSkip;
+  if (P.lc_rounds.size() != (size_t)ir || P.z_partial.size() != 64) return "lincheck: malformed";
+  std::vector<f128> x_inner(rhos.begin(), rhos.begin() + ir), x_outer(rhos.begin() + ir, rhos.end());
+  tr.label("flock-lincheck-v0");
+  const f128 alpha = tr.sample();
+  const f128 beta = tr.sample();
+  std::vector<f128> cv = V.comb(zz, x_inner, alpha, beta);
+  if (cv.size() != (size_t)kK) return "lincheck: matrix combination";
+  run = fx(fx(hmul(alpha, P.fa), P.fb), beta);
+  std::vector<f128> rr;
+  for (const auto& rd : P.lc_rounds) {
+    tr.f128v(rd.first);
+    tr.f128v(rd.second);
+    const f128 rk = tr.sample();
+    const f128 e0 = fx(run, rd.first), c1 = fx(fx(e0, rd.first), rd.second);
+    run = fx(fx(hmul(rd.second, hmul(rk, rk)), hmul(c1, rk)), e0);
+    const size_t h = cv.size() / 2;
+    for (size_t i = 0; i < h; i++) cv[i] = fx(cv[i], hmul(rk, fx(cv[i + h], cv[i])));
+    cv.resize(h);
+    rr.push_back(rk);
+  }
+  tr.f128s(P.z_partial.data(), 64);
+  if (!feq(run, ip(cv.data(), P.z_partial.data(), 64))) return "lincheck: final sum";
+  const f128 r_inner_skip = tr.sample();
+  std::vector<f128> lam = hlagrange(r_inner_skip, 0);
+  const f128 w = ip(lam.data(), P.z_partial.data(), 64);
+
+  RsClaim cl[2];
+  cl[0].z_skip = r_inner_skip;
+  cl[0].value = w;
+  cl[0].x.assign(rr.rbegin(), rr.rend());
+  cl[0].x.insert(cl[0].x.end(), x_outer.begin(), x_outer.end());
+  cl[1].z_skip = zz;
+  cl[1].value = P.fc;
+  cl[1].x.assign(r.begin() + ks, r.end());
+
+  // ---- hash chain: tau_pos, the shift argument from the public endpoints
+  std::vector<f128> pd_point;
+  if (P.chain) {
+    const f128 tp = tr.sample_vec(1)[0];
+    const size_t n = (size_t)n_log;
+    if (P.shift_rounds.size() != n + 1) return "chain: malformed shift proof";
+    std::vector<f128> tau = tr.sample_vec(n);
+    const f128 al = tr.sample();
+    f128 tprod = hone();
+    for (f128 t : tau) tprod = hmul(tprod, t);
+    f128 claim = fx(hmul(tprod, fold_cv(P.cv_last, tp)), hmul(al, fold_cv(P.cv0, tp)));
+    std::vector<f128> rs;
+    for (const auto& rd : P.shift_rounds) {
+      tr.f128v(rd.first);
+      tr.f128v(rd.second);
+      const f128 rk = tr.sample();
+      const f128 e0 = fx(claim, rd.first), c1 = fx(fx(e0, rd.first), rd.second);
+      claim = fx(fx(hmul(rd.second, hmul(rk, rk)), hmul(c1, rk)), e0);
+      rs.push_back(rk);
+    }
+    std::vector<f128> full(n + 1);
+    for (size_t k = 0; k <= n; k++) full[n - k] = rs[k];
+    std::vector<f128> taup(full.begin(), full.begin() + n), zero(n, mk(0, 0));
+    const f128 s0 = full[n], ops0 = fx(hone(), s0);
+    const f128 wf = fx(fx(hmul(shift_mle(tau, taup), ops0), hmul(eq_eval(tau.data(), taup.data(), n), s0)),
+                       hmul(hmul(al, eq_eval(taup.data(), zero.data(), n)), ops0));
+    if (!feq(claim, hmul(wf, P.g_at_point))) return "chain: shift argument";
+    pd_point.assign(7 + n, mk(0, 0));
+    pd_point[0] = tp;
+    pd_point[1] = s0;
+    for (size_t i = 0; i < n; i++) pd_point[7 + i] = taup[i];
+  }
+
+  // ---- batched open: ring switches, the packed-direct claim, the target
+  if (P.s_hat_v.size() != 2) return "open: expected two ring-switched claims";
+  tr.label("flock-pcs-open-batch-v0");
+  std::vector<f128> eqd[2];
+  f128 sc[2];
+  for (int k = 0; k < 2; k++) {
+    const std::vector<f128>& sv = P.s_hat_v[k];
+    if (sv.size() != 128) return "ring switch: malformed";
+    tr.label("flock-ring-switch-v0");
+    tr.f128s(sv.data(), 128);
+    // claim weights: L_i(z_skip) eq(x[0], bit 6) (ring_switch.rs:138-160)
+    std::vector<f128> L = hlagrange(cl[k].z_skip, 0);
+    f128 chk = mk(0, 0);
+    for (int i = 0; i < 128; i++)
+      chk = fx(chk, hmul(hmul(L[i & 63], (i >> 6) ? cl[k].x[0] : fx(hone(), cl[k].x[0])), sv[i]));
+    if (!feq(chk, cl[k].value)) return "ring switch: claim";
+    eqd[k] = heq(tr.sample_vec(7));
+    TA u;
+    for (int i = 0; i < 128; i++) u.e[i] = sv[i];
+    ta_transpose(u);
+    sc[k] = ip(u.e, eqd[k].data(), 128);
+  }
+  const f128 gam[2] = {tr.sample(), tr.sample()};
+  f128 target = fx(hmul(gam[0], sc[0]), hmul(gam[1], sc[1]));
+  f128 gpd = mk(0, 0);
+  if (P.chain) {
+    tr.label("flock-pcs-packed-direct-v0");
+    tr.f128v(P.g_at_point);
+    gpd = tr.sample();
+    target = fx(target, hmul(gpd, P.g_at_point));
+  }
+
+  // ---- Ligerito (recursive_verifier_with_basis_succinct)
+  const int log_n = m - 7, ik = Ld.initial_k, rsteps = (int)Ld.ks.size();
+  if (!Ld.ood.empty() && Ld.ood[0] != 0) return "ligerito: config";
+  if (P.lig_root != P.root) return "ligerito: initial root";
+  tr.label("flock-ligerito-basis-v0");
+  tr.f128v(target);
+  tr.bytes(P.root.data(), 32);
+  size_t tx = 0, fi = 0, oi = 0, ni = 0;
+  auto next_msg = [&](std::pair<f128, f128>& msg) {
+    if (tx >= P.sc_msgs.size()) return false;
+    msg = P.sc_msgs[tx++];
+    tr.f128v(msg.first);
+    tr.f128v(msg.second);
+    return true;
+  };
+  auto ood_n = [&](int lvl) { return lvl < (int)Ld.ood.size() ? Ld.ood[lvl] : 0; };
+  auto fold_bits = [&](int lvl, int j) { return lvl < (int)Ld.fold_grind.size() ? std::max(0, Ld.fold_grind[lvl] - j) : 0; };
+  f128 t_r = target;
+  std::pair<f128, f128> msg;
+  if (!next_msg(msg)) return "ligerito: transcript length";
+  Quad quad = Quad::from(msg, t_r);
+  struct OodCtx { std::vector<f128> z; size_t ris_start; f128 beta; };
+  struct LevelCtx { int log_msg_cols; std::vector<size_t> q; std::vector<f128> alpha; size_t ris_start; f128 beta; };
+  std::vector<OodCtx> oods;
+  std::vector<LevelCtx> lvls;
+  std::vector<f128> ris;
+  auto fold_rounds = [&](int lvl, int count, std::vector<f128>& out_rs) {
+    for (int j = 0; j < count; j++) {
+      const int bits = fold_bits(lvl, j);
+      if (bits > 0) {
+        if (fi >= P.fold_nonces.size() || !pow_ok(tr, P.fold_nonces[fi++], (uint32_t)bits)) return false;
+      }
+      const f128 ri = tr.sample();
+      ris.push_back(ri);
+      out_rs.push_back(ri);
+      t_r = quad.eval(ri);
+      if (!next_msg(msg)) return false;
+      quad = Quad::from(msg, t_r);
+    }
+    return true;
+  };
+  auto ood_round = [&](int count, int nvars) {
+    for (int s = 0; s < count; s++) {
+      std::vector<f128> zp = tr.sample_vec((size_t)nvars);
+      if (oi >= P.ood.size()) return false;
+      const f128 y = P.ood[oi++];
+      tr.f128v(y);
+      if (!next_msg(msg)) return false;
+      const Quad iq = Quad::from(msg, y);
+      const f128 be = tr.sample();
+      quad = Quad::fold(quad, iq, be);
+      t_r = fx(t_r, hmul(be, y));
+      oods.push_back({zp, ris.size(), be});
+    }
+    return true;
+  };
+  std::vector<f128> lane_rs;
+  if (!fold_rounds(0, ik, lane_rs)) return "ligerito: L0 fold rounds";
+  if (P.roots.empty()) return "ligerito: roots";
+  tr.bytes(P.roots[0].data(), 32);
+  // OOD samples of the folded message (ris holds the initial_k lane folds)
+  if (!ood_round(ood_n(1), log_n - ik)) return "ligerito: OOD";
+  if (ni >= P.grind_nonces.size() || !pow_ok(tr, P.grind_nonces[ni++], (uint32_t)Ld.grind[0]))
+    return "ligerito: L0 proof of work";
+  const size_t block0 = (size_t)1 << (log_n - ik + Ld.rate[0]);
+  std::vector<size_t> q0 = sample_distinct_queries(tr, block0, (size_t)Ld.queries[0]);
+  std::vector<f128> a0 = tr.sample_vec(ceil_log2((size_t)Ld.queries[0]));
+  if (!level_opens_ok(P.root, block0, q0, P.initial, (size_t)1 << ik)) return "ligerito: L0 openings";
+  const int n1 = log_n - ik;
+  {
+    const f128 es = enforced_sum(P.initial, lane_rs, q0, a0);
+    if (!next_msg(msg)) return "ligerito: transcript length";
+    const Quad iq = Quad::from(msg, es);
+    const f128 be = tr.sample();
+    quad = Quad::fold(quad, iq, be);
+    t_r = fx(t_r, hmul(be, es));
+    lvls.push_back({n1, q0, a0, (size_t)ik, be});
+  }
+  H32 prev_root = P.roots[0];
+  if (rsteps < 1) return "ligerito: config";
+  int prev_lni = Ld.ks[0], prev_lmc = n1 - Ld.ks[0], prev_rate = Ld.rate[1];
+  size_t next_root = 1, rp = 0;
+  int n_cur = n1;
+  for (int i = 0; i < rsteps; i++) {
+    const int k_i = Ld.ks[i];
+    if (n_cur < k_i) return "ligerito: config";
+    std::vector<f128> level_rs;
+    if (!fold_rounds(i + 1, k_i, level_rs)) return "ligerito: fold rounds";
+    n_cur -= k_i;
+    if (i == rsteps - 1) {
+      if (tx != P.sc_msgs.size() || oi != P.ood.size() || fi != P.fold_nonces.size())
+        return "ligerito: transcript length";
+      if (P.yr.size() != ((size_t)1 << n_cur)) return "ligerito: final message length";
+      for (f128 v : P.yr) tr.f128v(v);
+      if (ni >= P.grind_nonces.size() || !pow_ok(tr, P.grind_nonces[ni++], (uint32_t)Ld.grind[i + 1]))
+        return "ligerito: final proof of work";
+      const size_t pbl = (size_t)1 << (prev_lmc + prev_rate);
+      std::vector<size_t> ql = sample_distinct_queries(tr, pbl, (size_t)Ld.queries[i + 1]);
+      std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
+      if (!level_opens_ok(prev_root, pbl, ql, P.final_open, (size_t)1 << prev_lni)) return "ligerito: final openings";
+      const f128 es = enforced_sum(P.final_open, level_rs, ql, al);
+      const f128 be = tr.sample();
+      t_r = fx(t_r, hmul(be, es));
+      lvls.push_back({n_cur, ql, al, ris.size(), be});
+      const int yr_log_n = n_cur;
+      const size_t yl = P.yr.size();
+      std::vector<f128> comb_y(yl, mk(0, 0));
+      for (const LevelCtx& c : lvls) {
+        std::vector<f128> res = induce_residual(c.log_msg_cols, c.q, c.alpha, ris.data() + c.ris_start,
+                                                c.log_msg_cols - yr_log_n, yr_log_n);
+        for (size_t y = 0; y < yl; y++) comb_y[y] = fx(comb_y[y], hmul(c.beta, res[y]));
+      }
+      for (const OodCtx& c : oods) {
+        const size_t folded = c.z.size() - (size_t)yr_log_n;
+        if (c.z.size() < (size_t)yr_log_n || c.ris_start + folded > ris.size()) return "ligerito: OOD context";
+        f128 sca = c.beta;
+        for (size_t b = 0; b < folded; b++) sca = hmul(sca, fx(hone(), fx(c.z[b], ris[c.ris_start + b])));
+        std::vector<f128> tail = heq(std::vector<f128>(c.z.begin() + (long)folded, c.z.end()));
+        for (size_t y = 0; y < yl; y++) comb_y[y] = fx(comb_y[y], hmul(tail[y], sca));
+      }
+      // the combined basis b at (ris, y): the ring-switched claims in the
+      // tensor algebra, the packed-direct claim as an eq evaluation
+      const size_t pl = ris.size();
+      if (pl + (size_t)yr_log_n != (size_t)log_n) return "ligerito: residual arity";
+      for (int k = 0; k < 2; k++) {
+        const TA pre = rs_eq_prefix(cl[k].x.data() + 1, ris.data(), pl);
+        const f128* suf = cl[k].x.data() + 1 + pl;
+        for (size_t y = 0; y < yl; y++) {
+          f128 s = hone();
+          for (int j = 0; j < yr_log_n; j++) s = hmul(s, (y >> j) & 1 ? suf[j] : fx(hone(), suf[j]));
+          TA t = pre;
+          ta_scale(t, s);
+          comb_y[y] = fx(comb_y[y], hmul(gam[k], ta_fold_vertical(t, eqd[k])));
+        }
+      }
+      if (P.chain) {
+        const f128 pre = eq_eval(pd_point.data(), ris.data(), pl);
+        for (size_t y = 0; y < yl; y++)
+          comb_y[y] = fx(comb_y[y], hmul(hmul(gpd, pre), eq_binary(pd_point.data() + pl, (size_t)yr_log_n, y)));
+      }
+      const f128 inner = ip(P.yr.data(), comb_y.data(), yl);
+      if (!feq(inner, t_r)) return "ligerito: final inner product";
+      return "";
+    }
+    if (next_root >= P.roots.size()) return "ligerito: roots";
+    const H32 root_next = P.roots[next_root++];
+    tr.bytes(root_next.data(), 32);
+    if (!ood_round(ood_n(i + 2), n_cur)) return "ligerito: OOD";
+    if (ni >= P.grind_nonces.size() || !pow_ok(tr, P.grind_nonces[ni++], (uint32_t)Ld.grind[i + 1]))
+      return "ligerito: level proof of work";
+    const size_t pbl = (size_t)1 << (prev_lmc + prev_rate);
+    std::vector<size_t> qi = sample_distinct_queries(tr, pbl, (size_t)Ld.queries[i + 1]);
+    std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
+    if (rp >= P.levels.size()) return "ligerito: level openings missing";
+    const Opening& o = P.levels[rp++];
+    if (!level_opens_ok(prev_root, pbl, qi, o, (size_t)1 << prev_lni)) return "ligerito: level openings";
+    const f128 es = enforced_sum(o, level_rs, qi, al);
+    if (!next_msg(msg)) return "ligerito: transcript length";
+    const Quad iq = Quad::from(msg, es);
+    const f128 be = tr.sample();
+    quad = Quad::fold(quad, iq, be);
+    t_r = fx(t_r, hmul(be, es));
+    lvls.push_back({n_cur, qi, al, ris.size(), be});
+    prev_root = root_next;
+    if (i + 1 >= rsteps || n_cur < Ld.ks[i + 1]) return "ligerito: config";
+    prev_lni = Ld.ks[i + 1];
+    prev_lmc = n_cur - Ld.ks[i + 1];
+    prev_rate = Ld.rate[(size_t)i + 2];
+  }
+  return "ligerito: config";
+}
+
+// The device half of the verifier: the lincheck's matrix combination over
+// this setup's CSC copy of the block matrices, with the prover's kernels.
+std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& domain) {
+  VerifyStatement V;
+  V.m = m;
+  V.digest = digest;
+  V.comb = [this](f128 zskip, const std::vector<f128>& x_inner, f128 alpha, f128 beta) {
+    std::vector<f128> L = hlagrange(zskip, 0), cv(kK);
+    eq_build(x_inner.data(), (int)x_inner.size(), hone(), zv_pre, st);
+    outer64(L.data(), zv_pre, (size_t)1 << x_inner.size(), eq_inner, st);
+    lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, kZConst, comb, st);
+    CK(cudaMemcpyAsync(cv.data(), comb, kK * sizeof(f128), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return cv;
+  };
+  return verify_bundle(bytes, len, domain, V);
+}
+
+}  // namespace flock

@@ -28,10 +28,11 @@ EXPORTS = (
     "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove", "flock_merkle_root_noalloc",
     "flock_serve_start", "flock_submit", "flock_poll", "flock_sumcheck_round3", "flock_bench_sumcheck3",
     "flock_ntt_autotune", "flock_ntt_rs_encode_plan", "flock_prove_batch", "flock_host_alloc",
-    "flock_host_free", "flock_prove_chain", "flock_chain_blocks",
+    "flock_host_free", "flock_prove_chain", "flock_chain_blocks", "flock_verify", "flock_serve_verify",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
+FLOCK_ERR_VERIFY = 6
 
 
 class FlockJob(ctypes.Structure):
@@ -94,6 +95,8 @@ def load() -> ctypes.CDLL:
         lib.flock_prove_batch.argtypes = [vp, ctypes.POINTER(FlockJob), sz, ctypes.POINTER(FlockResult), i32]
         lib.flock_prove_chain.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_chain_blocks.argtypes = [u64, vp, sz, vp]
+        lib.flock_verify.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
+        lib.flock_serve_verify.argtypes = [vp, i32]
         _lib = lib
     return _lib
 
@@ -189,6 +192,10 @@ class Context:
     # ---- serving (continuous batching of proof jobs) ----
     def serve_start(self, slots: int = 4) -> None:
         self._check(self.lib.flock_serve_start(self.h, slots), "serve_start")
+
+    def serve_verify(self, on: bool = True) -> None:
+        """Self-check every served / batched proof with the verifier."""
+        self._check(self.lib.flock_serve_verify(self.h, 1 if on else 0), "serve_verify")
 
     def submit(self, log2: int, seed: int = 0, blocks=None, domain: bytes = None) -> int:
         """Queue one proof; returns its ticket.  blocks: (2^log2, 25) u32 or None."""
@@ -382,6 +389,17 @@ class Prover:
                                             _ptr(self._buf), self._buf.size, ctypes.byref(n))
         self.ctx._check(rc, "prove_chain")
         return self._buf[: n.value].tobytes()
+
+    def verify(self, bundle: bytes, domain: bytes = DOMAIN) -> str:
+        """'' when the FLOCK v4 bundle (compression or chain) verifies on this
+        setup's statement, otherwise the name of the failed check."""
+        rc = self.ctx.lib.flock_verify(self.h, bundle, len(bundle), domain, len(domain))
+        if rc == 0:
+            return ""
+        if rc == FLOCK_ERR_VERIFY:
+            return self.ctx.lib.flock_last_error(self.ctx.h).decode()
+        self.ctx._check(rc, "verify")
+        return "error"
 
     def bench(self, seed0: int, steps: int):
         """(total device ms of `steps` proofs, mean per-phase ms, kernel launches)."""

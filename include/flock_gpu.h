@@ -22,6 +22,9 @@
  *                           + ChainProofBundleLigerito::to_bytes (blake3.rs:
  *                           5195-5215, r1cs_hashes/chain_common.rs:287-350,
  *                           proof_io.rs:144-157, 943-950)
+ *  - flock_verify        <- Blake3Setup::verify / verify_chain on a decoded
+ *                           bundle (blake3.rs:5129-5145, 5217-5240;
+ *                           crates/flock-core/src/verifier.rs:95-232)
  *  - flock_chain_blocks  <- the flock_chain CLI's honest BLAKE3 chain
  *                           (crates/flock-prover/src/bin/flock_chain.rs:178-193,
  *                           236-260)
@@ -56,7 +59,8 @@ enum {
   FLOCK_ERR_CUDA = 2,
   FLOCK_ERR_CAPACITY = 3,
   FLOCK_ERR_INTERNAL = 4,
-  FLOCK_ERR_TIMEOUT = 5
+  FLOCK_ERR_TIMEOUT = 5,
+  FLOCK_ERR_VERIFY = 6
 };
 enum { FLOCK_HASH_BLAKE3 = 1 };
 enum { FLOCK_PROFILE_FAST = 0 };
@@ -92,6 +96,18 @@ int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const u
  * flags 0; x_{i+1} = out_lo(compress(record i)).  Runs on the host (each link
  * needs the previous output). */
 int flock_chain_blocks(uint64_t seed, const uint32_t* initial_cv, size_t steps, uint32_t* records);
+/* Verify a FLOCK v4 bundle of this setup's size: a compression proof
+ * (flavor 2) or a hash-chain proof (flavor 3, whose public endpoints are the
+ * ones the bundle carries), under the transcript domain it was proved with.
+ * Returns FLOCK_OK, or FLOCK_ERR_VERIFY with flock_last_error() naming the
+ * failed check.  The lincheck's matrix combination runs on the GPU; the rest
+ * (transcript replay, Merkle openings, proof of work, residual basis) on the
+ * calling thread. */
+int flock_verify(flock_setup* s, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen);
+/* Self-checking serving: with on != 0, every proof served by flock_submit /
+ * flock_prove_batch is verified on its setup before it is returned, and one
+ * that fails gets status FLOCK_ERR_VERIFY.  Call after flock_serve_start. */
+int flock_serve_verify(flock_ctx* ctx, int on);
 /* Page-locked host memory for inputs and outputs: flock_prove_blocks copies
  * compressions from such a buffer at the full host-to-device rate (a
  * pageable buffer is staged by the CUDA runtime first).  No counterpart in
