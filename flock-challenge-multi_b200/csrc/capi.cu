@@ -186,10 +186,8 @@ int flock_serve_verify(flock_ctx* c, int on) {
 
 int flock_chain_blocks(uint64_t seed, const uint32_t* initial_cv, size_t steps, uint32_t* records) {
   if (!records && steps) return FLOCK_ERR_ARG;
-  static const uint32_t kIV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
-                                  0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
   uint32_t cv[8];
-  memcpy(cv, initial_cv ? initial_cv : kIV, sizeof(cv));
+  memcpy(cv, initial_cv ? initial_cv : flock::kB3IV, sizeof(cv));
   uint64_t x = seed;
   for (size_t i = 0; i < steps; i++) {
     uint32_t* r = records + 28 * i;

@@ -100,7 +100,7 @@ std::vector<f128> hlagrange(f128 z, int base) {
 uint8_t hgf8_mul(uint8_t a, uint8_t b) { return gf8_mul_slow(a, b); }
 
 // --------------------------------------------------------------- BLAKE3 --
-static const uint32_t kIV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
+const uint32_t kB3IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
                                 0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
 static inline uint32_t ror(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
 
@@ -111,7 +111,7 @@ void b3_compress(const uint32_t cv[8], const uint32_t m[16], uint64_t ctr, uint3
                                   {0, 5, 10, 15}, {1, 6, 11, 12}, {2, 7, 8, 13}, {3, 4, 9, 14}};
   uint32_t s[16], w[16];
   memcpy(s, cv, 32);
-  memcpy(s + 8, kIV, 16);
+  memcpy(s + 8, kB3IV, 16);
   s[12] = (uint32_t)ctr;
   s[13] = (uint32_t)(ctr >> 32);
   s[14] = blen;
@@ -139,7 +139,7 @@ static void le_words(const uint8_t* b, uint32_t w[16]) {
   for (int i = 0; i < 16; i++) w[i] = (uint32_t)b[4 * i] | (uint32_t)b[4 * i + 1] << 8 | (uint32_t)b[4 * i + 2] << 16 | (uint32_t)b[4 * i + 3] << 24;
 }
 
-B3::B3() { memcpy(cv_, kIV, 32); }
+B3::B3() { memcpy(cv_, kB3IV, 32); }
 
 void B3::chunk_done() {
   uint32_t w[16], out[16];
@@ -153,12 +153,12 @@ void B3::chunk_done() {
     memcpy(blk, stack_.back().data(), 32);
     memcpy(blk + 8, cv.data(), 32);
     stack_.pop_back();
-    b3_compress(kIV, blk, 0, 64, 4 /*PARENT*/, out);
+    b3_compress(kB3IV, blk, 0, 64, 4 /*PARENT*/, out);
     memcpy(cv.data(), out, 32);
     total >>= 1;
   }
   stack_.push_back(cv);
-  memcpy(cv_, kIV, 32);
+  memcpy(cv_, kB3IV, 32);
   nblk_ = 0;
   blen_ = 0;
 }
@@ -201,7 +201,7 @@ void B3::xof(uint8_t* out, size_t n) const {
     memcpy(pw + 8, o, 32);
     for (int k = 0; k < 16; k++)
       for (int j = 0; j < 4; j++) blk[4 * k + j] = (uint8_t)(pw[k] >> (8 * j));
-    memcpy(cv, kIV, 32);
+    memcpy(cv, kB3IV, 32);
     blen = 64;
     ctr = 0;
     flags = 4;
@@ -351,7 +351,7 @@ Statement build() {
   ident_rows(TLO, 128);  // counter lo/hi, block_len, flags are contiguous
   std::array<SymWord, 16> st;
   for (int w = 0; w < 8; w++) st[w] = SymWord::slots(CV0 + 32 * w);
-  for (int i = 0; i < 4; i++) st[8 + i] = SymWord::konst(kIV[i]);
+  for (int i = 0; i < 4; i++) st[8 + i] = SymWord::konst(kB3IV[i]);
   st[12] = SymWord::slots(TLO);
   st[13] = SymWord::slots(THI);
   st[14] = SymWord::slots(BLEN);

@@ -39,6 +39,7 @@ class B3 {
   std::vector<std::array<uint32_t, 8>> stack_;
 };
 void b3_compress(const uint32_t cv[8], const uint32_t m[16], uint64_t ctr, uint32_t blen, uint32_t flags, uint32_t out[16]);
+extern const uint32_t kB3IV[8];  // the BLAKE3 IV (the SHA-256 initial hash words)
 
 // ---- Fiat-Shamir transcript (challenger.rs:170-600) ----
 class Transcript {

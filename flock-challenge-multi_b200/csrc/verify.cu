@@ -26,9 +26,6 @@
 namespace flock {
 namespace {
 
-const uint32_t kB3IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
-                           0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
-
 // ---------------------------------------------------------------- decode --
 struct Rd {
   const uint8_t* p;
