@@ -19,6 +19,8 @@
 #include <mutex>
 #include <wmmintrin.h>
 #include <emmintrin.h>
+#include <smmintrin.h>
+#include <tmmintrin.h>
 
 namespace flock {
 
@@ -102,42 +104,75 @@ uint8_t hgf8_mul(uint8_t a, uint8_t b) { return gf8_mul_slow(a, b); }
 // --------------------------------------------------------------- BLAKE3 --
 const uint32_t kB3IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
                                 0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
-static inline uint32_t ror(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+
+// One BLAKE3 compression with the 4x4 state held as four SSE rows: the four
+// column G functions run lane-parallel, the rows are rotated so the four
+// diagonal G functions do too, and rotated back (the row-parallel form of the
+// BLAKE3 specification's compression function).  The message schedule of
+// round r is the permutation (2,6,3,10,7,0,4,13,1,11,12,5,9,14,15,8) applied r
+// times.
+namespace {
+struct B3Sched {
+  uint8_t s[7][16];
+  B3Sched() {
+    static const uint8_t P[16] = {2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8};
+    for (int i = 0; i < 16; i++) s[0][i] = (uint8_t)i;
+    for (int r = 1; r < 7; r++)
+      for (int i = 0; i < 16; i++) s[r][i] = s[r - 1][P[i]];
+  }
+};
+const B3Sched kB3Sched;
+inline __m128i rotr16(__m128i x) {
+  return _mm_shuffle_epi8(x, _mm_set_epi8(13, 12, 15, 14, 9, 8, 11, 10, 5, 4, 7, 6, 1, 0, 3, 2));
+}
+inline __m128i rotr8(__m128i x) {
+  return _mm_shuffle_epi8(x, _mm_set_epi8(12, 15, 14, 13, 8, 11, 10, 9, 4, 7, 6, 5, 0, 3, 2, 1));
+}
+inline __m128i rotr12(__m128i x) { return _mm_or_si128(_mm_srli_epi32(x, 12), _mm_slli_epi32(x, 20)); }
+inline __m128i rotr7(__m128i x) { return _mm_or_si128(_mm_srli_epi32(x, 7), _mm_slli_epi32(x, 25)); }
+inline void b3_g(__m128i& r0, __m128i& r1, __m128i& r2, __m128i& r3, __m128i mx, __m128i my) {
+  r0 = _mm_add_epi32(_mm_add_epi32(r0, r1), mx);
+  r3 = rotr16(_mm_xor_si128(r3, r0));
+  r2 = _mm_add_epi32(r2, r3);
+  r1 = rotr12(_mm_xor_si128(r1, r2));
+  r0 = _mm_add_epi32(_mm_add_epi32(r0, r1), my);
+  r3 = rotr8(_mm_xor_si128(r3, r0));
+  r2 = _mm_add_epi32(r2, r3);
+  r1 = rotr7(_mm_xor_si128(r1, r2));
+}
+}  // namespace
 
 void b3_compress(const uint32_t cv[8], const uint32_t m[16], uint64_t ctr, uint32_t blen, uint32_t flags,
                  uint32_t out[16]) {
-  static const uint8_t P[16] = {2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8};
-  static const uint8_t G[8][4] = {{0, 4, 8, 12}, {1, 5, 9, 13}, {2, 6, 10, 14}, {3, 7, 11, 15},
-                                  {0, 5, 10, 15}, {1, 6, 11, 12}, {2, 7, 8, 13}, {3, 4, 9, 14}};
-  uint32_t s[16], w[16];
-  memcpy(s, cv, 32);
-  memcpy(s + 8, kB3IV, 16);
-  s[12] = (uint32_t)ctr;
-  s[13] = (uint32_t)(ctr >> 32);
-  s[14] = blen;
-  s[15] = flags;
-  memcpy(w, m, 64);
+  const __m128i c0 = _mm_loadu_si128(reinterpret_cast<const __m128i*>(cv));
+  const __m128i c1 = _mm_loadu_si128(reinterpret_cast<const __m128i*>(cv + 4));
+  __m128i r0 = c0, r1 = c1;
+  __m128i r2 = _mm_loadu_si128(reinterpret_cast<const __m128i*>(kB3IV));
+  __m128i r3 = _mm_set_epi32((int)flags, (int)blen, (int)(uint32_t)(ctr >> 32), (int)(uint32_t)ctr);
   for (int r = 0; r < 7; r++) {
-    for (int g = 0; g < 8; g++) {
-      uint32_t &a = s[G[g][0]], &b = s[G[g][1]], &c = s[G[g][2]], &d = s[G[g][3]];
-      a += b + w[2 * g];     d = ror(d ^ a, 16);
-      c += d;                b = ror(b ^ c, 12);
-      a += b + w[2 * g + 1]; d = ror(d ^ a, 8);
-      c += d;                b = ror(b ^ c, 7);
-    }
-    uint32_t t[16];
-    for (int i = 0; i < 16; i++) t[i] = w[P[i]];
-    memcpy(w, t, 64);
+    const uint8_t* s = kB3Sched.s[r];
+    // columns: G_g for g = 0..3 takes message words 2g, 2g + 1
+    b3_g(r0, r1, r2, r3, _mm_set_epi32((int)m[s[6]], (int)m[s[4]], (int)m[s[2]], (int)m[s[0]]),
+         _mm_set_epi32((int)m[s[7]], (int)m[s[5]], (int)m[s[3]], (int)m[s[1]]));
+    // diagonals: rotate rows 1, 2, 3 left by 1, 2, 3 lanes
+    r1 = _mm_shuffle_epi32(r1, _MM_SHUFFLE(0, 3, 2, 1));
+    r2 = _mm_shuffle_epi32(r2, _MM_SHUFFLE(1, 0, 3, 2));
+    r3 = _mm_shuffle_epi32(r3, _MM_SHUFFLE(2, 1, 0, 3));
+    b3_g(r0, r1, r2, r3, _mm_set_epi32((int)m[s[14]], (int)m[s[12]], (int)m[s[10]], (int)m[s[8]]),
+         _mm_set_epi32((int)m[s[15]], (int)m[s[13]], (int)m[s[11]], (int)m[s[9]]));
+    r1 = _mm_shuffle_epi32(r1, _MM_SHUFFLE(2, 1, 0, 3));
+    r2 = _mm_shuffle_epi32(r2, _MM_SHUFFLE(1, 0, 3, 2));
+    r3 = _mm_shuffle_epi32(r3, _MM_SHUFFLE(0, 3, 2, 1));
   }
-  for (int i = 0; i < 8; i++) {
-    out[i] = s[i] ^ s[i + 8];
-    out[i + 8] = s[i + 8] ^ cv[i];
-  }
+  _mm_storeu_si128(reinterpret_cast<__m128i*>(out), _mm_xor_si128(r0, r2));
+  _mm_storeu_si128(reinterpret_cast<__m128i*>(out + 4), _mm_xor_si128(r1, r3));
+  _mm_storeu_si128(reinterpret_cast<__m128i*>(out + 8), _mm_xor_si128(r2, c0));
+  _mm_storeu_si128(reinterpret_cast<__m128i*>(out + 12), _mm_xor_si128(r3, c1));
 }
 
-static void le_words(const uint8_t* b, uint32_t w[16]) {
-  for (int i = 0; i < 16; i++) w[i] = (uint32_t)b[4 * i] | (uint32_t)b[4 * i + 1] << 8 | (uint32_t)b[4 * i + 2] << 16 | (uint32_t)b[4 * i + 3] << 24;
-}
+// the host is little endian (x86-64), so a block's words are its bytes
+static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "little-endian host");
+static void le_words(const uint8_t* b, uint32_t w[16]) { memcpy(w, b, 64); }
 
 B3::B3() { memcpy(cv_, kB3IV, 32); }
 
@@ -199,8 +234,7 @@ void B3::xof(uint8_t* out, size_t n) const {
     uint32_t pw[16];
     memcpy(pw, stack_[i].data(), 32);
     memcpy(pw + 8, o, 32);
-    for (int k = 0; k < 16; k++)
-      for (int j = 0; j < 4; j++) blk[4 * k + j] = (uint8_t)(pw[k] >> (8 * j));
+    memcpy(blk, pw, 64);
     memcpy(cv, kB3IV, 32);
     blen = 64;
     ctr = 0;
@@ -210,7 +244,7 @@ void B3::xof(uint8_t* out, size_t n) const {
   for (uint64_t c = 0; n; c++) {
     b3_compress(cv, w, c, blen, flags | 8u /*ROOT*/, o);
     size_t take = std::min<size_t>(n, 64);
-    for (size_t k = 0; k < take; k++) out[k] = (uint8_t)(o[k / 4] >> (8 * (k % 4)));
+    memcpy(out, o, take);
     out += take;
     n -= take;
   }
