@@ -467,6 +467,9 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     size_t n_blocks128 = (size_t)1 << (m - 13);
     zc_round1(a, b, z, tabs_r1, scratch_eq(), n_blocks128, out, sms, st);
     fetch(out, 1024, h_out);
+    // from here on `out` is a ring of 128 zeroed 8-value slots: every round
+    // message accumulates into a fresh slot, so no round needs its own clear
+    CK(cudaMemsetAsync(out, 0, 1024 * sizeof(f128), st));
     // P_AB(l) = sum_k phi8(e_k) H(l, k)
     const f128* phi8 = phi8_table();
     P.r1_ab.assign(64, mk(0, 0));
@@ -513,6 +516,16 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     for (int i = 0; i < 64; i++) ce = fx(ce, hmul(LL[i], P.r1_c[i]));
     P.fc = ce;
   }
+  int out_slot = 0;
+  auto next_out = [&](int nslots) -> f128* {
+    if (out_slot + nslots > 128) {
+      CK(cudaMemsetAsync(out, 0, 1024 * sizeof(f128), st));
+      out_slot = 0;
+    }
+    f128* p = out + 8 * out_slot;
+    out_slot += nslots;
+    return p;
+  };
   const int n_mlv = m - 6;
   std::vector<f128> rhos;
   // Message of round k weights pair j by eq(r[7+k..m], j).  Its low bits sit
@@ -554,9 +567,9 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       etab_len /= 2;
       etab_off += etab_len;
     }
-    CK(cudaMemsetAsync(out, 0, 8 * sizeof(f128), st));
-    zc_round(mode, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, med0 - 9, etab, out, G, st);
-    fetch(out, 8, h_out);
+    f128* o = next_out(1);
+    zc_round(mode, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, med0 - 9, etab, o, G, st);
+    fetch(o, 8, h_out);
     f128 g1 = mk(0, 0), gi = mk(0, 0);
     for (int js = 0; js < (1 << ns); js++) {
       g1 = fx(g1, hmul(K[js], h_out[2 * js]));
@@ -585,8 +598,9 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
         std::swap(bv, bv2);
       }
     } else {
-      fold_pair_final(av, bv, rho, out, st);
-      fetch(out, 2, h_out);
+      f128* o = next_out(1);
+      fold_pair_final(av, bv, rho, o, st);
+      fetch(o, 2, h_out);
       P.fa = h_out[0];
       P.fb = h_out[1];
     }
@@ -615,19 +629,19 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   }
   std::vector<f128> rr;
   int len = kK;
-  // the round kernel adds its message atomically: clear it before each round
-  CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-  lc_round(comb, zv, len, false, mk(0, 0), true, out, st);
+  // the round kernel adds its message atomically into a fresh slot
+  f128* lo_ = next_out(1);
+  lc_round(comb, zv, len, false, mk(0, 0), true, lo_, st);
   for (int k = 0; k < ir; k++) {
-    fetch(out, 2, h_out);
+    fetch(lo_, 2, h_out);
     P.lc_rounds.push_back({h_out[0], h_out[1]});
     tr.f128v(h_out[0]);
     tr.f128v(h_out[1]);
     f128 rk = tr.sample();
     rr.push_back(rk);
     len >>= 1;
-    if (k + 1 < ir) CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-    lc_round(comb, zv, len, true, rk, k + 1 < ir, out, st);
+    if (k + 1 < ir) lo_ = next_out(1);
+    lc_round(comb, zv, len, true, rk, k + 1 < ir, lo_, st);
   }
   P.z_partial.resize(64);
   fetch(zv, 64, P.z_partial.data());
@@ -662,13 +676,13 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     CK(cudaMemcpyAsync(w + 1, w + N, (N - 1) * sizeof(f128), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(w, &alpha, sizeof(f128), cudaMemcpyHostToDevice, st));
     int len = (int)(2 * N);
-    CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-    lc_round(w, g, len, false, mk(0, 0), true, out, st);
+    f128* so = next_out(1);
+    lc_round(w, g, len, false, mk(0, 0), true, so, st);
     std::vector<f128> rs;
     for (int k = 0; k <= n_log; k++) {
       // the last message is over g[0], g[1]; the final fold happens here
       if (k == n_log) CK(cudaMemcpyAsync(h_out + 2, g, 2 * sizeof(f128), cudaMemcpyDeviceToHost, st));
-      fetch(out, 2, h_out);
+      fetch(so, 2, h_out);
       P.shift_rounds.push_back({h_out[0], h_out[1]});
       tr.f128v(h_out[0]);
       tr.f128v(h_out[1]);
@@ -676,8 +690,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       rs.push_back(rk);
       if (k < n_log) {
         len >>= 1;
-        CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-        lc_round(w, g, len, true, rk, true, out, st);
+        so = next_out(1);
+        lc_round(w, g, len, true, rk, true, so, st);
       } else {
         pd_value = fx(h_out[2], hmul(rk, fx(h_out[3], h_out[2])));
       }
@@ -700,9 +714,10 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   {
     std::vector<f128> eqt = heq(std::vector<f128>(r_inner_rest.begin() + 1, r_inner_rest.end()));
     CK(cudaMemcpyAsync(eq_inner, eqt.data(), eqt.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
-    ring_shat_ab(zv_pre, eq_inner, out, st);
+    f128* ro = next_out(16);
+    ring_shat_ab(zv_pre, eq_inner, ro, st);
     std::vector<f128> sv(128);
-    fetch(out, 128, sv.data());
+    fetch(ro, 128, sv.data());
     P.s_hat_v.push_back(sv);
     P.s_hat_v.push_back(s_hat_v_c);
   }
@@ -789,20 +804,21 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   f128* fo = pp[2];
   f128* bo = pp[3];
   size_t flen = n_words;
+  f128* mo = nullptr;  // the slot of the pending message
   auto push_msg = [&]() {
-    fetch(out, 2, h_out);
+    fetch(mo, 2, h_out);
     P.sc_msgs.push_back({h_out[0], h_out[1]});
     tr.f128v(h_out[0]);
     tr.f128v(h_out[1]);
   };
-  CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-  lig_msg(f, bb, flen / 2, out, G, st);
+  mo = next_out(1);
+  lig_msg(f, bb, flen / 2, mo, G, st);
   push_msg();
   auto fold_round = [&](int bits) -> f128 {
     if (bits > 0) P.fold_nonces.push_back(grind(tr, (uint32_t)bits));
     f128 rch = tr.sample();
-    CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-    lig_fold_msg(f, bb, fo, bo, rch, flen / 4, true, out, G, st);
+    mo = next_out(1);
+    lig_fold_msg(f, bb, fo, bo, rch, flen / 4, true, mo, G, st);
     // after the first fold f lives in the ping-pong pair (pp[0], pp[2]) / (pp[1], pp[3])
     if (f == z) { f = fo; fo = pp[0]; }
     else std::swap(f, fo);
@@ -812,8 +828,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     return rch;
   };
   auto introduce = [&](const f128* bnew) {
-    CK(cudaMemsetAsync(out, 0, 2 * sizeof(f128), st));
-    lig_msg(f, bnew, flen / 2, out, G, st);
+    mo = next_out(1);
+    lig_msg(f, bnew, flen / 2, mo, G, st);
     push_msg();
     f128 be = tr.sample();
     axpy(bb, bnew, be, flen, st);
@@ -824,10 +840,10 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       std::vector<f128> zp = tr.sample_vec((size_t)n_cur);
       f128* eqz = scratch_eq();
       eq_table(zp, eqz);
-      CK(cudaMemsetAsync(out, 0, sizeof(f128), st));
-      inner(f, eqz, flen, out, G, st);
+      f128* io = next_out(1);
+      inner(f, eqz, flen, io, G, st);
       f128 y;
-      fetch(out, 1, &y);
+      fetch(io, 1, &y);
       P.ood.push_back(y);
       tr.f128v(y);
       introduce(eqz);
