@@ -114,8 +114,8 @@ void build_round1_tables_host(const uint8_t M[64][64], const f128* phi8, void* d
 void zc_round1(const f128* a, const f128* b, const f128* c, const void* tabs, const f128* eqc, size_t n_blocks,
                f128* out, int grid, cudaStream_t s);
 void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag, f128 rho,
-              size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int grid, cudaStream_t s);
-void eq_halve(const f128* in, f128* out, size_t n_out, cudaStream_t s);
+              size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int grid, cudaStream_t s,
+              f128* halve_out = nullptr, size_t halve_n = 0);
 void fold_pair_final(const f128* a_in, const f128* b_in, f128 rho, f128* out, cudaStream_t s);
 void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
              const f128* eq, f128 alpha, f128 beta, int pin, f128* comb, cudaStream_t s);

@@ -560,15 +560,20 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       }
       K[js] = hmul(phi8_table()[g], C);
     }
-    if (st0 > 13) {  // drop r[st0 - 1]
-      f128* nxt = scratch_eq() + etab_off;
-      eq_halve(etab, nxt, etab_len / 2, st);
-      etab = nxt;
-      etab_len /= 2;
-      etab_off += etab_len;
+    // the next round's table drops r[st0]: this round's launch writes it
+    f128* nxt = nullptr;
+    size_t nxt_len = 0;
+    if (st0 + 1 > 13 && k + 1 < n_mlv) {
+      nxt = scratch_eq() + etab_off;
+      nxt_len = etab_len / 2;
     }
     f128* o = next_out(1);
-    zc_round(mode, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, med0 - 9, etab, o, G, st);
+    zc_round(mode, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, med0 - 9, etab, o, G, st, nxt, nxt_len);
+    if (nxt) {
+      etab = nxt;
+      etab_len = nxt_len;
+      etab_off += nxt_len;
+    }
     fetch(o, 8, h_out);
     f128 g1 = mk(0, 0), gi = mk(0, 0);
     for (int js = 0; js < (1 << ns); js++) {

@@ -42,6 +42,8 @@ struct ZcArgs {
   int ns, nm, msh;
   const f128* etab;  // eq over the random suffix, indexed by group
   f128* out;
+  f128* halve_out;   // next round's table: etab with its lowest variable summed out
+  size_t halve_n;    // (0: none)
 };
 
 __device__ __forceinline__ f128 lag_lookup(const f128* lag, uint64_t row) {
@@ -85,6 +87,8 @@ __global__ void __launch_bounds__(256, 2) k_zc_round(ZcArgs A) {
   } else {
     multab_build(rt, A.rho);
   }
+  for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < A.halve_n; j += (size_t)gridDim.x * blockDim.x)
+    st(A.halve_out + j, fx(ldg(A.etab + 2 * j), ldg(A.etab + 2 * j + 1)));
   const int lane = threadIdx.x & 31;
   const int ns = A.ns, nm = A.nm, gb = ns + nm;
   const int js = lane & ((1 << ns) - 1), gw = lane >> ns;
@@ -169,14 +173,18 @@ __global__ void __launch_bounds__(256, 2) k_zc_round(ZcArgs A) {
 
 // One zerocheck round launch: out[2 js + {0, 1}] ^= (T1, Tinf)(js) for js < 2^ns.
 // mode 0: packed message round, 1: packed fold + message, 2: fold + message.
+// halve_n > 0: also writes halve_out[j] = etab[2j] + etab[2j+1], j < halve_n,
+// the next round's eq table (one launch less per round).
 void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag, f128 rho,
-              size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int grid, cudaStream_t s) {
+              size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int grid, cudaStream_t s,
+              f128* halve_out, size_t halve_n) {
   if (ns < 0 || ns > 2 || nm < 0 || nm > 4 || msh < 0 || (nm > 0 && (((1 << nm) - 1) << msh) >= 64))
     throw CudaError("zc_round: bad eq structure");
   ZcArgs A;
   A.a_in = a_in; A.b_in = b_in; A.a_out = a_out; A.b_out = b_out; A.lag = lag; A.rho = rho;
   A.n_pairs = n_pairs; A.ns = ns; A.nm = nm; A.msh = msh;
   A.etab = etab; A.out = out;
+  A.halve_out = halve_out; A.halve_n = halve_n;
   const size_t smem = mode == 0 ? 2048 * sizeof(f128) : mode == 1 ? 4096 * sizeof(f128) : sizeof(MulTab8);
   const size_t lanes = (n_pairs + ((size_t)1 << nm) - 1) >> nm;
   const int g = (int)std::max<size_t>(1, std::min<size_t>((size_t)grid, (lanes + 255) / 256));
@@ -191,16 +199,4 @@ void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b
     CK(cudaFuncSetAttribute(k_zc_round<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_zc_round<2><<<g, 256, smem, s>>>(A);
   }
-}
-
-__global__ void k_eq_halve(const f128* __restrict__ in, f128* __restrict__ out, size_t n_out) {
-  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < n_out) st(out + j, fx(ldg(in + 2 * j), ldg(in + 2 * j + 1)));
-}
-
-// out[j] = in[2j] + in[2j+1]: eq over r[t+1..] from eq over r[t..] (the
-// dropped variable's two weights sum to one)
-void eq_halve(const f128* in, f128* out, size_t n_out, cudaStream_t s) {
-  count_launch();
-  k_eq_halve<<<(unsigned)((n_out + 255) / 256), 256, 0, s>>>(in, out, n_out);
 }
