@@ -302,6 +302,10 @@ def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: i
         wall = time.perf_counter() - t0
         lat = [r["latency_ms"] for r in res]
         cwall, clat = served_run(ctx, jobs)  # the same jobs through the continuous-batching queue
+        # and once more with every proof verified before it is returned
+        ctx.serve_verify(True)
+        vwall, vlat = served_run(ctx, jobs)
+        ctx.serve_verify(False)
         plain = plain_batch
         out["batched"] = {"jobs": len(jobs), "log2_range": [12, 18], "compressions": n,
                           "value": n / wall, "unit": "compressions/s", "plain_value": n / plain,
@@ -310,7 +314,11 @@ def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: i
                           "form": "flock_prove_batch: fused witness + commit graphs over groups of 8 jobs, "
                                   "each overlapping the earlier groups' remaining phases on concurrent streams",
                           "continuous": {"value": n / cwall, "p50_ms": pct(clat, 0.5), "p99_ms": pct(clat, 0.99),
-                                         "slots": slots}}
+                                         "slots": slots},
+                          "continuous_self_checked": {"value": n / vwall, "p50_ms": pct(vlat, 0.5),
+                                                      "p99_ms": pct(vlat, 0.99), "slots": slots,
+                                                      "form": "every proof verified (flock_verify) before it "
+                                                              "is returned"}}
         jobs = serve_jobs
         n = sum(1 << l for l, _ in jobs)
         served_run(ctx, jobs)  # warm
