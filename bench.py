@@ -477,6 +477,9 @@ def run_ours(args, world, rank, local):
         pa.array[:] = host_blocks(log2, seed_base + 500 + i)
         pinned.append(pa)
     blocks = [pa.array for pa in pinned]
+    # untimed warm-up of this entry point: its first call allocates the
+    # device staging buffer and loads the host-input witness kernel
+    prover.prove_blocks(host_blocks(log2, seed_base + 499))
     barrier(world)
     t0 = time.perf_counter()
     sizes = [len(prover.prove_blocks(b)) for b in blocks]

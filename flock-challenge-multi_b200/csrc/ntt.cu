@@ -57,11 +57,17 @@ __device__ __forceinline__ void ntt_tile(const PassArgs& p, uint64_t t_id, f128*
   const uint64_t hi = t_id >> lo_bits;     // l0 bits
   const int n_el = LG << R;
   // load
+  uint64_t any = 0;
   for (int e = threadIdx.x; e < n_el; e += blockDim.x) {
     uint64_t pl = (uint64_t)(e >> p.lg_shift);
     uint64_t pos = (hi << (log_d - l0)) | (pl << lo_bits) | lo;
     tile[e] = ld(p.data + pos * p.lanes + ((size_t)grp << p.lg_shift) + (e & (LG - 1)));
+    if (TRANSPOSE) any |= tile[e].lo | tile[e].hi;
   }
+  // The transposed transform (the query-basis induction) starts from a vector
+  // that is zero outside the queried positions, and a pass maps a zero tile
+  // to zeros in place: such tiles are left as they are.
+  if (TRANSPOSE && !__syncthreads_or(any != 0)) return;
   for (int k = threadIdx.x; k < (1 << R) - 1; k += blockDim.x) {
     int s = 31 - __clz(k + 1);               // stage
     uint64_t blk = (uint64_t)(k + 1 - (1 << s));
