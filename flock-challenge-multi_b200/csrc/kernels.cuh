@@ -99,6 +99,7 @@ void merkle_top_batch(const BatchJob* jobs, int n_jobs, cudaStream_t s);
 
 // K2 / K9
 void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, cudaStream_t s);
+void merkle_leaves(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* out, cudaStream_t s);
 __global__ void k_gather_nodes(const uint32_t* tree, const uint64_t* idx, size_t n, uint32_t* out);
 __global__ void k_gather_rows(const f128* cw, const uint64_t* pos, size_t n, int lanes, f128* out);
 uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, unsigned long long* d_found,

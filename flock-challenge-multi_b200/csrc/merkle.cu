@@ -100,6 +100,12 @@ __global__ void k_merkle_leaves(const uint8_t* __restrict__ data, size_t leaf_si
   leaf_cv(data + i * leaf_size, leaf_size, tree + 8 * i);
 }
 
+// leaf chaining values only (no tree): out[8 i..8 i + 8) for leaf i
+void merkle_leaves(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* out, cudaStream_t s) {
+  count_launch();
+  k_merkle_leaves<<<(unsigned)((n_leaves + 127) / 128), 128, 0, s>>>((const uint8_t*)data, leaf_size, n_leaves, out);
+}
+
 // the 1 KiB-leaf trees of every job of a batch (leaves, then one parent
 // level for all jobs per launch, then one CTA per job for its top levels)
 __global__ void k_merkle_leaves_batch(const BatchJob* __restrict__ jobs, int n_jobs, uint64_t total) {

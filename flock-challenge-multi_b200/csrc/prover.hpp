@@ -39,6 +39,11 @@ struct VerifyStatement {
   int m = 0;
   std::array<uint8_t, 32> digest{};
   std::function<std::vector<f128>(f128 z_skip, const std::vector<f128>& x_inner, f128 alpha, f128 beta)> comb;
+  // optional: BLAKE3 leaf chaining values of rows packed back to back, group
+  // k holding counts[k] rows of sizes[k] bytes; empty result = hash on the host
+  std::function<std::vector<H32>(const uint8_t* data, const std::vector<size_t>& sizes,
+                                 const std::vector<size_t>& counts)>
+      leaf_cvs;
 };
 // "" when the bundle verifies, otherwise the name of the failed check
 std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& domain, const VerifyStatement& V);

@@ -316,16 +316,52 @@ bool merkle_multi_verify(const H32& root, size_t n_leaves, const std::vector<siz
   }
   return pi == proof.size() && act.size() == 1 && act[0].second == root;
 }
-// verify_level_opens (pcs/ligerito.rs:12441-12468): rows of `lanes` values
+// verify_level_opens (pcs/ligerito.rs:12441-12468): rows of `lanes` values;
+// `cvs`, when given, holds the rows' leaf chaining values already hashed
 bool level_opens_ok(const H32& root, size_t block_len, const std::vector<size_t>& q, const Opening& o,
-                    size_t lanes) {
+                    size_t lanes, const std::vector<H32>* cvs) {
   if (q.size() != o.rows.size()) return false;
   std::vector<H32> leaves;
-  for (const auto& row : o.rows) {
+  for (size_t i = 0; i < o.rows.size(); i++) {
+    const auto& row = o.rows[i];
     if (row.size() != lanes || lanes * 16 > 1024) return false;
-    leaves.push_back(leaf_cv(reinterpret_cast<const uint8_t*>(row.data()), lanes * 16));
+    leaves.push_back(cvs ? (*cvs)[i] : leaf_cv(reinterpret_cast<const uint8_t*>(row.data()), lanes * 16));
   }
   return merkle_multi_verify(root, block_len, q, leaves, o.proof);
+}
+
+// The leaf chaining values of every opened row, per opening (initial,
+// levels, final), through V.leaf_cvs when it is set and the rows are
+// uniform within each opening; empty entries are hashed on the host.
+std::vector<std::vector<H32>> opened_leaf_cvs(const Proof& P, const VerifyStatement& V) {
+  std::vector<const Opening*> ops{&P.initial};
+  for (const Opening& o : P.levels) ops.push_back(&o);
+  ops.push_back(&P.final_open);
+  std::vector<std::vector<H32>> out(ops.size());
+  if (!V.leaf_cvs) return out;
+  std::vector<uint8_t> data;
+  std::vector<size_t> sizes, counts;
+  for (const Opening* o : ops) {
+    size_t sz = o->rows.empty() ? 0 : o->rows[0].size() * 16;
+    bool ok = sz > 0 && sz <= 1024;
+    for (const auto& r : o->rows) ok = ok && r.size() * 16 == sz;
+    sizes.push_back(ok ? sz : 0);
+    counts.push_back(ok ? o->rows.size() : 0);
+    if (!ok) continue;
+    for (const auto& r : o->rows) {
+      const uint8_t* b = reinterpret_cast<const uint8_t*>(r.data());
+      data.insert(data.end(), b, b + sz);
+    }
+  }
+  std::vector<H32> all = V.leaf_cvs(data.data(), sizes, counts);
+  size_t at = 0;
+  for (size_t k = 0; k < ops.size(); k++) {
+    if (!counts[k]) continue;
+    if (at + counts[k] > all.size()) return std::vector<std::vector<H32>>(ops.size());
+    out[k].assign(all.begin() + (long)at, all.begin() + (long)(at + counts[k]));
+    at += counts[k];
+  }
+  return out;
 }
 
 // ---------------------------------------------------- transcript checks --
@@ -657,7 +693,9 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
   const size_t block0 = (size_t)1 << (log_n - ik + Ld.rate[0]);
   std::vector<size_t> q0 = sample_distinct_queries(tr, block0, (size_t)Ld.queries[0]);
   std::vector<f128> a0 = tr.sample_vec(ceil_log2((size_t)Ld.queries[0]));
-  if (!level_opens_ok(P.root, block0, q0, P.initial, (size_t)1 << ik)) return "ligerito: L0 openings";
+  const std::vector<std::vector<H32>> lcv = opened_leaf_cvs(P, V);
+  auto cvs_of = [&](size_t k) { return lcv[k].empty() ? nullptr : &lcv[k]; };
+  if (!level_opens_ok(P.root, block0, q0, P.initial, (size_t)1 << ik, cvs_of(0))) return "ligerito: L0 openings";
   const int n1 = log_n - ik;
   {
     const f128 es = enforced_sum(P.initial, lane_rs, q0, a0);
@@ -689,7 +727,8 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
       const size_t pbl = (size_t)1 << (prev_lmc + prev_rate);
       std::vector<size_t> ql = sample_distinct_queries(tr, pbl, (size_t)Ld.queries[i + 1]);
       std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
-      if (!level_opens_ok(prev_root, pbl, ql, P.final_open, (size_t)1 << prev_lni)) return "ligerito: final openings";
+      if (!level_opens_ok(prev_root, pbl, ql, P.final_open, (size_t)1 << prev_lni, cvs_of(lcv.size() - 1)))
+        return "ligerito: final openings";
       const f128 es = enforced_sum(P.final_open, level_rs, ql, al);
       const f128 be = tr.sample();
       t_r = fx(t_r, hmul(be, es));
@@ -745,7 +784,7 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
     std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
     if (rp >= P.levels.size()) return "ligerito: level openings missing";
     const Opening& o = P.levels[rp++];
-    if (!level_opens_ok(prev_root, pbl, qi, o, (size_t)1 << prev_lni)) return "ligerito: level openings";
+    if (!level_opens_ok(prev_root, pbl, qi, o, (size_t)1 << prev_lni, cvs_of(rp))) return "ligerito: level openings";
     const f128 es = enforced_sum(o, level_rs, qi, al);
     if (!next_msg(msg)) return "ligerito: transcript length";
     const Quad iq = Quad::from(msg, es);
@@ -776,6 +815,28 @@ std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& d
     CK(cudaMemcpyAsync(cv.data(), comb, kK * sizeof(f128), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return cv;
+  };
+  // every opened row's leaf chaining value in one upload: the rows into the
+  // gather buffer (1 MiB), the values into the index buffer (512 KiB)
+  V.leaf_cvs = [this](const uint8_t* data, const std::vector<size_t>& sizes, const std::vector<size_t>& counts) {
+    size_t bytes = 0, n = 0;
+    for (size_t k = 0; k < sizes.size(); k++) bytes += sizes[k] * counts[k], n += counts[k];
+    std::vector<H32> cvs(n);
+    if (n == 0 || bytes > ((size_t)1 << 16) * sizeof(f128) || n * 32 > ((size_t)1 << 16) * sizeof(uint64_t))
+      return std::vector<H32>();
+    uint8_t* rows = reinterpret_cast<uint8_t*>(gather);
+    uint32_t* outv = reinterpret_cast<uint32_t*>(idx);
+    CK(cudaMemcpyAsync(rows, data, bytes, cudaMemcpyHostToDevice, st));
+    size_t off = 0, at = 0;
+    for (size_t k = 0; k < sizes.size(); k++) {
+      if (!counts[k]) continue;
+      merkle_leaves(rows + off, counts[k], sizes[k], outv + 8 * at, st);
+      off += sizes[k] * counts[k];
+      at += counts[k];
+    }
+    CK(cudaMemcpyAsync(cvs.data(), outv, n * 32, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return cvs;
   };
   return verify_bundle(bytes, len, domain, V);
 }
