@@ -26,6 +26,11 @@ def test_null_handles_rejected_without_a_device():
     assert lib.flock_submit(None, None, None) == ERR_ARG
     assert lib.flock_statement_digest(5, None) == ERR_ARG
     assert lib.flock_host_alloc(0, ctypes.byref(vp)) == ERR_ARG
+    # hash chains, the verifier and self-checking serving
+    assert lib.flock_prove_chain(None, None, 256, b"x", 1, None, 0, None) == ERR_ARG
+    assert lib.flock_chain_blocks(1, None, 4, None) == ERR_ARG
+    assert lib.flock_verify(None, b"FLOCK", 5, b"x", 1) == ERR_ARG
+    assert lib.flock_serve_verify(None, 1) == ERR_ARG
 
 
 @pytest.mark.gpu
@@ -87,7 +92,9 @@ def test_serving_arguments_and_timeout():
         assert lib.flock_submit(ctx.h, ctypes.byref(job), ctypes.byref(t)) == ERR_ARG
         res = flockgpu.FlockResult(None, 0, 0, 0, 0.0, 0.0, 0.0)
         assert lib.flock_poll(ctx.h, 12345, ctypes.byref(res), 0) == ERR_ARG  # serving not started
+        assert lib.flock_serve_verify(ctx.h, 1) == ERR_ARG  # nothing to self-check yet
         ctx.serve_start(1)
+        assert lib.flock_serve_verify(ctx.h, 0) == 0
         assert lib.flock_poll(ctx.h, 12345, ctypes.byref(res), 0) == ERR_TIMEOUT  # no such job yet
         assert lib.flock_serve_start(ctx.h, 2) == ERR_ARG  # already started
         jobs = (flockgpu.FlockJob * 1)(flockgpu.FlockJob(8, 1, None, b"d", 1))
