@@ -9,7 +9,6 @@ namespace flock {
 Server::Server(int device, uint64_t budget, int slots) : device_(device), budget_(budget) {
   if (slots < 1 || slots > 64) throw std::runtime_error("serving slots must be in 1..64");
   for (int i = 0; i < slots; i++) workers_.emplace_back([this] { worker(); });
-  for (int i = 0; i < kVerifiers; i++) vthreads_.emplace_back([this] { verifier(); });
 }
 
 Server::~Server() {
@@ -20,12 +19,6 @@ Server::~Server() {
   cv_jobs_.notify_all();
   cv_mem_.notify_all();
   for (auto& t : workers_) t.join();
-  {
-    std::lock_guard<std::mutex> lk(mu_);
-    vstop_ = true;
-  }
-  cv_verify_.notify_all();
-  for (auto& t : vthreads_) t.join();
   std::lock_guard<std::mutex> bl(batch_mu_);
   idle_.clear();  // frees the cached setups
   if (batch_st_) cudaStreamDestroy(batch_st_);
@@ -258,40 +251,6 @@ void Server::release(std::unique_ptr<Setup> s) {
   cv_mem_.notify_all();
 }
 
-void Server::verifier() {
-  cudaSetDevice(device_);
-  std::unique_ptr<Verifier> V;
-  std::unique_lock<std::mutex> lk(mu_);
-  for (;;) {
-    cv_verify_.wait(lk, [&] { return vstop_ || !vqueue_.empty(); });
-    if (vqueue_.empty()) return;  // stopping, nothing left to check
-    Checking c = std::move(vqueue_.front());
-    vqueue_.pop_front();
-    lk.unlock();
-    try {
-      if (!V) V.reset(new Verifier(device_));
-      const std::string why = V->verify(c.r.bytes.data(), c.r.bytes.size(), c.domain);
-      if (!why.empty()) {
-        c.r.status = FLOCK_ERR_VERIFY;
-        c.r.error = "self-check failed: " + why;
-      }
-    } catch (const CudaError& e) {
-      c.r.status = FLOCK_ERR_CUDA;
-      c.r.error = e.what();
-    } catch (const std::exception& e) {
-      c.r.status = FLOCK_ERR_INTERNAL;
-      c.r.error = e.what();
-    }
-    const auto t_end = Clock::now();
-    auto ms = [](Clock::duration d) { return std::chrono::duration<double, std::milli>(d).count(); };
-    c.r.run_ms = ms(t_end - c.run);
-    c.r.latency_ms = ms(t_end - c.submitted);
-    lk.lock();
-    done_[c.ticket] = std::move(c.r);
-    cv_done_.notify_all();
-  }
-}
-
 void Server::worker() {
   cudaSetDevice(device_);
   std::unique_lock<std::mutex> lk(mu_);
@@ -323,6 +282,7 @@ void Server::worker() {
           r.bytes = s->prove(&job.seed, nullptr, 0, job.domain);
         }
         r.status = FLOCK_OK;
+        self_check(*s, job.domain, r);
       } catch (const CudaError& e) {
         r.status = FLOCK_ERR_CUDA;
         r.error = e.what();
@@ -338,12 +298,6 @@ void Server::worker() {
     r.queue_ms = ms(t_run - job.submitted);
     r.run_ms = ms(t_end - t_run);
     r.latency_ms = ms(t_end - job.submitted);
-    if (verify_ && r.status == FLOCK_OK) {
-      // the proof is returned once a verifier thread has checked it
-      vqueue_.push_back(Checking{job.ticket, std::move(r), job.domain, job.submitted, t_run});
-      cv_verify_.notify_one();
-      continue;
-    }
     done_[job.ticket] = std::move(r);
     cv_done_.notify_all();
   }

@@ -59,11 +59,8 @@ class Server {
   };
   std::vector<JobResult> prove_batch(const std::vector<BatchItem>& jobs, int threads);
 
-  // self-check: verify every proof before returning it; a proof that fails
-  // gets FLOCK_ERR_VERIFY and the failed check's name.  Served proofs are
-  // verified by kVerifiers threads of their own (each with a Verifier), so a
-  // slot moves on to its next job while its last proof is checked; batched
-  // proofs are verified on their setups by the batch threads.
+  // self-check: verify every proof on its own setup before returning it; a
+  // proof that fails gets FLOCK_ERR_VERIFY and the failed check's name
   void set_verify(bool on) { verify_ = on; }
   int slots() const { return (int)workers_.size(); }
   uint64_t budget() const { return budget_; }
@@ -86,7 +83,6 @@ class Server {
   };
 
   void worker();
-  void verifier();
   void self_check(Setup& s, const std::string& domain, JobResult& r);
   // wait: block until memory frees up (else return nullptr when it does not fit now)
   std::unique_ptr<Setup> acquire(uint32_t log2, std::unique_lock<std::mutex>& lk, bool wait = true);
@@ -104,18 +100,6 @@ class Server {
   uint64_t next_ticket_ = 1, use_clock_ = 0;
   bool stop_ = false;
   std::atomic<bool> verify_{false};
-  // proofs of served jobs waiting for their self-check
-  struct Checking {
-    uint64_t ticket = 0;
-    JobResult r;
-    std::string domain;
-    Clock::time_point submitted, run;
-  };
-  static constexpr int kVerifiers = 2;
-  std::deque<Checking> vqueue_;
-  std::condition_variable cv_verify_;
-  bool vstop_ = false;
-  std::vector<std::thread> vthreads_;
   std::vector<std::thread> workers_;
   std::mutex batch_mu_;  // one batch at a time
   cudaStream_t batch_st_ = nullptr;
