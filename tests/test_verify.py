@@ -118,16 +118,31 @@ def test_chain_full_size_golden_verifies(gpu_ctx):
         p.close()
 
 
-def test_self_checking_serving():
+def test_self_checking_serving(gpu_ctx):
+    """Served proofs are checked by the server's verifier threads, batched
+    ones by the batch threads; either way the bytes are the plain proofs'."""
     import flockgpu
+    jobs = ((8, 1), (9, 2), (8, 3), (10, 6), (8, 7))
+    plain = {}
+    for l in sorted({l for l, _ in jobs}):
+        p = flockgpu.Prover(gpu_ctx, l)
+        try:
+            for ll, s in jobs:
+                if ll == l:
+                    plain[(l, s)] = p.prove_seed(s)
+        finally:
+            p.close()
     ctx = flockgpu.Context(0)
     try:
         ctx.serve_start(2)
         ctx.serve_verify(True)
-        tickets = [ctx.submit(l, s) for l, s in ((8, 1), (9, 2), (8, 3))]
-        for t in tickets:
-            assert ctx.poll(t) is not None  # a failed self-check raises
-        out = ctx.prove_batch([(8, 4), (9, 5)], threads=2)
-        assert len(out) == 2
+        tickets = [ctx.submit(l, s) for l, s in jobs]
+        for t, job in zip(tickets, jobs):
+            r = ctx.poll(t)  # a failed self-check raises
+            assert r["bytes"] == plain[job]
+        out = ctx.prove_batch([(8, 1), (9, 2)], threads=2)
+        assert [o["bytes"] for o in out] == [plain[(8, 1)], plain[(9, 2)]]
+        ctx.serve_verify(False)
+        assert ctx.poll(ctx.submit(8, 3))["bytes"] == plain[(8, 3)]
     finally:
         ctx.close()
