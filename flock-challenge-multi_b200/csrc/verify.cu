@@ -22,6 +22,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace flock {
 namespace {
@@ -176,16 +178,26 @@ f128 interp_lambda(const std::vector<f128>& v, f128 z) {
 }
 f128 interp_combined(const std::vector<f128>& v, f128 z) {
   const f128* P = phi8_table();
+  // the denominators prod_{j != i} (s_i + s_j) depend only on the nodes
+  static const std::vector<f128> inv_den = [P] {
+    std::vector<f128> d(64);
+    for (int i = 0; i < 64; i++) {
+      f128 den = hone();
+      for (int j = 0; j < 128; j++)
+        if (j != 64 + i) den = hmul(den, fx(P[64 + i], P[j]));
+      d[i] = hinv(den);
+    }
+    return d;
+  }();
+  // numerators prod_{j != i} (z + s_j) from prefix and suffix products
+  f128 pre[129], suf[129];
+  pre[0] = suf[128] = hone();
+  for (int j = 0; j < 128; j++) pre[j + 1] = hmul(pre[j], fx(z, P[j]));
+  for (int j = 128; j-- > 0;) suf[j] = hmul(suf[j + 1], fx(z, P[j]));
   f128 acc = mk(0, 0);
   for (int i = 0; i < 64; i++) {
     const int node = 64 + i;
-    f128 num = hone(), den = hone();
-    for (int j = 0; j < 128; j++) {
-      if (j == node) continue;
-      num = hmul(num, fx(z, P[j]));
-      den = hmul(den, fx(P[node], P[j]));
-    }
-    acc = fx(acc, hmul(hmul(num, hinv(den)), v[i]));
+    acc = fx(acc, hmul(hmul(hmul(pre[node], suf[node + 1]), inv_den[i]), v[i]));
   }
   return acc;
 }
@@ -427,8 +439,21 @@ f128 enforced_sum(const Opening& o, const std::vector<f128>& v, const std::vecto
 // induce_sumcheck_evaluate_at_residual (pcs/ligerito.rs:1346-1435)
 std::vector<f128> induce_residual(int log_msg_cols, const std::vector<size_t>& q, const std::vector<f128>& alpha,
                                   const f128* ris, int prefix_len, int yr_log_n) {
-  std::vector<f128> sks = eval_sk_at_vks(log_msg_cols), inv(sks.size());
-  for (size_t i = 0; i < sks.size(); i++) inv[i] = (sks[i].lo | sks[i].hi) ? hinv(sks[i]) : mk(0, 0);
+  // s_k(v_k) and their inverses depend only on the level's size: cached
+  static std::mutex mu;
+  static std::map<int, std::pair<std::vector<f128>, std::vector<f128>>> cache;
+  std::vector<f128> sks, inv;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(log_msg_cols);
+    if (it == cache.end()) {
+      std::vector<f128> s = eval_sk_at_vks(log_msg_cols), iv(s.size());
+      for (size_t i = 0; i < s.size(); i++) iv[i] = (s[i].lo | s[i].hi) ? hinv(s[i]) : mk(0, 0);
+      it = cache.emplace(log_msg_cols, std::make_pair(s, iv)).first;
+    }
+    sks = it->second.first;
+    inv = it->second.second;
+  }
   std::vector<f128> aw = heq(alpha);
   std::vector<f128> out((size_t)1 << yr_log_n, mk(0, 0));
   for (size_t i = 0; i < q.size(); i++) {
