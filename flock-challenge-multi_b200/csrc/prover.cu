@@ -88,7 +88,7 @@ Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
   d_found = dalloc<unsigned long long>(1);
   CK(cudaMallocHost(&h_found, 8));
   CK(cudaMallocHost(&h_out, 1024 * sizeof(f128)));
-  CK(cudaMallocHost(&h_stage, (size_t)1 << 20));
+  CK(cudaMallocHost(&h_stage, kStageBytes));
   const Statement& S = blake3_statement();
   at_ptr = dalloc<uint32_t>(S.at_ptr.size());
   bt_ptr = dalloc<uint32_t>(S.bt_ptr.size());
@@ -353,8 +353,8 @@ std::vector<size_t> Setup::sample_queries(Transcript& tr, size_t block_len, size
 // Opened rows + Merkle multi-proof (merkle.rs:1074-1120 index order).  The
 // sibling indices depend only on the queries, so both gathers are issued
 // together and read back with one synchronisation.
-Opening Setup::open(const f128* cw, const uint32_t* tree, size_t n_leaves, int lanes, const std::vector<size_t>& q) {
-  Opening o;
+void Setup::open(Opening& o, const f128* cw, const uint32_t* tree, size_t n_leaves, int lanes,
+                 const std::vector<size_t>& q) {
   std::vector<uint64_t> ids(q.begin(), q.end());
   // sibling indices of the multi-proof, after the query positions
   std::vector<size_t> act(q);
@@ -380,13 +380,27 @@ Opening Setup::open(const f128* cw, const uint32_t* tree, size_t n_leaves, int l
   if (ns) {
     count_launch(); k_gather_nodes<<<(unsigned)((ns + 127) / 128), 128, 0, st>>>(tree, idx + nq, ns, nodes);
   }
-  std::vector<f128> rows(nr);
-  o.proof.resize(ns);
-  CK(cudaMemcpyAsync(rows.data(), gather, nr * sizeof(f128), cudaMemcpyDeviceToHost, st));
-  if (ns) CK(cudaMemcpyAsync(o.proof.data(), nodes, ns * 32, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  for (size_t i = 0; i < nq; i++) o.rows.emplace_back(rows.begin() + i * lanes, rows.begin() + (i + 1) * lanes);
-  return o;
+  // nothing on the host reads the opening before the proof is encoded: copy
+  // it into the pinned staging area and unpack it after the proof's final
+  // synchronisation (finish_openings), with no wait of its own
+  const size_t need = nr * sizeof(f128) + ns * 32;
+  if (stage_off_ + need > kStageBytes) throw std::runtime_error("openings larger than the staging area");
+  CK(cudaMemcpyAsync(h_stage + stage_off_, gather, nr * sizeof(f128), cudaMemcpyDeviceToHost, st));
+  if (ns) CK(cudaMemcpyAsync(h_stage + stage_off_ + nr * sizeof(f128), nodes, ns * 32, cudaMemcpyDeviceToHost, st));
+  pending_.push_back(PendingOpen{&o, stage_off_, nq, (size_t)lanes, ns});
+  stage_off_ += need;
+}
+
+void Setup::finish_openings() {
+  for (const PendingOpen& p : pending_) {
+    const f128* rows = reinterpret_cast<const f128*>(h_stage + p.off);
+    p.o->rows.clear();
+    for (size_t i = 0; i < p.nq; i++) p.o->rows.emplace_back(rows + i * p.lanes, rows + (i + 1) * p.lanes);
+    p.o->proof.resize(p.ns);
+    if (p.ns) memcpy(p.o->proof.data(), h_stage + p.off + p.nq * p.lanes * sizeof(f128), p.ns * 32);
+  }
+  pending_.clear();
+  stage_off_ = 0;
 }
 
 H32 Setup::root_of(const uint32_t* tree, size_t n_leaves) {
@@ -409,6 +423,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
                                   const std::string& domain, bool committed, const ChainEnds* chain) {
   Proof P;
   P.m = (uint64_t)m;
+  pending_.clear();  // (left over only by a proof that threw)
+  stage_off_ = 0;
   const int G = sms * 4;
   const uint32_t n_slots = 1u << n_log;
   mark(0);
@@ -887,10 +903,11 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   {
     std::vector<size_t> q0 = sample_queries(tr, n_leaves0, (size_t)Ld.queries[0]);
     std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[0]));
-    P.initial = open(cw0, tree0, n_leaves0, 64, q0);
+    open(P.initial, cw0, tree0, n_leaves0, 64, q0);
     induce(q0, al, Ld.rate[0]);
   }
   const int rsteps = (int)Ld.ks.size();
+  P.levels.reserve((size_t)rsteps);  // pending openings point into it
   for (int i = 0; i < rsteps; i++) {
     for (int j = 0; j < Ld.ks[i]; j++) fold_round(std::max(0, Ld.fold_grind[i + 1] - j));
     n_cur -= Ld.ks[i];
@@ -902,7 +919,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       P.grind_nonces.push_back(grind(tr, (uint32_t)Ld.grind[i + 1]));
       std::vector<size_t> ql = sample_queries(tr, prev.positions, (size_t)Ld.queries[i + 1]);
       tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
-      P.final_open = open(prev.cw, prev.tree, prev.positions, prev.lanes, ql);
+      open(P.final_open, prev.cw, prev.tree, prev.positions, prev.lanes, ql);
       tr.sample();
       break;
     }
@@ -911,11 +928,13 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     P.grind_nonces.push_back(grind(tr, (uint32_t)Ld.grind[i + 1]));
     std::vector<size_t> qi = sample_queries(tr, prev.positions, (size_t)Ld.queries[i + 1]);
     std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
-    P.levels.push_back(open(prev.cw, prev.tree, prev.positions, prev.lanes, qi));
+    P.levels.emplace_back();
+    open(P.levels.back(), prev.cw, prev.tree, prev.positions, prev.lanes, qi);
     induce(qi, al, prev.rate);
   }
   mark(9);
   CK(cudaStreamSynchronize(st));
+  finish_openings();
   std::vector<uint8_t> bytes = encode(P);
   return bytes;
 }

@@ -98,7 +98,17 @@ class Setup {
   void fetch(const f128* dev, size_t n, f128* host);
   uint64_t grind(Transcript& tr, uint32_t bits);
   std::vector<size_t> sample_queries(Transcript& tr, size_t block_len, size_t count);
-  Opening open(const f128* cw, const uint32_t* tree, size_t n_leaves, int lanes, const std::vector<size_t>& q);
+  // queues the opening's gathers and its copy into the pinned staging area;
+  // `o` is filled by finish_openings once the stream has finished
+  void open(Opening& o, const f128* cw, const uint32_t* tree, size_t n_leaves, int lanes, const std::vector<size_t>& q);
+  void finish_openings();
+  struct PendingOpen {
+    Opening* o;
+    size_t off, nq, lanes, ns;
+  };
+  static constexpr size_t kStageBytes = (size_t)1 << 21;
+  std::vector<PendingOpen> pending_;
+  size_t stage_off_ = 0;
   H32 root_of(const uint32_t* tree, size_t n_leaves);
   void mark(int phase);
   f128* scratch_eq() { return eqbuf[0]; }
