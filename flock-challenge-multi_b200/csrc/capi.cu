@@ -14,6 +14,8 @@ struct flock_ctx {
   std::string err;
   std::mutex mu;
   std::unique_ptr<flock::Server> server;
+  std::mutex vmu;  // one verification at a time on the context's verifier
+  std::unique_ptr<flock::Verifier> verifier;
 };
 struct flock_setup {
   flock_ctx* ctx = nullptr;
@@ -169,6 +171,18 @@ int flock_verify(flock_setup* s, const uint8_t* bytes, size_t len, const uint8_t
     const std::string why = s->s->verify(bytes, len, std::string((const char*)domain, dlen));
     if (why.empty()) return (int)FLOCK_OK;
     s->ctx->err = "verify: " + why;
+    return (int)FLOCK_ERR_VERIFY;
+  });
+}
+
+int flock_verify_bundle(flock_ctx* c, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen) {
+  if (!c || !bytes || (!domain && dlen)) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    std::lock_guard<std::mutex> lk(c->vmu);
+    if (!c->verifier) c->verifier.reset(new flock::Verifier(c->device));
+    const std::string why = c->verifier->verify(bytes, len, std::string((const char*)domain, dlen));
+    if (why.empty()) return (int)FLOCK_OK;
+    c->err = "verify: " + why;
     return (int)FLOCK_ERR_VERIFY;
   });
 }

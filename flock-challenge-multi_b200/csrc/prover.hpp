@@ -48,6 +48,27 @@ struct VerifyStatement {
 // "" when the bundle verifies, otherwise the name of the failed check
 std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& domain, const VerifyStatement& V);
 
+// A verifier with its own device scratch (about 2 MiB) and stream, for any
+// statement size; the block matrices' device copy is shared per device.  One
+// thread at a time per Verifier.
+class Verifier {
+ public:
+  explicit Verifier(int device);
+  ~Verifier();
+  Verifier(const Verifier&) = delete;
+  Verifier& operator=(const Verifier&) = delete;
+  // "" when the bundle verifies, otherwise the name of the failed check
+  std::string verify(const uint8_t* bytes, size_t len, const std::string& domain);
+
+ private:
+  static constexpr size_t kRowsCap = (size_t)1 << 20, kCvsCap = (size_t)1 << 19;
+  int device_ = 0;
+  cudaStream_t st_ = nullptr;
+  f128 *eqx_ = nullptr, *eqi_ = nullptr, *comb_ = nullptr;
+  uint8_t* rows_ = nullptr;
+  uint32_t* cvs_ = nullptr;
+};
+
 struct Level {
   int lanes = 0, log_msg_pos = 0, rate = 0;
   size_t positions = 0;

@@ -828,42 +828,116 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
 
 // The device half of the verifier: the lincheck's matrix combination over
 // this setup's CSC copy of the block matrices, with the prover's kernels.
-std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& domain) {
+namespace {
+// Device scratch of one verification in flight: eq(x_inner) (256 values), the
+// lincheck's eq table and matrix combination (2^14 values each), the opened
+// rows (1 MiB) and their leaf chaining values (512 KiB).
+struct VerifyBufs {
+  f128 *eqx, *eqi, *comb;
+  uint8_t* rows;
+  uint32_t* cvs;
+  size_t rows_cap, cvs_cap;  // bytes
+};
+// the device half of the verifier over the CSC copy of the block matrices
+// given by at_*, bt_*: the matrix combination and the opened rows' leaves
+VerifyStatement device_statement(int m, const std::array<uint8_t, 32>& digest, const uint32_t* at_ptr,
+                                 const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
+                                 const VerifyBufs& B, cudaStream_t st) {
   VerifyStatement V;
   V.m = m;
   V.digest = digest;
-  V.comb = [this](f128 zskip, const std::vector<f128>& x_inner, f128 alpha, f128 beta) {
+  V.comb = [=](f128 zskip, const std::vector<f128>& x_inner, f128 alpha, f128 beta) {
     std::vector<f128> L = hlagrange(zskip, 0), cv(kK);
-    eq_build(x_inner.data(), (int)x_inner.size(), hone(), zv_pre, st);
-    outer64(L.data(), zv_pre, (size_t)1 << x_inner.size(), eq_inner, st);
-    lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, kZConst, comb, st);
-    CK(cudaMemcpyAsync(cv.data(), comb, kK * sizeof(f128), cudaMemcpyDeviceToHost, st));
+    eq_build(x_inner.data(), (int)x_inner.size(), hone(), B.eqx, st);
+    outer64(L.data(), B.eqx, (size_t)1 << x_inner.size(), B.eqi, st);
+    lc_comb(at_ptr, at_row, bt_ptr, bt_row, B.eqi, alpha, beta, kZConst, B.comb, st);
+    CK(cudaMemcpyAsync(cv.data(), B.comb, kK * sizeof(f128), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return cv;
   };
-  // every opened row's leaf chaining value in one upload: the rows into the
-  // gather buffer (1 MiB), the values into the index buffer (512 KiB)
-  V.leaf_cvs = [this](const uint8_t* data, const std::vector<size_t>& sizes, const std::vector<size_t>& counts) {
+  // every opened row's leaf chaining value in one upload
+  V.leaf_cvs = [=](const uint8_t* data, const std::vector<size_t>& sizes, const std::vector<size_t>& counts) {
     size_t bytes = 0, n = 0;
     for (size_t k = 0; k < sizes.size(); k++) bytes += sizes[k] * counts[k], n += counts[k];
     std::vector<H32> cvs(n);
-    if (n == 0 || bytes > ((size_t)1 << 16) * sizeof(f128) || n * 32 > ((size_t)1 << 16) * sizeof(uint64_t))
-      return std::vector<H32>();
-    uint8_t* rows = reinterpret_cast<uint8_t*>(gather);
-    uint32_t* outv = reinterpret_cast<uint32_t*>(idx);
-    CK(cudaMemcpyAsync(rows, data, bytes, cudaMemcpyHostToDevice, st));
+    if (n == 0 || bytes > B.rows_cap || n * 32 > B.cvs_cap) return std::vector<H32>();
+    CK(cudaMemcpyAsync(B.rows, data, bytes, cudaMemcpyHostToDevice, st));
     size_t off = 0, at = 0;
     for (size_t k = 0; k < sizes.size(); k++) {
       if (!counts[k]) continue;
-      merkle_leaves(rows + off, counts[k], sizes[k], outv + 8 * at, st);
+      merkle_leaves(B.rows + off, counts[k], sizes[k], B.cvs + 8 * at, st);
       off += sizes[k] * counts[k];
       at += counts[k];
     }
-    CK(cudaMemcpyAsync(cvs.data(), outv, n * 32, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(cvs.data(), B.cvs, n * 32, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return cvs;
   };
-  return verify_bundle(bytes, len, domain, V);
+  return V;
+}
+
+// One device copy of the block matrices' CSC per device, shared by every
+// Verifier on it (they are the same for every statement size).
+struct DevCsc {
+  uint32_t *at_ptr = nullptr, *bt_ptr = nullptr;
+  uint16_t *at_row = nullptr, *bt_row = nullptr;
+};
+const DevCsc& shared_csc(int device) {
+  static std::mutex mu;
+  static std::map<int, DevCsc> m;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = m.find(device);
+  if (it != m.end()) return it->second;
+  const Statement& S = blake3_statement();
+  DevCsc d;
+  auto up = [](auto& dst, const auto& src) {
+    CK(cudaMalloc(&dst, src.size() * sizeof(src[0])));
+    CK(cudaMemcpy(dst, src.data(), src.size() * sizeof(src[0]), cudaMemcpyHostToDevice));
+  };
+  up(d.at_ptr, S.at_ptr);
+  up(d.bt_ptr, S.bt_ptr);
+  up(d.at_row, S.at_row);
+  up(d.bt_row, S.bt_row);
+  return m[device] = d;
+}
+}  // namespace
+
+// The setup's own buffers and stream (flock_verify: the caller owns the setup).
+std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& domain) {
+  VerifyBufs B{zv_pre, eq_inner, comb, reinterpret_cast<uint8_t*>(gather), reinterpret_cast<uint32_t*>(idx),
+               ((size_t)1 << 16) * sizeof(f128), ((size_t)1 << 16) * sizeof(uint64_t)};
+  return verify_bundle(bytes, len, domain, device_statement(m, digest, at_ptr, at_row, bt_ptr, bt_row, B, st));
+}
+
+Verifier::Verifier(int device) : device_(device) {
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  CK(cudaMalloc(&eqx_, 256 * sizeof(f128)));
+  CK(cudaMalloc(&eqi_, kK * sizeof(f128)));
+  CK(cudaMalloc(&comb_, kK * sizeof(f128)));
+  CK(cudaMalloc(&rows_, kRowsCap));
+  CK(cudaMalloc(&cvs_, kCvsCap));
+}
+
+Verifier::~Verifier() {
+  if (st_) cudaStreamSynchronize(st_);
+  for (void* p : {(void*)eqx_, (void*)eqi_, (void*)comb_, (void*)rows_, (void*)cvs_}) cudaFree(p);
+  if (st_) cudaStreamDestroy(st_);
+}
+
+std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string& domain) {
+  if (len < 7 + 4 + 32 + 8) return "malformed bundle: truncated";
+  // the statement size is the bundle's m (after the header, the optional
+  // hash kind and the root); verify_bundle checks everything else
+  const size_t at = 7 + (bytes[6] == 3 ? 4 : 0) + 32;
+  uint64_t mm = 0;
+  for (int k = 0; k < 8; k++) mm |= (uint64_t)bytes[at + k] << (8 * k);
+  if (mm < (uint64_t)kKLog + 8 || mm > (uint64_t)kKLog + 20) return "bundle is for an unsupported statement size";
+  const DevCsc& C = shared_csc(device_);
+  const VerifyBufs B{eqx_, eqi_, comb_, rows_, cvs_, kRowsCap, kCvsCap};
+  return verify_bundle(bytes, len, domain,
+                       device_statement((int)mm, statement_digest((int)mm), C.at_ptr, C.at_row, C.bt_ptr, C.bt_row,
+                                        B, st_));
 }
 
 }  // namespace flock

@@ -28,7 +28,7 @@ EXPORTS = (
     "flock_bench_merkle", "flock_bench_sumcheck", "flock_bench_prove", "flock_merkle_root_noalloc",
     "flock_serve_start", "flock_submit", "flock_poll", "flock_sumcheck_round3", "flock_bench_sumcheck3",
     "flock_ntt_autotune", "flock_ntt_rs_encode_plan", "flock_prove_batch", "flock_host_alloc",
-    "flock_host_free", "flock_prove_chain", "flock_chain_blocks", "flock_verify", "flock_serve_verify",
+    "flock_host_free", "flock_prove_chain", "flock_chain_blocks", "flock_verify", "flock_serve_verify", "flock_verify_bundle",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -97,6 +97,7 @@ def load() -> ctypes.CDLL:
         lib.flock_chain_blocks.argtypes = [u64, vp, sz, vp]
         lib.flock_verify.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
         lib.flock_serve_verify.argtypes = [vp, i32]
+        lib.flock_verify_bundle.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
         _lib = lib
     return _lib
 
@@ -192,6 +193,17 @@ class Context:
     # ---- serving (continuous batching of proof jobs) ----
     def serve_start(self, slots: int = 4) -> None:
         self._check(self.lib.flock_serve_start(self.h, slots), "serve_start")
+
+    def verify(self, bundle: bytes, domain: bytes = DOMAIN) -> str:
+        """'' when the FLOCK v4 bundle verifies (any supported size, no prover
+        setup needed), otherwise the name of the failed check."""
+        rc = self.lib.flock_verify_bundle(self.h, bundle, len(bundle), domain, len(domain))
+        if rc == 0:
+            return ""
+        if rc == FLOCK_ERR_VERIFY:
+            return self.lib.flock_last_error(self.h).decode()
+        self._check(rc, "verify_bundle")
+        return "error"
 
     def serve_verify(self, on: bool = True) -> None:
         """Self-check every served / batched proof with the verifier."""

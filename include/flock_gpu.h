@@ -22,7 +22,8 @@
  *                           + ChainProofBundleLigerito::to_bytes (blake3.rs:
  *                           5195-5215, r1cs_hashes/chain_common.rs:287-350,
  *                           proof_io.rs:144-157, 943-950)
- *  - flock_verify        <- Blake3Setup::verify / verify_chain on a decoded
+ *  - flock_verify, flock_verify_bundle
+ *                        <- Blake3Setup::verify / verify_chain on a decoded
  *                           bundle (blake3.rs:5129-5145, 5217-5240;
  *                           crates/flock-core/src/verifier.rs:95-232)
  *  - flock_chain_blocks  <- the flock_chain CLI's honest BLAKE3 chain
@@ -104,6 +105,12 @@ int flock_chain_blocks(uint64_t seed, const uint32_t* initial_cv, size_t steps, 
  * (transcript replay, Merkle openings, proof of work, residual basis) on the
  * calling thread. */
 int flock_verify(flock_setup* s, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen);
+/* The same verification without a prover setup, for any supported size
+ * (2^8..2^20 compressions, read from the bundle): a verifier held by the
+ * context and created on first use, with about 2 MiB of device scratch, plus
+ * one device copy of the block matrices per device (about 45 MB, kept until
+ * the process exits).  Calls on one context are serialised. */
+int flock_verify_bundle(flock_ctx* ctx, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen);
 /* Self-checking serving: with on != 0, every proof served by flock_submit /
  * flock_prove_batch is verified on its setup before it is returned, and one
  * that fails gets status FLOCK_ERR_VERIFY.  Call after flock_serve_start. */

@@ -31,6 +31,7 @@ def test_null_handles_rejected_without_a_device():
     assert lib.flock_chain_blocks(1, None, 4, None) == ERR_ARG
     assert lib.flock_verify(None, b"FLOCK", 5, b"x", 1) == ERR_ARG
     assert lib.flock_serve_verify(None, 1) == ERR_ARG
+    assert lib.flock_verify_bundle(None, b"FLOCK", 5, b"x", 1) == ERR_ARG
 
 
 @pytest.mark.gpu

@@ -54,6 +54,7 @@ def test_accepts_full_size_golden(gpu_ctx):
         t0 = time.perf_counter()
         assert p.verify(proof) == ""
         print(f"verify 2^18: {1e3 * (time.perf_counter() - t0):.1f} ms")
+        assert gpu_ctx.verify(proof) == ""  # and without the setup
     finally:
         p.close()
 
@@ -146,3 +147,22 @@ def test_self_checking_serving(gpu_ctx):
         assert ctx.poll(ctx.submit(8, 3))["bytes"] == plain[(8, 3)]
     finally:
         ctx.close()
+
+
+def test_context_verifier_without_setup(gpu_ctx, p8):
+    """flock_verify_bundle: the context's own verifier, any size, no setup."""
+    import flockgpu
+    proof = p8.prove_seed(41)
+    chain = p8.prove_chain(flockgpu.chain_blocks(4, 1 << 8))
+    assert gpu_ctx.verify(proof) == ""
+    assert gpu_ctx.verify(chain, CHAIN_DOMAIN) == ""
+    bad = bytearray(proof)
+    bad[len(bad) // 2] ^= 1
+    assert gpu_ctx.verify(bytes(bad)) != ""
+    assert gpu_ctx.verify(proof, b"another-domain") != ""
+    assert "malformed" in gpu_ctx.verify(proof[:30])
+    p9 = flockgpu.Prover(gpu_ctx, 9)
+    try:
+        assert gpu_ctx.verify(p9.prove_seed(2)) == ""  # another size on the same verifier
+    finally:
+        p9.close()
