@@ -35,30 +35,54 @@ METRIC = "verified BLAKE3 compressions/sec on 1 B200 (2^18/proof); p50/p99 proof
 PUBLISHED_CPU = 381080.0  # reference, c7i.4xlarge 16 vCPU (README.md:95-98)
 SERVE_SLOTS = 4  # proofs in flight in the continuous-batching queue
 BATCH_THREADS = 8  # host threads (one stream each) driving the batched proofs' transcript phases
+def algorithmic_bytes(phase: str, log2: int) -> int:
+    """Minimum HBM bytes of one proof phase: the data the phase must read and
+    write once, whatever the implementation (m = 14 + log2 witness bits;
+    packed vectors hold 2^(m-7) F128 values; the commitment has 64 lanes, rate
+    1/2, 2^(m-13) message positions and 2^(m-12) leaves of 1 KiB)."""
+    m = 14 + log2
+    n = 1 << (m - 7)  # F128 values of one packed vector (z, a, b, b_combined)
+    return {
+        # read the 2^(m-7)-value message, write the 2^(m-6)-value codeword
+        "rs_encode": 16 * n + 16 * 2 * n,
+        # read the codeword (leaves x 1 KiB), write 32 B per leaf CV
+        "merkle_commit": (1 << (m - 12)) * 1024 + 32 * (1 << (m - 12)),
+        # write z, a, b (2^m bits each)
+        "witness": 3 * (1 << m) // 8,
+        # read a, b, c (c = z)
+        "zerocheck_round1": 3 * (1 << m) // 8,
+        # packed a, b read once, then per round over k values per vector
+        # 2 x 16 k read + 16 k written, k from 2^(m-7) halving
+        "zerocheck_rounds": 2 * (1 << m) // 8 + 48 * 2 * n,
+        # the z-fold reads z
+        "lincheck": (1 << m) // 8,
+        # per claim (two): read z, write a 2^(m-7)-value vector
+        "ring_switch_combine": 2 * ((1 << m) // 8 + 16 * n),
+        # 6 rounds over f and b: 2 x 16 k per round, k from 2^(m-7) halving
+        "ligerito_l0_folds": 2 * 16 * 2 * n,
+        # the first recursive level's codeword (2^(m-11) values) written and read
+        "ligerito_levels": 2 * 16 * (1 << (m - 11)),
+    }[phase]
+
+
+# phase -> (the phase's kernels, launches per proof, what the algorithmic bytes count)
 PHASE_KERNEL = {
-    # phase -> (kernel, algorithmic bytes per proof at m = 32, launches per proof, description)
-    "rs_encode": ("k_ntt_pass", 2 * 2 * (1 << 30), 2,
-                  "two passes (10 + 9 of the 19 butterfly layers), each reads and writes the 1 GiB codeword"),
-    "merkle_commit": ("k_merkle_leaves", (1 << 30) + (1 << 25), 1, "reads the 1 GiB codeword, writes 32 MiB of leaf CVs"),
-    "zerocheck_round1": ("k_zc_round1_ab", 2 * (1 << 29), 1, "reads packed a, b (2 x 512 MiB)"),
-    "zerocheck_rounds": ("k_zc_round", 2 * (1 << 29) + 4 * (1 << 29) + 3 * (1 << 29), 26,
-                         "round 0 reads a, b; round 1 reads a, b, writes the folded pair; then halving"),
-    "ring_switch_combine": ("k_bcombined_ct", 1 << 29, 1, "writes b_combined (512 MiB)"),
-    "ligerito_l0_folds": ("k_lig_fold_msg", 4 * (1 << 29), 6, "6 folds over f, b (2 x 512 MiB, halving)"),
-    "lincheck": ("k_lc_zvec", 1 << 29, 1, "reads z (512 MiB)"),
-    "witness": ("k_witness_seed", 3 * (1 << 29), 1, "writes z, a, b (3 x 512 MiB)"),
-    "ligerito_levels": ("levels", 1 << 27, 1, "recursive levels"),
+    "rs_encode": ("k_replicate + k_ntt_pass", 3, "read the message (2^25 F128), write the codeword (2^26 F128)"),
+    "merkle_commit": ("k_merkle_leaves/parents/top", 22, "read the 1 GiB codeword, write 32 B per leaf"),
+    "zerocheck_round1": ("k_zc_round1_ab + k_zc_round1_c", 2, "read packed a, b, c (3 x 512 MiB)"),
+    "zerocheck_rounds": ("k_zc_round", 26, "packed a, b once, then 3 x 16 B per value per halving round"),
+    "ring_switch_combine": ("k_bcombined_ct", 2, "per claim: read z, write 2^25 F128"),
+    "ligerito_l0_folds": ("k_lig_fold_msg", 12, "6 rounds over f, b (2 x 512 MiB, halving)"),
+    "lincheck": ("k_lc_zvec", 12, "read z (512 MiB)"),
+    "witness": ("k_witness_seed", 1, "write z, a, b (3 x 512 MiB)"),
+    "ligerito_levels": ("levels", 60, "the first recursive level's codeword written and read"),
 }
 
-
-# kernels whose bound is the integer pipe rather than HBM (ncu captures under profiles/)
-INT_NOTES = {
-    "k_ntt_pass": "6.4e8 GF(2^128) products per proof; FMA-heavy pipe (IMAD.WIDE) 83% and ALU 52% busy "
-                  "(ncu, profiles/kernels_prover_2p16.md); a register-only loop of the same product reaches "
-                  "3.8e10 products/s on this GPU",
-}
-# GF(2^128) products per proof of each integer-bound dominant kernel at m = 32
-INT_PRODUCTS = {"k_ntt_pass": 64 * (1 << 19) * 19}
+# GF(2^128) products per proof of the RS encode: 64 lanes x 2^19 pairs x 19
+# butterfly layers at m = 32 (layer 0 is a copy)
+NTT_PRODUCTS_2P18 = 64 * (1 << 19) * 19
+# register-only loop of the same product on this GPU (all 148 SMs)
+PRODUCT_REGISTER_ONLY = 3.8e10
 
 
 def peaks():
@@ -338,10 +362,10 @@ def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: i
     return out
 
 
-# Integer-pipe ceiling of the GF(2^128) product as built here: 144 IMAD.WIDE
-# (9 Karatsuba 32x32 carry-less products of 16 each) at 32 per SM per clock,
-# the FMA pipe's rate; the ~300 ALU operations at 64 per SM per clock bind at
-# the same rate.  148 SMs at the measured maximum SM clock.
+# Ceiling of the GF(2^128) product as built here (not an algorithmic bound: a
+# cheaper product raises it): 144 IMAD.WIDE (9 Karatsuba 32x32 carry-less
+# products of 16 each) at 32 per SM per clock, the FMA pipe's rate.  148 SMs
+# at the measured maximum SM clock.
 def int_product_peak() -> float:
     mhz = 1965.0
     p = REPO / "MEASURED_PEAKS.json"
@@ -490,15 +514,17 @@ def run_ours(args, world, rank, local):
     n = (1 << log2) * args.steps * world
     peak, peak_kind = peaks()
     dom = max(phases, key=phases.get)
-    kname, kbytes, klaunches, kdesc = PHASE_KERNEL[dom]
-    scale = 1 << (log2 - 18) if log2 >= 18 else 1.0 / (1 << (18 - log2))
-    kbytes = int(kbytes * scale)
-    # the phase's events bracket only its own launches on the prover stream
+    kname, klaunches, kdesc = PHASE_KERNEL[dom]
+    kbytes = algorithmic_bytes(dom, log2)
+    # the phase's events bracket only its own launches on the prover stream:
+    # algorithmic bytes of the phase over the phase's device time
     achieved = kbytes / (phases[dom] / 1e3) / 1e9
     traffic = None
     tfile = REPO / "profiles" / "traffic.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(kname)
+        t = json.loads(tfile.read_text()).get(dom)
+        if t:
+            traffic = t * (1 << log2) / (1 << 18)  # DRAM bytes grow with the codeword
     line = {
         "metric": METRIC, "value": value, "unit": "compressions/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -507,25 +533,31 @@ def run_ours(args, world, rank, local):
                                f"profile, BLAKE3 Merkle + transcript", "log2": log2, "proofs_per_step": 1,
                    "parallelism": f"replicas x{world}", "l2": "working set ~5 GB per proof > 126 MB L2",
                    "proof_bytes": sizes[0]},
+        "baseline_anchor": {"published_cpu_value": PUBLISHED_CPU, "unit": "compressions/s",
+                            "hardware": "reference Rust prover, c7i.4xlarge, 16 vCPU",
+                            "value_ratio": value / PUBLISHED_CPU, "e2e_ratio": n / e2e_s / PUBLISHED_CPU},
         "e2e": {"value": n / e2e_s, "unit": "compressions/s", "h2d_bytes_per_step": (1 << log2) * 100,
                 "d2h_bytes_per_step": sizes[0]},
         "gpu_launches": int(launches),
         "phases_ms": {k: round(v, 3) for k, v in phases.items()},
         "roofline": {"bound": "hbm", "kernel": kname, "phase": dom, "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": (traffic * scale / klaunches) if traffic else None,
-                     "algorithmic_bytes": kbytes // klaunches, "launches": klaunches,
-                     "note": f"{kdesc}; per launch; peak {peak_kind}" +
-                             ("; integer-pipe bound: " + INT_NOTES[kname] if kname in INT_NOTES else "")},
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes": kbytes, "traffic_over_algorithmic": (traffic / kbytes) if traffic else None,
+                     "launches": klaunches,
+                     "note": f"per phase (its {klaunches} launches): {kdesc}; peak {peak_kind}"},
         "clocks": clocks,
     }
-    if kname in INT_PRODUCTS:
-        prods = INT_PRODUCTS[kname] * scale
+    if dom == "rs_encode":
+        prods = NTT_PRODUCTS_2P18 * (1 << log2) / (1 << 18)
         rate = prods / (phases[dom] / 1e3)
-        line["roofline"]["int_pipe"] = {"achieved_products_per_s": rate, "peak_products_per_s": int_product_peak(),
-                                        "frac": rate / int_product_peak(),
-                                        "peak_def": "148 SMs x max SM clock x 32 IMAD.WIDE per SM per clock / "
-                                                    "144 IMAD.WIDE per product"}
+        ceil = int_product_peak()
+        line["roofline"]["int_pipe"] = {
+            "products": prods, "achieved_products_per_s": rate,
+            "ceiling_as_built_products_per_s": ceil, "utilisation_as_built": rate / ceil,
+            "register_only_products_per_s": PRODUCT_REGISTER_ONLY,
+            "floor_ms_at_ceiling": prods / ceil * 1e3,
+            "ceiling_def": "the product as built: 148 SMs x max SM clock x 32 IMAD.WIDE per SM per clock / "
+                           "144 IMAD.WIDE per product; a cheaper product raises it"}
     if world == 1 and not args.no_chain:
         line.update(chain_report(prover, log2))
         line.update(verify_report(prover, log2))

@@ -20,6 +20,26 @@ struct flock_ctx {
 struct flock_setup {
   flock_ctx* ctx = nullptr;
   std::unique_ptr<flock::Setup> s;
+  size_t n_blocks = 0;  // compressions per proof (Blake3Setup::new(n_blocks))
+};
+static_assert(sizeof(flock_compression) == 28 * sizeof(uint32_t), "flock_compression is 28 u32");
+// pcs::commit's retained prover state (commit.rs:143-185): the codeword and
+// the Merkle tree, resident on the context's device.
+struct flock_prover_data {
+  flock_ctx* ctx = nullptr;
+  uint32_t m = 0;
+  size_t n_leaves = 0;
+  f128* cw = nullptr;       // [pos * 64 + lane], 2^(m-12) positions
+  uint32_t* tree = nullptr;  // flat tree, 2 * n_leaves - 1 nodes of 32 B
+  ~flock_prover_data() {
+    if (cw) cudaFree(cw);
+    if (tree) cudaFree(tree);
+  }
+};
+// FsChallenger (challenger.rs:170-600) with the BLAKE3 hash.
+struct flock_challenger {
+  flock::Transcript tr;
+  explicit flock_challenger(const std::string& domain) : tr(domain) {}
 };
 
 std::atomic<uint64_t>& kernel_launch_counter() {
@@ -103,9 +123,28 @@ int flock_setup_create(flock_ctx* c, uint32_t log2_n, int hash, int profile, flo
     auto* s = new flock_setup();
     s->ctx = c;
     s->s.reset(new flock::Setup(c->device, log2_n));
+    s->n_blocks = (size_t)1 << log2_n;
     *out = s;
     return FLOCK_OK;
   });
+}
+
+int flock_setup_create_blocks(flock_ctx* c, size_t n_blocks, int hash, int profile, flock_setup** out) {
+  if (!c || !out) return FLOCK_ERR_ARG;
+  if (n_blocks == 0) {
+    c->err = "n_blocks must be at least 1";
+    return FLOCK_ERR_ARG;
+  }
+  // min_n_blocks_log (blake3.rs:1854-1858): 2^max(3, ceil(log2 n)) slots
+  uint32_t n_log = 3;
+  while (((size_t)1 << n_log) < n_blocks) n_log++;
+  if (n_log < 8 || n_log > 20) {
+    c->err = "unsupported n_blocks (129..=2^20: the Ligerito fast profile has ladders for m = 22..34)";
+    return FLOCK_ERR_ARG;
+  }
+  const int rc = flock_setup_create(c, n_log, hash, profile, out);
+  if (rc == FLOCK_OK) (*out)->n_blocks = n_blocks;
+  return rc;
 }
 
 void flock_setup_destroy(flock_setup* s) { delete s; }
@@ -142,6 +181,167 @@ int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const u
     std::string d((const char*)domain, dlen);
     return emit(s->ctx, s->s->prove(nullptr, s->s->blocks_buf, n, d), out, cap, out_len);
   });
+}
+
+int flock_prove_compressions(flock_setup* s, const flock_compression* blocks, size_t n, const uint8_t* domain,
+                             size_t dlen, uint8_t* out, size_t cap, size_t* out_len) {
+  if (!s || !blocks || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (n != s->n_blocks) {
+    s->ctx->err = "expected exactly the setup's n_blocks compressions";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(s->ctx, [&] {
+    const size_t slots = (size_t)1 << s->s->log2;
+    if (!s->s->records_buf) CK(cudaMalloc(&s->s->records_buf, slots * 28 * sizeof(uint32_t)));
+    CK(cudaMemcpyAsync(s->s->records_buf, blocks, n * sizeof(flock_compression), cudaMemcpyHostToDevice, s->s->st));
+    std::string d((const char*)domain, dlen);
+    return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d, false, nullptr, true), out, cap, out_len);
+  });
+}
+
+int flock_pcs_commit(flock_ctx* c, const uint64_t* z_packed, uint32_t m, uint8_t* root32, flock_prover_data** out) {
+  if (!c || !z_packed || !root32 || !out) return FLOCK_ERR_ARG;
+  if (m < 22 || m > 34) {
+    c->err = "pcs_commit: m must be in 22..=34 (log_batch_size 6, rate 1/2)";
+    return FLOCK_ERR_ARG;
+  }
+  *out = nullptr;
+  return guard(c, [&] {
+    std::unique_ptr<flock_prover_data> pd(new flock_prover_data());
+    pd->ctx = c;
+    pd->m = m;
+    const size_t n_msg = (size_t)1 << (m - 7);  // packed F128 values = 2^(m-13) positions x 64 lanes
+    pd->n_leaves = (size_t)1 << (m - 12);
+    CK(cudaMalloc(&pd->cw, 2 * n_msg * sizeof(f128)));
+    CK(cudaMalloc(&pd->tree, (2 * pd->n_leaves - 1) * 32));
+    DevBuf<f128> z(n_msg);
+    CK(cudaMemcpyAsync(z.p, z_packed, n_msg * sizeof(f128), cudaMemcpyHostToDevice, c->st));
+    ntt_rs_encode(z.p, pd->cw, (int)m - 13, 64, 1, c->st);
+    merkle_build(pd->cw, pd->n_leaves, 64 * sizeof(f128), pd->tree, c->st);
+    CK(cudaMemcpyAsync(root32, pd->tree + 8 * (2 * pd->n_leaves - 2), 32, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    *out = pd.release();
+    return FLOCK_OK;
+  });
+}
+
+int flock_prover_data_open(flock_prover_data* pd, const uint64_t* positions, size_t n, uint64_t* rows_out,
+                           uint8_t* proof_out, size_t proof_cap, size_t* proof_count) {
+  if (!pd || (!positions && n) || (!rows_out && n) || !proof_count) return FLOCK_ERR_ARG;
+  flock_ctx* c = pd->ctx;
+  for (size_t i = 0; i < n; i++)
+    if (positions[i] >= pd->n_leaves || (i && positions[i] <= positions[i - 1])) {
+      c->err = "prover_data_open: positions must be sorted, distinct and below the leaf count";
+      return FLOCK_ERR_ARG;
+    }
+  return guard(c, [&] {
+    const std::vector<size_t> q(positions, positions + n);
+    const std::vector<uint64_t> ids = multiproof_ids(q, pd->n_leaves);
+    const size_t ns = ids.size() - n;
+    *proof_count = ns;
+    if (ns > proof_cap || (ns && !proof_out)) {
+      c->err = "prover_data_open: proof buffer too small";
+      return (int)FLOCK_ERR_CAPACITY;
+    }
+    DevBuf<uint64_t> idx(ids.size());
+    DevBuf<f128> rows(n * 64 + 2 * ns);
+    CK(cudaMemcpyAsync(idx.p, ids.data(), ids.size() * 8, cudaMemcpyHostToDevice, c->st));
+    if (n) {
+      count_launch();
+      k_gather_rows<<<(unsigned)((n * 64 + 255) / 256), 256, 0, c->st>>>(pd->cw, idx.p, n, 64, rows.p);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(rows_out, rows.p, n * 64 * sizeof(f128), cudaMemcpyDeviceToHost, c->st));
+    }
+    if (ns) {
+      uint32_t* nodes = reinterpret_cast<uint32_t*>(rows.p + n * 64);
+      count_launch();
+      k_gather_nodes<<<(unsigned)((ns + 127) / 128), 128, 0, c->st>>>(pd->tree, idx.p + n, ns, nodes);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(proof_out, nodes, ns * 32, cudaMemcpyDeviceToHost, c->st));
+    }
+    CK(cudaStreamSynchronize(c->st));
+    return (int)FLOCK_OK;
+  });
+}
+
+void flock_prover_data_destroy(flock_prover_data* pd) { delete pd; }
+
+int flock_challenger_create(const uint8_t* domain, size_t dlen, flock_challenger** out) {
+  if (!out || (!domain && dlen)) return FLOCK_ERR_ARG;
+  try {
+    *out = new flock_challenger(std::string((const char*)domain, dlen));
+  } catch (...) {
+    return FLOCK_ERR_INTERNAL;
+  }
+  return FLOCK_OK;
+}
+void flock_challenger_destroy(flock_challenger* ch) { delete ch; }
+int flock_challenger_observe_label(flock_challenger* ch, const uint8_t* label, size_t len) {
+  if (!ch || (!label && len)) return FLOCK_ERR_ARG;
+  ch->tr.label_bytes(label, len);
+  return FLOCK_OK;
+}
+int flock_challenger_observe_bytes(flock_challenger* ch, const uint8_t* bytes, size_t len) {
+  if (!ch || (!bytes && len)) return FLOCK_ERR_ARG;
+  ch->tr.bytes(bytes, len);
+  return FLOCK_OK;
+}
+int flock_challenger_observe_f128(flock_challenger* ch, const uint64_t* value) {
+  if (!ch || !value) return FLOCK_ERR_ARG;
+  ch->tr.f128v(mk(value[0], value[1]));
+  return FLOCK_OK;
+}
+int flock_challenger_observe_f128_slice(flock_challenger* ch, const uint64_t* values, size_t n) {
+  if (!ch || (!values && n)) return FLOCK_ERR_ARG;
+  std::vector<f128> v(n);
+  for (size_t i = 0; i < n; i++) v[i] = mk(values[2 * i], values[2 * i + 1]);
+  ch->tr.f128s(v.data(), n);
+  return FLOCK_OK;
+}
+int flock_challenger_sample_f128(flock_challenger* ch, uint64_t* out) {
+  if (!ch || !out) return FLOCK_ERR_ARG;
+  const f128 v = ch->tr.sample();
+  out[0] = v.lo;
+  out[1] = v.hi;
+  return FLOCK_OK;
+}
+int flock_challenger_sample_f128_vec(flock_challenger* ch, size_t n, uint64_t* out) {
+  if (!ch || (!out && n)) return FLOCK_ERR_ARG;
+  const std::vector<f128> v = ch->tr.sample_vec(n);
+  for (size_t i = 0; i < n; i++) { out[2 * i] = v[i].lo; out[2 * i + 1] = v[i].hi; }
+  return FLOCK_OK;
+}
+int flock_challenger_grind_pow(flock_challenger* ch, flock_ctx* c, uint32_t bits, uint64_t* nonce) {
+  if (!ch || !c || !nonce || bits > 40) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    uint64_t n = 0;
+    if (bits) {
+      uint8_t d[32];
+      ch->tr.state_digest(d);
+      DevBuf<unsigned long long> found(1);
+      unsigned long long* h = nullptr;
+      CK(cudaMallocHost(&h, 8));
+      try {
+        n = pow_search(d, bits, c->st, found.p, h);
+      } catch (...) {
+        cudaFreeHost(h);
+        throw;
+      }
+      cudaFreeHost(h);
+    }
+    ch->tr.nonce(n);
+    *nonce = n;
+    return (int)FLOCK_OK;
+  });
+}
+int flock_challenger_verify_pow(flock_challenger* ch, uint64_t nonce, uint32_t bits) {
+  if (!ch) return FLOCK_ERR_ARG;
+  return ch->tr.verify_pow(nonce, bits) ? FLOCK_OK : FLOCK_ERR_VERIFY;
+}
+int flock_challenger_state_digest(flock_challenger* ch, uint8_t* out32) {
+  if (!ch || !out32) return FLOCK_ERR_ARG;
+  ch->tr.state_digest(out32);
+  return FLOCK_OK;
 }
 
 int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const uint8_t* domain, size_t dlen,

@@ -268,6 +268,29 @@ void Transcript::label(const char* s) {
   put(n, 8);
   put(s, len);
 }
+void Transcript::label_bytes(const void* p, size_t len) {
+  uint8_t op = 2, n[8];
+  le64(len, n);
+  put(&op, 1);
+  put(n, 8);
+  put(p, len);
+}
+bool Transcript::verify_pow(uint64_t nonce, uint32_t bits) {
+  bool ok = true;
+  if (bits == 0) {
+    ok = nonce == 0;
+  } else {
+    uint8_t pre[64] = {0}, h[32];
+    state_digest(pre);
+    for (int i = 0; i < 8; i++) pre[32 + i] = (uint8_t)(nonce >> (8 * i));
+    B3 b;
+    b.update(pre, 64);
+    b.digest(h);
+    for (uint32_t k = 0; k < bits && ok; k++) ok = ((h[k / 8] >> (7 - k % 8)) & 1) == 0;
+  }
+  this->nonce(nonce);
+  return ok;
+}
 void Transcript::f128v(f128 v) {
   uint8_t b[18] = {3, 1};
   le64(v.lo, b + 2);

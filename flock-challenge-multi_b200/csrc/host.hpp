@@ -53,6 +53,12 @@ class Transcript {
   std::vector<f128> sample_vec(size_t n);
   void state_digest(uint8_t out[32]) const { h_.digest(out); }
   void nonce(uint64_t n) { uint8_t b[8]; for (int i = 0; i < 8; i++) b[i] = (uint8_t)(n >> (8 * i)); bytes(b, 8); }
+  // a label of arbitrary bytes (label() takes a C string)
+  void label_bytes(const void* p, size_t n);
+  // FsChallenger::verify_pow (challenger.rs:502-545): the BLAKE3 hash of
+  // state digest || nonce (LE) || 0^24 has `bits` leading zero bits (bits =
+  // 0: the nonce is 0); the nonce is observed either way
+  bool verify_pow(uint64_t nonce, uint32_t bits);
  private:
   void put(const void* p, size_t n) { h_.update(p, n); }
   B3 h_;

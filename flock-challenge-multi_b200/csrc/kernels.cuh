@@ -38,6 +38,22 @@ struct CudaError : std::runtime_error {
                       std::to_string(__LINE__));                                                \
   } while (0)
 
+// Makes `device` current for a scope and restores the caller's device after
+// it, so that a library call leaves the calling thread's device as it was.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int device) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != device) CK(cudaSetDevice(device));
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
 // K0
 void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
                          f128* b, cudaStream_t s);
@@ -101,6 +117,11 @@ void merkle_top_batch(const BatchJob* jobs, int n_jobs, cudaStream_t s);
 void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, cudaStream_t s);
 void merkle_leaves(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* out, cudaStream_t s);
 __global__ void k_gather_nodes(const uint32_t* tree, const uint64_t* idx, size_t n, uint32_t* out);
+// The sorted distinct leaf positions q followed by the flat-tree indices of
+// their Merkle multi-proof's sibling nodes, in the order the proof lists them
+// (merkle.rs:1020-1072: per level, the sibling of every position whose
+// sibling is not itself opened).
+std::vector<uint64_t> multiproof_ids(const std::vector<size_t>& q, size_t n_leaves);
 __global__ void k_gather_rows(const f128* cw, const uint64_t* pos, size_t n, int lanes, f128* out);
 uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, unsigned long long* d_found,
                     unsigned long long* h_found);

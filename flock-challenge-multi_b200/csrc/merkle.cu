@@ -165,6 +165,25 @@ void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t*
   if (len > 1) count_launch(), k_merkle_top<<<1, 512, 0, s>>>(tree, start, len);
 }
 
+std::vector<uint64_t> multiproof_ids(const std::vector<size_t>& q, size_t n_leaves) {
+  std::vector<uint64_t> ids(q.begin(), q.end());
+  std::vector<size_t> act(q);
+  size_t ls = 0, ll = n_leaves;  // first index and width of the current level
+  while (ll > 1) {
+    size_t w = 0, i = 0;
+    while (i < act.size()) {
+      const size_t p = act[i];
+      if (i + 1 < act.size() && act[i + 1] == (p ^ 1)) i += 2;
+      else { ids.push_back(ls + (p ^ 1)); i += 1; }
+      act[w++] = p >> 1;
+    }
+    act.resize(w);
+    ls += ll;
+    ll >>= 1;
+  }
+  return ids;
+}
+
 __global__ void k_gather_nodes(const uint32_t* __restrict__ tree, const uint64_t* __restrict__ idx, size_t n,
                                uint32_t* __restrict__ out) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -1,13 +1,13 @@
 // Merkle root of device-resident leaves without allocating any memory.
 //
 // Who needs this: callers that are not allowed to allocate device memory at
-// the point where they want a commitment root — for example a host running
-// inside a CUDA stream capture (cudaMalloc is not permitted while a capture is
-// open on the legacy stream), a real-time or embedded host whose memory is
-// fixed up front, or a plugin that only receives buffers from an outer
-// framework which owns every allocation.  They already hold the leaves and a
-// 32-byte output slot in device-accessible memory; everything else this entry
-// point needs lives in the fixed array below.
+// the point where they want a commitment root — for example a real-time or
+// embedded host whose device memory is all reserved up front (an allocation
+// there may fail or stall for an unbounded time), or a plugin that only
+// receives buffers from an outer framework which owns every allocation and
+// its accounting.  They already hold the leaves and a 32-byte output slot in
+// device-accessible memory; everything else this entry point needs lives in
+// the fixed array below.
 //
 // The intermediate tree (all 2n - 1 nodes) is kept in a file-scope device
 // array sized for at most kMaxLeaves leaves.  Every GPU that loads the library
@@ -19,7 +19,11 @@
 // it keeps the previous call's contents: every node is written before it is
 // read, so nothing needs clearing, but two calls whose work overlaps on the
 // GPU (different streams, or different host threads on one device) race on the
-// array and must be serialised by the caller.
+// array and must be serialised by the caller.  The address is cached for the
+// life of the process, so resetting a device (cudaDeviceReset) after its first
+// call is not supported.  A CUDA error already pending on the calling thread
+// is left in place for its owner and the call returns FLOCK_ERR_CUDA without
+// doing any work.
 #include "../../include/flock_gpu.h"
 #include "kernels.cuh"
 #include <mutex>
@@ -54,6 +58,9 @@ extern "C" int flock_merkle_root_noalloc(const void* leaves, size_t n_leaves, si
       leaf_size > 1024 || (leaf_size % 16))
     return FLOCK_ERR_ARG;
   if (n_leaves > kMaxLeaves) return FLOCK_ERR_CAPACITY;  // the fixed array holds 2^15 leaves at most
+  // an earlier, unrelated error stays pending for its owner: this call neither
+  // clears it nor reports it as its own launch failure
+  if (cudaPeekAtLastError() != cudaSuccess) return FLOCK_ERR_CUDA;
   uint32_t* tree = nullptr;
   int rc = scratch_for_current_device(&tree);
   if (rc) return rc;

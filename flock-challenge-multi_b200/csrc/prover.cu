@@ -355,22 +355,7 @@ std::vector<size_t> Setup::sample_queries(Transcript& tr, size_t block_len, size
 // together and read back with one synchronisation.
 void Setup::open(Opening& o, const f128* cw, const uint32_t* tree, size_t n_leaves, int lanes,
                  const std::vector<size_t>& q) {
-  std::vector<uint64_t> ids(q.begin(), q.end());
-  // sibling indices of the multi-proof, after the query positions
-  std::vector<size_t> act(q);
-  size_t ls = 0, ll = n_leaves;
-  while (ll > 1) {
-    size_t w = 0, i = 0;
-    while (i < act.size()) {
-      size_t p = act[i];
-      if (i + 1 < act.size() && act[i + 1] == (p ^ 1)) i += 2;
-      else { ids.push_back(ls + (p ^ 1)); i += 1; }
-      act[w++] = p >> 1;
-    }
-    act.resize(w);
-    ls += ll;
-    ll >>= 1;
-  }
+  const std::vector<uint64_t> ids = multiproof_ids(q, n_leaves);
   const size_t nq = q.size(), ns = ids.size() - nq, nr = nq * lanes;
   if (ids.size() > ((size_t)1 << 16) || nr + 2 * ns > ((size_t)1 << 16))
     throw std::runtime_error("opening larger than the gather buffers");
@@ -420,7 +405,8 @@ void Setup::mark(int phase) {
 // the runtime stages before the call returns: the stream needs no
 // synchronisation except where the transcript reads a device value.
 std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
-                                  const std::string& domain, bool committed, const ChainEnds* chain) {
+                                  const std::string& domain, bool committed, const ChainEnds* chain,
+                                  bool full_records) {
   Proof P;
   P.m = (uint64_t)m;
   pending_.clear();  // (left over only by a proof that threw)
@@ -431,7 +417,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   if (!committed) {
     // ---- K0 witness
     if (seed) launch_witness_seed(*seed, log2, 1u << log2, n_slots, z, a, b, st);
-    else launch_witness_blocks(blocks_dev, (uint32_t)n_blocks, n_slots, z, a, b, st, chain != nullptr);
+    else launch_witness_blocks(blocks_dev, (uint32_t)n_blocks, n_slots, z, a, b, st, chain != nullptr || full_records);
     CK(cudaGetLastError());
   }
   mark(1);

@@ -91,8 +91,12 @@ class Setup {
   // chain != nullptr: a hash-chain proof (Blake3Setup::prove_chain,
   // blake3.rs:5195-5215) whose bundle carries these endpoints; blocks_dev
   // then holds 2^log2 records of 28 u32 (cv, m, counter u64, block_len, flags).
+  // full_records: blocks_dev holds n_blocks such 28-u32 records for a
+  // compression proof; the slots from n_blocks on hold the all-zero
+  // compression, as in the reference's padded prove_fast.
   std::vector<uint8_t> prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
-                             const std::string& domain, bool committed = false, const ChainEnds* chain = nullptr);
+                             const std::string& domain, bool committed = false, const ChainEnds* chain = nullptr,
+                             bool full_records = false);
   // Replays and checks a FLOCK v4 bundle of this statement size (compression
   // or hash chain; a chain's public endpoints are the bundle's); "" when it
   // verifies, otherwise the name of the failed check.  Uses this setup's

@@ -380,22 +380,7 @@ std::vector<std::vector<H32>> opened_leaf_cvs(const Proof& P, const VerifyStatem
 // FsChallenger::verify_pow (challenger.rs:502-545): the BLAKE3 hash of
 // state digest || nonce (LE) || 0^24 has `bits` leading zero bits (bits = 0:
 // the nonce is 0); the nonce is observed either way
-bool pow_ok(Transcript& tr, uint64_t nonce, uint32_t bits) {
-  bool ok = true;
-  if (bits == 0) {
-    ok = nonce == 0;
-  } else {
-    uint8_t pre[64] = {0}, h[32];
-    tr.state_digest(pre);
-    for (int i = 0; i < 8; i++) pre[32 + i] = (uint8_t)(nonce >> (8 * i));
-    B3 b;
-    b.update(pre, 64);
-    b.digest(h);
-    for (uint32_t k = 0; k < bits && ok; k++) ok = ((h[k / 8] >> (7 - k % 8)) & 1) == 0;
-  }
-  tr.nonce(nonce);
-  return ok;
-}
+bool pow_ok(Transcript& tr, uint64_t nonce, uint32_t bits) { return tr.verify_pow(nonce, bits); }
 
 // A Ligerito round's quadratic from its message (u0, u2) and running claim
 // (pcs/ligerito.rs:4929-4958)
@@ -910,7 +895,7 @@ std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& d
 }
 
 Verifier::Verifier(int device) : device_(device) {
-  CK(cudaSetDevice(device));
+  DeviceScope on(device);
   CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
   CK(cudaMalloc(&eqx_, 256 * sizeof(f128)));
   CK(cudaMalloc(&eqi_, kK * sizeof(f128)));
@@ -920,9 +905,13 @@ Verifier::Verifier(int device) : device_(device) {
 }
 
 Verifier::~Verifier() {
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device_);
   if (st_) cudaStreamSynchronize(st_);
   for (void* p : {(void*)eqx_, (void*)eqi_, (void*)comb_, (void*)rows_, (void*)cvs_}) cudaFree(p);
   if (st_) cudaStreamDestroy(st_);
+  if (prev >= 0) cudaSetDevice(prev);
 }
 
 std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string& domain) {
@@ -933,6 +922,9 @@ std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string
   uint64_t mm = 0;
   for (int k = 0; k < 8; k++) mm |= (uint64_t)bytes[at + k] << (8 * k);
   if (mm < (uint64_t)kKLog + 8 || mm > (uint64_t)kKLog + 20) return "bundle is for an unsupported statement size";
+  // the stream and buffers belong to device_, whichever device the calling
+  // thread has current; the caller's device is restored on return
+  DeviceScope on(device_);
   const DevCsc& C = shared_csc(device_);
   const VerifyBufs B{eqx_, eqi_, comb_, rows_, cvs_, kRowsCap, kCvsCap};
   return verify_bundle(bytes, len, domain,

@@ -1,11 +1,14 @@
 // flock_worker: the B200 prover behind the reference benchmark-worker process
 // protocol (benchmark-tools/worker/src/main.rs:14-49, harness worker_command
 // benchmark-tools/harness/src/main.rs:215-352):
-//   flock_worker LOG2 READY_PATH PROOF_PATH
+//   flock_worker LOG2 READY_PATH PROOF_PATH [RECORD_DIR]
 // Untimed: context, setup for 2^LOG2 compressions and one warm-up proof, then
 // READY_PATH is created.  Timed: read the decimal seed from stdin, prove the
 // benchmark inputs of that seed, write PROOF_PATH.tmp and rename it to
 // PROOF_PATH.  Uses only the C ABI of libflockgpu.so.
+// With RECORD_DIR (not part of the reference protocol; a wrapper script adds
+// it), the proof is also written to RECORD_DIR/proof_<LOG2>_<seed>.bin before
+// it is published, so a harness run leaves (seed, proof) pairs behind.
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -25,8 +28,8 @@ int fail(flock_ctx* ctx, const char* what, int rc) {
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 4) {
-    fprintf(stderr, "usage: flock_worker LOG2 READY_PATH PROOF_PATH\n");
+  if (argc != 4 && argc != 5) {
+    fprintf(stderr, "usage: flock_worker LOG2 READY_PATH PROOF_PATH [RECORD_DIR]\n");
     return 2;
   }
   const int log2 = atoi(argv[1]);
@@ -55,6 +58,12 @@ int main(int argc, char** argv) {
   const uint64_t seed = std::stoull(line);
   rc = flock_prove_seed(setup, seed, dom, strlen(kDomain), proof.data(), proof.size(), &len);
   if (rc) return fail(ctx, "proof", rc);
+  if (argc == 5) {
+    const std::string rec = std::string(argv[4]) + "/proof_" + std::to_string(log2) + "_" + std::to_string(seed) + ".bin";
+    FILE* f = fopen(rec.c_str(), "wb");
+    if (!f || fwrite(proof.data(), 1, len, f) != len) return fail(ctx, "writing the record", 0);
+    fclose(f);
+  }
   const std::string tmp = std::string(argv[3]) + ".tmp";
   FILE* pf = fopen(tmp.c_str(), "wb");
   if (!pf || fwrite(proof.data(), 1, len, pf) != len) return fail(ctx, "writing PROOF_PATH.tmp", 0);

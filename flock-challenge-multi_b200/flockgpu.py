@@ -29,6 +29,11 @@ EXPORTS = (
     "flock_serve_start", "flock_submit", "flock_poll", "flock_sumcheck_round3", "flock_bench_sumcheck3",
     "flock_ntt_autotune", "flock_ntt_rs_encode_plan", "flock_prove_batch", "flock_host_alloc",
     "flock_host_free", "flock_prove_chain", "flock_chain_blocks", "flock_verify", "flock_serve_verify", "flock_verify_bundle",
+    "flock_setup_create_blocks", "flock_prove_compressions", "flock_pcs_commit", "flock_prover_data_open",
+    "flock_prover_data_destroy", "flock_challenger_create", "flock_challenger_destroy",
+    "flock_challenger_observe_label", "flock_challenger_observe_bytes", "flock_challenger_observe_f128",
+    "flock_challenger_observe_f128_slice", "flock_challenger_sample_f128", "flock_challenger_sample_f128_vec",
+    "flock_challenger_grind_pow", "flock_challenger_verify_pow", "flock_challenger_state_digest",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -67,6 +72,22 @@ def load() -> ctypes.CDLL:
         lib.flock_ctx_destroy.argtypes = [vp]
         lib.flock_setup_create.argtypes = [vp, u32, i32, i32, ctypes.POINTER(vp)]
         lib.flock_setup_destroy.argtypes = [vp]
+        lib.flock_pcs_commit.argtypes = [vp, vp, u32, vp, ctypes.POINTER(vp)]
+        lib.flock_prover_data_open.argtypes = [vp, vp, sz, vp, vp, sz, ctypes.POINTER(sz)]
+        lib.flock_prover_data_destroy.argtypes = [vp]
+        lib.flock_challenger_create.argtypes = [ctypes.c_char_p, sz, ctypes.POINTER(vp)]
+        lib.flock_challenger_destroy.argtypes = [vp]
+        lib.flock_challenger_observe_label.argtypes = [vp, ctypes.c_char_p, sz]
+        lib.flock_challenger_observe_bytes.argtypes = [vp, ctypes.c_char_p, sz]
+        lib.flock_challenger_observe_f128.argtypes = [vp, vp]
+        lib.flock_challenger_observe_f128_slice.argtypes = [vp, vp, sz]
+        lib.flock_challenger_sample_f128.argtypes = [vp, vp]
+        lib.flock_challenger_sample_f128_vec.argtypes = [vp, sz, vp]
+        lib.flock_challenger_grind_pow.argtypes = [vp, vp, u32, ctypes.POINTER(u64)]
+        lib.flock_challenger_verify_pow.argtypes = [vp, u64, u32]
+        lib.flock_challenger_state_digest.argtypes = [vp, vp]
+        lib.flock_setup_create_blocks.argtypes = [vp, sz, i32, i32, ctypes.POINTER(vp)]
+        lib.flock_prove_compressions.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_prove_seed.argtypes = [vp, u64, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_prove_blocks.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_setup_phase_ms.argtypes = [vp, vp, i32]
@@ -104,6 +125,17 @@ def load() -> ctypes.CDLL:
 
 def _ptr(a: np.ndarray) -> ctypes.c_void_p:
     return ctypes.c_void_p(a.ctypes.data)
+
+
+def to_records(blocks: np.ndarray, block_len: int = 64, flags: int = 11) -> np.ndarray:
+    """(n, 25) benchmark compressions (cv, m, counter_lo) -> (n, 28)
+    flock_compression records with the given block_len and flags."""
+    blocks = np.ascontiguousarray(blocks, np.uint32).reshape(-1, 25)
+    rec = np.zeros((blocks.shape[0], 28), np.uint32)
+    rec[:, :25] = blocks
+    rec[:, 26] = block_len
+    rec[:, 27] = flags
+    return rec
 
 
 def generate_compressions(log2: int, seed: int) -> np.ndarray:
@@ -355,14 +387,116 @@ class Context:
         return ms.value
 
 
+class Challenger:
+    """FsChallenger with the BLAKE3 hash (crates/flock-core/src/challenger.rs:
+    170-600) behind the C ABI; values are (lo, hi) pairs of u64."""
+
+    def __init__(self, domain: bytes = DOMAIN):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        if self.lib.flock_challenger_create(domain, len(domain), ctypes.byref(h)):
+            raise FlockError("challenger_create failed")
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.flock_challenger_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def observe_label(self, label: bytes) -> None:
+        self.lib.flock_challenger_observe_label(self.h, label, len(label))
+
+    def observe_bytes(self, data: bytes) -> None:
+        self.lib.flock_challenger_observe_bytes(self.h, data, len(data))
+
+    def observe_f128(self, v) -> None:
+        a = np.array(v, np.uint64)
+        self.lib.flock_challenger_observe_f128(self.h, _ptr(a))
+
+    def observe_f128_slice(self, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, np.uint64).reshape(-1)
+        self.lib.flock_challenger_observe_f128_slice(self.h, _ptr(a), a.size // 2)
+
+    def sample_f128(self):
+        out = np.zeros(2, np.uint64)
+        self.lib.flock_challenger_sample_f128(self.h, _ptr(out))
+        return int(out[0]), int(out[1])
+
+    def sample_f128_vec(self, n: int) -> np.ndarray:
+        out = np.zeros(2 * max(n, 1), np.uint64)
+        self.lib.flock_challenger_sample_f128_vec(self.h, n, _ptr(out))
+        return out[: 2 * n]
+
+    def grind_pow(self, ctx: "Context", bits: int) -> int:
+        n = ctypes.c_uint64()
+        ctx._check(self.lib.flock_challenger_grind_pow(self.h, ctx.h, bits, ctypes.byref(n)), "challenger_grind_pow")
+        return n.value
+
+    def verify_pow(self, nonce: int, bits: int) -> bool:
+        return self.lib.flock_challenger_verify_pow(self.h, nonce, bits) == 0
+
+    def state_digest(self) -> bytes:
+        out = np.zeros(32, np.uint8)
+        self.lib.flock_challenger_state_digest(self.h, _ptr(out))
+        return out.tobytes()
+
+
+class ProverData:
+    """pcs::commit's retained state (codeword + Merkle tree) on the device."""
+
+    def __init__(self, ctx: "Context", z_packed: np.ndarray, m: int):
+        self.ctx = ctx
+        z = np.ascontiguousarray(z_packed, np.uint64)
+        assert z.size == 2 << (m - 7), "z_packed holds 2^(m-7) F128 values"
+        root = np.zeros(32, np.uint8)
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.flock_pcs_commit(ctx.h, _ptr(z), m, _ptr(root), ctypes.byref(h)), "pcs_commit")
+        self.h, self.m, self.root = h, m, root.tobytes()
+
+    def open(self, positions):
+        """(rows (n, 64, 2) u64, multi-proof sibling hashes (k, 32) u8)."""
+        pos = np.ascontiguousarray(positions, np.uint64)
+        rows = np.zeros((max(pos.size, 1), 64, 2), np.uint64)
+        cap = 64 * max(pos.size, 1) + 64
+        proof = np.zeros((cap, 32), np.uint8)
+        k = ctypes.c_size_t()
+        self.ctx._check(self.ctx.lib.flock_prover_data_open(self.h, _ptr(pos), pos.size, _ptr(rows), _ptr(proof), cap,
+                                                            ctypes.byref(k)), "prover_data_open")
+        return rows[: pos.size], proof[: k.value]
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.flock_prover_data_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Prover:
     """`Blake3Setup` for 2^log2 compressions with BLAKE3 Merkle hashing
-    (crates/flock-prover/src/r1cs_hashes/blake3.rs:4656-5170)."""
+    (crates/flock-prover/src/r1cs_hashes/blake3.rs:4656-5170), or, with
+    n_blocks, `Blake3Setup::new(n_blocks)` for any count (2^max(3, ceil(log2
+    n)) slots, blake3.rs:1854-1858)."""
 
-    def __init__(self, ctx: Context, log2: int):
-        self.ctx, self.log2 = ctx, log2
+    def __init__(self, ctx: Context, log2: int = None, n_blocks: int = None):
         h = ctypes.c_void_p()
-        ctx._check(ctx.lib.flock_setup_create(ctx.h, log2, 1, 0, ctypes.byref(h)), "setup_create")
+        if n_blocks is not None:
+            ctx._check(ctx.lib.flock_setup_create_blocks(ctx.h, n_blocks, 1, 0, ctypes.byref(h)), "setup_create_blocks")
+            log2 = max(3, (n_blocks - 1).bit_length())
+        else:
+            ctx._check(ctx.lib.flock_setup_create(ctx.h, log2, 1, 0, ctypes.byref(h)), "setup_create")
+            n_blocks = 1 << log2
+        self.ctx, self.log2, self.n_blocks = ctx, log2, n_blocks
         self.h = h
         self._buf = np.zeros(MAX_PROOF_BYTES * 2, np.uint8)
 
@@ -390,6 +524,17 @@ class Prover:
         rc = self.ctx.lib.flock_prove_blocks(self.h, _ptr(blocks), blocks.shape[0], domain, len(domain),
                                              _ptr(self._buf), self._buf.size, ctypes.byref(n))
         self.ctx._check(rc, "prove_blocks")
+        return self._buf[: n.value].tobytes()
+
+    def prove_compressions(self, records: np.ndarray, domain: bytes = DOMAIN) -> bytes:
+        """prove_fast over (n_blocks, 28) u32 flock_compression records (cv[8],
+        m[16], counter u64 little endian, block_len, flags); the statement's
+        slots from n_blocks on hold the all-zero compression."""
+        records = np.ascontiguousarray(records, np.uint32).reshape(-1, 28)
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_prove_compressions(self.h, _ptr(records), records.shape[0], domain, len(domain),
+                                                   _ptr(self._buf), self._buf.size, ctypes.byref(n))
+        self.ctx._check(rc, "prove_compressions")
         return self._buf[: n.value].tobytes()
 
     def prove_chain(self, records: np.ndarray, domain: bytes = CHAIN_DOMAIN) -> bytes:

@@ -18,6 +18,17 @@
  *                           blake3.rs:4846, proof_io.rs:165)
  *  - flock_prove_blocks  <- Blake3Setup::prove_fast(&blocks, &mut FsChallenger)
  *                           + to_bytes (blake3.rs:4846-4990)
+ *  - flock_pcs_commit, flock_prover_data_*
+ *                        <- pcs::commit -> (Commitment, ProverData) and the
+ *                           openings read from it (crates/flock-core/src/pcs/
+ *                           commit.rs:143-230, merkle.rs:1020-1072)
+ *  - flock_challenger_*  <- FsChallenger and the Challenger trait
+ *                           (crates/flock-core/src/challenger.rs:34-100,
+ *                           170-600)
+ *  - flock_setup_create_blocks, flock_prove_compressions
+ *                        <- Blake3Setup::new(n_blocks) (any n) + prove_fast
+ *                           over full Compression tuples (blake3.rs:1854-1861,
+ *                           4706, 4846)
  *  - flock_prove_chain   <- Blake3Setup::prove_chain(&blocks, &mut FsChallenger)
  *                           + ChainProofBundleLigerito::to_bytes (blake3.rs:
  *                           5195-5215, r1cs_hashes/chain_common.rs:287-350,
@@ -70,8 +81,26 @@ int flock_ctx_create(int device, uint64_t hbm_budget_bytes, flock_ctx** out);
 void flock_ctx_destroy(flock_ctx* ctx);
 const char* flock_last_error(flock_ctx* ctx);
 
+/* One BLAKE3 compression input, the reference's Compression tuple
+ * ([u32; 8], [u32; 16], u64, u32, u32) = (cv, m, counter, block_len, flags)
+ * (crates/flock-prover/src/r1cs_hashes/blake3.rs:1861) as a C struct of 28
+ * u32 (112 bytes; the counter little endian). */
+typedef struct flock_compression {
+  uint32_t cv[8];
+  uint32_t m[16];
+  uint64_t counter;
+  uint32_t block_len;
+  uint32_t flags;
+} flock_compression;
+
 /* Untimed setup for 2^log2_n compressions (8 <= log2_n <= 20). */
 int flock_setup_create(flock_ctx* ctx, uint32_t log2_n, int hash, int profile, flock_setup** out);
+/* Untimed setup for n_blocks compressions, any count (Blake3Setup::new(n_blocks),
+ * blake3.rs:4706-4780): the statement has 2^max(3, ceil(log2 n_blocks)) slots
+ * (min_n_blocks_log, blake3.rs:1854-1858).  Supported: 129 <= n_blocks <= 2^20
+ * (the fast profile's Ligerito ladders cover m = 22..34; the reference panics
+ * below that, FLOCK_ERR_ARG here). */
+int flock_setup_create_blocks(flock_ctx* ctx, size_t n_blocks, int hash, int profile, flock_setup** out);
 void flock_setup_destroy(flock_setup* s);
 
 /* One proof; inputs generated on the GPU from `seed` exactly as the
@@ -82,6 +111,14 @@ int flock_prove_seed(flock_setup* s, uint64_t seed, const uint8_t* domain, size_
  * block_len 64, flags 11, n == 2^log2_n. */
 int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const uint8_t* domain, size_t dlen,
                        uint8_t* out, size_t cap, size_t* out_len);
+/* One proof over caller compressions with every field free (u64 counter,
+ * block_len, flags): Blake3Setup::prove_fast(&blocks, &mut FsChallenger) +
+ * to_bytes (blake3.rs:4846-4990).  n must equal the setup's n_blocks
+ * (2^log2_n for flock_setup_create), as prove_fast asserts; the slots from n
+ * on hold the all-zero compression, the reference's padding
+ * (blake3.rs:2527, seed_pipe.rs:210-226). */
+int flock_prove_compressions(flock_setup* s, const flock_compression* blocks, size_t n, const uint8_t* domain,
+                             size_t dlen, uint8_t* out, size_t cap, size_t* out_len);
 /* One hash-chain proof: the 2^log2_n compressions form a chain
  * x_{i+1} = out_lo(compress(x_i)) with public endpoints.  records: n x 28
  * u32, each cv[8], m[16], counter (u64, little endian), block_len, flags
@@ -91,6 +128,46 @@ int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const u
  * broken chain gives a proof that the reference's verify_chain rejects. */
 int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const uint8_t* domain, size_t dlen,
                       uint8_t* out, size_t cap, size_t* out_len);
+/* The PCS layer: pcs::commit (crates/flock-core/src/pcs/commit.rs:187-230)
+ * under PcsParams {m, log_inv_rate 1, log_batch_size 6, Fast, Blake3}.  The
+ * packed polynomial z_packed (2^(m-7) F128 as {lo, hi} u64 pairs, host
+ * memory; 22 <= m <= 34) is RS-encoded as 64 interleaved lanes at rate 1/2
+ * and Merkle-hashed over its 2^(m-12) positions (1 KiB leaves, BLAKE3).
+ * Writes Commitment.root; the handle holds the ProverData (codeword and
+ * tree, commit.rs:143-185) on the context's device until it is destroyed. */
+typedef struct flock_prover_data flock_prover_data;
+int flock_pcs_commit(flock_ctx* ctx, const uint64_t* z_packed, uint32_t m, uint8_t* root32, flock_prover_data** out);
+/* The opening of sorted distinct positions that the Ligerito prover reads
+ * from ProverData (ligerito.rs:9721 merkle_multi_proof_for): their rows
+ * (n x 64 F128 into rows_out) and the Merkle multi-proof's sibling hashes
+ * (merkle.rs:1020-1072; *proof_count of 32 bytes into proof_out, or
+ * FLOCK_ERR_CAPACITY with *proof_count set when proof_cap is too small). */
+int flock_prover_data_open(flock_prover_data* pd, const uint64_t* positions, size_t n, uint64_t* rows_out,
+                           uint8_t* proof_out, size_t proof_cap, size_t* proof_count);
+void flock_prover_data_destroy(flock_prover_data* pd);
+
+/* The transcript layer: FsChallenger::with_hash(domain, Blake3) and the
+ * Challenger trait (crates/flock-core/src/challenger.rs:34-100, 170-600).
+ * observe_f128 absorbs one value and observe_f128_slice a framed slice;
+ * sample_f128 / sample_f128_vec squeeze one value / a framed vector
+ * ({lo, hi} u64 pairs).  grind_pow finds the smallest nonce whose BLAKE3
+ * hash of (state digest || nonce LE || 0^24) has `bits` leading zero bits on
+ * the context's GPU and absorbs it (grind_pow, challenger.rs:384-475);
+ * verify_pow checks a nonce and absorbs it (FLOCK_ERR_VERIFY when it fails,
+ * challenger.rs:502-545).  A challenger is used by one thread at a time. */
+typedef struct flock_challenger flock_challenger;
+int flock_challenger_create(const uint8_t* domain, size_t dlen, flock_challenger** out);
+void flock_challenger_destroy(flock_challenger* ch);
+int flock_challenger_observe_label(flock_challenger* ch, const uint8_t* label, size_t len);
+int flock_challenger_observe_bytes(flock_challenger* ch, const uint8_t* bytes, size_t len);
+int flock_challenger_observe_f128(flock_challenger* ch, const uint64_t* value);
+int flock_challenger_observe_f128_slice(flock_challenger* ch, const uint64_t* values, size_t n);
+int flock_challenger_sample_f128(flock_challenger* ch, uint64_t* out);
+int flock_challenger_sample_f128_vec(flock_challenger* ch, size_t n, uint64_t* out);
+int flock_challenger_grind_pow(flock_challenger* ch, flock_ctx* ctx, uint32_t bits, uint64_t* nonce);
+int flock_challenger_verify_pow(flock_challenger* ch, uint64_t nonce, uint32_t bits);
+int flock_challenger_state_digest(flock_challenger* ch, uint8_t* out32);
+
 /* The flock_chain CLI's honest chain of `steps` records: record i has
  * cv = x_i (x_0 = initial_cv, or the BLAKE3 IV when NULL), 16 message words
  * from SplitMix64(seed) (low 32 bits of each draw), counter 0, block_len 64,
@@ -229,8 +306,8 @@ int flock_poll(flock_ctx* ctx, uint64_t ticket, flock_result* res, int timeout_m
 int flock_prove_batch(flock_ctx* ctx, const flock_job* jobs, size_t n, flock_result* results, int threads);
 
 /* Merkle root of leaves already in device memory, for callers that may not
- * allocate device memory when they need the root (inside a stream capture,
- * fixed-memory hosts, plugins whose buffers are all owned by an outer
+ * allocate device memory when they need the root (hosts whose device memory
+ * is all reserved up front, plugins whose buffers are all owned by an outer
  * framework).  No counterpart in the reference: it exists only for such
  * callers.  `leaves` (n_leaves x leaf_size bytes) and `root_out` (32 bytes)
  * are device pointers; the work is queued on `stream` (a cudaStream_t, NULL
@@ -240,7 +317,10 @@ int flock_prove_batch(flock_ctx* ctx, const flock_job* jobs, size_t n, flock_res
  * FLOCK_ERR_CAPACITY.  Same leaf rules and same root as flock_merkle_tree.
  * The first call on a device looks the array's address up; make it before
  * any stream capture begins.  Calls share the array, so calls whose work
- * overlaps on the GPU race: serialise them. */
+ * overlaps on the GPU race: serialise them.  The address is kept for the
+ * process's lifetime: resetting the device after its first call is not
+ * supported.  A CUDA error already pending on the calling thread is left for
+ * its owner and the call returns FLOCK_ERR_CUDA without queuing work. */
 int flock_merkle_root_noalloc(const void* leaves, size_t n_leaves, size_t leaf_size, void* root_out, void* stream);
 
 #ifdef __cplusplus

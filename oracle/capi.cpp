@@ -32,6 +32,31 @@ void flockref_chain_blocks(uint64_t seed, const uint32_t* initial_cv, size_t ste
   memcpy(out28, v.data(), v.size() * sizeof(Compression));
 }
 
+// prove_fast over any n >= 1 given compressions (Blake3Setup::new(n) +
+// prove_fast, blake3.rs:1854-1858, 4706-4780, 4846): the statement has
+// 2^n_log slots with n_log = max(3, ceil(log2 n)) (min_n_blocks_log), and
+// slots n.. hold the all-zero compression (the `padding` of
+// generate_witness_with_ab_packed_and_round1_inner_impl_with_commit,
+// blake3.rs:2527, with BlockSource::with_block, seed_pipe.rs:210-226).
+int flockref_prove_records(const uint32_t* blocks28, size_t n, const uint8_t* domain, size_t dlen, uint8_t* out,
+                           size_t cap, size_t* out_len) {
+  try {
+    if (n == 0) return 3;
+    int n_log = 3;
+    while (((size_t)1 << n_log) < n) n_log++;
+    std::vector<Compression> blocks(n);
+    memcpy(blocks.data(), blocks28, n * sizeof(Compression));
+    Bundle b = prove(blocks, n_log, std::string((const char*)domain, dlen));
+    std::vector<uint8_t> bytes = serialize(b);
+    *out_len = bytes.size();
+    if (bytes.size() > cap) return 2;
+    memcpy(out, bytes.data(), bytes.size());
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
 // prove_chain over 2^log2 given compressions.  `check` receives 1 when the
 // shift argument verifies from the bundle's public endpoints and the batched
 // open's claim identity holds.  A non-null `cv_last` replaces the public

@@ -7,7 +7,7 @@ import pytest
 
 REPO = Path(__file__).resolve().parents[1]
 PKG = REPO / "flock-challenge-multi_b200"
-for p in (str(PKG), str(REPO / "tests")):
+for p in (str(PKG), str(REPO / "tests"), str(REPO / "tests" / "golden")):
     if p not in sys.path:
         sys.path.insert(0, p)
 

@@ -24,9 +24,25 @@
    from the public endpoints (chain.rs:238-300) and the batched open's claim
    identity sum_j b_combined[j] z[j] = target.  Needs no reference checkout.
 
-Usage (needs the reference checkout and a built oracle):
-    python tests/golden/make_golden.py /root/reference [--large]
+6. kernel_digests.json (--kernels) — sha256 of the oracle's outputs for the
+   largest kernel-microbenchmark shapes (additive-NTT RS encodes of up to
+   2^24 positions, Merkle trees of 2^22 x 32 B and 2^16 x 512 B leaves) over
+   seeded numpy inputs, so the GPU kernels are pinned at the sizes they are
+   benchmarked at without running the oracle on the GPU host.
+
+7. gpu_verified_proofs.json (--gpu-harness VERIFIER) — (log2, seed, sha256,
+   size) of proofs made by the GPU worker (flock-challenge-multi_b200/
+   flock_worker) under the reference's prebuilt trusted verifier, which draws
+   each seed, times the worker and verifies every proof it publishes.  Runs
+   on a machine with a GPU; VERIFIER is a copy of the reference's
+   benchmark-tools/trusted/flock_benchmark_verifier, --out names the JSON.
+   This pins sizes the oracle is too slow for (2^19, 2^20).
+
+Usage (a built oracle; REFERENCE is a checkout of the reference project):
+    python tests/golden/make_golden.py --ref REFERENCE [--large]
     python tests/golden/make_golden.py --chain
+    python tests/golden/make_golden.py --kernels
+    python tests/golden/make_golden.py --gpu-harness VERIFIER --sizes 19:2,20:2 --out FILE
 """
 import hashlib
 import json
@@ -49,9 +65,13 @@ def phi8(ref: Path) -> None:
 
 
 def verified_proofs(ref: Path, sizes=((8, 3), (9, 2), (10, 2)), name="verified_proofs.json",
-                    threads=1) -> None:
-    verifier = ref / "benchmark-tools/trusted/flock_benchmark_verifier"
-    worker = REPO / "oracle/_build/flockref_worker"
+                    threads=1, verifier: Path = None, worker: Path = None, out_path: Path = None) -> None:
+    """Runs `worker` (the oracle's by default) under the trusted verifier,
+    which draws the seeds; the wrapper appends a record directory argument, so
+    the worker leaves each published proof behind as proof_<log2>_<seed>.bin."""
+    verifier = verifier or ref / "benchmark-tools/trusted/flock_benchmark_verifier"
+    worker = worker or REPO / "oracle/_build/flockref_worker"
+    out_path = out_path or HERE / name
     out = []
     with tempfile.TemporaryDirectory() as td:
         td = Path(td)
@@ -75,10 +95,11 @@ def verified_proofs(ref: Path, sizes=((8, 3), (9, 2), (10, 2)), name="verified_p
                 seed = int(p.stem.split("_")[2])
                 data = p.read_bytes()
                 out.append({"log2": log2, "seed": seed, "sha256": hashlib.sha256(data).hexdigest(),
-                            "size": len(data), "verified_by": "reference trusted verifier"})
+                            "size": len(data), "verified_by": "reference trusted verifier",
+                            "median_s": metrics.get("median_seconds")})
             for p in rec.glob(f"proof_{log2}_*.bin"):
                 p.unlink()
-            (HERE / name).write_text(json.dumps(out, indent=1))  # after every size
+            out_path.write_text(json.dumps(out, indent=1))  # after every size
 
 
 def witness_digests() -> None:
@@ -115,16 +136,67 @@ def chain_proofs(sizes=(14, 16, 18), threads=8) -> None:
         (HERE / "chain_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
 
 
+# Largest shapes of the kernel microbenchmarks: (log2 message positions,
+# columns, log2 inverse rate) for the RS encode, (leaves, leaf bytes) for the
+# Merkle tree.  Inputs: numpy's PCG64 stream of the given seed.
+KERNEL_NTT = ((24, 1, 2), (20, 16, 1), (16, 256, 2))
+KERNEL_MERKLE = ((1 << 22, 32), (1 << 16, 512), (1 << 19, 1024))
+
+
+def ntt_input(log_msg, cols, rate):
+    import numpy as np
+    return np.random.default_rng(1000 + 37 * log_msg + cols + rate).integers(0, 2**64, 2 * (cols << log_msg),
+                                                                                dtype=np.uint64)
+
+
+def merkle_input(n_leaves, leaf_size):
+    import numpy as np
+    return np.random.default_rng(2000 + n_leaves.bit_length() + leaf_size).integers(0, 256, n_leaves * leaf_size,
+                                                                                     dtype=np.uint8)
+
+
+def kernel_digests(threads=8) -> None:
+    import os
+    os.environ["FLOCKREF_THREADS"] = str(threads)
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle_lib
+    orc = oracle_lib.Oracle()
+    out = {"ntt": [], "merkle": []}
+    for log_msg, cols, rate in KERNEL_NTT:
+        cw = orc.rs_encode(ntt_input(log_msg, cols, rate), 1 << log_msg, cols, rate)
+        out["ntt"].append({"log_msg": log_msg, "columns": cols, "log_inv_rate": rate,
+                           "sha256": hashlib.sha256(cw.tobytes()).hexdigest()})
+    for n_leaves, size in KERNEL_MERKLE:
+        tree = orc.merkle_tree(merkle_input(n_leaves, size), n_leaves, size)
+        out["merkle"].append({"leaves": n_leaves, "leaf_bytes": size,
+                              "sha256": hashlib.sha256(tree.tobytes()).hexdigest()})
+    (HERE / "kernel_digests.json").write_text(json.dumps(out, indent=1))
+
+
 if __name__ == "__main__":
-    if "--chain" in sys.argv:
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", type=Path, help="a checkout of the reference project")
+    ap.add_argument("--large", action="store_true")
+    ap.add_argument("--chain", action="store_true")
+    ap.add_argument("--kernels", action="store_true")
+    ap.add_argument("--gpu-harness", type=Path, metavar="VERIFIER")
+    ap.add_argument("--sizes", default="19:2,20:2", help="LOG2:RUNS,... for --gpu-harness")
+    ap.add_argument("--out", type=Path, default=HERE / "gpu_verified_proofs.json")
+    a = ap.parse_args()
+    if a.chain:
         chain_proofs()
-        sys.exit(0)
-    ref = Path(sys.argv[1])
-    if "--large" in sys.argv:
+    elif a.kernels:
+        kernel_digests()
+    elif a.gpu_harness:
+        sizes = tuple(tuple(int(x) for x in s.split(":")) for s in a.sizes.split(","))
+        verified_proofs(None, sizes=sizes, threads=16, verifier=a.gpu_harness,
+                        worker=REPO / "flock-challenge-multi_b200/flock_worker", out_path=a.out)
+    elif a.large:
         # full-size cases (the benchmark's 2^18 among them), one trial each:
         # the single-threaded oracle takes minutes per proof
-        verified_proofs(ref, sizes=((14, 1), (16, 1), (18, 1)), name="verified_proofs_large.json", threads=8)
+        verified_proofs(a.ref, sizes=((14, 1), (16, 1), (18, 1)), name="verified_proofs_large.json", threads=8)
     else:
-        phi8(ref)
+        phi8(a.ref)
         witness_digests()
-        verified_proofs(ref)
+        verified_proofs(a.ref)

@@ -60,6 +60,7 @@ class Oracle:
         L.flockref_chain_blocks.argtypes = [u64, vp, sz, vp]
         L.flockref_prove_chain_blocks.argtypes = [vp, u32, ctypes.c_char_p, sz, vp, vp, sz, ctypes.POINTER(sz),
                                                   ctypes.POINTER(ctypes.c_int)]
+        L.flockref_prove_records.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_time_prove.argtypes = [u32, u64, ctypes.POINTER(sz)]
         L.flockref_time_prove.restype = ctypes.c_double
         self.L = L
@@ -68,6 +69,17 @@ class Oracle:
         buf = np.zeros(1 << 20, np.uint8)
         n = ctypes.c_size_t()
         rc = self.L.flockref_prove(log2, seed, _p(buf), buf.size, ctypes.byref(n))
+        assert rc == 0, rc
+        return buf[: n.value].tobytes()
+
+    def prove_records(self, records: np.ndarray, domain: bytes = b"flock-bench-v0") -> bytes:
+        """prove_fast over (n, 28) u32 compression records, any n >= 1: the
+        statement's slots from n on hold the all-zero compression."""
+        records = np.ascontiguousarray(records, np.uint32).reshape(-1, 28)
+        buf = np.zeros(1 << 21, np.uint8)
+        n = ctypes.c_size_t()
+        rc = self.L.flockref_prove_records(_p(records), records.shape[0], domain, len(domain), _p(buf), buf.size,
+                                           ctypes.byref(n))
         assert rc == 0, rc
         return buf[: n.value].tobytes()
 

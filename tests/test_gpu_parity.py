@@ -222,3 +222,62 @@ def test_phase_times_reported(prover8):
     ph = prover8.phase_ms()
     import flockgpu
     assert list(ph) == list(flockgpu.PHASES) and all(v >= 0 for v in ph.values())
+
+
+# ---- the kernel microbenchmarks' largest shapes ----
+# The oracle's outputs for these seeded inputs are committed as digests
+# (tests/golden/kernel_digests.json, make_golden.py --kernels); the inputs are
+# regenerated here from the same PCG64 seeds.
+
+def _kernel_digests():
+    return json.loads((GOLD / "kernel_digests.json").read_text())
+
+
+@pytest.mark.parametrize("case", range(3))
+def test_ntt_largest_shapes(gpu_ctx, case):
+    import make_golden
+    row = _kernel_digests()["ntt"][case]
+    lm, cols, rate = row["log_msg"], row["columns"], row["log_inv_rate"]
+    assert (lm, cols, rate) == make_golden.KERNEL_NTT[case]
+    cw = gpu_ctx.ntt_rs_encode(make_golden.ntt_input(lm, cols, rate), lm, cols, rate)
+    assert hashlib.sha256(cw.tobytes()).hexdigest() == row["sha256"]
+
+
+@pytest.mark.parametrize("case", range(3))
+def test_merkle_largest_shapes(gpu_ctx, case):
+    import make_golden
+    row = _kernel_digests()["merkle"][case]
+    n, size = row["leaves"], row["leaf_bytes"]
+    assert (n, size) == make_golden.KERNEL_MERKLE[case]
+    tree = gpu_ctx.merkle_tree(make_golden.merkle_input(n, size), n, size)
+    assert hashlib.sha256(tree.tobytes()).hexdigest() == row["sha256"]
+
+
+def test_sumcheck_round_deg2_2p24(gpu_ctx, oracle):
+    """The degree-2 (Ligerito) round message over 2^24 values, against the
+    oracle's field products."""
+    n = 1 << 24
+    f, b = rng_u64(524, 2 * n), rng_u64(525, 2 * n)
+    F, B = f.reshape(-1, 2), b.reshape(-1, 2)
+    u0 = _xor_rows(oracle.f128_mul(F[0::2].reshape(-1), B[0::2].reshape(-1)))
+    u2 = _xor_rows(oracle.f128_mul((F[0::2] ^ F[1::2]).reshape(-1), (B[0::2] ^ B[1::2]).reshape(-1)))
+    assert list(gpu_ctx.sumcheck_round(f, b)) == [u0[0], u0[1], u2[0], u2[1]]
+
+
+@pytest.mark.parametrize("fold", [False, True])
+def test_sumcheck_round_deg3_2p24(gpu_ctx, oracle, fold):
+    """The degree-3 (zerocheck) round over 2^24 values, with and without the
+    fold at rho, against the oracle."""
+    n = 1 << 24
+    a, b = rng_u64(624 + fold, 2 * n), rng_u64(634 + fold, 2 * n)
+    if fold:
+        e = rng_u64(644, n // 2)
+        rho = (0x0F1E2D3C4B5A6978, 0x8796A5B4C3D2E1F0)
+        msg, ao, bo = gpu_ctx.sumcheck_round3(e, a, b, rho)
+        fa, fb = _fold(oracle, a, rho), _fold(oracle, b, rho)
+        assert np.array_equal(ao, fa) and np.array_equal(bo, fb)
+        assert list(msg) == _deg3_expect(oracle, e, fa, fb)
+    else:
+        e = rng_u64(654, n)
+        msg, _, _ = gpu_ctx.sumcheck_round3(e, a, b)
+        assert list(msg) == _deg3_expect(oracle, e, a, b)

@@ -121,3 +121,75 @@ def test_batch_mixes_blocks_and_waves():
         assert [hashlib.sha256(r["bytes"]).hexdigest() for r in got] == [want[j] for j in jobs]
     finally:
         ctx.close()
+
+
+def _splitmix64(seed):
+    state = seed & (2**64 - 1)
+    while True:
+        state = (state + 0x9E3779B97F4A7C15) & (2**64 - 1)
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & (2**64 - 1)
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & (2**64 - 1)
+        yield z ^ (z >> 31)
+
+
+def _job_mix(n, lo, hi, seed):
+    """The benchmark's uneven job lists: log2 = lo + floor(u (hi - lo + 1))
+    from SplitMix64(seed), each job with its own seed."""
+    g = _splitmix64(seed)
+    return [(lo + (next(g) * (hi - lo + 1) >> 64), next(g)) for _ in range(n)]
+
+
+def test_config3_mix_batched_and_queued_match_plain():
+    """BASELINE config 3 at its benchmarked size: 64 jobs of 2^12..2^18
+    compressions (SplitMix64 seed 3), plus the three full-size seeds whose
+    oracle proofs the reference's trusted verifier accepted.  Every proof of
+    the batched form and of the continuous-batching queue equals the plain
+    proof, the golden seeds equal the verified digests, and every proof passes
+    the verifier."""
+    import json
+    from pathlib import Path
+    import flockgpu
+    gold = json.loads((Path(__file__).resolve().parent / "golden/verified_proofs_large.json").read_text())
+    jobs = _job_mix(64, 12, 18, 3) + [(r["log2"], r["seed"]) for r in gold]
+    ctx = flockgpu.Context(0, hbm_budget_bytes=150 << 30)
+    try:
+        want = _alone(ctx, jobs)
+        for r in gold:
+            assert want[(r["log2"], r["seed"])] == r["sha256"]
+        ctx.serve_start(4)
+        got = ctx.prove_batch(jobs, threads=8)
+        for (l, s), r in zip(jobs, got):
+            assert hashlib.sha256(r["bytes"]).hexdigest() == want[(l, s)], ("batched", l, s)
+            assert ctx.verify(r["bytes"]) == "", ("verify", l, s)
+        tickets = [(ctx.submit(l, s), l, s) for l, s in jobs]
+        for t, l, s in tickets:
+            assert hashlib.sha256(ctx.poll(t)["bytes"]).hexdigest() == want[(l, s)], ("queued", l, s)
+    finally:
+        ctx.close()
+
+
+def test_config4_served_mix_with_largest_sizes_matches_plain():
+    """BASELINE config 4's size range (2^10..2^20): jobs arriving while others
+    run, admitted under the 150 GB budget, each equal to its plain proof; the
+    2^19 and 2^20 jobs among them pass the verifier."""
+    import random
+    import time
+    import flockgpu
+    jobs = _job_mix(20, 10, 20, 4) + [(19, 0x1919), (20, 0x2020)]
+    ctx = flockgpu.Context(0, hbm_budget_bytes=150 << 30)
+    try:
+        want = _alone(ctx, jobs)
+        ctx.serve_start(4)
+        rng = random.Random(11)
+        tickets = []
+        for l, s in jobs:
+            tickets.append((ctx.submit(l, s), l, s))
+            time.sleep(rng.expovariate(1 / 0.02))
+        for t, l, s in tickets:
+            b = ctx.poll(t)["bytes"]
+            assert hashlib.sha256(b).hexdigest() == want[(l, s)], (l, s)
+            if l >= 19:
+                assert ctx.verify(b) == "", (l, s)
+    finally:
+        ctx.close()

@@ -166,3 +166,26 @@ def test_context_verifier_without_setup(gpu_ctx, p8):
         assert gpu_ctx.verify(p9.prove_seed(2)) == ""  # another size on the same verifier
     finally:
         p9.close()
+
+
+def test_context_verifier_full_size_goldens(gpu_ctx):
+    """The setup-free verifier on the largest bundles: the 2^14, 2^16 and
+    2^18 proofs the reference's trusted verifier accepted (reproduced bit for
+    bit) and the 2^14..2^18 chain goldens, whose opened rows come closest to
+    its fixed row buffer."""
+    import flockgpu
+    proofs = json.loads((GOLD / "verified_proofs_large.json").read_text())
+    chains = json.loads((GOLD / "chain_proofs.json").read_text())
+    for log2 in sorted({r["log2"] for r in proofs} | {r["log2"] for r in chains}):
+        p = flockgpu.Prover(gpu_ctx, log2)
+        try:
+            for r in [r for r in proofs if r["log2"] == log2]:
+                b = p.prove_seed(r["seed"])
+                assert hashlib.sha256(b).hexdigest() == r["sha256"]
+                assert gpu_ctx.verify(b) == "", log2
+            for r in [r for r in chains if r["log2"] == log2]:
+                b = p.prove_chain(flockgpu.chain_blocks(r["seed"], 1 << log2))
+                assert hashlib.sha256(b).hexdigest() == r["sha256"]
+                assert gpu_ctx.verify(b, CHAIN_DOMAIN) == "", log2
+        finally:
+            p.close()

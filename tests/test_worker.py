@@ -15,14 +15,17 @@ def test_worker_rejects_bad_arguments():
     assert WORKER.exists(), "flock_worker is not built"
     assert subprocess.run([str(WORKER)], capture_output=True).returncode == 2
     assert subprocess.run([str(WORKER), "7", "r", "p"], capture_output=True).returncode == 2
+    assert subprocess.run([str(WORKER), "9", "r", "p", "d", "x"], capture_output=True).returncode == 2
 
 
 @pytest.mark.gpu
 def test_worker_protocol_matches_prover(tmp_path):
     import flockgpu
     log2, seed = 9, 424242
-    ready, proof = tmp_path / "ready", tmp_path / "proof.bin"
-    p = subprocess.Popen([str(WORKER), str(log2), str(ready), str(proof)], stdin=subprocess.PIPE)
+    ready, proof, rec = tmp_path / "ready", tmp_path / "proof.bin", tmp_path / "rec"
+    rec.mkdir()
+    # the optional fourth argument records (seed, proof) for harness runs
+    p = subprocess.Popen([str(WORKER), str(log2), str(ready), str(proof), str(rec)], stdin=subprocess.PIPE)
     try:
         t0 = time.time()
         while not ready.exists():
@@ -36,6 +39,7 @@ def test_worker_protocol_matches_prover(tmp_path):
         if p.poll() is None:
             p.kill()
     assert not (tmp_path / "proof.bin.tmp").exists()
+    assert (rec / f"proof_{log2}_{seed}.bin").read_bytes() == proof.read_bytes()
     ctx = flockgpu.Context(0)
     try:
         pr = flockgpu.Prover(ctx, log2)
