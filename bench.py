@@ -262,21 +262,44 @@ def job_mix(n: int, lo: int, hi: int, seed: int):
     return [(lo + (next(g) * (hi - lo + 1) >> 64), next(g)) for _ in range(n)]
 
 
-def plain_seconds(ctx, jobs):
+def plain_seconds(ctx, jobs, per_job=False):
     """Wall time of the jobs proved one at a time through the plain entry point
-    (setups made beforehand, untimed)."""
+    (setups made beforehand, untimed); with per_job, also each job's own
+    time alone (ms), in job order."""
     import flockgpu
     provers = {l: flockgpu.Prover(ctx, l) for l in sorted({l for l, _ in jobs})}
     try:
         for l, p in provers.items():
             p.prove_seed(1)  # warm
+        each = []
         t0 = time.perf_counter()
         for l, s in jobs:
+            t1 = time.perf_counter()
             provers[l].prove_seed(s)
-        return time.perf_counter() - t0
+            each.append((time.perf_counter() - t1) * 1e3)
+        total = time.perf_counter() - t0
+        return (total, each) if per_job else total
     finally:
         for p in provers.values():
             p.close()
+
+
+# size classes of the served report (log2 ranges, inclusive)
+SIZE_CLASSES = ((10, 12), (13, 16), (17, 18), (19, 20))
+
+
+def by_size_class(jobs, lat, alone):
+    """p50 / p99 latency per size class, beside the same jobs' latency alone."""
+    out = []
+    for lo, hi in SIZE_CLASSES:
+        idx = [i for i, (l, _) in enumerate(jobs) if lo <= l <= hi]
+        if not idx:
+            continue
+        L, A = [lat[i] for i in idx], [alone[i] for i in idx]
+        out.append({"log2": [lo, hi], "jobs": len(idx), "p50_ms": pct(L, 0.5), "p99_ms": pct(L, 0.99),
+                    "alone_p50_ms": pct(A, 0.5), "alone_p99_ms": pct(A, 0.99),
+                    "p99_over_alone_p99": pct(L, 0.99) / pct(A, 0.99)})
+    return out
 
 
 def served_run(ctx, jobs, rate=None):
@@ -316,7 +339,7 @@ def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: i
         # the plain one-at-a-time times first, before the serving cache holds
         # its setups (the plain provers' memory is outside that budget)
         plain_batch = plain_seconds(ctx, batch_jobs)
-        plain_serve = plain_seconds(ctx, serve_jobs)
+        plain_serve, alone_serve = plain_seconds(ctx, serve_jobs, per_job=True)
         ctx.serve_start(slots)
         jobs = batch_jobs
         n = sum(1 << l for l, _ in jobs)
@@ -356,7 +379,8 @@ def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: i
                                   "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
                                   "sustained_value": n / wall, "plain_value": n / plain,
                                   "unit": "compressions/s", "slots": slots,
-                                  "hbm_budget_gb": 150})
+                                  "hbm_budget_gb": 150,
+                                  "by_size_class": by_size_class(jobs, lat, alone_serve)})
     finally:
         ctx.close()
     return out

@@ -745,6 +745,36 @@ int flock_bench_ntt(flock_ctx* c, uint32_t log_msg_pos, uint32_t lanes, uint32_t
   });
 }
 
+int flock_ntt_plan_desc(uint32_t log_msg_pos, uint32_t lanes, uint32_t rate, uint32_t plan_index, char* desc,
+                        size_t desc_cap) {
+  if (!desc || !desc_cap || lanes == 0 || (lanes & (lanes - 1)) || log_msg_pos + rate > 30 || rate < 1)
+    return FLOCK_ERR_ARG;
+  try {
+    const std::string d = ntt_plan_desc_at((int)(log_msg_pos + rate), (int)lanes, (int)rate, plan_index);
+    if (d.empty()) return FLOCK_ERR_ARG;
+    std::snprintf(desc, desc_cap, "%s", d.c_str());
+  } catch (...) {
+    return FLOCK_ERR_INTERNAL;
+  }
+  return FLOCK_OK;
+}
+
+int flock_bench_ntt_plan(flock_ctx* c, uint32_t log_msg_pos, uint32_t lanes, uint32_t rate, uint32_t plan_index,
+                         int iters, double* ms) {
+  if (!c || !ms || iters < 1 || lanes == 0 || (lanes & (lanes - 1)) || rate < 1 || log_msg_pos + rate > 30)
+    return FLOCK_ERR_ARG;
+  if (plan_index >= ntt_plan_count((int)(log_msg_pos + rate), (int)lanes, (int)rate)) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    size_t n = ((size_t)lanes) << log_msg_pos, nc = n << rate;
+    DevBuf<f128> dm(n), dc(nc);
+    k_fill<<<(unsigned)((2 * n + 255) / 256), 256, 0, c->st>>>((uint64_t*)dm.p, 2 * n, 1);
+    *ms = time_launches(c->st, iters, [&] {
+      ntt_rs_encode_plan(dm.p, dc.p, (int)log_msg_pos, (int)lanes, (int)rate, plan_index, c->st);
+    });
+    return FLOCK_OK;
+  });
+}
+
 int flock_bench_merkle(flock_ctx* c, size_t n_leaves, size_t leaf_size, int iters, double* ms) {
   if (!c || !ms || iters < 1 || leaf_size % 16 || leaf_size > 1024) return FLOCK_ERR_ARG;
   return guard(c, [&] {

@@ -66,6 +66,11 @@ void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n
 // tile, threads per CTA) that cover layers layer_begin..log_d-1.
 struct NttPass {
   int l0, R, lgs, threads;
+  // 0: a thread owns a position pair and its lanes, products by integer
+  // multiplies; 1: a warp owns a position pair's 64 lanes (lgs = 6) and
+  // multiplies through a 4-bit window table of the warp-uniform twiddle;
+  // 2: as 1, with half of the lanes through the integer product
+  int kind = 0;
 };
 using NttPlan = std::vector<NttPass>;
 // Times the candidate plans of a shape on `scratch` (lanes << log_d values,
@@ -77,6 +82,8 @@ const f128* ntt_evals(int log_d);  // device table of the per-layer basis values
 std::string ntt_plan_desc(const NttPlan& plan);
 // every candidate plan of a shape, for parity tests of the tiling
 size_t ntt_plan_count(int log_d, int lanes, int layer_begin);
+// the description of candidate plan `index` ("" past the last one)
+std::string ntt_plan_desc_at(int log_d, int lanes, int layer_begin, size_t index);
 void ntt_rs_encode_plan(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, size_t plan_idx,
                         cudaStream_t s);
 void ntt_rs_encode(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, cudaStream_t s);
@@ -96,8 +103,8 @@ struct BatchJob {
   int log_d;
   uint64_t msg_len, rep0;  // message values; first element in the replicate launch
   int n_pass;
-  NttPass pass[3];
-  uint64_t tile0[3];  // first tile of this job in the launch of pass p
+  NttPass pass[4];
+  uint64_t tile0[4];  // first tile of this job in the launch of pass p
   uint32_t* tree;     // Merkle tree over 2^log_d leaves of 1 KiB
   uint64_t n_leaves, leaf0;
   uint64_t par0[24];  // first node of this job in the launch of parent level k

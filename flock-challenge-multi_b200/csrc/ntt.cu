@@ -33,7 +33,15 @@ struct PassArgs {
   f128* data;
   const f128* ev;  // ev[l * 32 + j] = W^_{d-l-1}(beta_{d-l+j}), j < l
   int log_d, lanes, lg_shift, l0, R;
+  // The first pass of an RS encode reads its tiles from the message instead
+  // of from a replicated codeword: position p of the data holds message
+  // position p & src_mask (the rate-2^-r replicate, layer 0..r-1 copies).
+  const f128* src = nullptr;
+  uint64_t src_mask = 0;
 };
+__device__ __forceinline__ const f128* tile_src(const PassArgs& p, uint64_t pos) {
+  return p.src ? p.src + (pos & p.src_mask) * p.lanes : p.data + pos * p.lanes;
+}
 
 __device__ __forceinline__ f128 twiddle(const f128* ev, int l, uint64_t b) {
   f128 t = mk(0, 0);
@@ -61,7 +69,7 @@ __device__ __forceinline__ void ntt_tile(const PassArgs& p, uint64_t t_id, f128*
   for (int e = threadIdx.x; e < n_el; e += blockDim.x) {
     uint64_t pl = (uint64_t)(e >> p.lg_shift);
     uint64_t pos = (hi << (log_d - l0)) | (pl << lo_bits) | lo;
-    tile[e] = ld(p.data + pos * p.lanes + ((size_t)grp << p.lg_shift) + (e & (LG - 1)));
+    tile[e] = ld(tile_src(p, pos) + ((size_t)grp << p.lg_shift) + (e & (LG - 1)));
     if (TRANSPOSE) any |= tile[e].lo | tile[e].hi;
   }
   // The transposed transform (the query-basis induction) starts from a vector
@@ -149,6 +157,160 @@ __device__ __forceinline__ void ntt_tile(const PassArgs& p, uint64_t t_id, f128*
   }
 }
 
+// ---- warp-per-pair passes: warp-uniform twiddles, table products ----
+// A tile holds 2^R positions x 64 lanes.  A warp owns one position pair at a
+// time (thread t takes lanes t and t + 32), so the pair's twiddle is uniform
+// across the warp in every stage, and the warp multiplies by it through a
+// 4-bit window table of the twiddle: entry n of window w is
+// t * n(x) * x^(4w), and a product is the XOR of 32 lookups, one per nibble
+// of the other factor.  The halves of an entry sit in separate 8-byte arrays
+// and window w's entries are permuted by n -> n ^ (w mod 16), so the warp's
+// lookups into one window, and the builder's stores, hit 16 distinct bank
+// pairs.  A warp's consecutive pairs share the twiddle in all but the last
+// stages, and the table is rebuilt only when the twiddle changes.  The
+// table lookups load the shared-memory pipe instead of the integer
+// multipliers; KIND 2 sends lane t + 32 through the integer product, so both
+// pipes work.
+struct Tab4 {
+  uint64_t lo[32][16], hi[32][16];
+};
+constexpr size_t kTab4Bytes = sizeof(Tab4);  // 8 KiB
+
+__device__ __forceinline__ f128 mul_x128(f128 a, int k) {  // a * x^k, 0 <= k < 128
+  if (k >= 64) {
+    a = reduce256(0, a.lo, a.hi, 0);
+    k -= 64;
+  }
+  return mul_xk(a, k);
+}
+// thread `lane` of the warp writes window `lane`
+__device__ __forceinline__ void tab4_build(Tab4* T, f128 t, int lane) {
+  const f128 b0 = mul_x128(t, 4 * lane), b1 = mul_xk(b0, 1), b2 = mul_xk(b0, 2), b3 = mul_xk(b0, 3);
+  f128 e[16];
+  e[0] = mk(0, 0);
+  e[1] = b0;
+  e[2] = b1;
+  e[3] = fx(b0, b1);
+#pragma unroll
+  for (int j = 4; j < 8; j++) e[j] = fx(e[j - 4], b2);
+#pragma unroll
+  for (int j = 8; j < 16; j++) e[j] = fx(e[j - 8], b3);
+  const int r = lane & 15;
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    T->lo[lane][j ^ r] = e[j].lo;
+    T->hi[lane][j ^ r] = e[j].hi;
+  }
+}
+__device__ __forceinline__ f128 tab4_mul(const Tab4* T, f128 y) {
+  uint64_t alo = 0, ahi = 0;
+#pragma unroll
+  for (int w = 0; w < 32; w++) {
+    const uint64_t word = w < 16 ? y.lo : y.hi;
+    const uint32_t n = ((uint32_t)(word >> (4 * (w & 15))) & 15u) ^ (uint32_t)(w & 15);
+    alo ^= T->lo[w][n];
+    ahi ^= T->hi[w][n];
+  }
+  return mk(alo, ahi);
+}
+
+size_t pass_w_smem(int R, int threads) {
+  return ((size_t)64 << R) * sizeof(f128) + ((size_t)1 << R) * sizeof(f128) + (size_t)(threads / 32) * kTab4Bytes;
+}
+
+template <bool TRANSPOSE, int KIND>
+__device__ __forceinline__ void ntt_tile_w(const PassArgs& p, uint64_t t_id, f128* smem) {
+  const int R = p.R;
+  f128* tile = smem;                         // [2^R][64]
+  f128* tw = smem + ((size_t)64 << R);       // [2^R - 1], padded to 2^R
+  Tab4* tabs = reinterpret_cast<Tab4*>(tw + (1 << R));
+  const int log_d = p.log_d, l0 = p.l0;
+  const int lo_bits = log_d - l0 - R;
+  const int groups = p.lanes >> 6;
+  const int grp = (int)(t_id % groups);
+  t_id /= groups;
+  const uint64_t lo = t_id & ((1ull << lo_bits) - 1);
+  const uint64_t hi = t_id >> lo_bits;
+  const int n_el = 64 << R;
+  uint64_t any = 0;
+  for (int e = threadIdx.x; e < n_el; e += blockDim.x) {
+    const uint64_t pl = (uint64_t)(e >> 6);
+    const uint64_t pos = (hi << (log_d - l0)) | (pl << lo_bits) | lo;
+    tile[e] = ld(tile_src(p, pos) + ((size_t)grp << 6) + (e & 63));
+    if (TRANSPOSE) any |= tile[e].lo | tile[e].hi;
+  }
+  if (TRANSPOSE && !__syncthreads_or(any != 0)) return;
+  for (int k = threadIdx.x; k < (1 << R) - 1; k += blockDim.x) {
+    const int s = 31 - __clz(k + 1);
+    const uint64_t blk = (uint64_t)(k + 1 - (1 << s));
+    tw[k] = twiddle(p.ev, l0 + s, (hi << s) | blk);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  Tab4* T = tabs + warp;
+  const int chunk = (1 << (R - 1)) / nw;  // position pairs per warp per stage (the host keeps nw <= 2^(R-1))
+  for (int stg = 0; stg < R; stg++) {
+    const int s = TRANSPOSE ? R - 1 - stg : stg;
+    const int hb = R - 1 - s;
+    int cur = -1;
+    MulConst M;  // KIND 2: the class split of the current twiddle
+    for (int pq = warp * chunk; pq < (warp + 1) * chunk; pq++) {
+      const int top = ((pq >> hb) << (hb + 1)) | (pq & ((1 << hb) - 1));
+      const int bot = top | (1 << hb);
+      const int k = (1 << s) - 1 + (top >> (hb + 1));
+      const f128 tv = tw[k];
+      f128* ut = tile + ((size_t)top << 6);
+      f128* vt = tile + ((size_t)bot << 6);
+      if (fz(tv)) {  // block 0 of every layer: the twiddle is the empty sum
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int l = lane + 32 * q;
+          if (!TRANSPOSE) vt[l] = fx(vt[l], ut[l]);
+          else ut[l] = fx(ut[l], vt[l]);
+        }
+        continue;
+      }
+      if (k != cur) {
+        __syncwarp();  // every lane has finished with the previous table
+        tab4_build(T, tv, lane);
+        if (KIND == 2) M = mulconst(tv);
+        __syncwarp();
+        cur = k;
+      }
+      f128 u0 = ut[lane], v0 = vt[lane], u1 = ut[lane + 32], v1 = vt[lane + 32];
+      if (!TRANSPOSE) {
+        u0 = fx(u0, tab4_mul(T, v0));
+        if (KIND == 1) u1 = fx(u1, tab4_mul(T, v1));
+        else u1 = fx(u1, fmul_c(v1, M));
+        v0 = fx(v0, u0);
+        v1 = fx(v1, u1);
+      } else {
+        u0 = fx(u0, v0);
+        u1 = fx(u1, v1);
+        v0 = fx(v0, tab4_mul(T, u0));
+        if (KIND == 1) v1 = fx(v1, tab4_mul(T, u1));
+        else v1 = fx(v1, fmul_c(u1, M));
+      }
+      ut[lane] = u0;
+      vt[lane] = v0;
+      ut[lane + 32] = u1;
+      vt[lane + 32] = v1;
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < n_el; e += blockDim.x) {
+    const uint64_t pl = (uint64_t)(e >> 6);
+    const uint64_t pos = (hi << (log_d - l0)) | (pl << lo_bits) | lo;
+    st(p.data + pos * p.lanes + ((size_t)grp << 6) + (e & 63), tile[e]);
+  }
+}
+
+template <bool TRANSPOSE, int KIND>
+__global__ void __launch_bounds__(256, 1) k_ntt_pass_w(PassArgs p) {
+  extern __shared__ f128 smem[];
+  ntt_tile_w<TRANSPOSE, KIND>(p, blockIdx.x, smem);
+}
+
 template <bool TRANSPOSE>
 __global__ void __launch_bounds__(256, 2) k_ntt_pass(PassArgs p) {
   extern __shared__ f128 smem[];
@@ -169,9 +331,15 @@ __global__ void __launch_bounds__(256, 2) k_ntt_pass_batch(const BatchJob* __res
     }
     const BatchJob& J = jobs[lo];
     const NttPass& ps = J.pass[pass];
-    const PassArgs a{J.cw, J.ev, J.log_d, 64, ps.lgs, ps.l0, ps.R};
+    PassArgs a{J.cw, J.ev, J.log_d, 64, ps.lgs, ps.l0, ps.R};
+    if (pass == 0) {  // rate 1/2: the message fills both halves of the codeword
+      a.src = J.z;
+      a.src_mask = ((uint64_t)1 << (J.log_d - 1)) - 1;
+    }
     __syncthreads();  // the previous tile's stores have read the shared tile
-    ntt_tile<false>(a, t - J.tile0[pass], smem);
+    if (ps.kind == 1) ntt_tile_w<false, 1>(a, t - J.tile0[pass], smem);
+    else if (ps.kind == 2) ntt_tile_w<false, 2>(a, t - J.tile0[pass], smem);
+    else ntt_tile<false>(a, t - J.tile0[pass], smem);
   }
 }
 
@@ -245,6 +413,7 @@ const f128* device_evals(int dim) {
 // fastest combination per (device, log_d, lanes, layer_begin).
 
 size_t pass_smem(int lgs, int R) { return ((size_t)(1 << lgs) << R) * sizeof(f128) + ((1 << R) - 1) * sizeof(f128); }
+size_t pass_bytes(const NttPass& p) { return p.kind ? pass_w_smem(p.R, p.threads) : pass_smem(p.lgs, p.R); }
 constexpr size_t kSmem2 = (size_t)112 << 10;  // two CTAs per SM
 constexpr size_t kSmem1 = (size_t)200 << 10;  // one CTA per SM
 
@@ -297,7 +466,22 @@ std::vector<std::vector<std::pair<int, int>>> candidate_splits(int begin, int n_
   return out;
 }
 
-// per-pass launch shapes to try: (lgs, threads)
+// splits for the warp-per-pair passes (at most kMaxRw layers: a 64-lane tile
+// and the warps' tables share the CTA's shared memory)
+constexpr int kMaxRw = 7;
+std::vector<std::vector<std::pair<int, int>>> candidate_splits_w(int begin, int n_layers) {
+  std::vector<std::vector<std::pair<int, int>>> out;
+  const int p0 = (n_layers + kMaxRw - 1) / kMaxRw;
+  for (int np = p0; np <= p0 + 1 && np <= n_layers; np++) {
+    auto v = balanced_split(begin, n_layers, np);
+    bool ok = true;
+    for (auto& pr : v) ok = ok && pr.second >= 4 && pr.second <= kMaxRw;
+    if (ok) out.push_back(v);
+  }
+  return out;
+}
+
+// per-pass launch shapes to try: (lgs, threads) of the thread-per-pair passes
 std::vector<std::pair<int, int>> candidate_shapes(int lanes, int R) {
   std::vector<std::pair<int, int>> out;
   const int top = max_lgs(lanes);
@@ -320,11 +504,43 @@ std::vector<std::pair<int, int>> candidate_shapes(int lanes, int R) {
   return out;
 }
 
+// the warp-per-pair shapes of a pass of R layers: (threads, kind) with the
+// tile and every warp's table within one CTA's shared memory
+std::vector<NttPass> candidate_shapes_w(int lanes, int l0, int R) {
+  std::vector<NttPass> out;
+  if (lanes % 64 || R < 4 || R > kMaxRw) return out;
+  for (int kind : {1, 2})
+    for (int t : {128, 256}) {
+      if (t / 32 > (1 << (R - 1)) || pass_w_smem(R, t) > kSmem1) continue;
+      NttPass p{l0, R, 6, t};
+      p.kind = kind;
+      out.push_back(p);
+    }
+  return out;
+}
+
+template <bool TR>
+void launch_pass_w(const NttPass& ps, const PassArgs& a, uint64_t tiles, cudaStream_t s) {
+  auto k = ps.kind == 1 ? k_ntt_pass_w<TR, 1> : k_ntt_pass_w<TR, 2>;
+  CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem1));
+  count_launch();
+  k<<<(unsigned)tiles, ps.threads, pass_w_smem(ps.R, ps.threads), s>>>(a);
+}
+
 void launch_pass(const NttPass& ps, f128* data, const f128* ev, int log_d, int lanes, bool transpose,
-                 cudaStream_t s) {
+                 cudaStream_t s, const f128* src = nullptr) {
   PassArgs a{data, ev, log_d, lanes, ps.lgs, ps.l0, ps.R};
+  if (src) {
+    a.src = src;
+    a.src_mask = ((uint64_t)1 << (log_d - ps.l0)) - 1;
+  }
   const size_t smem = pass_smem(ps.lgs, ps.R);
   const uint64_t tiles = ((uint64_t)1 << (log_d - ps.R)) * (uint64_t)(lanes >> ps.lgs);
+  if (ps.kind) {
+    if (transpose) launch_pass_w<true>(ps, a, tiles, s);
+    else launch_pass_w<false>(ps, a, tiles, s);
+    return;
+  }
   // The attribute is the same upper bound for every launch: it is global to
   // the kernel, so a per-launch size set by one host thread could undercut
   // another thread's launch of a larger tile.
@@ -368,6 +584,18 @@ std::vector<NttPlan> all_plans(int log_d, int lanes, int layer_begin) {
       out.push_back(plan);
     }
   }
+  for (auto& split : candidate_splits_w(layer_begin, n_layers)) {
+    size_t n_shapes = 0;
+    for (auto& pr : split) n_shapes = std::max(n_shapes, candidate_shapes_w(lanes, pr.first, pr.second).size());
+    for (size_t k = 0; k < n_shapes; k++) {
+      NttPlan plan;
+      for (auto& pr : split) {
+        auto sh = candidate_shapes_w(lanes, pr.first, pr.second);
+        if (!sh.empty()) plan.push_back(sh[std::min(k, sh.size() - 1)]);
+      }
+      if (plan.size() == split.size()) out.push_back(plan);
+    }
+  }
   return out;
 }
 
@@ -391,13 +619,16 @@ NttPlan plan_for(int log_d, int lanes, int layer_begin) {
   return it != tuned_plans().end() ? it->second : default_plan(log_d, lanes, layer_begin);
 }
 
-void run_plan(const NttPlan& plan, f128* data, int log_d, int lanes, bool transpose, cudaStream_t s) {
+// src != nullptr (forward only): the message whose replicate the first pass
+// reads in place of data
+void run_plan(const NttPlan& plan, f128* data, int log_d, int lanes, bool transpose, cudaStream_t s,
+              const f128* src = nullptr) {
   if (plan.empty()) return;
   const f128* ev = device_evals(log_d);
   if (transpose)
     for (auto it = plan.rbegin(); it != plan.rend(); ++it) launch_pass(*it, data, ev, log_d, lanes, true, s);
   else
-    for (auto& ps : plan) launch_pass(ps, data, ev, log_d, lanes, false, s);
+    for (size_t i = 0; i < plan.size(); i++) launch_pass(plan[i], data, ev, log_d, lanes, false, s, i ? nullptr : src);
 }
 
 void run_passes(f128* data, int log_d, int lanes, int layer_begin, bool transpose, cudaStream_t s) {
@@ -409,7 +640,8 @@ void ntt_replicate_batch(const BatchJob* jobs, int n_jobs, uint64_t total, cudaS
   count_launch();
   k_replicate_batch<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(jobs, n_jobs, total);
 }
-size_t ntt_pass_batch_smem(const NttPass& p) { return pass_smem(p.lgs, p.R); }
+// the batched pass kernel runs 256 threads: a warp-per-pair pass holds 8 tables
+size_t ntt_pass_batch_smem(const NttPass& p) { return p.kind ? pass_w_smem(p.R, 256) : pass_smem(p.lgs, p.R); }
 void ntt_pass_batch(const BatchJob* jobs, int n_jobs, int pass, uint64_t total_tiles, size_t smem, int grid,
                     cudaStream_t s) {
   if (smem > kSmem1) throw CudaError("ntt_pass_batch: tile larger than the shared-memory bound");
@@ -456,7 +688,10 @@ NttPlan ntt_autotune(f128* scratch, int log_d, int lanes, int layer_begin, cudaS
   std::map<std::pair<int, int>, std::pair<NttPass, double>> best_pass;  // (l0, R) -> fastest shape
   NttPlan best_plan;
   double best_total = 1e300;
-  for (auto& split : candidate_splits(layer_begin, n_layers)) {
+  auto splits = candidate_splits(layer_begin, n_layers);
+  for (auto& sp : candidate_splits_w(layer_begin, n_layers))
+    if (std::find(splits.begin(), splits.end(), sp) == splits.end()) splits.push_back(sp);
+  for (auto& split : splits) {
     NttPlan plan;
     double total = 0;
     for (auto& pr : split) {
@@ -464,8 +699,11 @@ NttPlan ntt_autotune(f128* scratch, int log_d, int lanes, int layer_begin, cudaS
       if (it == best_pass.end()) {
         NttPass bp{};
         double bt = 1e300;
-        for (auto& sh : candidate_shapes(lanes, pr.second)) {
-          const NttPass ps{pr.first, pr.second, sh.first, sh.second};
+        std::vector<NttPass> shapes;
+        if (pr.second <= kMaxR + 1)
+          for (auto& sh : candidate_shapes(lanes, pr.second)) shapes.push_back({pr.first, pr.second, sh.first, sh.second});
+        for (auto& ps : candidate_shapes_w(lanes, pr.first, pr.second)) shapes.push_back(ps);
+        for (auto& ps : shapes) {
           const double t = time_pass(ps);
           if (t < bt) { bt = t; bp = ps; }
         }
@@ -492,12 +730,16 @@ std::string ntt_plan_desc(const NttPlan& plan) {
   for (auto& ps : plan) {
     if (!d.empty()) d += " + ";
     d += "R" + std::to_string(ps.R) + "@l" + std::to_string(ps.l0) + " x" + std::to_string(1 << ps.lgs) +
-         " lanes/" + std::to_string(ps.threads) + "t";
+         " lanes/" + std::to_string(ps.threads) + "t" + (ps.kind == 1 ? "/tab" : ps.kind == 2 ? "/tab+imad" : "");
   }
   return d;
 }
 
 size_t ntt_plan_count(int log_d, int lanes, int layer_begin) { return all_plans(log_d, lanes, layer_begin).size(); }
+std::string ntt_plan_desc_at(int log_d, int lanes, int layer_begin, size_t index) {
+  const auto plans = all_plans(log_d, lanes, layer_begin);
+  return index < plans.size() ? ntt_plan_desc(plans[index]) : std::string();
+}
 
 void ntt_rs_encode_plan(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, size_t plan_idx,
                         cudaStream_t s) {
@@ -505,14 +747,23 @@ void ntt_rs_encode_plan(const f128* msg, f128* cw, int log_msg_pos, int lanes, i
   auto plans = all_plans(log_d, lanes, log_inv_rate);
   if (plan_idx >= plans.size()) throw std::out_of_range("ntt plan index");
   size_t msg_len = ((size_t)lanes) << log_msg_pos;
-  count_launch(); k_replicate<<<(unsigned)((msg_len + 255) / 256), 256, 0, s>>>(msg, cw, msg_len, 1 << log_inv_rate);
-  run_plan(plans[plan_idx], cw, log_d, lanes, false, s);
+  if (plans[plan_idx].empty() || plans[plan_idx][0].l0 != log_inv_rate) {
+    count_launch(); k_replicate<<<(unsigned)((msg_len + 255) / 256), 256, 0, s>>>(msg, cw, msg_len, 1 << log_inv_rate);
+    run_plan(plans[plan_idx], cw, log_d, lanes, false, s);
+  } else {
+    run_plan(plans[plan_idx], cw, log_d, lanes, false, s, msg);
+  }
 }
 
 void ntt_rs_encode(const f128* msg, f128* cw, int log_msg_pos, int lanes, int log_inv_rate, cudaStream_t s) {
-  size_t msg_len = ((size_t)lanes) << log_msg_pos;
-  count_launch(); k_replicate<<<(unsigned)((msg_len + 255) / 256), 256, 0, s>>>(msg, cw, msg_len, 1 << log_inv_rate);
-  run_passes(cw, log_msg_pos + log_inv_rate, lanes, log_inv_rate, false, s);
+  const int log_d = log_msg_pos + log_inv_rate;
+  const NttPlan plan = plan_for(log_d, lanes, log_inv_rate);
+  if (plan.empty()) {  // no butterfly layer: the codeword is the replicate
+    size_t msg_len = ((size_t)lanes) << log_msg_pos;
+    count_launch(); k_replicate<<<(unsigned)((msg_len + 255) / 256), 256, 0, s>>>(msg, cw, msg_len, 1 << log_inv_rate);
+    return;
+  }
+  run_plan(plan, cw, log_d, lanes, false, s, msg);  // the first pass reads the message's replicate in place
 }
 
 void ntt_forward(f128* data, int log_d, int lanes, int start_layer, cudaStream_t s) {

@@ -41,7 +41,7 @@ size_t Setup::estimate_bytes(uint32_t log2) {
   return n_words * 16 * 10 + n_words * 2 + n_words * 2 + (n_words / 128) * 212 + ((size_t)96 << 20);
 }
 
-Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
+Setup::Setup(int device, uint32_t log2_, int stream_priority) : log2(log2_) {
   CK(cudaSetDevice(device));
   const size_t bytes0 = t_alloc_bytes;
   n_log = std::max<int>(3, (int)log2);
@@ -50,7 +50,7 @@ Setup::Setup(int device, uint32_t log2_) : log2(log2_) {
   if (!lad) throw std::runtime_error("no Ligerito configuration for this size (m = " + std::to_string(m) + ")");
   n_words = (size_t)1 << (m - 7);
   digest = statement_digest(m);
-  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, stream_priority));
   z = dalloc<f128>(n_words);
   a = dalloc<f128>(n_words);
   b = dalloc<f128>(n_words);
@@ -175,7 +175,7 @@ BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vec
   if (n == 0) return h;
   if ((int)seeds.size() != n) throw std::runtime_error("batch_commit: one seed per setup");
   std::vector<BatchJob> J(n);
-  uint64_t wcta = 0, rep = 0, leaves = 0, tiles[3] = {0, 0, 0}, par[24] = {0};
+  uint64_t wcta = 0, rep = 0, leaves = 0, tiles[4] = {0, 0, 0, 0}, par[24] = {0};
   size_t smem = 0;
   int max_pass = 0, max_level = 0;
   for (int i = 0; i < n; i++) {
@@ -196,10 +196,10 @@ BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vec
     b.rep0 = rep;
     rep += b.msg_len;
     const NttPlan plan = ntt_plan(b.log_d, 64, 1);
-    if (plan.size() > 3) throw std::runtime_error("batch_commit: more than three NTT passes");
+    if (plan.size() > 4) throw std::runtime_error("batch_commit: more than four NTT passes");
     b.n_pass = (int)plan.size();
     max_pass = std::max(max_pass, b.n_pass);
-    for (int p = 0; p < 3; p++) {
+    for (int p = 0; p < 4; p++) {
       b.tile0[p] = tiles[p];
       if (p < b.n_pass) {
         b.pass[p] = plan[p];
@@ -240,7 +240,7 @@ BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vec
     uint64_t launches = 0;
     cudaGraphExec_t g = capture(st, &launches, [&] {
       launch_witness_seed_batch(dj, n, (uint32_t)wcta, st);
-      ntt_replicate_batch(dj, n, rep, st);
+      // pass 0 reads each job's message as its replicated codeword
       for (int p = 0; p < max_pass; p++) ntt_pass_batch(dj, n, p, tiles[p], smem, 2 * sms, st);
       merkle_leaves_batch(dj, n, leaves, st);
       for (int l = 1; l <= max_level; l++) merkle_parents_batch(dj, n, l, par[l], st);

@@ -80,7 +80,9 @@ class Setup {
  public:
   static constexpr int kPhases = 9;  // witness, RS encode, Merkle commit, round1, zc rounds, lincheck,
                                      // ring switch, L0 folds, levels
-  Setup(int device, uint32_t log2);
+  // stream_priority: the CUDA priority of the setup's stream (0: default;
+  // lower numbers are served first when streams compete for the SMs)
+  Setup(int device, uint32_t log2, int stream_priority = 0);
   ~Setup();
   Setup(const Setup&) = delete;
   Setup& operator=(const Setup&) = delete;

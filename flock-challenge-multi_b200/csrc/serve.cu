@@ -8,7 +8,31 @@ namespace flock {
 
 Server::Server(int device, uint64_t budget, int slots) : device_(device), budget_(budget) {
   if (slots < 1 || slots > 64) throw std::runtime_error("serving slots must be in 1..64");
-  for (int i = 0; i < slots; i++) workers_.emplace_back([this] { worker(); });
+  for (int i = 0; i < slots; i++) {
+    const bool small_only = slots >= 3 && i == 0;  // the express slot
+    workers_.emplace_back([this, small_only] { worker(small_only); });
+  }
+}
+
+// One proof's device time: about 6 M compressions per second plus a fixed
+// per-proof cost (host round trips, launches) of about 1 ms.
+double Server::expected_ms(uint32_t log2) { return 1.0 + (double)(1u << log2) / 6.0e3; }
+
+size_t Server::pick(bool small_only) const {
+  const auto now = Clock::now();
+  size_t best = queue_.size();
+  double best_score = 0;
+  for (size_t i = 0; i < queue_.size(); i++) {
+    const Job& j = queue_[i];
+    if (small_only && j.log2 > kSmallLog2) continue;
+    const double waited = std::chrono::duration<double, std::milli>(now - j.submitted).count();
+    const double score = expected_ms(j.log2) - waited / kAging;
+    if (best == queue_.size() || score < best_score) {
+      best = i;
+      best_score = score;
+    }
+  }
+  return best;
 }
 
 Server::~Server() {
@@ -165,7 +189,7 @@ uint64_t Server::submit(uint32_t log2, uint64_t seed, const uint32_t* blocks, co
     t = j.ticket = next_ticket_++;
     queue_.push_back(std::move(j));
   }
-  cv_jobs_.notify_one();
+  cv_jobs_.notify_all();  // the express slot takes only small jobs: wake every slot
   return t;
 }
 
@@ -225,7 +249,9 @@ std::unique_ptr<Setup> Server::acquire(uint32_t log2, std::unique_lock<std::mute
       std::unique_ptr<Setup> s;
       std::string err;
       try {
-        s.reset(new Setup(device_, log2));
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        s.reset(new Setup(device_, log2, log2 <= kSmallLog2 ? greatest : least));
       } catch (const std::exception& e) {
         err = e.what();
       }
@@ -251,14 +277,15 @@ void Server::release(std::unique_ptr<Setup> s) {
   cv_mem_.notify_all();
 }
 
-void Server::worker() {
+void Server::worker(bool small_only) {
   cudaSetDevice(device_);
   std::unique_lock<std::mutex> lk(mu_);
   for (;;) {
-    cv_jobs_.wait(lk, [&] { return stop_ || !queue_.empty(); });
+    size_t idx = 0;
+    cv_jobs_.wait(lk, [&] { return stop_ || (idx = pick(small_only)) < queue_.size(); });
     if (stop_) return;
-    Job job = std::move(queue_.front());
-    queue_.pop_front();
+    Job job = std::move(queue_[idx]);
+    queue_.erase(queue_.begin() + (long)idx);
     JobResult r;
     std::unique_ptr<Setup> s;
     try {

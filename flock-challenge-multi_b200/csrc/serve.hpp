@@ -1,9 +1,14 @@
 // Serving scheduler: continuous batching of proof jobs of different sizes on
-// one GPU.  Jobs are admitted in arrival order as proof slots and device
-// memory free up: each slot is a host thread that drives one proof at a time
-// on its own CUDA stream, so the kernels of up to `slots` proofs overlap on
-// the device and fill each other's host round-trip gaps (the Fiat-Shamir
-// transcript stays on the host).  Setups (device buffers + tables for one
+// one GPU.  Jobs are admitted as proof slots and device memory free up: each
+// slot is a host thread that drives one proof at a time on its own CUDA
+// stream, so the kernels of up to `slots` proofs overlap on the device and
+// fill each other's host round-trip gaps (the Fiat-Shamir transcript stays on
+// the host).  The queue is size-aware, so that small jobs do not wait behind
+// 2^19 / 2^20 proofs: a free slot takes the job with the shortest expected
+// proof, aged by its waiting time (a job that has waited kAging times its own
+// expected run time goes ahead of any fresh job); with 3 or more slots one
+// slot takes only small jobs (at most 2^kSmallLog2 compressions), and small
+// jobs' setups run on the highest-priority CUDA stream.  Setups (device buffers + tables for one
 // size) are cached per size and reused; admission keeps the bytes of all
 // cached setups within the HBM budget, evicting idle setups of other sizes
 // (least recently used first) when a new size needs room.
@@ -82,7 +87,12 @@ class Server {
     uint64_t last_use = 0;
   };
 
-  void worker();
+  static constexpr uint32_t kSmallLog2 = 16;
+  static constexpr double kAging = 2.0;
+  static double expected_ms(uint32_t log2);
+  // index of the queued job a free slot takes next (queue_.size() if none)
+  size_t pick(bool small_only) const;
+  void worker(bool small_only);
   void self_check(Setup& s, const std::string& domain, JobResult& r);
   // wait: block until memory frees up (else return nullptr when it does not fit now)
   std::unique_ptr<Setup> acquire(uint32_t log2, std::unique_lock<std::mutex>& lk, bool wait = true);

@@ -34,6 +34,7 @@ EXPORTS = (
     "flock_challenger_observe_label", "flock_challenger_observe_bytes", "flock_challenger_observe_f128",
     "flock_challenger_observe_f128_slice", "flock_challenger_sample_f128", "flock_challenger_sample_f128_vec",
     "flock_challenger_grind_pow", "flock_challenger_verify_pow", "flock_challenger_state_digest",
+    "flock_ntt_plan_desc", "flock_bench_ntt_plan",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -72,6 +73,8 @@ def load() -> ctypes.CDLL:
         lib.flock_ctx_destroy.argtypes = [vp]
         lib.flock_setup_create.argtypes = [vp, u32, i32, i32, ctypes.POINTER(vp)]
         lib.flock_setup_destroy.argtypes = [vp]
+        lib.flock_ntt_plan_desc.argtypes = [u32, u32, u32, u32, ctypes.c_char_p, sz]
+        lib.flock_bench_ntt_plan.argtypes = [vp, u32, u32, u32, u32, i32, ctypes.POINTER(ctypes.c_double)]
         lib.flock_pcs_commit.argtypes = [vp, vp, u32, vp, ctypes.POINTER(vp)]
         lib.flock_prover_data_open.argtypes = [vp, vp, sz, vp, vp, sz, ctypes.POINTER(sz)]
         lib.flock_prover_data_destroy.argtypes = [vp]
@@ -136,6 +139,15 @@ def to_records(blocks: np.ndarray, block_len: int = 64, flags: int = 11) -> np.n
     rec[:, 26] = block_len
     rec[:, 27] = flags
     return rec
+
+
+def ntt_plan_descs(log_msg_pos: int, lanes: int, log_inv_rate: int) -> list:
+    """Descriptions of every candidate pass plan of an RS-encode shape."""
+    lib = load()
+    out, buf = [], ctypes.create_string_buffer(512)
+    while lib.flock_ntt_plan_desc(log_msg_pos, lanes, log_inv_rate, len(out), buf, len(buf)) == 0:
+        out.append(buf.value.decode())
+    return out
 
 
 def generate_compressions(log2: int, seed: int) -> np.ndarray:
@@ -368,6 +380,12 @@ class Context:
     def bench_ntt(self, log_msg_pos: int, lanes: int, rate: int, iters: int = 5) -> float:
         ms = ctypes.c_double()
         self._check(self.lib.flock_bench_ntt(self.h, log_msg_pos, lanes, rate, iters, ctypes.byref(ms)), "bench_ntt")
+        return ms.value
+
+    def bench_ntt_plan(self, log_msg_pos: int, lanes: int, rate: int, plan: int, iters: int = 5) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.flock_bench_ntt_plan(self.h, log_msg_pos, lanes, rate, plan, iters, ctypes.byref(ms)),
+                    "bench_ntt_plan")
         return ms.value
 
     def bench_merkle(self, n_leaves: int, leaf_size: int, iters: int = 5) -> float:

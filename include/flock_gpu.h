@@ -221,6 +221,12 @@ int flock_ntt_autotune(flock_ctx* ctx, uint32_t log_msg_pos, uint32_t lanes, uin
                        char* desc, size_t desc_cap);
 int flock_ntt_rs_encode_plan(flock_ctx* ctx, const uint64_t* msg, uint32_t log_msg_pos, uint32_t lanes,
                              uint32_t log_inv_rate, uint32_t plan_index, uint64_t* out);
+/* The description of candidate plan plan_index (host only; FLOCK_ERR_ARG past
+ * the last one), and its device time on seeded resident inputs. */
+int flock_ntt_plan_desc(uint32_t log_msg_pos, uint32_t lanes, uint32_t log_inv_rate, uint32_t plan_index, char* desc,
+                        size_t desc_cap);
+int flock_bench_ntt_plan(flock_ctx* ctx, uint32_t log_msg_pos, uint32_t lanes, uint32_t log_inv_rate,
+                         uint32_t plan_index, int iters, double* ms);
 
 int flock_sumcheck_round(flock_ctx* ctx, const uint64_t* f, const uint64_t* b, size_t n, uint64_t* msg_out);
 /* Degree-3 (zerocheck-style) round over plain F128 vectors: msg_out =

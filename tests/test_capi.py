@@ -37,3 +37,15 @@ def test_no_cpu_fallback_without_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(flockgpu.FlockError):
         flockgpu.Context(0)
+
+
+def test_ntt_plans_cover_every_pass_kind():
+    """The candidate plans of a 64-lane shape include the warp-per-pair table
+    passes (and their mix with integer products) beside the thread-per-pair
+    passes, so the parity test of every plan covers all three kernels."""
+    import flockgpu
+    descs = flockgpu.ntt_plan_descs(13, 64, 1)
+    assert any("/tab+imad" in d for d in descs)
+    assert any("/tab" in d and "/tab+imad" not in d for d in descs)
+    assert any("/tab" not in d for d in descs)
+    assert not any("/tab" in d for d in flockgpu.ntt_plan_descs(16, 1, 2))  # one lane: no warp tiles

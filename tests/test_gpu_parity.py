@@ -49,7 +49,8 @@ def test_ntt_rs_encode(gpu_ctx, oracle, lanes, log_pos, rate):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("lanes,log_pos,rate", [(64, 10, 1), (1, 16, 2), (8, 13, 3), (256, 6, 1), (4, 19, 1)])
+@pytest.mark.parametrize("lanes,log_pos,rate", [(64, 10, 1), (1, 16, 2), (8, 13, 3), (256, 6, 1), (4, 19, 1),
+                                                 (64, 13, 1), (128, 9, 2)])
 def test_ntt_every_plan(gpu_ctx, oracle, lanes, log_pos, rate):
     """Every pass plan the autotuner may pick gives the oracle's codeword."""
     msg = rng_u64(lanes * 7 + log_pos, 2 * (lanes << log_pos))
@@ -207,6 +208,24 @@ def test_golden_full_size(gpu_ctx, log2):
     and 2^18 compressions that the reference's trusted verifier accepted."""
     import flockgpu
     rows = [r for r in json.loads((GOLD / "verified_proofs_large.json").read_text()) if r["log2"] == log2]
+    assert rows
+    p = flockgpu.Prover(gpu_ctx, log2)
+    try:
+        for r in rows:
+            proof = p.prove_seed(r["seed"])
+            assert len(proof) == r["size"] and hashlib.sha256(proof).hexdigest() == r["sha256"]
+    finally:
+        p.close()
+
+
+@pytest.mark.parametrize("log2", [12, 19, 20])
+def test_golden_gpu_proofs_trusted_harness(gpu_ctx, log2):
+    """GPU proofs at sizes the oracle is too slow for (2^19, 2^20) and at
+    2^12, made by flock_worker under the reference's trusted harness, which
+    drew each seed and verified every proof (make_golden.py --gpu-harness):
+    the prover reproduces them bit for bit."""
+    import flockgpu
+    rows = [r for r in json.loads((GOLD / "gpu_verified_proofs.json").read_text()) if r["log2"] == log2]
     assert rows
     p = flockgpu.Prover(gpu_ctx, log2)
     try:
