@@ -409,6 +409,10 @@ def kernel_report(device: int) -> list:
     ipk = int_product_peak()
     rows = []
     try:
+        for variant, name in ((0, "integer (bit classes + Karatsuba)"), (1, "4-bit window table"), (2, "half each")):
+            rate = ctx.bench_f128_product(variant)
+            rows.append({"kernel": "f128_product_by_warp_constant", "variant": name, "products_per_s": rate,
+                         "int_frac": rate / ipk})
         for log_msg, cols in [(16, 1), (16, 64), (16, 256), (20, 1), (20, 16), (20, 64), (24, 1), (24, 4)]:
             for rate in (1, 2):
                 if log_msg + cols.bit_length() - 1 + rate > 27:
@@ -607,6 +611,9 @@ def main():
     ap.add_argument("--ntt-case", default=None, metavar="LOG_MSG,LANES,RATE,PLAN",
                     help="one RS encode with candidate pass plan PLAN (no autotuning launches): the case that "
                          "the NTT's ncu captures profile")
+    ap.add_argument("--proof-once", type=int, default=None, metavar="LOG2",
+                    help="setup + one warm-up proof, print the library's kernel launches so far, then one more "
+                         "proof: the case a profiler's launch list covers (skip the printed count)")
     ap.add_argument("--kernels", action="store_true",
                     help="only the kernel microbenchmarks (NTT / Merkle / sumcheck sweeps), one JSON line each")
     ap.add_argument("--slots", type=int, default=SERVE_SLOTS, help="serving: proofs in flight")
@@ -626,6 +633,16 @@ def main():
         if out is None:
             raise SystemExit(f"no candidate plan {plan} for this shape")
         print(json.dumps({"ntt_case": args.ntt_case, "codeword_values": int(out.size // 2)}))
+        return
+    if args.proof_once is not None:
+        import flockgpu
+        ctx = flockgpu.Context(0)
+        prover = flockgpu.Prover(ctx, args.proof_once)
+        prover.prove_seed(1)
+        print(json.dumps({"launches_before_proof": int(flockgpu.load().flock_launch_count())}), flush=True)
+        prover.prove_seed(2)
+        prover.close()
+        ctx.close()
         return
     if args.kernels:
         if rank == 0:

@@ -74,6 +74,32 @@ __global__ void k_fill(uint64_t* p, size_t n, uint64_t seed) {
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   p[i] = z ^ (z >> 31);
 }
+// GF(2^128) product rate: every thread multiplies four running values by its
+// warp's constant `iters` times.  V = 0: the integer product (bit classes +
+// Karatsuba, the constant's classes split once); 1: the 4-bit window table of
+// the constant in shared memory; 2: two values each way.
+template <int V>
+__global__ void __launch_bounds__(256) k_bench_product(const f128* tw, f128* out, int iters) {
+  extern __shared__ __align__(16) uint8_t bsm[];
+  Tab4* tabs = reinterpret_cast<Tab4*>(bsm);
+  const int warp = threadIdx.x >> 5;
+  const f128 t = tw[(blockIdx.x * 8 + warp) & 1023];
+  const MulConst M = mulconst(t);
+  if (V) {
+    tab4_build(&tabs[warp], t, threadIdx.x & 31);
+    __syncwarp();
+  }
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  f128 x[4] = {mk(g * 0x9E3779B97F4A7C15ull, ~g), mk(g ^ 0x1234, g * 7), mk(g + 99, g * 13), mk(g * 31, g ^ 0xFFFF)};
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const bool table = V == 1 || (V == 2 && k >= 2);
+      x[k] = fx(table ? tab4_mul(&tabs[warp], x[k]) : fmul_c(x[k], M), mk(1, 0));
+    }
+  }
+  st(out + g, fx(fx(x[0], x[1]), fx(x[2], x[3])));
+}
 __global__ void k_mul(const f128* a, const f128* b, size_t n, f128* out) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) st(out + i, fmul(ld(a + i), ld(b + i)));
@@ -771,6 +797,29 @@ int flock_bench_ntt_plan(flock_ctx* c, uint32_t log_msg_pos, uint32_t lanes, uin
     *ms = time_launches(c->st, iters, [&] {
       ntt_rs_encode_plan(dm.p, dc.p, (int)log_msg_pos, (int)lanes, (int)rate, plan_index, c->st);
     });
+    return FLOCK_OK;
+  });
+}
+
+uint64_t flock_launch_count(void) { return kernel_launch_counter().load(); }
+
+int flock_bench_f128_product(flock_ctx* c, int variant, int iters, double* products_per_s) {
+  if (!c || !products_per_s || variant < 0 || variant > 2 || iters < 1) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const unsigned blocks = (unsigned)sms * 8;
+    const size_t smem = 8 * kTab4Bytes;
+    DevBuf<f128> tw(1024), out((size_t)blocks * 256);
+    k_fill<<<8, 256, 0, c->st>>>((uint64_t*)tw.p, 2048, 3);
+    auto kern = variant == 0 ? k_bench_product<0> : variant == 1 ? k_bench_product<1> : k_bench_product<2>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const double ms = time_launches(c->st, 3, [&] {
+      count_launch();
+      kern<<<blocks, 256, smem, c->st>>>(tw.p, out.p, iters);
+    });
+    *products_per_s = (double)blocks * 256 * 4 * iters / (ms * 1e-3);
     return FLOCK_OK;
   });
 }

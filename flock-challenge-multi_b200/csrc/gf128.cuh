@@ -147,6 +147,58 @@ __device__ __forceinline__ f128 multab_mul(const MulTab8* T, f128 y) {
   return acc;
 }
 
+// ---- multiplication by a warp-uniform constant through a 4-bit window table ----
+// Entry n of window w is t * n(x) * x^(4w); a product t * y is the XOR of 32
+// lookups, one per nibble of y.  The halves of an entry sit in separate
+// 8-byte arrays and window w's entries are permuted by n -> n ^ (w mod 16):
+// a window's 16 entries of one half fill the 32 banks exactly once, so a
+// warp's lookups into one window never conflict, whatever the nibbles, and
+// the builder's stores (thread w writes window w) do not conflict either.
+// 8 KiB per table; 32 lookups of 8 bytes per product on the shared-memory
+// pipe and no integer multiplies.
+struct Tab4 {
+  uint64_t lo[32][16], hi[32][16];
+};
+constexpr size_t kTab4Bytes = sizeof(Tab4);  // 8 KiB
+
+__device__ __forceinline__ f128 mul_x128(f128 a, int k) {  // a * x^k, 0 <= k < 128
+  if (k >= 64) {
+    a = reduce256(0, a.lo, a.hi, 0);
+    k -= 64;
+  }
+  return mul_xk(a, k);
+}
+// thread `lane` of the warp writes window `lane`
+__device__ __forceinline__ void tab4_build(Tab4* T, f128 t, int lane) {
+  const f128 b0 = mul_x128(t, 4 * lane), b1 = mul_xk(b0, 1), b2 = mul_xk(b0, 2), b3 = mul_xk(b0, 3);
+  f128 e[16];
+  e[0] = mk(0, 0);
+  e[1] = b0;
+  e[2] = b1;
+  e[3] = fx(b0, b1);
+#pragma unroll
+  for (int j = 4; j < 8; j++) e[j] = fx(e[j - 4], b2);
+#pragma unroll
+  for (int j = 8; j < 16; j++) e[j] = fx(e[j - 8], b3);
+  const int r = lane & 15;
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    T->lo[lane][j ^ r] = e[j].lo;
+    T->hi[lane][j ^ r] = e[j].hi;
+  }
+}
+__device__ __forceinline__ f128 tab4_mul(const Tab4* T, f128 y) {
+  uint64_t alo = 0, ahi = 0;
+#pragma unroll
+  for (int w = 0; w < 32; w++) {
+    const uint64_t word = w < 16 ? y.lo : y.hi;
+    const uint32_t n = ((uint32_t)(word >> (4 * (w & 15))) & 15u) ^ (uint32_t)(w & 15);
+    alo ^= T->lo[w][n];
+    ahi ^= T->hi[w][n];
+  }
+  return mk(alo, ahi);
+}
+
 // ---- products by a factor reused across many products ----
 // The factor's side of the Karatsuba tree (its nine 32-bit operands) is
 // split into the four bit classes once; each product then masks only its

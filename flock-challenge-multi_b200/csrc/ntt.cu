@@ -171,49 +171,6 @@ __device__ __forceinline__ void ntt_tile(const PassArgs& p, uint64_t t_id, f128*
 // table lookups load the shared-memory pipe instead of the integer
 // multipliers; KIND 2 sends lane t + 32 through the integer product, so both
 // pipes work.
-struct Tab4 {
-  uint64_t lo[32][16], hi[32][16];
-};
-constexpr size_t kTab4Bytes = sizeof(Tab4);  // 8 KiB
-
-__device__ __forceinline__ f128 mul_x128(f128 a, int k) {  // a * x^k, 0 <= k < 128
-  if (k >= 64) {
-    a = reduce256(0, a.lo, a.hi, 0);
-    k -= 64;
-  }
-  return mul_xk(a, k);
-}
-// thread `lane` of the warp writes window `lane`
-__device__ __forceinline__ void tab4_build(Tab4* T, f128 t, int lane) {
-  const f128 b0 = mul_x128(t, 4 * lane), b1 = mul_xk(b0, 1), b2 = mul_xk(b0, 2), b3 = mul_xk(b0, 3);
-  f128 e[16];
-  e[0] = mk(0, 0);
-  e[1] = b0;
-  e[2] = b1;
-  e[3] = fx(b0, b1);
-#pragma unroll
-  for (int j = 4; j < 8; j++) e[j] = fx(e[j - 4], b2);
-#pragma unroll
-  for (int j = 8; j < 16; j++) e[j] = fx(e[j - 8], b3);
-  const int r = lane & 15;
-#pragma unroll
-  for (int j = 0; j < 16; j++) {
-    T->lo[lane][j ^ r] = e[j].lo;
-    T->hi[lane][j ^ r] = e[j].hi;
-  }
-}
-__device__ __forceinline__ f128 tab4_mul(const Tab4* T, f128 y) {
-  uint64_t alo = 0, ahi = 0;
-#pragma unroll
-  for (int w = 0; w < 32; w++) {
-    const uint64_t word = w < 16 ? y.lo : y.hi;
-    const uint32_t n = ((uint32_t)(word >> (4 * (w & 15))) & 15u) ^ (uint32_t)(w & 15);
-    alo ^= T->lo[w][n];
-    ahi ^= T->hi[w][n];
-  }
-  return mk(alo, ahi);
-}
-
 size_t pass_w_smem(int R, int threads) {
   return ((size_t)64 << R) * sizeof(f128) + ((size_t)1 << R) * sizeof(f128) + (size_t)(threads / 32) * kTab4Bytes;
 }

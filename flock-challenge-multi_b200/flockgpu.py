@@ -34,7 +34,7 @@ EXPORTS = (
     "flock_challenger_observe_label", "flock_challenger_observe_bytes", "flock_challenger_observe_f128",
     "flock_challenger_observe_f128_slice", "flock_challenger_sample_f128", "flock_challenger_sample_f128_vec",
     "flock_challenger_grind_pow", "flock_challenger_verify_pow", "flock_challenger_state_digest",
-    "flock_ntt_plan_desc", "flock_bench_ntt_plan",
+    "flock_ntt_plan_desc", "flock_bench_ntt_plan", "flock_bench_f128_product", "flock_launch_count",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -73,6 +73,9 @@ def load() -> ctypes.CDLL:
         lib.flock_ctx_destroy.argtypes = [vp]
         lib.flock_setup_create.argtypes = [vp, u32, i32, i32, ctypes.POINTER(vp)]
         lib.flock_setup_destroy.argtypes = [vp]
+        lib.flock_launch_count.restype = u64
+        lib.flock_launch_count.argtypes = []
+        lib.flock_bench_f128_product.argtypes = [vp, i32, i32, ctypes.POINTER(ctypes.c_double)]
         lib.flock_ntt_plan_desc.argtypes = [u32, u32, u32, u32, ctypes.c_char_p, sz]
         lib.flock_bench_ntt_plan.argtypes = [vp, u32, u32, u32, u32, i32, ctypes.POINTER(ctypes.c_double)]
         lib.flock_pcs_commit.argtypes = [vp, vp, u32, vp, ctypes.POINTER(vp)]
@@ -387,6 +390,12 @@ class Context:
         self._check(self.lib.flock_bench_ntt_plan(self.h, log_msg_pos, lanes, rate, plan, iters, ctypes.byref(ms)),
                     "bench_ntt_plan")
         return ms.value
+
+    def bench_f128_product(self, variant: int, iters: int = 400) -> float:
+        """GF(2^128) products/s by a warp-uniform constant: 0 integer, 1 table, 2 mixed."""
+        r = ctypes.c_double()
+        self._check(self.lib.flock_bench_f128_product(self.h, variant, iters, ctypes.byref(r)), "bench_f128_product")
+        return r.value
 
     def bench_merkle(self, n_leaves: int, leaf_size: int, iters: int = 5) -> float:
         ms = ctypes.c_double()

@@ -250,6 +250,14 @@ int flock_statement_digest(uint32_t m, uint8_t* out32);
 int flock_bench_ntt(flock_ctx* ctx, uint32_t log_msg_pos, uint32_t lanes, uint32_t log_inv_rate, int iters,
                     double* ms);
 int flock_bench_merkle(flock_ctx* ctx, size_t n_leaves, size_t leaf_size, int iters, double* ms);
+/* GF(2^128) products per second by a warp-uniform constant on all SMs (a
+ * register loop, `iters` x 4 products per thread): variant 0 the integer
+ * product (bit classes + Karatsuba), 1 the 4-bit window table in shared
+ * memory, 2 half of the products each way. */
+int flock_bench_f128_product(flock_ctx* ctx, int variant, int iters, double* products_per_s);
+/* Number of this library's kernel launches issued by the process so far
+ * (lets a profiler skip a setup's autotuning launches). */
+uint64_t flock_launch_count(void);
 int flock_bench_sumcheck(flock_ctx* ctx, size_t n, int iters, double* ms);
 /* fused fold + degree-3 message of flock_sumcheck_round3 over n values */
 int flock_bench_sumcheck3(flock_ctx* ctx, size_t n, int iters, double* ms);
