@@ -67,7 +67,8 @@ def algorithmic_bytes(phase: str, log2: int) -> int:
 
 # phase -> (the phase's kernels, launches per proof, what the algorithmic bytes count)
 PHASE_KERNEL = {
-    "rs_encode": ("k_replicate + k_ntt_pass", 3, "read the message (2^25 F128), write the codeword (2^26 F128)"),
+    "rs_encode": ("k_ntt_pass_w (4-bit table passes; the first reads the message)", 0,
+                  "read the message (2^25 F128), write the codeword (2^26 F128)"),
     "merkle_commit": ("k_merkle_leaves/parents/top", 22, "read the 1 GiB codeword, write 32 B per leaf"),
     "zerocheck_round1": ("k_zc_round1_ab + k_zc_round1_c", 2, "read packed a, b, c (3 x 512 MiB)"),
     "zerocheck_rounds": ("k_zc_round", 26, "packed a, b once, then 3 x 16 B per value per halving round"),
@@ -81,10 +82,6 @@ PHASE_KERNEL = {
 # GF(2^128) products per proof of the RS encode: 64 lanes x 2^19 pairs x 19
 # butterfly layers at m = 32 (layer 0 is a copy)
 NTT_PRODUCTS_2P18 = 64 * (1 << 19) * 19
-# register-only loop of the same product on this GPU (all 148 SMs)
-PRODUCT_REGISTER_ONLY = 3.8e10
-
-
 def peaks():
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
@@ -390,12 +387,34 @@ def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: i
 # cheaper product raises it): 144 IMAD.WIDE (9 Karatsuba 32x32 carry-less
 # products of 16 each) at 32 per SM per clock, the FMA pipe's rate.  148 SMs
 # at the measured maximum SM clock.
-def int_product_peak() -> float:
+def sm_mhz() -> float:
     mhz = 1965.0
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
         mhz = float(json.loads(p.read_text()).get("sm_max_mhz", mhz))
-    return 148 * mhz * 1e6 * 32 / 144
+    return mhz
+
+
+def int_product_peak() -> float:
+    return 148 * sm_mhz() * 1e6 * 32 / 144
+
+
+# Ceiling of the 4-bit window table product: 64 eight-byte lookups (512 B) per
+# product on the shared-memory pipe, 128 B per SM per clock.
+def table_product_peak() -> float:
+    return 148 * sm_mhz() * 1e6 * 128 / 512
+
+
+def product_ceiling(plan_desc: str) -> tuple:
+    """(ceiling, definition) of the GF(2^128) product as the tuned plan's
+    passes compute it: integer multiplies, table lookups, or both pipes at
+    once (the mixed passes send half of the lanes each way)."""
+    if "/tab+imad" in plan_desc:
+        return 2 * min(int_product_peak(), table_product_peak()), "mixed: both pipes, half of the products each"
+    if "/tab" in plan_desc:
+        return table_product_peak(), "4-bit window tables: 148 SMs x max SM clock x 128 B / 512 B per product"
+    return int_product_peak(), ("integer products: 148 SMs x max SM clock x 32 IMAD.WIDE per SM per clock / "
+                                "144 IMAD.WIDE per product")
 
 
 def kernel_report(device: int) -> list:
@@ -409,7 +428,8 @@ def kernel_report(device: int) -> list:
     ipk = int_product_peak()
     rows = []
     try:
-        for variant, name in ((0, "integer (bit classes + Karatsuba)"), (1, "4-bit window table"), (2, "half each")):
+        for variant, name in ((0, "integer (bit classes + Karatsuba)"), (1, "4-bit window table"), (2, "half each"),
+                              (3, "8-bit window table, one per CTA")):
             rate = ctx.bench_f128_product(variant)
             rows.append({"kernel": "f128_product_by_warp_constant", "variant": name, "products_per_s": rate,
                          "int_frac": rate / ipk})
@@ -512,6 +532,7 @@ def run_ours(args, world, rank, local):
     log2 = args.log2
     ctx = flockgpu.Context(local)
     prover = flockgpu.Prover(ctx, log2)
+    _, plan_desc = ctx.ntt_autotune(log2 + 1, 64, 1)  # the commitment's tuned plan (tuned by the setup)
     seed_base = rank_seed_base(rank)
     for i in range(args.warmup):
         prover.prove_seed(seed_base + 900 + i)
@@ -543,6 +564,10 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = peaks()
     dom = max(phases, key=phases.get)
     kname, klaunches, kdesc = PHASE_KERNEL[dom]
+    if dom == "rs_encode":  # one launch per pass of the tuned plan
+        klaunches = plan_desc.count(" + ") + 1
+        if "/tab" not in plan_desc:
+            kname = "k_ntt_pass (integer products; the first pass reads the message)"
     kbytes = algorithmic_bytes(dom, log2)
     # the phase's events bracket only its own launches on the prover stream:
     # algorithmic bytes of the phase over the phase's device time
@@ -578,14 +603,12 @@ def run_ours(args, world, rank, local):
     if dom == "rs_encode":
         prods = NTT_PRODUCTS_2P18 * (1 << log2) / (1 << 18)
         rate = prods / (phases[dom] / 1e3)
-        ceil = int_product_peak()
+        ceil, cdef = product_ceiling(plan_desc)
         line["roofline"]["int_pipe"] = {
-            "products": prods, "achieved_products_per_s": rate,
+            "plan": plan_desc, "products": prods, "achieved_products_per_s": rate,
             "ceiling_as_built_products_per_s": ceil, "utilisation_as_built": rate / ceil,
-            "register_only_products_per_s": PRODUCT_REGISTER_ONLY,
             "floor_ms_at_ceiling": prods / ceil * 1e3,
-            "ceiling_def": "the product as built: 148 SMs x max SM clock x 32 IMAD.WIDE per SM per clock / "
-                           "144 IMAD.WIDE per product; a cheaper product raises it"}
+            "ceiling_def": cdef + " (the product as built, not an algorithmic bound)"}
     if world == 1 and not args.no_chain:
         line.update(chain_report(prover, log2))
         line.update(verify_report(prover, log2))
@@ -611,6 +634,9 @@ def main():
     ap.add_argument("--ntt-case", default=None, metavar="LOG_MSG,LANES,RATE,PLAN",
                     help="one RS encode with candidate pass plan PLAN (no autotuning launches): the case that "
                          "the NTT's ncu captures profile")
+    ap.add_argument("--ntt-plans", default=None, metavar="LOG_MSG,LANES,RATE",
+                    help="time every candidate pass plan of one RS-encode shape (device-resident seeded inputs), "
+                         "then the autotuner's pick; one JSON line")
     ap.add_argument("--proof-once", type=int, default=None, metavar="LOG2",
                     help="setup + one warm-up proof, print the library's kernel launches so far, then one more "
                          "proof: the case a profiler's launch list covers (skip the printed count)")
@@ -633,6 +659,23 @@ def main():
         if out is None:
             raise SystemExit(f"no candidate plan {plan} for this shape")
         print(json.dumps({"ntt_case": args.ntt_case, "codeword_values": int(out.size // 2)}))
+        return
+    if args.ntt_plans:
+        import flockgpu
+        lm, lanes, rate = (int(x) for x in args.ntt_plans.split(","))
+        ctx = flockgpu.Context(0)
+        plans = sorted((ctx.bench_ntt_plan(lm, lanes, rate, i, iters=5), i, d)
+                       for i, d in enumerate(flockgpu.ntt_plan_descs(lm, lanes, rate)))
+        t0 = time.perf_counter()
+        _, pick = ctx.ntt_autotune(lm, lanes, rate)
+        tune_s = time.perf_counter() - t0
+        ms = ctx.bench_ntt(lm, lanes, rate, iters=5)
+        prods = lanes * (1 << (lm + rate - 1)) * lm
+        print(json.dumps({"log_msg": lm, "lanes": lanes, "rate": rate,
+                          "plans": [{"ms": p[0], "index": p[1], "desc": p[2]} for p in plans],
+                          "autotune": {"pick": pick, "tune_s": tune_s, "encode_ms": ms,
+                                       "products_per_s": prods / (ms / 1e3)}}), flush=True)
+        ctx.close()
         return
     if args.proof_once is not None:
         import flockgpu

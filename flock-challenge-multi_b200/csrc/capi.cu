@@ -77,25 +77,28 @@ __global__ void k_fill(uint64_t* p, size_t n, uint64_t seed) {
 // GF(2^128) product rate: every thread multiplies four running values by its
 // warp's constant `iters` times.  V = 0: the integer product (bit classes +
 // Karatsuba, the constant's classes split once); 1: the 4-bit window table of
-// the constant in shared memory; 2: two values each way.
+// the constant in shared memory; 2: two values each way; 3: the CTA-wide
+// 8-bit window table (MulTab8) of one constant per CTA.
 template <int V>
 __global__ void __launch_bounds__(256) k_bench_product(const f128* tw, f128* out, int iters) {
   extern __shared__ __align__(16) uint8_t bsm[];
   Tab4* tabs = reinterpret_cast<Tab4*>(bsm);
+  MulTab8* t8 = reinterpret_cast<MulTab8*>(bsm);
   const int warp = threadIdx.x >> 5;
-  const f128 t = tw[(blockIdx.x * 8 + warp) & 1023];
+  const f128 t = tw[(blockIdx.x * 8 + (V == 3 ? 0 : warp)) & 1023];
   const MulConst M = mulconst(t);
-  if (V) {
+  if (V == 1 || V == 2) {
     tab4_build(&tabs[warp], t, threadIdx.x & 31);
     __syncwarp();
   }
+  if (V == 3) multab_build(t8, t);
   const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   f128 x[4] = {mk(g * 0x9E3779B97F4A7C15ull, ~g), mk(g ^ 0x1234, g * 7), mk(g + 99, g * 13), mk(g * 31, g ^ 0xFFFF)};
   for (int i = 0; i < iters; i++) {
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       const bool table = V == 1 || (V == 2 && k >= 2);
-      x[k] = fx(table ? tab4_mul(&tabs[warp], x[k]) : fmul_c(x[k], M), mk(1, 0));
+      x[k] = fx(V == 3 ? multab_mul(t8, x[k]) : table ? tab4_mul(&tabs[warp], x[k]) : fmul_c(x[k], M), mk(1, 0));
     }
   }
   st(out + g, fx(fx(x[0], x[1]), fx(x[2], x[3])));
@@ -804,16 +807,19 @@ int flock_bench_ntt_plan(flock_ctx* c, uint32_t log_msg_pos, uint32_t lanes, uin
 uint64_t flock_launch_count(void) { return kernel_launch_counter().load(); }
 
 int flock_bench_f128_product(flock_ctx* c, int variant, int iters, double* products_per_s) {
-  if (!c || !products_per_s || variant < 0 || variant > 2 || iters < 1) return FLOCK_ERR_ARG;
+  if (!c || !products_per_s || variant < 0 || variant > 3 || iters < 1) return FLOCK_ERR_ARG;
   return guard(c, [&] {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const unsigned blocks = (unsigned)sms * 8;
-    const size_t smem = 8 * kTab4Bytes;
+    const size_t smem = variant == 3 ? sizeof(MulTab8) : 8 * kTab4Bytes;
     DevBuf<f128> tw(1024), out((size_t)blocks * 256);
     k_fill<<<8, 256, 0, c->st>>>((uint64_t*)tw.p, 2048, 3);
-    auto kern = variant == 0 ? k_bench_product<0> : variant == 1 ? k_bench_product<1> : k_bench_product<2>;
+    auto kern = variant == 0   ? k_bench_product<0>
+                : variant == 1 ? k_bench_product<1>
+                : variant == 2 ? k_bench_product<2>
+                               : k_bench_product<3>;
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const double ms = time_launches(c->st, 3, [&] {
       count_launch();

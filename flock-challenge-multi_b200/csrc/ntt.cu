@@ -323,6 +323,18 @@ __global__ void k_replicate(const f128* __restrict__ msg, f128* __restrict__ cw,
   for (int c = 0; c < copies; c++) st(cw + (size_t)c * msg_len + i, v);
 }
 
+// SplitMix64 words: the tuner's scratch holds random values, so that the table
+// passes' lookups meet the nibble patterns of real data (all-zero data would
+// turn every lookup into a broadcast and time those passes too fast)
+__global__ void k_fill_random(uint64_t* p, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t z = (i + 1) * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  p[i] = z ^ (z >> 31);
+}
+
 __global__ void k_fold_copies(const f128* __restrict__ in, f128* __restrict__ out, size_t len, int copies) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= len) return;
@@ -467,7 +479,7 @@ std::vector<NttPass> candidate_shapes_w(int lanes, int l0, int R) {
   std::vector<NttPass> out;
   if (lanes % 64 || R < 4 || R > kMaxRw) return out;
   for (int kind : {1, 2})
-    for (int t : {128, 256}) {
+    for (int t : {64, 128, 256}) {
       if (t / 32 > (1 << (R - 1)) || pass_w_smem(R, t) > kSmem1) continue;
       NttPass p{l0, R, 6, t};
       p.kind = kind;
@@ -623,11 +635,17 @@ NttPlan ntt_autotune(f128* scratch, int log_d, int lanes, int layer_begin, cudaS
   const int n_layers = log_d - layer_begin;
   if (n_layers <= 0) return {};
   const f128* ev = device_evals(log_d);
+  {
+    const size_t words = ((size_t)lanes << log_d) * 2;
+    count_launch();
+    k_fill_random<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(reinterpret_cast<uint64_t*>(scratch), words);
+    CK(cudaGetLastError());
+  }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   // one warm launch, then the best of two timed launches (CUDA events on
-  // the launching stream); the scratch contents do not affect the timing
+  // the launching stream), on the random scratch filled above
   auto time_pass = [&](const NttPass& ps) {
     launch_pass(ps, scratch, ev, log_d, lanes, false, s);
     float best = 1e30f;

@@ -253,7 +253,8 @@ int flock_bench_merkle(flock_ctx* ctx, size_t n_leaves, size_t leaf_size, int it
 /* GF(2^128) products per second by a warp-uniform constant on all SMs (a
  * register loop, `iters` x 4 products per thread): variant 0 the integer
  * product (bit classes + Karatsuba), 1 the 4-bit window table in shared
- * memory, 2 half of the products each way. */
+ * memory, 2 half of the products each way, 3 a CTA-wide 8-bit window table
+ * (64 KiB, 16 lookups of 16 bytes per product). */
 int flock_bench_f128_product(flock_ctx* ctx, int variant, int iters, double* products_per_s);
 /* Number of this library's kernel launches issued by the process so far
  * (lets a profiler skip a setup's autotuning launches). */
