@@ -341,7 +341,14 @@ int flock_challenger_sample_f128_vec(flock_challenger* ch, size_t n, uint64_t* o
   return FLOCK_OK;
 }
 int flock_challenger_grind_pow(flock_challenger* ch, flock_ctx* c, uint32_t bits, uint64_t* nonce) {
-  if (!ch || !c || !nonce || bits > 40) return FLOCK_ERR_ARG;
+  if (!ch || !nonce || bits > 40 || (!c && bits > flock::kHostPowBits)) return FLOCK_ERR_ARG;
+  if (bits <= flock::kHostPowBits) {  // a few dozen hashes: on the calling thread
+    uint8_t d[32];
+    ch->tr.state_digest(d);
+    *nonce = bits ? flock::pow_search_host(d, bits) : 0;
+    ch->tr.nonce(*nonce);
+    return FLOCK_OK;
+  }
   return guard(c, [&] {
     uint64_t n = 0;
     if (bits) {

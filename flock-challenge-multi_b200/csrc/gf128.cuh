@@ -168,9 +168,9 @@ __device__ __forceinline__ f128 mul_x128(f128 a, int k) {  // a * x^k, 0 <= k < 
   }
   return mul_xk(a, k);
 }
-// thread `lane` of the warp writes window `lane`
-__device__ __forceinline__ void tab4_build(Tab4* T, f128 t, int lane) {
-  const f128 b0 = mul_x128(t, 4 * lane), b1 = mul_xk(b0, 1), b2 = mul_xk(b0, 2), b3 = mul_xk(b0, 3);
+// Window w of the table of any GF(2)-linear map L from the images
+// b_i = L(x^(4w + i)), i < 4 (the table of a product by t has b_i = t x^(4w+i)).
+__device__ __forceinline__ void tab4_window(Tab4* T, int w, f128 b0, f128 b1, f128 b2, f128 b3) {
   f128 e[16];
   e[0] = mk(0, 0);
   e[1] = b0;
@@ -180,13 +180,19 @@ __device__ __forceinline__ void tab4_build(Tab4* T, f128 t, int lane) {
   for (int j = 4; j < 8; j++) e[j] = fx(e[j - 4], b2);
 #pragma unroll
   for (int j = 8; j < 16; j++) e[j] = fx(e[j - 8], b3);
-  const int r = lane & 15;
+  const int r = w & 15;
 #pragma unroll
   for (int j = 0; j < 16; j++) {
-    T->lo[lane][j ^ r] = e[j].lo;
-    T->hi[lane][j ^ r] = e[j].hi;
+    T->lo[w][j ^ r] = e[j].lo;
+    T->hi[w][j ^ r] = e[j].hi;
   }
 }
+// thread `lane` of the warp writes window `lane` of the table of t
+__device__ __forceinline__ void tab4_build(Tab4* T, f128 t, int lane) {
+  const f128 b0 = mul_x128(t, 4 * lane);
+  tab4_window(T, lane, b0, mul_xk(b0, 1), mul_xk(b0, 2), mul_xk(b0, 3));
+}
+
 __device__ __forceinline__ f128 tab4_mul(const Tab4* T, f128 y) {
   uint64_t alo = 0, ahi = 0;
 #pragma unroll

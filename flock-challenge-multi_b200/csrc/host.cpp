@@ -275,6 +275,19 @@ void Transcript::label_bytes(const void* p, size_t len) {
   put(n, 8);
   put(p, len);
 }
+uint64_t pow_search_host(const uint8_t digest[32], uint32_t bits) {
+  uint8_t pre[64] = {0}, h[32];
+  memcpy(pre, digest, 32);
+  for (uint64_t n = 0;; n++) {
+    for (int i = 0; i < 8; i++) pre[32 + i] = (uint8_t)(n >> (8 * i));
+    B3 b;
+    b.update(pre, 64);
+    b.digest(h);
+    bool ok = true;
+    for (uint32_t k = 0; k < bits && ok; k++) ok = ((h[k / 8] >> (7 - k % 8)) & 1) == 0;
+    if (ok) return n;
+  }
+}
 bool Transcript::verify_pow(uint64_t nonce, uint32_t bits) {
   bool ok = true;
   if (bits == 0) {

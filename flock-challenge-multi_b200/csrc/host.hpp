@@ -64,6 +64,13 @@ class Transcript {
   B3 h_;
 };
 
+// The smallest nonce whose BLAKE3 root hash of (digest || nonce LE || 0^24)
+// has `bits` leading zero bits, searched on the host (grind_pow,
+// challenger.rs:384-475): for a few bits this is cheaper than a GPU round trip.
+uint64_t pow_search_host(const uint8_t digest[32], uint32_t bits);
+// grinds of at most this many bits run on the host
+constexpr uint32_t kHostPowBits = 6;
+
 // Ligerito query positions: `count` distinct values sample().lo % block_len,
 // first occurrences kept, sorted (pcs/ligerito.rs:9665-9718)
 std::vector<size_t> sample_distinct_queries(Transcript& tr, size_t block_len, size_t count);

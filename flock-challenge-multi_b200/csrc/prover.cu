@@ -340,7 +340,8 @@ uint64_t Setup::grind(Transcript& tr, uint32_t bits) {
   if (bits) {
     uint8_t d[32];
     tr.state_digest(d);
-    nonce = pow_search(d, bits, st, d_found, h_found);
+    // a few dozen hashes on the host cost less than a round trip to the GPU
+    nonce = bits <= kHostPowBits ? pow_search_host(d, bits) : pow_search(d, bits, st, d_found, h_found);
   }
   tr.nonce(nonce);
   return nonce;
@@ -411,7 +412,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   P.m = (uint64_t)m;
   pending_.clear();  // (left over only by a proof that threw)
   stage_off_ = 0;
-  const int G = sms * 4;
+  const int gs = grid_sms > 0 && grid_sms < sms ? grid_sms : sms;
+  const int G = gs * 4;
   const uint32_t n_slots = 1u << n_log;
   mark(0);
   if (!committed) {
@@ -467,7 +469,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     eq_split(elo, ehi, s, (size_t)1 << rh.size(), scratch_eq(), st);
     CK(cudaMemsetAsync(out, 0, 1024 * sizeof(f128), st));
     size_t n_blocks128 = (size_t)1 << (m - 13);
-    zc_round1(a, b, z, tabs_r1, scratch_eq(), n_blocks128, out, sms, st);
+    zc_round1(a, b, z, tabs_r1, scratch_eq(), n_blocks128, out, gs, st);
     fetch(out, 1024, h_out);
     // from here on `out` is a ring of 128 zeroed 8-value slots: every round
     // message accumulates into a fresh slot, so no round needs its own clear
@@ -585,6 +587,36 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     h_out[0] = g1;
     h_out[1] = gi;
   };
+  // The last rounds' vectors are small.  Once a round has at most
+  // kHostZcPairs pairs and only the random suffix weights its pairs (round 7
+  // on), the remaining rounds run on the host from one copy of the vectors
+  // and the eq table: the same folds and sums, without a GPU round trip per
+  // round (a 512-pair round is about 4 K host products, 20 us).
+  constexpr size_t kHostZcPairs = 512;
+  bool host_tail = false;
+  std::vector<f128> ha, hb, he;  // the vectors and eq table once on the host
+  auto host_round = [&](f128 rho) {
+    // fold the 4n values of a and b at rho into 2n, then the message over the
+    // n folded pairs with this round's eq weights, then halve the eq table
+    const size_t n = he.size();
+    for (size_t j = 0; j < 2 * n; j++) {
+      ha[j] = fx(ha[2 * j], hmul(rho, fx(ha[2 * j], ha[2 * j + 1])));
+      hb[j] = fx(hb[2 * j], hmul(rho, fx(hb[2 * j], hb[2 * j + 1])));
+    }
+    ha.resize(2 * n);
+    hb.resize(2 * n);
+    f128 g1 = mk(0, 0), gi = mk(0, 0);
+    for (size_t j = 0; j < n; j++) {
+      const f128 a0 = ha[2 * j], a1 = ha[2 * j + 1], b0 = hb[2 * j], b1 = hb[2 * j + 1];
+      g1 = fx(g1, hmul(he[j], hmul(a1, b1)));
+      gi = fx(gi, hmul(he[j], hmul(fx(a0, a1), fx(b0, b1))));
+    }
+    const f128 K0 = hmul(phi8_table()[1], C_inv);  // ns = nm = 0: phi8(1) * C_round / C_full
+    h_out[0] = hmul(K0, g1);
+    h_out[1] = hmul(K0, gi);
+    for (size_t j = 0; j < n / 2; j++) he[j] = fx(he[2 * j], he[2 * j + 1]);
+    he.resize(n / 2);
+  };
   run_round(0, 0, a, b, nullptr, nullptr, mk(0, 0), n_words);
   f128* av = pp[0];
   f128* bv = pp[1];
@@ -598,12 +630,27 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     rhos.push_back(rho);
     if (i < n_mlv - 1) {
       size_t n_pairs_out = (size_t)1 << (n_mlv - i - 2);
-      if (i == 0) run_round(1, 1, a, b, av, bv, rho, n_pairs_out);
+      if (!host_tail && i + 1 >= 7 && n_pairs_out <= kHostZcPairs) {
+        // av, bv hold the 4 n values the round folds; etab its n eq weights
+        ha.resize(4 * n_pairs_out);
+        hb.resize(4 * n_pairs_out);
+        he.resize(n_pairs_out);
+        CK(cudaMemcpyAsync(ha.data(), av, ha.size() * sizeof(f128), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hb.data(), bv, hb.size() * sizeof(f128), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(he.data(), etab, he.size() * sizeof(f128), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        host_tail = true;
+      }
+      if (host_tail) host_round(rho);
+      else if (i == 0) run_round(1, 1, a, b, av, bv, rho, n_pairs_out);
       else {
         run_round(i + 1, 2, av, bv, av2, bv2, rho, n_pairs_out);
         std::swap(av, av2);
         std::swap(bv, bv2);
       }
+    } else if (host_tail) {  // the last pair, folded at rho
+      P.fa = fx(ha[0], hmul(rho, fx(ha[0], ha[1])));
+      P.fb = fx(hb[0], hmul(rho, fx(hb[0], hb[1])));
     } else {
       f128* o = next_out(1);
       fold_pair_final(av, bv, rho, o, st);
@@ -786,7 +833,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       eq_build(xf.data() + 1 + lo_bits, hi_bits, hone(), base + nlo, st);
     }
     ring_bcombined_ct(d, d + nlo, d + nlo + nhi, d + 2 * nlo + nhi, bc_tabs, bc_tabs + 4096, lo_bits, nhi, pp[1],
-                      sms, st);
+                      gs, st);
   }
   if (chain) {
     // b_combined += gpd eq(point): words w = 0..3 of block i get

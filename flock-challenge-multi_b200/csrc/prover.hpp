@@ -114,6 +114,10 @@ class Setup {
                                         cudaStream_t st);
   uint32_t log2 = 0;
   int n_log = 0, m = 0, sms = 0;
+  // SMs the grid-stride kernels of this setup spread over (0: all).  The
+  // serving queue lowers it for large proofs so that their long persistent
+  // kernels leave some SMs to small proofs' kernels.
+  int grid_sms = 0;
   size_t n_words = 0, n_leaves0 = 0;
   cudaStream_t st = nullptr;
   uint32_t* blocks_buf = nullptr;  // device staging for caller-provided compressions

@@ -12,8 +12,9 @@
 //    statistic is captured by zerocheck round 1 (round1.cu).
 //  * b_combined: with eq(suffix, i) = eq_lo(i_lo) * eq_hi(i_hi), the map
 //    u -> gamma_k L_k(u * eq_hi(i_hi)) is GF(2)-linear; per 2^12-element
-//    chunk it is tabulated once (128 columns, then byte-window doubling) and
-//    applied to eq_lo with 16 lookups per claim — no general products.
+//    chunk it is tabulated once as a 4-bit window table (the images of the
+//    128 basis vectors, then the 16 subset sums of each window) and applied
+//    to eq_lo with 32 conflict-free lookups per claim — no general products.
 #include "kernels.cuh"
 
 // one CTA per output r, one thread per t; the 128 products are XOR-reduced
@@ -47,32 +48,20 @@ __global__ void __launch_bounds__(512) k_bcombined_ct(const f128* __restrict__ e
                                                       const f128* __restrict__ L0, const f128* __restrict__ L1,
                                                       int lo_bits, size_t n_chunks, f128* __restrict__ out) {
   extern __shared__ __align__(16) uint8_t sm[];
-  MulTab8* C0 = reinterpret_cast<MulTab8*>(sm);
-  MulTab8* C1 = C0 + 1;
+  Tab4* C = reinterpret_cast<Tab4*>(sm);  // [2]: the chunk's maps of claims 0 and 1
   const size_t chunk_len = (size_t)1 << lo_bits;
   for (size_t ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
-    const f128 E0 = ldg(ehi0 + ch), E1 = ldg(ehi1 + ch);
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-      int k = i >> 7, j = i & 127;
-      f128 y = k ? E1 : E0;
-      for (int left = j; left > 0; left -= 32) y = mul_xk(y, left < 32 ? left : 32);
-      MulTab8* C = k ? C1 : C0;
-      C->t[j >> 3][1 << (j & 7)] = apply_tab(k ? L1 : L0, y);
-      if ((j & 7) == 0) C->t[j >> 3][0] = mk(0, 0);
+    if (threadIdx.x < 64) {  // thread (k, w): window w of claim k's map
+      const int k = threadIdx.x >> 5, w = threadIdx.x & 31;
+      const f128* L = k ? L1 : L0;
+      const f128 y = mul_x128(ldg((k ? ehi1 : ehi0) + ch), 4 * w);  // E x^(4w)
+      tab4_window(C + k, w, apply_tab(L, y), apply_tab(L, mul_xk(y, 1)), apply_tab(L, mul_xk(y, 2)),
+                  apply_tab(L, mul_xk(y, 3)));
     }
     __syncthreads();
-    for (int lvl = 1; lvl < 8; lvl++) {
-      int base = 1 << lvl, cnt = base - 1;
-      for (int i = threadIdx.x; i < 2 * 16 * cnt; i += blockDim.x) {
-        int k = i / (16 * cnt), rem = i % (16 * cnt), p = rem / cnt, w = 1 + rem % cnt;
-        MulTab8* C = k ? C1 : C0;
-        C->t[p][base + w] = fx(C->t[p][w], C->t[p][base]);
-      }
-      __syncthreads();
-    }
     for (size_t i = threadIdx.x; i < chunk_len; i += blockDim.x)
-      st(out + ch * chunk_len + i, fx(multab_mul(C0, ldg(elo0 + i)), multab_mul(C1, ldg(elo1 + i))));
-    __syncthreads();
+      st(out + ch * chunk_len + i, fx(tab4_mul(C, ldg(elo0 + i)), tab4_mul(C + 1, ldg(elo1 + i))));
+    __syncthreads();  // the next chunk's tables replace these
   }
 }
 
@@ -83,7 +72,7 @@ void ring_shat_ab(const f128* zv_pre, const f128* eqt, f128* out, cudaStream_t s
 
 void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, const f128* ehi1, const f128* L0,
                        const f128* L1, int lo_bits, size_t n_chunks, f128* out, int grid, cudaStream_t s) {
-  size_t smem = 2 * sizeof(MulTab8);
+  size_t smem = 2 * kTab4Bytes;
   CK(cudaFuncSetAttribute(k_bcombined_ct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   count_launch();
   k_bcombined_ct<<<(unsigned)std::min<size_t>(n_chunks, (size_t)grid), 512, smem, s>>>(elo0, ehi0, elo1, ehi1, L0, L1,

@@ -8,8 +8,9 @@ namespace flock {
 
 Server::Server(int device, uint64_t budget, int slots) : device_(device), budget_(budget) {
   if (slots < 1 || slots > 64) throw std::runtime_error("serving slots must be in 1..64");
+  n_slots_ = slots;
   for (int i = 0; i < slots; i++) {
-    const bool small_only = slots >= 3 && i == 0;  // the express slot
+    const bool small_only = slots >= 3 && i < std::max(1, slots / 4);  // the express slots
     workers_.emplace_back([this, small_only] { worker(small_only); });
   }
 }
@@ -113,6 +114,7 @@ std::vector<JobResult> Server::prove_batch(const std::vector<BatchItem>& jobs, i
         }
         const BatchItem& job = jobs[wave[i].first];
         Setup& S = *wave[i].second;
+        S.grid_sms = 0;  // a batch keeps every SM busy
         JobResult& r = res[wave[i].first];
         try {
           if (ready[i].load() == 2) throw std::runtime_error("batch commit: " + commit_err[i]);
@@ -226,18 +228,24 @@ std::unique_ptr<Setup> Server::acquire(uint32_t log2, std::unique_lock<std::mute
       return s;
     }
     const uint64_t need = Setup::estimate_bytes(log2);
-    // evict idle setups of other sizes, least recently used first, until it fits
+    // evict idle setups until it fits: the largest first (least recently used
+    // among equals).  Small setups free little room and are the cheapest to
+    // keep, and rebuilding one would stall a small job far longer than its
+    // proof takes.
     while (bytes_ + need > budget_) {
       uint32_t victim = 0;
       size_t vi = 0;
-      uint64_t oldest = UINT64_MAX;
+      uint64_t oldest = UINT64_MAX, biggest = 0;
       for (auto& kv : idle_)
-        for (size_t i = 0; i < kv.second.size(); i++)
-          if (kv.second[i].last_use < oldest) {
+        for (size_t i = 0; i < kv.second.size(); i++) {
+          const uint64_t sz = kv.second[i].setup->device_bytes;
+          if (sz > biggest || (sz == biggest && kv.second[i].last_use < oldest)) {
+            biggest = sz;
             oldest = kv.second[i].last_use;
             victim = kv.first;
             vi = i;
           }
+        }
       if (oldest == UINT64_MAX) break;  // nothing idle to evict
       auto& vec = idle_[victim];
       bytes_ -= vec[vi].setup->device_bytes;
@@ -295,6 +303,7 @@ void Server::worker(bool small_only) {
       r.error = e.what();
     }
     if (stop_ && !s) return;
+    if (s) s->grid_sms = n_slots_ >= 3 && job.log2 > kSmallLog2 ? s->sms - kReservedSms : 0;
     const auto t_run = Clock::now();
     if (s) {
       lk.unlock();

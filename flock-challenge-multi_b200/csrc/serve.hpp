@@ -6,12 +6,13 @@
 // the host).  The queue is size-aware, so that small jobs do not wait behind
 // 2^19 / 2^20 proofs: a free slot takes the job with the shortest expected
 // proof, aged by its waiting time (a job that has waited kAging times its own
-// expected run time goes ahead of any fresh job); with 3 or more slots one
-// slot takes only small jobs (at most 2^kSmallLog2 compressions), and small
-// jobs' setups run on the highest-priority CUDA stream.  Setups (device buffers + tables for one
+// expected run time goes ahead of any fresh job); with 3 or more slots a
+// quarter of the slots (at least one) take only small jobs (at most
+// 2^kSmallLog2 compressions), and small jobs' setups run on the
+// highest-priority CUDA stream.  Setups (device buffers + tables for one
 // size) are cached per size and reused; admission keeps the bytes of all
-// cached setups within the HBM budget, evicting idle setups of other sizes
-// (least recently used first) when a new size needs room.
+// cached setups within the HBM budget, evicting idle setups (the largest
+// first) when a new setup needs room.
 #pragma once
 #include <atomic>
 #include <chrono>
@@ -67,7 +68,7 @@ class Server {
   // self-check: verify every proof on its own setup before returning it; a
   // proof that fails gets FLOCK_ERR_VERIFY and the failed check's name
   void set_verify(bool on) { verify_ = on; }
-  int slots() const { return (int)workers_.size(); }
+  int slots() const { return n_slots_; }
   uint64_t budget() const { return budget_; }
   uint64_t cached_bytes();
 
@@ -88,6 +89,9 @@ class Server {
   };
 
   static constexpr uint32_t kSmallLog2 = 16;
+  // with an express slot, large proofs' grid-stride kernels leave this many
+  // SMs free, so that a small proof's kernels need not wait for them
+  static constexpr int kReservedSms = 16;
   static constexpr double kAging = 2.0;
   static double expected_ms(uint32_t log2);
   // index of the queued job a free slot takes next (queue_.size() if none)
@@ -110,6 +114,7 @@ class Server {
   uint64_t next_ticket_ = 1, use_clock_ = 0;
   bool stop_ = false;
   std::atomic<bool> verify_{false};
+  int n_slots_ = 0;  // set before the slot threads start (they read it)
   std::vector<std::thread> workers_;
   std::mutex batch_mu_;  // one batch at a time
   cudaStream_t batch_st_ = nullptr;

@@ -461,8 +461,13 @@ class Challenger:
         return out[: 2 * n]
 
     def grind_pow(self, ctx: "Context", bits: int) -> int:
+        """Smallest valid nonce, absorbed; ctx may be None for at most 6 bits (host search)."""
         n = ctypes.c_uint64()
-        ctx._check(self.lib.flock_challenger_grind_pow(self.h, ctx.h, bits, ctypes.byref(n)), "challenger_grind_pow")
+        rc = self.lib.flock_challenger_grind_pow(self.h, ctx.h if ctx else None, bits, ctypes.byref(n))
+        if rc:
+            if ctx:
+                ctx._check(rc, "challenger_grind_pow")
+            raise FlockError(f"challenger_grind_pow failed ({rc})")
         return n.value
 
     def verify_pow(self, nonce: int, bits: int) -> bool:

@@ -151,8 +151,9 @@ void flock_prover_data_destroy(flock_prover_data* pd);
  * observe_f128 absorbs one value and observe_f128_slice a framed slice;
  * sample_f128 / sample_f128_vec squeeze one value / a framed vector
  * ({lo, hi} u64 pairs).  grind_pow finds the smallest nonce whose BLAKE3
- * hash of (state digest || nonce LE || 0^24) has `bits` leading zero bits on
- * the context's GPU and absorbs it (grind_pow, challenger.rs:384-475);
+ * hash of (state digest || nonce LE || 0^24) has `bits` leading zero bits and
+ * absorbs it (grind_pow, challenger.rs:384-475): on the context's GPU, or on
+ * the calling thread for at most 6 bits (ctx may then be NULL);
  * verify_pow checks a nonce and absorbs it (FLOCK_ERR_VERIFY when it fails,
  * challenger.rs:502-545).  A challenger is used by one thread at a time. */
 typedef struct flock_challenger flock_challenger;
@@ -269,11 +270,13 @@ int flock_bench_prove(flock_setup* s, uint64_t seed0, int steps, double* total_m
                       uint64_t* launches);
 
 /* Serving: continuous batching of proof jobs of different sizes on the
- * context's device.  Jobs run in arrival order as proof slots and device
- * memory free up; the kernels of up to `slots` proofs overlap on the GPU.
- * Per-size setups are cached and reused within the HBM budget given to
- * flock_ctx_create (0: the free device memory less 4 GiB), evicting idle
- * setups of other sizes when a new size needs room.  The result of a job is
+ * context's device.  Jobs run as proof slots and device memory free up,
+ * shortest expected proof first (aged by waiting time, with a quarter of the
+ * slots kept for jobs of at most 2^16 compressions); the kernels of up to
+ * `slots` proofs overlap on the GPU.  Per-size setups are cached and reused
+ * within the HBM budget given to flock_ctx_create (0: the free device memory
+ * less 4 GiB), evicting idle setups (the largest first) when a new setup
+ * needs room.  The result of a job is
  * byte-identical to flock_prove_seed / flock_prove_blocks of the same inputs.
  * No counterpart in the reference, which proves one request at a time
  * (benchmark-tools/worker/src/main.rs); this is the served form of the same

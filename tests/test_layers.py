@@ -84,6 +84,25 @@ def test_challenger_verify_pow(oracle):
         L.flockref_ch_free(c)
 
 
+def test_challenger_grind_on_host(oracle):
+    """Grinds of at most 6 bits run on the calling thread (no GPU): the
+    smallest nonce, as the oracle's grind_pow finds it."""
+    import flockgpu
+    L = oracle.L
+    for bits in range(0, 7):
+        c = L.flockref_ch_new(DOM)
+        g = flockgpu.Challenger(DOM)
+        try:
+            L.flockref_ch_label(c, b"host-grind-%d" % bits)
+            g.observe_label(b"host-grind-%d" % bits)
+            assert g.grind_pow(None, bits) == L.flockref_ch_grind(c, bits)
+            assert g.state_digest() == _o_digest(L, c)
+        finally:
+            L.flockref_ch_free(c)
+    with pytest.raises(flockgpu.FlockError):
+        flockgpu.Challenger(DOM).grind_pow(None, 9)  # more bits need the GPU
+
+
 @pytest.mark.gpu
 def test_challenger_grind_on_gpu(gpu_ctx, oracle):
     import flockgpu
