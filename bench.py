@@ -285,8 +285,9 @@ def plain_seconds(ctx, jobs, per_job=False):
 SIZE_CLASSES = ((10, 12), (13, 16), (17, 18), (19, 20))
 
 
-def by_size_class(jobs, lat, alone):
-    """p50 / p99 latency per size class, beside the same jobs' latency alone."""
+def by_size_class(jobs, lat, alone, parts=None):
+    """p50 / p99 latency per size class, beside the same jobs' latency alone;
+    with parts, also where the slowest job of the class spent its time."""
     out = []
     for lo, hi in SIZE_CLASSES:
         idx = [i for i, (l, _) in enumerate(jobs) if lo <= l <= hi]
@@ -296,12 +297,16 @@ def by_size_class(jobs, lat, alone):
         out.append({"log2": [lo, hi], "jobs": len(idx), "p50_ms": pct(L, 0.5), "p99_ms": pct(L, 0.99),
                     "alone_p50_ms": pct(A, 0.5), "alone_p99_ms": pct(A, 0.99),
                     "p99_over_alone_p99": pct(L, 0.99) / pct(A, 0.99)})
+        if parts:
+            w = max(idx, key=lambda i: lat[i])
+            out[-1]["slowest"] = {"log2": jobs[w][0], "latency_ms": lat[w], "queue_ms": parts[w][0],
+                                  "run_ms": parts[w][1], "alone_ms": alone[w]}
     return out
 
 
 def served_run(ctx, jobs, rate=None):
     """Submit the jobs (all at once, or Poisson arrivals at `rate` jobs/s) and
-    collect them; returns (wall seconds, latencies in ms)."""
+    collect them; returns (wall seconds, latencies in ms, (queue ms, run ms) per job)."""
     rng = random.Random(7)
     t0 = time.perf_counter()
     tickets, when = [], 0.0
@@ -312,8 +317,8 @@ def served_run(ctx, jobs, rate=None):
             if dt > 0:
                 time.sleep(dt)
         tickets.append(ctx.submit(l, s))
-    lat = [ctx.poll(t)["latency_ms"] for t in tickets]
-    return time.perf_counter() - t0, lat
+    res = [ctx.poll(t) for t in tickets]
+    return time.perf_counter() - t0, [r["latency_ms"] for r in res], [(r["queue_ms"], r["run_ms"]) for r in res]
 
 
 def pct(v, q):
@@ -345,10 +350,10 @@ def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: i
         res = ctx.prove_batch(jobs, threads=threads)
         wall = time.perf_counter() - t0
         lat = [r["latency_ms"] for r in res]
-        cwall, clat = served_run(ctx, jobs)  # the same jobs through the continuous-batching queue
+        cwall, clat, _ = served_run(ctx, jobs)  # the same jobs through the continuous-batching queue
         # and once more with every proof verified before it is returned
         ctx.serve_verify(True)
-        vwall, vlat = served_run(ctx, jobs)
+        vwall, vlat, _ = served_run(ctx, jobs)
         ctx.serve_verify(False)
         plain = plain_batch
         out["batched"] = {"jobs": len(jobs), "log2_range": [12, 18], "compressions": n,
@@ -371,13 +376,13 @@ def serving_report(device: int, full: bool, slots: int = SERVE_SLOTS, threads: i
         rates = [0.25, 0.5, 1.0, 2.0] if full else [1.0]
         out["served"] = []
         for f in rates:
-            wall, lat = served_run(ctx, jobs, rate=f * cap)
+            wall, lat, parts = served_run(ctx, jobs, rate=f * cap)
             out["served"].append({"arrival_rate_x_plain_capacity": f, "jobs": len(jobs), "log2_range": [lo, hi],
                                   "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
                                   "sustained_value": n / wall, "plain_value": n / plain,
                                   "unit": "compressions/s", "slots": slots,
                                   "hbm_budget_gb": 150,
-                                  "by_size_class": by_size_class(jobs, lat, alone_serve)})
+                                  "by_size_class": by_size_class(jobs, lat, alone_serve, parts)})
     finally:
         ctx.close()
     return out
