@@ -205,7 +205,8 @@ int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const u
     return FLOCK_ERR_ARG;
   }
   return guard(s->ctx, [&] {
-    if (!s->s->blocks_buf) CK(cudaMalloc(&s->s->blocks_buf, n * 25 * sizeof(uint32_t)));
+    if (!s->s->blocks_buf)
+      CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->blocks_buf), n * 25 * sizeof(uint32_t), s->s->st));
     CK(cudaMemcpyAsync(s->s->blocks_buf, blocks, n * 25 * sizeof(uint32_t), cudaMemcpyHostToDevice, s->s->st));
     std::string d((const char*)domain, dlen);
     return emit(s->ctx, s->s->prove(nullptr, s->s->blocks_buf, n, d), out, cap, out_len);
@@ -221,7 +222,8 @@ int flock_prove_compressions(flock_setup* s, const flock_compression* blocks, si
   }
   return guard(s->ctx, [&] {
     const size_t slots = (size_t)1 << s->s->log2;
-    if (!s->s->records_buf) CK(cudaMalloc(&s->s->records_buf, slots * 28 * sizeof(uint32_t)));
+    if (!s->s->records_buf)
+      CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->records_buf), slots * 28 * sizeof(uint32_t), s->s->st));
     CK(cudaMemcpyAsync(s->s->records_buf, blocks, n * sizeof(flock_compression), cudaMemcpyHostToDevice, s->s->st));
     std::string d((const char*)domain, dlen);
     return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d, false, nullptr, true), out, cap, out_len);
@@ -394,7 +396,8 @@ int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const u
     uint32_t st16[16];
     flock::b3_compress(last, last + 8, (uint64_t)last[24] | (uint64_t)last[25] << 32, last[26], last[27], st16);
     memcpy(ends.cv_last, st16, sizeof(ends.cv_last));
-    if (!s->s->records_buf) CK(cudaMalloc(&s->s->records_buf, n * 28 * sizeof(uint32_t)));
+    if (!s->s->records_buf)
+      CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->records_buf), n * 28 * sizeof(uint32_t), s->s->st));
     CK(cudaMemcpyAsync(s->s->records_buf, records, n * 28 * sizeof(uint32_t), cudaMemcpyHostToDevice, s->s->st));
     std::string d((const char*)domain, dlen);
     return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d, false, &ends), out, cap, out_len);

@@ -382,7 +382,6 @@ const f128* device_evals(int dim) {
 // fastest combination per (device, log_d, lanes, layer_begin).
 
 size_t pass_smem(int lgs, int R) { return ((size_t)(1 << lgs) << R) * sizeof(f128) + ((1 << R) - 1) * sizeof(f128); }
-size_t pass_bytes(const NttPass& p) { return p.kind ? pass_w_smem(p.R, p.threads) : pass_smem(p.lgs, p.R); }
 constexpr size_t kSmem2 = (size_t)112 << 10;  // two CTAs per SM
 constexpr size_t kSmem1 = (size_t)200 << 10;  // one CTA per SM
 

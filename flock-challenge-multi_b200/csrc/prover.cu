@@ -15,18 +15,46 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <set>
 
 namespace flock {
 
 namespace {
 thread_local size_t t_alloc_bytes = 0;  // device bytes allocated by this thread's setups
+// Setup buffers come from the stream-ordered allocator on the setup's own
+// stream and go back to it the same way: cudaFree (and cudaFreeHost) wait for
+// the whole device, so a setup built or evicted while other proofs run would
+// stall every one of them until the longest kernel in flight ends.
 template <class T>
-T* dalloc(size_t n) {
+T* dalloc(size_t n, cudaStream_t st) {
   T* p = nullptr;
-  CK(cudaMalloc(&p, n * sizeof(T) + 256));
+  CK(cudaMallocAsync(reinterpret_cast<void**>(&p), n * sizeof(T) + 256, st));
   t_alloc_bytes += n * sizeof(T) + 256;
   return p;
+}
+// Page-locked host blocks are recycled rather than freed, for the same reason.
+std::mutex g_pin_mu;
+std::multimap<size_t, void*> g_pin_free;
+void* pinned_take(size_t bytes) {
+  {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto it = g_pin_free.find(bytes);
+    if (it != g_pin_free.end()) {
+      void* p = it->second;
+      g_pin_free.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  CK(cudaMallocHost(&p, bytes));
+  return p;
+}
+void pinned_give(void* p, size_t bytes) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_pin_mu);
+  g_pin_free.emplace(bytes, p);
 }
 
 }  // namespace
@@ -51,14 +79,14 @@ Setup::Setup(int device, uint32_t log2_, int stream_priority) : log2(log2_) {
   n_words = (size_t)1 << (m - 7);
   digest = statement_digest(m);
   CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, stream_priority));
-  z = dalloc<f128>(n_words);
-  a = dalloc<f128>(n_words);
-  b = dalloc<f128>(n_words);
-  cw0 = dalloc<f128>(2 * n_words);
+  z = dalloc<f128>(n_words, st);
+  a = dalloc<f128>(n_words, st);
+  b = dalloc<f128>(n_words, st);
+  cw0 = dalloc<f128>(2 * n_words, st);
   n_leaves0 = (size_t)1 << (m - 12);
-  tree0 = dalloc<uint32_t>(8 * (2 * n_leaves0 - 1));
-  for (int i = 0; i < 4; i++) pp[i] = dalloc<f128>(n_words);
-  eqbuf[0] = dalloc<f128>(n_words);
+  tree0 = dalloc<uint32_t>(8 * (2 * n_leaves0 - 1), st);
+  for (int i = 0; i < 4; i++) pp[i] = dalloc<f128>(n_words, st);
+  eqbuf[0] = dalloc<f128>(n_words, st);
   // recursive Ligero levels
   int n_cur = m - 7 - lad->initial_k;
   for (size_t i = 0; i < lad->ks.size(); i++) {
@@ -67,33 +95,36 @@ Setup::Setup(int device, uint32_t log2_, int stream_priority) : log2(log2_) {
     L.log_msg_pos = n_cur - lad->ks[i];
     L.rate = lad->rate[i + 1];
     L.positions = (size_t)1 << (L.log_msg_pos + L.rate);
-    L.cw = dalloc<f128>(L.positions * L.lanes);
-    L.tree = dalloc<uint32_t>(8 * (2 * L.positions - 1));
+    L.cw = dalloc<f128>(L.positions * L.lanes, st);
+    L.tree = dalloc<uint32_t>(8 * (2 * L.positions - 1), st);
     levels.push_back(L);
     n_cur -= lad->ks[i];
   }
-  induce_buf = dalloc<f128>((size_t)1 << (m - 7 - lad->initial_k + lad->rate[0]));
-  out = dalloc<f128>(1024);
-  tabs_r1 = dalloc<uint8_t>(round1_tables_size());
-  lag = dalloc<f128>(8 * 256);
-  elo = dalloc<f128>(1 << 13);
-  ehi = dalloc<f128>(1 << 16);
-  comb = dalloc<f128>(kK);
-  zv = dalloc<f128>(kK);
-  zv_pre = dalloc<f128>(kK);
-  eq_inner = dalloc<f128>(kK);
-  bc_tabs = dalloc<f128>(2 * 16 * 256);
-  idx = dalloc<uint64_t>(1 << 16);
-  gather = dalloc<f128>(1 << 16);
-  d_found = dalloc<unsigned long long>(1);
-  CK(cudaMallocHost(&h_found, 8));
-  CK(cudaMallocHost(&h_out, 1024 * sizeof(f128)));
-  CK(cudaMallocHost(&h_stage, kStageBytes));
+  induce_buf = dalloc<f128>((size_t)1 << (m - 7 - lad->initial_k + lad->rate[0]), st);
+  out = dalloc<f128>(1024, st);
+  tabs_r1 = dalloc<uint8_t>(round1_tables_size(), st);
+  lag = dalloc<f128>(8 * 256, st);
+  elo = dalloc<f128>(1 << 13, st);
+  ehi = dalloc<f128>(1 << 16, st);
+  comb = dalloc<f128>(kK, st);
+  zv = dalloc<f128>(kK, st);
+  zv_pre = dalloc<f128>(kK, st);
+  eq_inner = dalloc<f128>(kK, st);
+  bc_tabs = dalloc<f128>(2 * 16 * 256, st);
+  idx = dalloc<uint64_t>(1 << 16, st);
+  gather = dalloc<f128>(1 << 16, st);
+  d_found = dalloc<unsigned long long>(1, st);
+  h_found = static_cast<unsigned long long*>(pinned_take(8));
+  h_out = static_cast<f128*>(pinned_take(1024 * sizeof(f128)));
+  h_stage = static_cast<uint8_t*>(pinned_take(kStageBytes));
   const Statement& S = blake3_statement();
-  at_ptr = dalloc<uint32_t>(S.at_ptr.size());
-  bt_ptr = dalloc<uint32_t>(S.bt_ptr.size());
-  at_row = dalloc<uint16_t>(S.at_row.size());
-  bt_row = dalloc<uint16_t>(S.bt_row.size());
+  at_ptr = dalloc<uint32_t>(S.at_ptr.size(), st);
+  bt_ptr = dalloc<uint32_t>(S.bt_ptr.size(), st);
+  at_row = dalloc<uint16_t>(S.at_row.size(), st);
+  bt_row = dalloc<uint16_t>(S.bt_row.size(), st);
+  // the allocations above are ordered on st: complete them before other
+  // streams (the synchronous copies below, later a batch stream) touch them
+  CK(cudaStreamSynchronize(st));
   CK(cudaMemcpy(at_ptr, S.at_ptr.data(), S.at_ptr.size() * 4, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(bt_ptr, S.bt_ptr.data(), S.bt_ptr.size() * 4, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(at_row, S.at_row.data(), S.at_row.size() * 2, cudaMemcpyHostToDevice));
@@ -105,6 +136,7 @@ Setup::Setup(int device, uint32_t log2_, int stream_priority) : log2(log2_) {
   for (int i = 0; i < kPhases + 1; i++) CK(cudaEventCreate(&ev[i]));
   tune_ntt_plans();
   capture_commit();
+  CK(cudaStreamSynchronize(st));  // the buffers exist for every stream from here on
   device_bytes = t_alloc_bytes - bytes0;
 }
 
@@ -230,8 +262,9 @@ BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vec
   for (int i = 0; i < n; i++)
     for (int l = 0; l < 24; l++) J[i].par0[l] = std::min<uint64_t>(J[i].par0[l], par[l]);
   BatchJob* dj = nullptr;
-  CK(cudaMalloc(&dj, n * sizeof(BatchJob)));
+  CK(cudaMallocAsync(reinterpret_cast<void**>(&dj), n * sizeof(BatchJob), st));
   h.jobs = dj;
+  h.st = st;
   try {
     CK(cudaMemcpyAsync(dj, J.data(), n * sizeof(BatchJob), cudaMemcpyHostToDevice, st));
     int dev = 0, sms = 0;
@@ -263,7 +296,7 @@ BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vec
 void batch_commit_release(BatchCommit& h) {
   if (h.done) cudaEventDestroy(h.done);
   if (h.graph) cudaGraphExecDestroy(h.graph);
-  if (h.jobs) cudaFree(h.jobs);
+  if (h.jobs) cudaFreeAsync(h.jobs, h.st);
   h = BatchCommit{};
 }
 
@@ -279,11 +312,15 @@ Setup::~Setup() {
   void* ptrs[] = {z, a, b, cw0, tree0, pp[0], pp[1], pp[2], pp[3], eqbuf[0], zv_pre, induce_buf, out, blocks_buf, records_buf,
                   tabs_r1, lag, elo, ehi, comb, zv, eq_inner, bc_tabs, idx, gather, d_found, at_ptr, bt_ptr,
                   at_row, bt_row};
-  for (void* p : ptrs) cudaFree(p);
-  for (auto& L : levels) { cudaFree(L.cw); cudaFree(L.tree); }
-  cudaFreeHost(h_found);
-  cudaFreeHost(h_out);
-  cudaFreeHost(h_stage);
+  for (void* p : ptrs)
+    if (p) cudaFreeAsync(p, st);
+  for (auto& L : levels) {
+    if (L.cw) cudaFreeAsync(L.cw, st);
+    if (L.tree) cudaFreeAsync(L.tree, st);
+  }
+  pinned_give(h_found, 8);
+  pinned_give(h_out, 1024 * sizeof(f128));
+  pinned_give(h_stage, kStageBytes);
   for (auto g : commit_graph)
     if (g) cudaGraphExecDestroy(g);
   for (int i = 0; i < kPhases + 1; i++) cudaEventDestroy(ev[i]);

@@ -17,7 +17,8 @@ class Setup;
 // the commit; batch_commit_async only queues it and returns the resources to
 // release (batch_commit_release) once st has finished.
 struct BatchCommit {
-  BatchJob* jobs = nullptr;  // device job table
+  BatchJob* jobs = nullptr;  // device job table (stream-ordered on st)
+  cudaStream_t st = nullptr;
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t done = nullptr;
 };

@@ -120,7 +120,8 @@ std::vector<JobResult> Server::prove_batch(const std::vector<BatchItem>& jobs, i
           if (ready[i].load() == 2) throw std::runtime_error("batch commit: " + commit_err[i]);
           if (job.blocks) {
             const size_t n = (size_t)1 << job.log2;
-            if (!S.blocks_buf) CK(cudaMalloc(&S.blocks_buf, n * 25 * sizeof(uint32_t)));
+            if (!S.blocks_buf)
+              CK(cudaMallocAsync(reinterpret_cast<void**>(&S.blocks_buf), n * 25 * sizeof(uint32_t), S.st));
             CK(cudaMemcpyAsync(S.blocks_buf, job.blocks, n * 25 * sizeof(uint32_t), cudaMemcpyHostToDevice, S.st));
             r.bytes = S.prove(nullptr, S.blocks_buf, n, job.domain);
           } else {
@@ -310,7 +311,8 @@ void Server::worker(bool small_only) {
       try {
         if (job.has_blocks) {
           const size_t n = (size_t)1 << job.log2;
-          if (!s->blocks_buf) CK(cudaMalloc(&s->blocks_buf, n * 25 * sizeof(uint32_t)));
+          if (!s->blocks_buf)
+            CK(cudaMallocAsync(reinterpret_cast<void**>(&s->blocks_buf), n * 25 * sizeof(uint32_t), s->st));
           CK(cudaMemcpyAsync(s->blocks_buf, job.blocks.data(), n * 25 * sizeof(uint32_t), cudaMemcpyHostToDevice,
                              s->st));
           r.bytes = s->prove(nullptr, s->blocks_buf, n, job.domain);
