@@ -471,6 +471,20 @@ void flock_host_free(void* p) {
   if (p) cudaFreeHost(p);
 }
 
+int flock_serve_prewarm(flock_ctx* c, uint32_t log2_n, int count, int* cached) {
+  if (!c || log2_n < 8 || log2_n > 20 || count < 0) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->server) {
+      c->err = "serving not started";
+      return (int)FLOCK_ERR_ARG;
+    }
+    const int n = c->server->prewarm(log2_n, count);
+    if (cached) *cached = n;
+    return (int)FLOCK_OK;
+  });
+}
+
 int flock_serve_start(flock_ctx* c, int slots) {
   if (!c || slots < 1 || slots > 64) return FLOCK_ERR_ARG;
   return guard(c, [&] {

@@ -217,6 +217,26 @@ uint64_t Server::cached_bytes() {
   return bytes_;
 }
 
+int Server::prewarm(uint32_t log2, int count) {
+  std::unique_lock<std::mutex> lk(mu_);
+  std::vector<std::unique_ptr<Setup>> held;  // taken so that acquire builds new ones
+  const uint64_t need = Setup::estimate_bytes(log2);
+  try {
+    while ((int)(idle_[log2].size() + held.size()) < count) {
+      // build only into free room: prewarming never evicts a cached setup
+      if (idle_[log2].empty() && bytes_ + need > budget_) break;
+      std::unique_ptr<Setup> s = acquire(log2, lk, false);
+      if (!s) break;
+      held.push_back(std::move(s));
+    }
+  } catch (...) {
+    for (auto& s : held) release(std::move(s));
+    throw;
+  }
+  for (auto& s : held) release(std::move(s));
+  return (int)idle_[log2].size();
+}
+
 // Called with the lock held; may drop it while constructing a setup.
 std::unique_ptr<Setup> Server::acquire(uint32_t log2, std::unique_lock<std::mutex>& lk, bool wait) {
   for (;;) {

@@ -65,6 +65,11 @@ class Server {
   };
   std::vector<JobResult> prove_batch(const std::vector<BatchItem>& jobs, int threads);
 
+  // Builds setups of size log2 until `count` of them are cached idle (as
+  // many as fit the free budget: it evicts nothing); returns how many are.  Building a setup takes
+  // tens of milliseconds, so a server that expects bursts of a size builds
+  // them before the jobs arrive.
+  int prewarm(uint32_t log2, int count);
   // self-check: verify every proof on its own setup before returning it; a
   // proof that fails gets FLOCK_ERR_VERIFY and the failed check's name
   void set_verify(bool on) { verify_ = on; }

@@ -35,6 +35,7 @@ EXPORTS = (
     "flock_challenger_observe_f128_slice", "flock_challenger_sample_f128", "flock_challenger_sample_f128_vec",
     "flock_challenger_grind_pow", "flock_challenger_verify_pow", "flock_challenger_state_digest",
     "flock_ntt_plan_desc", "flock_bench_ntt_plan", "flock_bench_f128_product", "flock_launch_count",
+    "flock_serve_prewarm",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -115,6 +116,7 @@ def load() -> ctypes.CDLL:
                                           ctypes.POINTER(u64)]
         lib.flock_merkle_root_noalloc.argtypes = [vp, sz, sz, vp, vp]
         lib.flock_serve_start.argtypes = [vp, i32]
+        lib.flock_serve_prewarm.argtypes = [vp, u32, i32, ctypes.POINTER(i32)]
         lib.flock_submit.argtypes = [vp, ctypes.POINTER(FlockJob), ctypes.POINTER(u64)]
         lib.flock_poll.argtypes = [vp, u64, ctypes.POINTER(FlockResult), i32]
         lib.flock_host_alloc.argtypes = [sz, ctypes.POINTER(vp)]
@@ -240,6 +242,13 @@ class Context:
     # ---- serving (continuous batching of proof jobs) ----
     def serve_start(self, slots: int = 4) -> None:
         self._check(self.lib.flock_serve_start(self.h, slots), "serve_start")
+
+    def serve_prewarm(self, log2: int, count: int = 1) -> int:
+        """Cache `count` idle setups of 2^log2 in free HBM budget (never
+        evicting one); returns how many are cached."""
+        n = ctypes.c_int()
+        self._check(self.lib.flock_serve_prewarm(self.h, log2, count, ctypes.byref(n)), "serve_prewarm")
+        return n.value
 
     def verify(self, bundle: bytes, domain: bytes = DOMAIN) -> str:
         """'' when the FLOCK v4 bundle verifies (any supported size, no prover

@@ -301,6 +301,14 @@ typedef struct flock_result {
  * starts it with 4). */
 int flock_serve_start(flock_ctx* ctx, int slots);
 int flock_submit(flock_ctx* ctx, const flock_job* job, uint64_t* ticket);
+/* Builds setups for 2^log2_n compressions until `count` are cached idle (as
+ * many as fit the free HBM budget: prewarming evicts no cached setup);
+ * *cached receives how many are.  A setup
+ * takes tens of milliseconds to build (device buffers, statement tables,
+ * tuned NTT plans, captured commit graphs), which a job that finds none
+ * waits for; a server that expects bursts of a size builds them first.  No
+ * counterpart in the reference. */
+int flock_serve_prewarm(flock_ctx* ctx, uint32_t log2_n, int count, int* cached);
 /* FLOCK_OK once the job finished (then res->status is the proof's status),
  * FLOCK_ERR_TIMEOUT if it did not finish within timeout_ms (< 0: wait), or
  * FLOCK_ERR_CAPACITY with res->out_len set when res->cap is too small (the

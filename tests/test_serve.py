@@ -74,6 +74,40 @@ def test_budget_evicts_and_rejects():
         ctx.close()
 
 
+def test_prewarm_fills_free_budget_only():
+    import flockgpu
+    ctx = flockgpu.Context(0, hbm_budget_bytes=150 << 20)
+    try:
+        with pytest.raises(flockgpu.FlockError):
+            ctx.serve_prewarm(8, 1)  # serving not started
+        ctx.serve_start(1)
+        # one ~100 MiB setup fits the budget, a second does not
+        assert ctx.serve_prewarm(8, 3) == 1
+        assert ctx.serve_prewarm(8, 1) == 1
+        # prewarming another size evicts nothing: no room, nothing built
+        assert ctx.serve_prewarm(9, 1) == 0
+        want = _alone(flockgpu.Context(0), [(8, 41)])
+        t = ctx.submit(8, 41)
+        assert hashlib.sha256(ctx.poll(t)["bytes"]).hexdigest() == want[(8, 41)]
+    finally:
+        ctx.close()
+    ctx = flockgpu.Context(0)
+    try:
+        ctx.serve_start(2)
+        assert ctx.serve_prewarm(10, 2) == 2
+        jobs = [(10, 42), (10, 43), (11, 44)]
+        tickets = [ctx.submit(l, s) for l, s in jobs]
+        got = [hashlib.sha256(ctx.poll(t)["bytes"]).hexdigest() for t in tickets]
+        ref = flockgpu.Context(0)
+        try:
+            want = _alone(ref, jobs)
+        finally:
+            ref.close()
+        assert got == [want[j] for j in jobs]
+    finally:
+        ctx.close()
+
+
 def test_poll_timeout_returns_none():
     import flockgpu
     ctx = flockgpu.Context(0)
