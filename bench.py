@@ -512,6 +512,44 @@ def chain_report(prover, log2: int, steps: int = 5) -> dict:
                       "h2d_bytes_per_proof": n * 112, "phases_ms": {k: round(v, 3) for k, v in ph.items()}}}
 
 
+def sha256_report(ctx, sizes=(16, 18), steps: int = 5) -> dict:
+    """The SHA-256 compression statement (Sha256HybridSetup::prove_fast,
+    r1cs_hashes/sha2.rs) on its own setups: 2^16 compressions (the largest
+    default size of the reference's benches/sha2_proof.rs) and 2^18 (the
+    headline's count), inputs from that bench's generator.  Device time is
+    the sum of the proof's phase events (seeded inputs generated on the GPU);
+    e2e goes through flock_sha256_prove from pinned host compressions (H2D of
+    the records, prove, D2H of the bundle), host clock, medians of `steps`."""
+    import flockgpu
+    rows = []
+    for log2 in sizes:
+        n = 1 << log2
+        prover = flockgpu.Sha256Prover(ctx, n)
+        comps = flockgpu.PinnedArray((n, 24), np.uint32)
+        comps.array[:] = flockgpu.sha256_bench_inputs(n, flockgpu.sha256_bench_seed(n))
+        for _ in range(2):
+            prover.prove(comps.array)
+        dev, wall = [], []
+        for i in range(steps):
+            prover.prove_seed(flockgpu.sha256_bench_seed(n, i + 1))
+            ph = prover.phase_ms()
+            dev.append(sum(ph.values()))
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            size = len(prover.prove(comps.array))
+            wall.append(time.perf_counter() - t0)
+        why = prover.verify(prover.prove(comps.array))
+        prover.close()
+        if why:
+            raise SystemExit(f"sha256_report: proof rejected: {why}")
+        d, e = pct(dev, 0.5), pct(wall, 0.5)
+        rows.append({"log2": log2, "m": 15 + log2, "device_ms_median": d, "device_compressions_per_s": n / (d / 1e3),
+                     "e2e_ms_median": e * 1e3, "e2e_compressions_per_s": n / e, "proof_bytes": size,
+                     "h2d_bytes_per_proof": n * 96, "phases_ms": {k: round(v, 3) for k, v in ph.items()}})
+    return {"sha256": {"statement": "SHA-256 compressions, one per 2^15-bit block (hybrid R1CS, sha2.rs)",
+                       "proofs": rows}}
+
+
 def verify_report(prover, log2: int, reps: int = 3) -> dict:
     """The verifier behind flock_verify on this setup: one compression proof
     and one chain proof of 2^log2 compressions, host wall clock per call
@@ -617,6 +655,8 @@ def run_ours(args, world, rank, local):
     if world == 1 and not args.no_chain:
         line.update(chain_report(prover, log2))
         line.update(verify_report(prover, log2))
+    if world == 1 and not args.no_sha256:
+        line.update(sha256_report(ctx))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     if world == 1 and not args.no_serve:
@@ -636,6 +676,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the batched / served measurements")
     ap.add_argument("--no-chain", action="store_true", help="skip the hash-chain measurement")
+    ap.add_argument("--no-sha256", action="store_true", help="skip the SHA-256 statement measurement")
+    ap.add_argument("--sha256", default=None, metavar="LOG2[,LOG2...]",
+                    help="only the SHA-256 statement report at these sizes")
     ap.add_argument("--ntt-case", default=None, metavar="LOG_MSG,LANES,RATE,PLAN",
                     help="one RS encode with candidate pass plan PLAN (no autotuning launches): the case that "
                          "the NTT's ncu captures profile")
@@ -690,6 +733,12 @@ def main():
         print(json.dumps({"launches_before_proof": int(flockgpu.load().flock_launch_count())}), flush=True)
         prover.prove_seed(2)
         prover.close()
+        ctx.close()
+        return
+    if args.sha256:
+        import flockgpu
+        ctx = flockgpu.Context(0)
+        print(json.dumps(sha256_report(ctx, tuple(int(x) for x in args.sha256.split(",")))), flush=True)
         ctx.close()
         return
     if args.kernels:

@@ -193,13 +193,22 @@ int flock_prove_seed(flock_setup* s, uint64_t seed, const uint8_t* domain, size_
   if (!s || (!domain && dlen)) return FLOCK_ERR_ARG;
   return guard(s->ctx, [&] {
     std::string d((const char*)domain, dlen);
-    return emit(s->ctx, s->s->prove(&seed, nullptr, 0, d), out, cap, out_len);
+    // a SHA-256 setup generates its n_blocks compressions; a BLAKE3 one 2^log2
+    const size_t n = s->s->hash == flock::kHashSha256 ? s->n_blocks : 0;
+    return emit(s->ctx, s->s->prove(&seed, nullptr, n, d), out, cap, out_len);
   });
+}
+
+static bool is_blake3(flock_setup* s) {
+  if (s->s->hash == flock::kHashBlake3) return true;
+  s->ctx->err = "this entry point proves BLAKE3 compressions; the setup is a SHA-256 statement";
+  return false;
 }
 
 int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const uint8_t* domain, size_t dlen,
                        uint8_t* out, size_t cap, size_t* out_len) {
   if (!s || !blocks || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (!is_blake3(s)) return FLOCK_ERR_ARG;
   if (n != ((size_t)1 << s->s->log2)) {
     s->ctx->err = "expected exactly 2^log2 compressions";
     return FLOCK_ERR_ARG;
@@ -216,6 +225,7 @@ int flock_prove_blocks(flock_setup* s, const uint32_t* blocks, size_t n, const u
 int flock_prove_compressions(flock_setup* s, const flock_compression* blocks, size_t n, const uint8_t* domain,
                              size_t dlen, uint8_t* out, size_t cap, size_t* out_len) {
   if (!s || !blocks || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (!is_blake3(s)) return FLOCK_ERR_ARG;
   if (n != s->n_blocks) {
     s->ctx->err = "expected exactly the setup's n_blocks compressions";
     return FLOCK_ERR_ARG;
@@ -227,6 +237,179 @@ int flock_prove_compressions(flock_setup* s, const flock_compression* blocks, si
     CK(cudaMemcpyAsync(s->s->records_buf, blocks, n * sizeof(flock_compression), cudaMemcpyHostToDevice, s->s->st));
     std::string d((const char*)domain, dlen);
     return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d, false, nullptr, true), out, cap, out_len);
+  });
+}
+
+// ---- SHA-256 compressions (r1cs_hashes/sha2.rs)
+int flock_sha256_setup_create(flock_ctx* c, size_t n_compressions, int hash, int profile, flock_setup** out) {
+  if (!c || !out) return FLOCK_ERR_ARG;
+  // min_n_blocks_log (sha2.rs:1217-1221): 2^max(3, ceil(log2 n)) slots
+  uint32_t n_log = 3;
+  while (n_compressions && ((size_t)1 << n_log) < n_compressions) n_log++;
+  if (n_compressions == 0 || n_log < 7 || n_log > 19 || hash != FLOCK_HASH_BLAKE3 || profile != FLOCK_PROFILE_FAST) {
+    c->err = "unsupported SHA-256 setup (65..=2^19 compressions: the fast profile's Ligerito ladders cover "
+             "m = 22..34; BLAKE3 Merkle hash, fast profile)";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(c, [&] {
+    auto* s = new flock_setup();
+    s->ctx = c;
+    s->s.reset(new flock::Setup(c->device, n_log, 0, flock::kHashSha256));
+    s->n_blocks = n_compressions;
+    *out = s;
+    return FLOCK_OK;
+  });
+}
+
+int flock_sha256_prove(flock_setup* s, const flock_sha256_compression* comps, size_t n, const uint8_t* domain,
+                       size_t dlen, uint8_t* out, size_t cap, size_t* out_len) {
+  if (!s || !comps || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (s->s->hash != flock::kHashSha256) {
+    s->ctx->err = "not a SHA-256 setup";
+    return FLOCK_ERR_ARG;
+  }
+  if (n != s->n_blocks) {
+    s->ctx->err = "expected exactly the setup's n_compressions compressions";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(s->ctx, [&] {
+    if (!s->s->records_buf)
+      CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->records_buf), n * sizeof(flock_sha256_compression),
+                         s->s->st));
+    CK(cudaMemcpyAsync(s->s->records_buf, comps, n * sizeof(flock_sha256_compression), cudaMemcpyHostToDevice,
+                       s->s->st));
+    std::string d((const char*)domain, dlen);
+    return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d), out, cap, out_len);
+  });
+}
+
+int flock_sha256_merkle_prove(flock_setup* s, const flock_sha256_compression* comps, size_t n, const uint8_t* b_bits,
+                              uint32_t path_log, const uint8_t* domain, size_t dlen, uint8_t* out, size_t cap,
+                              size_t* out_len) {
+  if (!s || !comps || !b_bits || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (s->s->hash != flock::kHashSha256 || n != s->n_blocks || n != ((size_t)1 << s->s->n_log) ||
+      path_log > (uint32_t)s->s->n_log) {
+    s->ctx->err = "a Merkle-path proof needs a SHA-256 setup whose n_compressions (a power of two) it fills, "
+                  "and path_log <= log2(n)";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(s->ctx, [&] {
+    if (!s->s->records_buf)
+      CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->records_buf), n * sizeof(flock_sha256_compression),
+                         s->s->st));
+    CK(cudaMemcpyAsync(s->s->records_buf, comps, n * sizeof(flock_sha256_compression), cudaMemcpyHostToDevice,
+                       s->s->st));
+    flock::MerkleArgs ma;
+    ma.path_log = (int)path_log;
+    ma.b_bits = b_bits;
+    std::string d((const char*)domain, dlen);
+    return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d, false, nullptr, false, &ma), out, cap,
+                out_len);
+  });
+}
+
+int flock_sha256_merkle_verify(flock_ctx* c, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen,
+                               uint32_t path_log, const uint8_t* b_bits, size_t n, const uint32_t* leaves,
+                               const uint32_t* root) {
+  if (!c || !bytes || !b_bits || !leaves || !root || (!domain && dlen) || path_log > 30 || n == 0 ||
+      (n & (n - 1)) || ((size_t)1 << path_log) > n)
+    return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    flock::MerklePublic mp;
+    mp.path_log = (int)path_log;
+    mp.b_bits.assign(b_bits, b_bits + n);
+    mp.leaves.resize((size_t)1 << path_log);
+    for (size_t p = 0; p < mp.leaves.size(); p++) memcpy(mp.leaves[p].data(), leaves + 8 * p, 32);
+    memcpy(mp.root.data(), root, 32);
+    std::lock_guard<std::mutex> lk(c->vmu);
+    if (!c->verifier) c->verifier.reset(new flock::Verifier(c->device));
+    const std::string why =
+        c->verifier->verify(bytes, len, std::string((const char*)domain, dlen), flock::kHashSha256, &mp);
+    if (why.empty()) return (int)FLOCK_OK;
+    c->err = "verify: " + why;
+    return (int)FLOCK_ERR_VERIFY;
+  });
+}
+
+int flock_sha256_merkle_inputs(uint32_t n_log, uint32_t path_log, uint64_t seed, flock_sha256_compression* comps,
+                               uint8_t* b_bits, uint32_t* leaves, uint32_t* root) {
+  if (!comps || !b_bits || !leaves || !root || n_log > 24 || path_log > n_log) return FLOCK_ERR_ARG;
+  static const uint32_t kIv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                                  0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+  uint64_t st = seed;
+  auto nx = [&]() {
+    st += 0x9E3779B97F4A7C15ull;
+    uint64_t z = st;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return (uint32_t)(z ^ (z >> 31));
+  };
+  const size_t L = (size_t)1 << (n_log - path_log), P = (size_t)1 << path_log;
+  uint32_t cur[8];
+  for (int k = 0; k < 8; k++) cur[k] = nx();
+  for (size_t p = 0; p < P; p++) memcpy(leaves + 8 * p, cur, 32);
+  b_bits[0] = 0;
+  for (size_t i = 1; i < L; i++) b_bits[i] = nx() & 1;
+  for (size_t i = 0; i < L; i++) {
+    uint32_t sib[8];
+    for (int k = 0; k < 8; k++) sib[k] = nx();
+    flock_sha256_compression& cp = comps[i];
+    memcpy(cp.h, kIv, 32);
+    memcpy(cp.m + (b_bits[i] ? 8 : 0), cur, 32);
+    memcpy(cp.m + (b_bits[i] ? 0 : 8), sib, 32);
+    flock::sha256_compress(cp.h, cp.m, cur);
+  }
+  memcpy(root, cur, 32);
+  for (size_t p = 1; p < P; p++) {
+    memcpy(comps + p * L, comps, L * sizeof(flock_sha256_compression));
+    memcpy(b_bits + p * L, b_bits, L);
+  }
+  return FLOCK_OK;
+}
+
+void flock_sha256_compress(const uint32_t* h_in, const uint32_t* m, uint32_t* out) {
+  if (h_in && m && out) flock::sha256_compress(h_in, m, out);
+}
+
+int flock_sha256_verify_bundle(flock_ctx* c, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen) {
+  if (!c || !bytes || (!domain && dlen)) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    std::lock_guard<std::mutex> lk(c->vmu);
+    if (!c->verifier) c->verifier.reset(new flock::Verifier(c->device));
+    const std::string why =
+        c->verifier->verify(bytes, len, std::string((const char*)domain, dlen), flock::kHashSha256);
+    if (why.empty()) return (int)FLOCK_OK;
+    c->err = "verify: " + why;
+    return (int)FLOCK_ERR_VERIFY;
+  });
+}
+
+int flock_sha256_statement_digest(uint32_t m, uint8_t* out32) {
+  if (!out32 || m < 18 || m > 40) return FLOCK_ERR_ARG;
+  try {
+    auto d = flock::statement_digest(flock::kHashSha256, (int)m);
+    memcpy(out32, d.data(), 32);
+    return FLOCK_OK;
+  } catch (...) {
+    return FLOCK_ERR_INTERNAL;
+  }
+}
+
+int flock_sha256_witness(flock_ctx* c, const flock_sha256_compression* comps, size_t n, uint32_t n_log, uint64_t* z,
+                         uint64_t* a, uint64_t* b) {
+  if (!c || !z || !a || !b || n_log < 3 || n_log > 20 || n > ((size_t)1 << n_log) || (n && !comps))
+    return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    const size_t slots = (size_t)1 << n_log, words = slots * 256;
+    DevBuf<f128> dz(words), da(words), db(words);
+    DevBuf<uint32_t> dr(n ? n * 24 : 1);
+    if (n) CK(cudaMemcpyAsync(dr.p, comps, n * 96, cudaMemcpyHostToDevice, c->st));
+    launch_witness_sha(dr.p, 0, (uint32_t)n, (uint32_t)slots, dz.p, da.p, db.p, c->st);
+    CK(cudaMemcpyAsync(z, dz.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(a, da.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(b, db.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
   });
 }
 
@@ -385,6 +568,7 @@ int flock_challenger_state_digest(flock_challenger* ch, uint8_t* out32) {
 int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const uint8_t* domain, size_t dlen,
                       uint8_t* out, size_t cap, size_t* out_len) {
   if (!s || !records || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (!is_blake3(s)) return FLOCK_ERR_ARG;
   if (n != ((size_t)1 << s->s->log2)) {
     s->ctx->err = "a chain fills every slot: expected exactly 2^log2 compressions";
     return FLOCK_ERR_ARG;

@@ -368,7 +368,7 @@ Set prefix(int base, int n) {  // {base, ..., base + n - 1}
 struct SymWord {
   std::array<Set, 32> b;
   static SymWord slots(int base) { SymWord w; for (int i = 0; i < 32; i++) w.b[i] = {(uint16_t)(base + i)}; return w; }
-  static SymWord konst(uint32_t v) { SymWord w; for (int i = 0; i < 32; i++) if (v >> i & 1) w.b[i] = {(uint16_t)kZConst}; return w; }
+  static SymWord konst(uint32_t v, int pin = kZConst) { SymWord w; for (int i = 0; i < 32; i++) if (v >> i & 1) w.b[i] = {(uint16_t)pin}; return w; }
   SymWord operator^(const SymWord& o) const { SymWord w; for (int i = 0; i < 32; i++) w.b[i] = sdiff(b[i], o.b[i]); return w; }
   SymWord rotr(int n) const { SymWord w; for (int i = 0; i < 32; i++) w.b[i] = b[(i + n) & 31]; return w; }
 };
@@ -399,12 +399,13 @@ void to_csr(const std::vector<Set>& rows, std::vector<uint32_t>& ptr, std::vecto
 }
 void to_csc(const std::vector<uint32_t>& ptr, const std::vector<uint16_t>& col,
             std::vector<uint32_t>& cptr, std::vector<uint16_t>& crow) {
-  cptr.assign(kK + 1, 0);
+  const int k = (int)ptr.size() - 1;
+  cptr.assign(k + 1, 0);
   for (uint16_t c : col) cptr[c + 1]++;
-  for (int c = 0; c < kK; c++) cptr[c + 1] += cptr[c];
+  for (int c = 0; c < k; c++) cptr[c + 1] += cptr[c];
   crow.resize(col.size());
   std::vector<uint32_t> fill(cptr.begin(), cptr.end() - 1);
-  for (int r = 0; r < kK; r++)
+  for (int r = 0; r < k; r++)
     for (uint32_t j = ptr[r]; j < ptr[r + 1]; j++) crow[fill[col[j]]++] = (uint16_t)r;
 }
 
@@ -473,12 +474,86 @@ Statement build() {
   return s;
 }
 
+const uint32_t kShaRc[64] = {
+    0x428a2f98, 0x71374491, 0xb5c0fbcf, 0xe9b5dba5, 0x3956c25b, 0x59f111f1, 0x923f82a4, 0xab1c5ed5,
+    0xd807aa98, 0x12835b01, 0x243185be, 0x550c7dc3, 0x72be5d74, 0x80deb1fe, 0x9bdc06a7, 0xc19bf174,
+    0xe49b69c1, 0xefbe4786, 0x0fc19dc6, 0x240ca1cc, 0x2de92c6f, 0x4a7484aa, 0x5cb0a9dc, 0x76f988da,
+    0x983e5152, 0xa831c66d, 0xb00327c8, 0xbf597fc7, 0xc6e00bf3, 0xd5a79147, 0x06ca6351, 0x14292967,
+    0x27b70a85, 0x2e1b2138, 0x4d2c6dfc, 0x53380d13, 0x650a7354, 0x766a0abb, 0x81c2c92e, 0x92722c85,
+    0xa2bfe8a1, 0xa81a664b, 0xc24b8b70, 0xc76c51a3, 0xd192e819, 0xd6990624, 0xf40e3585, 0x106aa070,
+    0x19a4c116, 0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a, 0x5b9cca4f, 0x682e6ff3,
+    0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7, 0xc67178f2};
+
+// SHA-256 compression (r1cs_hashes/sha2.rs:332-520): one 32-bit ADD of
+// x + y is 31 carry rows (x_i ^ cin_i)(y_i ^ cin_i) at cb..cb+30 (the `add`
+// above), its sum inlined into the consumer or materialised as 32 rows
+// (sum bits) * 1; Ch and Maj are one AND row per bit, e (f ^ g) and
+// (a ^ b)(a ^ c).  Layout: H_in 0, H_out 256, M 512, ch 1024, maj 3072,
+// round carries 5120 (7 adds x 31 per round), W[16..63] 19008, schedule
+// carries 20544 (3 x 31 per word), T1 25008, E_NEW 27056, A_NEW 29104,
+// output carries 31152, constant 31400.
+Statement build_sha256() {
+  constexpr int HB = 0, HOUT = 256, MB = 512, CH = 1024, MAJ = 3072, RC = 5120, WB = 19008, SC = 20544,
+                T1 = 25008, EN = 27056, AN = 29104, OC = 31152;
+  const int K = 1 << kShaKLog;
+  std::vector<Set> A(K), B(K);
+  const Set one = {(uint16_t)kShaZConst};
+  A[kShaZConst] = one;
+  B[kShaZConst] = one;
+  for (int j = 0; j < 256; j++) { A[HB + j] = {(uint16_t)(HB + j)}; B[HB + j] = one; }
+  for (int j = 0; j < 512; j++) { A[MB + j] = {(uint16_t)(MB + j)}; B[MB + j] = one; }
+  auto shr = [](const SymWord& x, int n) { SymWord w; for (int i = 0; i + n < 32; i++) w.b[i] = x.b[i + n]; return w; };
+  auto mat = [&](const SymWord& raw, int base) {
+    for (int i = 0; i < 32; i++) { A[base + i] = raw.b[i]; B[base + i] = one; }
+    return SymWord::slots(base);
+  };
+  std::array<SymWord, 64> W;
+  for (int t = 0; t < 16; t++) W[t] = SymWord::slots(MB + 32 * t);
+  for (int t = 16; t < 64; t++) {
+    const SymWord s1 = W[t - 2].rotr(17) ^ W[t - 2].rotr(19) ^ shr(W[t - 2], 10);
+    const SymWord s0 = W[t - 15].rotr(7) ^ W[t - 15].rotr(18) ^ shr(W[t - 15], 3);
+    const int cb = SC + (t - 16) * 93;
+    W[t] = mat(add(A, B, add(A, B, add(A, B, s1, W[t - 7], cb), s0, cb + 31), W[t - 16], cb + 62), WB + 32 * (t - 16));
+  }
+  std::array<SymWord, 8> h_in, s;
+  for (int w = 0; w < 8; w++) s[w] = h_in[w] = SymWord::slots(HB + 32 * w);
+  for (int r = 0; r < 64; r++) {
+    for (int i = 0; i < 32; i++) {
+      A[CH + 32 * r + i] = s[4].b[i];
+      B[CH + 32 * r + i] = sdiff(s[5].b[i], s[6].b[i]);
+      A[MAJ + 32 * r + i] = sdiff(s[0].b[i], s[1].b[i]);
+      B[MAJ + 32 * r + i] = sdiff(s[0].b[i], s[2].b[i]);
+    }
+    const SymWord ch = SymWord::slots(CH + 32 * r) ^ s[6], maj = SymWord::slots(MAJ + 32 * r) ^ s[0];
+    const SymWord S1 = s[4].rotr(6) ^ s[4].rotr(11) ^ s[4].rotr(25);
+    const SymWord S0 = s[0].rotr(2) ^ s[0].rotr(13) ^ s[0].rotr(22);
+    const int cb = RC + 217 * r;
+    const SymWord t12 = add(A, B, add(A, B, add(A, B, s[7], S1, cb), ch, cb + 31), SymWord::konst(kShaRc[r], kShaZConst),
+                            cb + 62);
+    const SymWord t1 = mat(add(A, B, t12, W[r], cb + 93), T1 + 32 * r);
+    const SymWord t2 = add(A, B, S0, maj, cb + 124);
+    const SymWord e_new = mat(add(A, B, s[3], t1, cb + 155), EN + 32 * r);
+    const SymWord a_new = mat(add(A, B, t1, t2, cb + 186), AN + 32 * r);
+    s = {a_new, s[0], s[1], s[2], e_new, s[4], s[5], s[6]};
+  }
+  for (int w = 0; w < 8; w++) mat(add(A, B, s[w], h_in[w], OC + 31 * w), HOUT + 32 * w);
+  Statement st;
+  st.k_log = kShaKLog;
+  st.z_const = kShaZConst;
+  st.useful = kShaUseful;
+  to_csr(A, st.a_ptr, st.a_col);
+  to_csr(B, st.b_ptr, st.b_col);
+  to_csc(st.a_ptr, st.a_col, st.at_ptr, st.at_row);
+  to_csc(st.b_ptr, st.b_col, st.bt_ptr, st.bt_row);
+  return st;
+}
+
 void put_u64(B3& h, uint64_t v) { uint8_t b[8]; le64(v, b); h.update(b, 8); }
-void put_matrix(B3& h, const std::vector<uint32_t>* ptr, const std::vector<uint16_t>* col) {
-  put_u64(h, kK);
-  put_u64(h, kK);
+void put_matrix(B3& h, int kk, const std::vector<uint32_t>* ptr, const std::vector<uint16_t>* col) {
+  put_u64(h, kk);
+  put_u64(h, kk);
   std::vector<uint8_t> buf;
-  for (int r = 0; r < kK; r++) {
+  for (int r = 0; r < kk; r++) {
     uint32_t s = ptr ? (*ptr)[r] : (uint32_t)r, e = ptr ? (*ptr)[r + 1] : (uint32_t)r + 1;
     buf.assign(8 * (e - s + 1), 0);
     le64(e - s, buf.data());
@@ -488,33 +563,55 @@ void put_matrix(B3& h, const std::vector<uint32_t>* ptr, const std::vector<uint1
 }
 }  // namespace
 
-const Statement& blake3_statement() {
-  static std::once_flag once;
-  static std::unique_ptr<Statement> s;
-  std::call_once(once, [] { s.reset(new Statement(build())); });
-  return *s;
+void sha256_compress(const uint32_t h_in[8], const uint32_t m[16], uint32_t out[8]) {
+  auto rr = [](uint32_t x, int n) { return (x >> n) | (x << (32 - n)); };
+  uint32_t w[64];
+  for (int t = 0; t < 16; t++) w[t] = m[t];
+  for (int t = 16; t < 64; t++)
+    w[t] = (rr(w[t - 2], 17) ^ rr(w[t - 2], 19) ^ (w[t - 2] >> 10)) + w[t - 7] +
+           (rr(w[t - 15], 7) ^ rr(w[t - 15], 18) ^ (w[t - 15] >> 3)) + w[t - 16];
+  uint32_t s[8];
+  for (int i = 0; i < 8; i++) s[i] = h_in[i];
+  for (int r = 0; r < 64; r++) {
+    const uint32_t e = s[4], a = s[0];
+    const uint32_t t1 = s[7] + (rr(e, 6) ^ rr(e, 11) ^ rr(e, 25)) + ((e & (s[5] ^ s[6])) ^ s[6]) + kShaRc[r] + w[r];
+    const uint32_t t2 = (rr(a, 2) ^ rr(a, 13) ^ rr(a, 22)) + (((a ^ s[1]) & (a ^ s[2])) ^ a);
+    for (int i = 7; i > 0; i--) s[i] = s[i - 1];
+    s[4] += t1;
+    s[0] = t1 + t2;
+  }
+  for (int i = 0; i < 8; i++) out[i] = h_in[i] + s[i];
 }
 
-std::array<uint8_t, 32> statement_digest(int m) {
+const Statement& statement(int hash) {
+  static std::once_flag once[2];
+  static std::unique_ptr<Statement> s[2];
+  const int k = hash == kHashSha256 ? 1 : 0;
+  std::call_once(once[k], [k] { s[k].reset(new Statement(k ? build_sha256() : build())); });
+  return *s[k];
+}
+
+std::array<uint8_t, 32> statement_digest(int hash, int m) {
   static std::mutex mu;
-  static std::map<int, std::array<uint8_t, 32>> cache;
+  static std::map<std::pair<int, int>, std::array<uint8_t, 32>> cache;
   std::lock_guard<std::mutex> lk(mu);
-  auto it = cache.find(m);
+  auto it = cache.find({hash, m});
   if (it != cache.end()) return it->second;
-  const Statement& st = blake3_statement();
+  const Statement& st = statement(hash);
+  const int kk = 1 << st.k_log;
   B3 h;
   h.update("flock-r1cs-stmt-v1", 18);
   put_u64(h, (uint64_t)m);
-  put_u64(h, kKLog);
+  put_u64(h, (uint64_t)st.k_log);
   put_u64(h, kKSkip);
   uint8_t row_major = 0;
   h.update(&row_major, 1);
-  put_matrix(h, &st.a_ptr, &st.a_col);
-  put_matrix(h, &st.b_ptr, &st.b_col);
-  put_matrix(h, nullptr, nullptr);  // C = I
+  put_matrix(h, kk, &st.a_ptr, &st.a_col);
+  put_matrix(h, kk, &st.b_ptr, &st.b_col);
+  put_matrix(h, kk, nullptr, nullptr);  // C = I
   std::array<uint8_t, 32> d;
   h.digest(d.data());
-  cache[m] = d;
+  cache[{hash, m}] = d;
   return d;
 }
 
@@ -612,12 +709,17 @@ struct Enc {
 std::vector<uint8_t> encode(const Proof& p) {
   Enc e;
   e.o.reserve(512 * 1024);
-  for (char c : std::string("FLOCK")) e.o.push_back((uint8_t)c);
-  e.o.push_back(4);
   // R1csProofBundleLigerito (flavor 2) or ChainProofBundleLigerito (flavor 3:
   // hash_kind first, the shift proof after the lincheck, the endpoints last;
-  // proof_io.rs:144-157, chain_common.rs:247-253)
-  e.o.push_back(p.chain ? 3 : 2);
+  // proof_io.rs:144-157, chain_common.rs:247-253).  A Merkle-path proof has
+  // no bundle type in the reference: its bytes are bincode of (Commitment,
+  // MerklePathProofLigerito { zerocheck, lincheck, shift, pcs_open }), as the
+  // reference's tests serialise them (r1cs_hashes/sha2.rs:2519-2526).
+  if (!p.merkle) {
+    for (char c : std::string("FLOCK")) e.o.push_back((uint8_t)c);
+    e.o.push_back(4);
+    e.o.push_back(p.chain ? 3 : 2);
+  }
   if (p.chain) e.u32(0);  // HashKind::Blake3
   e.h(p.root);
   e.u64(p.m);
@@ -635,6 +737,12 @@ std::vector<uint8_t> encode(const Proof& p) {
   e.fs(p.z_partial);
   if (p.chain) {
     e.pairs(p.shift_rounds);
+    e.f(p.g_at_point);
+  }
+  if (p.merkle) {
+    e.u64(p.mp_rounds.size());
+    for (const auto& q : p.mp_rounds)
+      for (const f128& v : q) e.f(v);
     e.f(p.g_at_point);
   }
   e.u64(p.s_hat_v.size());

@@ -81,16 +81,28 @@ size_t ceil_log2(size_t n);
 std::vector<f128> small_consts();
 std::vector<f128> medium_consts();
 
-// ---- R1CS statement for 2^n_log BLAKE3 compressions ----
+// ---- R1CS statements: one compression per 2^k_log-bit block ----
+// The hash a statement encodes.  BLAKE3 (r1cs_hashes/blake3.rs): 2^14-bit
+// blocks, constant wire at bit 512.  SHA-256 (r1cs_hashes/sha2.rs): 2^15-bit
+// blocks, constant wire at bit 31400.
+enum HashKind : int { kHashBlake3 = 0, kHashSha256 = 1 };
 constexpr int kKLog = 14, kK = 1 << kKLog, kKSkip = 6, kZConst = 512, kUseful = 15409;
+constexpr int kShaKLog = 15, kShaZConst = 31400, kShaUseful = 31401;
 struct Statement {
+  int k_log = kKLog, z_const = kZConst, useful = kUseful;
   std::vector<uint32_t> a_ptr, b_ptr;    // CSR rows
   std::vector<uint16_t> a_col, b_col;
   std::vector<uint32_t> at_ptr, bt_ptr;  // CSC (column -> rows)
   std::vector<uint16_t> at_row, bt_row;
 };
-const Statement& blake3_statement();     // matrices (built once per process)
-std::array<uint8_t, 32> statement_digest(int m);
+const Statement& statement(int hash);    // matrices (built once per process)
+inline const Statement& blake3_statement() { return statement(kHashBlake3); }
+std::array<uint8_t, 32> statement_digest(int hash, int m);
+inline std::array<uint8_t, 32> statement_digest(int m) { return statement_digest(kHashBlake3, m); }
+// sha256_compress (r1cs_hashes/sha2.rs:1502-1546): out = h_in + rounds(h_in, m)
+void sha256_compress(const uint32_t h_in[8], const uint32_t m[16], uint32_t out[8]);
+// block size of a hash's statement (log2 bits)
+inline int hash_k_log(int hash) { return hash == kHashSha256 ? kShaKLog : kKLog; }
 
 // ---- Ligerito fast ladder (configs/ligerito/m*_fast.toml) ----
 struct Ladder {
@@ -125,6 +137,11 @@ struct Proof {
   std::vector<std::pair<f128, f128>> shift_rounds;
   f128 g_at_point{};
   uint32_t cv0[8] = {}, cv_last[8] = {};
+  // SHA-256 Merkle-path proof: the shift sumcheck's (q(1), q(w), q(w+1))
+  // rounds (g_at_point above); encoded as bincode of (Commitment,
+  // MerklePathProofLigerito), without a FLOCK header
+  bool merkle = false;
+  std::vector<std::array<f128, 3>> mp_rounds;
 };
 std::vector<uint8_t> encode(const Proof& p);
 

@@ -11,7 +11,6 @@
 #include "gf128.cuh"
 #include "blake3.cuh"
 
-constexpr int kK_ = 16384;  // bits per compression block (2^14)
 
 // Number of this library's kernel launches issued by this process (reported
 // by the benchmark; every launch wrapper adds its launches here).
@@ -54,6 +53,33 @@ struct DeviceScope {
   DeviceScope& operator=(const DeviceScope&) = delete;
 };
 
+// XOR-reduce v over the CTA and add the sum into *out (atomically): every
+// thread of the CTA must call it.
+__device__ __forceinline__ void block_xor_out(f128 v, f128* out) {
+  __shared__ f128 red[32];
+  v = warp_xor(v);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int nw = (blockDim.x + 31) >> 5;
+    f128 x = l < nw ? red[l] : mk(0, 0);
+    x = warp_xor(x);
+    if (l == 0) atomic_xor128(out, x);
+  }
+  __syncthreads();
+}
+
+// Merkle-path shift sumcheck (SHA-256 statement): the seven tables of a
+// y-round (ta, te, tb, gz, gxl, gxr, g_other) and the claim's eight word
+// coefficients
+struct MpTables {
+  f128* t[7];
+};
+struct MpCoeffs {
+  f128 c[8];
+};
+
 // K0
 void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
                          f128* b, cudaStream_t s);
@@ -61,6 +87,10 @@ void launch_witness_seed(uint64_t seed, uint32_t log2, uint32_t n_blocks, uint32
 // otherwise 25 (cv, m, counter_lo of the benchmark generator)
 void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a, f128* b,
                            cudaStream_t s, bool records = false);
+// SHA-256 compressions, 2^15-bit blocks: records of 24 u32 (h_in, m), or
+// records == nullptr for the benchmark generator from `seed`
+void launch_witness_sha(const uint32_t* records, uint64_t seed, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
+                        f128* b, cudaStream_t s);
 // K1
 // NTT pass plans: the passes (first layer l0, layer count R, 2^lgs lanes per
 // tile, threads per CTA) that cover layers layer_begin..log_d-1.
@@ -146,11 +176,13 @@ void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b
               size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int grid, cudaStream_t s,
               f128* halve_out = nullptr, size_t halve_n = 0);
 void fold_pair_final(const f128* a_in, const f128* b_in, f128 rho, f128* out, cudaStream_t s);
+// k: columns of the block matrices (2^k_log)
 void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
-             const f128* eq, f128 alpha, f128 beta, int pin, f128* comb, cudaStream_t s);
-void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, f128* zv, cudaStream_t s);
+             const f128* eq, f128 alpha, f128 beta, int pin, int k, f128* comb, cudaStream_t s);
+void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, int k_log, f128* zv, cudaStream_t s);
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s);
-void ring_shat_ab(const f128* zv_pre, const f128* eqt, f128* out, cudaStream_t s);
+// s_hat_v of the ab claim from the block-folded z (2^k_log values)
+void ring_shat_ab(const f128* zv_pre, const f128* eqt, int k_log, f128* out, cudaStream_t s);
 void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, const f128* ehi1, const f128* L0,
                        const f128* L1, int lo_bits, size_t n_chunks, f128* out, int grid, cudaStream_t s);
 void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int grid, cudaStream_t s);
@@ -160,5 +192,12 @@ void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size
 // 2 n_inst values) and the packed-direct claim's scatter into b_combined
 void chain_fold(const f128* z, size_t n_inst, f128 e0, f128 e1, f128* g, cudaStream_t s);
 void chain_scatter(f128* bc, const f128* eq_inst, size_t n_inst, const f128 c[4], cudaStream_t s);
+// Merkle path (2^15-bit blocks): the four slot folds (out: 4 x n_inst), the
+// weight tables ta, tb, one y-round, and the claim's scatter into b_combined
+void mp_fold(const f128* z, size_t n_inst, f128 e0, f128 e1, f128* out, cudaStream_t s);
+void mp_tables(const f128* eq_q, const f128* eq_p, f128 alpha, int pos_log, size_t n, const uint8_t* b, f128* ta,
+               f128* tb, cudaStream_t s);
+void mp_round(const MpTables& T, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s);
+void mp_scatter(f128* bc, const f128* eq_inst, size_t n_inst, const MpCoeffs& c, cudaStream_t s);
 void sc3_round(const f128* a, const f128* b, const f128* e, f128* ao, f128* bo, const f128* rho, size_t n_pairs,
                f128* out, int grid, cudaStream_t s);

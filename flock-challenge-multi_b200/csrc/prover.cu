@@ -60,8 +60,8 @@ void pinned_give(void* p, size_t bytes) {
 }  // namespace
 
 // ---------------------------------------------------------------- setup --
-size_t Setup::estimate_bytes(uint32_t log2) {
-  const size_t n_words = (size_t)1 << (kKLog + std::max<int>(3, (int)log2) - 7);
+size_t Setup::estimate_bytes(uint32_t log2, int hash) {
+  const size_t n_words = (size_t)1 << (hash_k_log(hash) + std::max<int>(3, (int)log2) - 7);
   // z, a, b, 4 fold buffers, eq scratch, the rate-1/2 codeword (2x), its tree
   // (1/16 of a word per word), the Ligero levels and query basis (< 1/8),
   // blocks staging (25 u32 per compression) and chain records (28 u32),
@@ -69,15 +69,17 @@ size_t Setup::estimate_bytes(uint32_t log2) {
   return n_words * 16 * 10 + n_words * 2 + n_words * 2 + (n_words / 128) * 212 + ((size_t)96 << 20);
 }
 
-Setup::Setup(int device, uint32_t log2_, int stream_priority) : log2(log2_) {
+Setup::Setup(int device, uint32_t log2_, int stream_priority, int hash_) : log2(log2_), hash(hash_) {
   CK(cudaSetDevice(device));
   const size_t bytes0 = t_alloc_bytes;
+  if (hash != kHashBlake3 && hash != kHashSha256) throw std::runtime_error("unknown statement hash");
+  k_log = hash_k_log(hash);
   n_log = std::max<int>(3, (int)log2);
-  m = kKLog + n_log;
+  m = k_log + n_log;
   lad = ladder_for(m);
   if (!lad) throw std::runtime_error("no Ligerito configuration for this size (m = " + std::to_string(m) + ")");
   n_words = (size_t)1 << (m - 7);
-  digest = statement_digest(m);
+  digest = statement_digest(hash, m);
   CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, stream_priority));
   z = dalloc<f128>(n_words, st);
   a = dalloc<f128>(n_words, st);
@@ -106,10 +108,11 @@ Setup::Setup(int device, uint32_t log2_, int stream_priority) : log2(log2_) {
   lag = dalloc<f128>(8 * 256, st);
   elo = dalloc<f128>(1 << 13, st);
   ehi = dalloc<f128>(1 << 16, st);
-  comb = dalloc<f128>(kK, st);
-  zv = dalloc<f128>(kK, st);
-  zv_pre = dalloc<f128>(kK, st);
-  eq_inner = dalloc<f128>(kK, st);
+  const size_t kk = (size_t)1 << k_log;
+  comb = dalloc<f128>(kk, st);
+  zv = dalloc<f128>(kk, st);
+  zv_pre = dalloc<f128>(kk, st);
+  eq_inner = dalloc<f128>(kk, st);
   bc_tabs = dalloc<f128>(2 * 16 * 256, st);
   idx = dalloc<uint64_t>(1 << 16, st);
   gather = dalloc<f128>(1 << 16, st);
@@ -117,7 +120,7 @@ Setup::Setup(int device, uint32_t log2_, int stream_priority) : log2(log2_) {
   h_found = static_cast<unsigned long long*>(pinned_take(8));
   h_out = static_cast<f128*>(pinned_take(1024 * sizeof(f128)));
   h_stage = static_cast<uint8_t*>(pinned_take(kStageBytes));
-  const Statement& S = blake3_statement();
+  const Statement& S = statement(hash);
   at_ptr = dalloc<uint32_t>(S.at_ptr.size(), st);
   bt_ptr = dalloc<uint32_t>(S.bt_ptr.size(), st);
   at_row = dalloc<uint16_t>(S.at_row.size(), st);
@@ -444,7 +447,7 @@ void Setup::mark(int phase) {
 // synchronisation except where the transcript reads a device value.
 std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
                                   const std::string& domain, bool committed, const ChainEnds* chain,
-                                  bool full_records) {
+                                  bool full_records, const MerkleArgs* merkle) {
   Proof P;
   P.m = (uint64_t)m;
   pending_.clear();  // (left over only by a proof that threw)
@@ -453,7 +456,17 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   const int G = gs * 4;
   const uint32_t n_slots = 1u << n_log;
   mark(0);
-  if (!committed) {
+  if (hash != kHashBlake3 && (committed || chain))
+    throw std::runtime_error("batched commits and hash chains are BLAKE3 statements");
+  if (merkle && (hash != kHashSha256 || n_blocks != n_slots || !merkle->b_bits || merkle->path_log < 0 ||
+                 merkle->path_log > n_log))
+    throw std::runtime_error("a Merkle path is a SHA-256 statement whose paths fill every slot");
+  if (!committed && hash == kHashSha256) {
+    // ---- K0 witness of SHA-256 compressions
+    const uint32_t nb = n_blocks ? (uint32_t)n_blocks : 1u << log2;
+    launch_witness_sha(seed ? nullptr : blocks_dev, seed ? *seed : 0, nb, n_slots, z, a, b, st);
+    CK(cudaGetLastError());
+  } else if (!committed) {
     // ---- K0 witness
     if (seed) launch_witness_seed(*seed, log2, 1u << log2, n_slots, z, a, b, st);
     else launch_witness_blocks(blocks_dev, (uint32_t)n_blocks, n_slots, z, a, b, st, chain != nullptr || full_records);
@@ -701,7 +714,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   mark(5);
 
   // ---- lincheck
-  const int ir = kKLog - kKSkip;
+  const int ir = k_log - kKSkip;
+  const int kk = 1 << k_log;
   std::vector<f128> x_inner(rhos.begin(), rhos.begin() + ir), x_outer(rhos.begin() + ir, rhos.end());
   tr.label("flock-lincheck-v0");
   f128 alpha = tr.sample();
@@ -711,15 +725,15 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     std::vector<f128> L = hlagrange(zc_z, 0);
     eq_build(x_inner.data(), (int)x_inner.size(), hone(), zv_pre, st);
     outer64(L.data(), zv_pre, (size_t)1 << x_inner.size(), eq_inner, st);
-    lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, kZConst, comb, st);
+    lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, statement(hash).z_const, kk, comb, st);
     eq_table(x_outer, scratch_eq());
-    CK(cudaMemsetAsync(zv, 0, kK * sizeof(f128), st));
-    lc_zvec(z, scratch_eq(), (size_t)1 << (m - kKLog), zv, st);
+    CK(cudaMemsetAsync(zv, 0, kk * sizeof(f128), st));
+    lc_zvec(z, scratch_eq(), (size_t)1 << (m - k_log), k_log, zv, st);
     // pre-sumcheck z_vec: the ab-claim's ring-switch statistic is read from it
-    CK(cudaMemcpyAsync(zv_pre, zv, kK * sizeof(f128), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(zv_pre, zv, kk * sizeof(f128), cudaMemcpyDeviceToDevice, st));
   }
   std::vector<f128> rr;
-  int len = kK;
+  int len = kk;
   // the round kernel adds its message atomically into a fresh slot
   f128* lo_ = next_out(1);
   lc_round(comb, zv, len, false, mk(0, 0), true, lo_, st);
@@ -795,6 +809,88 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     for (int k = 1; k <= n_log; k++) pd_point[7 + (size_t)(n_log - k)] = rs[k];
   }
 
+  // ---- Merkle paths (merkle_path_common.rs:314-430): tau_pos folds each
+  // instance's four 256-bit slots (H_in, H_out = Z, M_lo = X_L, M_hi = X_R);
+  // the shift sumcheck (merkle_path.rs:226-467) runs n degree-3 rounds over
+  // seven tables on the device, binding the top instance variable, then two
+  // degree-2 rounds over the slot selector on the host; it leaves one
+  // packed-direct claim z(point) = g, point = [tau_pos, sel_slot, side, 0^5,
+  // instance].  pp[2] holds the slot folds, pp[3] the weight tables.
+  if (merkle) {
+    P.merkle = true;
+    const size_t N = n_slots;
+    const int n = n_log, pos_log = n_log - merkle->path_log;
+    const f128 tau_pos = tr.sample_vec(1)[0];
+    f128* sl = pp[2];  // [H_in | H_out | M_lo | M_hi], N each
+    f128 *ta = pp[3], *te = pp[3] + N, *tb = pp[3] + 2 * N, *eq_q = pp[3] + 3 * N, *eq_p = pp[3] + 4 * N;
+    uint8_t* bdev = reinterpret_cast<uint8_t*>(pp[3] + 5 * N);
+    mp_fold(z, N, fx(hone(), tau_pos), tau_pos, sl, st);
+    const std::vector<f128> tau = tr.sample_vec((size_t)n);
+    const f128 alpha = tr.sample();
+    const std::vector<f128> tq(tau.begin(), tau.begin() + pos_log), tp(tau.begin() + pos_log, tau.end());
+    const std::vector<f128> eqp = heq(tp);
+    eq_table(tau, te);
+    eq_table(tq, eq_q);
+    CK(cudaMemcpyAsync(eq_p, eqp.data(), eqp.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(bdev, merkle->b_bits, N, cudaMemcpyHostToDevice, st));
+    mp_tables(eq_q, eq_p, alpha, pos_log, N, bdev, ta, tb, st);
+    MpTables T{{ta, te, tb, sl + N, sl + 2 * N, sl + 3 * N, sl}};
+    int len = (int)N;
+    f128* so = next_out(1);
+    mp_round(T, len, false, mk(0, 0), true, so, st);
+    std::vector<f128> rs;
+    f128 last[7];
+    for (int k = 0; k < n; k++) {
+      // the last message is over the tables' two values; they fold here
+      if (k == n - 1)
+        for (int t = 0; t < 7; t++)
+          CK(cudaMemcpyAsync(h_out + 4 + 2 * t, T.t[t], 2 * sizeof(f128), cudaMemcpyDeviceToHost, st));
+      fetch(so, 3, h_out);
+      P.mp_rounds.push_back({h_out[0], h_out[1], h_out[2]});
+      for (int e = 0; e < 3; e++) tr.f128v(h_out[e]);
+      const f128 rk = tr.sample();
+      rs.push_back(rk);
+      if (k + 1 < n) {
+        len >>= 1;
+        so = next_out(1);
+        mp_round(T, len, true, rk, true, so, st);
+      } else {
+        for (int t = 0; t < 7; t++) {
+          const f128 lo = h_out[4 + 2 * t], hi = h_out[5 + 2 * t];
+          last[t] = fx(lo, hmul(rk, fx(hi, lo)));
+        }
+      }
+    }
+    // slot rounds (sd, then ss) over W, g indexed ss | sd << 1: slot 0 H_in
+    // (no weight), 1 Z, 2 X_L, 3 X_R
+    f128 w[4] = {mk(0, 0), last[1], hmul(last[0], fx(hone(), last[2])), hmul(last[0], last[2])};
+    f128 g[4] = {last[6], last[3], last[4], last[5]};
+    const f128 om = mk(2, 0), pts[3] = {hone(), om, fx(om, hone())};
+    for (int h = 2; h >= 1; h >>= 1) {
+      f128 sum[3] = {mk(0, 0), mk(0, 0), mk(0, 0)};
+      for (int e = 0; e < 3; e++)
+        for (int i = 0; i < h; i++) {
+          const f128 wx = fx(w[i], hmul(pts[e], fx(w[i + h], w[i])));
+          const f128 gx = fx(g[i], hmul(pts[e], fx(g[i + h], g[i])));
+          sum[e] = fx(sum[e], hmul(wx, gx));
+        }
+      P.mp_rounds.push_back({sum[0], sum[1], sum[2]});
+      for (int e = 0; e < 3; e++) tr.f128v(sum[e]);
+      const f128 rk = tr.sample();
+      rs.push_back(rk);
+      for (int i = 0; i < h; i++) {
+        w[i] = fx(w[i], hmul(rk, fx(w[i + h], w[i])));
+        g[i] = fx(g[i], hmul(rk, fx(g[i + h], g[i])));
+      }
+    }
+    P.g_at_point = pd_value = g[0];
+    pd_point.assign(8 + (size_t)n, mk(0, 0));
+    pd_point[0] = tau_pos;
+    pd_point[1] = rs[(size_t)n + 1];  // sel_slot
+    pd_point[2] = rs[(size_t)n];      // side
+    for (int j = 0; j < n; j++) pd_point[8 + j] = rs[(size_t)(n - 1 - j)];
+  }
+
   // ---- PCS open: ring switches + combine
   tr.label("flock-pcs-open-batch-v0");
   std::vector<f128> x_ab = r_inner_rest;
@@ -806,7 +902,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     std::vector<f128> eqt = heq(std::vector<f128>(r_inner_rest.begin() + 1, r_inner_rest.end()));
     CK(cudaMemcpyAsync(eq_inner, eqt.data(), eqt.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
     f128* ro = next_out(16);
-    ring_shat_ab(zv_pre, eq_inner, ro, st);
+    ring_shat_ab(zv_pre, eq_inner, k_log, ro, st);
     std::vector<f128> sv(128);
     fetch(ro, 128, sv.data());
     P.s_hat_v.push_back(sv);
@@ -834,7 +930,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   f128 target = fx(hmul(gam[0], claim[0]), hmul(gam[1], claim[1]));
   // the packed-direct claim after the ring-switched ones (pcs.rs:844-872)
   f128 gpd = mk(0, 0);
-  if (chain) {
+  if (chain || merkle) {
     tr.label("flock-pcs-packed-direct-v0");
     tr.f128v(pd_value);
     gpd = tr.sample();
@@ -881,6 +977,18 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     for (int wd = 0; wd < 4; wd++) c[wd] = hmul(gpd, hmul(ep[wd & 1], es[wd >> 1]));
     eq_table(std::vector<f128>(pd_point.begin() + 7, pd_point.end()), scratch_eq());
     chain_scatter(pp[1], scratch_eq(), n_slots, c, st);
+  }
+  if (merkle) {
+    // words w = 0..7 of block i get gpd eq(tau_pos, w & 1) eq(sel, w >> 1 & 1)
+    // eq(side, w >> 2) eq(instance, i)
+    MpCoeffs c;
+    for (int wd = 0; wd < 8; wd++) {
+      f128 v = gpd;
+      for (int j = 0; j < 3; j++) v = hmul(v, (wd >> j) & 1 ? pd_point[j] : fx(hone(), pd_point[j]));
+      c.c[wd] = v;
+    }
+    eq_table(std::vector<f128>(pd_point.begin() + 8, pd_point.end()), scratch_eq());
+    mp_scatter(pp[1], scratch_eq(), n_slots, c, st);
   }
   mark(7);
 

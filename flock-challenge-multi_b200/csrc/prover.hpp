@@ -27,6 +27,23 @@ BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vec
 void batch_commit_release(BatchCommit& h);
 void batch_commit(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds, cudaStream_t st);
 
+// A Merkle-path proof over a SHA-256 setup (prove_merkle_paths_ligerito,
+// r1cs_hashes/sha2.rs:1740-1783): 2^path_log paths of 2^(n_log - path_log)
+// hashes each, path-id major; b_bits (host, one byte per slot) selects which
+// half of each hash's message is the previous hash's output.
+struct MerkleArgs {
+  int path_log = 0;
+  const uint8_t* b_bits = nullptr;
+};
+// Its public inputs on the verifier side: the leaf of every path and the
+// shared root (8 u32 each) and the bit vector.
+struct MerklePublic {
+  int path_log = 0;
+  std::vector<uint8_t> b_bits;
+  std::vector<std::array<uint32_t, 8>> leaves;
+  std::array<uint32_t, 8> root{};
+};
+
 // Public endpoints of a hash chain: the input cv of the first compression and
 // the output cv (out_lo) of the last.
 struct ChainEnds {
@@ -37,7 +54,8 @@ struct ChainEnds {
 // lincheck's matrix combination alpha A^T eq + B^T eq (+ beta at the constant
 // column) for eq = L(z_skip) (x) eq(x_inner) (lincheck.rs:5940-5960).
 struct VerifyStatement {
-  int m = 0;
+  int m = 0, k_log = kKLog;
+  const MerklePublic* merkle = nullptr;  // a Merkle-path proof's public inputs
   std::array<uint8_t, 32> digest{};
   std::function<std::vector<f128>(f128 z_skip, const std::vector<f128>& x_inner, f128 alpha, f128 beta)> comb;
   // optional: BLAKE3 leaf chaining values of rows packed back to back, group
@@ -58,8 +76,10 @@ class Verifier {
   ~Verifier();
   Verifier(const Verifier&) = delete;
   Verifier& operator=(const Verifier&) = delete;
-  // "" when the bundle verifies, otherwise the name of the failed check
-  std::string verify(const uint8_t* bytes, size_t len, const std::string& domain);
+  // "" when the bundle verifies, otherwise the name of the failed check;
+  // hash: the statement the bundle is for (the R1CS bundle does not say)
+  std::string verify(const uint8_t* bytes, size_t len, const std::string& domain, int hash = kHashBlake3,
+                     const MerklePublic* merkle = nullptr);
 
  private:
   static constexpr size_t kRowsCap = (size_t)1 << 20, kCvsCap = (size_t)1 << 19;
@@ -82,8 +102,10 @@ class Setup {
   static constexpr int kPhases = 9;  // witness, RS encode, Merkle commit, round1, zc rounds, lincheck,
                                      // ring switch, L0 folds, levels
   // stream_priority: the CUDA priority of the setup's stream (0: default;
-  // lower numbers are served first when streams compete for the SMs)
-  Setup(int device, uint32_t log2, int stream_priority = 0);
+  // lower numbers are served first when streams compete for the SMs).
+  // hash: the statement (kHashBlake3: 2^log2 BLAKE3 compressions in 2^14-bit
+  // blocks; kHashSha256: SHA-256 compressions in 2^15-bit blocks).
+  Setup(int device, uint32_t log2, int stream_priority = 0, int hash = kHashBlake3);
   ~Setup();
   Setup(const Setup&) = delete;
   Setup& operator=(const Setup&) = delete;
@@ -97,23 +119,28 @@ class Setup {
   // full_records: blocks_dev holds n_blocks such 28-u32 records for a
   // compression proof; the slots from n_blocks on hold the all-zero
   // compression, as in the reference's padded prove_fast.
+  // A SHA-256 setup takes records of 24 u32 (h_in, m) in blocks_dev, or the
+  // benchmark generator's seed; its padding slots hold the compression of
+  // the all-zero (h_in, m) (Sha256HybridSetup::prove_fast, sha2.rs:1185-1209).
   std::vector<uint8_t> prove(const uint64_t* seed, const uint32_t* blocks_dev, size_t n_blocks,
                              const std::string& domain, bool committed = false, const ChainEnds* chain = nullptr,
-                             bool full_records = false);
+                             bool full_records = false, const MerkleArgs* merkle = nullptr);
   // Replays and checks a FLOCK v4 bundle of this statement size (compression
   // or hash chain; a chain's public endpoints are the bundle's); "" when it
   // verifies, otherwise the name of the failed check.  Uses this setup's
   // device statement and stream.
-  std::string verify(const uint8_t* bytes, size_t len, const std::string& domain);
+  std::string verify(const uint8_t* bytes, size_t len, const std::string& domain,
+                     const MerklePublic* merkle = nullptr);
   void phase_times(double* ms) const;
   // device bytes a setup for 2^log2 compressions holds (an upper estimate,
   // used for admission before allocating)
-  static size_t estimate_bytes(uint32_t log2);
+  static size_t estimate_bytes(uint32_t log2, int hash = kHashBlake3);
   size_t device_bytes = 0;  // allocated by the constructor
 
   friend BatchCommit batch_commit_async(const std::vector<Setup*>& setups, const std::vector<uint64_t>& seeds,
                                         cudaStream_t st);
   uint32_t log2 = 0;
+  int hash = kHashBlake3, k_log = kKLog;
   int n_log = 0, m = 0, sms = 0;
   // SMs the grid-stride kernels of this setup spread over (0: all).  The
   // serving queue lowers it for large proofs so that their long persistent

@@ -19,14 +19,19 @@
 
 // one CTA per output r, one thread per t; the 128 products are XOR-reduced
 // across the CTA (warp shuffles, then the four warp sums)
-__global__ void __launch_bounds__(128) k_shat_from_zvec(const f128* __restrict__ zv, const f128* __restrict__ eqt,
+// a thread per 128-bit word of the block (128 or 256 words), a CTA per bit r
+__global__ void __launch_bounds__(256) k_shat_from_zvec(const f128* __restrict__ zv, const f128* __restrict__ eqt,
                                                         f128* __restrict__ out) {
-  __shared__ f128 red[4];
+  __shared__ f128 red[8];
   const int r = blockIdx.x, t = threadIdx.x;
   f128 v = warp_xor(fmul(ldg(eqt + t), ldg(zv + 128 * t + r)));
   if ((t & 31) == 0) red[t >> 5] = v;
   __syncthreads();
-  if (t == 0) out[r] = fx(fx(red[0], red[1]), fx(red[2], red[3]));
+  if (t == 0) {
+    f128 s = mk(0, 0);
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s = fx(s, red[w]);
+    out[r] = s;
+  }
 }
 
 namespace {
@@ -65,9 +70,9 @@ __global__ void __launch_bounds__(512) k_bcombined_ct(const f128* __restrict__ e
   }
 }
 
-void ring_shat_ab(const f128* zv_pre, const f128* eqt, f128* out, cudaStream_t s) {
+void ring_shat_ab(const f128* zv_pre, const f128* eqt, int k_log, f128* out, cudaStream_t s) {
   count_launch();
-  k_shat_from_zvec<<<128, 128, 0, s>>>(zv_pre, eqt, out);
+  k_shat_from_zvec<<<128, 1 << (k_log - 7), 0, s>>>(zv_pre, eqt, out);
 }
 
 void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, const f128* ehi1, const f128* L0,

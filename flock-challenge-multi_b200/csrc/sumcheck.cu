@@ -29,20 +29,6 @@
 #include <algorithm>
 
 namespace {
-__device__ __forceinline__ void block_xor_out(f128 v, f128* out) {
-  __shared__ f128 red[32];
-  v = warp_xor(v);
-  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  if (w == 0) {
-    int nw = (blockDim.x + 31) >> 5;
-    f128 x = l < nw ? red[l] : mk(0, 0);
-    x = warp_xor(x);
-    if (l == 0) atomic_xor128(out, x);
-  }
-  __syncthreads();
-}
 }  // namespace
 
 // ------------------------------------------------------------------ K3 --
@@ -116,10 +102,10 @@ __global__ void __launch_bounds__(256) k_lc_comb(const uint32_t* __restrict__ at
                                                  const uint16_t* __restrict__ at_row,
                                                  const uint32_t* __restrict__ bt_ptr,
                                                  const uint16_t* __restrict__ bt_row, const f128* __restrict__ eq,
-                                                 f128 alpha, f128 beta, int pin, f128* __restrict__ comb) {
+                                                 f128 alpha, f128 beta, int pin, int k, f128* __restrict__ comb) {
   const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
-  if (c >= kK_) return;
+  if (c >= k) return;
   f128 sa = mk(0, 0), sb = mk(0, 0);
   for (uint32_t j = at_ptr[c] + lane; j < at_ptr[c + 1]; j += 32) sa = fx(sa, ldg(eq + at_row[j]));
   for (uint32_t j = bt_ptr[c] + lane; j < bt_ptr[c + 1]; j += 32) sb = fx(sb, ldg(eq + bt_row[j]));
@@ -133,9 +119,10 @@ __global__ void __launch_bounds__(256) k_lc_comb(const uint32_t* __restrict__ at
 }
 
 // z_vec[i] = XOR over compressions o of eq(x_outer, o) where bit i of o's
-// 2^14-bit block is set (lincheck.rs:2423 partial_fold_packed_z_block_major).
-// A CTA owns 4096 bit positions (one quarter of the block) and a run of
-// compressions; a thread owns 16 positions (one u16 of each block).  For
+// 2^k_log-bit block is set (lincheck.rs:2423 partial_fold_packed_z_block_major).
+// A CTA owns 4096 bit positions (a quarter of a 2^14-bit block, an eighth of
+// a 2^15-bit one) and a run of compressions; a thread owns 16 positions (one
+// u16 of each block).  For
 // every 8 compressions the CTA builds the 256 subset sums of their eq
 // weights; a thread transposes its 8 u16 words into 16 bytes (bit k of byte
 // p = bit p of compression k) and XORs in one table entry per position.
@@ -155,9 +142,9 @@ __device__ __forceinline__ uint64_t transpose8x8(uint64_t x) {
 }  // namespace
 
 __global__ void __launch_bounds__(256) k_lc_zvec(const uint16_t* __restrict__ z, const f128* __restrict__ eqo,
-                                                 size_t n_outer, int chunk, f128* __restrict__ zv) {
+                                                 size_t n_outer, int chunk, int bw, f128* __restrict__ zv) {
   __shared__ __align__(16) f128 T[kZvGroups][256];
-  const int col = blockIdx.x;  // quarter of the 2^14-bit block
+  const int col = blockIdx.x;  // 4096-bit column of the block (bw u16 per block)
   const int t = threadIdx.x;
   const size_t o0 = (size_t)blockIdx.y * chunk;
   const size_t o1 = o0 + chunk < n_outer ? o0 + chunk : n_outer;
@@ -181,7 +168,7 @@ __global__ void __launch_bounds__(256) k_lc_zvec(const uint16_t* __restrict__ z,
     // the next group's words are loaded while the current one is folded in
     uint32_t r[8], rn[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) r[k] = ob + k < o1 ? z[(ob + k) * 1024 + col * 256 + t] : 0u;
+    for (int k = 0; k < 8; k++) r[k] = ob + k < o1 ? z[(ob + k) * bw + col * 256 + t] : 0u;
 #pragma unroll 1
     for (int g = 0; g < kZvGroups; g++) {
       const size_t og = ob + 8 * g;
@@ -189,7 +176,7 @@ __global__ void __launch_bounds__(256) k_lc_zvec(const uint16_t* __restrict__ z,
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         const size_t o = og + 8 + k;
-        rn[k] = (g + 1 < kZvGroups && o < o1) ? z[o * 1024 + col * 256 + t] : 0u;
+        rn[k] = (g + 1 < kZvGroups && o < o1) ? z[o * bw + col * 256 + t] : 0u;
       }
       const uint32_t t01 = __byte_perm(r[0], r[1], 0x5140), t23 = __byte_perm(r[2], r[3], 0x5140);
       const uint32_t t45 = __byte_perm(r[4], r[5], 0x5140), t67 = __byte_perm(r[6], r[7], 0x5140);
@@ -246,13 +233,15 @@ __global__ void __launch_bounds__(256) k_lc_round(f128* comb, f128* zv, int len,
 }
 
 void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
-             const f128* eq, f128 alpha, f128 beta, int pin, f128* comb, cudaStream_t s) {
-  count_launch(); k_lc_comb<<<kK_ * 32 / 256, 256, 0, s>>>(at_ptr, at_row, bt_ptr, bt_row, eq, alpha, beta, pin, comb);
+             const f128* eq, f128 alpha, f128 beta, int pin, int k, f128* comb, cudaStream_t s) {
+  count_launch();
+  k_lc_comb<<<k * 32 / 256, 256, 0, s>>>(at_ptr, at_row, bt_ptr, bt_row, eq, alpha, beta, pin, k, comb);
 }
-void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, f128* zv, cudaStream_t s) {
+void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, int k_log, f128* zv, cudaStream_t s) {
   const int chunk = 1024;  // compressions per CTA (a multiple of 64)
-  dim3 grid(4, (unsigned)((n_outer + chunk - 1) / chunk));
-  count_launch(); k_lc_zvec<<<grid, 256, 0, s>>>((const uint16_t*)z, eqo, n_outer, chunk, zv);
+  dim3 grid(1u << (k_log - 12), (unsigned)((n_outer + chunk - 1) / chunk));
+  count_launch();
+  k_lc_zvec<<<grid, 256, 0, s>>>((const uint16_t*)z, eqo, n_outer, chunk, 1 << (k_log - 4), zv);
 }
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s) {
   const int threads = std::max(1, len / 2);

@@ -108,13 +108,17 @@ struct Rd {
 
 // FLOCK v4 R1csProofBundleLigerito (flavor 2) or ChainProofBundleLigerito
 // (flavor 3), the inverse of encode()
-bool decode(const uint8_t* bytes, size_t n, Proof& P, std::string& why) {
+// merkle: the header-less bincode of (Commitment, MerklePathProofLigerito)
+bool decode(const uint8_t* bytes, size_t n, Proof& P, std::string& why, bool merkle = false) {
   Rd r{bytes, n};
-  if (n < 7 || memcmp(bytes, "FLOCK", 5) != 0) return why = "bad magic", false;
-  if (bytes[5] != 4) return why = "unsupported version", false;
-  if (bytes[6] != 2 && bytes[6] != 3) return why = "unknown flavor", false;
-  r.i = 7;
-  P.chain = bytes[6] == 3;
+  if (!merkle) {
+    if (n < 7 || memcmp(bytes, "FLOCK", 5) != 0) return why = "bad magic", false;
+    if (bytes[5] != 4) return why = "unsupported version", false;
+    if (bytes[6] != 2 && bytes[6] != 3) return why = "unknown flavor", false;
+    r.i = 7;
+  }
+  P.merkle = merkle;
+  P.chain = !merkle && bytes[6] == 3;
   if (P.chain && r.u32() != 0) return why = "hash kind is not BLAKE3", false;
   P.root = r.h();
   P.m = r.u64();
@@ -130,6 +134,12 @@ bool decode(const uint8_t* bytes, size_t n, Proof& P, std::string& why) {
   P.z_partial = r.fs();
   if (P.chain) {
     P.shift_rounds = r.pairs();
+    P.g_at_point = r.f();
+  }
+  if (P.merkle) {
+    P.mp_rounds.resize(r.len(48));
+    for (auto& q : P.mp_rounds)
+      for (f128& v : q) v = r.f();
     P.g_at_point = r.f();
   }
   P.s_hat_v.resize(r.len(8));
@@ -490,8 +500,8 @@ struct RsClaim {
 std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& domain, const VerifyStatement& V) {
   Proof P;
   std::string why;
-  if (!decode(bytes, len, P, why)) return "malformed bundle: " + why;
-  const int m = V.m, n_log = V.m - kKLog;
+  if (!decode(bytes, len, P, why, V.merkle != nullptr)) return "malformed bundle: " + why;
+  const int m = V.m, n_log = V.m - V.k_log;
   if (P.m != (uint64_t)m) return "bundle is for another statement size";
   const Ladder* lad = ladder_for(m);
   if (!lad) return "no Ligerito configuration for this size";
@@ -534,15 +544,15 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
   tr.f128v(P.fb);
 
   // ---- lincheck: comb = alpha A^T eq + B^T eq (+ beta at the constant
-  // column) over the block's 2^14 columns, built on the device
-  const int ir = kKLog - kKSkip;
+  // column) over the block's 2^k_log columns, built on the device
+  const int ir = V.k_log - kKSkip;
   if (P.lc_rounds.size() != (size_t)ir || P.z_partial.size() != 64) return "lincheck: malformed";
   std::vector<f128> x_inner(rhos.begin(), rhos.begin() + ir), x_outer(rhos.begin() + ir, rhos.end());
   tr.label("flock-lincheck-v0");
   const f128 alpha = tr.sample();
   const f128 beta = tr.sample();
   std::vector<f128> cv = V.comb(zz, x_inner, alpha, beta);
-  if (cv.size() != (size_t)kK) return "lincheck: matrix combination";
+  if (cv.size() != (size_t)1 << V.k_log) return "lincheck: matrix combination";
   run = fx(fx(hmul(alpha, P.fa), P.fb), beta);
   std::vector<f128> rr;
   for (const auto& rd : P.lc_rounds) {
@@ -604,6 +614,65 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
     for (size_t i = 0; i < n; i++) pd_point[7 + i] = taup[i];
   }
 
+  // ---- Merkle paths: tau_pos, the shift sumcheck from the public leaves
+  // and root (merkle_path.rs:469-590, merkle_path_common.rs:459-537)
+  if (V.merkle) {
+    const MerklePublic& M = *V.merkle;
+    const f128 tp = tr.sample_vec(1)[0];
+    const size_t n = (size_t)n_log;
+    if (M.path_log < 0 || (size_t)M.path_log > n || M.b_bits.size() != ((size_t)1 << n) ||
+        M.leaves.size() != ((size_t)1 << M.path_log))
+      return "merkle: public inputs do not match the statement size";
+    if (P.mp_rounds.size() != n + 2) return "merkle: malformed shift proof";
+    const size_t pos_log = n - (size_t)M.path_log;
+    const std::vector<f128> tau = tr.sample_vec(n);
+    const f128 al = tr.sample();
+    const std::vector<f128> tq(tau.begin(), tau.begin() + (long)pos_log), tpp(tau.begin() + (long)pos_log, tau.end());
+    f128 ones = hone();
+    for (f128 t : tq) ones = hmul(ones, t);
+    const std::vector<f128> eqp = heq(tpp);
+    f128 leaf = mk(0, 0);
+    for (size_t i = 0; i < eqp.size(); i++) leaf = fx(leaf, hmul(eqp[i], fold_cv(M.leaves[i].data(), tp)));
+    f128 claim = fx(hmul(ones, fold_cv(M.root.data(), tp)), hmul(al, leaf));
+    // Lagrange over {0, 1, w, w + 1}, w = x
+    const f128 om = mk(2, 0), om1 = fx(om, hone());
+    const f128 d0 = hinv(hmul(om, om1)), d1 = hinv(hmul(om1, om));
+    std::vector<f128> rs;
+    for (const auto& q : P.mp_rounds) {
+      for (const f128& v : q) tr.f128v(v);
+      const f128 rk = tr.sample();
+      const f128 q0 = fx(claim, q[0]);
+      const f128 a = fx(rk, hone()), b = fx(rk, om), c = fx(rk, om1);
+      claim = fx(fx(hmul(hmul(hmul(a, b), c), hmul(q0, d0)), hmul(hmul(hmul(rk, b), c), hmul(q[0], d1))),
+                 fx(hmul(hmul(hmul(rk, a), c), hmul(q[1], d0)), hmul(hmul(hmul(rk, a), b), hmul(q[2], d1))));
+      rs.push_back(rk);
+    }
+    std::vector<f128> ipt(n);
+    for (size_t j = 0; j < n; j++) ipt[j] = rs[n - 1 - j];
+    const f128 side = rs[n], sel = rs[n + 1];
+    const std::vector<f128> yq(ipt.begin(), ipt.begin() + (long)pos_log), yp(ipt.begin() + (long)pos_log, ipt.end());
+    f128 z0 = hone();
+    for (f128 t : yq) z0 = hmul(z0, fx(hone(), t));
+    const f128 tsa = hmul(eq_eval(tpp.data(), yp.data(), yp.size()), fx(shift_mle(tq, yq), hmul(al, z0)));
+    const f128 teq = eq_eval(tau.data(), ipt.data(), n);
+    const std::vector<f128> eqi = heq(ipt);
+    f128 tb = mk(0, 0);
+    const size_t mask = ((size_t)1 << pos_log) - 1;
+    for (size_t i = 0; i < M.b_bits.size(); i++)
+      if (M.b_bits[i] && (i & mask) != 0) tb = fx(tb, eqi[i]);
+    // slot indicator of s = ss | sd << 1: Z = 1, X_L = 2, X_R = 3
+    auto ind = [&](int s) {
+      return hmul((s & 1) ? sel : fx(hone(), sel), (s >> 1) ? side : fx(hone(), side));
+    };
+    const f128 wf = fx(hmul(ind(1), teq), fx(hmul(hmul(ind(2), tsa), fx(hone(), tb)), hmul(hmul(ind(3), tsa), tb)));
+    if (!feq(claim, hmul(wf, P.g_at_point))) return "merkle: shift sumcheck";
+    pd_point.assign(8 + n, mk(0, 0));
+    pd_point[0] = tp;
+    pd_point[1] = sel;
+    pd_point[2] = side;
+    for (size_t j = 0; j < n; j++) pd_point[8 + j] = ipt[j];
+  }
+
   // ---- batched open: ring switches, the packed-direct claim, the target
   if (P.s_hat_v.size() != 2) return "open: expected two ring-switched claims";
   tr.label("flock-pcs-open-batch-v0");
@@ -629,7 +698,7 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
   const f128 gam[2] = {tr.sample(), tr.sample()};
   f128 target = fx(hmul(gam[0], sc[0]), hmul(gam[1], sc[1]));
   f128 gpd = mk(0, 0);
-  if (P.chain) {
+  if (P.chain || P.merkle) {
     tr.label("flock-pcs-packed-direct-v0");
     tr.f128v(P.g_at_point);
     gpd = tr.sample();
@@ -774,7 +843,7 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
           comb_y[y] = fx(comb_y[y], hmul(gam[k], ta_fold_vertical(t, eqd[k])));
         }
       }
-      if (P.chain) {
+      if (P.chain || P.merkle) {
         const f128 pre = eq_eval(pd_point.data(), ris.data(), pl);
         for (size_t y = 0; y < yl; y++)
           comb_y[y] = fx(comb_y[y], hmul(hmul(gpd, pre), eq_binary(pd_point.data() + pl, (size_t)yr_log_n, y)));
@@ -825,18 +894,20 @@ struct VerifyBufs {
 };
 // the device half of the verifier over the CSC copy of the block matrices
 // given by at_*, bt_*: the matrix combination and the opened rows' leaves
-VerifyStatement device_statement(int m, const std::array<uint8_t, 32>& digest, const uint32_t* at_ptr,
+VerifyStatement device_statement(int m, int hash, const std::array<uint8_t, 32>& digest, const uint32_t* at_ptr,
                                  const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
                                  const VerifyBufs& B, cudaStream_t st) {
   VerifyStatement V;
   V.m = m;
+  V.k_log = hash_k_log(hash);
   V.digest = digest;
+  const int kk = 1 << V.k_log, pin = statement(hash).z_const;
   V.comb = [=](f128 zskip, const std::vector<f128>& x_inner, f128 alpha, f128 beta) {
-    std::vector<f128> L = hlagrange(zskip, 0), cv(kK);
+    std::vector<f128> L = hlagrange(zskip, 0), cv(kk);
     eq_build(x_inner.data(), (int)x_inner.size(), hone(), B.eqx, st);
     outer64(L.data(), B.eqx, (size_t)1 << x_inner.size(), B.eqi, st);
-    lc_comb(at_ptr, at_row, bt_ptr, bt_row, B.eqi, alpha, beta, kZConst, B.comb, st);
-    CK(cudaMemcpyAsync(cv.data(), B.comb, kK * sizeof(f128), cudaMemcpyDeviceToHost, st));
+    lc_comb(at_ptr, at_row, bt_ptr, bt_row, B.eqi, alpha, beta, pin, kk, B.comb, st);
+    CK(cudaMemcpyAsync(cv.data(), B.comb, kk * sizeof(f128), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return cv;
   };
@@ -861,19 +932,19 @@ VerifyStatement device_statement(int m, const std::array<uint8_t, 32>& digest, c
   return V;
 }
 
-// One device copy of the block matrices' CSC per device, shared by every
-// Verifier on it (they are the same for every statement size).
+// One device copy of each hash's block matrices (CSC) per device, shared by
+// every Verifier on it (they are the same for every statement size).
 struct DevCsc {
   uint32_t *at_ptr = nullptr, *bt_ptr = nullptr;
   uint16_t *at_row = nullptr, *bt_row = nullptr;
 };
-const DevCsc& shared_csc(int device) {
+const DevCsc& shared_csc(int device, int hash) {
   static std::mutex mu;
-  static std::map<int, DevCsc> m;
+  static std::map<std::pair<int, int>, DevCsc> m;
   std::lock_guard<std::mutex> lk(mu);
-  auto it = m.find(device);
+  auto it = m.find({device, hash});
   if (it != m.end()) return it->second;
-  const Statement& S = blake3_statement();
+  const Statement& S = statement(hash);
   DevCsc d;
   auto up = [](auto& dst, const auto& src) {
     CK(cudaMalloc(&dst, src.size() * sizeof(src[0])));
@@ -883,23 +954,26 @@ const DevCsc& shared_csc(int device) {
   up(d.bt_ptr, S.bt_ptr);
   up(d.at_row, S.at_row);
   up(d.bt_row, S.bt_row);
-  return m[device] = d;
+  return m[{device, hash}] = d;
 }
 }  // namespace
 
 // The setup's own buffers and stream (flock_verify: the caller owns the setup).
-std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& domain) {
+std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& domain, const MerklePublic* merkle) {
   VerifyBufs B{zv_pre, eq_inner, comb, reinterpret_cast<uint8_t*>(gather), reinterpret_cast<uint32_t*>(idx),
                ((size_t)1 << 16) * sizeof(f128), ((size_t)1 << 16) * sizeof(uint64_t)};
-  return verify_bundle(bytes, len, domain, device_statement(m, digest, at_ptr, at_row, bt_ptr, bt_row, B, st));
+  if (merkle && hash != kHashSha256) return "a Merkle path is a SHA-256 statement";
+  VerifyStatement V = device_statement(m, hash, digest, at_ptr, at_row, bt_ptr, bt_row, B, st);
+  V.merkle = merkle;
+  return verify_bundle(bytes, len, domain, V);
 }
 
 Verifier::Verifier(int device) : device_(device) {
   DeviceScope on(device);
   CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-  CK(cudaMalloc(&eqx_, 256 * sizeof(f128)));
-  CK(cudaMalloc(&eqi_, kK * sizeof(f128)));
-  CK(cudaMalloc(&comb_, kK * sizeof(f128)));
+  CK(cudaMalloc(&eqx_, ((size_t)1 << (kShaKLog - kKSkip)) * sizeof(f128)));  // eq(x_inner), 2^(k_log - 6)
+  CK(cudaMalloc(&eqi_, ((size_t)1 << kShaKLog) * sizeof(f128)));  // the larger block of the two hashes
+  CK(cudaMalloc(&comb_, ((size_t)1 << kShaKLog) * sizeof(f128)));
   CK(cudaMalloc(&rows_, kRowsCap));
   CK(cudaMalloc(&cvs_, kCvsCap));
 }
@@ -914,22 +988,29 @@ Verifier::~Verifier() {
   if (prev >= 0) cudaSetDevice(prev);
 }
 
-std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string& domain) {
+std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string& domain, int hash,
+                             const MerklePublic* merkle) {
   if (len < 7 + 4 + 32 + 8) return "malformed bundle: truncated";
+  if (merkle && hash != kHashSha256) return "a Merkle path is a SHA-256 statement";
   // the statement size is the bundle's m (after the header, the optional
-  // hash kind and the root); verify_bundle checks everything else
-  const size_t at = 7 + (bytes[6] == 3 ? 4 : 0) + 32;
+  // hash kind and the root; a Merkle-path proof has neither header nor hash
+  // kind); verify_bundle checks everything else
+  const size_t at = merkle ? 32 : 7 + (bytes[6] == 3 ? 4 : 0) + 32;
   uint64_t mm = 0;
   for (int k = 0; k < 8; k++) mm |= (uint64_t)bytes[at + k] << (8 * k);
-  if (mm < (uint64_t)kKLog + 8 || mm > (uint64_t)kKLog + 20) return "bundle is for an unsupported statement size";
+  if (hash != kHashBlake3 && hash != kHashSha256) return "unknown statement hash";
+  if (hash != kHashBlake3 && !merkle && bytes[6] != 2) return "hash chains are BLAKE3 statements";
+  // BLAKE3: 2^8..2^20 compressions; SHA-256: 2^7..2^19 (the same m range)
+  if (mm < 22 || mm > 34) return "bundle is for an unsupported statement size";
   // the stream and buffers belong to device_, whichever device the calling
   // thread has current; the caller's device is restored on return
   DeviceScope on(device_);
-  const DevCsc& C = shared_csc(device_);
+  const DevCsc& C = shared_csc(device_, hash);
   const VerifyBufs B{eqx_, eqi_, comb_, rows_, cvs_, kRowsCap, kCvsCap};
-  return verify_bundle(bytes, len, domain,
-                       device_statement((int)mm, statement_digest((int)mm), C.at_ptr, C.at_row, C.bt_ptr, C.bt_row,
-                                        B, st_));
+  VerifyStatement V = device_statement((int)mm, hash, statement_digest(hash, (int)mm), C.at_ptr, C.at_row, C.bt_ptr,
+                                       C.bt_row, B, st_);
+  V.merkle = merkle;
+  return verify_bundle(bytes, len, domain, V);
 }
 
 }  // namespace flock

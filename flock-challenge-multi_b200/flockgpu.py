@@ -35,7 +35,8 @@ EXPORTS = (
     "flock_challenger_observe_f128_slice", "flock_challenger_sample_f128", "flock_challenger_sample_f128_vec",
     "flock_challenger_grind_pow", "flock_challenger_verify_pow", "flock_challenger_state_digest",
     "flock_ntt_plan_desc", "flock_bench_ntt_plan", "flock_bench_f128_product", "flock_launch_count",
-    "flock_serve_prewarm",
+    "flock_serve_prewarm", "flock_sha256_setup_create", "flock_sha256_prove", "flock_sha256_verify_bundle",
+    "flock_sha256_compress", "flock_sha256_statement_digest", "flock_sha256_witness",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -117,6 +118,13 @@ def load() -> ctypes.CDLL:
         lib.flock_merkle_root_noalloc.argtypes = [vp, sz, sz, vp, vp]
         lib.flock_serve_start.argtypes = [vp, i32]
         lib.flock_serve_prewarm.argtypes = [vp, u32, i32, ctypes.POINTER(i32)]
+        lib.flock_sha256_setup_create.argtypes = [vp, sz, i32, i32, ctypes.POINTER(vp)]
+        lib.flock_sha256_prove.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        lib.flock_sha256_verify_bundle.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
+        lib.flock_sha256_compress.argtypes = [vp, vp, vp]
+        lib.flock_sha256_compress.restype = None
+        lib.flock_sha256_statement_digest.argtypes = [u32, vp]
+        lib.flock_sha256_witness.argtypes = [vp, vp, sz, u32, vp, vp, vp]
         lib.flock_submit.argtypes = [vp, ctypes.POINTER(FlockJob), ctypes.POINTER(u64)]
         lib.flock_poll.argtypes = [vp, u64, ctypes.POINTER(FlockResult), i32]
         lib.flock_host_alloc.argtypes = [sz, ctypes.POINTER(vp)]
@@ -172,6 +180,42 @@ def generate_compressions(log2: int, seed: int) -> np.ndarray:
 
 
 CHAIN_DOMAIN = b"flock_chain-cli"
+
+
+def sha256_bench_inputs(n: int, seed: int) -> np.ndarray:
+    """The sha2_proof bench inputs on the host, (n, 24) u32: h[8], m[16]
+    (crates/flock-prover/benches/sha2_proof.rs:56-71): one SplitMix64 stream
+    from `seed`, draw j of compression i at state seed + (24 i + j + 1) gamma."""
+    g = np.uint64(0x9E3779B97F4A7C15)
+    idx = np.arange(24 * n, dtype=np.uint64) + np.uint64(1)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed & (2**64 - 1)) + idx * g
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z.astype(np.uint32).reshape(-1, 24)
+
+
+def sha256_bench_seed(n: int, run: int = 0) -> int:
+    """The seed sha2_proof.rs:112 gives run `run` of n compressions."""
+    return 0xC0FFEE_5A55 ^ n ^ run
+
+
+def sha256_compress(h, m) -> np.ndarray:
+    """sha256_compress (sha2.rs:1502-1546): h_in + rounds(h_in, m), 8 u32."""
+    h = np.ascontiguousarray(h, np.uint32)
+    m = np.ascontiguousarray(m, np.uint32)
+    out = np.zeros(8, np.uint32)
+    load().flock_sha256_compress(_ptr(h), _ptr(m), _ptr(out))
+    return out
+
+
+def sha256_statement_digest(m: int) -> bytes:
+    out = np.zeros(32, np.uint8)
+    rc = load().flock_sha256_statement_digest(m, _ptr(out))
+    if rc != 0:
+        raise FlockError(f"sha256_statement_digest: {rc}")
+    return out.tobytes()
 
 
 def chain_blocks(seed: int, steps: int, initial_cv=None) -> np.ndarray:
@@ -260,6 +304,26 @@ class Context:
             return self.lib.flock_last_error(self.h).decode()
         self._check(rc, "verify_bundle")
         return "error"
+
+    def sha256_verify(self, bundle: bytes, domain: bytes = DOMAIN) -> str:
+        """Sha256HybridSetup::verify for any supported size: '' when the
+        bundle verifies as a SHA-256 statement, otherwise the failed check."""
+        rc = self.lib.flock_sha256_verify_bundle(self.h, bundle, len(bundle), domain, len(domain))
+        if rc == 0:
+            return ""
+        if rc == FLOCK_ERR_VERIFY:
+            return self.lib.flock_last_error(self.h).decode()
+        self._check(rc, "sha256_verify_bundle")
+        return "error"
+
+    def sha256_witness(self, comps: np.ndarray, n_log: int):
+        """(z, a, b) packed row witness of (n, 24) u32 SHA-256 compressions
+        over 2^n_log blocks, each (2^n_log, 512) u64."""
+        comps = np.ascontiguousarray(comps, np.uint32).reshape(-1, 24)
+        z, a, b = (np.zeros((1 << n_log, 512), np.uint64) for _ in range(3))
+        self._check(self.lib.flock_sha256_witness(self.h, _ptr(comps), comps.shape[0], n_log, _ptr(z), _ptr(a),
+                                                  _ptr(b)), "sha256_witness")
+        return z, a, b
 
     def serve_verify(self, on: bool = True) -> None:
         """Self-check every served / batched proof with the verifier."""
@@ -521,6 +585,61 @@ class ProverData:
             self.close()
         except Exception:
             pass
+
+
+class Sha256Prover:
+    """`Sha256HybridSetup::new(n)` (crates/flock-prover/src/r1cs_hashes/
+    sha2.rs:1252-1330): SHA-256 compressions, one per 2^15-bit block,
+    2^max(3, ceil(log2 n)) slots, BLAKE3 Merkle hashing, fast profile."""
+
+    def __init__(self, ctx: Context, n: int):
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.flock_sha256_setup_create(ctx.h, n, 1, 0, ctypes.byref(h)), "sha256_setup_create")
+        self.ctx, self.n, self.h = ctx, n, h
+        self.n_log = max(3, (n - 1).bit_length())
+        self._buf = np.zeros(MAX_PROOF_BYTES * 2, np.uint8)
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.flock_setup_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def prove(self, comps: np.ndarray, domain: bytes = DOMAIN) -> bytes:
+        """prove_fast over (n, 24) u32 compressions (h_in[8], m[16])."""
+        comps = np.ascontiguousarray(comps, np.uint32).reshape(-1, 24)
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_sha256_prove(self.h, _ptr(comps), comps.shape[0], domain, len(domain),
+                                             _ptr(self._buf), self._buf.size, ctypes.byref(n))
+        self.ctx._check(rc, "sha256_prove")
+        return self._buf[: n.value].tobytes()
+
+    def prove_seed(self, seed: int, domain: bytes = DOMAIN) -> bytes:
+        """prove_fast over sha256_bench_inputs(n, seed), generated on the GPU."""
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_prove_seed(self.h, seed, domain, len(domain), _ptr(self._buf), self._buf.size,
+                                           ctypes.byref(n))
+        self.ctx._check(rc, "prove_seed")
+        return self._buf[: n.value].tobytes()
+
+    def verify(self, bundle: bytes, domain: bytes = DOMAIN) -> str:
+        rc = self.ctx.lib.flock_verify(self.h, bundle, len(bundle), domain, len(domain))
+        if rc == 0:
+            return ""
+        if rc == FLOCK_ERR_VERIFY:
+            return self.ctx.lib.flock_last_error(self.ctx.h).decode()
+        self.ctx._check(rc, "verify")
+        return "error"
+
+    def phase_ms(self) -> dict:
+        out = np.zeros(len(PHASES), np.float64)
+        k = self.ctx.lib.flock_setup_phase_ms(self.h, _ptr(out), len(PHASES))
+        return dict(zip(PHASES[:k], out[:k].tolist()))
 
 
 class Prover:

@@ -169,6 +169,69 @@ int flock_challenger_grind_pow(flock_challenger* ch, flock_ctx* ctx, uint32_t bi
 int flock_challenger_verify_pow(flock_challenger* ch, uint64_t nonce, uint32_t bits);
 int flock_challenger_state_digest(flock_challenger* ch, uint8_t* out32);
 
+/* ---- SHA-256 compressions (crates/flock-prover/src/r1cs_hashes/sha2.rs) ----
+ * The same prover (witness -> RS encode + Merkle commit -> zerocheck ->
+ * lincheck -> ring switch -> Ligerito) over the hybrid SHA-256 R1CS: one
+ * compression per 2^15-bit block (H_in, H_out, M, Ch/Maj AND rows, carry
+ * rows of every 32-bit ADD, materialised W[16..63], T1, E_NEW, A_NEW), the
+ * constant wire at bit 31400 pinned to 1 in every block. */
+/* One input, the reference's ([u32; 8], [u32; 16]) = (h_in, m) (sha2.rs:1377). */
+typedef struct flock_sha256_compression {
+  uint32_t h[8];
+  uint32_t m[16];
+} flock_sha256_compression;
+/* Sha256HybridSetup::new(n_compressions) (sha2.rs:1252-1330): the statement
+ * has 2^max(3, ceil(log2 n)) slots (min_n_blocks_log, sha2.rs:1217-1221).
+ * Supported: 65 <= n <= 2^19 (m = 15 + n_log in 22..34, the fast profile's
+ * Ligerito ladders).  hash / profile as for flock_setup_create.  The setup
+ * also serves flock_prove_seed (the sha2_proof bench generator:
+ * benches/sha2_proof.rs:56-71, one SplitMix64 stream from the seed, h then m
+ * per compression, n_compressions of them) and flock_verify. */
+int flock_sha256_setup_create(flock_ctx* ctx, size_t n_compressions, int hash, int profile, flock_setup** out);
+/* Sha256HybridSetup::prove_fast(&compressions, &mut FsChallenger) + to_bytes
+ * (sha2.rs:1377-1408): n must equal the setup's n_compressions; the slots
+ * from n on hold the compression of the all-zero (h_in, m) (sha2.rs:1195). */
+int flock_sha256_prove(flock_setup* s, const flock_sha256_compression* comps, size_t n, const uint8_t* domain,
+                       size_t dlen, uint8_t* out, size_t cap, size_t* out_len);
+/* Sha256HybridSetup::verify (sha2.rs:1441-1486) without a prover setup, for
+ * any supported size (read from the bundle); the context's verifier, as in
+ * flock_verify_bundle.  The R1CS bundle does not name its hash, so the
+ * statement is chosen by the entry point. */
+int flock_sha256_verify_bundle(flock_ctx* ctx, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen);
+/* Merkle paths over SHA-256 compressions: Sha256HybridSetup::
+ * prove_merkle_paths_ligerito (sha2.rs:1740-1783; path_log = 0 is
+ * prove_merkle_path_ligerito, :1662-1697).  2^path_log paths of
+ * 2^(n_log - path_log) hashes each fill the setup's n = 2^n_log slots, path-id
+ * major; b_bits[i] (one byte each) says which half of hash i's message is the
+ * previous hash's output (the first hash of every path takes its leaf in the
+ * left half whatever its bit).  The setup must hold a power of two.  Output:
+ * bincode of (Commitment, MerklePathProofLigerito) -- the reference has no
+ * FLOCK bundle type for this proof; its tests serialise the two this way
+ * (sha2.rs:2519-2526). */
+int flock_sha256_merkle_prove(flock_setup* s, const flock_sha256_compression* comps, size_t n, const uint8_t* b_bits,
+                              uint32_t path_log, const uint8_t* domain, size_t dlen, uint8_t* out, size_t cap,
+                              size_t* out_len);
+/* verify_merkle_paths_ligerito (sha2.rs:1785-1843): the public leaves (8 u32
+ * per path), the shared root and the n bits. */
+int flock_sha256_merkle_verify(flock_ctx* ctx, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen,
+                               uint32_t path_log, const uint8_t* b_bits, size_t n, const uint32_t* leaves,
+                               const uint32_t* root);
+/* Honest inputs (host): the path of benches/sha2_merkle_proof.rs:49-76
+ * (every H_in the SHA-256 IV; leaf, bits and siblings from one SplitMix64
+ * stream, low 32 bits) of 2^(n_log - path_log) hashes, repeated for each of
+ * the 2^path_log paths (sha2.rs:2475-2497).  comps: 2^n_log, b_bits: 2^n_log,
+ * leaves: 8 u32 per path, root: 8 u32. */
+int flock_sha256_merkle_inputs(uint32_t n_log, uint32_t path_log, uint64_t seed, flock_sha256_compression* comps,
+                               uint8_t* b_bits, uint32_t* leaves, uint32_t* root);
+/* sha256_compress (sha2.rs:1502-1546) on the host: out = h_in + rounds(h_in, m). */
+void flock_sha256_compress(const uint32_t* h_in, const uint32_t* m, uint32_t* out);
+/* BlockR1cs::statement_digest of the SHA-256 statement of size m. */
+int flock_sha256_statement_digest(uint32_t m, uint8_t* out32);
+/* Debug/test: the packed row witness z, a = A_0 z, b = B_0 z of n
+ * compressions over 2^n_log blocks (2^(n_log + 8) u64 pairs each). */
+int flock_sha256_witness(flock_ctx* ctx, const flock_sha256_compression* comps, size_t n, uint32_t n_log, uint64_t* z,
+                         uint64_t* a, uint64_t* b);
+
 /* The flock_chain CLI's honest chain of `steps` records: record i has
  * cv = x_i (x_0 = initial_cv, or the BLAKE3 IV when NULL), 16 message words
  * from SplitMix64(seed) (low 32 bits of each draw), counter 0, block_len 64,

@@ -223,6 +223,113 @@ uint64_t flockref_ch_grind(void* c, uint32_t bits) { return ((Challenger*)c)->gr
 void flockref_ch_digest(void* c, uint8_t* out32) { ((Challenger*)c)->state_digest(out32); }
 int flockref_pow_ok(const uint8_t* digest, uint64_t nonce, uint32_t bits) { return pow_ok(digest, nonce, bits); }
 
+// ---- SHA-256 compressions.  A record is 24 u32: h_in[8], m[16].
+static_assert(sizeof(sha::Compression) == 96, "sha-256 record");
+
+void flockref_sha256_compress(const uint32_t* h, const uint32_t* m, uint32_t* out8) { sha::compress(h, m, out8); }
+void flockref_sha256_bench_inputs(size_t n, uint64_t seed, uint32_t* out24) {
+  auto v = sha::bench_inputs(n, seed);
+  memcpy(out24, v.data(), v.size() * sizeof(sha::Compression));
+}
+int flockref_sha256_min_n_blocks_log(size_t n) { return sha::min_n_blocks_log(n); }
+void flockref_sha256_digest(uint32_t n_log, uint8_t* out32) {
+  memcpy(out32, sha256_r1cs((int)n_log).digest.data(), 32);
+}
+uint64_t flockref_sha256_matrix_nnz(int which) {
+  const R1cs& rc = sha256_r1cs(3);
+  return which == 0 ? rc.a0.col.size() : rc.b0.col.size();
+}
+// CSR export of A0 (which=0) / B0 (which=1): ptr[2^15 + 1], col[nnz]
+void flockref_sha256_matrix_csr(int which, uint32_t* ptr, uint16_t* col) {
+  const R1cs& rc = sha256_r1cs(3);
+  const SparseRows& s = which == 0 ? rc.a0 : rc.b0;
+  memcpy(ptr, s.ptr.data(), s.ptr.size() * 4);
+  memcpy(col, s.col.data(), s.col.size() * 2);
+}
+// z, a, b: 2^(15 + n_log - 7) F128 each, for n records over 2^n_log blocks
+void flockref_sha256_witness(const uint32_t* rec24, size_t n, uint32_t n_log, uint64_t* z, uint64_t* a,
+                             uint64_t* b) {
+  std::vector<sha::Compression> blocks(n);
+  memcpy(blocks.data(), rec24, n * sizeof(sha::Compression));
+  std::vector<F128> vz, va, vb;
+  generate_sha256_witness(blocks, (int)n_log, vz, va, vb);
+  memcpy(z, vz.data(), vz.size() * 16);
+  memcpy(a, va.data(), va.size() * 16);
+  memcpy(b, vb.data(), vb.size() * 16);
+}
+// Sha256HybridSetup::new(n) + prove_fast over n >= 1 records
+int flockref_prove_sha256(const uint32_t* rec24, size_t n, const uint8_t* domain, size_t dlen, uint8_t* out,
+                          size_t cap, size_t* out_len) {
+  try {
+    if (n == 0) return 3;
+    std::vector<sha::Compression> blocks(n);
+    memcpy(blocks.data(), rec24, n * sizeof(sha::Compression));
+    Bundle b = prove_sha256(blocks, sha::min_n_blocks_log(n), std::string((const char*)domain, dlen));
+    std::vector<uint8_t> bytes = serialize(b);
+    *out_len = bytes.size();
+    if (bytes.size() > cap) return 2;
+    memcpy(out, bytes.data(), bytes.size());
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
+// A proof of the all-zero witness of the SHA-256 statement over 2^n_log
+// blocks (it satisfies every row but the constant wire's pin; sha2.rs:2292
+// const_pin_all_zero_rejected)
+int flockref_prove_sha256_zero(uint32_t n_log, const uint8_t* domain, size_t dlen, uint8_t* out, size_t cap,
+                               size_t* out_len) {
+  try {
+    const size_t words = (size_t)1 << (sha::K_LOG_SHA + n_log - 7);
+    std::vector<F128> z(words, ZERO), a(words, ZERO), b(words, ZERO);
+    Bundle bd = prove_core(sha256_r1cs((int)n_log), std::move(z), a, b, std::string((const char*)domain, dlen),
+                           CoreHook());
+    std::vector<uint8_t> bytes = serialize(bd);
+    *out_len = bytes.size();
+    if (bytes.size() > cap) return 2;
+    memcpy(out, bytes.data(), bytes.size());
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
+// SHA-256 Merkle paths: the honest inputs (records 24 u32, b bits, leaves
+// 8 u32 each, root) and the proof over given inputs; `check` as for chains.
+void flockref_sha256_merkle_inputs(uint32_t n_log, uint32_t path_log, uint64_t seed, uint32_t* rec24, uint8_t* b,
+                                   uint32_t* leaves, uint32_t* root) {
+  MerklePathInputs in = sha256_merkle_paths((int)n_log, (int)path_log, seed);
+  memcpy(rec24, in.blocks.data(), in.blocks.size() * 96);
+  memcpy(b, in.b_bits.data(), in.b_bits.size());
+  for (size_t p = 0; p < in.leaves.size(); p++) memcpy(leaves + 8 * p, in.leaves[p].data(), 32);
+  memcpy(root, in.root.data(), 32);
+}
+int flockref_prove_sha256_merkle(const uint32_t* rec24, const uint8_t* b, const uint32_t* leaves,
+                                 const uint32_t* root, uint32_t n_log, uint32_t path_log, const uint8_t* domain,
+                                 size_t dlen, uint8_t* out, size_t cap, size_t* out_len, int* check) {
+  try {
+    const size_t N = (size_t)1 << n_log;
+    MerklePathInputs in;
+    in.blocks.resize(N);
+    memcpy(in.blocks.data(), rec24, N * 96);
+    in.b_bits.assign(b, b + N);
+    in.leaves.resize((size_t)1 << path_log);
+    for (size_t p = 0; p < in.leaves.size(); p++) memcpy(in.leaves[p].data(), leaves + 8 * p, 32);
+    memcpy(in.root.data(), root, 32);
+    bool ok = false;
+    MerkleBundle mb = prove_sha256_merkle(in, (int)n_log, (int)path_log, std::string((const char*)domain, dlen), &ok);
+    if (check) *check = ok ? 1 : 0;
+    std::vector<uint8_t> bytes = serialize_merkle(mb);
+    *out_len = bytes.size();
+    if (bytes.size() > cap) return 2;
+    memcpy(out, bytes.data(), bytes.size());
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
 // Wall-clock seconds of one full oracle prove at log2 (for the CPU baseline).
 double flockref_time_prove(uint32_t log2, uint64_t seed, size_t* proof_len) {
   auto blocks = generate_compressions(log2, seed);

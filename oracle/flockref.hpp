@@ -141,16 +141,50 @@ std::vector<Compression> generate_compressions(uint32_t log2, uint64_t seed);
 struct SparseRows { std::vector<uint32_t> ptr; std::vector<uint16_t> col; };  // CSR, K rows
 struct R1cs {
   int m = 0, n_log = 0;
+  int k_log = K_LOG, z_const = Z_CONST_POS;  // block size and the pinned constant column
   SparseRows a0, b0;
   std::array<uint8_t, 32> digest{};
 };
+// crates/flock-core/src/r1cs.rs:334-385: BLAKE3 of the tag, m, k_log,
+// k_skip, the row-major layout byte and the length-prefixed A_0, B_0, C_0 = I
+std::array<uint8_t, 32> statement_digest(int m, int k_log, int k_skip, const SparseRows& a0, const SparseRows& b0);
 const R1cs& blake3_r1cs(int n_log);   // cached per n_log; matrices shared
 void build_matrices(SparseRows& a, SparseRows& b);
 // packed witness: z, a, b each 2^(m-7) F128 (bit r of word i = bit 128 i + r)
 void generate_witness(const std::vector<Compression>& blocks, int n_log,
                       std::vector<F128>& z, std::vector<F128>& a, std::vector<F128>& b);
+// out = (I_n (x) M_0) z for blocks of m0's row count (2^k_log) bits
 void apply_block_diag(const SparseRows& m0, const std::vector<F128>& z, int n_blocks,
                       std::vector<F128>& out);
+
+// ---------------------------------------------------------------------------
+// SHA-256 compression R1CS.  crates/flock-prover/src/r1cs_hashes/sha2.rs
+// (one compression per 2^15-bit block, the I/O-aligned layout).
+// ---------------------------------------------------------------------------
+namespace sha {
+constexpr int K_LOG_SHA = 15;
+constexpr int K_SHA = 1 << K_LOG_SHA;
+constexpr int Z_CONST_POS = 31400;
+constexpr int USEFUL_BITS = 31401;
+extern const uint32_t IV[8];   // FIPS 180-4 5.3.3
+extern const uint32_t RC[64];  // FIPS 180-4 4.2.2
+struct Compression { uint32_t h[8]; uint32_t m[16]; };
+// sha256_compress (sha2.rs:1502-1546): H_out = H_in + rounds(H_in, M)
+void compress(const uint32_t h[8], const uint32_t m[16], uint32_t out[8]);
+// benches/sha2_proof.rs:56-71: one SplitMix64 stream from `seed`, h then m
+std::vector<Compression> bench_inputs(size_t n, uint64_t seed);
+// sha2.rs:1217-1221: log2 of the block slots for n compressions (>= 3)
+int min_n_blocks_log(size_t n);
+void build_matrices(SparseRows& a, SparseRows& b);
+// the 2^15-bit boolean witness of one compression (sha2.rs:545-606), ORed
+// into a zeroed 512-word block
+void block_witness(const Compression& c, uint64_t* z);
+}  // namespace sha
+const R1cs& sha256_r1cs(int n_log);
+// z by the boolean witness (padding blocks: the all-zero (h_in, m)
+// compression), a = A_0 z and b = B_0 z from the matrices
+void generate_sha256_witness(const std::vector<sha::Compression>& blocks, int n_log, std::vector<F128>& z,
+                             std::vector<F128>& a, std::vector<F128>& b);
 
 // ---------------------------------------------------------------------------
 // Additive NTT over F128 (novel basis, neighbours-last) and GF(2^8) NTT.
@@ -248,6 +282,12 @@ struct DirectClaim { std::vector<F128> point; F128 value; };
 using CoreHook = std::function<std::vector<DirectClaim>(Challenger&, const std::vector<F128>&)>;
 Bundle prove_with(const std::vector<Compression>& blocks, int n_log, const std::string& domain,
                   const CoreHook& after_core);
+// the statement-independent prover (prover.rs:373-473 after the witness):
+// commit z, zerocheck, lincheck, the batched open
+Bundle prove_core(const R1cs& rc, std::vector<F128> z, const std::vector<F128>& a, const std::vector<F128>& b,
+                  const std::string& domain, const CoreHook& after_core);
+// Sha256HybridSetup::prove_fast (sha2.rs:1377-1408) over 2^n_log blocks
+Bundle prove_sha256(const std::vector<sha::Compression>& blocks, int n_log, const std::string& domain);
 // sum_j bc[j] * z[j] == target (the batched open's claim)
 bool open_identity(const std::vector<F128>& z, const std::vector<F128>& bc, F128 target);
 // that identity, as checked by the last prove_with with a hook on this thread
@@ -287,5 +327,39 @@ F128 fold_public_cv(const uint32_t cv[8], F128 tau_pos);
 ChainBundle prove_chain(const std::vector<Compression>& blocks, int n_log, const std::string& domain,
                         bool* check = nullptr, const uint32_t* claimed_cv_last = nullptr);
 std::vector<uint8_t> serialize_chain(const ChainBundle& cb);
+
+// ---------------------------------------------------------------------------
+// SHA-256 Merkle paths.  crates/flock-prover/src/merkle_path.rs (shift
+// sumcheck with a bit selector), r1cs_hashes/merkle_path_common.rs (slot
+// folds, claim point, generic prover), r1cs_hashes/sha2.rs:1634-1845
+// (MERKLE_LAYOUT, prove/verify_merkle_paths_ligerito).
+// ---------------------------------------------------------------------------
+struct MerkleShiftProof { std::vector<std::array<F128, 3>> rounds; F128 g_at_point; };
+struct MerkleClaims { std::vector<F128> instance_point; F128 sel_slot, side, value; };
+struct MerklePathInputs {
+  std::vector<sha::Compression> blocks;   // path-id major, 2^n_log of them
+  std::vector<uint8_t> b_bits;            // one per block
+  std::vector<std::array<uint32_t, 8>> leaves;  // one per path
+  std::array<uint32_t, 8> root{};
+};
+struct MerkleBundle { Bundle core; MerkleShiftProof shift; };
+// slot vectors slot[0..4) (H_in, H_out, M_lo, M_hi), each 2^n values
+MerkleShiftProof mp_shift_prove(int path_log, const std::vector<F128> slot[4], const std::vector<uint8_t>& b_bits,
+                                Challenger& ch, MerkleClaims& claims);
+bool mp_shift_verify(int path_log, const MerkleShiftProof& pf, const std::vector<F128>& leaf_evals, F128 root_r,
+                     const std::vector<uint8_t>& b_bits, int n, Challenger& ch, MerkleClaims& claims);
+// 2^path_log copies of one honest path of 2^(n_log - path_log) hashes
+// (benches/sha2_merkle_proof.rs:49-76; sha2.rs:2475-2497)
+MerklePathInputs sha256_merkle_paths(int n_log, int path_log, uint64_t seed);
+// prove_merkle_paths_ligerito; `check` receives the shift argument verified
+// from the public leaves and root on a copy of the transcript and the
+// batched open's claim identity
+MerkleBundle prove_sha256_merkle(const MerklePathInputs& in, int n_log, int path_log, const std::string& domain,
+                                 bool* check = nullptr);
+// bincode of (Commitment, MerklePathProofLigerito { zerocheck, lincheck,
+// shift { rounds: Vec<RoundMsg { q_1, q_omega, q_omega_plus_1 }>,
+// g_at_point }, pcs_open }) -- what the reference's own tests serialise
+// (sha2.rs:2519-2526); there is no FLOCK header for this proof
+std::vector<uint8_t> serialize_merkle(const MerkleBundle& mb);
 
 }  // namespace flockref

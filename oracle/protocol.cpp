@@ -300,6 +300,7 @@ static LincheckProof lincheck_prove(const std::vector<F128>& zp, int m, const R1
   F128 alpha = ch.sample_f128();
   std::vector<F128> lam = lagrange_weights(K_SKIP, z_skip, 0);
   std::vector<F128> eqr = build_eq(x_inner_rest);
+  const int K = 1 << rc.k_log;
   std::vector<F128> eq_inner(K);
   for (int ir = 0; ir < (int)eqr.size(); ir++)
     for (int is = 0; is < 64; is++) eq_inner[is + 64 * ir] = lam[is] * eqr[ir];
@@ -310,9 +311,9 @@ static LincheckProof lincheck_prove(const std::vector<F128>& zp, int m, const R1
     for (uint32_t j = rc.b0.ptr[row]; j < rc.b0.ptr[row + 1]; j++) comb[rc.b0.col[j]] += e;
   }
   F128 beta = ch.sample_f128();
-  comb[Z_CONST_POS] += beta;
+  comb[rc.z_const] += beta;
 
-  // z_vec[c] = sum_o eq(x_outer, o) z[c + 2^14 o]
+  // z_vec[c] = sum_o eq(x_outer, o) z[c + 2^k_log o]
   std::vector<F128> eqo = build_eq(x_outer);
   std::vector<F128> zv(K, ZERO);
   size_t n_outer = eqo.size();
@@ -320,12 +321,12 @@ static LincheckProof lincheck_prove(const std::vector<F128>& zp, int m, const R1
     for (size_t cidx = c0; cidx < c1; cidx++) {
       F128 acc = ZERO;
       for (size_t o = 0; o < n_outer; o++)
-        if (bit_of(zp, cidx + (o << K_LOG))) acc += eqo[o];
+        if (bit_of(zp, cidx + (o << rc.k_log))) acc += eqo[o];
       zv[cidx] = acc;
     }
   });
   std::vector<F128> rr;
-  for (int round = 0; round < K_LOG - K_SKIP; round++) {
+  for (int round = 0; round < rc.k_log - K_SKIP; round++) {
     size_t half = comb.size() / 2;
     F128 q1 = ZERO, qinf = ZERO;
     for (size_t i = 0; i < half; i++) {
@@ -719,6 +720,17 @@ std::vector<uint8_t> serialize(const Bundle& bd) {
   return w.out;
 }
 
+std::vector<uint8_t> serialize_merkle(const MerkleBundle& mb) {
+  W w;
+  put_core(w, mb.core);
+  w.u64(mb.shift.rounds.size());
+  for (const auto& r : mb.shift.rounds)
+    for (const F128& v : r) w.f(v);
+  w.f(mb.shift.g_at_point);
+  put_open(w, mb.core);
+  return w.out;
+}
+
 // ChainProofBundleLigerito { hash_kind, commitment, proof { zerocheck,
 // lincheck, shift { rounds, g_at_point }, pcs_open }, cv_0_phys, cv_last_phys }
 // (proof_io.rs:144-157, 943-950; chain_common.rs:247-253; chain.rs:103-112);
@@ -750,11 +762,15 @@ std::vector<uint8_t> serialize_chain(const ChainBundle& cb) {
 // --------------------------------------------------------------------------
 Bundle prove_with(const std::vector<Compression>& blocks, int n_log, const std::string& domain,
                   const CoreHook& after_core) {
-  const R1cs& rc = blake3_r1cs(n_log);
-  int m = rc.m;
-  const LigeritoConfig& cfg = ligerito_config(m);
   std::vector<F128> z, a, b;
   generate_witness(blocks, n_log, z, a, b);
+  return prove_core(blake3_r1cs(n_log), std::move(z), a, b, domain, after_core);
+}
+
+Bundle prove_core(const R1cs& rc, std::vector<F128> z, const std::vector<F128>& a, const std::vector<F128>& b,
+                  const std::string& domain, const CoreHook& after_core) {
+  int m = rc.m;
+  const LigeritoConfig& cfg = ligerito_config(m);
 
   // commit: RS-encode 64 interleaved lanes at rate 1/2, Merkle over positions
   LigeroLevel l0 = ligero_commit(z, 6, 1);
@@ -769,7 +785,7 @@ Bundle prove_with(const std::vector<Compression>& blocks, int n_log, const std::
 
   ZcClaim zc;
   bd.zc = zerocheck_prove(a, b, z, m, ch, zc);
-  int ir = K_LOG - K_SKIP;
+  int ir = rc.k_log - K_SKIP;
   std::vector<F128> x_inner(zc.mlv.begin(), zc.mlv.begin() + ir);
   std::vector<F128> x_outer(zc.mlv.begin() + ir, zc.mlv.end());
   LcClaim lc;

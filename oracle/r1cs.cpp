@@ -204,10 +204,11 @@ static void absorb_u64(b3::Hasher& h, uint64_t v) {
 }
 
 static void absorb_matrix(b3::Hasher& h, const SparseRows& m) {
-  absorb_u64(h, K);
-  absorb_u64(h, K);
+  const int rows = (int)m.ptr.size() - 1;
+  absorb_u64(h, rows);
+  absorb_u64(h, rows);
   std::vector<uint8_t> buf;
-  for (int r = 0; r < K; r++) {
+  for (int r = 0; r < rows; r++) {
     uint32_t s = m.ptr[r], e = m.ptr[r + 1];
     buf.resize(8 * (size_t)(e - s + 1));
     uint64_t v = e - s;
@@ -218,6 +219,29 @@ static void absorb_matrix(b3::Hasher& h, const SparseRows& m) {
     }
     h.update(buf.data(), buf.size());
   }
+}
+
+std::array<uint8_t, 32> statement_digest(int m, int k_log, int k_skip, const SparseRows& a0, const SparseRows& b0) {
+  const int k = 1 << k_log;
+  SparseRows I;
+  I.ptr.resize(k + 1);
+  I.col.resize(k);
+  for (int i = 0; i < k; i++) { I.ptr[i] = i; I.col[i] = (uint16_t)i; }
+  I.ptr[k] = k;
+  b3::Hasher h;
+  const char* tag = "flock-r1cs-stmt-v1";
+  h.update(tag, strlen(tag));
+  absorb_u64(h, (uint64_t)m);
+  absorb_u64(h, (uint64_t)k_log);
+  absorb_u64(h, (uint64_t)k_skip);
+  uint8_t layout = 0;  // RowMajor
+  h.update(&layout, 1);
+  absorb_matrix(h, a0);
+  absorb_matrix(h, b0);
+  absorb_matrix(h, I);
+  std::array<uint8_t, 32> d;
+  h.finalize(d.data());
+  return d;
 }
 
 const R1cs& blake3_r1cs(int n_log) {
@@ -237,23 +261,7 @@ const R1cs& blake3_r1cs(int n_log) {
   r->m = K_LOG + n_log;
   r->a0 = *A;
   r->b0 = *B;
-  SparseRows I;
-  I.ptr.resize(K + 1);
-  I.col.resize(K);
-  for (int i = 0; i < K; i++) { I.ptr[i] = i; I.col[i] = (uint16_t)i; }
-  I.ptr[K] = K;
-  b3::Hasher h;
-  const char* tag = "flock-r1cs-stmt-v1";
-  h.update(tag, strlen(tag));
-  absorb_u64(h, (uint64_t)r->m);
-  absorb_u64(h, K_LOG);
-  absorb_u64(h, K_SKIP);
-  uint8_t layout = 0;  // RowMajor
-  h.update(&layout, 1);
-  absorb_matrix(h, r->a0);
-  absorb_matrix(h, r->b0);
-  absorb_matrix(h, I);
-  h.finalize(r->digest.data());
+  r->digest = statement_digest(r->m, K_LOG, K_SKIP, r->a0, r->b0);
   const R1cs& ref = *r;
   cache[n_log] = std::move(r);
   return ref;
@@ -352,12 +360,14 @@ void generate_witness(const std::vector<Compression>& blocks, int n_log,
 
 void apply_block_diag(const SparseRows& m0, const std::vector<F128>& z, int n_blocks,
                       std::vector<F128>& out) {
-  size_t per = K / 128;
+  const int rows = (int)m0.ptr.size() - 1;
+  const size_t per = (size_t)rows / 128;
   out.assign((size_t)n_blocks * per, ZERO);
-  for (int o = 0; o < n_blocks; o++) {
+  par_for((size_t)n_blocks, [&](size_t o0, size_t o1, int) {
+  for (size_t o = o0; o < o1; o++) {
     const uint64_t* zw = (const uint64_t*)&z[o * per];
     uint64_t* ow = (uint64_t*)&out[o * per];
-    for (int r = 0; r < K; r++) {
+    for (int r = 0; r < rows; r++) {
       uint64_t acc = 0;
       for (uint32_t j = m0.ptr[r]; j < m0.ptr[r + 1]; j++) {
         int c = m0.col[j];
@@ -366,6 +376,7 @@ void apply_block_diag(const SparseRows& m0, const std::vector<F128>& z, int n_bl
       if (acc) ow[r >> 6] |= 1ull << (r & 63);
     }
   }
+  });
 }
 
 }  // namespace flockref

@@ -38,10 +38,20 @@
    benchmark-tools/trusted/flock_benchmark_verifier, --out names the JSON.
    This pins sizes the oracle is too slow for (2^19, 2^20).
 
+8. sha256_proofs.json (--sha256) — the SHA-256 compression statement
+   (r1cs_hashes/sha2.rs): its statement digests for m = 22..34, and sha256
+   of the oracle's Sha256HybridSetup::prove_fast bundles over the sha2_proof
+   bench inputs (benches/sha2_proof.rs:56-71, seed 0xC0FFEE_5A55 ^ n) at the
+   bench's sizes n = 256, 4096, 16384 and 65536, plus n = 300 (padded).  No
+   reference verifier runs SHA-256 statements, so these pin the GPU to the
+   oracle, whose own checks are recorded per entry: every block's witness
+   satisfies (A_0 z) (B_0 z) = z and carries H_out = sha256_compress(h, m).
+
 Usage (a built oracle; REFERENCE is a checkout of the reference project):
     python tests/golden/make_golden.py --ref REFERENCE [--large]
     python tests/golden/make_golden.py --chain
     python tests/golden/make_golden.py --kernels
+    python tests/golden/make_golden.py --sha256
     python tests/golden/make_golden.py --gpu-harness VERIFIER --sizes 19:2,20:2 --out FILE
 """
 import hashlib
@@ -173,6 +183,35 @@ def kernel_digests(threads=8) -> None:
     (HERE / "kernel_digests.json").write_text(json.dumps(out, indent=1))
 
 
+SHA256_SIZES = (256, 300, 4096, 16384, 65536)
+
+
+def sha256_proofs(threads=8) -> None:
+    import os
+    os.environ["FLOCKREF_THREADS"] = str(threads)
+    sys.path.insert(0, str(REPO / "tests"))
+    import numpy as np
+    import oracle_lib
+    orc = oracle_lib.Oracle()
+    out = {"digests": {str(m): orc.sha256_digest(m - 15).hex() for m in range(22, 35)}, "proofs": []}
+    for n in SHA256_SIZES:
+        seed = 0xC0FFEE_5A55 ^ n
+        comps = orc.sha256_bench_inputs(n, seed)
+        n_log = max(3, (n - 1).bit_length())
+        z, a, b = orc.sha256_witness(comps, n_log)
+        assert np.array_equal(a & b, z), n
+        zb = np.unpackbits(z.view(np.uint8), axis=1, bitorder="little")
+        for i in range(1 << n_log):
+            c = comps[i] if i < n else np.zeros(24, np.uint32)
+            hout = np.packbits(zb[i, 256:512], bitorder="little").view(np.uint32)
+            assert np.array_equal(hout, orc.sha256_compress(c[:8], c[8:])), (n, i)
+        data = orc.prove_sha256(comps)
+        out["proofs"].append({"n": n, "seed": seed, "domain": "flock-bench-v0", "m": 15 + n_log,
+                              "sha256": hashlib.sha256(data).hexdigest(), "size": len(data),
+                              "checked_by": "oracle: (A_0 z)(B_0 z) = z and H_out = sha256_compress in every block"})
+        (HERE / "sha256_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
+
+
 if __name__ == "__main__":
     import argparse
     ap = argparse.ArgumentParser()
@@ -180,12 +219,15 @@ if __name__ == "__main__":
     ap.add_argument("--large", action="store_true")
     ap.add_argument("--chain", action="store_true")
     ap.add_argument("--kernels", action="store_true")
+    ap.add_argument("--sha256", action="store_true")
     ap.add_argument("--gpu-harness", type=Path, metavar="VERIFIER")
     ap.add_argument("--sizes", default="19:2,20:2", help="LOG2:RUNS,... for --gpu-harness")
     ap.add_argument("--out", type=Path, default=HERE / "gpu_verified_proofs.json")
     a = ap.parse_args()
     if a.chain:
         chain_proofs()
+    elif a.sha256:
+        sha256_proofs()
     elif a.kernels:
         kernel_digests()
     elif a.gpu_harness:

@@ -58,12 +58,68 @@ class Oracle:
         L.flockref_ch_digest.argtypes = [vp, vp]
         L.flockref_pow_ok.argtypes = [vp, u64, u32]
         L.flockref_chain_blocks.argtypes = [u64, vp, sz, vp]
+        L.flockref_sha256_compress.argtypes = [vp, vp, vp]
+        L.flockref_sha256_bench_inputs.argtypes = [sz, u64, vp]
+        L.flockref_sha256_min_n_blocks_log.argtypes = [sz]
+        L.flockref_sha256_digest.argtypes = [u32, vp]
+        L.flockref_sha256_matrix_nnz.argtypes = [i32]
+        L.flockref_sha256_matrix_nnz.restype = u64
+        L.flockref_sha256_matrix_csr.argtypes = [i32, vp, vp]
+        L.flockref_sha256_witness.argtypes = [vp, sz, u32, vp, vp, vp]
+        L.flockref_prove_sha256.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        L.flockref_prove_sha256_zero.argtypes = [u32, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_prove_chain_blocks.argtypes = [vp, u32, ctypes.c_char_p, sz, vp, vp, sz, ctypes.POINTER(sz),
                                                   ctypes.POINTER(ctypes.c_int)]
         L.flockref_prove_records.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_time_prove.argtypes = [u32, u64, ctypes.POINTER(sz)]
         L.flockref_time_prove.restype = ctypes.c_double
         self.L = L
+
+    # ---- SHA-256 compressions (r1cs_hashes/sha2.rs)
+    def sha256_compress(self, h, m) -> np.ndarray:
+        h, m = np.ascontiguousarray(h, np.uint32), np.ascontiguousarray(m, np.uint32)
+        out = np.zeros(8, np.uint32)
+        self.L.flockref_sha256_compress(_p(h), _p(m), _p(out))
+        return out
+
+    def sha256_bench_inputs(self, n: int, seed: int) -> np.ndarray:
+        out = np.zeros((n, 24), np.uint32)
+        self.L.flockref_sha256_bench_inputs(n, seed, _p(out))
+        return out
+
+    def sha256_digest(self, n_log: int) -> bytes:
+        out = np.zeros(32, np.uint8)
+        self.L.flockref_sha256_digest(n_log, _p(out))
+        return out.tobytes()
+
+    def sha256_matrix(self, which: int):
+        nnz = self.L.flockref_sha256_matrix_nnz(which)
+        ptr = np.zeros((1 << 15) + 1, np.uint32)
+        col = np.zeros(nnz, np.uint16)
+        self.L.flockref_sha256_matrix_csr(which, _p(ptr), _p(col))
+        return ptr, col
+
+    def sha256_witness(self, comps: np.ndarray, n_log: int):
+        comps = np.ascontiguousarray(comps, np.uint32).reshape(-1, 24)
+        z, a, b = (np.zeros((1 << n_log, 512), np.uint64) for _ in range(3))
+        self.L.flockref_sha256_witness(_p(comps), comps.shape[0], n_log, _p(z), _p(a), _p(b))
+        return z, a, b
+
+    def prove_sha256(self, comps: np.ndarray, domain: bytes = b"flock-bench-v0") -> bytes:
+        comps = np.ascontiguousarray(comps, np.uint32).reshape(-1, 24)
+        buf = np.zeros(2_000_000, np.uint8)
+        n = ctypes.c_size_t()
+        rc = self.L.flockref_prove_sha256(_p(comps), comps.shape[0], domain, len(domain), _p(buf), buf.size,
+                                          ctypes.byref(n))
+        assert rc == 0, rc
+        return buf[: n.value].tobytes()
+
+    def prove_sha256_zero(self, n_log: int, domain: bytes = b"flock-bench-v0") -> bytes:
+        buf = np.zeros(2_000_000, np.uint8)
+        n = ctypes.c_size_t()
+        rc = self.L.flockref_prove_sha256_zero(n_log, domain, len(domain), _p(buf), buf.size, ctypes.byref(n))
+        assert rc == 0, rc
+        return buf[: n.value].tobytes()
 
     def prove(self, log2: int, seed: int) -> bytes:
         buf = np.zeros(1 << 20, np.uint8)
