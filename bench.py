@@ -546,8 +546,28 @@ def sha256_report(ctx, sizes=(16, 18), steps: int = 5) -> dict:
         rows.append({"log2": log2, "m": 15 + log2, "device_ms_median": d, "device_compressions_per_s": n / (d / 1e3),
                      "e2e_ms_median": e * 1e3, "e2e_compressions_per_s": n / e, "proof_bytes": size,
                      "h2d_bytes_per_proof": n * 96, "phases_ms": {k: round(v, 3) for k, v in ph.items()}})
+    # Merkle paths (prove_merkle_path_ligerito) at the Merkle bench's largest
+    # size, 2^15 hashes on one path (benches/sha2_merkle_proof.rs:264-268)
+    n_log = 15
+    comps, b, leaves, root = flockgpu.sha256_merkle_inputs(n_log)
+    prover = flockgpu.Sha256Prover(ctx, 1 << n_log)
+    for _ in range(2):
+        prover.prove_merkle(comps, b)
+    wall = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        size = len(prover.prove_merkle(comps, b))
+        wall.append(time.perf_counter() - t0)
+    ph = prover.phase_ms()
+    why = ctx.sha256_merkle_verify(prover.prove_merkle(comps, b), 0, b, leaves, root)
+    prover.close()
+    if why:
+        raise SystemExit(f"sha256_report: Merkle-path proof rejected: {why}")
+    e = pct(wall, 0.5)
+    merkle = {"log2": n_log, "paths": 1, "e2e_ms_median": e * 1e3, "e2e_hashes_per_s": (1 << n_log) / e,
+              "proof_bytes": size, "phases_ms": {k: round(v, 3) for k, v in ph.items()}}
     return {"sha256": {"statement": "SHA-256 compressions, one per 2^15-bit block (hybrid R1CS, sha2.rs)",
-                       "proofs": rows}}
+                       "proofs": rows, "merkle_path": merkle}}
 
 
 def verify_report(prover, log2: int, reps: int = 3) -> dict:

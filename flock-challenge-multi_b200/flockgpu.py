@@ -36,7 +36,8 @@ EXPORTS = (
     "flock_challenger_grind_pow", "flock_challenger_verify_pow", "flock_challenger_state_digest",
     "flock_ntt_plan_desc", "flock_bench_ntt_plan", "flock_bench_f128_product", "flock_launch_count",
     "flock_serve_prewarm", "flock_sha256_setup_create", "flock_sha256_prove", "flock_sha256_verify_bundle",
-    "flock_sha256_compress", "flock_sha256_statement_digest", "flock_sha256_witness",
+    "flock_sha256_compress", "flock_sha256_statement_digest", "flock_sha256_witness", "flock_sha256_merkle_prove",
+    "flock_sha256_merkle_verify", "flock_sha256_merkle_inputs",
 )
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
@@ -125,6 +126,10 @@ def load() -> ctypes.CDLL:
         lib.flock_sha256_compress.restype = None
         lib.flock_sha256_statement_digest.argtypes = [u32, vp]
         lib.flock_sha256_witness.argtypes = [vp, vp, sz, u32, vp, vp, vp]
+        lib.flock_sha256_merkle_prove.argtypes = [vp, vp, sz, vp, u32, ctypes.c_char_p, sz, vp, sz,
+                                                  ctypes.POINTER(sz)]
+        lib.flock_sha256_merkle_verify.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz, u32, vp, sz, vp, vp]
+        lib.flock_sha256_merkle_inputs.argtypes = [u32, u32, u64, vp, vp, vp, vp]
         lib.flock_submit.argtypes = [vp, ctypes.POINTER(FlockJob), ctypes.POINTER(u64)]
         lib.flock_poll.argtypes = [vp, u64, ctypes.POINTER(FlockResult), i32]
         lib.flock_host_alloc.argtypes = [sz, ctypes.POINTER(vp)]
@@ -199,6 +204,26 @@ def sha256_bench_inputs(n: int, seed: int) -> np.ndarray:
 def sha256_bench_seed(n: int, run: int = 0) -> int:
     """The seed sha2_proof.rs:112 gives run `run` of n compressions."""
     return 0xC0FFEE_5A55 ^ n ^ run
+
+
+MERKLE_DOMAIN = b"flock-merkle-bench-v0"
+
+
+def sha256_merkle_inputs(n_log: int, path_log: int = 0, seed: int = None):
+    """Honest SHA-256 Merkle paths (benches/sha2_merkle_proof.rs:49-76, the
+    path repeated for each of 2^path_log paths): (compressions (2^n_log, 24)
+    u32, b_bits (2^n_log,) u8, leaves (2^path_log, 8) u32, root (8,) u32).
+    The bench's seed is 0xD15EA5E ^ n."""
+    n = 1 << n_log
+    seed = 0xD15EA5E ^ n if seed is None else seed
+    comps = np.zeros((n, 24), np.uint32)
+    b = np.zeros(n, np.uint8)
+    leaves = np.zeros((1 << path_log, 8), np.uint32)
+    root = np.zeros(8, np.uint32)
+    rc = load().flock_sha256_merkle_inputs(n_log, path_log, seed, _ptr(comps), _ptr(b), _ptr(leaves), _ptr(root))
+    if rc != 0:
+        raise FlockError(f"sha256_merkle_inputs: {rc}")
+    return comps, b, leaves, root
 
 
 def sha256_compress(h, m) -> np.ndarray:
@@ -314,6 +339,22 @@ class Context:
         if rc == FLOCK_ERR_VERIFY:
             return self.lib.flock_last_error(self.h).decode()
         self._check(rc, "sha256_verify_bundle")
+        return "error"
+
+    def sha256_merkle_verify(self, bundle: bytes, path_log: int, b_bits, leaves, root,
+                             domain: bytes = MERKLE_DOMAIN) -> str:
+        """verify_merkle_paths_ligerito: '' when the proof verifies against
+        the public leaves ((2^path_log, 8) u32), root (8 u32) and bits."""
+        b = np.ascontiguousarray(b_bits, np.uint8)
+        lv = np.ascontiguousarray(leaves, np.uint32).reshape(-1, 8)
+        rt = np.ascontiguousarray(root, np.uint32)
+        rc = self.lib.flock_sha256_merkle_verify(self.h, bundle, len(bundle), domain, len(domain), path_log, _ptr(b),
+                                                 b.size, _ptr(lv), _ptr(rt))
+        if rc == 0:
+            return ""
+        if rc == FLOCK_ERR_VERIFY:
+            return self.lib.flock_last_error(self.h).decode()
+        self._check(rc, "sha256_merkle_verify")
         return "error"
 
     def sha256_witness(self, comps: np.ndarray, n_log: int):
@@ -617,6 +658,18 @@ class Sha256Prover:
         rc = self.ctx.lib.flock_sha256_prove(self.h, _ptr(comps), comps.shape[0], domain, len(domain),
                                              _ptr(self._buf), self._buf.size, ctypes.byref(n))
         self.ctx._check(rc, "sha256_prove")
+        return self._buf[: n.value].tobytes()
+
+    def prove_merkle(self, comps: np.ndarray, b_bits, path_log: int = 0, domain: bytes = MERKLE_DOMAIN) -> bytes:
+        """prove_merkle_paths_ligerito over (n, 24) u32 compressions that fill
+        the setup (n a power of two) and n selector bits; bincode of
+        (Commitment, MerklePathProofLigerito)."""
+        comps = np.ascontiguousarray(comps, np.uint32).reshape(-1, 24)
+        b = np.ascontiguousarray(b_bits, np.uint8)
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_sha256_merkle_prove(self.h, _ptr(comps), comps.shape[0], _ptr(b), path_log, domain,
+                                                    len(domain), _ptr(self._buf), self._buf.size, ctypes.byref(n))
+        self.ctx._check(rc, "sha256_merkle_prove")
         return self._buf[: n.value].tobytes()
 
     def prove_seed(self, seed: int, domain: bytes = DOMAIN) -> bytes:

@@ -47,11 +47,20 @@
    oracle, whose own checks are recorded per entry: every block's witness
    satisfies (A_0 z) (B_0 z) = z and carries H_out = sha256_compress(h, m).
 
+9. sha256_merkle_proofs.json (--sha256-merkle) — SHA-256 Merkle-path proofs
+   (prove_merkle_paths_ligerito, sha2.rs:1740-1783) of the oracle over the
+   honest paths of benches/sha2_merkle_proof.rs:49-76 (seed 0xD15EA5E ^ n):
+   the bench's sizes n = 4096, 16384 and 32768 single-path, and n = 128 and
+   256 with 4 and 8 replicated paths.  Each entry records the oracle's own
+   check: the shift argument verified from the public leaves and root, and
+   the batched open's claim identity.
+
 Usage (a built oracle; REFERENCE is a checkout of the reference project):
     python tests/golden/make_golden.py --ref REFERENCE [--large]
     python tests/golden/make_golden.py --chain
     python tests/golden/make_golden.py --kernels
     python tests/golden/make_golden.py --sha256
+    python tests/golden/make_golden.py --sha256-merkle
     python tests/golden/make_golden.py --gpu-harness VERIFIER --sizes 19:2,20:2 --out FILE
 """
 import hashlib
@@ -212,6 +221,28 @@ def sha256_proofs(threads=8) -> None:
         (HERE / "sha256_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
 
 
+SHA256_MERKLE = ((12, 0), (14, 0), (15, 0), (7, 2), (8, 3))
+
+
+def sha256_merkle_proofs(threads=8) -> None:
+    import os
+    os.environ["FLOCKREF_THREADS"] = str(threads)
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle_lib
+    orc = oracle_lib.Oracle()
+    out = []
+    for n_log, path_log in SHA256_MERKLE:
+        seed = 0xD15EA5E ^ (1 << n_log)
+        comps, b, leaves, root = orc.sha256_merkle_inputs(n_log, path_log, seed)
+        data, ok = orc.prove_sha256_merkle(comps, b, leaves, root, path_log)
+        assert ok, (n_log, path_log)
+        out.append({"n_log": n_log, "path_log": path_log, "seed": seed, "domain": "flock-merkle-bench-v0",
+                    "sha256": hashlib.sha256(data).hexdigest(), "size": len(data),
+                    "checked_by": "oracle: shift argument verified from the public leaves and root; "
+                                  "batched-open claim identity"})
+        (HERE / "sha256_merkle_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
+
+
 if __name__ == "__main__":
     import argparse
     ap = argparse.ArgumentParser()
@@ -220,6 +251,7 @@ if __name__ == "__main__":
     ap.add_argument("--chain", action="store_true")
     ap.add_argument("--kernels", action="store_true")
     ap.add_argument("--sha256", action="store_true")
+    ap.add_argument("--sha256-merkle", action="store_true")
     ap.add_argument("--gpu-harness", type=Path, metavar="VERIFIER")
     ap.add_argument("--sizes", default="19:2,20:2", help="LOG2:RUNS,... for --gpu-harness")
     ap.add_argument("--out", type=Path, default=HERE / "gpu_verified_proofs.json")
@@ -228,6 +260,8 @@ if __name__ == "__main__":
         chain_proofs()
     elif a.sha256:
         sha256_proofs()
+    elif a.sha256_merkle:
+        sha256_merkle_proofs()
     elif a.kernels:
         kernel_digests()
     elif a.gpu_harness:

@@ -68,6 +68,9 @@ class Oracle:
         L.flockref_sha256_witness.argtypes = [vp, sz, u32, vp, vp, vp]
         L.flockref_prove_sha256.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_prove_sha256_zero.argtypes = [u32, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        L.flockref_sha256_merkle_inputs.argtypes = [u32, u32, u64, vp, vp, vp, vp]
+        L.flockref_prove_sha256_merkle.argtypes = [vp, vp, vp, vp, u32, u32, ctypes.c_char_p, sz, vp, sz,
+                                                   ctypes.POINTER(sz), ctypes.POINTER(ctypes.c_int)]
         L.flockref_prove_chain_blocks.argtypes = [vp, u32, ctypes.c_char_p, sz, vp, vp, sz, ctypes.POINTER(sz),
                                                   ctypes.POINTER(ctypes.c_int)]
         L.flockref_prove_records.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
@@ -113,6 +116,32 @@ class Oracle:
                                           ctypes.byref(n))
         assert rc == 0, rc
         return buf[: n.value].tobytes()
+
+    def sha256_merkle_inputs(self, n_log: int, path_log: int, seed: int):
+        n = 1 << n_log
+        comps = np.zeros((n, 24), np.uint32)
+        b = np.zeros(n, np.uint8)
+        leaves = np.zeros((1 << path_log, 8), np.uint32)
+        root = np.zeros(8, np.uint32)
+        self.L.flockref_sha256_merkle_inputs(n_log, path_log, seed, _p(comps), _p(b), _p(leaves), _p(root))
+        return comps, b, leaves, root
+
+    def prove_sha256_merkle(self, comps, b, leaves, root, path_log: int,
+                            domain: bytes = b"flock-merkle-bench-v0") -> tuple:
+        """(bytes, check): check = the shift argument verified from the public
+        leaves and root, and the batched open's claim identity."""
+        comps = np.ascontiguousarray(comps, np.uint32).reshape(-1, 24)
+        b = np.ascontiguousarray(b, np.uint8)
+        leaves = np.ascontiguousarray(leaves, np.uint32)
+        root = np.ascontiguousarray(root, np.uint32)
+        n_log = comps.shape[0].bit_length() - 1
+        buf = np.zeros(2_000_000, np.uint8)
+        n = ctypes.c_size_t()
+        chk = ctypes.c_int()
+        rc = self.L.flockref_prove_sha256_merkle(_p(comps), _p(b), _p(leaves), _p(root), n_log, path_log, domain,
+                                                 len(domain), _p(buf), buf.size, ctypes.byref(n), ctypes.byref(chk))
+        assert rc == 0, rc
+        return buf[: n.value].tobytes(), bool(chk.value)
 
     def prove_sha256_zero(self, n_log: int, domain: bytes = b"flock-bench-v0") -> bytes:
         buf = np.zeros(2_000_000, np.uint8)
