@@ -14,6 +14,7 @@ struct flock_ctx {
   std::string err;
   std::mutex mu;
   std::unique_ptr<flock::Server> server;
+  int fs_fn = flock::kFnBlake3;  // the transcript hash of the verify-bundle entry points
   std::mutex vmu;  // one verification at a time on the context's verifier
   std::unique_ptr<flock::Verifier> verifier;
 };
@@ -39,7 +40,7 @@ struct flock_prover_data {
 // FsChallenger (challenger.rs:170-600) with the BLAKE3 hash.
 struct flock_challenger {
   flock::Transcript tr;
-  explicit flock_challenger(const std::string& domain) : tr(domain) {}
+  flock_challenger(const std::string& domain, int fn) : tr(domain, fn) {}
 };
 
 std::atomic<uint64_t>& kernel_launch_counter() {
@@ -144,14 +145,15 @@ const char* flock_last_error(flock_ctx* c) { return c ? c->err.c_str() : "null c
 
 int flock_setup_create(flock_ctx* c, uint32_t log2_n, int hash, int profile, flock_setup** out) {
   if (!c || !out) return FLOCK_ERR_ARG;
-  if (log2_n < 8 || log2_n > 20 || hash != FLOCK_HASH_BLAKE3 || profile != FLOCK_PROFILE_FAST) {
-    c->err = "unsupported setup (log2 in 8..=20, BLAKE3 Merkle hash, fast profile)";
+  if (log2_n < 8 || log2_n > 20 || (hash != FLOCK_HASH_BLAKE3 && hash != FLOCK_HASH_SHA256) ||
+      profile != FLOCK_PROFILE_FAST) {
+    c->err = "unsupported setup (log2 in 8..=20, BLAKE3 or SHA-256 Merkle hash, fast profile)";
     return FLOCK_ERR_ARG;
   }
   return guard(c, [&] {
     auto* s = new flock_setup();
     s->ctx = c;
-    s->s.reset(new flock::Setup(c->device, log2_n));
+    s->s.reset(new flock::Setup(c->device, log2_n, 0, flock::kHashBlake3, hash));
     s->n_blocks = (size_t)1 << log2_n;
     *out = s;
     return FLOCK_OK;
@@ -177,6 +179,19 @@ int flock_setup_create_blocks(flock_ctx* c, size_t n_blocks, int hash, int profi
 }
 
 void flock_setup_destroy(flock_setup* s) { delete s; }
+
+int flock_setup_set_transcript(flock_setup* s, int hash) {
+  if (!s || (hash != FLOCK_HASH_SHA256 && hash != FLOCK_HASH_BLAKE3)) return FLOCK_ERR_ARG;
+  s->s->fs_fn = hash;
+  return FLOCK_OK;
+}
+
+int flock_ctx_set_transcript(flock_ctx* c, int hash) {
+  if (!c || (hash != FLOCK_HASH_SHA256 && hash != FLOCK_HASH_BLAKE3)) return FLOCK_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->vmu);
+  c->fs_fn = hash;
+  return FLOCK_OK;
+}
 
 static int emit(flock_ctx* c, const std::vector<uint8_t>& bytes, uint8_t* out, size_t cap, size_t* out_len) {
   if (out_len) *out_len = bytes.size();
@@ -246,15 +261,16 @@ int flock_sha256_setup_create(flock_ctx* c, size_t n_compressions, int hash, int
   // min_n_blocks_log (sha2.rs:1217-1221): 2^max(3, ceil(log2 n)) slots
   uint32_t n_log = 3;
   while (n_compressions && ((size_t)1 << n_log) < n_compressions) n_log++;
-  if (n_compressions == 0 || n_log < 7 || n_log > 19 || hash != FLOCK_HASH_BLAKE3 || profile != FLOCK_PROFILE_FAST) {
+  if (n_compressions == 0 || n_log < 7 || n_log > 19 || (hash != FLOCK_HASH_BLAKE3 && hash != FLOCK_HASH_SHA256) ||
+      profile != FLOCK_PROFILE_FAST) {
     c->err = "unsupported SHA-256 setup (65..=2^19 compressions: the fast profile's Ligerito ladders cover "
-             "m = 22..34; BLAKE3 Merkle hash, fast profile)";
+             "m = 22..34; BLAKE3 or SHA-256 Merkle hash, fast profile)";
     return FLOCK_ERR_ARG;
   }
   return guard(c, [&] {
     auto* s = new flock_setup();
     s->ctx = c;
-    s->s.reset(new flock::Setup(c->device, n_log, 0, flock::kHashSha256));
+    s->s.reset(new flock::Setup(c->device, n_log, 0, flock::kHashSha256, hash));
     s->n_blocks = n_compressions;
     *out = s;
     return FLOCK_OK;
@@ -324,7 +340,7 @@ int flock_sha256_merkle_verify(flock_ctx* c, const uint8_t* bytes, size_t len, c
     std::lock_guard<std::mutex> lk(c->vmu);
     if (!c->verifier) c->verifier.reset(new flock::Verifier(c->device));
     const std::string why =
-        c->verifier->verify(bytes, len, std::string((const char*)domain, dlen), flock::kHashSha256, &mp);
+        c->verifier->verify(bytes, len, std::string((const char*)domain, dlen), flock::kHashSha256, &mp, c->fs_fn);
     if (why.empty()) return (int)FLOCK_OK;
     c->err = "verify: " + why;
     return (int)FLOCK_ERR_VERIFY;
@@ -377,7 +393,7 @@ int flock_sha256_verify_bundle(flock_ctx* c, const uint8_t* bytes, size_t len, c
     std::lock_guard<std::mutex> lk(c->vmu);
     if (!c->verifier) c->verifier.reset(new flock::Verifier(c->device));
     const std::string why =
-        c->verifier->verify(bytes, len, std::string((const char*)domain, dlen), flock::kHashSha256);
+        c->verifier->verify(bytes, len, std::string((const char*)domain, dlen), flock::kHashSha256, nullptr, c->fs_fn);
     if (why.empty()) return (int)FLOCK_OK;
     c->err = "verify: " + why;
     return (int)FLOCK_ERR_VERIFY;
@@ -483,7 +499,17 @@ void flock_prover_data_destroy(flock_prover_data* pd) { delete pd; }
 int flock_challenger_create(const uint8_t* domain, size_t dlen, flock_challenger** out) {
   if (!out || (!domain && dlen)) return FLOCK_ERR_ARG;
   try {
-    *out = new flock_challenger(std::string((const char*)domain, dlen));
+    *out = new flock_challenger(std::string((const char*)domain, dlen), flock::kFnBlake3);
+  } catch (...) {
+    return FLOCK_ERR_INTERNAL;
+  }
+  return FLOCK_OK;
+}
+
+int flock_challenger_create_hash(const uint8_t* domain, size_t dlen, int hash, flock_challenger** out) {
+  if (!out || (!domain && dlen) || (hash != FLOCK_HASH_SHA256 && hash != FLOCK_HASH_BLAKE3)) return FLOCK_ERR_ARG;
+  try {
+    *out = new flock_challenger(std::string((const char*)domain, dlen), hash);
   } catch (...) {
     return FLOCK_ERR_INTERNAL;
   }
@@ -530,7 +556,7 @@ int flock_challenger_grind_pow(flock_challenger* ch, flock_ctx* c, uint32_t bits
   if (bits <= flock::kHostPowBits) {  // a few dozen hashes: on the calling thread
     uint8_t d[32];
     ch->tr.state_digest(d);
-    *nonce = bits ? flock::pow_search_host(d, bits) : 0;
+    *nonce = bits ? flock::pow_search_host(d, bits, ch->tr.fn()) : 0;
     ch->tr.nonce(*nonce);
     return FLOCK_OK;
   }
@@ -543,7 +569,7 @@ int flock_challenger_grind_pow(flock_challenger* ch, flock_ctx* c, uint32_t bits
       unsigned long long* h = nullptr;
       CK(cudaMallocHost(&h, 8));
       try {
-        n = pow_search(d, bits, c->st, found.p, h);
+        n = pow_search(d, bits, c->st, found.p, h, ch->tr.fn());
       } catch (...) {
         cudaFreeHost(h);
         throw;
@@ -603,7 +629,8 @@ int flock_verify_bundle(flock_ctx* c, const uint8_t* bytes, size_t len, const ui
   return guard(c, [&] {
     std::lock_guard<std::mutex> lk(c->vmu);
     if (!c->verifier) c->verifier.reset(new flock::Verifier(c->device));
-    const std::string why = c->verifier->verify(bytes, len, std::string((const char*)domain, dlen));
+    const std::string why = c->verifier->verify(bytes, len, std::string((const char*)domain, dlen), flock::kHashBlake3,
+                                                nullptr, c->fs_fn);
     if (why.empty()) return (int)FLOCK_OK;
     c->err = "verify: " + why;
     return (int)FLOCK_ERR_VERIFY;
@@ -871,14 +898,19 @@ int flock_ntt_autotune(flock_ctx* c, uint32_t log_msg_pos, uint32_t lanes, uint3
 }
 
 int flock_merkle_tree(flock_ctx* c, const uint8_t* data, size_t n_leaves, size_t leaf_size, uint8_t* tree_out) {
+  return flock_merkle_tree_hash(c, data, n_leaves, leaf_size, FLOCK_HASH_BLAKE3, tree_out);
+}
+
+int flock_merkle_tree_hash(flock_ctx* c, const uint8_t* data, size_t n_leaves, size_t leaf_size, int hash,
+                           uint8_t* tree_out) {
   if (!c || !data || !tree_out || n_leaves == 0 || (n_leaves & (n_leaves - 1)) || leaf_size == 0 ||
-      leaf_size > 1024 || (leaf_size % 16))
+      leaf_size > 1024 || (leaf_size % 16) || (hash != FLOCK_HASH_SHA256 && hash != FLOCK_HASH_BLAKE3))
     return FLOCK_ERR_ARG;
   return guard(c, [&] {
     DevBuf<uint8_t> dd(n_leaves * leaf_size);
     DevBuf<uint32_t> dt(8 * (2 * n_leaves - 1));
     CK(cudaMemcpyAsync(dd.p, data, n_leaves * leaf_size, cudaMemcpyHostToDevice, c->st));
-    merkle_build(dd.p, n_leaves, leaf_size, dt.p, c->st);
+    merkle_build(dd.p, n_leaves, leaf_size, dt.p, hash, c->st);
     CK(cudaMemcpyAsync(tree_out, dt.p, (2 * n_leaves - 1) * 32, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return FLOCK_OK;

@@ -253,7 +253,43 @@ void B3::xof(uint8_t* out, size_t n) const {
 // ----------------------------------------------------------- transcript --
 static void le64(uint64_t v, uint8_t* b) { for (int i = 0; i < 8; i++) b[i] = (uint8_t)(v >> (8 * i)); }
 
-Transcript::Transcript(const std::string& domain) {
+S256::S256() { memcpy(h_, kB3IV, 32); }
+void S256::update(const void* p, size_t n) {
+  const uint8_t* b = static_cast<const uint8_t*>(p);
+  total_ += n;
+  while (n) {
+    const size_t k = std::min(n, 64 - blen_);
+    memcpy(buf_ + blen_, b, k);
+    blen_ += k;
+    b += k;
+    n -= k;
+    if (blen_ == 64) {
+      uint32_t m[16];
+      for (int i = 0; i < 16; i++)
+        m[i] = (uint32_t)buf_[4 * i] << 24 | (uint32_t)buf_[4 * i + 1] << 16 | (uint32_t)buf_[4 * i + 2] << 8 |
+               buf_[4 * i + 3];
+      sha256_compress(h_, m, h_);
+      blen_ = 0;
+    }
+  }
+}
+void S256::digest(uint8_t out[32]) const {
+  S256 s = *this;
+  const uint64_t bits = total_ * 8;
+  uint8_t pad[72] = {0x80};
+  const size_t padn = (blen_ < 56 ? 56 - blen_ : 120 - blen_);
+  for (int i = 0; i < 8; i++) pad[padn + i] = (uint8_t)(bits >> (56 - 8 * i));
+  s.update(pad, padn + 8);
+  for (int i = 0; i < 8; i++)
+    for (int k = 0; k < 4; k++) out[4 * i + k] = (uint8_t)(s.h_[i] >> (24 - 8 * k));
+}
+void sha256_bytes(const void* p, size_t n, uint8_t out[32]) {
+  S256 s;
+  s.update(p, n);
+  s.digest(out);
+}
+
+Transcript::Transcript(const std::string& domain, int fn) : fn_(fn) {
   uint8_t op = 1, n[8];
   le64(domain.size(), n);
   put(&op, 1);
@@ -275,34 +311,50 @@ void Transcript::label_bytes(const void* p, size_t len) {
   put(n, 8);
   put(p, len);
 }
-uint64_t pow_search_host(const uint8_t digest[32], uint32_t bits) {
+bool pow_hash_ok(const uint8_t digest[32], uint64_t nonce, uint32_t bits, int fn) {
   uint8_t pre[64] = {0}, h[32];
   memcpy(pre, digest, 32);
-  for (uint64_t n = 0;; n++) {
-    for (int i = 0; i < 8; i++) pre[32 + i] = (uint8_t)(n >> (8 * i));
+  for (int i = 0; i < 8; i++) pre[32 + i] = (uint8_t)(nonce >> (8 * i));
+  if (fn == kFnSha256) {
+    sha256_bytes(pre, 40, h);
+  } else {
     B3 b;
     b.update(pre, 64);
     b.digest(h);
-    bool ok = true;
-    for (uint32_t k = 0; k < bits && ok; k++) ok = ((h[k / 8] >> (7 - k % 8)) & 1) == 0;
-    if (ok) return n;
   }
+  bool ok = true;
+  for (uint32_t k = 0; k < bits && ok; k++) ok = ((h[k / 8] >> (7 - k % 8)) & 1) == 0;
+  return ok;
+}
+uint64_t pow_search_host(const uint8_t digest[32], uint32_t bits, int fn) {
+  for (uint64_t n = 0;; n++)
+    if (pow_hash_ok(digest, n, bits, fn)) return n;
 }
 bool Transcript::verify_pow(uint64_t nonce, uint32_t bits) {
   bool ok = true;
   if (bits == 0) {
     ok = nonce == 0;
   } else {
-    uint8_t pre[64] = {0}, h[32];
-    state_digest(pre);
-    for (int i = 0; i < 8; i++) pre[32 + i] = (uint8_t)(nonce >> (8 * i));
-    B3 b;
-    b.update(pre, 64);
-    b.digest(h);
-    for (uint32_t k = 0; k < bits && ok; k++) ok = ((h[k / 8] >> (7 - k % 8)) & 1) == 0;
+    uint8_t d[32];
+    state_digest(d);
+    ok = pow_hash_ok(d, nonce, bits, fn_);
   }
   this->nonce(nonce);
   return ok;
+}
+void Transcript::squeeze(uint8_t* out, size_t n) const {
+  if (fn_ != kFnSha256) {
+    h_.xof(out, n);
+    return;
+  }
+  for (uint64_t ctr = 0, off = 0; off < n; ctr++, off += 32) {
+    S256 s = s_;
+    uint8_t c[8], blk[32];
+    le64(ctr, c);
+    s.update(c, 8);
+    s.digest(blk);
+    memcpy(out + off, blk, std::min<size_t>(32, n - off));
+  }
 }
 void Transcript::f128v(f128 v) {
   uint8_t b[18] = {3, 1};
@@ -335,7 +387,7 @@ static f128 from_le(const uint8_t* b) {
 f128 Transcript::sample() {
   uint8_t t[2] = {4, 1}, buf[16];
   put(t, 2);
-  h_.xof(buf, 16);
+  squeeze(buf, 16);
   put(buf, 16);
   return from_le(buf);
 }
@@ -344,7 +396,7 @@ std::vector<f128> Transcript::sample_vec(size_t n) {
   le64(n, t + 2);
   put(t, 10);
   std::vector<uint8_t> buf(16 * n);
-  if (n) h_.xof(buf.data(), buf.size());
+  if (n) squeeze(buf.data(), buf.size());
   put(buf.data(), buf.size());
   std::vector<f128> v(n);
   for (size_t i = 0; i < n; i++) v[i] = from_le(&buf[16 * i]);
@@ -726,7 +778,7 @@ std::vector<uint8_t> encode(const Proof& p) {
   e.u64(1);  // log_inv_rate
   e.u64(6);  // log_batch_size
   e.u32(0);  // profile Fast
-  e.u32(1);  // merkle hash Blake3
+  e.u32((uint32_t)p.merkle_fn);  // merkle hash: 0 Sha256, 1 Blake3
   e.fs(p.r1_ab);
   e.fs(p.r1_c);
   e.pairs(p.zc_rounds);

@@ -41,33 +41,68 @@ class B3 {
 void b3_compress(const uint32_t cv[8], const uint32_t m[16], uint64_t ctr, uint32_t blen, uint32_t flags, uint32_t out[16]);
 extern const uint32_t kB3IV[8];  // the BLAKE3 IV (the SHA-256 initial hash words)
 
+// The hash function behind a Merkle tree or a Fiat-Shamir transcript
+// (HashKind, crates/flock-core/src/hash.rs:20-30; these are its serde
+// discriminants, and Sha256 is the reference's default).
+enum HashFn : int { kFnSha256 = 0, kFnBlake3 = 1 };
+
+// ---- SHA-256 hasher (FIPS 180-4), incremental; copies are snapshots ----
+class S256 {
+ public:
+  S256();
+  void update(const void* p, size_t n);
+  void digest(uint8_t out[32]) const;
+ private:
+  uint32_t h_[8];
+  uint8_t buf_[64];
+  size_t blen_ = 0;
+  uint64_t total_ = 0;
+};
+void sha256_bytes(const void* p, size_t n, uint8_t out[32]);
+
 // ---- Fiat-Shamir transcript (challenger.rs:170-600) ----
 class Transcript {
  public:
-  explicit Transcript(const std::string& domain);
+  // FsChallenger::with_hash(domain, fn) (challenger.rs:227-250)
+  explicit Transcript(const std::string& domain, int fn = kFnBlake3);
   void label(const char* s);
   void f128v(f128 v);
   void f128s(const f128* v, size_t n);
   void bytes(const void* p, size_t n);
   f128 sample();
   std::vector<f128> sample_vec(size_t n);
-  void state_digest(uint8_t out[32]) const { h_.digest(out); }
+  void state_digest(uint8_t out[32]) const {
+    if (fn_ == kFnSha256) s_.digest(out);
+    else h_.digest(out);
+  }
+  int fn() const { return fn_; }
   void nonce(uint64_t n) { uint8_t b[8]; for (int i = 0; i < 8; i++) b[i] = (uint8_t)(n >> (8 * i)); bytes(b, 8); }
   // a label of arbitrary bytes (label() takes a C string)
   void label_bytes(const void* p, size_t n);
-  // FsChallenger::verify_pow (challenger.rs:502-545): the BLAKE3 hash of
-  // state digest || nonce (LE) || 0^24 has `bits` leading zero bits (bits =
-  // 0: the nonce is 0); the nonce is observed either way
+  // FsChallenger::verify_pow (challenger.rs:502-545, 580-601): the hash of
+  // state digest || nonce (LE) -- BLAKE3 pads the preimage with 0^24, SHA-256
+  // does not -- has `bits` leading zero bits (bits = 0: the nonce is 0); the
+  // nonce is observed either way
   bool verify_pow(uint64_t nonce, uint32_t bits);
  private:
-  void put(const void* p, size_t n) { h_.update(p, n); }
+  void put(const void* p, size_t n) {
+    if (fn_ == kFnSha256) s_.update(p, n);
+    else h_.update(p, n);
+  }
+  // squeeze_into (challenger.rs:288-303): the BLAKE3 XOF of the state, or
+  // SHA256(state || ctr LE) for ctr = 0, 1, ... (32 bytes each)
+  void squeeze(uint8_t* out, size_t n) const;
+  int fn_ = kFnBlake3;
   B3 h_;
+  S256 s_;
 };
 
 // The smallest nonce whose BLAKE3 root hash of (digest || nonce LE || 0^24)
 // has `bits` leading zero bits, searched on the host (grind_pow,
 // challenger.rs:384-475): for a few bits this is cheaper than a GPU round trip.
-uint64_t pow_search_host(const uint8_t digest[32], uint32_t bits);
+uint64_t pow_search_host(const uint8_t digest[32], uint32_t bits, int fn = kFnBlake3);
+// the PoW predicate (challenger.rs:580-601)
+bool pow_hash_ok(const uint8_t digest[32], uint64_t nonce, uint32_t bits, int fn);
 // grinds of at most this many bits run on the host
 constexpr uint32_t kHostPowBits = 6;
 
@@ -142,6 +177,7 @@ struct Proof {
   // MerklePathProofLigerito), without a FLOCK header
   bool merkle = false;
   std::vector<std::array<f128, 3>> mp_rounds;
+  int merkle_fn = kFnBlake3;  // PcsParams::merkle_hash of the commitment
 };
 std::vector<uint8_t> encode(const Proof& p);
 

@@ -153,6 +153,10 @@ void merkle_top_batch(const BatchJob* jobs, int n_jobs, cudaStream_t s);
 // K2 / K9
 void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, cudaStream_t s);
 void merkle_leaves(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* out, cudaStream_t s);
+// the same over the Merkle hash fn (0 SHA-256: leaf SHA256(bytes), parent
+// SHA256(l || r), leaf sizes multiples of 4 bytes; 1 BLAKE3: the above)
+void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, int fn, cudaStream_t s);
+void merkle_leaves(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* out, int fn, cudaStream_t s);
 __global__ void k_gather_nodes(const uint32_t* tree, const uint64_t* idx, size_t n, uint32_t* out);
 // The sorted distinct leaf positions q followed by the flat-tree indices of
 // their Merkle multi-proof's sibling nodes, in the order the proof lists them
@@ -160,8 +164,9 @@ __global__ void k_gather_nodes(const uint32_t* tree, const uint64_t* idx, size_t
 // sibling is not itself opened).
 std::vector<uint64_t> multiproof_ids(const std::vector<size_t>& q, size_t n_leaves);
 __global__ void k_gather_rows(const f128* cw, const uint64_t* pos, size_t n, int lanes, f128* out);
+// fn: the PoW hash (0 SHA-256, 1 BLAKE3; HashKind)
 uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, unsigned long long* d_found,
-                    unsigned long long* h_found);
+                    unsigned long long* h_found, int fn = 1);
 // K3..K8
 void eq_split(const f128* lo, const f128* hi, int s_bits, size_t n, f128* out, cudaStream_t s);
 void axpy(f128* out, const f128* x, f128 beta, size_t n, cudaStream_t s);

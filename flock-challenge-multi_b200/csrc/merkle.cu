@@ -9,6 +9,8 @@
 // challenger.rs:384-475,549-600 — the smallest nonce n such that the root
 // BLAKE3 hash of (state_digest || n_le || 0^24) has `bits` leading zero bits.
 #include "kernels.cuh"
+#include "sha256.cuh"
+#include "host.hpp"
 
 namespace {
 // non-root chaining value of one leaf of leaf_size <= 1024 bytes (a single
@@ -153,6 +155,74 @@ void merkle_top_batch(const BatchJob* jobs, int n_jobs, cudaStream_t s) {
   k_merkle_top_batch<<<n_jobs, 512, 0, s>>>(jobs);
 }
 
+// ---- SHA-256 trees (merkle.rs:205-230): leaf = SHA256(leaf bytes),
+// parent = SHA256(left || right); digests stored as their 32 bytes
+// (big-endian words).  Leaf sizes are multiples of 4 bytes.
+__global__ void k_merkle_leaves_sha(const uint8_t* __restrict__ data, size_t leaf_size, size_t n_leaves,
+                                    uint32_t* __restrict__ tree) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_leaves) return;
+  const uint32_t* d = reinterpret_cast<const uint32_t*>(data + i * leaf_size);
+  uint32_t st[8], w[16];
+#pragma unroll
+  for (int k = 0; k < 8; k++) st[k] = sha_d::kIV[k];
+  const size_t full = leaf_size / 64, rem_words = (leaf_size % 64) / 4;
+  for (size_t b = 0; b < full; b++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) w[k] = sha_d::bswap(__ldg(d + 16 * b + k));
+    sha_d::compress(st, w);
+  }
+#pragma unroll
+  for (int k = 0; k < 16; k++) w[k] = (size_t)k < rem_words ? sha_d::bswap(__ldg(d + 16 * full + k)) : 0u;
+  w[rem_words] = 0x80000000u;
+  const uint64_t bits = (uint64_t)leaf_size * 8;
+  if (rem_words >= 14) {
+    sha_d::compress(st, w);
+#pragma unroll
+    for (int k = 0; k < 16; k++) w[k] = 0;
+  }
+  w[14] = (uint32_t)(bits >> 32);
+  w[15] = (uint32_t)bits;
+  sha_d::compress(st, w);
+#pragma unroll
+  for (int k = 0; k < 8; k++) tree[8 * i + k] = sha_d::bswap(st[k]);
+}
+
+__global__ void k_merkle_parents_sha(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, size_t n_out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_out) return;
+  uint32_t st[8], w[16];
+#pragma unroll
+  for (int k = 0; k < 8; k++) st[k] = sha_d::kIV[k];
+#pragma unroll
+  for (int k = 0; k < 16; k++) w[k] = sha_d::bswap(in[16 * i + k]);
+  sha_d::compress(st, w);
+#pragma unroll
+  for (int k = 0; k < 16; k++) w[k] = 0;
+  w[0] = 0x80000000u;
+  w[15] = 512;
+  sha_d::compress(st, w);
+#pragma unroll
+  for (int k = 0; k < 8; k++) out[8 * i + k] = sha_d::bswap(st[k]);
+}
+
+void merkle_leaves(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* out, int fn, cudaStream_t s) {
+  if (fn != flock::kFnSha256) return merkle_leaves(data, n_leaves, leaf_size, out, s);
+  count_launch();
+  k_merkle_leaves_sha<<<(unsigned)((n_leaves + 127) / 128), 128, 0, s>>>((const uint8_t*)data, leaf_size, n_leaves,
+                                                                         out);
+}
+
+void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, int fn, cudaStream_t s) {
+  if (fn != flock::kFnSha256) return merkle_build(data, n_leaves, leaf_size, tree, s);
+  merkle_leaves(data, n_leaves, leaf_size, tree, fn, s);
+  for (size_t start = 0, len = n_leaves; len > 1; start += len, len >>= 1) {
+    const size_t n = len >> 1;
+    count_launch();
+    k_merkle_parents_sha<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(tree + 8 * start, tree + 8 * (start + len), n);
+  }
+}
+
 void merkle_build(const void* data, size_t n_leaves, size_t leaf_size, uint32_t* tree, cudaStream_t s) {
   count_launch(); k_merkle_leaves<<<(unsigned)((n_leaves + 127) / 128), 128, 0, s>>>((const uint8_t*)data, leaf_size, n_leaves, tree);
   size_t start = 0, len = n_leaves;
@@ -228,8 +298,30 @@ __global__ void k_pow(uint4 d0, uint4 d1, uint32_t bits, uint64_t start, uint64_
   if (ok) atomicMin(found, (unsigned long long)n);
 }
 
+// SHA256(digest || nonce LE), one padded block (challenger.rs:589-595)
+__global__ void k_pow_sha(uint4 d0, uint4 d1, uint32_t bits, uint64_t start, uint64_t count,
+                          unsigned long long* __restrict__ found) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint64_t n = start + i;
+  if (n >= *found) return;
+  uint32_t w[16] = {sha_d::bswap(d0.x), sha_d::bswap(d0.y), sha_d::bswap(d0.z), sha_d::bswap(d0.w),
+                    sha_d::bswap(d1.x), sha_d::bswap(d1.y), sha_d::bswap(d1.z), sha_d::bswap(d1.w),
+                    sha_d::bswap((uint32_t)n), sha_d::bswap((uint32_t)(n >> 32)), 0x80000000u, 0, 0, 0, 0, 320};
+  uint32_t st[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) st[k] = sha_d::kIV[k];
+  sha_d::compress(st, w);
+  // leading zero bits of the digest bytes (big-endian words)
+  uint32_t full = bits >> 3, extra = bits & 7;
+  bool ok = true;
+  for (uint32_t k = 0; k < full && ok; k++) ok = ((st[k >> 2] >> (24 - 8 * (k & 3))) & 0xFF) == 0;
+  if (ok && extra) ok = ((((st[full >> 2] >> (24 - 8 * (full & 3))) & 0xFF) >> (8 - extra)) == 0);
+  if (ok) atomicMin(found, (unsigned long long)n);
+}
+
 uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, unsigned long long* d_found,
-                    unsigned long long* h_found) {
+                    unsigned long long* h_found, int fn) {
   if (bits == 0) return 0;
   uint4 d0, d1;
   memcpy(&d0, digest, 16);
@@ -240,7 +332,9 @@ uint64_t pow_search(const uint8_t digest[32], uint32_t bits, cudaStream_t s, uns
   for (uint64_t start = 0;; start += chunk) {
     *h_found = ~0ull;
     CK(cudaMemcpyAsync(d_found, h_found, 8, cudaMemcpyHostToDevice, s));
-    count_launch(); k_pow<<<(unsigned)(chunk / 256), 256, 0, s>>>(d0, d1, bits, start, chunk, d_found);
+    count_launch();
+    if (fn == flock::kFnSha256) k_pow_sha<<<(unsigned)(chunk / 256), 256, 0, s>>>(d0, d1, bits, start, chunk, d_found);
+    else k_pow<<<(unsigned)(chunk / 256), 256, 0, s>>>(d0, d1, bits, start, chunk, d_found);
     CK(cudaMemcpyAsync(h_found, d_found, 8, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (*h_found != ~0ull) return *h_found;

@@ -69,10 +69,12 @@ size_t Setup::estimate_bytes(uint32_t log2, int hash) {
   return n_words * 16 * 10 + n_words * 2 + n_words * 2 + (n_words / 128) * 212 + ((size_t)96 << 20);
 }
 
-Setup::Setup(int device, uint32_t log2_, int stream_priority, int hash_) : log2(log2_), hash(hash_) {
+Setup::Setup(int device, uint32_t log2_, int stream_priority, int hash_, int merkle_fn_)
+    : log2(log2_), hash(hash_), merkle_fn(merkle_fn_) {
   CK(cudaSetDevice(device));
   const size_t bytes0 = t_alloc_bytes;
   if (hash != kHashBlake3 && hash != kHashSha256) throw std::runtime_error("unknown statement hash");
+  if (merkle_fn != kFnBlake3 && merkle_fn != kFnSha256) throw std::runtime_error("unknown Merkle hash");
   k_log = hash_k_log(hash);
   n_log = std::max<int>(3, (int)log2);
   m = k_log + n_log;
@@ -194,7 +196,8 @@ void Setup::capture_commit() {
   const char* env = getenv("FLOCK_COMMIT_GRAPHS");
   if (env && strcmp(env, "0") == 0) return;
   commit_graph[0] = capture(st, &commit_launches[0], [&] { ntt_rs_encode(z, cw0, m - 13, 64, 1, st); });
-  commit_graph[1] = capture(st, &commit_launches[1], [&] { merkle_build(cw0, n_leaves0, 64 * 16, tree0, st); });
+  commit_graph[1] =
+      capture(st, &commit_launches[1], [&] { merkle_build(cw0, n_leaves0, 64 * 16, tree0, merkle_fn, st); });
 }
 
 // Fused witness + RS encode + Merkle commit of several seeded proofs: every
@@ -381,7 +384,8 @@ uint64_t Setup::grind(Transcript& tr, uint32_t bits) {
     uint8_t d[32];
     tr.state_digest(d);
     // a few dozen hashes on the host cost less than a round trip to the GPU
-    nonce = bits <= kHostPowBits ? pow_search_host(d, bits) : pow_search(d, bits, st, d_found, h_found);
+    nonce = bits <= kHostPowBits ? pow_search_host(d, bits, tr.fn())
+                                 : pow_search(d, bits, st, d_found, h_found, tr.fn());
   }
   tr.nonce(nonce);
   return nonce;
@@ -450,6 +454,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
                                   bool full_records, const MerkleArgs* merkle) {
   Proof P;
   P.m = (uint64_t)m;
+  P.merkle_fn = merkle_fn;
   pending_.clear();  // (left over only by a proof that threw)
   stage_off_ = 0;
   const int gs = grid_sms > 0 && grid_sms < sms ? grid_sms : sms;
@@ -490,13 +495,13 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       CK(cudaGraphLaunch(commit_graph[1], st));
       count_launch(commit_launches[1]);
     } else {
-      merkle_build(cw0, n_leaves0, 64 * 16, tree0, st);
+      merkle_build(cw0, n_leaves0, 64 * 16, tree0, merkle_fn, st);
     }
   }
   P.root = root_of(tree0, n_leaves0);
   mark(3);
 
-  Transcript tr(domain);
+  Transcript tr(domain, fs_fn);
   tr.label("flock-r1cs-v0");
   tr.bytes(digest.data(), 32);
   tr.bytes(P.root.data(), 32);
@@ -1070,7 +1075,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   // level 1 commit
   auto commit = [&](Level& L) {
     ntt_rs_encode(f, L.cw, L.log_msg_pos, L.lanes, L.rate, st);
-    merkle_build(L.cw, L.positions, (size_t)L.lanes * 16, L.tree, st);
+    merkle_build(L.cw, L.positions, (size_t)L.lanes * 16, L.tree, merkle_fn, st);
     H32 rt = root_of(L.tree, L.positions);
     P.roots.push_back(rt);
     tr.bytes(rt.data(), 32);

@@ -55,13 +55,14 @@ struct ChainEnds {
 // column) for eq = L(z_skip) (x) eq(x_inner) (lincheck.rs:5940-5960).
 struct VerifyStatement {
   int m = 0, k_log = kKLog;
+  int fs_fn = kFnBlake3;                 // the transcript's hash
   const MerklePublic* merkle = nullptr;  // a Merkle-path proof's public inputs
   std::array<uint8_t, 32> digest{};
   std::function<std::vector<f128>(f128 z_skip, const std::vector<f128>& x_inner, f128 alpha, f128 beta)> comb;
   // optional: BLAKE3 leaf chaining values of rows packed back to back, group
   // k holding counts[k] rows of sizes[k] bytes; empty result = hash on the host
   std::function<std::vector<H32>(const uint8_t* data, const std::vector<size_t>& sizes,
-                                 const std::vector<size_t>& counts)>
+                                 const std::vector<size_t>& counts, int merkle_fn)>
       leaf_cvs;
 };
 // "" when the bundle verifies, otherwise the name of the failed check
@@ -78,8 +79,10 @@ class Verifier {
   Verifier& operator=(const Verifier&) = delete;
   // "" when the bundle verifies, otherwise the name of the failed check;
   // hash: the statement the bundle is for (the R1CS bundle does not say)
+  // fs_fn: the transcript's hash (the bundle does not say; its Merkle hash
+  // it does)
   std::string verify(const uint8_t* bytes, size_t len, const std::string& domain, int hash = kHashBlake3,
-                     const MerklePublic* merkle = nullptr);
+                     const MerklePublic* merkle = nullptr, int fs_fn = kFnBlake3);
 
  private:
   static constexpr size_t kRowsCap = (size_t)1 << 20, kCvsCap = (size_t)1 << 19;
@@ -105,7 +108,9 @@ class Setup {
   // lower numbers are served first when streams compete for the SMs).
   // hash: the statement (kHashBlake3: 2^log2 BLAKE3 compressions in 2^14-bit
   // blocks; kHashSha256: SHA-256 compressions in 2^15-bit blocks).
-  Setup(int device, uint32_t log2, int stream_priority = 0, int hash = kHashBlake3);
+  // merkle_fn: the hash of the PCS Merkle trees (PcsParams::merkle_hash;
+  // kFnBlake3, the benchmark's, or kFnSha256, the reference's default)
+  Setup(int device, uint32_t log2, int stream_priority = 0, int hash = kHashBlake3, int merkle_fn = kFnBlake3);
   ~Setup();
   Setup(const Setup&) = delete;
   Setup& operator=(const Setup&) = delete;
@@ -141,6 +146,10 @@ class Setup {
                                         cudaStream_t st);
   uint32_t log2 = 0;
   int hash = kHashBlake3, k_log = kKLog;
+  int merkle_fn = kFnBlake3;
+  // the Fiat-Shamir transcript's hash (FsChallenger::with_hash); settable
+  // between proofs
+  int fs_fn = kFnBlake3;
   int n_log = 0, m = 0, sms = 0;
   // SMs the grid-stride kernels of this setup spread over (0: all).  The
   // serving queue lowers it for large proofs so that their long persistent

@@ -122,8 +122,9 @@ bool decode(const uint8_t* bytes, size_t n, Proof& P, std::string& why, bool mer
   if (P.chain && r.u32() != 0) return why = "hash kind is not BLAKE3", false;
   P.root = r.h();
   P.m = r.u64();
-  if (r.u64() != 1 || r.u64() != 6 || r.u32() != 0 || r.u32() != 1)
-    return why = "PCS parameters are not (rate 1/2, batch 2^6, Fast, BLAKE3)", false;
+  if (r.u64() != 1 || r.u64() != 6 || r.u32() != 0) return why = "PCS parameters are not (rate 1/2, batch 2^6, Fast)", false;
+  P.merkle_fn = (int)r.u32();
+  if (P.merkle_fn != kFnSha256 && P.merkle_fn != kFnBlake3) return why = "unknown Merkle hash", false;
   P.r1_ab = r.fs();
   P.r1_c = r.fs();
   P.zc_rounds = r.pairs();
@@ -278,8 +279,14 @@ H32 cv_bytes(const uint32_t w[8]) {
     for (int k = 0; k < 4; k++) h[4 * i + k] = (uint8_t)(w[i] >> (8 * k));
   return h;
 }
-// non-root chaining value of a leaf of at most one chunk (merkle.rs:192-197)
-H32 leaf_cv(const uint8_t* d, size_t len) {
+// non-root chaining value of a leaf of at most one chunk (merkle.rs:192-197);
+// with SHA-256 Merkle hashing, SHA256(leaf) (merkle.rs:205-214)
+H32 leaf_cv(const uint8_t* d, size_t len, int fn = kFnBlake3) {
+  if (fn == kFnSha256) {
+    H32 h;
+    sha256_bytes(d, len, h.data());
+    return h;
+  }
   uint32_t cv[8], out[16], m[16];
   memcpy(cv, kB3IV, 32);
   const size_t nb = std::max<size_t>(1, (len + 63) / 64);
@@ -295,7 +302,15 @@ H32 leaf_cv(const uint8_t* d, size_t len) {
   }
   return cv_bytes(cv);
 }
-H32 parent_cv(const H32& l, const H32& r) {
+H32 parent_cv(const H32& l, const H32& r, int fn = kFnBlake3) {
+  if (fn == kFnSha256) {
+    uint8_t b[64];
+    memcpy(b, l.data(), 32);
+    memcpy(b + 32, r.data(), 32);
+    H32 h;
+    sha256_bytes(b, 64, h.data());
+    return h;
+  }
   uint32_t m[16], out[16];
   for (int i = 0; i < 8; i++) {
     m[i] = (uint32_t)l[4 * i] | (uint32_t)l[4 * i + 1] << 8 | (uint32_t)l[4 * i + 2] << 16 | (uint32_t)l[4 * i + 3] << 24;
@@ -307,7 +322,7 @@ H32 parent_cv(const H32& l, const H32& r) {
 }
 // verify_merkle_multi_proof (merkle.rs:1122-1190)
 bool merkle_multi_verify(const H32& root, size_t n_leaves, const std::vector<size_t>& pos,
-                         const std::vector<H32>& leaves, const std::vector<H32>& proof) {
+                         const std::vector<H32>& leaves, const std::vector<H32>& proof, int fn) {
   if (n_leaves == 0 || (n_leaves & (n_leaves - 1)) || pos.size() != leaves.size()) return false;
   if (pos.empty()) return proof.empty();
   for (size_t i = 0; i < pos.size(); i++)
@@ -332,7 +347,7 @@ bool merkle_multi_verify(const H32& root, size_t n_leaves, const std::vector<siz
         else { l = act[i].second; r = sib; }
         i += 1;
       }
-      nx.push_back({p >> 1, parent_cv(l, r)});
+      nx.push_back({p >> 1, parent_cv(l, r, fn)});
     }
     act.swap(nx);
   }
@@ -341,15 +356,15 @@ bool merkle_multi_verify(const H32& root, size_t n_leaves, const std::vector<siz
 // verify_level_opens (pcs/ligerito.rs:12441-12468): rows of `lanes` values;
 // `cvs`, when given, holds the rows' leaf chaining values already hashed
 bool level_opens_ok(const H32& root, size_t block_len, const std::vector<size_t>& q, const Opening& o,
-                    size_t lanes, const std::vector<H32>* cvs) {
+                    size_t lanes, const std::vector<H32>* cvs, int fn) {
   if (q.size() != o.rows.size()) return false;
   std::vector<H32> leaves;
   for (size_t i = 0; i < o.rows.size(); i++) {
     const auto& row = o.rows[i];
     if (row.size() != lanes || lanes * 16 > 1024) return false;
-    leaves.push_back(cvs ? (*cvs)[i] : leaf_cv(reinterpret_cast<const uint8_t*>(row.data()), lanes * 16));
+    leaves.push_back(cvs ? (*cvs)[i] : leaf_cv(reinterpret_cast<const uint8_t*>(row.data()), lanes * 16, fn));
   }
-  return merkle_multi_verify(root, block_len, q, leaves, o.proof);
+  return merkle_multi_verify(root, block_len, q, leaves, o.proof, fn);
 }
 
 // The leaf chaining values of every opened row, per opening (initial,
@@ -375,7 +390,7 @@ std::vector<std::vector<H32>> opened_leaf_cvs(const Proof& P, const VerifyStatem
       data.insert(data.end(), b, b + sz);
     }
   }
-  std::vector<H32> all = V.leaf_cvs(data.data(), sizes, counts);
+  std::vector<H32> all = V.leaf_cvs(data.data(), sizes, counts, P.merkle_fn);
   size_t at = 0;
   for (size_t k = 0; k < ops.size(); k++) {
     if (!counts[k]) continue;
@@ -506,7 +521,7 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
   const Ladder* lad = ladder_for(m);
   if (!lad) return "no Ligerito configuration for this size";
   const Ladder& Ld = *lad;
-  Transcript tr(domain);
+  Transcript tr(domain, V.fs_fn);
   tr.label("flock-r1cs-v0");
   tr.bytes(V.digest.data(), 32);
   tr.bytes(P.root.data(), 32);
@@ -774,7 +789,7 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
   std::vector<f128> a0 = tr.sample_vec(ceil_log2((size_t)Ld.queries[0]));
   const std::vector<std::vector<H32>> lcv = opened_leaf_cvs(P, V);
   auto cvs_of = [&](size_t k) { return lcv[k].empty() ? nullptr : &lcv[k]; };
-  if (!level_opens_ok(P.root, block0, q0, P.initial, (size_t)1 << ik, cvs_of(0))) return "ligerito: L0 openings";
+  if (!level_opens_ok(P.root, block0, q0, P.initial, (size_t)1 << ik, cvs_of(0), P.merkle_fn)) return "ligerito: L0 openings";
   const int n1 = log_n - ik;
   {
     const f128 es = enforced_sum(P.initial, lane_rs, q0, a0);
@@ -806,7 +821,8 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
       const size_t pbl = (size_t)1 << (prev_lmc + prev_rate);
       std::vector<size_t> ql = sample_distinct_queries(tr, pbl, (size_t)Ld.queries[i + 1]);
       std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
-      if (!level_opens_ok(prev_root, pbl, ql, P.final_open, (size_t)1 << prev_lni, cvs_of(lcv.size() - 1)))
+      if (!level_opens_ok(prev_root, pbl, ql, P.final_open, (size_t)1 << prev_lni, cvs_of(lcv.size() - 1),
+                          P.merkle_fn))
         return "ligerito: final openings";
       const f128 es = enforced_sum(P.final_open, level_rs, ql, al);
       const f128 be = tr.sample();
@@ -863,7 +879,7 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
     std::vector<f128> al = tr.sample_vec(ceil_log2((size_t)Ld.queries[i + 1]));
     if (rp >= P.levels.size()) return "ligerito: level openings missing";
     const Opening& o = P.levels[rp++];
-    if (!level_opens_ok(prev_root, pbl, qi, o, (size_t)1 << prev_lni, cvs_of(rp))) return "ligerito: level openings";
+    if (!level_opens_ok(prev_root, pbl, qi, o, (size_t)1 << prev_lni, cvs_of(rp), P.merkle_fn)) return "ligerito: level openings";
     const f128 es = enforced_sum(o, level_rs, qi, al);
     if (!next_msg(msg)) return "ligerito: transcript length";
     const Quad iq = Quad::from(msg, es);
@@ -912,7 +928,8 @@ VerifyStatement device_statement(int m, int hash, const std::array<uint8_t, 32>&
     return cv;
   };
   // every opened row's leaf chaining value in one upload
-  V.leaf_cvs = [=](const uint8_t* data, const std::vector<size_t>& sizes, const std::vector<size_t>& counts) {
+  V.leaf_cvs = [=](const uint8_t* data, const std::vector<size_t>& sizes, const std::vector<size_t>& counts,
+                   int merkle_fn) {
     size_t bytes = 0, n = 0;
     for (size_t k = 0; k < sizes.size(); k++) bytes += sizes[k] * counts[k], n += counts[k];
     std::vector<H32> cvs(n);
@@ -921,7 +938,7 @@ VerifyStatement device_statement(int m, int hash, const std::array<uint8_t, 32>&
     size_t off = 0, at = 0;
     for (size_t k = 0; k < sizes.size(); k++) {
       if (!counts[k]) continue;
-      merkle_leaves(B.rows + off, counts[k], sizes[k], B.cvs + 8 * at, st);
+      merkle_leaves(B.rows + off, counts[k], sizes[k], B.cvs + 8 * at, merkle_fn, st);
       off += sizes[k] * counts[k];
       at += counts[k];
     }
@@ -965,6 +982,7 @@ std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& d
   if (merkle && hash != kHashSha256) return "a Merkle path is a SHA-256 statement";
   VerifyStatement V = device_statement(m, hash, digest, at_ptr, at_row, bt_ptr, bt_row, B, st);
   V.merkle = merkle;
+  V.fs_fn = fs_fn;
   return verify_bundle(bytes, len, domain, V);
 }
 
@@ -989,7 +1007,7 @@ Verifier::~Verifier() {
 }
 
 std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string& domain, int hash,
-                             const MerklePublic* merkle) {
+                             const MerklePublic* merkle, int fs_fn) {
   if (len < 7 + 4 + 32 + 8) return "malformed bundle: truncated";
   if (merkle && hash != kHashSha256) return "a Merkle path is a SHA-256 statement";
   // the statement size is the bundle's m (after the header, the optional
@@ -1010,6 +1028,7 @@ std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string
   VerifyStatement V = device_statement((int)mm, hash, statement_digest(hash, (int)mm), C.at_ptr, C.at_row, C.bt_ptr,
                                        C.bt_row, B, st_);
   V.merkle = merkle;
+  V.fs_fn = fs_fn;
   return verify_bundle(bytes, len, domain, V);
 }
 

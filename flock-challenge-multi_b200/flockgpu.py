@@ -37,8 +37,11 @@ EXPORTS = (
     "flock_ntt_plan_desc", "flock_bench_ntt_plan", "flock_bench_f128_product", "flock_launch_count",
     "flock_serve_prewarm", "flock_sha256_setup_create", "flock_sha256_prove", "flock_sha256_verify_bundle",
     "flock_sha256_compress", "flock_sha256_statement_digest", "flock_sha256_witness", "flock_sha256_merkle_prove",
-    "flock_sha256_merkle_verify", "flock_sha256_merkle_inputs",
+    "flock_sha256_merkle_verify", "flock_sha256_merkle_inputs", "flock_setup_set_transcript",
+    "flock_ctx_set_transcript", "flock_challenger_create_hash", "flock_merkle_tree_hash",
 )
+# the hash behind Merkle trees / the transcript (HashKind discriminants)
+HASH = {"sha256": 0, "blake3": 1}
 FLOCK_ERR_CAPACITY = 3
 FLOCK_ERR_TIMEOUT = 5
 FLOCK_ERR_VERIFY = 6
@@ -130,6 +133,10 @@ def load() -> ctypes.CDLL:
                                                   ctypes.POINTER(sz)]
         lib.flock_sha256_merkle_verify.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz, u32, vp, sz, vp, vp]
         lib.flock_sha256_merkle_inputs.argtypes = [u32, u32, u64, vp, vp, vp, vp]
+        lib.flock_setup_set_transcript.argtypes = [vp, i32]
+        lib.flock_ctx_set_transcript.argtypes = [vp, i32]
+        lib.flock_challenger_create_hash.argtypes = [ctypes.c_char_p, sz, i32, ctypes.POINTER(vp)]
+        lib.flock_merkle_tree_hash.argtypes = [vp, vp, sz, sz, i32, vp]
         lib.flock_submit.argtypes = [vp, ctypes.POINTER(FlockJob), ctypes.POINTER(u64)]
         lib.flock_poll.argtypes = [vp, u64, ctypes.POINTER(FlockResult), i32]
         lib.flock_host_alloc.argtypes = [sz, ctypes.POINTER(vp)]
@@ -455,11 +462,16 @@ class Context:
                     "ntt_autotune")
         return ms.value, d.value.decode()
 
-    def merkle_tree(self, data: np.ndarray, n_leaves: int, leaf_size: int) -> np.ndarray:
+    def merkle_tree(self, data: np.ndarray, n_leaves: int, leaf_size: int, hash: str = "blake3") -> np.ndarray:
         data = np.ascontiguousarray(data, np.uint8)
         out = np.zeros((2 * n_leaves - 1) * 32, np.uint8)
-        self._check(self.lib.flock_merkle_tree(self.h, _ptr(data), n_leaves, leaf_size, _ptr(out)), "merkle_tree")
+        self._check(self.lib.flock_merkle_tree_hash(self.h, _ptr(data), n_leaves, leaf_size, HASH[hash], _ptr(out)),
+                    "merkle_tree")
         return out
+
+    def set_transcript(self, hash: str) -> None:
+        """The transcript hash the verify-bundle entry points assume."""
+        self._check(self.lib.flock_ctx_set_transcript(self.h, HASH[hash]), "ctx_set_transcript")
 
     def sumcheck_round(self, f: np.ndarray, b: np.ndarray) -> np.ndarray:
         f = np.ascontiguousarray(f, np.uint64)
@@ -529,13 +541,14 @@ class Context:
 
 
 class Challenger:
-    """FsChallenger with the BLAKE3 hash (crates/flock-core/src/challenger.rs:
-    170-600) behind the C ABI; values are (lo, hi) pairs of u64."""
+    """FsChallenger::with_hash(domain, hash) (crates/flock-core/src/
+    challenger.rs:170-600) behind the C ABI; values are (lo, hi) pairs of
+    u64.  hash: "blake3" (the benchmark's) or "sha256" (FsChallenger::new)."""
 
-    def __init__(self, domain: bytes = DOMAIN):
+    def __init__(self, domain: bytes = DOMAIN, hash: str = "blake3"):
         self.lib = load()
         h = ctypes.c_void_p()
-        if self.lib.flock_challenger_create(domain, len(domain), ctypes.byref(h)):
+        if self.lib.flock_challenger_create_hash(domain, len(domain), HASH[hash], ctypes.byref(h)):
             raise FlockError("challenger_create failed")
         self.h = h
 
@@ -633,10 +646,12 @@ class Sha256Prover:
     sha2.rs:1252-1330): SHA-256 compressions, one per 2^15-bit block,
     2^max(3, ceil(log2 n)) slots, BLAKE3 Merkle hashing, fast profile."""
 
-    def __init__(self, ctx: Context, n: int):
+    def __init__(self, ctx: Context, n: int, merkle_hash: str = "blake3", transcript: str = "blake3"):
         h = ctypes.c_void_p()
-        ctx._check(ctx.lib.flock_sha256_setup_create(ctx.h, n, 1, 0, ctypes.byref(h)), "sha256_setup_create")
+        ctx._check(ctx.lib.flock_sha256_setup_create(ctx.h, n, HASH[merkle_hash], 0, ctypes.byref(h)),
+                   "sha256_setup_create")
         self.ctx, self.n, self.h = ctx, n, h
+        ctx._check(ctx.lib.flock_setup_set_transcript(h, HASH[transcript]), "setup_set_transcript")
         self.n_log = max(3, (n - 1).bit_length())
         self._buf = np.zeros(MAX_PROOF_BYTES * 2, np.uint8)
 
@@ -701,16 +716,19 @@ class Prover:
     n_blocks, `Blake3Setup::new(n_blocks)` for any count (2^max(3, ceil(log2
     n)) slots, blake3.rs:1854-1858)."""
 
-    def __init__(self, ctx: Context, log2: int = None, n_blocks: int = None):
+    def __init__(self, ctx: Context, log2: int = None, n_blocks: int = None, merkle_hash: str = "blake3",
+                 transcript: str = "blake3"):
         h = ctypes.c_void_p()
+        mh = HASH[merkle_hash]
         if n_blocks is not None:
-            ctx._check(ctx.lib.flock_setup_create_blocks(ctx.h, n_blocks, 1, 0, ctypes.byref(h)), "setup_create_blocks")
+            ctx._check(ctx.lib.flock_setup_create_blocks(ctx.h, n_blocks, mh, 0, ctypes.byref(h)), "setup_create_blocks")
             log2 = max(3, (n_blocks - 1).bit_length())
         else:
-            ctx._check(ctx.lib.flock_setup_create(ctx.h, log2, 1, 0, ctypes.byref(h)), "setup_create")
+            ctx._check(ctx.lib.flock_setup_create(ctx.h, log2, mh, 0, ctypes.byref(h)), "setup_create")
             n_blocks = 1 << log2
         self.ctx, self.log2, self.n_blocks = ctx, log2, n_blocks
         self.h = h
+        ctx._check(ctx.lib.flock_setup_set_transcript(h, HASH[transcript]), "setup_set_transcript")
         self._buf = np.zeros(MAX_PROOF_BYTES * 2, np.uint8)
 
     def close(self) -> None:

@@ -74,7 +74,12 @@ enum {
   FLOCK_ERR_TIMEOUT = 5,
   FLOCK_ERR_VERIFY = 6
 };
-enum { FLOCK_HASH_BLAKE3 = 1 };
+/* The hash behind the PCS Merkle trees and the Fiat-Shamir transcript
+ * (HashKind, crates/flock-core/src/hash.rs:20-30, with its serde
+ * discriminants).  SHA-256 is the reference's default (FsChallenger::new,
+ * PcsParams::default); the benchmark uses BLAKE3 for both
+ * (benchmark-tools/worker/src/main.rs:23-29). */
+enum { FLOCK_HASH_SHA256 = 0, FLOCK_HASH_BLAKE3 = 1 };
 enum { FLOCK_PROFILE_FAST = 0 };
 
 int flock_ctx_create(int device, uint64_t hbm_budget_bytes, flock_ctx** out);
@@ -93,7 +98,9 @@ typedef struct flock_compression {
   uint32_t flags;
 } flock_compression;
 
-/* Untimed setup for 2^log2_n compressions (8 <= log2_n <= 20). */
+/* Untimed setup for 2^log2_n compressions (8 <= log2_n <= 20).  hash: the
+ * PCS Merkle hash (pcs_params.merkle_hash; the commitment records it).  The
+ * setup's transcript hash is BLAKE3 until flock_setup_set_transcript. */
 int flock_setup_create(flock_ctx* ctx, uint32_t log2_n, int hash, int profile, flock_setup** out);
 /* Untimed setup for n_blocks compressions, any count (Blake3Setup::new(n_blocks),
  * blake3.rs:4706-4780): the statement has 2^max(3, ceil(log2 n_blocks)) slots
@@ -102,6 +109,13 @@ int flock_setup_create(flock_ctx* ctx, uint32_t log2_n, int hash, int profile, f
  * below that, FLOCK_ERR_ARG here). */
 int flock_setup_create_blocks(flock_ctx* ctx, size_t n_blocks, int hash, int profile, flock_setup** out);
 void flock_setup_destroy(flock_setup* s);
+/* The transcript of this setup's proofs and of flock_verify on it:
+ * FsChallenger::with_hash(domain, hash) (challenger.rs:227-250; SHA-256:
+ * squeezes SHA256(state || ctr), PoW SHA256(digest || nonce)). */
+int flock_setup_set_transcript(flock_setup* s, int hash);
+/* The transcript hash of the context's verify-bundle entry points (the
+ * bundle records its Merkle hash but not its transcript's). */
+int flock_ctx_set_transcript(flock_ctx* ctx, int hash);
 
 /* One proof; inputs generated on the GPU from `seed` exactly as the
  * benchmark generator does.  Writes the FLOCK v4 bundle bytes. */
@@ -158,6 +172,8 @@ void flock_prover_data_destroy(flock_prover_data* pd);
  * challenger.rs:502-545).  A challenger is used by one thread at a time. */
 typedef struct flock_challenger flock_challenger;
 int flock_challenger_create(const uint8_t* domain, size_t dlen, flock_challenger** out);
+/* FsChallenger::with_hash(domain, hash); flock_challenger_create is BLAKE3. */
+int flock_challenger_create_hash(const uint8_t* domain, size_t dlen, int hash, flock_challenger** out);
 void flock_challenger_destroy(flock_challenger* ch);
 int flock_challenger_observe_label(flock_challenger* ch, const uint8_t* label, size_t len);
 int flock_challenger_observe_bytes(flock_challenger* ch, const uint8_t* bytes, size_t len);
@@ -272,6 +288,10 @@ int flock_witness(flock_ctx* ctx, uint32_t log2, uint64_t seed, uint64_t* z, uin
 int flock_ntt_rs_encode(flock_ctx* ctx, const uint64_t* msg, uint32_t log_msg_pos, uint32_t lanes,
                         uint32_t log_inv_rate, uint64_t* out);
 int flock_merkle_tree(flock_ctx* ctx, const uint8_t* data, size_t n_leaves, size_t leaf_size, uint8_t* tree_out);
+/* The same with the Merkle hash chosen (FLOCK_HASH_SHA256: leaf SHA256(bytes),
+ * parent SHA256(left || right); merkle.rs:205-230). */
+int flock_merkle_tree_hash(flock_ctx* ctx, const uint8_t* data, size_t n_leaves, size_t leaf_size, int hash,
+                           uint8_t* tree_out);
 /* NTT pass plans.  A plan splits the butterfly layers into passes over
  * shared-memory tiles (layers per pass, lanes per tile, threads per CTA);
  * flock_ntt_autotune times the candidate plans of a shape on this device and

@@ -330,6 +330,63 @@ int flockref_prove_sha256_merkle(const uint32_t* rec24, const uint8_t* b, const 
   }
 }
 
+// The hash kinds (0 SHA-256, 1 BLAKE3) of the proofs this thread makes next:
+// the PCS Merkle trees and the transcript (PcsParams::merkle_hash,
+// FsChallenger::with_hash).
+void flockref_set_hash_kinds(int merkle, int transcript) {
+  hash_kinds().merkle = merkle;
+  hash_kinds().transcript = transcript;
+}
+void flockref_sha256(const uint8_t* d, size_t n, uint8_t* out32) { sha::hash(d, n, out32); }
+void flockref_merkle_tree_hash(const uint8_t* data, size_t n_leaves, size_t leaf_size, int kind, uint8_t* tree_out) {
+  auto t = merkle_tree(data, n_leaves, leaf_size, kind);
+  memcpy(tree_out, t.data(), t.size() * 32);
+}
+void* flockref_ch_new_hash(const char* domain, int kind) { return new Challenger(domain, kind); }
+
+// ---- Keccak-f[1600].  A state is 25 u64 lanes (lane x + 5y, bit z).
+static_assert(sizeof(keccak::State) == 200, "keccak state");
+void flockref_keccak_f(uint64_t* lanes25) { keccak::permute(lanes25); }
+void flockref_keccak_bench_inputs(size_t n, uint64_t seed, uint64_t* out25) {
+  auto v = keccak::bench_inputs(n, seed);
+  memcpy(out25, v.data(), v.size() * sizeof(keccak::State));
+}
+void flockref_keccak_digest(uint32_t n_log, uint8_t* out32) { memcpy(out32, keccak_r1cs((int)n_log).digest.data(), 32); }
+// z, a, b: 2^(16 + n_log - 7) F128 each
+void flockref_keccak_witness(const uint64_t* states, size_t n, uint32_t n_log, uint64_t* z, uint64_t* a,
+                             uint64_t* b) {
+  std::vector<keccak::State> s(n);
+  memcpy(s.data(), states, n * sizeof(keccak::State));
+  std::vector<F128> vz, va, vb;
+  generate_keccak_witness(s, (int)n_log, vz, va, vb);
+  memcpy(z, vz.data(), vz.size() * 16);
+  memcpy(a, va.data(), va.size() * 16);
+  memcpy(b, vb.data(), vb.size() * 16);
+}
+// the walker's alpha A^T e + B^T e over 2^16 rows
+void flockref_keccak_comb(const uint64_t* alpha, const uint64_t* e, uint64_t* out) {
+  std::vector<F128> ev(keccak::K_KECCAK);
+  memcpy(ev.data(), e, ev.size() * 16);
+  auto c = keccak::lincheck_comb(F128(alpha[0], alpha[1]), ev);
+  memcpy(out, c.data(), c.size() * 16);
+}
+int flockref_prove_keccak(const uint64_t* states, size_t n, const uint8_t* domain, size_t dlen, uint8_t* out,
+                          size_t cap, size_t* out_len) {
+  try {
+    if (n == 0) return 3;
+    std::vector<keccak::State> s(n);
+    memcpy(s.data(), states, n * sizeof(keccak::State));
+    Bundle b = prove_keccak(s, keccak::min_n_log(n), std::string((const char*)domain, dlen));
+    std::vector<uint8_t> bytes = serialize(b);
+    *out_len = bytes.size();
+    if (bytes.size() > cap) return 2;
+    memcpy(out, bytes.data(), bytes.size());
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
 // Wall-clock seconds of one full oracle prove at log2 (for the CPU baseline).
 double flockref_time_prove(uint32_t log2, uint64_t seed, size_t* proof_len) {
   auto blocks = generate_compressions(log2, seed);

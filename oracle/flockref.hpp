@@ -104,11 +104,37 @@ void parent_cv(const uint8_t l[32], const uint8_t r[32], uint8_t out32[32]);
 using Hash = std::array<uint8_t, 32>;
 
 // ---------------------------------------------------------------------------
+// The hash behind Merkle trees and the transcript: HashKind
+// (crates/flock-core/src/hash.rs:20-30; Sha256 = 0 is the default).
+// ---------------------------------------------------------------------------
+enum HashKind : int { SHA256 = 0, BLAKE3 = 1 };
+namespace sha {
+// SHA-256 (FIPS 180-4) over bytes, incremental
+class Hasher {
+ public:
+  Hasher();
+  void update(const void* data, size_t len);
+  void finalize(uint8_t out32[32]) const;
+ private:
+  uint32_t h_[8];
+  uint8_t buf_[64];
+  size_t blen_ = 0;
+  uint64_t total_ = 0;
+};
+void hash(const void* data, size_t len, uint8_t out32[32]);
+}  // namespace sha
+// The hash kinds of the proofs the oracle makes on this thread (Merkle
+// trees, transcript); both BLAKE3 unless set (the benchmark's choice).
+struct HashKinds { int merkle = BLAKE3, transcript = BLAKE3; };
+HashKinds& hash_kinds();
+
+// ---------------------------------------------------------------------------
 // Fiat-Shamir challenger over BLAKE3.  crates/flock-core/src/challenger.rs:170-380
 // ---------------------------------------------------------------------------
 class Challenger {
  public:
-  explicit Challenger(const std::string& domain);
+  // FsChallenger::with_hash (challenger.rs:227-250)
+  explicit Challenger(const std::string& domain, int kind = BLAKE3);
   void observe_label(const std::string& label);
   void observe_f128(F128 v);
   void observe_f128_slice(const std::vector<F128>& v);
@@ -118,11 +144,20 @@ class Challenger {
   uint64_t grind_pow(uint32_t bits);           // smallest satisfying nonce
   bool verify_pow(uint64_t nonce, uint32_t bits);
   void state_digest(uint8_t out[32]) const;
+  int kind() const { return kind_; }
  private:
-  void absorb(const void* p, size_t n) { h_.update(p, n); }
+  void absorb(const void* p, size_t n) {
+    if (kind_ == SHA256) s_.update(p, n);
+    else h_.update(p, n);
+  }
+  // squeeze_into (challenger.rs:288-303)
+  void squeeze(uint8_t* out, size_t n) const;
+  int kind_ = BLAKE3;
   b3::Hasher h_;
+  sha::Hasher s_;
 };
-bool pow_ok(const uint8_t digest[32], uint64_t nonce, uint32_t bits);
+// pow_has_leading_zero_bits (challenger.rs:580-601)
+bool pow_ok(const uint8_t digest[32], uint64_t nonce, uint32_t bits, int kind = BLAKE3);
 
 // ---------------------------------------------------------------------------
 // BLAKE3 compression R1CS.  crates/flock-prover/src/r1cs_hashes/blake3.rs
@@ -142,6 +177,7 @@ struct SparseRows { std::vector<uint32_t> ptr; std::vector<uint16_t> col; };  //
 struct R1cs {
   int m = 0, n_log = 0;
   int k_log = K_LOG, z_const = Z_CONST_POS;  // block size and the pinned constant column
+  bool walker = false;  // the lincheck marginal comes from the Keccak walker, not a0 / b0
   SparseRows a0, b0;
   std::array<uint8_t, 32> digest{};
 };
@@ -181,6 +217,32 @@ void build_matrices(SparseRows& a, SparseRows& b);
 void block_witness(const Compression& c, uint64_t* z);
 }  // namespace sha
 const R1cs& sha256_r1cs(int n_log);
+
+// ---------------------------------------------------------------------------
+// Keccak-f[1600] R1CS.  crates/flock-prover/src/r1cs_hashes/keccak.rs (one
+// permutation per 2^16-bit block; implicit matrices and a lincheck walker).
+// ---------------------------------------------------------------------------
+namespace keccak {
+constexpr int K_LOG_KECCAK = 16;
+constexpr int K_KECCAK = 1 << K_LOG_KECCAK;
+constexpr int Z_CONST = 4096;
+constexpr int T_BASE = 4160;
+constexpr int USEFUL_BITS = T_BASE + 24 * 1600;  // 42,560
+extern const uint64_t RC[24];
+struct State { uint64_t lanes[25]; };  // lane x + 5y, bit z
+// Keccak-f[1600] (FIPS 202) on lanes, in place
+void permute(uint64_t lanes[25]);
+// benches/keccak3_proof.rs:80-93: 25 SplitMix64 draws per state, bit i (index
+// x + 5y + 25z) = bit i mod 64 of draw i / 64
+std::vector<State> bench_inputs(size_t n, uint64_t seed);
+int min_n_log(size_t n);  // keccak.rs:508-514
+void block_witness(const State& in, uint64_t* z, uint64_t* a, uint64_t* b);
+// fold_alpha_batched: alpha A^T e + B^T e for e over the block's 2^16 rows
+std::vector<F128> lincheck_comb(F128 alpha, const std::vector<F128>& e);
+}  // namespace keccak
+const R1cs& keccak_r1cs(int n_log);
+void generate_keccak_witness(const std::vector<keccak::State>& states, int n_log, std::vector<F128>& z,
+                             std::vector<F128>& a, std::vector<F128>& b);
 // z by the boolean witness (padding blocks: the all-zero (h_in, m)
 // compression), a = A_0 z and b = B_0 z from the matrices
 void generate_sha256_witness(const std::vector<sha::Compression>& blocks, int n_log, std::vector<F128>& z,
@@ -212,7 +274,9 @@ struct Gf8Ntt {
 // ---------------------------------------------------------------------------
 // Merkle (BLAKE3 leaf/parent CVs, flat 2n-1 layout).  merkle.rs:16-21,192-240,753-1072
 // ---------------------------------------------------------------------------
-std::vector<Hash> merkle_tree(const uint8_t* data, size_t n_leaves, size_t leaf_size);
+// hash_leaf / hash_pair (merkle.rs:205-230): BLAKE3 non-root chaining
+// values, or SHA256(leaf) and SHA256(left || right)
+std::vector<Hash> merkle_tree(const uint8_t* data, size_t n_leaves, size_t leaf_size, int kind = BLAKE3);
 std::vector<Hash> merkle_multi_proof(const std::vector<Hash>& tree, size_t n_leaves,
                                      std::vector<size_t> positions);
 
@@ -288,6 +352,8 @@ Bundle prove_core(const R1cs& rc, std::vector<F128> z, const std::vector<F128>& 
                   const std::string& domain, const CoreHook& after_core);
 // Sha256HybridSetup::prove_fast (sha2.rs:1377-1408) over 2^n_log blocks
 Bundle prove_sha256(const std::vector<sha::Compression>& blocks, int n_log, const std::string& domain);
+// KeccakSetup::prove_fast (keccak.rs:956-978); padding: keccak_f(0)
+Bundle prove_keccak(const std::vector<keccak::State>& states, int n_log, const std::string& domain);
 // sum_j bc[j] * z[j] == target (the batched open's claim)
 bool open_identity(const std::vector<F128>& z, const std::vector<F128>& bc, F128 target);
 // that identity, as checked by the last prove_with with a hook on this thread

@@ -1,0 +1,262 @@
+// Keccak-f[1600] R1CS of the oracle (test infrastructure; see flockref.hpp).
+// Restates crates/flock-prover/src/r1cs_hashes/keccak.rs:
+//  * Keccak-f[1600] over 1600 state bits (FIPS 202 3.2: theta, rho, pi,
+//    chi, iota), bit index x + 5y + 25z (:78-82), RHO_OFFSETS and
+//    ROUND_CONSTANTS (:39-75), theta_rho_pi_preimage (:89-117);
+//  * the monolithic encoder at K_LOG = 16 (:430-560): state_0 in slot 0,
+//    state_24 in slot 1 (2048-bit slots, lane-contiguous: bit j of a state at
+//    64 (j mod 25) + j / 25), the constant at bit 4096, t_0..t_23 from bit
+//    4160; rows: constant (1,1,1), state_0 (v, v, 1), t_r = chi AND
+//    (~B[x+1], B[x+2]) with B = pi(rho(theta(state_r))), state_24 pin
+//    (v, v, 1); padding blocks hold keccak_f of the zero state (:562-676);
+//  * the lincheck walker KeccakLincheckCircuit::fold_alpha_batched (:681-828),
+//    the column marginal alpha A^T e + B^T e of the implicit matrices;
+//  * the empty-stub statement (common.rs:120-138: A_0 = B_0 empty, C_0 = I);
+//  * the keccak3_proof bench inputs (benches/keccak3_proof.rs:66-93, 114-124).
+// Unlike the product, the oracle evaluates the permutation bit by bit on
+// 1600-bit states.
+#include "flockref.hpp"
+#include <map>
+#include <memory>
+#include <mutex>
+
+namespace flockref {
+namespace keccak {
+
+namespace {
+const int RHO[5][5] = {{0, 36, 3, 41, 18}, {1, 44, 10, 45, 2}, {62, 6, 43, 15, 61}, {28, 55, 25, 21, 56},
+                       {27, 20, 39, 8, 14}};
+inline int sidx(int x, int y, int z) { return x + 5 * y + 25 * z; }
+using Bits = std::vector<uint8_t>;  // 1600 state bits, 0/1
+
+// the 11 state_in bits whose XOR is B[x, y, z], B = pi(rho(theta(A)))
+std::array<int, 11> preimage(int x, int y, int z) {
+  const int a = (x + 3 * y) % 5, b = x, r = RHO[a][b] % 64;
+  const int c = (z + 64 - r) % 64, cp = (c + 63) % 64;
+  std::array<int, 11> out;
+  out[0] = sidx(a, b, c);
+  for (int yp = 0; yp < 5; yp++) out[1 + yp] = sidx((a + 4) % 5, yp, c);
+  for (int yp = 0; yp < 5; yp++) out[6 + yp] = sidx((a + 1) % 5, yp, cp);
+  return out;
+}
+Bits phi(const Bits& s) {  // pi o rho o theta
+  Bits o(1600, 0);
+  for (int z = 0; z < 64; z++)
+    for (int y = 0; y < 5; y++)
+      for (int x = 0; x < 5; x++) {
+        uint8_t v = 0;
+        for (int k : preimage(x, y, z)) v ^= s[k];
+        o[sidx(x, y, z)] = v;
+      }
+  return o;
+}
+int lane_pos(int j) { return 64 * (j % 25) + j / 25; }  // within_lane_contiguous
+}  // namespace
+
+const uint64_t RC[24] = {
+    0x0000000000000001ull, 0x0000000000008082ull, 0x800000000000808Aull, 0x8000000080008000ull,
+    0x000000000000808Bull, 0x0000000080000001ull, 0x8000000080008081ull, 0x8000000000008009ull,
+    0x000000000000008Aull, 0x0000000000000088ull, 0x0000000080008009ull, 0x000000008000000Aull,
+    0x000000008000808Bull, 0x800000000000008Bull, 0x8000000000008089ull, 0x8000000000008003ull,
+    0x8000000000008002ull, 0x8000000000000080ull, 0x000000000000800Aull, 0x800000008000000Aull,
+    0x8000000080008081ull, 0x8000000000008080ull, 0x0000000080000001ull, 0x8000000080008008ull};
+
+void permute(uint64_t lanes[25]) {
+  Bits s(1600);
+  for (int j = 0; j < 1600; j++) s[j] = (lanes[j % 25] >> (j / 25)) & 1;
+  for (int r = 0; r < 24; r++) {
+    const Bits b = phi(s);
+    for (int z = 0; z < 64; z++)
+      for (int y = 0; y < 5; y++)
+        for (int x = 0; x < 5; x++)
+          s[sidx(x, y, z)] = b[sidx(x, y, z)] ^ ((b[sidx((x + 1) % 5, y, z)] ^ 1) & b[sidx((x + 2) % 5, y, z)]);
+    for (int z = 0; z < 64; z++) s[sidx(0, 0, z)] ^= (RC[r] >> z) & 1;
+  }
+  for (int l = 0; l < 25; l++) {
+    lanes[l] = 0;
+    for (int z = 0; z < 64; z++) lanes[l] |= (uint64_t)s[l + 25 * z] << z;
+  }
+}
+
+std::vector<State> bench_inputs(size_t n, uint64_t seed) {
+  uint64_t st = seed;
+  auto nx = [&]() {
+    st += 0x9E3779B97F4A7C15ull;
+    uint64_t z = st;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  std::vector<State> out(n);
+  for (auto& s : out) {
+    uint64_t draws[25];
+    for (int w = 0; w < 25; w++) draws[w] = nx();
+    // bit i of the state (index x + 5y + 25z) is bit i mod 64 of draw i / 64
+    for (int l = 0; l < 25; l++) {
+      s.lanes[l] = 0;
+      for (int z = 0; z < 64; z++) {
+        const int i = l + 25 * z;
+        s.lanes[l] |= ((draws[i / 64] >> (i % 64)) & 1) << z;
+      }
+    }
+  }
+  return out;
+}
+
+int min_n_log(size_t n) {
+  size_t p = 8;
+  int l = 3;
+  while (p < n) { p <<= 1; l++; }
+  return l;
+}
+
+void block_witness(const State& in, uint64_t* z, uint64_t* a, uint64_t* b) {
+  Bits s(1600);
+  for (int j = 0; j < 1600; j++) s[j] = (in.lanes[j % 25] >> (j / 25)) & 1;
+  auto put = [](uint64_t* v, int pos, uint8_t bit) { if (bit) v[pos >> 6] |= 1ull << (pos & 63); };
+  put(z, Z_CONST, 1);
+  put(a, Z_CONST, 1);
+  put(b, Z_CONST, 1);
+  for (int j = 0; j < 1600; j++) {
+    put(z, lane_pos(j), s[j]);
+    put(a, lane_pos(j), s[j]);
+    put(b, lane_pos(j), 1);
+  }
+  for (int r = 0; r < 24; r++) {
+    const Bits bs = phi(s);
+    for (int zz = 0; zz < 64; zz++)
+      for (int y = 0; y < 5; y++)
+        for (int x = 0; x < 5; x++) {
+          const int j = sidx(x, y, zz), pos = T_BASE + 1600 * r + lane_pos(j);
+          const uint8_t l = bs[sidx((x + 1) % 5, y, zz)] ^ 1, rr = bs[sidx((x + 2) % 5, y, zz)];
+          put(z, pos, l & rr);
+          put(a, pos, l);
+          put(b, pos, rr);
+          s[j] = bs[j] ^ (l & rr);
+        }
+    for (int zz = 0; zz < 64; zz++) s[sidx(0, 0, zz)] ^= (RC[r] >> zz) & 1;
+  }
+  for (int j = 0; j < 1600; j++) {
+    put(z, 2048 + lane_pos(j), s[j]);
+    put(a, 2048 + lane_pos(j), s[j]);
+    put(b, 2048 + lane_pos(j), 1);
+  }
+}
+
+std::vector<F128> lincheck_comb(F128 alpha, const std::vector<F128>& e) {
+  std::vector<F128> comb(K_KECCAK, ZERO);
+  auto t_pos = [](int r, int j) { return T_BASE + 1600 * r + lane_pos(j); };
+  // constant row: A = B = [const]
+  comb[Z_CONST] += alpha * e[Z_CONST] + e[Z_CONST];
+  // state_0 rows: A = [row], B = [const]
+  for (int j = 0; j < 1600; j++) {
+    comb[lane_pos(j)] += alpha * e[lane_pos(j)];
+    comb[Z_CONST] += e[lane_pos(j)];
+  }
+  // state_24 pin rows: A = L_24[j] (through the recurrence below), B = [const]
+  std::vector<F128> pin(1600);
+  for (int j = 0; j < 1600; j++) {
+    pin[j] = e[2048 + lane_pos(j)];
+    comb[Z_CONST] += pin[j];
+  }
+  // chi rows of round r: A = 1 + B[x+1], B = B[x+2]; their marginals on state_r
+  std::vector<std::vector<F128>> ca(24, std::vector<F128>(1600, ZERO)), cb = ca;
+  F128 sum_t = ZERO;
+  for (int r = 0; r < 24; r++)
+    for (int zz = 0; zz < 64; zz++)
+      for (int y = 0; y < 5; y++)
+        for (int x = 0; x < 5; x++) {
+          const F128 ev = e[t_pos(r, sidx(x, y, zz))];
+          sum_t += ev;
+          for (int k : preimage((x + 1) % 5, y, zz)) ca[r][k] += ev;
+          for (int k : preimage((x + 2) % 5, y, zz)) cb[r][k] += ev;
+        }
+  comb[Z_CONST] += alpha * sum_t;
+  // the round constants' share: state_r = phi^r state_0 + ... + RC_r
+  Bits rc(1600, 0);
+  F128 rca = ZERO, rcb = ZERO;
+  for (int r = 0; r < 24; r++) {
+    for (int k = 0; k < 1600; k++)
+      if (rc[k]) { rca += ca[r][k]; rcb += cb[r][k]; }
+    rc = phi(rc);
+    for (int zz = 0; zz < 64; zz++) rc[sidx(0, 0, zz)] ^= (RC[r] >> zz) & 1;
+  }
+  F128 rcp = ZERO;
+  for (int k = 0; k < 1600; k++)
+    if (rc[k]) rcp += pin[k];
+  comb[Z_CONST] += alpha * rca + rcb + alpha * rcp;
+  // phi^T
+  auto phi_t = [](const std::vector<F128>& v) {
+    std::vector<F128> o(1600, ZERO);
+    for (int zz = 0; zz < 64; zz++)
+      for (int y = 0; y < 5; y++)
+        for (int x = 0; x < 5; x++)
+          for (int k : preimage(x, y, zz)) o[k] += v[sidx(x, y, zz)];
+    return o;
+  };
+  // A side: K_24 = pin -> t_23; K_r = phi^T(K_{r+1}) + chi_A(r) -> t_{r-1}; K_0 -> state_0
+  for (int j = 0; j < 1600; j++) comb[t_pos(23, j)] += alpha * pin[j];
+  std::vector<F128> k = phi_t(pin);
+  for (int j = 0; j < 1600; j++) k[j] += ca[23][j];
+  for (int r = 23; r >= 1; r--) {
+    for (int j = 0; j < 1600; j++) comb[t_pos(r - 1, j)] += alpha * k[j];
+    std::vector<F128> nk = phi_t(k);
+    for (int j = 0; j < 1600; j++) nk[j] += ca[r - 1][j];
+    k = nk;
+  }
+  for (int j = 0; j < 1600; j++) comb[lane_pos(j)] += alpha * k[j];
+  // B side: K_23 = chi_B(23)
+  k = cb[23];
+  for (int r = 23; r >= 1; r--) {
+    for (int j = 0; j < 1600; j++) comb[t_pos(r - 1, j)] += k[j];
+    std::vector<F128> nk = phi_t(k);
+    for (int j = 0; j < 1600; j++) nk[j] += cb[r - 1][j];
+    k = nk;
+  }
+  for (int j = 0; j < 1600; j++) comb[lane_pos(j)] += k[j];
+  return comb;
+}
+
+}  // namespace keccak
+
+const R1cs& keccak_r1cs(int n_log) {
+  static std::mutex mu;
+  static std::map<int, std::unique_ptr<R1cs>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(n_log);
+  if (it != cache.end()) return *it->second;
+  std::unique_ptr<R1cs> r(new R1cs());
+  r->n_log = n_log;
+  r->k_log = keccak::K_LOG_KECCAK;
+  r->z_const = keccak::Z_CONST;
+  r->m = r->k_log + n_log;
+  r->a0.ptr.assign(keccak::K_KECCAK + 1, 0);
+  r->b0.ptr.assign(keccak::K_KECCAK + 1, 0);
+  r->walker = true;
+  r->digest = statement_digest(r->m, r->k_log, K_SKIP, r->a0, r->b0);
+  const R1cs& ref = *r;
+  cache[n_log] = std::move(r);
+  return ref;
+}
+
+void generate_keccak_witness(const std::vector<keccak::State>& states, int n_log, std::vector<F128>& z,
+                             std::vector<F128>& a, std::vector<F128>& b) {
+  const size_t n_total = (size_t)1 << n_log, per = keccak::K_KECCAK / 128;
+  z.assign(n_total * per, ZERO);
+  a.assign(n_total * per, ZERO);
+  b.assign(n_total * per, ZERO);
+  const keccak::State pad{};
+  par_for(n_total, [&](size_t o0, size_t o1, int) {
+    for (size_t o = o0; o < o1; o++)
+      keccak::block_witness(o < states.size() ? states[o] : pad, (uint64_t*)&z[o * per], (uint64_t*)&a[o * per],
+                            (uint64_t*)&b[o * per]);
+  });
+}
+
+Bundle prove_keccak(const std::vector<keccak::State>& states, int n_log, const std::string& domain) {
+  std::vector<F128> z, a, b;
+  generate_keccak_witness(states, n_log, z, a, b);
+  return prove_core(keccak_r1cs(n_log), std::move(z), a, b, domain, CoreHook());
+}
+
+}  // namespace flockref

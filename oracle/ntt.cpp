@@ -136,17 +136,28 @@ void Gf8Ntt::forward(uint8_t* v) const { fft_rec(v, (size_t)1 << k, tw.data(), 1
 void Gf8Ntt::inverse(uint8_t* v) const { ifft_rec(v, (size_t)1 << k, tw.data(), 1); }
 
 // ---- Merkle ----
-std::vector<Hash> merkle_tree(const uint8_t* data, size_t n_leaves, size_t leaf_size) {
+std::vector<Hash> merkle_tree(const uint8_t* data, size_t n_leaves, size_t leaf_size, int kind) {
   std::vector<Hash> tree(2 * n_leaves - 1);
   par_for(n_leaves, [&](size_t i0, size_t i1, int) {
-    for (size_t i = i0; i < i1; i++) b3::leaf_cv(data + i * leaf_size, leaf_size, tree[i].data());
+    for (size_t i = i0; i < i1; i++) {
+      if (kind == SHA256) sha::hash(data + i * leaf_size, leaf_size, tree[i].data());
+      else b3::leaf_cv(data + i * leaf_size, leaf_size, tree[i].data());
+    }
   });
   size_t rs = 0, rl = n_leaves;
   while (rl > 1) {
     size_t nl = rl >> 1;
     par_for(nl, [&](size_t j0, size_t j1, int) {
-      for (size_t j = j0; j < j1; j++)
-        b3::parent_cv(tree[rs + 2 * j].data(), tree[rs + 2 * j + 1].data(), tree[rs + rl + j].data());
+      for (size_t j = j0; j < j1; j++) {
+        if (kind == SHA256) {
+          uint8_t lr[64];
+          memcpy(lr, tree[rs + 2 * j].data(), 32);
+          memcpy(lr + 32, tree[rs + 2 * j + 1].data(), 32);
+          sha::hash(lr, 64, tree[rs + rl + j].data());
+        } else {
+          b3::parent_cv(tree[rs + 2 * j].data(), tree[rs + 2 * j + 1].data(), tree[rs + rl + j].data());
+        }
+      }
     });
     rs += rl;
     rl = nl;

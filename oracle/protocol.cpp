@@ -305,10 +305,14 @@ static LincheckProof lincheck_prove(const std::vector<F128>& zp, int m, const R1
   for (int ir = 0; ir < (int)eqr.size(); ir++)
     for (int is = 0; is < 64; is++) eq_inner[is + 64 * ir] = lam[is] * eqr[ir];
   std::vector<F128> comb(K, ZERO);
-  for (int row = 0; row < K; row++) {
-    F128 ea = alpha * eq_inner[row], e = eq_inner[row];
-    for (uint32_t j = rc.a0.ptr[row]; j < rc.a0.ptr[row + 1]; j++) comb[rc.a0.col[j]] += ea;
-    for (uint32_t j = rc.b0.ptr[row]; j < rc.b0.ptr[row + 1]; j++) comb[rc.b0.col[j]] += e;
+  if (rc.walker) {
+    comb = keccak::lincheck_comb(alpha, eq_inner);
+  } else {
+    for (int row = 0; row < K; row++) {
+      F128 ea = alpha * eq_inner[row], e = eq_inner[row];
+      for (uint32_t j = rc.a0.ptr[row]; j < rc.a0.ptr[row + 1]; j++) comb[rc.a0.col[j]] += ea;
+      for (uint32_t j = rc.b0.ptr[row]; j < rc.b0.ptr[row + 1]; j++) comb[rc.b0.col[j]] += e;
+    }
   }
   F128 beta = ch.sample_f128();
   comb[rc.z_const] += beta;
@@ -394,12 +398,17 @@ struct LigeroLevel {
   size_t block_len = 0, lanes = 0;
 };
 
+HashKinds& hash_kinds() {
+  static thread_local HashKinds k;
+  return k;
+}
+
 static LigeroLevel ligero_commit(const std::vector<F128>& poly, int log_lanes, int log_inv_rate) {
   LigeroLevel lv;
   lv.lanes = (size_t)1 << log_lanes;
   rs_encode(poly, lv.lanes, log_inv_rate, lv.cw);
   lv.block_len = lv.cw.size() / lv.lanes;
-  lv.tree = merkle_tree((const uint8_t*)lv.cw.data(), lv.block_len, lv.lanes * 16);
+  lv.tree = merkle_tree((const uint8_t*)lv.cw.data(), lv.block_len, lv.lanes * 16, hash_kinds().merkle);
   return lv;
 }
 
@@ -777,8 +786,9 @@ Bundle prove_core(const R1cs& rc, std::vector<F128> z, const std::vector<F128>& 
   Bundle bd;
   bd.root = l0.tree.back();
   bd.m = (uint64_t)m;
+  bd.merkle_hash = (uint32_t)hash_kinds().merkle;
 
-  Challenger ch(domain);
+  Challenger ch(domain, hash_kinds().transcript);
   ch.observe_label("flock-r1cs-v0");
   ch.observe_bytes(rc.digest.data(), 32);
   ch.observe_bytes(bd.root.data(), 32);

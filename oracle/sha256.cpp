@@ -189,6 +189,43 @@ std::vector<Compression> bench_inputs(size_t n, uint64_t seed) {
   return v;
 }
 
+Hasher::Hasher() { memcpy(h_, IV, 32); }
+void Hasher::update(const void* data, size_t len) {
+  const uint8_t* p = static_cast<const uint8_t*>(data);
+  total_ += len;
+  for (size_t i = 0; i < len; i++) {
+    buf_[blen_++] = p[i];
+    if (blen_ == 64) {
+      uint32_t m[16];
+      for (int k = 0; k < 16; k++)
+        m[k] = (uint32_t)buf_[4 * k] << 24 | (uint32_t)buf_[4 * k + 1] << 16 | (uint32_t)buf_[4 * k + 2] << 8 |
+               (uint32_t)buf_[4 * k + 3];
+      uint32_t out[8];
+      compress(h_, m, out);
+      memcpy(h_, out, 32);
+      blen_ = 0;
+    }
+  }
+}
+void Hasher::finalize(uint8_t out32[32]) const {
+  Hasher s = *this;
+  const uint64_t bits = total_ * 8;
+  const uint8_t one = 0x80, zero = 0;
+  s.update(&one, 1);
+  while (s.blen_ != 56) s.update(&zero, 1);
+  for (int i = 7; i >= 0; i--) {
+    const uint8_t b = (uint8_t)(bits >> (8 * i));
+    s.update(&b, 1);
+  }
+  for (int w = 0; w < 8; w++)
+    for (int k = 0; k < 4; k++) out32[4 * w + k] = (uint8_t)(s.h_[w] >> (24 - 8 * k));
+}
+void hash(const void* data, size_t len, uint8_t out32[32]) {
+  Hasher h;
+  h.update(data, len);
+  h.finalize(out32);
+}
+
 int min_n_blocks_log(size_t n) {
   size_t p = 8;
   int l = 3;

@@ -16,7 +16,7 @@ static void le64(uint64_t v, uint8_t out[8]) {
   for (int i = 0; i < 8; i++) out[i] = (uint8_t)(v >> (8 * i));
 }
 
-Challenger::Challenger(const std::string& domain) {
+Challenger::Challenger(const std::string& domain, int kind) : kind_(kind) {
   uint8_t op = OP_DOMAIN, len[8];
   le64(domain.size(), len);
   absorb(&op, 1);
@@ -73,7 +73,7 @@ static F128 f128_from_le(const uint8_t* b) {
 F128 Challenger::sample_f128() {
   uint8_t tag[2] = {OP_SQUEEZE, KIND_SCALAR}, buf[16];
   absorb(tag, 2);
-  h_.finalize_xof(buf, 16);
+  squeeze(buf, 16);
   absorb(buf, 16);
   return f128_from_le(buf);
 }
@@ -84,21 +84,42 @@ std::vector<F128> Challenger::sample_f128_vec(size_t n) {
   absorb(tag, 2);
   absorb(len, 8);
   std::vector<uint8_t> buf(n * 16);
-  if (n) h_.finalize_xof(buf.data(), buf.size());
+  if (n) squeeze(buf.data(), buf.size());
   absorb(buf.data(), buf.size());
   std::vector<F128> out(n);
   for (size_t i = 0; i < n; i++) out[i] = f128_from_le(&buf[16 * i]);
   return out;
 }
 
-void Challenger::state_digest(uint8_t out[32]) const { h_.finalize(out); }
+void Challenger::state_digest(uint8_t out[32]) const {
+  if (kind_ == SHA256) s_.finalize(out);
+  else h_.finalize(out);
+}
 
-bool pow_ok(const uint8_t digest[32], uint64_t nonce, uint32_t bits) {
+// BLAKE3: the XOF of the state; SHA-256: SHA256(state || ctr LE), 32 bytes
+// per counter value
+void Challenger::squeeze(uint8_t* out, size_t n) const {
+  if (kind_ != SHA256) {
+    h_.finalize_xof(out, n);
+    return;
+  }
+  for (uint64_t ctr = 0; 32 * ctr < n; ctr++) {
+    sha::Hasher s = s_;
+    uint8_t c[8], blk[32];
+    le64(ctr, c);
+    s.update(c, 8);
+    s.finalize(blk);
+    memcpy(out + 32 * ctr, blk, std::min<size_t>(32, n - 32 * ctr));
+  }
+}
+
+bool pow_ok(const uint8_t digest[32], uint64_t nonce, uint32_t bits, int kind) {
   uint8_t pre[64] = {0};
   memcpy(pre, digest, 32);
   le64(nonce, pre + 32);
   uint8_t h[32];
-  b3::hash(pre, 64, h);
+  if (kind == SHA256) sha::hash(pre, 40, h);  // digest || nonce, no padding
+  else b3::hash(pre, 64, h);
   uint32_t full = bits / 8, extra = bits % 8;
   for (uint32_t i = 0; i < full; i++)
     if (h[i] != 0) return false;
@@ -111,7 +132,7 @@ uint64_t Challenger::grind_pow(uint32_t bits) {
   if (bits != 0) {
     uint8_t d[32];
     state_digest(d);
-    while (!pow_ok(d, nonce, bits)) nonce++;
+    while (!pow_ok(d, nonce, bits, kind_)) nonce++;
   }
   uint8_t b[8];
   le64(nonce, b);
@@ -122,7 +143,7 @@ uint64_t Challenger::grind_pow(uint32_t bits) {
 bool Challenger::verify_pow(uint64_t nonce, uint32_t bits) {
   uint8_t d[32];
   state_digest(d);
-  bool ok = bits == 0 ? nonce == 0 : pow_ok(d, nonce, bits);
+  bool ok = bits == 0 ? nonce == 0 : pow_ok(d, nonce, bits, kind_);
   uint8_t b[8];
   le64(nonce, b);
   observe_bytes(b, 8);

@@ -55,12 +55,20 @@
    check: the shift argument verified from the public leaves and root, and
    the batched open's claim identity.
 
+10. default_hash_proofs.json (--default-hashes) — proofs of the oracle with
+   the SHA-256 Merkle hash and / or the SHA-256 transcript (the reference's
+   defaults: PcsParams::default, FsChallenger::new): the SHA-256 statement
+   over the sha2_proof bench inputs at n = 256 and 4096, and the BLAKE3
+   statement over the benchmark inputs at 2^8 and 2^12 compressions, each with
+   the hash pair named in the entry.
+
 Usage (a built oracle; REFERENCE is a checkout of the reference project):
     python tests/golden/make_golden.py --ref REFERENCE [--large]
     python tests/golden/make_golden.py --chain
     python tests/golden/make_golden.py --kernels
     python tests/golden/make_golden.py --sha256
     python tests/golden/make_golden.py --sha256-merkle
+    python tests/golden/make_golden.py --default-hashes
     python tests/golden/make_golden.py --gpu-harness VERIFIER --sizes 19:2,20:2 --out FILE
 """
 import hashlib
@@ -243,6 +251,35 @@ def sha256_merkle_proofs(threads=8) -> None:
         (HERE / "sha256_merkle_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
 
 
+DEFAULT_HASH_CASES = (("sha256", 256, "sha256", "sha256"), ("sha256", 4096, "sha256", "sha256"),
+                      ("blake3", 8, "sha256", "sha256"), ("blake3", 12, "sha256", "sha256"),
+                      ("blake3", 8, "sha256", "blake3"), ("blake3", 8, "blake3", "sha256"))
+
+
+def default_hash_proofs(threads=8) -> None:
+    import os
+    os.environ["FLOCKREF_THREADS"] = str(threads)
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle_lib
+    orc = oracle_lib.Oracle()
+    out = []
+    for statement, size, merkle, transcript in DEFAULT_HASH_CASES:
+        orc.set_hash_kinds(merkle, transcript)
+        if statement == "sha256":
+            seed = 0xC0FFEE_5A55 ^ size
+            data = orc.prove_sha256(orc.sha256_bench_inputs(size, seed))
+            e = {"statement": "sha256", "n": size, "seed": seed}
+        else:
+            seed = 0x5EED0000 + size
+            data = orc.prove(size, seed)
+            e = {"statement": "blake3", "log2": size, "seed": seed}
+        e.update({"merkle_hash": merkle, "transcript": transcript, "domain": "flock-bench-v0",
+                  "sha256": hashlib.sha256(data).hexdigest(), "size": len(data)})
+        out.append(e)
+        (HERE / "default_hash_proofs.json").write_text(json.dumps(out, indent=1))
+    orc.set_hash_kinds()
+
+
 if __name__ == "__main__":
     import argparse
     ap = argparse.ArgumentParser()
@@ -252,6 +289,7 @@ if __name__ == "__main__":
     ap.add_argument("--kernels", action="store_true")
     ap.add_argument("--sha256", action="store_true")
     ap.add_argument("--sha256-merkle", action="store_true")
+    ap.add_argument("--default-hashes", action="store_true")
     ap.add_argument("--gpu-harness", type=Path, metavar="VERIFIER")
     ap.add_argument("--sizes", default="19:2,20:2", help="LOG2:RUNS,... for --gpu-harness")
     ap.add_argument("--out", type=Path, default=HERE / "gpu_verified_proofs.json")
@@ -262,6 +300,8 @@ if __name__ == "__main__":
         sha256_proofs()
     elif a.sha256_merkle:
         sha256_merkle_proofs()
+    elif a.default_hashes:
+        default_hash_proofs()
     elif a.kernels:
         kernel_digests()
     elif a.gpu_harness:

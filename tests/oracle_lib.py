@@ -69,6 +69,11 @@ class Oracle:
         L.flockref_prove_sha256.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_prove_sha256_zero.argtypes = [u32, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_sha256_merkle_inputs.argtypes = [u32, u32, u64, vp, vp, vp, vp]
+        L.flockref_set_hash_kinds.argtypes = [i32, i32]
+        L.flockref_sha256.argtypes = [ctypes.c_char_p, sz, vp]
+        L.flockref_ch_new_hash.argtypes = [ctypes.c_char_p, i32]
+        L.flockref_ch_new_hash.restype = vp
+        L.flockref_merkle_tree_hash.argtypes = [vp, sz, sz, i32, vp]
         L.flockref_prove_sha256_merkle.argtypes = [vp, vp, vp, vp, u32, u32, ctypes.c_char_p, sz, vp, sz,
                                                    ctypes.POINTER(sz), ctypes.POINTER(ctypes.c_int)]
         L.flockref_prove_chain_blocks.argtypes = [vp, u32, ctypes.c_char_p, sz, vp, vp, sz, ctypes.POINTER(sz),
@@ -77,6 +82,22 @@ class Oracle:
         L.flockref_time_prove.argtypes = [u32, u64, ctypes.POINTER(sz)]
         L.flockref_time_prove.restype = ctypes.c_double
         self.L = L
+
+    # ---- hash kinds (0 SHA-256, 1 BLAKE3) of the next proofs on this thread
+    def set_hash_kinds(self, merkle: str = "blake3", transcript: str = "blake3") -> None:
+        k = {"sha256": 0, "blake3": 1}
+        self.L.flockref_set_hash_kinds(k[merkle], k[transcript])
+
+    def sha256(self, data: bytes) -> bytes:
+        out = np.zeros(32, np.uint8)
+        self.L.flockref_sha256(data, len(data), _p(out))
+        return out.tobytes()
+
+    def merkle_tree_hash(self, data: np.ndarray, n_leaves: int, leaf_size: int, hash: str) -> np.ndarray:
+        data = np.ascontiguousarray(data, np.uint8)
+        out = np.zeros((2 * n_leaves - 1) * 32, np.uint8)
+        self.L.flockref_merkle_tree_hash(_p(data), n_leaves, leaf_size, {"sha256": 0, "blake3": 1}[hash], _p(out))
+        return out
 
     # ---- SHA-256 compressions (r1cs_hashes/sha2.rs)
     def sha256_compress(self, h, m) -> np.ndarray:
@@ -269,14 +290,38 @@ class Oracle:
         self.L.flockref_lagrange(_p(z), node_base, _p(out))
         return out
 
-    def grind(self, domain: bytes, label: bytes, bits: int) -> tuple:
-        c = self.L.flockref_ch_new(domain)
+    def grind(self, domain: bytes, label: bytes, bits: int, hash: str = "blake3") -> tuple:
+        c = self.L.flockref_ch_new_hash(domain, {"sha256": 0, "blake3": 1}[hash])
         self.L.flockref_ch_label(c, label)
         d = np.zeros(32, np.uint8)
         self.L.flockref_ch_digest(c, _p(d))
         n = self.L.flockref_ch_grind(c, bits)
         self.L.flockref_ch_free(c)
         return d.tobytes(), n
+
+    def challenger_script(self, domain: bytes, hash: str) -> list:
+        """The fixed op script of the transcript tests; returns every sample
+        and the final state digest."""
+        c = self.L.flockref_ch_new_hash(domain, {"sha256": 0, "blake3": 1}[hash])
+        out = []
+        self.L.flockref_ch_label(c, b"flock-test-label")
+        v = np.array([0x0123456789ABCDEF, 0xFEDCBA9876543210], np.uint64)
+        self.L.flockref_ch_observe(c, _p(v))
+        s = np.arange(10, dtype=np.uint64)
+        self.L.flockref_ch_observe_slice(c, _p(s), 5)
+        self.L.flockref_ch_bytes(c, b"\x01\x02\x03", 3)
+        one = np.zeros(2, np.uint64)
+        self.L.flockref_ch_sample(c, _p(one))
+        out.append(one.copy())
+        vec = np.zeros(14, np.uint64)
+        self.L.flockref_ch_sample_vec(c, 7, _p(vec))
+        out.append(vec.copy())
+        out.append(self.L.flockref_ch_grind(c, 5))
+        d = np.zeros(32, np.uint8)
+        self.L.flockref_ch_digest(c, _p(d))
+        out.append(d.tobytes())
+        self.L.flockref_ch_free(c)
+        return out
 
     def time_prove(self, log2: int, seed: int) -> tuple:
         n = ctypes.c_size_t()
