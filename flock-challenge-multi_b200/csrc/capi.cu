@@ -208,15 +208,16 @@ int flock_prove_seed(flock_setup* s, uint64_t seed, const uint8_t* domain, size_
   if (!s || (!domain && dlen)) return FLOCK_ERR_ARG;
   return guard(s->ctx, [&] {
     std::string d((const char*)domain, dlen);
-    // a SHA-256 setup generates its n_blocks compressions; a BLAKE3 one 2^log2
-    const size_t n = s->s->hash == flock::kHashSha256 ? s->n_blocks : 0;
+    // a SHA-256 / Keccak setup generates its n_blocks inputs; a BLAKE3 one 2^log2
+    const size_t n = s->s->hash != flock::kHashBlake3 ? s->n_blocks : 0;
     return emit(s->ctx, s->s->prove(&seed, nullptr, n, d), out, cap, out_len);
   });
 }
 
 static bool is_blake3(flock_setup* s) {
   if (s->s->hash == flock::kHashBlake3) return true;
-  s->ctx->err = "this entry point proves BLAKE3 compressions; the setup is a SHA-256 statement";
+  s->ctx->err = std::string("this entry point proves BLAKE3 compressions; the setup is a ") +
+                (s->s->hash == flock::kHashKeccak ? "Keccak" : "SHA-256") + " statement";
   return false;
 }
 
@@ -424,6 +425,133 @@ int flock_sha256_witness(flock_ctx* c, const flock_sha256_compression* comps, si
     CK(cudaMemcpyAsync(z, dz.p, words * 16, cudaMemcpyDeviceToHost, c->st));
     CK(cudaMemcpyAsync(a, da.p, words * 16, cudaMemcpyDeviceToHost, c->st));
     CK(cudaMemcpyAsync(b, db.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+
+// ---- Keccak-f[1600] permutations (r1cs_hashes/keccak.rs)
+static_assert(sizeof(flock_keccak_state) == 200, "flock_keccak_state is 25 u64");
+int flock_keccak_setup_create(flock_ctx* c, size_t n_keccaks, int hash, int profile, flock_setup** out) {
+  if (!c || !out) return FLOCK_ERR_ARG;
+  // min_n_keccaks_log (keccak.rs:513-518): 2^max(3, ceil(log2 n)) slots
+  uint32_t n_log = 3;
+  while (n_keccaks && ((size_t)1 << n_log) < n_keccaks) n_log++;
+  if (n_keccaks == 0 || n_log < 6 || n_log > 18 || (hash != FLOCK_HASH_BLAKE3 && hash != FLOCK_HASH_SHA256) ||
+      profile != FLOCK_PROFILE_FAST) {
+    c->err = "unsupported Keccak setup (33..=2^18 permutations: the fast profile's Ligerito ladders cover "
+             "m = 22..34; BLAKE3 or SHA-256 Merkle hash, fast profile)";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(c, [&] {
+    auto* s = new flock_setup();
+    s->ctx = c;
+    s->s.reset(new flock::Setup(c->device, n_log, 0, flock::kHashKeccak, hash));
+    s->n_blocks = n_keccaks;
+    *out = s;
+    return FLOCK_OK;
+  });
+}
+
+int flock_keccak_prove(flock_setup* s, const flock_keccak_state* states, size_t n, const uint8_t* domain, size_t dlen,
+                       uint8_t* out, size_t cap, size_t* out_len) {
+  if (!s || !states || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (s->s->hash != flock::kHashKeccak) {
+    s->ctx->err = "not a Keccak setup";
+    return FLOCK_ERR_ARG;
+  }
+  if (n != s->n_blocks) {
+    s->ctx->err = "expected exactly the setup's n_keccaks states";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(s->ctx, [&] {
+    if (!s->s->records_buf)
+      CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->records_buf), n * sizeof(flock_keccak_state), s->s->st));
+    CK(cudaMemcpyAsync(s->s->records_buf, states, n * sizeof(flock_keccak_state), cudaMemcpyHostToDevice, s->s->st));
+    std::string d((const char*)domain, dlen);
+    return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d), out, cap, out_len);
+  });
+}
+
+int flock_keccak_verify_bundle(flock_ctx* c, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen) {
+  if (!c || !bytes || (!domain && dlen)) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    std::lock_guard<std::mutex> lk(c->vmu);
+    if (!c->verifier) c->verifier.reset(new flock::Verifier(c->device));
+    const std::string why =
+        c->verifier->verify(bytes, len, std::string((const char*)domain, dlen), flock::kHashKeccak, nullptr, c->fs_fn);
+    if (why.empty()) return (int)FLOCK_OK;
+    c->err = "verify: " + why;
+    return (int)FLOCK_ERR_VERIFY;
+  });
+}
+
+void flock_keccak_f(uint64_t* lanes25) {
+  if (lanes25) flock::keccak_f(lanes25);
+}
+
+int flock_keccak_bench_inputs(size_t n, uint64_t seed, flock_keccak_state* out) {
+  if (!out && n) return FLOCK_ERR_ARG;
+  uint64_t st = seed;
+  for (size_t k = 0; k < n; k++) {
+    uint64_t d[25];
+    for (int w = 0; w < 25; w++) {
+      st += 0x9E3779B97F4A7C15ull;
+      uint64_t z = st;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      d[w] = z ^ (z >> 31);
+    }
+    for (int l = 0; l < 25; l++) {
+      uint64_t v = 0;
+      for (int z = 0; z < 64; z++) {
+        const int i = l + 25 * z;  // state bit (x, y, z), l = x + 5y
+        v |= ((d[i / 64] >> (i % 64)) & 1ull) << z;
+      }
+      out[k].lanes[l] = v;
+    }
+  }
+  return FLOCK_OK;
+}
+
+int flock_keccak_statement_digest(uint32_t m, uint8_t* out32) {
+  if (!out32 || m < 19 || m > 40) return FLOCK_ERR_ARG;
+  try {
+    auto d = flock::statement_digest(flock::kHashKeccak, (int)m);
+    memcpy(out32, d.data(), 32);
+    return FLOCK_OK;
+  } catch (...) {
+    return FLOCK_ERR_INTERNAL;
+  }
+}
+
+int flock_keccak_witness(flock_ctx* c, const flock_keccak_state* states, size_t n, uint32_t n_log, uint64_t* z,
+                         uint64_t* a, uint64_t* b) {
+  if (!c || !z || !a || !b || n_log < 3 || n_log > 18 || n > ((size_t)1 << n_log) || (n && !states))
+    return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    const size_t slots = (size_t)1 << n_log, words = slots * 512;
+    DevBuf<f128> dz(words), da(words), db(words);
+    DevBuf<flock_keccak_state> ds(n ? n : 1);
+    if (n) CK(cudaMemcpyAsync(ds.p, states, n * sizeof(flock_keccak_state), cudaMemcpyHostToDevice, c->st));
+    launch_witness_keccak(reinterpret_cast<const uint64_t*>(ds.p), 0, (uint32_t)n, (uint32_t)slots, dz.p, da.p, db.p,
+                          c->st);
+    CK(cudaMemcpyAsync(z, dz.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(a, da.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(b, db.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+
+int flock_keccak_comb(flock_ctx* c, const uint64_t* e, const uint64_t* alpha, const uint64_t* beta, uint64_t* comb) {
+  if (!c || !e || !alpha || !beta || !comb) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    const size_t kk = (size_t)1 << flock::kKeccakKLog;
+    DevBuf<f128> de(kk), dc(kk), dw(keccak_comb_scratch());
+    CK(cudaMemcpyAsync(de.p, e, kk * 16, cudaMemcpyHostToDevice, c->st));
+    keccak_comb(de.p, mk(alpha[0], alpha[1]), mk(beta[0], beta[1]), keccak_masks(c->device), dw.p, dc.p, c->st);
+    CK(cudaMemcpyAsync(comb, dc.p, kk * 16, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return FLOCK_OK;
   });

@@ -600,6 +600,23 @@ Statement build_sha256() {
   return st;
 }
 
+// KeccakSetup's BlockR1cs (keccak.rs:558-560, common.rs:120-138): A_0 and
+// B_0 without entries, so the digest binds the sizes and C = I only; the
+// lincheck applies the real matrices through keccak_comb
+Statement build_keccak() {
+  const int K = 1 << kKeccakKLog;
+  Statement st;
+  st.k_log = kKeccakKLog;
+  st.z_const = kKeccakZConst;
+  st.useful = kKeccakUseful;
+  st.implicit = true;
+  st.a_ptr.assign(K + 1, 0);
+  st.b_ptr.assign(K + 1, 0);
+  st.at_ptr.assign(K + 1, 0);
+  st.bt_ptr.assign(K + 1, 0);
+  return st;
+}
+
 void put_u64(B3& h, uint64_t v) { uint8_t b[8]; le64(v, b); h.update(b, 8); }
 void put_matrix(B3& h, int kk, const std::vector<uint32_t>* ptr, const std::vector<uint16_t>* col) {
   put_u64(h, kk);
@@ -635,11 +652,36 @@ void sha256_compress(const uint32_t h_in[8], const uint32_t m[16], uint32_t out[
   for (int i = 0; i < 8; i++) out[i] = h_in[i] + s[i];
 }
 
+void keccak_f(uint64_t s[25]) {
+  static const int rho[25] = {0,  36, 3,  41, 18, 1,  44, 10, 45, 2,  62, 6, 43,
+                              15, 61, 28, 55, 25, 21, 56, 27, 20, 39, 8,  14};  // r[x][y] at 5x + y
+  static const uint64_t rc[24] = {
+      0x0000000000000001ull, 0x0000000000008082ull, 0x800000000000808Aull, 0x8000000080008000ull,
+      0x000000000000808Bull, 0x0000000080000001ull, 0x8000000080008081ull, 0x8000000000008009ull,
+      0x000000000000008Aull, 0x0000000000000088ull, 0x0000000080008009ull, 0x000000008000000Aull,
+      0x000000008000808Bull, 0x800000000000008Bull, 0x8000000000008089ull, 0x8000000000008003ull,
+      0x8000000000008002ull, 0x8000000000000080ull, 0x000000000000800Aull, 0x800000008000000Aull,
+      0x8000000080008081ull, 0x8000000000008080ull, 0x0000000080000001ull, 0x8000000080008008ull};
+  auto rotl = [](uint64_t v, int n) { return n ? (v << n) | (v >> (64 - n)) : v; };
+  for (int r = 0; r < 24; r++) {
+    uint64_t c[5], b[25];
+    for (int x = 0; x < 5; x++) c[x] = s[x] ^ s[x + 5] ^ s[x + 10] ^ s[x + 15] ^ s[x + 20];
+    for (int l = 0; l < 25; l++) s[l] ^= c[(l % 5 + 4) % 5] ^ rotl(c[(l % 5 + 1) % 5], 1);
+    for (int x = 0; x < 5; x++)  // rho, then pi: lane (x, y) moves to (y, 2x + 3y)
+      for (int y = 0; y < 5; y++) b[y + 5 * ((2 * x + 3 * y) % 5)] = rotl(s[x + 5 * y], rho[5 * x + y]);
+    for (int y = 0; y < 5; y++)
+      for (int x = 0; x < 5; x++) s[x + 5 * y] = b[x + 5 * y] ^ (~b[(x + 1) % 5 + 5 * y] & b[(x + 2) % 5 + 5 * y]);
+    s[0] ^= rc[r];
+  }
+}
+
 const Statement& statement(int hash) {
-  static std::once_flag once[2];
-  static std::unique_ptr<Statement> s[2];
-  const int k = hash == kHashSha256 ? 1 : 0;
-  std::call_once(once[k], [k] { s[k].reset(new Statement(k ? build_sha256() : build())); });
+  static std::once_flag once[3];
+  static std::unique_ptr<Statement> s[3];
+  const int k = hash == kHashSha256 ? 1 : hash == kHashKeccak ? 2 : 0;
+  std::call_once(once[k], [k] {
+    s[k].reset(new Statement(k == 1 ? build_sha256() : k == 2 ? build_keccak() : build()));
+  });
   return *s[k];
 }
 

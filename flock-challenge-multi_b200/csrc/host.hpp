@@ -119,12 +119,18 @@ std::vector<f128> medium_consts();
 // ---- R1CS statements: one compression per 2^k_log-bit block ----
 // The hash a statement encodes.  BLAKE3 (r1cs_hashes/blake3.rs): 2^14-bit
 // blocks, constant wire at bit 512.  SHA-256 (r1cs_hashes/sha2.rs): 2^15-bit
-// blocks, constant wire at bit 31400.
-enum HashKind : int { kHashBlake3 = 0, kHashSha256 = 1 };
+// blocks, constant wire at bit 31400.  Keccak-f[1600] (r1cs_hashes/keccak.rs):
+// 2^16-bit blocks, constant wire at bit 4096, implicit matrices (the block
+// statement is the empty stub of common.rs:120-138; the lincheck applies
+// them through keccak_comb).
+enum HashKind : int { kHashBlake3 = 0, kHashSha256 = 1, kHashKeccak = 2 };
 constexpr int kKLog = 14, kK = 1 << kKLog, kKSkip = 6, kZConst = 512, kUseful = 15409;
 constexpr int kShaKLog = 15, kShaZConst = 31400, kShaUseful = 31401;
+constexpr int kKeccakKLog = 16, kKeccakZConst = 4096, kKeccakUseful = 42560;
+constexpr int kMaxKLog = kKeccakKLog;  // the largest block of the statements
 struct Statement {
   int k_log = kKLog, z_const = kZConst, useful = kUseful;
+  bool implicit = false;                 // matrices applied by a walker, not stored
   std::vector<uint32_t> a_ptr, b_ptr;    // CSR rows
   std::vector<uint16_t> a_col, b_col;
   std::vector<uint32_t> at_ptr, bt_ptr;  // CSC (column -> rows)
@@ -136,8 +142,14 @@ std::array<uint8_t, 32> statement_digest(int hash, int m);
 inline std::array<uint8_t, 32> statement_digest(int m) { return statement_digest(kHashBlake3, m); }
 // sha256_compress (r1cs_hashes/sha2.rs:1502-1546): out = h_in + rounds(h_in, m)
 void sha256_compress(const uint32_t h_in[8], const uint32_t m[16], uint32_t out[8]);
+// keccak_f (keccak.rs:423-428, FIPS 202 Keccak-f[1600]) on 25 lanes (lane
+// x + 5y, bit z), in place
+void keccak_f(uint64_t lanes[25]);
 // block size of a hash's statement (log2 bits)
-inline int hash_k_log(int hash) { return hash == kHashSha256 ? kShaKLog : kKLog; }
+inline int hash_k_log(int hash) {
+  return hash == kHashSha256 ? kShaKLog : hash == kHashKeccak ? kKeccakKLog : kKLog;
+}
+inline bool known_hash(int hash) { return hash == kHashBlake3 || hash == kHashSha256 || hash == kHashKeccak; }
 
 // ---- Ligerito fast ladder (configs/ligerito/m*_fast.toml) ----
 struct Ladder {

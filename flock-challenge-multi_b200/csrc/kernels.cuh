@@ -91,6 +91,16 @@ void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n
 // records == nullptr for the benchmark generator from `seed`
 void launch_witness_sha(const uint32_t* records, uint64_t seed, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
                         f128* b, cudaStream_t s);
+// Keccak-f[1600] permutations, 2^16-bit blocks: states of 25 u64 lanes, or
+// states == nullptr for the benchmark generator from `seed`
+void launch_witness_keccak(const uint64_t* states, uint64_t seed, uint32_t n_perm, uint32_t n_slots, f128* z, f128* a,
+                           f128* b, cudaStream_t s);
+// K6 of the Keccak statement: comb = alpha A^T e + B^T e + beta [const] over
+// the 2^16 rows of a block (e and comb: 2^16 values); W: keccak_comb_scratch()
+// values; masks: keccak_masks(device), the round constants' share
+const uint64_t* keccak_masks(int device);
+size_t keccak_comb_scratch();
+void keccak_comb(const f128* e, f128 alpha, f128 beta, const uint64_t* masks, f128* W, f128* comb, cudaStream_t s);
 // K1
 // NTT pass plans: the passes (first layer l0, layer count R, 2^lgs lanes per
 // tile, threads per CTA) that cover layers layer_begin..log_d-1.

@@ -73,7 +73,7 @@ Setup::Setup(int device, uint32_t log2_, int stream_priority, int hash_, int mer
     : log2(log2_), hash(hash_), merkle_fn(merkle_fn_) {
   CK(cudaSetDevice(device));
   const size_t bytes0 = t_alloc_bytes;
-  if (hash != kHashBlake3 && hash != kHashSha256) throw std::runtime_error("unknown statement hash");
+  if (!known_hash(hash)) throw std::runtime_error("unknown statement hash");
   if (merkle_fn != kFnBlake3 && merkle_fn != kFnSha256) throw std::runtime_error("unknown Merkle hash");
   k_log = hash_k_log(hash);
   n_log = std::max<int>(3, (int)log2);
@@ -115,6 +115,10 @@ Setup::Setup(int device, uint32_t log2_, int stream_priority, int hash_, int mer
   zv = dalloc<f128>(kk, st);
   zv_pre = dalloc<f128>(kk, st);
   eq_inner = dalloc<f128>(kk, st);
+  if (hash == kHashKeccak) {
+    kc_w = dalloc<f128>(keccak_comb_scratch(), st);
+    kc_masks = keccak_masks(device);
+  }
   bc_tabs = dalloc<f128>(2 * 16 * 256, st);
   idx = dalloc<uint64_t>(1 << 16, st);
   gather = dalloc<f128>(1 << 16, st);
@@ -317,7 +321,7 @@ Setup::~Setup() {
   cudaStreamSynchronize(st);
   void* ptrs[] = {z, a, b, cw0, tree0, pp[0], pp[1], pp[2], pp[3], eqbuf[0], zv_pre, induce_buf, out, blocks_buf, records_buf,
                   tabs_r1, lag, elo, ehi, comb, zv, eq_inner, bc_tabs, idx, gather, d_found, at_ptr, bt_ptr,
-                  at_row, bt_row};
+                  at_row, bt_row, kc_w};
   for (void* p : ptrs)
     if (p) cudaFreeAsync(p, st);
   for (auto& L : levels) {
@@ -466,7 +470,13 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   if (merkle && (hash != kHashSha256 || n_blocks != n_slots || !merkle->b_bits || merkle->path_log < 0 ||
                  merkle->path_log > n_log))
     throw std::runtime_error("a Merkle path is a SHA-256 statement whose paths fill every slot");
-  if (!committed && hash == kHashSha256) {
+  if (!committed && hash == kHashKeccak) {
+    // ---- K0 witness of Keccak-f[1600] permutations (states of 25 u64)
+    const uint32_t nb = n_blocks ? (uint32_t)n_blocks : 1u << log2;
+    launch_witness_keccak(seed ? nullptr : reinterpret_cast<const uint64_t*>(blocks_dev), seed ? *seed : 0, nb,
+                          n_slots, z, a, b, st);
+    CK(cudaGetLastError());
+  } else if (!committed && hash == kHashSha256) {
     // ---- K0 witness of SHA-256 compressions
     const uint32_t nb = n_blocks ? (uint32_t)n_blocks : 1u << log2;
     launch_witness_sha(seed ? nullptr : blocks_dev, seed ? *seed : 0, nb, n_slots, z, a, b, st);
@@ -730,7 +740,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     std::vector<f128> L = hlagrange(zc_z, 0);
     eq_build(x_inner.data(), (int)x_inner.size(), hone(), zv_pre, st);
     outer64(L.data(), zv_pre, (size_t)1 << x_inner.size(), eq_inner, st);
-    lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, statement(hash).z_const, kk, comb, st);
+    if (hash == kHashKeccak) keccak_comb(eq_inner, alpha, beta, kc_masks, kc_w, comb, st);
+    else lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, statement(hash).z_const, kk, comb, st);
     eq_table(x_outer, scratch_eq());
     CK(cudaMemsetAsync(zv, 0, kk * sizeof(f128), st));
     lc_zvec(z, scratch_eq(), (size_t)1 << (m - k_log), k_log, zv, st);

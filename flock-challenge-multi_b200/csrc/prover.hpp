@@ -88,7 +88,7 @@ class Verifier {
   static constexpr size_t kRowsCap = (size_t)1 << 20, kCvsCap = (size_t)1 << 19;
   int device_ = 0;
   cudaStream_t st_ = nullptr;
-  f128 *eqx_ = nullptr, *eqi_ = nullptr, *comb_ = nullptr;
+  f128 *eqx_ = nullptr, *eqi_ = nullptr, *comb_ = nullptr, *kcw_ = nullptr;
   uint8_t* rows_ = nullptr;
   uint32_t* cvs_ = nullptr;
 };
@@ -200,6 +200,8 @@ class Setup {
   uint8_t* h_stage = nullptr;
   uint32_t *at_ptr = nullptr, *bt_ptr = nullptr;
   uint16_t *at_row = nullptr, *bt_row = nullptr;
+  f128* kc_w = nullptr;                // Keccak statement: the walker's W rows
+  const uint64_t* kc_masks = nullptr;  // Keccak statement: round-constant masks (per device)
   cudaEvent_t ev[kPhases + 1] = {};
   // The commitment's RS encode (z -> cw0) and Merkle tree (cw0 -> tree0) on
   // fixed buffers, each captured once as a CUDA graph (after the NTT plans

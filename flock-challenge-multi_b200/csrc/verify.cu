@@ -904,12 +904,14 @@ namespace {
 // rows (1 MiB) and their leaf chaining values (512 KiB).
 struct VerifyBufs {
   f128 *eqx, *eqi, *comb;
+  f128* kcw;  // the Keccak walker's W rows (Keccak statements only)
   uint8_t* rows;
   uint32_t* cvs;
   size_t rows_cap, cvs_cap;  // bytes
 };
 // the device half of the verifier over the CSC copy of the block matrices
-// given by at_*, bt_*: the matrix combination and the opened rows' leaves
+// given by at_*, bt_* (the Keccak statement's implicit matrices by its
+// walker): the matrix combination and the opened rows' leaves
 VerifyStatement device_statement(int m, int hash, const std::array<uint8_t, 32>& digest, const uint32_t* at_ptr,
                                  const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
                                  const VerifyBufs& B, cudaStream_t st) {
@@ -922,7 +924,13 @@ VerifyStatement device_statement(int m, int hash, const std::array<uint8_t, 32>&
     std::vector<f128> L = hlagrange(zskip, 0), cv(kk);
     eq_build(x_inner.data(), (int)x_inner.size(), hone(), B.eqx, st);
     outer64(L.data(), B.eqx, (size_t)1 << x_inner.size(), B.eqi, st);
-    lc_comb(at_ptr, at_row, bt_ptr, bt_row, B.eqi, alpha, beta, pin, kk, B.comb, st);
+    if (hash == kHashKeccak) {
+      int dev = 0;
+      CK(cudaGetDevice(&dev));
+      keccak_comb(B.eqi, alpha, beta, keccak_masks(dev), B.kcw, B.comb, st);
+    } else {
+      lc_comb(at_ptr, at_row, bt_ptr, bt_row, B.eqi, alpha, beta, pin, kk, B.comb, st);
+    }
     CK(cudaMemcpyAsync(cv.data(), B.comb, kk * sizeof(f128), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return cv;
@@ -977,7 +985,7 @@ const DevCsc& shared_csc(int device, int hash) {
 
 // The setup's own buffers and stream (flock_verify: the caller owns the setup).
 std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& domain, const MerklePublic* merkle) {
-  VerifyBufs B{zv_pre, eq_inner, comb, reinterpret_cast<uint8_t*>(gather), reinterpret_cast<uint32_t*>(idx),
+  VerifyBufs B{zv_pre, eq_inner, comb, kc_w, reinterpret_cast<uint8_t*>(gather), reinterpret_cast<uint32_t*>(idx),
                ((size_t)1 << 16) * sizeof(f128), ((size_t)1 << 16) * sizeof(uint64_t)};
   if (merkle && hash != kHashSha256) return "a Merkle path is a SHA-256 statement";
   VerifyStatement V = device_statement(m, hash, digest, at_ptr, at_row, bt_ptr, bt_row, B, st);
@@ -989,9 +997,10 @@ std::string Setup::verify(const uint8_t* bytes, size_t len, const std::string& d
 Verifier::Verifier(int device) : device_(device) {
   DeviceScope on(device);
   CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-  CK(cudaMalloc(&eqx_, ((size_t)1 << (kShaKLog - kKSkip)) * sizeof(f128)));  // eq(x_inner), 2^(k_log - 6)
-  CK(cudaMalloc(&eqi_, ((size_t)1 << kShaKLog) * sizeof(f128)));  // the larger block of the two hashes
-  CK(cudaMalloc(&comb_, ((size_t)1 << kShaKLog) * sizeof(f128)));
+  CK(cudaMalloc(&eqx_, ((size_t)1 << (kMaxKLog - kKSkip)) * sizeof(f128)));  // eq(x_inner), 2^(k_log - 6)
+  CK(cudaMalloc(&eqi_, ((size_t)1 << kMaxKLog) * sizeof(f128)));  // the largest block of the statements
+  CK(cudaMalloc(&comb_, ((size_t)1 << kMaxKLog) * sizeof(f128)));
+  CK(cudaMalloc(&kcw_, keccak_comb_scratch() * sizeof(f128)));
   CK(cudaMalloc(&rows_, kRowsCap));
   CK(cudaMalloc(&cvs_, kCvsCap));
 }
@@ -1001,7 +1010,7 @@ Verifier::~Verifier() {
   cudaGetDevice(&prev);
   cudaSetDevice(device_);
   if (st_) cudaStreamSynchronize(st_);
-  for (void* p : {(void*)eqx_, (void*)eqi_, (void*)comb_, (void*)rows_, (void*)cvs_}) cudaFree(p);
+  for (void* p : {(void*)eqx_, (void*)eqi_, (void*)comb_, (void*)kcw_, (void*)rows_, (void*)cvs_}) cudaFree(p);
   if (st_) cudaStreamDestroy(st_);
   if (prev >= 0) cudaSetDevice(prev);
 }
@@ -1016,15 +1025,16 @@ std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string
   const size_t at = merkle ? 32 : 7 + (bytes[6] == 3 ? 4 : 0) + 32;
   uint64_t mm = 0;
   for (int k = 0; k < 8; k++) mm |= (uint64_t)bytes[at + k] << (8 * k);
-  if (hash != kHashBlake3 && hash != kHashSha256) return "unknown statement hash";
+  if (!known_hash(hash)) return "unknown statement hash";
   if (hash != kHashBlake3 && !merkle && bytes[6] != 2) return "hash chains are BLAKE3 statements";
-  // BLAKE3: 2^8..2^20 compressions; SHA-256: 2^7..2^19 (the same m range)
+  // BLAKE3: 2^8..2^20 compressions; SHA-256: 2^7..2^19; Keccak: 2^6..2^18
+  // permutations (the same m range)
   if (mm < 22 || mm > 34) return "bundle is for an unsupported statement size";
   // the stream and buffers belong to device_, whichever device the calling
   // thread has current; the caller's device is restored on return
   DeviceScope on(device_);
   const DevCsc& C = shared_csc(device_, hash);
-  const VerifyBufs B{eqx_, eqi_, comb_, rows_, cvs_, kRowsCap, kCvsCap};
+  const VerifyBufs B{eqx_, eqi_, comb_, kcw_, rows_, cvs_, kRowsCap, kCvsCap};
   VerifyStatement V = device_statement((int)mm, hash, statement_digest(hash, (int)mm), C.at_ptr, C.at_row, C.bt_ptr,
                                        C.bt_row, B, st_);
   V.merkle = merkle;

@@ -39,6 +39,8 @@ EXPORTS = (
     "flock_sha256_compress", "flock_sha256_statement_digest", "flock_sha256_witness", "flock_sha256_merkle_prove",
     "flock_sha256_merkle_verify", "flock_sha256_merkle_inputs", "flock_setup_set_transcript",
     "flock_ctx_set_transcript", "flock_challenger_create_hash", "flock_merkle_tree_hash",
+    "flock_keccak_setup_create", "flock_keccak_prove", "flock_keccak_verify_bundle", "flock_keccak_f",
+    "flock_keccak_bench_inputs", "flock_keccak_statement_digest", "flock_keccak_witness", "flock_keccak_comb",
 )
 # the hash behind Merkle trees / the transcript (HashKind discriminants)
 HASH = {"sha256": 0, "blake3": 1}
@@ -122,6 +124,15 @@ def load() -> ctypes.CDLL:
         lib.flock_merkle_root_noalloc.argtypes = [vp, sz, sz, vp, vp]
         lib.flock_serve_start.argtypes = [vp, i32]
         lib.flock_serve_prewarm.argtypes = [vp, u32, i32, ctypes.POINTER(i32)]
+        lib.flock_keccak_setup_create.argtypes = [vp, sz, i32, i32, ctypes.POINTER(vp)]
+        lib.flock_keccak_prove.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        lib.flock_keccak_verify_bundle.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
+        lib.flock_keccak_f.argtypes = [vp]
+        lib.flock_keccak_f.restype = None
+        lib.flock_keccak_bench_inputs.argtypes = [sz, u64, vp]
+        lib.flock_keccak_statement_digest.argtypes = [u32, vp]
+        lib.flock_keccak_witness.argtypes = [vp, vp, sz, u32, vp, vp, vp]
+        lib.flock_keccak_comb.argtypes = [vp, vp, vp, vp, vp]
         lib.flock_sha256_setup_create.argtypes = [vp, sz, i32, i32, ctypes.POINTER(vp)]
         lib.flock_sha256_prove.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_sha256_verify_bundle.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
@@ -250,6 +261,38 @@ def sha256_statement_digest(m: int) -> bytes:
     return out.tobytes()
 
 
+def keccak_f(lanes) -> np.ndarray:
+    """keccak_f (keccak.rs:423-428, FIPS 202 Keccak-f[1600]) of 25 u64 lanes
+    (bit z of lane x + 5y is state bit x + 5y + 25z)."""
+    s = np.array(lanes, np.uint64).reshape(25).copy()
+    load().flock_keccak_f(_ptr(s))
+    return s
+
+
+def keccak_bench_inputs(n: int, seed: int) -> np.ndarray:
+    """The keccak3_proof bench states on the host, (n, 25) u64 lanes
+    (benches/keccak3_proof.rs:66-93): one SplitMix64 stream from `seed`, 25
+    draws per state, state bit i = bit i mod 64 of draw i / 64."""
+    out = np.zeros((n, 25), np.uint64)
+    rc = load().flock_keccak_bench_inputs(n, seed, _ptr(out))
+    if rc != 0:
+        raise FlockError(f"keccak_bench_inputs: {rc}")
+    return out
+
+
+def keccak_bench_seed(n: int, run: int = 0) -> int:
+    """The seed benches/keccak3_proof.rs:121-124 gives run `run` of n states."""
+    return 0xC0FFEE_BEEF ^ n ^ run
+
+
+def keccak_statement_digest(m: int) -> bytes:
+    out = np.zeros(32, np.uint8)
+    rc = load().flock_keccak_statement_digest(m, _ptr(out))
+    if rc != 0:
+        raise FlockError(f"keccak_statement_digest: {rc}")
+    return out.tobytes()
+
+
 def chain_blocks(seed: int, steps: int, initial_cv=None) -> np.ndarray:
     """The flock_chain CLI's honest BLAKE3 chain, (steps, 28) u32 records
     cv[8], m[16], counter lo/hi, block_len, flags
@@ -372,6 +415,35 @@ class Context:
         self._check(self.lib.flock_sha256_witness(self.h, _ptr(comps), comps.shape[0], n_log, _ptr(z), _ptr(a),
                                                   _ptr(b)), "sha256_witness")
         return z, a, b
+
+    def keccak_verify(self, bundle: bytes, domain: bytes = DOMAIN) -> str:
+        """KeccakSetup::verify for any supported size: '' when the bundle
+        verifies as a Keccak statement, otherwise the failed check."""
+        rc = self.lib.flock_keccak_verify_bundle(self.h, bundle, len(bundle), domain, len(domain))
+        if rc == 0:
+            return ""
+        if rc == FLOCK_ERR_VERIFY:
+            return self.lib.flock_last_error(self.h).decode()
+        self._check(rc, "keccak_verify_bundle")
+        return "error"
+
+    def keccak_witness(self, states: np.ndarray, n_log: int):
+        """(z, a, b) packed row witness of (n, 25) u64 Keccak states over
+        2^n_log blocks, each (2^n_log, 1024) u64."""
+        states = np.ascontiguousarray(states, np.uint64).reshape(-1, 25)
+        z, a, b = (np.zeros((1 << n_log, 1024), np.uint64) for _ in range(3))
+        self._check(self.lib.flock_keccak_witness(self.h, _ptr(states), states.shape[0], n_log, _ptr(z), _ptr(a),
+                                                  _ptr(b)), "keccak_witness")
+        return z, a, b
+
+    def keccak_comb(self, e: np.ndarray, alpha, beta) -> np.ndarray:
+        """The Keccak lincheck's alpha A^T e + B^T e + beta [const] on the GPU
+        (e: (2^16, 2) u64 lo/hi; alpha, beta: (lo, hi))."""
+        e = np.ascontiguousarray(e, np.uint64).reshape(1 << 16, 2)
+        al, be = np.array(alpha, np.uint64), np.array(beta, np.uint64)
+        out = np.zeros((1 << 16, 2), np.uint64)
+        self._check(self.lib.flock_keccak_comb(self.h, _ptr(e), _ptr(al), _ptr(be), _ptr(out)), "keccak_comb")
+        return out
 
     def serve_verify(self, on: bool = True) -> None:
         """Self-check every served / batched proof with the verifier."""
@@ -689,6 +761,64 @@ class Sha256Prover:
 
     def prove_seed(self, seed: int, domain: bytes = DOMAIN) -> bytes:
         """prove_fast over sha256_bench_inputs(n, seed), generated on the GPU."""
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_prove_seed(self.h, seed, domain, len(domain), _ptr(self._buf), self._buf.size,
+                                           ctypes.byref(n))
+        self.ctx._check(rc, "prove_seed")
+        return self._buf[: n.value].tobytes()
+
+    def verify(self, bundle: bytes, domain: bytes = DOMAIN) -> str:
+        rc = self.ctx.lib.flock_verify(self.h, bundle, len(bundle), domain, len(domain))
+        if rc == 0:
+            return ""
+        if rc == FLOCK_ERR_VERIFY:
+            return self.ctx.lib.flock_last_error(self.ctx.h).decode()
+        self.ctx._check(rc, "verify")
+        return "error"
+
+    def phase_ms(self) -> dict:
+        out = np.zeros(len(PHASES), np.float64)
+        k = self.ctx.lib.flock_setup_phase_ms(self.h, _ptr(out), len(PHASES))
+        return dict(zip(PHASES[:k], out[:k].tolist()))
+
+
+class KeccakProver:
+    """`KeccakSetup::new(n)` (crates/flock-prover/src/r1cs_hashes/keccak.rs:
+    870-912): Keccak-f[1600] permutations, one per 2^16-bit block,
+    2^max(3, ceil(log2 n)) slots, fast profile; BLAKE3 Merkle hashing unless
+    merkle_hash says otherwise."""
+
+    def __init__(self, ctx: Context, n: int, merkle_hash: str = "blake3", transcript: str = "blake3"):
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.flock_keccak_setup_create(ctx.h, n, HASH[merkle_hash], 0, ctypes.byref(h)),
+                   "keccak_setup_create")
+        self.ctx, self.n, self.h = ctx, n, h
+        ctx._check(ctx.lib.flock_setup_set_transcript(h, HASH[transcript]), "setup_set_transcript")
+        self.n_log = max(3, (n - 1).bit_length())
+        self._buf = np.zeros(MAX_PROOF_BYTES * 2, np.uint8)
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.flock_setup_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def prove(self, states: np.ndarray, domain: bytes = DOMAIN) -> bytes:
+        """prove_fast over (n, 25) u64 states."""
+        states = np.ascontiguousarray(states, np.uint64).reshape(-1, 25)
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_keccak_prove(self.h, _ptr(states), states.shape[0], domain, len(domain),
+                                             _ptr(self._buf), self._buf.size, ctypes.byref(n))
+        self.ctx._check(rc, "keccak_prove")
+        return self._buf[: n.value].tobytes()
+
+    def prove_seed(self, seed: int, domain: bytes = DOMAIN) -> bytes:
+        """prove_fast over keccak_bench_inputs(n, seed), generated on the GPU."""
         n = ctypes.c_size_t()
         rc = self.ctx.lib.flock_prove_seed(self.h, seed, domain, len(domain), _ptr(self._buf), self._buf.size,
                                            ctypes.byref(n))

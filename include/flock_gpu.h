@@ -248,6 +248,50 @@ int flock_sha256_statement_digest(uint32_t m, uint8_t* out32);
 int flock_sha256_witness(flock_ctx* ctx, const flock_sha256_compression* comps, size_t n, uint32_t n_log, uint64_t* z,
                          uint64_t* a, uint64_t* b);
 
+/* ---- Keccak-f[1600] permutations (crates/flock-prover/src/r1cs_hashes/keccak.rs) ----
+ * The same prover over the monolithic Keccak R1CS at K_LOG = 16
+ * (keccak.rs:430-660): one permutation per 2^16-bit block holding state_0,
+ * state_24, the constant wire (bit 4096) and the 24 x 1600 chi AND rows t_r.
+ * The block matrices are implicit (the statement digest binds the empty stub
+ * of common.rs:120-138); the lincheck applies them by the transposed
+ * recurrence of KeccakLincheckCircuit (keccak.rs:681-848) on the GPU. */
+/* One input: the reference's State = [bool; 1600] (keccak.rs:124), as 25
+ * lanes: bit z of lanes[x + 5y] is state bit x + 5y + 25z. */
+typedef struct flock_keccak_state {
+  uint64_t lanes[25];
+} flock_keccak_state;
+/* KeccakSetup::new(n_keccaks) (keccak.rs:870-912): 2^max(3, ceil(log2 n))
+ * slots (min_n_keccaks_log, keccak.rs:513-518).  Supported: 33 <= n <= 2^18
+ * (m = 16 + n_log in 22..34, the fast profile's Ligerito ladders).  hash /
+ * profile as for flock_setup_create (the reference's default Merkle hash is
+ * SHA-256).  The setup also serves flock_prove_seed (the keccak3_proof bench
+ * generator: benches/keccak3_proof.rs:66-93, one SplitMix64 stream from the
+ * seed, 25 draws per state) and flock_verify. */
+int flock_keccak_setup_create(flock_ctx* ctx, size_t n_keccaks, int hash, int profile, flock_setup** out);
+/* KeccakSetup::prove_fast(&states, &mut FsChallenger) + to_bytes
+ * (keccak.rs:956-978): n must equal the setup's n_keccaks; the slots from n on
+ * hold keccak_f of the zero state (keccak.rs:646-660). */
+int flock_keccak_prove(flock_setup* s, const flock_keccak_state* states, size_t n, const uint8_t* domain, size_t dlen,
+                       uint8_t* out, size_t cap, size_t* out_len);
+/* KeccakSetup::verify (keccak.rs:979-998) without a prover setup, for any
+ * supported size (read from the bundle); the context's verifier, as in
+ * flock_verify_bundle. */
+int flock_keccak_verify_bundle(flock_ctx* ctx, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen);
+/* keccak_f (keccak.rs:423-428; FIPS 202 Keccak-f[1600]) on the host, in place. */
+void flock_keccak_f(uint64_t* lanes25);
+/* The keccak3_proof bench's states (benches/keccak3_proof.rs:66-93) on the host. */
+int flock_keccak_bench_inputs(size_t n, uint64_t seed, flock_keccak_state* out);
+/* BlockR1cs::statement_digest of the Keccak statement of size m. */
+int flock_keccak_statement_digest(uint32_t m, uint8_t* out32);
+/* Debug/test: the packed row witness z, a, b of n permutations over 2^n_log
+ * blocks (2^(n_log + 9) u64 pairs each). */
+int flock_keccak_witness(flock_ctx* ctx, const flock_keccak_state* states, size_t n, uint32_t n_log, uint64_t* z,
+                         uint64_t* a, uint64_t* b);
+/* Debug/test: the lincheck's column combination alpha A^T e + B^T e + beta
+ * [const] over the 2^16 rows of a block, on the GPU (e, comb: 2^16 F128 as
+ * lo, hi u64 pairs; alpha, beta: one F128). */
+int flock_keccak_comb(flock_ctx* ctx, const uint64_t* e, const uint64_t* alpha, const uint64_t* beta, uint64_t* comb);
+
 /* The flock_chain CLI's honest chain of `steps` records: record i has
  * cv = x_i (x_0 = initial_cv, or the BLAKE3 IV when NULL), 16 message words
  * from SplitMix64(seed) (low 32 bits of each draw), counter 0, block_len 64,

@@ -387,6 +387,10 @@ int flockref_prove_keccak(const uint64_t* states, size_t n, const uint8_t* domai
   }
 }
 
+// Whether the last proof on this thread that records it (chain, Merkle-path
+// and Keccak proofs) had sum_j b_combined[j] z[j] == target.
+int flockref_last_open_identity_ok(void) { return last_open_identity_ok() ? 1 : 0; }
+
 // Wall-clock seconds of one full oracle prove at log2 (for the CPU baseline).
 double flockref_time_prove(uint32_t log2, uint64_t seed, size_t* proof_len) {
   auto blocks = generate_compressions(log2, seed);

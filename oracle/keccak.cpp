@@ -256,7 +256,9 @@ void generate_keccak_witness(const std::vector<keccak::State>& states, int n_log
 Bundle prove_keccak(const std::vector<keccak::State>& states, int n_log, const std::string& domain) {
   std::vector<F128> z, a, b;
   generate_keccak_witness(states, n_log, z, a, b);
-  return prove_core(keccak_r1cs(n_log), std::move(z), a, b, domain, CoreHook());
+  // a hook that adds no claim, so that prove_core records the open identity
+  const CoreHook none = [](Challenger&, const std::vector<F128>&) { return std::vector<DirectClaim>(); };
+  return prove_core(keccak_r1cs(n_log), std::move(z), a, b, domain, none);
 }
 
 }  // namespace flockref

@@ -62,6 +62,16 @@
    statement over the benchmark inputs at 2^8 and 2^12 compressions, each with
    the hash pair named in the entry.
 
+11. keccak_proofs.json (--keccak) — the Keccak-f[1600] statement
+   (r1cs_hashes/keccak.rs): its statement digests for m = 22..34, and sha256
+   of the oracle's KeccakSetup::prove_fast bundles over the keccak3_proof
+   bench states (benches/keccak3_proof.rs:66-93, seed 0xC0FFEE_BEEF ^ n) at
+   n = 64, 100 (padded), 1024, 4096 and 16384.  No reference verifier runs
+   Keccak statements, so these pin the GPU to the oracle, whose own checks are
+   recorded per entry: every block's witness has a & b = z and state_24 =
+   keccak_f(state_0) (the permutation itself pinned to hashlib's SHA-3 by the
+   tests), and the batched open's claim identity holds.
+
 Usage (a built oracle; REFERENCE is a checkout of the reference project):
     python tests/golden/make_golden.py --ref REFERENCE [--large]
     python tests/golden/make_golden.py --chain
@@ -69,6 +79,7 @@ Usage (a built oracle; REFERENCE is a checkout of the reference project):
     python tests/golden/make_golden.py --sha256
     python tests/golden/make_golden.py --sha256-merkle
     python tests/golden/make_golden.py --default-hashes
+    python tests/golden/make_golden.py --keccak
     python tests/golden/make_golden.py --gpu-harness VERIFIER --sizes 19:2,20:2 --out FILE
 """
 import hashlib
@@ -229,6 +240,35 @@ def sha256_proofs(threads=8) -> None:
         (HERE / "sha256_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
 
 
+KECCAK_SIZES = (64, 100, 1024, 4096, 16384)
+
+
+def keccak_proofs(threads=8) -> None:
+    import os
+    os.environ["FLOCKREF_THREADS"] = str(threads)
+    sys.path.insert(0, str(REPO / "tests"))
+    import numpy as np
+    import oracle_lib
+    orc = oracle_lib.Oracle()
+    out = {"digests": {str(m): orc.keccak_digest(m - 16).hex() for m in range(22, 35)}, "proofs": []}
+    for n in KECCAK_SIZES:
+        seed = 0xC0FFEE_BEEF ^ n
+        states = orc.keccak_bench_inputs(n, seed)
+        n_log = max(3, (n - 1).bit_length())
+        z, a, b = orc.keccak_witness(states, n_log)
+        assert np.array_equal(a & b, z), n
+        for i in range(1 << n_log):
+            s0 = states[i] if i < n else np.zeros(25, np.uint64)
+            assert np.array_equal(z[i, :25], s0) and np.array_equal(z[i, 32:57], orc.keccak_f(s0)), (n, i)
+        data = orc.prove_keccak(states)
+        assert orc.last_open_identity_ok(), n
+        out["proofs"].append({"n": n, "seed": seed, "domain": "flock-bench-v0", "m": 16 + n_log,
+                              "sha256": hashlib.sha256(data).hexdigest(), "size": len(data),
+                              "checked_by": "oracle: a & b = z and state_24 = keccak_f(state_0) in every block; "
+                                            "open claim identity"})
+        (HERE / "keccak_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
+
+
 SHA256_MERKLE = ((12, 0), (14, 0), (15, 0), (7, 2), (8, 3))
 
 
@@ -290,6 +330,7 @@ if __name__ == "__main__":
     ap.add_argument("--sha256", action="store_true")
     ap.add_argument("--sha256-merkle", action="store_true")
     ap.add_argument("--default-hashes", action="store_true")
+    ap.add_argument("--keccak", action="store_true")
     ap.add_argument("--gpu-harness", type=Path, metavar="VERIFIER")
     ap.add_argument("--sizes", default="19:2,20:2", help="LOG2:RUNS,... for --gpu-harness")
     ap.add_argument("--out", type=Path, default=HERE / "gpu_verified_proofs.json")
@@ -300,6 +341,8 @@ if __name__ == "__main__":
         sha256_proofs()
     elif a.sha256_merkle:
         sha256_merkle_proofs()
+    elif a.keccak:
+        keccak_proofs()
     elif a.default_hashes:
         default_hash_proofs()
     elif a.kernels:

@@ -79,6 +79,13 @@ class Oracle:
         L.flockref_prove_chain_blocks.argtypes = [vp, u32, ctypes.c_char_p, sz, vp, vp, sz, ctypes.POINTER(sz),
                                                   ctypes.POINTER(ctypes.c_int)]
         L.flockref_prove_records.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        L.flockref_keccak_f.argtypes = [vp]
+        L.flockref_keccak_bench_inputs.argtypes = [sz, u64, vp]
+        L.flockref_keccak_digest.argtypes = [u32, vp]
+        L.flockref_keccak_witness.argtypes = [vp, sz, u32, vp, vp, vp]
+        L.flockref_keccak_comb.argtypes = [vp, vp, vp]
+        L.flockref_prove_keccak.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        L.flockref_last_open_identity_ok.argtypes = []
         L.flockref_time_prove.argtypes = [u32, u64, ctypes.POINTER(sz)]
         L.flockref_time_prove.restype = ctypes.c_double
         self.L = L
@@ -98,6 +105,50 @@ class Oracle:
         out = np.zeros((2 * n_leaves - 1) * 32, np.uint8)
         self.L.flockref_merkle_tree_hash(_p(data), n_leaves, leaf_size, {"sha256": 0, "blake3": 1}[hash], _p(out))
         return out
+
+    # ---- Keccak-f[1600] permutations (r1cs_hashes/keccak.rs); a state is 25 u64 lanes
+    def keccak_f(self, lanes) -> np.ndarray:
+        s = np.array(lanes, np.uint64).copy()
+        self.L.flockref_keccak_f(_p(s))
+        return s
+
+    def keccak_bench_inputs(self, n: int, seed: int) -> np.ndarray:
+        out = np.zeros((n, 25), np.uint64)
+        self.L.flockref_keccak_bench_inputs(n, seed, _p(out))
+        return out
+
+    def keccak_digest(self, n_log: int) -> bytes:
+        out = np.zeros(32, np.uint8)
+        self.L.flockref_keccak_digest(n_log, _p(out))
+        return out.tobytes()
+
+    def keccak_witness(self, states: np.ndarray, n_log: int):
+        states = np.ascontiguousarray(states, np.uint64).reshape(-1, 25)
+        z, a, b = (np.zeros((1 << n_log, 1024), np.uint64) for _ in range(3))
+        self.L.flockref_keccak_witness(_p(states), states.shape[0], n_log, _p(z), _p(a), _p(b))
+        return z, a, b
+
+    def keccak_comb(self, alpha, e: np.ndarray) -> np.ndarray:
+        """alpha A^T e + B^T e over a block's 2^16 rows (e: 2^16 x (lo, hi))."""
+        al = np.array(alpha, np.uint64)
+        e = np.ascontiguousarray(e, np.uint64).reshape(1 << 16, 2)
+        out = np.zeros((1 << 16, 2), np.uint64)
+        self.L.flockref_keccak_comb(_p(al), _p(e), _p(out))
+        return out
+
+    def prove_keccak(self, states: np.ndarray, domain: bytes = b"flock-bench-v0") -> bytes:
+        states = np.ascontiguousarray(states, np.uint64).reshape(-1, 25)
+        buf = np.zeros(2_000_000, np.uint8)
+        n = ctypes.c_size_t()
+        rc = self.L.flockref_prove_keccak(_p(states), states.shape[0], domain, len(domain), _p(buf), buf.size,
+                                         ctypes.byref(n))
+        assert rc == 0, rc
+        return buf[: n.value].tobytes()
+
+    def last_open_identity_ok(self) -> bool:
+        """The batched open's claim identity of this thread's last Keccak,
+        chain or Merkle-path proof."""
+        return bool(self.L.flockref_last_open_identity_ok())
 
     # ---- SHA-256 compressions (r1cs_hashes/sha2.rs)
     def sha256_compress(self, h, m) -> np.ndarray:

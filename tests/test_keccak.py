@@ -1,0 +1,144 @@
+"""The Keccak-f[1600] statement on the CPU (crates/flock-prover/src/
+r1cs_hashes/keccak.rs): the oracle's permutation against the SHA-3 standard
+(hashlib's SHA3-256 and SHAKE128 of single-block messages), the product
+library's host permutation and bench inputs against the oracle, the oracle's
+row witness against the R1CS semantics (a & b = z, state_24 = keccak_f(state_0),
+constant wire, zero padding; the reference's witness and roundtrip tests,
+keccak.rs:1580-1770), its lincheck walker against the witness through random
+parity checks (A z = a and B z = b, read through alpha A^T e + B^T e), the
+statement digests, and the oracle's proofs against the committed fixtures."""
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "keccak_proofs.json"
+
+
+def _absorb(block: bytes) -> np.ndarray:
+    """A zero state XOR a full-rate block (little-endian lanes)."""
+    s = np.zeros(25, np.uint64)
+    w = np.frombuffer(block + b"\0" * (200 - len(block)), "<u8")
+    return s ^ w
+
+
+def _sponge_one_block(keccak_f, msg: bytes, rate: int, pad: int, out_len: int) -> bytes:
+    blk = bytearray(msg + bytes([pad]) + b"\0" * (rate - len(msg) - 1))
+    blk[rate - 1] ^= 0x80
+    return keccak_f(_absorb(bytes(blk))).astype("<u8").tobytes()[:out_len]
+
+
+@pytest.mark.parametrize("msg", [b"", b"abc", b"flock keccak-f[1600]", bytes(range(100))])
+def test_oracle_permutation_is_sha3(oracle, msg):
+    assert _sponge_one_block(oracle.keccak_f, msg, 136, 0x06, 32) == hashlib.sha3_256(msg).digest()
+    assert _sponge_one_block(oracle.keccak_f, msg, 168, 0x1F, 64) == hashlib.shake_128(msg).digest(64)
+
+
+def test_zero_state_known_answer(oracle):
+    """keccak_f of the zero state (the Keccak team's known answer, lane 0)."""
+    assert int(oracle.keccak_f(np.zeros(25, np.uint64))[0]) == 0xF1258F7940E1DDE7
+
+
+def test_product_host_permutation_matches_oracle(oracle):
+    import flockgpu
+    rng = np.random.default_rng(11)
+    for _ in range(16):
+        s = rng.integers(0, 2**63, 25, np.uint64) ^ (rng.integers(0, 2, 25, np.uint64) << np.uint64(63))
+        assert np.array_equal(flockgpu.keccak_f(s), oracle.keccak_f(s))
+    assert _sponge_one_block(flockgpu.keccak_f, b"abc", 136, 0x06, 32) == hashlib.sha3_256(b"abc").digest()
+
+
+def test_bench_inputs_match(oracle):
+    import flockgpu
+    for n, seed in ((8, 1), (100, flockgpu.keccak_bench_seed(100))):
+        assert np.array_equal(flockgpu.keccak_bench_inputs(n, seed), oracle.keccak_bench_inputs(n, seed))
+
+
+def _bits(v):
+    return np.unpackbits(np.ascontiguousarray(v).view(np.uint8), axis=-1, bitorder="little")
+
+
+def test_witness_rows(oracle):
+    """a & b == z in every row; state_0 and state_24 (words 0..24 and 32..56)
+    are the input and keccak_f of it with b = 1; the constant word 64 is 1;
+    t_r fills words 65..664 and everything after is zero; padding blocks hold
+    keccak_f of the zero state."""
+    n_log, n = 3, 5
+    st = oracle.keccak_bench_inputs(n, 21)
+    z, a, b = oracle.keccak_witness(st, n_log)
+    assert np.array_equal(a & b, z)
+    ones = np.full(25, 2**64 - 1, np.uint64)
+    for i in range(1 << n_log):
+        s0 = st[i] if i < n else np.zeros(25, np.uint64)
+        assert np.array_equal(z[i, :25], s0) and np.array_equal(a[i, :25], s0) and np.array_equal(b[i, :25], ones)
+        s24 = oracle.keccak_f(s0)
+        assert np.array_equal(z[i, 32:57], s24) and np.array_equal(b[i, 32:57], ones)
+        assert z[i, 64] == a[i, 64] == b[i, 64] == 1
+        assert not z[i, 25:32].any() and not z[i, 57:64].any()
+        assert not (z[i, 665:].any() or a[i, 665:].any() or b[i, 665:].any())
+
+
+def _parity_checks(oracle, z, a, b, seed):
+    """<e, a> == <A^T e, z> and <e, b> == <B^T e, z> for 128 random 0/1
+    vectors e at once (bit k of each F128 of e is vector k)."""
+    rng = np.random.default_rng(seed)
+    e = rng.integers(0, 2**63, (1 << 16, 2), np.uint64) ^ (rng.integers(0, 2, (1 << 16, 2), np.uint64)
+                                                          << np.uint64(63))
+    bt = oracle.keccak_comb((0, 0), e)        # alpha = 0: B^T e
+    at = oracle.keccak_comb((1, 0), e) ^ bt    # alpha = 1: (A + B)^T e
+    zb, ab, bb = _bits(z).astype(bool), _bits(a).astype(bool), _bits(b).astype(bool)
+    ok_a = np.array_equal(np.bitwise_xor.reduce(e[ab], axis=0), np.bitwise_xor.reduce(at[zb], axis=0))
+    ok_b = np.array_equal(np.bitwise_xor.reduce(e[bb], axis=0), np.bitwise_xor.reduce(bt[zb], axis=0))
+    return ok_a and ok_b
+
+
+def test_walker_matches_witness(oracle):
+    """The lincheck walker (KeccakLincheckCircuit::fold_alpha_batched,
+    keccak.rs:681-848) applies the matrices the witness satisfies: 128 random
+    parity checks of A z = a and B z = b per block, for bench states, the
+    zero state and the all-ones state."""
+    states = np.concatenate([oracle.keccak_bench_inputs(2, 4), np.zeros((1, 25), np.uint64),
+                             np.full((1, 25), 2**64 - 1, np.uint64)])
+    z, a, b = oracle.keccak_witness(states, 3)
+    for i in range(4):
+        assert _parity_checks(oracle, z[i], a[i], b[i], 100 + i), i
+
+
+def test_tampered_witness_fails_the_walker(oracle):
+    """A flipped bit of z in state_0 or a t_r row breaks A z = a or B z = b
+    (the walker reads every column those rows feed); a flipped state_24 bit
+    keeps A z = a (its pin row's A side is the recurrence, its z column is
+    read only through C = I) and breaks (A z)(B z) = z instead."""
+    z, a, b = oracle.keccak_witness(oracle.keccak_bench_inputs(1, 8), 3)
+    for bit in (3, 64 * 7 + 9, 4160 + 1600 * 11 + 100, 4160 + 1600 * 23 + 1599):
+        zz = z[0].copy()
+        zz[bit // 64] ^= np.uint64(1) << np.uint64(bit % 64)
+        assert not _parity_checks(oracle, zz, a[0], b[0], 7), bit
+    bit = 2048 + 64 * 24 + 63
+    zz = z[0].copy()
+    zz[bit // 64] ^= np.uint64(1) << np.uint64(bit % 64)
+    assert _parity_checks(oracle, zz, a[0], b[0], 7) and not np.array_equal(a[0] & b[0], zz)
+
+
+def test_product_statement_digest_matches_oracle(oracle):
+    import flockgpu
+    for m in (22, 24, 29, 34):
+        assert flockgpu.keccak_statement_digest(m) == oracle.keccak_digest(m - 16)
+    assert flockgpu.keccak_statement_digest(24) != flockgpu.sha256_statement_digest(24)
+    assert flockgpu.keccak_statement_digest(24) != oracle.statement_digest(10)
+
+
+def test_fixture_digests():
+    import flockgpu
+    g = json.loads(GOLDEN.read_text())
+    for m, d in g["digests"].items():
+        assert flockgpu.keccak_statement_digest(int(m)) == bytes.fromhex(d), m
+
+
+def test_oracle_proof_matches_fixture(oracle):
+    g = json.loads(GOLDEN.read_text())
+    e = next(p for p in g["proofs"] if p["n"] == 64)
+    proof = oracle.prove_keccak(oracle.keccak_bench_inputs(e["n"], e["seed"]))
+    assert hashlib.sha256(proof).hexdigest() == e["sha256"] and len(proof) == e["size"]
