@@ -86,6 +86,7 @@ class Oracle:
         L.flockref_keccak_comb.argtypes = [vp, vp, vp]
         L.flockref_prove_keccak.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_last_open_identity_ok.argtypes = []
+        L.flockref_round1_deg4.argtypes = [vp, vp, vp, vp, vp, u32, vp, vp, vp]
         L.flockref_time_prove.argtypes = [u32, u64, ctypes.POINTER(sz)]
         L.flockref_time_prove.restype = ctypes.c_double
         self.L = L
@@ -149,6 +150,16 @@ class Oracle:
         """The batched open's claim identity of this thread's last Keccak,
         chain or Merkle-path proof."""
         return bool(self.L.flockref_last_open_identity_ok())
+
+    # ---- degree-4 zerocheck round 1 (zerocheck/univariate_skip_deg4.rs)
+    def round1_deg4(self, a, b, c, d, z, m: int, r: np.ndarray):
+        """round1_deg4_naive over packed rows (2^(m-6) u64 each) and r
+        ((m, 2) u64): (p_abcd, p_z), each (192, 2) u64."""
+        vs = [np.ascontiguousarray(v, np.uint64) for v in (a, b, c, d, z)]
+        rr = np.ascontiguousarray(r, np.uint64).reshape(m, 2)
+        pa, pz = np.zeros((192, 2), np.uint64), np.zeros((192, 2), np.uint64)
+        self.L.flockref_round1_deg4(*[_p(v) for v in vs], m, _p(rr), _p(pa), _p(pz))
+        return pa, pz
 
     # ---- SHA-256 compressions (r1cs_hashes/sha2.rs)
     def sha256_compress(self, h, m) -> np.ndarray:
