@@ -422,6 +422,21 @@ def product_ceiling(plan_desc: str) -> tuple:
                                 "144 IMAD.WIDE per product")
 
 
+def round1_deg4_rows(ctx, hbm: float, sizes=(16, 18, 20, 22, 24, 26)) -> list:
+    """Degree-4 zerocheck round 1 (round1_deg4_naive's message, the sizes of
+    benches/round1_deg4.rs): device-resident seeded bit vectors, mean device
+    time of one message (eq table + kernel).  Algorithmic bytes: the five bit
+    vectors (5 * 2^m / 8) and the eq table (16 * 2^(m-6), written and read)."""
+    out = []
+    for m in sizes:
+        ms, _, _ = ctx.bench_round1_deg4(m, 0xDEC0DE ^ m, iters=5)
+        byts = 5 * (1 << m) // 8 + 2 * 16 * (1 << (m - 6))
+        out.append({"kernel": "zerocheck_round1_deg4", "m": m, "ms": ms, "constraints_per_s": (1 << m) / (ms / 1e3),
+                    "gbs": byts / (ms / 1e3) / 1e9, "hbm_frac": byts / (ms / 1e3) / 1e9 / hbm,
+                    "l2_resident": byts < (126 << 20)})
+    return out
+
+
 def kernel_report(device: int) -> list:
     """Kernel microbenchmarks (additive NTT / RS encode, Merkle trees, degree-2
     and degree-3 sumcheck rounds) on device-resident seeded inputs, CUDA-event
@@ -474,6 +489,7 @@ def kernel_report(device: int) -> list:
             rows.append({"kernel": "sumcheck_deg3_fold_round", "n": n, "ms": ms, "gbs": byts / (ms / 1e3) / 1e9,
                          "hbm_frac": byts / (ms / 1e3) / 1e9 / hbm, "gf_products_per_s": prods / (ms / 1e3),
                          "int_frac": prods / (ms / 1e3) / ipk, "l2_resident": 16 * 2 * n < (126 << 20)})
+        rows += round1_deg4_rows(ctx, hbm)
     finally:
         ctx.close()
     for r in rows:
@@ -568,6 +584,47 @@ def sha256_report(ctx, sizes=(16, 18), steps: int = 5) -> dict:
               "proof_bytes": size, "phases_ms": {k: round(v, 3) for k, v in ph.items()}}
     return {"sha256": {"statement": "SHA-256 compressions, one per 2^15-bit block (hybrid R1CS, sha2.rs)",
                        "proofs": rows, "merkle_path": merkle}}
+
+
+KECCAK_SIZES = (6144, 8192, 12288, 24576, 65536)
+
+
+def keccak_report(ctx, sizes=KECCAK_SIZES, steps: int = 5) -> dict:
+    """The Keccak-f[1600] statement (KeccakSetup::prove_fast, r1cs_hashes/
+    keccak.rs, one permutation per 2^16-bit block) at the permutation counts
+    of the reference's benches/keccak3_proof.rs:301-305 and at 2^16, states
+    from that bench's generator.  Device time is the sum of the proof's phase
+    events (states generated on the GPU); e2e goes through flock_keccak_prove
+    from pinned host states (H2D of the states, prove, D2H of the bundle), host
+    clock, medians of `steps`."""
+    import flockgpu
+    rows = []
+    for n in sizes:
+        prover = flockgpu.KeccakProver(ctx, n)
+        states = flockgpu.PinnedArray((n, 25), np.uint64)
+        states.array[:] = flockgpu.keccak_bench_inputs(n, flockgpu.keccak_bench_seed(n))
+        for _ in range(2):
+            prover.prove(states.array)
+        dev, wall = [], []
+        for i in range(steps):
+            prover.prove_seed(flockgpu.keccak_bench_seed(n, i + 1))
+            ph = prover.phase_ms()
+            dev.append(sum(ph.values()))
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            size = len(prover.prove(states.array))
+            wall.append(time.perf_counter() - t0)
+        why = ctx.keccak_verify(prover.prove(states.array))
+        prover.close()
+        if why:
+            raise SystemExit(f"keccak_report: proof rejected: {why}")
+        d, e = pct(dev, 0.5), pct(wall, 0.5)
+        n_log = max(3, (n - 1).bit_length())
+        rows.append({"n": n, "m": 16 + n_log, "device_ms_median": d, "device_permutations_per_s": n / (d / 1e3),
+                     "e2e_ms_median": e * 1e3, "e2e_permutations_per_s": n / e, "proof_bytes": size,
+                     "h2d_bytes_per_proof": n * 200, "phases_ms": {k: round(v, 3) for k, v in ph.items()}})
+    return {"keccak": {"statement": "Keccak-f[1600] permutations, one per 2^16-bit block (keccak.rs)",
+                       "proofs": rows}}
 
 
 def verify_report(prover, log2: int, reps: int = 3) -> dict:
@@ -677,6 +734,8 @@ def run_ours(args, world, rank, local):
         line.update(verify_report(prover, log2))
     if world == 1 and not args.no_sha256:
         line.update(sha256_report(ctx))
+    if world == 1 and not args.no_keccak:
+        line.update(keccak_report(ctx))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample()
     if world == 1 and not args.no_serve:
@@ -699,6 +758,9 @@ def main():
     ap.add_argument("--no-sha256", action="store_true", help="skip the SHA-256 statement measurement")
     ap.add_argument("--sha256", default=None, metavar="LOG2[,LOG2...]",
                     help="only the SHA-256 statement report at these sizes")
+    ap.add_argument("--no-keccak", action="store_true", help="skip the Keccak statement measurement")
+    ap.add_argument("--keccak", default=None, metavar="N[,N...]",
+                    help="only the Keccak statement report at these permutation counts")
     ap.add_argument("--ntt-case", default=None, metavar="LOG_MSG,LANES,RATE,PLAN",
                     help="one RS encode with candidate pass plan PLAN (no autotuning launches): the case that "
                          "the NTT's ncu captures profile")
@@ -759,6 +821,12 @@ def main():
         import flockgpu
         ctx = flockgpu.Context(0)
         print(json.dumps(sha256_report(ctx, tuple(int(x) for x in args.sha256.split(",")))), flush=True)
+        ctx.close()
+        return
+    if args.keccak:
+        import flockgpu
+        ctx = flockgpu.Context(0)
+        print(json.dumps(keccak_report(ctx, tuple(int(x) for x in args.keccak.split(",")))), flush=True)
         ctx.close()
         return
     if args.kernels:

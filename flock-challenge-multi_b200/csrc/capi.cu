@@ -1270,4 +1270,100 @@ int flock_bench_sumcheck3(flock_ctx* c, size_t n, int iters, double* ms) {
   });
 }
 
+// ---- degree-4 zerocheck round 1 (zerocheck/univariate_skip_deg4.rs)
+namespace {
+// eq(r, .) over n <= 30 variables on the device, low variables first
+void eq_device(const f128* r, int n, f128* lo, f128* hi, f128* out, cudaStream_t st) {
+  const int s = std::min(n, 12);
+  eq_build(r, s, flock::hone(), lo, st);
+  eq_build(r + s, n - s, flock::hone(), hi, st);
+  eq_split(lo, hi, s, (size_t)1 << n, out, st);
+}
+struct Deg4Bufs {
+  size_t rows;
+  DevBuf<uint64_t> v;  // a, b, c, d, z rows
+  DevBuf<f128> eq, lo, hi, sums;  // sums: H (1536) then Zs (64)
+  DevBuf<uint8_t> tab;
+  explicit Deg4Bufs(uint32_t m)
+      : rows((size_t)1 << (m - 6)), v(5 * rows), eq(rows), lo(1 << 12), hi(std::max<size_t>(1, rows >> 12)),
+        sums(1600), tab(deg4_tables_bytes()) {}
+  void run(const std::vector<f128>& r, int m, int sms, cudaStream_t st) {
+    eq_device(r.data() + 6, m - 6, lo.p, hi.p, eq.p, st);
+    CK(cudaMemsetAsync(sums.p, 0, 1600 * sizeof(f128), st));
+    round1_deg4(v.p, v.p + rows, v.p + 2 * rows, v.p + 3 * rows, v.p + 4 * rows, eq.p, rows, tab.p, sums.p,
+                sums.p + 1536, 2 * sms, st);
+  }
+  void finish(uint64_t* p_abcd, uint64_t* p_z, cudaStream_t st) {
+    std::vector<f128> h(1600);
+    CK(cudaMemcpyAsync(h.data(), sums.p, 1600 * sizeof(f128), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    round1_deg4_finish(h.data(), h.data() + 1536, reinterpret_cast<f128*>(p_abcd), reinterpret_cast<f128*>(p_z));
+  }
+};
+int sm_count(int device) {
+  int n = 0;
+  CK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device));
+  return n;
+}
+std::vector<uint8_t> deg4_host_tables() {
+  std::vector<uint8_t> t(deg4_tables_bytes());
+  deg4_build_tables(t.data());
+  return t;
+}
+}  // namespace
+
+int flock_zerocheck_round1_deg4(flock_ctx* c, const uint64_t* a, const uint64_t* b, const uint64_t* cc,
+                                const uint64_t* d, const uint64_t* z, uint32_t m, const uint64_t* r, uint64_t* p_abcd,
+                                uint64_t* p_z) {
+  if (!c || !a || !b || !cc || !d || !z || !r || !p_abcd || !p_z) return FLOCK_ERR_ARG;
+  if (m < 6 || m > 30) {
+    c->err = "round1_deg4: m must be in 6..=30";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(c, [&] {
+    DeviceScope on(c->device);
+    Deg4Bufs B(m);
+    const uint64_t* in[5] = {a, b, cc, d, z};
+    for (int f = 0; f < 5; f++)
+      CK(cudaMemcpyAsync(B.v.p + f * B.rows, in[f], B.rows * 8, cudaMemcpyHostToDevice, c->st));
+    static const std::vector<uint8_t> tabs = deg4_host_tables();
+    CK(cudaMemcpyAsync(B.tab.p, tabs.data(), tabs.size(), cudaMemcpyHostToDevice, c->st));
+    std::vector<f128> rv(m);
+    memcpy(rv.data(), r, m * sizeof(f128));
+    B.run(rv, (int)m, sm_count(c->device), c->st);
+    B.finish(p_abcd, p_z, c->st);
+    return FLOCK_OK;
+  });
+}
+
+int flock_bench_round1_deg4(flock_ctx* c, uint32_t m, uint64_t seed, int iters, double* ms, uint64_t* p_abcd,
+                            uint64_t* p_z) {
+  if (!c || !ms || iters < 1 || m < 6 || m > 30) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    DeviceScope on(c->device);
+    Deg4Bufs B(m);
+    k_fill<<<(unsigned)((5 * B.rows + 255) / 256), 256, 0, c->st>>>(B.v.p, 5 * B.rows, seed);
+    static const std::vector<uint8_t> tabs = deg4_host_tables();
+    CK(cudaMemcpyAsync(B.tab.p, tabs.data(), tabs.size(), cudaMemcpyHostToDevice, c->st));
+    // r: SplitMix64 from seed ^ 1, lo then hi per value
+    std::vector<f128> rv(m);
+    uint64_t st = seed ^ 1;
+    auto nx = [&] {
+      st += 0x9E3779B97F4A7C15ull;
+      uint64_t x = st;
+      x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+      x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+      return x ^ (x >> 31);
+    };
+    for (auto& v : rv) {
+      v.lo = nx();
+      v.hi = nx();
+    }
+    const int sms = sm_count(c->device);
+    *ms = time_launches(c->st, iters, [&] { B.run(rv, (int)m, sms, c->st); });
+    if (p_abcd && p_z) B.finish(p_abcd, p_z, c->st);
+    return FLOCK_OK;
+  });
+}
+
 }  // extern "C"

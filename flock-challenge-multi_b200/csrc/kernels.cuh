@@ -101,6 +101,17 @@ void launch_witness_keccak(const uint64_t* states, uint64_t seed, uint32_t n_per
 const uint64_t* keccak_masks(int device);
 size_t keccak_comb_scratch();
 void keccak_comb(const f128* e, f128 alpha, f128 beta, const uint64_t* masks, f128* W, f128* comb, cudaStream_t s);
+// Degree-4 zerocheck round 1 (zerocheck/univariate_skip_deg4.rs): device
+// sums H[8 l + k] (eq over the rows whose a b c d at lambda 64 + l has bit k)
+// and Zs[s] (eq over the rows whose z bit s is set), XOR-ed into H (1536
+// values) and Zs (64 values); round1_deg4_finish turns them into the two
+// 192-value messages on the host.  tables: deg4_tables_bytes() on the device,
+// filled by deg4_build_tables on the host.
+size_t deg4_tables_bytes();
+void deg4_build_tables(uint8_t* host);
+void round1_deg4(const uint64_t* a, const uint64_t* b, const uint64_t* c, const uint64_t* d, const uint64_t* z,
+                 const f128* eq, size_t n_rows, const uint8_t* tables, f128* H, f128* Zs, int grid, cudaStream_t s);
+void round1_deg4_finish(const f128* H, const f128* Zs, f128* p_abcd, f128* p_z);
 // K1
 // NTT pass plans: the passes (first layer l0, layer count R, 2^lgs lanes per
 // tile, threads per CTA) that cover layers layer_begin..log_d-1.

@@ -41,6 +41,7 @@ EXPORTS = (
     "flock_ctx_set_transcript", "flock_challenger_create_hash", "flock_merkle_tree_hash",
     "flock_keccak_setup_create", "flock_keccak_prove", "flock_keccak_verify_bundle", "flock_keccak_f",
     "flock_keccak_bench_inputs", "flock_keccak_statement_digest", "flock_keccak_witness", "flock_keccak_comb",
+    "flock_zerocheck_round1_deg4", "flock_bench_round1_deg4",
 )
 # the hash behind Merkle trees / the transcript (HashKind discriminants)
 HASH = {"sha256": 0, "blake3": 1}
@@ -124,6 +125,8 @@ def load() -> ctypes.CDLL:
         lib.flock_merkle_root_noalloc.argtypes = [vp, sz, sz, vp, vp]
         lib.flock_serve_start.argtypes = [vp, i32]
         lib.flock_serve_prewarm.argtypes = [vp, u32, i32, ctypes.POINTER(i32)]
+        lib.flock_zerocheck_round1_deg4.argtypes = [vp, vp, vp, vp, vp, vp, u32, vp, vp, vp]
+        lib.flock_bench_round1_deg4.argtypes = [vp, u32, u64, i32, ctypes.POINTER(ctypes.c_double), vp, vp]
         lib.flock_keccak_setup_create.argtypes = [vp, sz, i32, i32, ctypes.POINTER(vp)]
         lib.flock_keccak_prove.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_keccak_verify_bundle.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
@@ -444,6 +447,25 @@ class Context:
         out = np.zeros((1 << 16, 2), np.uint64)
         self._check(self.lib.flock_keccak_comb(self.h, _ptr(e), _ptr(al), _ptr(be), _ptr(out)), "keccak_comb")
         return out
+
+    def round1_deg4(self, a, b, c, d, z, m: int, r):
+        """round1_deg4_naive (univariate_skip_deg4.rs:77-165) on the GPU:
+        packed rows (2^(m-6) u64 per vector), r ((m, 2) u64) -> (p_abcd, p_z),
+        each (192, 2) u64."""
+        vs = [np.ascontiguousarray(v, np.uint64) for v in (a, b, c, d, z)]
+        rr = np.ascontiguousarray(r, np.uint64).reshape(m, 2)
+        pa, pz = np.zeros((192, 2), np.uint64), np.zeros((192, 2), np.uint64)
+        self._check(self.lib.flock_zerocheck_round1_deg4(self.h, *[_ptr(v) for v in vs], m, _ptr(rr), _ptr(pa),
+                                                         _ptr(pz)), "zerocheck_round1_deg4")
+        return pa, pz
+
+    def bench_round1_deg4(self, m: int, seed: int = 1, iters: int = 10):
+        """(mean ms, p_abcd, p_z) of the seeded degree-4 round-1 benchmark."""
+        ms = ctypes.c_double()
+        pa, pz = np.zeros((192, 2), np.uint64), np.zeros((192, 2), np.uint64)
+        self._check(self.lib.flock_bench_round1_deg4(self.h, m, seed, iters, ctypes.byref(ms), _ptr(pa), _ptr(pz)),
+                    "bench_round1_deg4")
+        return ms.value, pa, pz
 
     def serve_verify(self, on: bool = True) -> None:
         """Self-check every served / batched proof with the verifier."""

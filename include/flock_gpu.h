@@ -52,6 +52,12 @@
  *                           generate_compressions (benchmark-tools/common/src/lib.rs:25)
  *  - flock_pow           <- FsChallenger::grind_pow (crates/flock-core/src/challenger.rs:384)
  *  - flock_f128_mul      <- F128 * F128 (crates/flock-core/src/field/gf2_128.rs:140-165)
+ *  - flock_keccak_*      <- KeccakSetup::{new, prove_fast, verify}, keccak_f
+ *                           (crates/flock-prover/src/r1cs_hashes/keccak.rs:
+ *                           423-428, 863-998)
+ *  - flock_zerocheck_round1_deg4
+ *                        <- round1_deg4_naive (crates/flock-core/src/zerocheck/
+ *                           univariate_skip_deg4.rs:77-165)
  */
 #ifndef FLOCK_GPU_H
 #define FLOCK_GPU_H
@@ -291,6 +297,25 @@ int flock_keccak_witness(flock_ctx* ctx, const flock_keccak_state* states, size_
  * [const] over the 2^16 rows of a block, on the GPU (e, comb: 2^16 F128 as
  * lo, hi u64 pairs; alpha, beta: one F128). */
 int flock_keccak_comb(flock_ctx* ctx, const uint64_t* e, const uint64_t* alpha, const uint64_t* beta, uint64_t* comb);
+
+/* ---- Degree-4 zerocheck round 1 (crates/flock-core/src/zerocheck/univariate_skip_deg4.rs) ----
+ * round1_deg4_naive(a, b, c, d, z, m, r) (univariate_skip_deg4.rs:77-165)
+ * on the GPU: the round-1 message of the constraint a b c d + z = 0 over 2^m
+ * rows, each factor extended from S = {0..63} to Lambda4 = {64..255} of
+ * GF(2^8).  The bit vectors are packed, 2^(m-6) u64 each (bit s of word x is
+ * index 64 x + s); r: m F128 (lo, hi); p_abcd, p_z: 192 F128 each, the
+ * evaluations at lambda = 64 + i.  6 <= m <= 30. */
+int flock_zerocheck_round1_deg4(flock_ctx* ctx, const uint64_t* a, const uint64_t* b, const uint64_t* c,
+                                const uint64_t* d, const uint64_t* z, uint32_t m, const uint64_t* r, uint64_t* p_abcd,
+                                uint64_t* p_z);
+/* Microbenchmark (benches/round1_deg4.rs): device-resident inputs, five
+ * vectors of words SplitMix64(seed) (word i of the concatenation a|b|c|d|z is
+ * the draw at state seed + (i + 1) gamma) and r from SplitMix64(seed ^ 1)
+ * (lo then hi); *ms = mean device time of one message (eq table + kernel)
+ * over `iters` after a warm-up; the last message into p_abcd / p_z when both
+ * are non-null. */
+int flock_bench_round1_deg4(flock_ctx* ctx, uint32_t m, uint64_t seed, int iters, double* ms, uint64_t* p_abcd,
+                            uint64_t* p_z);
 
 /* The flock_chain CLI's honest chain of `steps` records: record i has
  * cv = x_i (x_0 = initial_cv, or the BLAKE3 IV when NULL), 16 message words

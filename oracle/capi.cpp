@@ -387,6 +387,18 @@ int flockref_prove_keccak(const uint64_t* states, size_t n, const uint8_t* domai
   }
 }
 
+// round1_deg4_naive over packed rows (2^(m-6) u64 per vector); r: m F128;
+// outputs: 192 F128 each
+void flockref_round1_deg4(const uint64_t* a, const uint64_t* b, const uint64_t* c, const uint64_t* d,
+                          const uint64_t* z, uint32_t m, const uint64_t* r, uint64_t* p_abcd, uint64_t* p_z) {
+  std::vector<F128> rv(m);
+  memcpy(rv.data(), r, m * 16);
+  std::vector<F128> pa, pz;
+  round1_deg4(a, b, c, d, z, (int)m, rv, pa, pz);
+  memcpy(p_abcd, pa.data(), 192 * 16);
+  memcpy(p_z, pz.data(), 192 * 16);
+}
+
 // Whether the last proof on this thread that records it (chain, Merkle-path
 // and Keccak proofs) had sum_j b_combined[j] z[j] == target.
 int flockref_last_open_identity_ok(void) { return last_open_identity_ok() ? 1 : 0; }

@@ -359,6 +359,13 @@ bool open_identity(const std::vector<F128>& z, const std::vector<F128>& bc, F128
 // that identity, as checked by the last prove_with with a hook on this thread
 bool& last_open_identity_ok();
 
+// Degree-4 zerocheck round 1 (zerocheck/univariate_skip_deg4.rs:77-165,
+// round1_deg4_naive): five bit vectors of 2^m bits as 2^(m-6) u64 rows (bit s
+// of row x is index 64 x + s), r of length m; p_abcd and p_z get the 192
+// evaluations on Lambda4 = {64..255}.
+void round1_deg4(const uint64_t* a, const uint64_t* b, const uint64_t* c, const uint64_t* d, const uint64_t* z,
+                 int m, const std::vector<F128>& r, std::vector<F128>& p_abcd, std::vector<F128>& p_z);
+
 // ---------------------------------------------------------------------------
 // BLAKE3 hash chain.  crates/flock-prover/src/chain.rs (shift argument),
 // r1cs_hashes/chain_common.rs (region fold, claim point, generic prover),
