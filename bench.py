@@ -761,6 +761,8 @@ def main():
     ap.add_argument("--no-keccak", action="store_true", help="skip the Keccak statement measurement")
     ap.add_argument("--keccak", default=None, metavar="N[,N...]",
                     help="only the Keccak statement report at these permutation counts")
+    ap.add_argument("--deg4", default=None, metavar="M[,M...]",
+                    help="only the degree-4 zerocheck round-1 microbenchmark at these m")
     ap.add_argument("--ntt-case", default=None, metavar="LOG_MSG,LANES,RATE,PLAN",
                     help="one RS encode with candidate pass plan PLAN (no autotuning launches): the case that "
                          "the NTT's ncu captures profile")
@@ -821,6 +823,13 @@ def main():
         import flockgpu
         ctx = flockgpu.Context(0)
         print(json.dumps(sha256_report(ctx, tuple(int(x) for x in args.sha256.split(",")))), flush=True)
+        ctx.close()
+        return
+    if args.deg4:
+        import flockgpu
+        ctx = flockgpu.Context(0)
+        for row in round1_deg4_rows(ctx, peaks()[0], tuple(int(x) for x in args.deg4.split(","))):
+            print(json.dumps(row), flush=True)
         ctx.close()
         return
     if args.keccak:

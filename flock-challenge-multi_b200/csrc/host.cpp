@@ -84,17 +84,30 @@ std::vector<f128> heq(const std::vector<f128>& r) {
 }
 
 std::vector<f128> hlagrange(f128 z, int base) {
-  // L_i(z) = prod_{j != i} (z + s_j) / (s_i + s_j),  s_j = phi8(base + j)
-  std::vector<f128> w(64);
+  // L_i(z) = prod_{j != i} (z + s_j) / (s_i + s_j),  s_j = phi8(base + j).
+  // The denominators depend only on the nodes (one table per base, 0 or 64,
+  // built once); the numerators come from prefix and suffix products of
+  // (z + s_j), so a call costs 256 products and no inversion.
   const auto& P = kPhiArr;
-  for (int i = 0; i < 64; i++) {
-    f128 num = hone(), den = hone();
-    for (int j = 0; j < 64; j++) {
-      if (j == i) continue;
-      num = hmul(num, fx(z, P[base + j]));
-      den = hmul(den, fx(P[base + i], P[base + j]));
+  static std::once_flag once[2];
+  static std::array<f128, 64> inv_den[2];
+  const int t = base ? 1 : 0;
+  std::call_once(once[t], [&P, base, t] {
+    for (int i = 0; i < 64; i++) {
+      f128 den = hone();
+      for (int j = 0; j < 64; j++)
+        if (j != i) den = hmul(den, fx(P[base + i], P[base + j]));
+      inv_den[t][i] = hinv(den);
     }
-    w[i] = hmul(num, hinv(den));
+  });
+  f128 suf[65];
+  suf[64] = hone();
+  for (int j = 63; j >= 0; j--) suf[j] = hmul(suf[j + 1], fx(z, P[base + j]));
+  std::vector<f128> w(64);
+  f128 pre = hone();
+  for (int i = 0; i < 64; i++) {
+    w[i] = hmul(hmul(pre, suf[i + 1]), inv_den[t][i]);
+    pre = hmul(pre, fx(z, P[base + i]));
   }
   return w;
 }
