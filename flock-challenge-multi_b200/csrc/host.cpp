@@ -114,6 +114,44 @@ std::vector<f128> hlagrange(f128 z, int base) {
 
 uint8_t hgf8_mul(uint8_t a, uint8_t b) { return gf8_mul_slow(a, b); }
 
+// six rounds of swapping the off-diagonal j x j blocks inside every 2j x 2j block
+void transpose64(uint64_t a[64]) {
+  static const uint64_t M[6] = {0x00000000FFFFFFFFull, 0x0000FFFF0000FFFFull, 0x00FF00FF00FF00FFull,
+                                0x0F0F0F0F0F0F0F0Full, 0x3333333333333333ull, 0x5555555555555555ull};
+  for (int k = 0, j = 32; j; k++, j >>= 1)
+    for (int r = 0; r < 64; r++)
+      if (!(r & j)) {
+        const uint64_t t = ((a[r] >> j) ^ a[r | j]) & M[k];
+        a[r | j] ^= t;
+        a[r] ^= t << j;
+      }
+}
+
+std::vector<f128> transpose128(const std::vector<f128>& rows) {
+  uint64_t A[64], B[64], C[64], D[64];  // [rows 0..63 | 64..127] x [bits 0..63 | 64..127]
+  for (int i = 0; i < 64; i++) {
+    A[i] = rows[i].lo;
+    B[i] = rows[i].hi;
+    C[i] = rows[64 + i].lo;
+    D[i] = rows[64 + i].hi;
+  }
+  transpose64(A);
+  transpose64(B);
+  transpose64(C);
+  transpose64(D);
+  std::vector<f128> out(128);
+  for (int j = 0; j < 64; j++) {
+    out[j] = mk(A[j], C[j]);
+    out[64 + j] = mk(B[j], D[j]);
+  }
+  return out;
+}
+
+void subset_sums8(const f128* v8, f128* out) {
+  out[0] = mk(0, 0);
+  for (int v = 1; v < 256; v++) out[v] = fx(out[v & (v - 1)], v8[__builtin_ctz(v)]);
+}
+
 // --------------------------------------------------------------- BLAKE3 --
 const uint32_t kB3IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
                                 0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};

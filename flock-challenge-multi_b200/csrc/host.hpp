@@ -20,6 +20,12 @@ const f128* phi8_table();              // field/phi8.rs:18-1050 (basis-expanded)
 inline const f128 hone() { return mk(1, 0); }
 std::vector<f128> heq(const std::vector<f128>& r);           // eq table, bit i <-> r[i]
 std::vector<f128> hlagrange(f128 z, int node_base);           // 64 weights over phi8 nodes
+// 64 x 64 bit transpose in place (row r = a[r], column c = bit c)
+void transpose64(uint64_t a[64]);
+// 128 x 128 bit transpose: bit i of out[j] = bit j of rows[i] (128 rows)
+std::vector<f128> transpose128(const std::vector<f128>& rows);
+// out[v] = XOR of v8[j] over the set bits j of v, v < 256
+void subset_sums8(const f128* v8, f128* out);
 uint8_t hgf8_mul(uint8_t a, uint8_t b);
 
 // ---- BLAKE3 hasher (incremental, root / XOF) ----

@@ -572,13 +572,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   {
     std::vector<f128> L = hlagrange(zc_z, 0);
     std::vector<f128> lagt(8 * 256);
-    for (int k = 0; k < 8; k++)
-      for (int v = 0; v < 256; v++) {
-        f128 acc = mk(0, 0);
-        for (int j = 0; j < 8; j++)
-          if ((v >> j) & 1) acc = fx(acc, L[8 * k + j]);
-        lagt[k * 256 + v] = acc;
-      }
+    for (int k = 0; k < 8; k++) subset_sums8(L.data() + 8 * k, lagt.data() + k * 256);
     CK(cudaMemcpyAsync(lag, lagt.data(), lagt.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
     std::vector<f128> LL = hlagrange(zc_z, 64);
     f128 ce = mk(0, 0);
@@ -931,15 +925,9 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     std::vector<f128> rdp = tr.sample_vec(7);
     eqdd[k] = heq(rdp);
     // s_hat_u[b] bit i = bit b of s_hat_v[i];  claim = sum_b s_hat_u[b] eq''[b]
+    std::vector<f128> u = transpose128(sv);
     f128 c = mk(0, 0);
-    for (int bb = 0; bb < 128; bb++) {
-      f128 u = mk(0, 0);
-      for (int i = 0; i < 128; i++) {
-        uint64_t bit = bb < 64 ? (sv[i].lo >> bb) & 1 : (sv[i].hi >> (bb - 64)) & 1;
-        if (bit) { if (i < 64) u.lo |= 1ull << i; else u.hi |= 1ull << (i - 64); }
-      }
-      c = fx(c, hmul(u, eqdd[k][bb]));
-    }
+    for (int bb = 0; bb < 128; bb++) c = fx(c, hmul(u[bb], eqdd[k][bb]));
     claim[k] = c;
   }
   f128 gam[2] = {tr.sample(), tr.sample()};
@@ -957,13 +945,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     for (int k = 0; k < 2; k++) {
       std::vector<f128> sc(128);
       for (int bb = 0; bb < 128; bb++) sc[bb] = hmul(gam[k], eqdd[k][bb]);
-      for (int byte = 0; byte < 16; byte++)
-        for (int v = 0; v < 256; v++) {
-          f128 acc = mk(0, 0);
-          for (int j = 0; j < 8; j++)
-            if ((v >> j) & 1) acc = fx(acc, sc[8 * byte + j]);
-          T[(size_t)k * 4096 + byte * 256 + v] = acc;
-        }
+      for (int byte = 0; byte < 16; byte++) subset_sums8(sc.data() + 8 * byte, T.data() + (size_t)k * 4096 + byte * 256);
     }
     CK(cudaMemcpyAsync(bc_tabs, T.data(), T.size() * sizeof(f128), cudaMemcpyHostToDevice, st));
     // eq(suffix_k, i) = lo_k(i mod 2^lo_bits) * hi_k(i >> lo_bits), both tables

@@ -218,35 +218,9 @@ f128 interp_combined(const std::vector<f128>& v, f128 z) {
 struct TA {
   f128 e[128];
 };
-// 64 x 64 bit transpose in place (row r = a[r], column c = bit c): six rounds
-// of swapping the off-diagonal j x j blocks inside every 2j x 2j block.
-void transpose64(uint64_t a[64]) {
-  static const uint64_t M[6] = {0x00000000FFFFFFFFull, 0x0000FFFF0000FFFFull, 0x00FF00FF00FF00FFull,
-                                0x0F0F0F0F0F0F0F0Full, 0x3333333333333333ull, 0x5555555555555555ull};
-  for (int k = 0, j = 32; j; k++, j >>= 1)
-    for (int r = 0; r < 64; r++)
-      if (!(r & j)) {
-        const uint64_t t = ((a[r] >> j) ^ a[r | j]) & M[k];
-        a[r | j] ^= t;
-        a[r] ^= t << j;
-      }
-}
 void ta_transpose(TA& t) {
-  uint64_t A[64], B[64], C[64], D[64];  // [rows 0..63 | 64..127] x [bits 0..63 | 64..127]
-  for (int i = 0; i < 64; i++) {
-    A[i] = t.e[i].lo;
-    B[i] = t.e[i].hi;
-    C[i] = t.e[64 + i].lo;
-    D[i] = t.e[64 + i].hi;
-  }
-  transpose64(A);
-  transpose64(B);
-  transpose64(C);
-  transpose64(D);
-  for (int j = 0; j < 64; j++) {
-    t.e[j] = mk(A[j], C[j]);
-    t.e[64 + j] = mk(B[j], D[j]);
-  }
+  const std::vector<f128> out = transpose128(std::vector<f128>(t.e, t.e + 128));
+  for (int j = 0; j < 128; j++) t.e[j] = out[j];
 }
 void ta_scale(TA& t, f128 s) {
   for (auto& x : t.e) x = hmul(x, s);
