@@ -217,7 +217,7 @@ int flock_prove_seed(flock_setup* s, uint64_t seed, const uint8_t* domain, size_
 static bool is_blake3(flock_setup* s) {
   if (s->s->hash == flock::kHashBlake3) return true;
   s->ctx->err = std::string("this entry point proves BLAKE3 compressions; the setup is a ") +
-                (s->s->hash == flock::kHashKeccak ? "Keccak" : "SHA-256") + " statement";
+                (flock::is_keccak(s->s->hash) ? "Keccak" : "SHA-256") + " statement";
   return false;
 }
 
@@ -432,31 +432,102 @@ int flock_sha256_witness(flock_ctx* c, const flock_sha256_compression* comps, si
 
 // ---- Keccak-f[1600] permutations (r1cs_hashes/keccak.rs)
 static_assert(sizeof(flock_keccak_state) == 200, "flock_keccak_state is 25 u64");
-int flock_keccak_setup_create(flock_ctx* c, size_t n_keccaks, int hash, int profile, flock_setup** out) {
+namespace {
+// width 1: KeccakSetup of keccak.rs; 3: the 3-wide one of keccak3.rs
+int keccak_hash_of(int width) { return width == 3 ? flock::kHashKeccak3 : flock::kHashKeccak; }
+int keccak_setup(flock_ctx* c, size_t n_keccaks, int width, int hash, int profile, flock_setup** out) {
   if (!c || !out) return FLOCK_ERR_ARG;
-  // min_n_keccaks_log (keccak.rs:513-518): 2^max(3, ceil(log2 n)) slots
+  // min_n_keccaks_log (keccak.rs:513-518) / min_n_blocks_log (keccak3.rs:144-150):
+  // 2^max(3, ceil(log2 ceil(n / width))) blocks
+  const size_t blocks = (n_keccaks + width - 1) / width;
   uint32_t n_log = 3;
-  while (n_keccaks && ((size_t)1 << n_log) < n_keccaks) n_log++;
-  if (n_keccaks == 0 || n_log < 6 || n_log > 18 || (hash != FLOCK_HASH_BLAKE3 && hash != FLOCK_HASH_SHA256) ||
-      profile != FLOCK_PROFILE_FAST) {
-    c->err = "unsupported Keccak setup (33..=2^18 permutations: the fast profile's Ligerito ladders cover "
-             "m = 22..34; BLAKE3 or SHA-256 Merkle hash, fast profile)";
+  while (((size_t)1 << n_log) < blocks) n_log++;
+  const int k_log = flock::hash_k_log(keccak_hash_of(width));
+  if (n_keccaks == 0 || (int)n_log + k_log < 22 || (int)n_log + k_log > 34 ||
+      (hash != FLOCK_HASH_BLAKE3 && hash != FLOCK_HASH_SHA256) || profile != FLOCK_PROFILE_FAST) {
+    c->err = width == 3 ? "unsupported 3-wide Keccak setup (49..=3 * 2^17 permutations: the fast profile's Ligerito "
+                          "ladders cover m = 22..34; BLAKE3 or SHA-256 Merkle hash, fast profile)"
+                        : "unsupported Keccak setup (33..=2^18 permutations: the fast profile's Ligerito ladders cover "
+                          "m = 22..34; BLAKE3 or SHA-256 Merkle hash, fast profile)";
     return FLOCK_ERR_ARG;
   }
   return guard(c, [&] {
     auto* s = new flock_setup();
     s->ctx = c;
-    s->s.reset(new flock::Setup(c->device, n_log, 0, flock::kHashKeccak, hash));
+    s->s.reset(new flock::Setup(c->device, n_log, 0, keccak_hash_of(width), hash));
     s->n_blocks = n_keccaks;
     *out = s;
     return FLOCK_OK;
   });
 }
+int keccak_verify(flock_ctx* c, int width, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen) {
+  if (!c || !bytes || (!domain && dlen)) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    std::lock_guard<std::mutex> lk(c->vmu);
+    if (!c->verifier) c->verifier.reset(new flock::Verifier(c->device));
+    const std::string why = c->verifier->verify(bytes, len, std::string((const char*)domain, dlen),
+                                                keccak_hash_of(width), nullptr, c->fs_fn);
+    if (why.empty()) return (int)FLOCK_OK;
+    c->err = "verify: " + why;
+    return (int)FLOCK_ERR_VERIFY;
+  });
+}
+int keccak_digest(int width, uint32_t m, uint8_t* out32) {
+  if (!out32 || m < 19 || m > 40) return FLOCK_ERR_ARG;
+  try {
+    auto d = flock::statement_digest(keccak_hash_of(width), (int)m);
+    memcpy(out32, d.data(), 32);
+    return FLOCK_OK;
+  } catch (...) {
+    return FLOCK_ERR_INTERNAL;
+  }
+}
+int keccak_witness(flock_ctx* c, int width, const flock_keccak_state* states, size_t n, uint32_t n_log, uint64_t* z,
+                   uint64_t* a, uint64_t* b) {
+  if (!c || !z || !a || !b || n_log < 3 || n_log > 18 || n > ((size_t)width << n_log) || (n && !states))
+    return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    const size_t slots = (size_t)1 << n_log;
+    const size_t words = slots << (flock::hash_k_log(keccak_hash_of(width)) - 7);  // F128 per vector
+    DevBuf<f128> dz(words), da(words), db(words);
+    DevBuf<flock_keccak_state> ds(n ? n : 1);
+    if (n) CK(cudaMemcpyAsync(ds.p, states, n * sizeof(flock_keccak_state), cudaMemcpyHostToDevice, c->st));
+    launch_witness_keccak(reinterpret_cast<const uint64_t*>(ds.p), 0, (uint32_t)n, (uint32_t)slots, dz.p, da.p, db.p,
+                          c->st, width);
+    CK(cudaMemcpyAsync(z, dz.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(a, da.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(b, db.p, words * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+int keccak_comb_call(flock_ctx* c, int width, const uint64_t* e, const uint64_t* alpha, const uint64_t* beta,
+                     uint64_t* comb) {
+  if (!c || !e || !alpha || !beta || !comb) return FLOCK_ERR_ARG;
+  return guard(c, [&] {
+    const size_t kk = (size_t)1 << flock::hash_k_log(keccak_hash_of(width));
+    DevBuf<f128> de(kk), dc(kk), dw(keccak_comb_scratch(width));
+    CK(cudaMemcpyAsync(de.p, e, kk * 16, cudaMemcpyHostToDevice, c->st));
+    keccak_comb(de.p, mk(alpha[0], alpha[1]), mk(beta[0], beta[1]), keccak_masks(c->device), dw.p, dc.p, c->st,
+                width);
+    CK(cudaMemcpyAsync(comb, dc.p, kk * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return FLOCK_OK;
+  });
+}
+}  // namespace
+
+int flock_keccak_setup_create(flock_ctx* c, size_t n_keccaks, int hash, int profile, flock_setup** out) {
+  return keccak_setup(c, n_keccaks, 1, hash, profile, out);
+}
+int flock_keccak3_setup_create(flock_ctx* c, size_t n_keccaks, int hash, int profile, flock_setup** out) {
+  return keccak_setup(c, n_keccaks, 3, hash, profile, out);
+}
 
 int flock_keccak_prove(flock_setup* s, const flock_keccak_state* states, size_t n, const uint8_t* domain, size_t dlen,
                        uint8_t* out, size_t cap, size_t* out_len) {
   if (!s || !states || (!domain && dlen)) return FLOCK_ERR_ARG;
-  if (s->s->hash != flock::kHashKeccak) {
+  if (!flock::is_keccak(s->s->hash)) {
     s->ctx->err = "not a Keccak setup";
     return FLOCK_ERR_ARG;
   }
@@ -474,16 +545,10 @@ int flock_keccak_prove(flock_setup* s, const flock_keccak_state* states, size_t 
 }
 
 int flock_keccak_verify_bundle(flock_ctx* c, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen) {
-  if (!c || !bytes || (!domain && dlen)) return FLOCK_ERR_ARG;
-  return guard(c, [&] {
-    std::lock_guard<std::mutex> lk(c->vmu);
-    if (!c->verifier) c->verifier.reset(new flock::Verifier(c->device));
-    const std::string why =
-        c->verifier->verify(bytes, len, std::string((const char*)domain, dlen), flock::kHashKeccak, nullptr, c->fs_fn);
-    if (why.empty()) return (int)FLOCK_OK;
-    c->err = "verify: " + why;
-    return (int)FLOCK_ERR_VERIFY;
-  });
+  return keccak_verify(c, 1, bytes, len, domain, dlen);
+}
+int flock_keccak3_verify_bundle(flock_ctx* c, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen) {
+  return keccak_verify(c, 3, bytes, len, domain, dlen);
 }
 
 void flock_keccak_f(uint64_t* lanes25) {
@@ -514,47 +579,23 @@ int flock_keccak_bench_inputs(size_t n, uint64_t seed, flock_keccak_state* out) 
   return FLOCK_OK;
 }
 
-int flock_keccak_statement_digest(uint32_t m, uint8_t* out32) {
-  if (!out32 || m < 19 || m > 40) return FLOCK_ERR_ARG;
-  try {
-    auto d = flock::statement_digest(flock::kHashKeccak, (int)m);
-    memcpy(out32, d.data(), 32);
-    return FLOCK_OK;
-  } catch (...) {
-    return FLOCK_ERR_INTERNAL;
-  }
-}
+int flock_keccak_statement_digest(uint32_t m, uint8_t* out32) { return keccak_digest(1, m, out32); }
+int flock_keccak3_statement_digest(uint32_t m, uint8_t* out32) { return keccak_digest(3, m, out32); }
 
 int flock_keccak_witness(flock_ctx* c, const flock_keccak_state* states, size_t n, uint32_t n_log, uint64_t* z,
                          uint64_t* a, uint64_t* b) {
-  if (!c || !z || !a || !b || n_log < 3 || n_log > 18 || n > ((size_t)1 << n_log) || (n && !states))
-    return FLOCK_ERR_ARG;
-  return guard(c, [&] {
-    const size_t slots = (size_t)1 << n_log, words = slots * 512;
-    DevBuf<f128> dz(words), da(words), db(words);
-    DevBuf<flock_keccak_state> ds(n ? n : 1);
-    if (n) CK(cudaMemcpyAsync(ds.p, states, n * sizeof(flock_keccak_state), cudaMemcpyHostToDevice, c->st));
-    launch_witness_keccak(reinterpret_cast<const uint64_t*>(ds.p), 0, (uint32_t)n, (uint32_t)slots, dz.p, da.p, db.p,
-                          c->st);
-    CK(cudaMemcpyAsync(z, dz.p, words * 16, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(a, da.p, words * 16, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(b, db.p, words * 16, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return FLOCK_OK;
-  });
+  return keccak_witness(c, 1, states, n, n_log, z, a, b);
+}
+int flock_keccak3_witness(flock_ctx* c, const flock_keccak_state* states, size_t n, uint32_t n_log, uint64_t* z,
+                          uint64_t* a, uint64_t* b) {
+  return keccak_witness(c, 3, states, n, n_log, z, a, b);
 }
 
 int flock_keccak_comb(flock_ctx* c, const uint64_t* e, const uint64_t* alpha, const uint64_t* beta, uint64_t* comb) {
-  if (!c || !e || !alpha || !beta || !comb) return FLOCK_ERR_ARG;
-  return guard(c, [&] {
-    const size_t kk = (size_t)1 << flock::kKeccakKLog;
-    DevBuf<f128> de(kk), dc(kk), dw(keccak_comb_scratch());
-    CK(cudaMemcpyAsync(de.p, e, kk * 16, cudaMemcpyHostToDevice, c->st));
-    keccak_comb(de.p, mk(alpha[0], alpha[1]), mk(beta[0], beta[1]), keccak_masks(c->device), dw.p, dc.p, c->st);
-    CK(cudaMemcpyAsync(comb, dc.p, kk * 16, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return FLOCK_OK;
-  });
+  return keccak_comb_call(c, 1, e, alpha, beta, comb);
+}
+int flock_keccak3_comb(flock_ctx* c, const uint64_t* e, const uint64_t* alpha, const uint64_t* beta, uint64_t* comb) {
+  return keccak_comb_call(c, 3, e, alpha, beta, comb);
 }
 
 int flock_pcs_commit(flock_ctx* c, const uint64_t* z_packed, uint32_t m, uint8_t* root32, flock_prover_data** out) {

@@ -651,15 +651,16 @@ Statement build_sha256() {
   return st;
 }
 
-// KeccakSetup's BlockR1cs (keccak.rs:558-560, common.rs:120-138): A_0 and
+// KeccakSetup's BlockR1cs (keccak.rs:558-560, keccak3.rs:151-153,
+// common.rs:120-138): A_0 and
 // B_0 without entries, so the digest binds the sizes and C = I only; the
 // lincheck applies the real matrices through keccak_comb
-Statement build_keccak() {
-  const int K = 1 << kKeccakKLog;
+Statement build_keccak(bool wide) {
+  const int k_log = wide ? kKeccak3KLog : kKeccakKLog, K = 1 << k_log;
   Statement st;
-  st.k_log = kKeccakKLog;
-  st.z_const = kKeccakZConst;
-  st.useful = kKeccakUseful;
+  st.k_log = k_log;
+  st.z_const = wide ? kKeccak3ZConst : kKeccakZConst;
+  st.useful = wide ? kKeccak3Useful : kKeccakUseful;
   st.implicit = true;
   st.a_ptr.assign(K + 1, 0);
   st.b_ptr.assign(K + 1, 0);
@@ -727,11 +728,11 @@ void keccak_f(uint64_t s[25]) {
 }
 
 const Statement& statement(int hash) {
-  static std::once_flag once[3];
-  static std::unique_ptr<Statement> s[3];
-  const int k = hash == kHashSha256 ? 1 : hash == kHashKeccak ? 2 : 0;
+  static std::once_flag once[4];
+  static std::unique_ptr<Statement> s[4];
+  const int k = known_hash(hash) ? hash : 0;
   std::call_once(once[k], [k] {
-    s[k].reset(new Statement(k == 1 ? build_sha256() : k == 2 ? build_keccak() : build()));
+    s[k].reset(new Statement(k == kHashSha256 ? build_sha256() : is_keccak(k) ? build_keccak(k == kHashKeccak3) : build()));
   });
   return *s[k];
 }

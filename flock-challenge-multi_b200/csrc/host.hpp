@@ -128,12 +128,14 @@ std::vector<f128> medium_consts();
 // blocks, constant wire at bit 31400.  Keccak-f[1600] (r1cs_hashes/keccak.rs):
 // 2^16-bit blocks, constant wire at bit 4096, implicit matrices (the block
 // statement is the empty stub of common.rs:120-138; the lincheck applies
-// them through keccak_comb).
-enum HashKind : int { kHashBlake3 = 0, kHashSha256 = 1, kHashKeccak = 2 };
+// them through keccak_comb).  3-wide Keccak (r1cs_hashes/keccak3.rs): three
+// permutations per 2^17-bit block, constant wire at bit 12288.
+enum HashKind : int { kHashBlake3 = 0, kHashSha256 = 1, kHashKeccak = 2, kHashKeccak3 = 3 };
 constexpr int kKLog = 14, kK = 1 << kKLog, kKSkip = 6, kZConst = 512, kUseful = 15409;
 constexpr int kShaKLog = 15, kShaZConst = 31400, kShaUseful = 31401;
 constexpr int kKeccakKLog = 16, kKeccakZConst = 4096, kKeccakUseful = 42560;
-constexpr int kMaxKLog = kKeccakKLog;  // the largest block of the statements
+constexpr int kKeccak3KLog = 17, kKeccak3ZConst = 12288, kKeccak3Useful = 127552;
+constexpr int kMaxKLog = kKeccak3KLog;  // the largest block of the statements
 struct Statement {
   int k_log = kKLog, z_const = kZConst, useful = kUseful;
   bool implicit = false;                 // matrices applied by a walker, not stored
@@ -153,9 +155,12 @@ void sha256_compress(const uint32_t h_in[8], const uint32_t m[16], uint32_t out[
 void keccak_f(uint64_t lanes[25]);
 // block size of a hash's statement (log2 bits)
 inline int hash_k_log(int hash) {
-  return hash == kHashSha256 ? kShaKLog : hash == kHashKeccak ? kKeccakKLog : kKLog;
+  return hash == kHashSha256 ? kShaKLog : hash == kHashKeccak ? kKeccakKLog : hash == kHashKeccak3 ? kKeccak3KLog : kKLog;
 }
-inline bool known_hash(int hash) { return hash == kHashBlake3 || hash == kHashSha256 || hash == kHashKeccak; }
+inline bool known_hash(int hash) { return hash >= kHashBlake3 && hash <= kHashKeccak3; }
+inline bool is_keccak(int hash) { return hash == kHashKeccak || hash == kHashKeccak3; }
+// permutations per block of a Keccak statement
+inline int keccak_width(int hash) { return hash == kHashKeccak3 ? 3 : 1; }
 
 // ---- Ligerito fast ladder (configs/ligerito/m*_fast.toml) ----
 struct Ladder {

@@ -35,6 +35,13 @@
 // theta^T(u)(x, y, z) = u(x, y, z) + sum_y' u(x + 1, y', z) + sum_y' u(x - 1, y', z + 1).
 // Vectors over a state are indexed lane-major, p = 64 (x + 5y) + z, which is
 // also the offset of bit (x, y, z) inside a state's or t_r's region.
+//
+// The 3-wide encoder (keccak3.rs, K_LOG = 17) packs three independent
+// permutations per block: sub-keccak i has state_0 in slot 2i (words 64 i..),
+// state_24 in slot 2i + 1, the constant is shared at word 192 (bit 12288) and
+// t[i, r] is tight from word 193 in the order i * 24 + r.  Its walker is three
+// copies of the recurrence (one CTA each) into one comb, the constant column
+// collected atomically.  A Shape names the layout.
 #include "kernels.cuh"
 
 #include <map>
@@ -43,12 +50,21 @@
 namespace {
 constexpr uint64_t kGamma = 0x9E3779B97F4A7C15ull;
 constexpr int kWarps = 8;           // permutations per CTA of the witness kernel
-constexpr int kBlockWords = 1024;   // u64 words of a 2^16-bit block
-constexpr int kTWord = 65;          // first word of t_0
 constexpr int kState = 1600;
-constexpr int kTBase = 4160;        // first bit of t_0
-constexpr int kZConstBit = 4096;
-constexpr int kWRows = 26;          // W_0..W_23, alpha pin, alpha e over state_0
+constexpr int kWRows = 26;          // per permutation: W_0..W_23, alpha pin, alpha e over state_0
+
+// block layout: `width` permutations per block of `words` u64 words
+struct Shape {
+  int width, words;
+  int const_word;  // the constant wire (bit 0 of this word)
+  int t_word;      // first word of t[0, 0]
+  __host__ __device__ int s0_word(int i) const { return 64 * i; }
+  __host__ __device__ int s24_word(int i) const { return 64 * i + 32; }
+  __host__ __device__ int t_first(int i) const { return t_word + 25 * 24 * i; }  // t[i, 0]
+};
+Shape shape_of(int width) {
+  return width == 3 ? Shape{3, 2048, 192, 193} : Shape{1, 1024, 64, 65};
+}
 
 // rotation offsets r[x][y] of rho (FIPS 202 3.2.2), index 5 x + y
 __constant__ uint8_t kRho[25] = {0,  36, 3,  41, 18, 1,  44, 10, 45, 2,  62, 6, 43,
@@ -83,22 +99,26 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {  // SplitMix64's output 
 // states: n_perm x 25 u64 lanes, or nullptr for the benchmark generator
 // (benches/keccak3_proof.rs:66-93: 25 SplitMix64 draws per state, state bit
 // i = x + 5y + 25z is bit i mod 64 of draw i / 64; draw k of the stream uses
-// state seed + (k + 1) gamma).  Slots n_perm.. hold the zero state.
+// state seed + (k + 1) gamma).  Permutation i of block o is input o * width +
+// i; inputs n_perm.. (and padding blocks) are the zero state.
 __global__ void __launch_bounds__(32 * kWarps) k_witness_keccak(const uint64_t* __restrict__ states, uint64_t seed,
-                                                                uint32_t n_perm, uint32_t n_slots,
+                                                                uint32_t n_perm, uint32_t n_slots, Shape S,
                                                                 uint64_t* __restrict__ z, uint64_t* __restrict__ a,
                                                                 uint64_t* __restrict__ b) {
   const int lane = threadIdx.x & 31;
-  const uint32_t o = blockIdx.x * kWarps + (threadIdx.x >> 5);
+  const uint32_t wid = blockIdx.x * kWarps + (threadIdx.x >> 5);
+  const uint32_t o = wid / S.width;  // block
+  const int sub = (int)(wid % S.width);
   if (o >= n_slots) return;  // warp-uniform
+  const uint32_t perm = o * S.width + sub;
   const bool on = lane < 25;
   const int x = lane % 5, y = lane / 5;
   uint64_t s = 0;
-  if (o < n_perm) {
+  if (perm < n_perm) {
     if (states) {
-      s = on ? states[(size_t)o * 25 + lane] : 0;
+      s = on ? states[(size_t)perm * 25 + lane] : 0;
     } else {
-      const uint64_t d = mix64(seed + (uint64_t)(25ull * o + lane + 1) * kGamma);
+      const uint64_t d = mix64(seed + (uint64_t)(25ull * perm + lane + 1) * kGamma);
 #pragma unroll 8
       for (int zz = 0; zz < 64; zz++) {
         const int i = lane + 25 * zz;
@@ -113,12 +133,14 @@ __global__ void __launch_bounds__(32 * kWarps) k_witness_keccak(const uint64_t* 
   const int src = pa + 5 * pb, rot = on ? kRho[5 * pa + pb] : 0;
   const int n1 = (x + 1) % 5 + 5 * y, n2 = (x + 2) % 5 + 5 * y;
   const int cm = (x + 4) % 5, cp = (x + 1) % 5;
-  uint64_t* zb = z + (size_t)o * kBlockWords;
-  uint64_t* ab = a + (size_t)o * kBlockWords;
-  uint64_t* bb = b + (size_t)o * kBlockWords;
-  zb[lane] = s;  // lanes 25..31 write the zero words 25..31
-  ab[lane] = s;
-  bb[lane] = on ? ~0ull : 0ull;
+  uint64_t* zb = z + (size_t)o * S.words;
+  uint64_t* ab = a + (size_t)o * S.words;
+  uint64_t* bb = b + (size_t)o * S.words;
+  const int w0 = S.s0_word(sub);
+  zb[w0 + lane] = s;  // lanes 25..31 write the slot's zero words 25..31
+  ab[w0 + lane] = s;
+  bb[w0 + lane] = on ? ~0ull : 0ull;
+  const int tw = S.t_first(sub);
   for (int r = 0; r < 24; r++) {
     uint64_t c = 0;
 #pragma unroll
@@ -128,7 +150,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_witness_keccak(const uint64_t* 
     const uint64_t b1 = __shfl_sync(0xffffffffu, bv, n1 & 31), b2 = __shfl_sync(0xffffffffu, bv, n2 & 31);
     const uint64_t t = ~b1 & b2;
     if (on) {
-      const int w = kTWord + 25 * r + lane;
+      const int w = tw + 25 * r + lane;
       zb[w] = t;
       ab[w] = ~b1;
       bb[w] = b2;
@@ -136,52 +158,58 @@ __global__ void __launch_bounds__(32 * kWarps) k_witness_keccak(const uint64_t* 
     s = bv ^ t;
     if (lane == 0) s ^= kRc[r];
   }
-  zb[32 + lane] = on ? s : 0;
-  ab[32 + lane] = on ? s : 0;
-  bb[32 + lane] = on ? ~0ull : 0ull;
-  if (lane == 0) zb[64] = ab[64] = bb[64] = 1;
-  for (int w = kTWord + 25 * 24 + lane; w < kBlockWords; w += 32) zb[w] = ab[w] = bb[w] = 0;
+  const int w24 = S.s24_word(sub);
+  zb[w24 + lane] = on ? s : 0;
+  ab[w24 + lane] = on ? s : 0;
+  bb[w24 + lane] = on ? ~0ull : 0ull;
+  if (sub == 0 && lane == 0) zb[S.const_word] = ab[S.const_word] = bb[S.const_word] = 1;
+  if (sub == S.width - 1)  // the block's zero tail after the last t row
+    for (int w = S.t_first(S.width) + lane; w < S.words; w += 32) zb[w] = ab[w] = bb[w] = 0;
 }
 
-// W rows (see the file comment) and the zero columns of comb.
-// W[r][p], r < 24: alpha E_r(x - 1, y, z) + E_r(x - 2, y, z); W[24] = alpha pin;
-// W[25] = alpha e over state_0.
-__global__ void __launch_bounds__(256) k_keccak_w(const f128* __restrict__ e, f128 alpha, f128* __restrict__ W,
-                                                  f128* __restrict__ comb) {
+// W rows (see the file comment) and the zero columns of comb (the constant
+// column too: the walkers XOR their parts into it).
+// W[i][r][p], r < 24: alpha E_r(x - 1, y, z) + E_r(x - 2, y, z); W[i][24] =
+// alpha pin; W[i][25] = alpha e over state_0 (permutation i of the block).
+__global__ void __launch_bounds__(256) k_keccak_w(const f128* __restrict__ e, f128 alpha, Shape S,
+                                                  f128* __restrict__ W, f128* __restrict__ comb) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < kWRows * kState) {
-    const int r = i / kState, p = i % kState;
+  if (i < S.width * kWRows * kState) {
+    const int sub = i / (kWRows * kState), r = i / kState % kWRows, p = i % kState;
     f128 v;
     if (r < 24) {
       const int l = p >> 6, zz = p & 63, x = l % 5, y5 = l - x;
-      const f128* E = e + kTBase + kState * r;
+      const f128* E = e + 64 * S.t_first(sub) + kState * r;
       v = fx(fmul(alpha, ldg(E + 64 * ((x + 4) % 5 + y5) + zz)), ldg(E + 64 * ((x + 3) % 5 + y5) + zz));
     } else {
-      v = fmul(alpha, ldg(e + (r == 24 ? 2048 : 0) + p));
+      v = fmul(alpha, ldg(e + 64 * (r == 24 ? S.s24_word(sub) : S.s0_word(sub)) + p));
     }
     st(W + i, v);
   }
-  // comb is written by the walker on state_0, t_0..t_23 and the constant;
-  // every other column is zero
-  for (int c = i; c < (1 << 16); c += gridDim.x * blockDim.x) {
-    const bool walked = c < kState || c == kZConstBit || (c >= kTBase && c < kTBase + 24 * kState);
+  // comb is written by the walkers on state_0 and t of every permutation
+  const int t0 = 64 * S.t_word, t1 = 64 * S.t_first(S.width);
+  for (int c = i; c < 64 * S.words; c += gridDim.x * blockDim.x) {
+    const bool walked = (c < 64 * S.const_word && (c & 4095) < kState) || (c >= t0 && c < t1);
     if (!walked) st(comb + c, mk(0, 0));
   }
 }
 
 // One CTA: the transposed recurrence over 24 rounds (3 barriers a round).
 // masks: 25 x 25 u64, masks[r] = phi(c_r) (r < 24), masks[24] = c_24.
+// CTA i walks permutation i of the block.
 constexpr int kWalkThreads = 800;  // two state positions per thread
-__global__ void __launch_bounds__(kWalkThreads) k_keccak_walk(const f128* __restrict__ e, const f128* __restrict__ W,
+__global__ void __launch_bounds__(kWalkThreads) k_keccak_walk(const f128* __restrict__ e, const f128* __restrict__ Wg,
                                                               const uint64_t* __restrict__ masks, f128 alpha,
-                                                              f128 beta, f128* __restrict__ comb) {
+                                                              f128 beta, Shape S, f128* __restrict__ comb) {
   extern __shared__ __align__(16) uint8_t wsm[];
   f128* K = reinterpret_cast<f128*>(wsm);  // [1600] the running K
   f128* U = K + kState;                    // [1600] K pulled back through rho-pi
   f128* D = U + kState;                    // [5][64] column sums of U
   __shared__ uint16_t dst[kState];         // rho-pi destination of each source position
   __shared__ f128 red[3][32];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, sub = blockIdx.x;
+  const f128* W = Wg + (size_t)sub * kWRows * kState;
+  const int tb = 64 * S.t_first(sub), b0 = 64 * S.s0_word(sub), b24 = 64 * S.s24_word(sub);
   for (int q = tid; q < kState; q += kWalkThreads) {
     const int l = q >> 6, zz = q & 63, pa = l % 5, pb = l / 5;  // source (pa, pb, zz)
     const int dx = pb, dy = (2 * pa + 3 * pb) % 5, dz = (zz + kRho[5 * pa + pb]) & 63;
@@ -191,15 +219,15 @@ __global__ void __launch_bounds__(kWalkThreads) k_keccak_walk(const f128* __rest
   for (int p = tid; p < kState; p += kWalkThreads) {
     const f128 k = ldg(W + 24 * kState + p);
     K[p] = k;
-    st(comb + kTBase + 23 * kState + p, k);
+    st(comb + tb + 23 * kState + p, k);
     if ((masks[24 * 25 + (p >> 6)] >> (p & 63)) & 1) acc = fx(acc, k);
-    acc_row = fx(acc_row, fx(ldg(e + p), ldg(e + 2048 + p)));  // state_0 and state_24 rows' B = [const]
+    acc_row = fx(acc_row, fx(ldg(e + b0 + p), ldg(e + b24 + p)));  // state_0 and state_24 rows' B = [const]
   }
   for (int r = 23; r >= 0; r--) {
     for (int p = tid; p < kState; p += kWalkThreads) {
       const f128 w = ldg(W + r * kState + p);
       if ((masks[r * 25 + (p >> 6)] >> (p & 63)) & 1) acc = fx(acc, w);
-      acc_t = fx(acc_t, ldg(e + kTBase + r * kState + p));
+      acc_t = fx(acc_t, ldg(e + tb + r * kState + p));
       K[p] = fx(K[p], w);
     }
     __syncthreads();
@@ -217,8 +245,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_keccak_walk(const f128* __rest
       const int l = k >> 6, zz = k & 63, x = l % 5;
       const f128 v = fx(U[k], fx(D[64 * ((x + 1) % 5) + zz], D[64 * ((x + 4) % 5) + ((zz + 1) & 63)]));
       K[k] = v;
-      if (r > 0) st(comb + kTBase + (r - 1) * kState + k, v);
-      else st(comb + k, fx(v, ldg(W + 25 * kState + k)));
+      if (r > 0) st(comb + tb + (r - 1) * kState + k, v);
+      else st(comb + b0 + k, fx(v, ldg(W + 25 * kState + k)));
     }
     // the next round's update touches only this thread's own K entries; the
     // barrier after it orders them before the gather
@@ -239,11 +267,15 @@ __global__ void __launch_bounds__(kWalkThreads) k_keccak_walk(const f128* __rest
       s1 = fx(s1, red[1][w]);
       s2 = fx(s2, red[2][w]);
     }
-    // constant row (1, 1, 1): (alpha + 1) e[const]; chi rows' A = 1 + B[x+1]:
-    // alpha sum E; plus the rows' B = [const] and the round constants
-    const f128 ec = ldg(e + kZConstBit);
-    f128 v = fx(fx(s0, s1), fx(fmul(alpha, s2), fx(fmul(alpha, ec), ec)));
-    st(comb + kZConstBit, fx(v, beta));
+    // chi rows' A = 1 + B[x+1]: alpha sum E; the rows' B = [const] and the
+    // round constants; once per block: the constant row (1, 1, 1),
+    // (alpha + 1) e[const], and the pin beta
+    f128 v = fx(fx(s0, s1), fmul(alpha, s2));
+    if (sub == 0) {
+      const f128 ec = ldg(e + 64 * S.const_word);
+      v = fx(v, fx(fx(fmul(alpha, ec), ec), beta));
+    }
+    atomic_xor128(comb + 64 * S.const_word, v);
   }
 }
 constexpr size_t kWalkSmem = (2 * kState + 320) * sizeof(f128);
@@ -271,10 +303,12 @@ std::vector<uint64_t> round_constant_masks() {
 }  // namespace
 
 void launch_witness_keccak(const uint64_t* states, uint64_t seed, uint32_t n_perm, uint32_t n_slots, f128* z, f128* a,
-                           f128* b, cudaStream_t s) {
+                           f128* b, cudaStream_t s, int width) {
+  const Shape S = shape_of(width);
+  const uint64_t warps = (uint64_t)n_slots * S.width;
   count_launch();
-  k_witness_keccak<<<(n_slots + kWarps - 1) / kWarps, 32 * kWarps, 0, s>>>(
-      states, seed, n_perm, n_slots, reinterpret_cast<uint64_t*>(z), reinterpret_cast<uint64_t*>(a),
+  k_witness_keccak<<<(unsigned)((warps + kWarps - 1) / kWarps), 32 * kWarps, 0, s>>>(
+      states, seed, n_perm, n_slots, S, reinterpret_cast<uint64_t*>(z), reinterpret_cast<uint64_t*>(a),
       reinterpret_cast<uint64_t*>(b));
 }
 
@@ -293,11 +327,13 @@ const uint64_t* keccak_masks(int device) {
   return p;
 }
 
-size_t keccak_comb_scratch() { return (size_t)kWRows * kState; }
+size_t keccak_comb_scratch(int width) { return (size_t)shape_of(width).width * kWRows * kState; }
 
-void keccak_comb(const f128* e, f128 alpha, f128 beta, const uint64_t* masks, f128* W, f128* comb, cudaStream_t s) {
+void keccak_comb(const f128* e, f128 alpha, f128 beta, const uint64_t* masks, f128* W, f128* comb, cudaStream_t s,
+                 int width) {
+  const Shape S = shape_of(width);
   count_launch(2);
-  k_keccak_w<<<(kWRows * kState + 255) / 256, 256, 0, s>>>(e, alpha, W, comb);
+  k_keccak_w<<<(S.width * kWRows * kState + 255) / 256, 256, 0, s>>>(e, alpha, S, W, comb);
   CK(cudaFuncSetAttribute(k_keccak_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkSmem));
-  k_keccak_walk<<<1, kWalkThreads, kWalkSmem, s>>>(e, W, masks, alpha, beta, comb);
+  k_keccak_walk<<<S.width, kWalkThreads, kWalkSmem, s>>>(e, W, masks, alpha, beta, S, comb);
 }

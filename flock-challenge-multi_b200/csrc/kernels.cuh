@@ -91,16 +91,19 @@ void launch_witness_blocks(const uint32_t* blocks, uint32_t n_blocks, uint32_t n
 // records == nullptr for the benchmark generator from `seed`
 void launch_witness_sha(const uint32_t* records, uint64_t seed, uint32_t n_blocks, uint32_t n_slots, f128* z, f128* a,
                         f128* b, cudaStream_t s);
-// Keccak-f[1600] permutations, 2^16-bit blocks: states of 25 u64 lanes, or
-// states == nullptr for the benchmark generator from `seed`
+// Keccak-f[1600] permutations: states of 25 u64 lanes, or states == nullptr
+// for the benchmark generator from `seed`; width 1: one permutation per
+// 2^16-bit block (keccak.rs), 3: three per 2^17-bit block (keccak3.rs)
 void launch_witness_keccak(const uint64_t* states, uint64_t seed, uint32_t n_perm, uint32_t n_slots, f128* z, f128* a,
-                           f128* b, cudaStream_t s);
-// K6 of the Keccak statement: comb = alpha A^T e + B^T e + beta [const] over
-// the 2^16 rows of a block (e and comb: 2^16 values); W: keccak_comb_scratch()
-// values; masks: keccak_masks(device), the round constants' share
+                           f128* b, cudaStream_t s, int width = 1);
+// K6 of the Keccak statements: comb = alpha A^T e + B^T e + beta [const] over
+// the rows of a block (e and comb: 2^16 or 2^17 values); W:
+// keccak_comb_scratch(width) values; masks: keccak_masks(device), the round
+// constants' share
 const uint64_t* keccak_masks(int device);
-size_t keccak_comb_scratch();
-void keccak_comb(const f128* e, f128 alpha, f128 beta, const uint64_t* masks, f128* W, f128* comb, cudaStream_t s);
+size_t keccak_comb_scratch(int width = 1);
+void keccak_comb(const f128* e, f128 alpha, f128 beta, const uint64_t* masks, f128* W, f128* comb, cudaStream_t s,
+                 int width = 1);
 // Degree-4 zerocheck round 1 (zerocheck/univariate_skip_deg4.rs): device
 // sums H[8 l + k] (eq over the rows whose a b c d at lambda 64 + l has bit k)
 // and Zs[s] (eq over the rows whose z bit s is set), XOR-ed into H (1536

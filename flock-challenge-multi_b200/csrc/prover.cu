@@ -116,8 +116,8 @@ Setup::Setup(int device, uint32_t log2_, int stream_priority, int hash_, int mer
   zv = dalloc<f128>(kk, st);
   zv_pre = dalloc<f128>(kk, st);
   eq_inner = dalloc<f128>(kk, st);
-  if (hash == kHashKeccak) {
-    kc_w = dalloc<f128>(keccak_comb_scratch(), st);
+  if (is_keccak(hash)) {
+    kc_w = dalloc<f128>(keccak_comb_scratch(keccak_width(hash)), st);
     kc_masks = keccak_masks(device);
   }
   bc_tabs = dalloc<f128>(2 * 16 * 256, st);
@@ -483,11 +483,11 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   if (merkle && (hash != kHashSha256 || n_blocks != n_slots || !merkle->b_bits || merkle->path_log < 0 ||
                  merkle->path_log > n_log))
     throw std::runtime_error("a Merkle path is a SHA-256 statement whose paths fill every slot");
-  if (!committed && hash == kHashKeccak) {
+  if (!committed && is_keccak(hash)) {
     // ---- K0 witness of Keccak-f[1600] permutations (states of 25 u64)
     const uint32_t nb = n_blocks ? (uint32_t)n_blocks : 1u << log2;
     launch_witness_keccak(seed ? nullptr : reinterpret_cast<const uint64_t*>(blocks_dev), seed ? *seed : 0, nb,
-                          n_slots, z, a, b, st);
+                          n_slots, z, a, b, st, keccak_width(hash));
     CK(cudaGetLastError());
   } else if (!committed && hash == kHashSha256) {
     // ---- K0 witness of SHA-256 compressions
@@ -747,7 +747,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     std::vector<f128> L = hlagrange(zc_z, 0);
     eq_build(x_inner.data(), (int)x_inner.size(), hone(), zv_pre, st);
     outer64(L.data(), zv_pre, (size_t)1 << x_inner.size(), eq_inner, st);
-    if (hash == kHashKeccak) keccak_comb(eq_inner, alpha, beta, kc_masks, kc_w, comb, st);
+    if (is_keccak(hash)) keccak_comb(eq_inner, alpha, beta, kc_masks, kc_w, comb, st, keccak_width(hash));
     else lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, statement(hash).z_const, kk, comb, st);
     eq_table(x_outer, scratch_eq());
     CK(cudaMemsetAsync(zv, 0, kk * sizeof(f128), st));

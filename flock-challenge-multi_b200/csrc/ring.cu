@@ -19,10 +19,10 @@
 
 // one CTA per output r, one thread per t; the 128 products are XOR-reduced
 // across the CTA (warp shuffles, then the four warp sums)
-// a thread per 128-bit word of the block (128, 256 or 512 words), a CTA per bit r
-__global__ void __launch_bounds__(512) k_shat_from_zvec(const f128* __restrict__ zv, const f128* __restrict__ eqt,
-                                                        f128* __restrict__ out) {
-  __shared__ f128 red[16];
+// a thread per 128-bit word of the block (128 to 1024 words), a CTA per bit r
+__global__ void __launch_bounds__(1024) k_shat_from_zvec(const f128* __restrict__ zv, const f128* __restrict__ eqt,
+                                                         f128* __restrict__ out) {
+  __shared__ f128 red[32];
   const int r = blockIdx.x, t = threadIdx.x;
   f128 v = warp_xor(fmul(ldg(eqt + t), ldg(zv + 128 * t + r)));
   if ((t & 31) == 0) red[t >> 5] = v;

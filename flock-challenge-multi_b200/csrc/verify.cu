@@ -898,10 +898,10 @@ VerifyStatement device_statement(int m, int hash, const std::array<uint8_t, 32>&
     std::vector<f128> L = hlagrange(zskip, 0), cv(kk);
     eq_build(x_inner.data(), (int)x_inner.size(), hone(), B.eqx, st);
     outer64(L.data(), B.eqx, (size_t)1 << x_inner.size(), B.eqi, st);
-    if (hash == kHashKeccak) {
+    if (is_keccak(hash)) {
       int dev = 0;
       CK(cudaGetDevice(&dev));
-      keccak_comb(B.eqi, alpha, beta, keccak_masks(dev), B.kcw, B.comb, st);
+      keccak_comb(B.eqi, alpha, beta, keccak_masks(dev), B.kcw, B.comb, st, keccak_width(hash));
     } else {
       lc_comb(at_ptr, at_row, bt_ptr, bt_row, B.eqi, alpha, beta, pin, kk, B.comb, st);
     }
@@ -974,7 +974,7 @@ Verifier::Verifier(int device) : device_(device) {
   CK(cudaMalloc(&eqx_, ((size_t)1 << (kMaxKLog - kKSkip)) * sizeof(f128)));  // eq(x_inner), 2^(k_log - 6)
   CK(cudaMalloc(&eqi_, ((size_t)1 << kMaxKLog) * sizeof(f128)));  // the largest block of the statements
   CK(cudaMalloc(&comb_, ((size_t)1 << kMaxKLog) * sizeof(f128)));
-  CK(cudaMalloc(&kcw_, keccak_comb_scratch() * sizeof(f128)));
+  CK(cudaMalloc(&kcw_, keccak_comb_scratch(3) * sizeof(f128)));
   CK(cudaMalloc(&rows_, kRowsCap));
   CK(cudaMalloc(&cvs_, kCvsCap));
 }
@@ -1002,7 +1002,7 @@ std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string
   if (!known_hash(hash)) return "unknown statement hash";
   if (hash != kHashBlake3 && !merkle && bytes[6] != 2) return "hash chains are BLAKE3 statements";
   // BLAKE3: 2^8..2^20 compressions; SHA-256: 2^7..2^19; Keccak: 2^6..2^18
-  // permutations (the same m range)
+  // blocks of one permutation, 2^5..2^17 of three (the same m range)
   if (mm < 22 || mm > 34) return "bundle is for an unsupported statement size";
   // the stream and buffers belong to device_, whichever device the calling
   // thread has current; the caller's device is restored on return

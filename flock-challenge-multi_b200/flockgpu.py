@@ -41,7 +41,8 @@ EXPORTS = (
     "flock_ctx_set_transcript", "flock_challenger_create_hash", "flock_merkle_tree_hash",
     "flock_keccak_setup_create", "flock_keccak_prove", "flock_keccak_verify_bundle", "flock_keccak_f",
     "flock_keccak_bench_inputs", "flock_keccak_statement_digest", "flock_keccak_witness", "flock_keccak_comb",
-    "flock_zerocheck_round1_deg4", "flock_bench_round1_deg4",
+    "flock_zerocheck_round1_deg4", "flock_bench_round1_deg4", "flock_keccak3_setup_create",
+    "flock_keccak3_verify_bundle", "flock_keccak3_statement_digest", "flock_keccak3_witness", "flock_keccak3_comb",
 )
 # the hash behind Merkle trees / the transcript (HashKind discriminants)
 HASH = {"sha256": 0, "blake3": 1}
@@ -127,7 +128,12 @@ def load() -> ctypes.CDLL:
         lib.flock_serve_prewarm.argtypes = [vp, u32, i32, ctypes.POINTER(i32)]
         lib.flock_zerocheck_round1_deg4.argtypes = [vp, vp, vp, vp, vp, vp, u32, vp, vp, vp]
         lib.flock_bench_round1_deg4.argtypes = [vp, u32, u64, i32, ctypes.POINTER(ctypes.c_double), vp, vp]
-        lib.flock_keccak_setup_create.argtypes = [vp, sz, i32, i32, ctypes.POINTER(vp)]
+        for w in ("", "3"):
+            getattr(lib, f"flock_keccak{w}_setup_create").argtypes = [vp, sz, i32, i32, ctypes.POINTER(vp)]
+            getattr(lib, f"flock_keccak{w}_verify_bundle").argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
+            getattr(lib, f"flock_keccak{w}_statement_digest").argtypes = [u32, vp]
+            getattr(lib, f"flock_keccak{w}_witness").argtypes = [vp, vp, sz, u32, vp, vp, vp]
+            getattr(lib, f"flock_keccak{w}_comb").argtypes = [vp, vp, vp, vp, vp]
         lib.flock_keccak_prove.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_keccak_verify_bundle.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
         lib.flock_keccak_f.argtypes = [vp]
@@ -288,9 +294,17 @@ def keccak_bench_seed(n: int, run: int = 0) -> int:
     return 0xC0FFEE_BEEF ^ n ^ run
 
 
-def keccak_statement_digest(m: int) -> bytes:
+def _kw(width: int) -> str:
+    """entry-point suffix: "" for the single encoder (keccak.rs), "3" for the
+    3-wide one (keccak3.rs)"""
+    if width not in (1, 3):
+        raise ValueError("width is 1 (keccak.rs) or 3 (keccak3.rs)")
+    return "" if width == 1 else "3"
+
+
+def keccak_statement_digest(m: int, width: int = 1) -> bytes:
     out = np.zeros(32, np.uint8)
-    rc = load().flock_keccak_statement_digest(m, _ptr(out))
+    rc = getattr(load(), f"flock_keccak{_kw(width)}_statement_digest")(m, _ptr(out))
     if rc != 0:
         raise FlockError(f"keccak_statement_digest: {rc}")
     return out.tobytes()
@@ -419,10 +433,11 @@ class Context:
                                                   _ptr(b)), "sha256_witness")
         return z, a, b
 
-    def keccak_verify(self, bundle: bytes, domain: bytes = DOMAIN) -> str:
-        """KeccakSetup::verify for any supported size: '' when the bundle
-        verifies as a Keccak statement, otherwise the failed check."""
-        rc = self.lib.flock_keccak_verify_bundle(self.h, bundle, len(bundle), domain, len(domain))
+    def keccak_verify(self, bundle: bytes, domain: bytes = DOMAIN, width: int = 1) -> str:
+        """KeccakSetup::verify (keccak.rs, or keccak3.rs for width 3) for any
+        supported size: '' when the bundle verifies, otherwise the failed check."""
+        rc = getattr(self.lib, f"flock_keccak{_kw(width)}_verify_bundle")(self.h, bundle, len(bundle), domain,
+                                                                         len(domain))
         if rc == 0:
             return ""
         if rc == FLOCK_ERR_VERIFY:
@@ -430,22 +445,25 @@ class Context:
         self._check(rc, "keccak_verify_bundle")
         return "error"
 
-    def keccak_witness(self, states: np.ndarray, n_log: int):
+    def keccak_witness(self, states: np.ndarray, n_log: int, width: int = 1):
         """(z, a, b) packed row witness of (n, 25) u64 Keccak states over
-        2^n_log blocks, each (2^n_log, 1024) u64."""
+        2^n_log blocks, each (2^n_log, 1024 * (1 or 2)) u64."""
         states = np.ascontiguousarray(states, np.uint64).reshape(-1, 25)
-        z, a, b = (np.zeros((1 << n_log, 1024), np.uint64) for _ in range(3))
-        self._check(self.lib.flock_keccak_witness(self.h, _ptr(states), states.shape[0], n_log, _ptr(z), _ptr(a),
-                                                  _ptr(b)), "keccak_witness")
+        words = 1024 if width == 1 else 2048
+        z, a, b = (np.zeros((1 << n_log, words), np.uint64) for _ in range(3))
+        self._check(getattr(self.lib, f"flock_keccak{_kw(width)}_witness")(
+            self.h, _ptr(states), states.shape[0], n_log, _ptr(z), _ptr(a), _ptr(b)), "keccak_witness")
         return z, a, b
 
-    def keccak_comb(self, e: np.ndarray, alpha, beta) -> np.ndarray:
+    def keccak_comb(self, e: np.ndarray, alpha, beta, width: int = 1) -> np.ndarray:
         """The Keccak lincheck's alpha A^T e + B^T e + beta [const] on the GPU
-        (e: (2^16, 2) u64 lo/hi; alpha, beta: (lo, hi))."""
-        e = np.ascontiguousarray(e, np.uint64).reshape(1 << 16, 2)
+        (e: (2^k_log, 2) u64 lo/hi; alpha, beta: (lo, hi))."""
+        k = 1 << (16 if width == 1 else 17)
+        e = np.ascontiguousarray(e, np.uint64).reshape(k, 2)
         al, be = np.array(alpha, np.uint64), np.array(beta, np.uint64)
-        out = np.zeros((1 << 16, 2), np.uint64)
-        self._check(self.lib.flock_keccak_comb(self.h, _ptr(e), _ptr(al), _ptr(be), _ptr(out)), "keccak_comb")
+        out = np.zeros((k, 2), np.uint64)
+        self._check(getattr(self.lib, f"flock_keccak{_kw(width)}_comb")(self.h, _ptr(e), _ptr(al), _ptr(be),
+                                                                        _ptr(out)), "keccak_comb")
         return out
 
     def round1_deg4(self, a, b, c, d, z, m: int, r):
@@ -808,15 +826,18 @@ class KeccakProver:
     """`KeccakSetup::new(n)` (crates/flock-prover/src/r1cs_hashes/keccak.rs:
     870-912): Keccak-f[1600] permutations, one per 2^16-bit block,
     2^max(3, ceil(log2 n)) slots, fast profile; BLAKE3 Merkle hashing unless
-    merkle_hash says otherwise."""
+    merkle_hash says otherwise.  width = 3: the 3-wide `keccak3::KeccakSetup`
+    (keccak3.rs:491-540), three permutations per 2^17-bit block."""
 
-    def __init__(self, ctx: Context, n: int, merkle_hash: str = "blake3", transcript: str = "blake3"):
+    def __init__(self, ctx: Context, n: int, merkle_hash: str = "blake3", transcript: str = "blake3",
+                 width: int = 1):
         h = ctypes.c_void_p()
-        ctx._check(ctx.lib.flock_keccak_setup_create(ctx.h, n, HASH[merkle_hash], 0, ctypes.byref(h)),
+        ctx._check(getattr(ctx.lib, f"flock_keccak{_kw(width)}_setup_create")(ctx.h, n, HASH[merkle_hash], 0,
+                                                                               ctypes.byref(h)),
                    "keccak_setup_create")
-        self.ctx, self.n, self.h = ctx, n, h
+        self.ctx, self.n, self.h, self.width = ctx, n, h, width
         ctx._check(ctx.lib.flock_setup_set_transcript(h, HASH[transcript]), "setup_set_transcript")
-        self.n_log = max(3, (n - 1).bit_length())
+        self.n_log = max(3, (-(-n // width) - 1).bit_length())
         self._buf = np.zeros(MAX_PROOF_BYTES * 2, np.uint8)
 
     def close(self) -> None:

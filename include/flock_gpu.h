@@ -55,6 +55,8 @@
  *  - flock_keccak_*      <- KeccakSetup::{new, prove_fast, verify}, keccak_f
  *                           (crates/flock-prover/src/r1cs_hashes/keccak.rs:
  *                           423-428, 863-998)
+ *  - flock_keccak3_*     <- keccak3::KeccakSetup (crates/flock-prover/src/
+ *                           r1cs_hashes/keccak3.rs:491-580)
  *  - flock_zerocheck_round1_deg4
  *                        <- round1_deg4_naive (crates/flock-core/src/zerocheck/
  *                           univariate_skip_deg4.rs:77-165)
@@ -297,6 +299,26 @@ int flock_keccak_witness(flock_ctx* ctx, const flock_keccak_state* states, size_
  * [const] over the 2^16 rows of a block, on the GPU (e, comb: 2^16 F128 as
  * lo, hi u64 pairs; alpha, beta: one F128). */
 int flock_keccak_comb(flock_ctx* ctx, const uint64_t* e, const uint64_t* alpha, const uint64_t* beta, uint64_t* comb);
+/* The 3-wide encoder (crates/flock-prover/src/r1cs_hashes/keccak3.rs): three
+ * independent permutations per 2^17-bit block (sub-keccak i: state_0 in slot
+ * 2i, state_24 in slot 2i + 1, t[i, r] tight from bit 12352 in the order
+ * i * 24 + r; one shared constant wire at bit 12288).
+ * keccak3::KeccakSetup::new(n_keccaks) (keccak3.rs:498-540): 2^max(3, ceil(
+ * log2 ceil(n / 3))) blocks (min_n_blocks_log, :144-150); supported 49 <= n
+ * <= 3 * 2^17 (m = 17 + n_log in 22..34).  Proofs through flock_keccak_prove
+ * (n = the setup's n_keccaks; missing permutations of the last block and
+ * padding blocks are keccak_f of the zero state, keccak3.rs:254-286) and
+ * flock_prove_seed. */
+int flock_keccak3_setup_create(flock_ctx* ctx, size_t n_keccaks, int hash, int profile, flock_setup** out);
+/* keccak3::KeccakSetup::verify (keccak3.rs:560-580) without a prover setup. */
+int flock_keccak3_verify_bundle(flock_ctx* ctx, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen);
+/* BlockR1cs::statement_digest of the 3-wide statement of size m. */
+int flock_keccak3_statement_digest(uint32_t m, uint8_t* out32);
+/* Debug/test: the 3-wide packed witness (2^(n_log + 10) u64 pairs each) and
+ * the walker's column combination over 2^17 rows. */
+int flock_keccak3_witness(flock_ctx* ctx, const flock_keccak_state* states, size_t n, uint32_t n_log, uint64_t* z,
+                          uint64_t* a, uint64_t* b);
+int flock_keccak3_comb(flock_ctx* ctx, const uint64_t* e, const uint64_t* alpha, const uint64_t* beta, uint64_t* comb);
 
 /* ---- Degree-4 zerocheck round 1 (crates/flock-core/src/zerocheck/univariate_skip_deg4.rs) ----
  * round1_deg4_naive(a, b, c, d, z, m, r) (univariate_skip_deg4.rs:77-165)

@@ -344,39 +344,47 @@ void flockref_merkle_tree_hash(const uint8_t* data, size_t n_leaves, size_t leaf
 }
 void* flockref_ch_new_hash(const char* domain, int kind) { return new Challenger(domain, kind); }
 
-// ---- Keccak-f[1600].  A state is 25 u64 lanes (lane x + 5y, bit z).
+// ---- Keccak-f[1600].  A state is 25 u64 lanes (lane x + 5y, bit z).  width:
+// 1 = the single encoder (keccak.rs), 3 = the 3-wide one (keccak3.rs).
 static_assert(sizeof(keccak::State) == 200, "keccak state");
+static const keccak::Layout& layout_of(int width) {
+  return width == 3 ? keccak::wide_layout() : keccak::single_layout();
+}
 void flockref_keccak_f(uint64_t* lanes25) { keccak::permute(lanes25); }
 void flockref_keccak_bench_inputs(size_t n, uint64_t seed, uint64_t* out25) {
   auto v = keccak::bench_inputs(n, seed);
   memcpy(out25, v.data(), v.size() * sizeof(keccak::State));
 }
-void flockref_keccak_digest(uint32_t n_log, uint8_t* out32) { memcpy(out32, keccak_r1cs((int)n_log).digest.data(), 32); }
-// z, a, b: 2^(16 + n_log - 7) F128 each
-void flockref_keccak_witness(const uint64_t* states, size_t n, uint32_t n_log, uint64_t* z, uint64_t* a,
+void flockref_keccak_digest(int width, uint32_t n_log, uint8_t* out32) {
+  memcpy(out32, keccak_r1cs(layout_of(width), (int)n_log).digest.data(), 32);
+}
+// z, a, b: 2^(k_log + n_log - 7) F128 each
+void flockref_keccak_witness(int width, const uint64_t* states, size_t n, uint32_t n_log, uint64_t* z, uint64_t* a,
                              uint64_t* b) {
   std::vector<keccak::State> s(n);
   memcpy(s.data(), states, n * sizeof(keccak::State));
   std::vector<F128> vz, va, vb;
-  generate_keccak_witness(s, (int)n_log, vz, va, vb);
+  generate_keccak_witness(layout_of(width), s, (int)n_log, vz, va, vb);
   memcpy(z, vz.data(), vz.size() * 16);
   memcpy(a, va.data(), va.size() * 16);
   memcpy(b, vb.data(), vb.size() * 16);
 }
-// the walker's alpha A^T e + B^T e over 2^16 rows
-void flockref_keccak_comb(const uint64_t* alpha, const uint64_t* e, uint64_t* out) {
-  std::vector<F128> ev(keccak::K_KECCAK);
+// the walker's alpha A^T e + B^T e over the block's 2^k_log rows
+void flockref_keccak_comb(int width, const uint64_t* alpha, const uint64_t* e, uint64_t* out) {
+  const keccak::Layout& L = layout_of(width);
+  std::vector<F128> ev((size_t)1 << L.k_log);
   memcpy(ev.data(), e, ev.size() * 16);
-  auto c = keccak::lincheck_comb(F128(alpha[0], alpha[1]), ev);
+  auto c = keccak::lincheck_comb(L, F128(alpha[0], alpha[1]), ev);
   memcpy(out, c.data(), c.size() * 16);
 }
-int flockref_prove_keccak(const uint64_t* states, size_t n, const uint8_t* domain, size_t dlen, uint8_t* out,
-                          size_t cap, size_t* out_len) {
+int flockref_prove_keccak(int width, const uint64_t* states, size_t n, const uint8_t* domain, size_t dlen,
+                          uint8_t* out, size_t cap, size_t* out_len) {
   try {
     if (n == 0) return 3;
+    const keccak::Layout& L = layout_of(width);
     std::vector<keccak::State> s(n);
     memcpy(s.data(), states, n * sizeof(keccak::State));
-    Bundle b = prove_keccak(s, keccak::min_n_log(n), std::string((const char*)domain, dlen));
+    Bundle b = prove_keccak(L, s, keccak::min_n_blocks_log(L, n), std::string((const char*)domain, dlen));
     std::vector<uint8_t> bytes = serialize(b);
     *out_len = bytes.size();
     if (bytes.size() > cap) return 2;

@@ -174,10 +174,12 @@ struct Compression { uint32_t cv[8]; uint32_t m[16]; uint64_t counter; uint32_t 
 std::vector<Compression> generate_compressions(uint32_t log2, uint64_t seed);
 
 struct SparseRows { std::vector<uint32_t> ptr; std::vector<uint16_t> col; };  // CSR, K rows
+namespace keccak { struct Layout; }
 struct R1cs {
   int m = 0, n_log = 0;
   int k_log = K_LOG, z_const = Z_CONST_POS;  // block size and the pinned constant column
   bool walker = false;  // the lincheck marginal comes from the Keccak walker, not a0 / b0
+  const keccak::Layout* keccak = nullptr;  // the walker's block layout
   SparseRows a0, b0;
   std::array<uint8_t, 32> digest{};
 };
@@ -228,6 +230,14 @@ constexpr int K_KECCAK = 1 << K_LOG_KECCAK;
 constexpr int Z_CONST = 4096;
 constexpr int T_BASE = 4160;
 constexpr int USEFUL_BITS = T_BASE + 24 * 1600;  // 42,560
+// the 3-wide encoder (keccak3.rs:52-100)
+constexpr int K_LOG_KECCAK3 = 17;
+constexpr int Z_CONST3 = 12288;
+constexpr int T_BASE3 = 12352;
+// a block layout: n_sub permutations per 2^k_log-bit block
+struct Layout { int k_log, n_sub, z_const, t_base; };
+const Layout& single_layout();  // keccak.rs
+const Layout& wide_layout();    // keccak3.rs
 extern const uint64_t RC[24];
 struct State { uint64_t lanes[25]; };  // lane x + 5y, bit z
 // Keccak-f[1600] (FIPS 202) on lanes, in place
@@ -235,14 +245,16 @@ void permute(uint64_t lanes[25]);
 // benches/keccak3_proof.rs:80-93: 25 SplitMix64 draws per state, bit i (index
 // x + 5y + 25z) = bit i mod 64 of draw i / 64
 std::vector<State> bench_inputs(size_t n, uint64_t seed);
-int min_n_log(size_t n);  // keccak.rs:508-514
-void block_witness(const State& in, uint64_t* z, uint64_t* a, uint64_t* b);
-// fold_alpha_batched: alpha A^T e + B^T e for e over the block's 2^16 rows
-std::vector<F128> lincheck_comb(F128 alpha, const std::vector<F128>& e);
+// min_n_keccaks_log (keccak.rs:513-518) / min_n_blocks_log (keccak3.rs:144-150)
+int min_n_blocks_log(const Layout& L, size_t n);
+// one block's z, a, b (zeroed by the caller) from its L.n_sub input states
+void block_witness(const Layout& L, const State* in, uint64_t* z, uint64_t* a, uint64_t* b);
+// fold_alpha_batched: alpha A^T e + B^T e for e over the block's 2^k_log rows
+std::vector<F128> lincheck_comb(const Layout& L, F128 alpha, const std::vector<F128>& e);
 }  // namespace keccak
-const R1cs& keccak_r1cs(int n_log);
-void generate_keccak_witness(const std::vector<keccak::State>& states, int n_log, std::vector<F128>& z,
-                             std::vector<F128>& a, std::vector<F128>& b);
+const R1cs& keccak_r1cs(const keccak::Layout& L, int n_log);
+void generate_keccak_witness(const keccak::Layout& L, const std::vector<keccak::State>& states, int n_log,
+                             std::vector<F128>& z, std::vector<F128>& a, std::vector<F128>& b);
 // z by the boolean witness (padding blocks: the all-zero (h_in, m)
 // compression), a = A_0 z and b = B_0 z from the matrices
 void generate_sha256_witness(const std::vector<sha::Compression>& blocks, int n_log, std::vector<F128>& z,
@@ -353,7 +365,8 @@ Bundle prove_core(const R1cs& rc, std::vector<F128> z, const std::vector<F128>& 
 // Sha256HybridSetup::prove_fast (sha2.rs:1377-1408) over 2^n_log blocks
 Bundle prove_sha256(const std::vector<sha::Compression>& blocks, int n_log, const std::string& domain);
 // KeccakSetup::prove_fast (keccak.rs:956-978); padding: keccak_f(0)
-Bundle prove_keccak(const std::vector<keccak::State>& states, int n_log, const std::string& domain);
+Bundle prove_keccak(const keccak::Layout& L, const std::vector<keccak::State>& states, int n_log,
+                    const std::string& domain);
 // sum_j bc[j] * z[j] == target (the batched open's claim)
 bool open_identity(const std::vector<F128>& z, const std::vector<F128>& bc, F128 target);
 // that identity, as checked by the last prove_with with a hook on this thread

@@ -12,7 +12,13 @@
 //  * the lincheck walker KeccakLincheckCircuit::fold_alpha_batched (:681-828),
 //    the column marginal alpha A^T e + B^T e of the implicit matrices;
 //  * the empty-stub statement (common.rs:120-138: A_0 = B_0 empty, C_0 = I);
-//  * the keccak3_proof bench inputs (benches/keccak3_proof.rs:66-93, 114-124).
+//  * the keccak3_proof bench inputs (benches/keccak3_proof.rs:66-93, 114-124);
+//  * the 3-wide encoder of keccak3.rs at K_LOG = 17 (:1-140, 151-300, 430-490):
+//    three independent permutations per block, sub-keccak i with state_0 in
+//    slot 2i, state_24 in slot 2i + 1, one shared constant at bit 12288,
+//    t[i, r] tight from bit 12352 in the order i * 24 + r; its walker is three
+//    copies of the single recurrence into one comb (min_n_blocks_log :144-150:
+//    ceil(n / 3) blocks, at least 8).
 // Unlike the product, the oracle evaluates the permutation bit by bit on
 // 1600-bit states.
 #include "flockref.hpp"
@@ -103,31 +109,33 @@ std::vector<State> bench_inputs(size_t n, uint64_t seed) {
   return out;
 }
 
-int min_n_log(size_t n) {
-  size_t p = 8;
-  int l = 3;
-  while (p < n) { p <<= 1; l++; }
-  return l;
+const Layout& single_layout() {
+  static const Layout L{K_LOG_KECCAK, 1, Z_CONST, T_BASE};
+  return L;
+}
+const Layout& wide_layout() {
+  static const Layout L{K_LOG_KECCAK3, 3, Z_CONST3, T_BASE3};
+  return L;
 }
 
-void block_witness(const State& in, uint64_t* z, uint64_t* a, uint64_t* b) {
+// sub-keccak i of a block: state_0 at slot 2i, state_24 at slot 2i + 1,
+// t_r at t_base + 1600 (24 i + r)
+static void sub_witness(const Layout& L, int i, const State& in, uint64_t* z, uint64_t* a, uint64_t* b) {
+  const int s0 = 2 * i * 2048, s24 = (2 * i + 1) * 2048, tb = L.t_base + 1600 * 24 * i;
   Bits s(1600);
   for (int j = 0; j < 1600; j++) s[j] = (in.lanes[j % 25] >> (j / 25)) & 1;
   auto put = [](uint64_t* v, int pos, uint8_t bit) { if (bit) v[pos >> 6] |= 1ull << (pos & 63); };
-  put(z, Z_CONST, 1);
-  put(a, Z_CONST, 1);
-  put(b, Z_CONST, 1);
   for (int j = 0; j < 1600; j++) {
-    put(z, lane_pos(j), s[j]);
-    put(a, lane_pos(j), s[j]);
-    put(b, lane_pos(j), 1);
+    put(z, s0 + lane_pos(j), s[j]);
+    put(a, s0 + lane_pos(j), s[j]);
+    put(b, s0 + lane_pos(j), 1);
   }
   for (int r = 0; r < 24; r++) {
     const Bits bs = phi(s);
     for (int zz = 0; zz < 64; zz++)
       for (int y = 0; y < 5; y++)
         for (int x = 0; x < 5; x++) {
-          const int j = sidx(x, y, zz), pos = T_BASE + 1600 * r + lane_pos(j);
+          const int j = sidx(x, y, zz), pos = tb + 1600 * r + lane_pos(j);
           const uint8_t l = bs[sidx((x + 1) % 5, y, zz)] ^ 1, rr = bs[sidx((x + 2) % 5, y, zz)];
           put(z, pos, l & rr);
           put(a, pos, l);
@@ -137,27 +145,33 @@ void block_witness(const State& in, uint64_t* z, uint64_t* a, uint64_t* b) {
     for (int zz = 0; zz < 64; zz++) s[sidx(0, 0, zz)] ^= (RC[r] >> zz) & 1;
   }
   for (int j = 0; j < 1600; j++) {
-    put(z, 2048 + lane_pos(j), s[j]);
-    put(a, 2048 + lane_pos(j), s[j]);
-    put(b, 2048 + lane_pos(j), 1);
+    put(z, s24 + lane_pos(j), s[j]);
+    put(a, s24 + lane_pos(j), s[j]);
+    put(b, s24 + lane_pos(j), 1);
   }
 }
 
-std::vector<F128> lincheck_comb(F128 alpha, const std::vector<F128>& e) {
-  std::vector<F128> comb(K_KECCAK, ZERO);
-  auto t_pos = [](int r, int j) { return T_BASE + 1600 * r + lane_pos(j); };
-  // constant row: A = B = [const]
-  comb[Z_CONST] += alpha * e[Z_CONST] + e[Z_CONST];
+void block_witness(const Layout& L, const State* in, uint64_t* z, uint64_t* a, uint64_t* b) {
+  z[L.z_const >> 6] |= 1ull << (L.z_const & 63);
+  a[L.z_const >> 6] |= 1ull << (L.z_const & 63);
+  b[L.z_const >> 6] |= 1ull << (L.z_const & 63);
+  for (int i = 0; i < L.n_sub; i++) sub_witness(L, i, in[i], z, a, b);
+}
+
+// sub-keccak i's rows into comb (the shared constant row excluded)
+static void sub_comb(const Layout& L, int i, F128 alpha, const std::vector<F128>& e, std::vector<F128>& comb) {
+  const int s0 = 2 * i * 2048, s24 = (2 * i + 1) * 2048, tb = L.t_base + 1600 * 24 * i, zc = L.z_const;
+  auto t_pos = [tb](int r, int j) { return tb + 1600 * r + lane_pos(j); };
   // state_0 rows: A = [row], B = [const]
   for (int j = 0; j < 1600; j++) {
-    comb[lane_pos(j)] += alpha * e[lane_pos(j)];
-    comb[Z_CONST] += e[lane_pos(j)];
+    comb[s0 + lane_pos(j)] += alpha * e[s0 + lane_pos(j)];
+    comb[zc] += e[s0 + lane_pos(j)];
   }
   // state_24 pin rows: A = L_24[j] (through the recurrence below), B = [const]
   std::vector<F128> pin(1600);
   for (int j = 0; j < 1600; j++) {
-    pin[j] = e[2048 + lane_pos(j)];
-    comb[Z_CONST] += pin[j];
+    pin[j] = e[s24 + lane_pos(j)];
+    comb[zc] += pin[j];
   }
   // chi rows of round r: A = 1 + B[x+1], B = B[x+2]; their marginals on state_r
   std::vector<std::vector<F128>> ca(24, std::vector<F128>(1600, ZERO)), cb = ca;
@@ -171,7 +185,7 @@ std::vector<F128> lincheck_comb(F128 alpha, const std::vector<F128>& e) {
           for (int k : preimage((x + 1) % 5, y, zz)) ca[r][k] += ev;
           for (int k : preimage((x + 2) % 5, y, zz)) cb[r][k] += ev;
         }
-  comb[Z_CONST] += alpha * sum_t;
+  comb[zc] += alpha * sum_t;
   // the round constants' share: state_r = phi^r state_0 + ... + RC_r
   Bits rc(1600, 0);
   F128 rca = ZERO, rcb = ZERO;
@@ -184,7 +198,7 @@ std::vector<F128> lincheck_comb(F128 alpha, const std::vector<F128>& e) {
   F128 rcp = ZERO;
   for (int k = 0; k < 1600; k++)
     if (rc[k]) rcp += pin[k];
-  comb[Z_CONST] += alpha * rca + rcb + alpha * rcp;
+  comb[zc] += alpha * rca + rcb + alpha * rcp;
   // phi^T
   auto phi_t = [](const std::vector<F128>& v) {
     std::vector<F128> o(1600, ZERO);
@@ -204,7 +218,7 @@ std::vector<F128> lincheck_comb(F128 alpha, const std::vector<F128>& e) {
     for (int j = 0; j < 1600; j++) nk[j] += ca[r - 1][j];
     k = nk;
   }
-  for (int j = 0; j < 1600; j++) comb[lane_pos(j)] += alpha * k[j];
+  for (int j = 0; j < 1600; j++) comb[s0 + lane_pos(j)] += alpha * k[j];
   // B side: K_23 = chi_B(23)
   k = cb[23];
   for (int r = 23; r >= 1; r--) {
@@ -213,52 +227,74 @@ std::vector<F128> lincheck_comb(F128 alpha, const std::vector<F128>& e) {
     for (int j = 0; j < 1600; j++) nk[j] += cb[r - 1][j];
     k = nk;
   }
-  for (int j = 0; j < 1600; j++) comb[lane_pos(j)] += k[j];
+  for (int j = 0; j < 1600; j++) comb[s0 + lane_pos(j)] += k[j];
+}
+
+std::vector<F128> lincheck_comb(const Layout& L, F128 alpha, const std::vector<F128>& e) {
+  std::vector<F128> comb((size_t)1 << L.k_log, ZERO);
+  // the shared constant row: A = B = [const]
+  comb[L.z_const] += alpha * e[L.z_const] + e[L.z_const];
+  for (int i = 0; i < L.n_sub; i++) sub_comb(L, i, alpha, e, comb);
   return comb;
+}
+
+int min_n_blocks_log(const Layout& L, size_t n) {
+  size_t blocks = (n + L.n_sub - 1) / L.n_sub, p = 8;
+  int l = 3;
+  while (p < blocks) { p <<= 1; l++; }
+  return l;
 }
 
 }  // namespace keccak
 
-const R1cs& keccak_r1cs(int n_log) {
+const R1cs& keccak_r1cs(const keccak::Layout& L, int n_log) {
   static std::mutex mu;
-  static std::map<int, std::unique_ptr<R1cs>> cache;
+  static std::map<std::pair<int, int>, std::unique_ptr<R1cs>> cache;
   std::lock_guard<std::mutex> lk(mu);
-  auto it = cache.find(n_log);
+  auto it = cache.find({L.n_sub, n_log});
   if (it != cache.end()) return *it->second;
   std::unique_ptr<R1cs> r(new R1cs());
   r->n_log = n_log;
-  r->k_log = keccak::K_LOG_KECCAK;
-  r->z_const = keccak::Z_CONST;
+  r->k_log = L.k_log;
+  r->z_const = L.z_const;
   r->m = r->k_log + n_log;
-  r->a0.ptr.assign(keccak::K_KECCAK + 1, 0);
-  r->b0.ptr.assign(keccak::K_KECCAK + 1, 0);
+  r->a0.ptr.assign(((size_t)1 << L.k_log) + 1, 0);
+  r->b0.ptr.assign(((size_t)1 << L.k_log) + 1, 0);
   r->walker = true;
+  r->keccak = &L;
   r->digest = statement_digest(r->m, r->k_log, K_SKIP, r->a0, r->b0);
   const R1cs& ref = *r;
-  cache[n_log] = std::move(r);
+  cache[{L.n_sub, n_log}] = std::move(r);
   return ref;
 }
 
-void generate_keccak_witness(const std::vector<keccak::State>& states, int n_log, std::vector<F128>& z,
-                             std::vector<F128>& a, std::vector<F128>& b) {
-  const size_t n_total = (size_t)1 << n_log, per = keccak::K_KECCAK / 128;
+void generate_keccak_witness(const keccak::Layout& L, const std::vector<keccak::State>& states, int n_log,
+                             std::vector<F128>& z, std::vector<F128>& a, std::vector<F128>& b) {
+  const size_t n_total = (size_t)1 << n_log, per = ((size_t)1 << L.k_log) / 128;
   z.assign(n_total * per, ZERO);
   a.assign(n_total * per, ZERO);
   b.assign(n_total * per, ZERO);
-  const keccak::State pad{};
   par_for(n_total, [&](size_t o0, size_t o1, int) {
-    for (size_t o = o0; o < o1; o++)
-      keccak::block_witness(o < states.size() ? states[o] : pad, (uint64_t*)&z[o * per], (uint64_t*)&a[o * per],
-                            (uint64_t*)&b[o * per]);
+    for (size_t o = o0; o < o1; o++) {
+      // the block's permutations; states past the input (and padding blocks)
+      // are the zero state
+      keccak::State in[3] = {};
+      for (int i = 0; i < L.n_sub; i++) {
+        const size_t idx = o * L.n_sub + i;
+        if (idx < states.size()) in[i] = states[idx];
+      }
+      keccak::block_witness(L, in, (uint64_t*)&z[o * per], (uint64_t*)&a[o * per], (uint64_t*)&b[o * per]);
+    }
   });
 }
 
-Bundle prove_keccak(const std::vector<keccak::State>& states, int n_log, const std::string& domain) {
+Bundle prove_keccak(const keccak::Layout& L, const std::vector<keccak::State>& states, int n_log,
+                    const std::string& domain) {
   std::vector<F128> z, a, b;
-  generate_keccak_witness(states, n_log, z, a, b);
+  generate_keccak_witness(L, states, n_log, z, a, b);
   // a hook that adds no claim, so that prove_core records the open identity
   const CoreHook none = [](Challenger&, const std::vector<F128>&) { return std::vector<DirectClaim>(); };
-  return prove_core(keccak_r1cs(n_log), std::move(z), a, b, domain, none);
+  return prove_core(keccak_r1cs(L, n_log), std::move(z), a, b, domain, none);
 }
 
 }  // namespace flockref

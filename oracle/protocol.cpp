@@ -306,7 +306,7 @@ static LincheckProof lincheck_prove(const std::vector<F128>& zp, int m, const R1
     for (int is = 0; is < 64; is++) eq_inner[is + 64 * ir] = lam[is] * eqr[ir];
   std::vector<F128> comb(K, ZERO);
   if (rc.walker) {
-    comb = keccak::lincheck_comb(alpha, eq_inner);
+    comb = keccak::lincheck_comb(*rc.keccak, alpha, eq_inner);
   } else {
     for (int row = 0; row < K; row++) {
       F128 ea = alpha * eq_inner[row], e = eq_inner[row];

@@ -221,13 +221,21 @@ static void absorb_matrix(b3::Hasher& h, const SparseRows& m) {
   }
 }
 
+// C = I of k rows, absorbed as absorb_matrix would (one entry per row); the
+// column index of row r is r, which for 2^17-row blocks does not fit a u16
+static void absorb_identity(b3::Hasher& h, int k) {
+  absorb_u64(h, (uint64_t)k);
+  absorb_u64(h, (uint64_t)k);
+  for (int r = 0; r < k; r++) {
+    uint8_t buf[16];
+    for (int i = 0; i < 8; i++) buf[i] = (uint8_t)(i == 0);
+    for (int i = 0; i < 8; i++) buf[8 + i] = (uint8_t)((uint64_t)r >> (8 * i));
+    h.update(buf, 16);
+  }
+}
+
 std::array<uint8_t, 32> statement_digest(int m, int k_log, int k_skip, const SparseRows& a0, const SparseRows& b0) {
   const int k = 1 << k_log;
-  SparseRows I;
-  I.ptr.resize(k + 1);
-  I.col.resize(k);
-  for (int i = 0; i < k; i++) { I.ptr[i] = i; I.col[i] = (uint16_t)i; }
-  I.ptr[k] = k;
   b3::Hasher h;
   const char* tag = "flock-r1cs-stmt-v1";
   h.update(tag, strlen(tag));
@@ -238,7 +246,7 @@ std::array<uint8_t, 32> statement_digest(int m, int k_log, int k_skip, const Spa
   h.update(&layout, 1);
   absorb_matrix(h, a0);
   absorb_matrix(h, b0);
-  absorb_matrix(h, I);
+  absorb_identity(h, k);
   std::array<uint8_t, 32> d;
   h.finalize(d.data());
   return d;

@@ -70,7 +70,9 @@
    Keccak statements, so these pin the GPU to the oracle, whose own checks are
    recorded per entry: every block's witness has a & b = z and state_24 =
    keccak_f(state_0) (the permutation itself pinned to hashlib's SHA-3 by the
-   tests), and the batched open's claim identity holds.
+   tests), and the batched open's claim identity holds.  keccak3_proofs.json
+   holds the same for the 3-wide encoder (keccak3.rs, three permutations per
+   2^17-bit block) at n = 49, 100 (partial last block), 6144 and 12288.
 
 Usage (a built oracle; REFERENCE is a checkout of the reference project):
     python tests/golden/make_golden.py --ref REFERENCE [--large]
@@ -241,32 +243,42 @@ def sha256_proofs(threads=8) -> None:
 
 
 KECCAK_SIZES = (64, 100, 1024, 4096, 16384)
+KECCAK3_SIZES = (49, 100, 6144, 12288)
 
 
 def keccak_proofs(threads=8) -> None:
+    keccak_width_proofs(1, KECCAK_SIZES, "keccak_proofs.json", threads)
+    keccak_width_proofs(3, KECCAK3_SIZES, "keccak3_proofs.json", threads)
+
+
+def keccak_width_proofs(width, sizes, name, threads) -> None:
     import os
     os.environ["FLOCKREF_THREADS"] = str(threads)
     sys.path.insert(0, str(REPO / "tests"))
     import numpy as np
     import oracle_lib
     orc = oracle_lib.Oracle()
-    out = {"digests": {str(m): orc.keccak_digest(m - 16).hex() for m in range(22, 35)}, "proofs": []}
-    for n in KECCAK_SIZES:
+    k_log = 16 if width == 1 else 17
+    out = {"digests": {str(m): orc.keccak_digest(m - k_log, width).hex() for m in range(22, 35)}, "proofs": []}
+    for n in sizes:
         seed = 0xC0FFEE_BEEF ^ n
         states = orc.keccak_bench_inputs(n, seed)
-        n_log = max(3, (n - 1).bit_length())
-        z, a, b = orc.keccak_witness(states, n_log)
+        n_log = max(3, (-(-n // width) - 1).bit_length())
+        z, a, b = orc.keccak_witness(states, n_log, width)
         assert np.array_equal(a & b, z), n
         for i in range(1 << n_log):
-            s0 = states[i] if i < n else np.zeros(25, np.uint64)
-            assert np.array_equal(z[i, :25], s0) and np.array_equal(z[i, 32:57], orc.keccak_f(s0)), (n, i)
-        data = orc.prove_keccak(states)
+            for s in range(width):
+                k = width * i + s
+                s0 = states[k] if k < n else np.zeros(25, np.uint64)
+                assert np.array_equal(z[i, 64 * s:64 * s + 25], s0), (n, i, s)
+                assert np.array_equal(z[i, 64 * s + 32:64 * s + 57], orc.keccak_f(s0)), (n, i, s)
+        data = orc.prove_keccak(states, width=width)
         assert orc.last_open_identity_ok(), n
-        out["proofs"].append({"n": n, "seed": seed, "domain": "flock-bench-v0", "m": 16 + n_log,
+        out["proofs"].append({"n": n, "seed": seed, "domain": "flock-bench-v0", "m": k_log + n_log,
                               "sha256": hashlib.sha256(data).hexdigest(), "size": len(data),
-                              "checked_by": "oracle: a & b = z and state_24 = keccak_f(state_0) in every block; "
-                                            "open claim identity"})
-        (HERE / "keccak_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
+                              "checked_by": "oracle: a & b = z and state_24 = keccak_f(state_0) for every "
+                                            "permutation of every block; open claim identity"})
+        (HERE / name).write_text(json.dumps(out, indent=1))  # after every size
 
 
 SHA256_MERKLE = ((12, 0), (14, 0), (15, 0), (7, 2), (8, 3))

@@ -81,10 +81,10 @@ class Oracle:
         L.flockref_prove_records.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_keccak_f.argtypes = [vp]
         L.flockref_keccak_bench_inputs.argtypes = [sz, u64, vp]
-        L.flockref_keccak_digest.argtypes = [u32, vp]
-        L.flockref_keccak_witness.argtypes = [vp, sz, u32, vp, vp, vp]
-        L.flockref_keccak_comb.argtypes = [vp, vp, vp]
-        L.flockref_prove_keccak.argtypes = [vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        L.flockref_keccak_digest.argtypes = [i32, u32, vp]
+        L.flockref_keccak_witness.argtypes = [i32, vp, sz, u32, vp, vp, vp]
+        L.flockref_keccak_comb.argtypes = [i32, vp, vp, vp]
+        L.flockref_prove_keccak.argtypes = [i32, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_last_open_identity_ok.argtypes = []
         L.flockref_round1_deg4.argtypes = [vp, vp, vp, vp, vp, u32, vp, vp, vp]
         L.flockref_time_prove.argtypes = [u32, u64, ctypes.POINTER(sz)]
@@ -118,31 +118,35 @@ class Oracle:
         self.L.flockref_keccak_bench_inputs(n, seed, _p(out))
         return out
 
-    def keccak_digest(self, n_log: int) -> bytes:
+    # width: 1 = the single encoder (keccak.rs, 2^16-bit blocks), 3 = the
+    # 3-wide one (keccak3.rs, 2^17-bit blocks of three permutations)
+    def keccak_digest(self, n_log: int, width: int = 1) -> bytes:
         out = np.zeros(32, np.uint8)
-        self.L.flockref_keccak_digest(n_log, _p(out))
+        self.L.flockref_keccak_digest(width, n_log, _p(out))
         return out.tobytes()
 
-    def keccak_witness(self, states: np.ndarray, n_log: int):
+    def keccak_witness(self, states: np.ndarray, n_log: int, width: int = 1):
         states = np.ascontiguousarray(states, np.uint64).reshape(-1, 25)
-        z, a, b = (np.zeros((1 << n_log, 1024), np.uint64) for _ in range(3))
-        self.L.flockref_keccak_witness(_p(states), states.shape[0], n_log, _p(z), _p(a), _p(b))
+        words = 1024 if width == 1 else 2048
+        z, a, b = (np.zeros((1 << n_log, words), np.uint64) for _ in range(3))
+        self.L.flockref_keccak_witness(width, _p(states), states.shape[0], n_log, _p(z), _p(a), _p(b))
         return z, a, b
 
-    def keccak_comb(self, alpha, e: np.ndarray) -> np.ndarray:
-        """alpha A^T e + B^T e over a block's 2^16 rows (e: 2^16 x (lo, hi))."""
+    def keccak_comb(self, alpha, e: np.ndarray, width: int = 1) -> np.ndarray:
+        """alpha A^T e + B^T e over a block's rows (e: 2^k_log x (lo, hi))."""
+        k = 1 << (16 if width == 1 else 17)
         al = np.array(alpha, np.uint64)
-        e = np.ascontiguousarray(e, np.uint64).reshape(1 << 16, 2)
-        out = np.zeros((1 << 16, 2), np.uint64)
-        self.L.flockref_keccak_comb(_p(al), _p(e), _p(out))
+        e = np.ascontiguousarray(e, np.uint64).reshape(k, 2)
+        out = np.zeros((k, 2), np.uint64)
+        self.L.flockref_keccak_comb(width, _p(al), _p(e), _p(out))
         return out
 
-    def prove_keccak(self, states: np.ndarray, domain: bytes = b"flock-bench-v0") -> bytes:
+    def prove_keccak(self, states: np.ndarray, domain: bytes = b"flock-bench-v0", width: int = 1) -> bytes:
         states = np.ascontiguousarray(states, np.uint64).reshape(-1, 25)
         buf = np.zeros(2_000_000, np.uint8)
         n = ctypes.c_size_t()
-        rc = self.L.flockref_prove_keccak(_p(states), states.shape[0], domain, len(domain), _p(buf), buf.size,
-                                         ctypes.byref(n))
+        rc = self.L.flockref_prove_keccak(width, _p(states), states.shape[0], domain, len(domain), _p(buf),
+                                         buf.size, ctypes.byref(n))
         assert rc == 0, rc
         return buf[: n.value].tobytes()
 

@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "keccak_proofs.json"
+GOLDEN3 = Path(__file__).resolve().parent / "golden" / "keccak3_proofs.json"
 
 
 def _absorb(block: bytes) -> np.ndarray:
@@ -141,4 +142,69 @@ def test_oracle_proof_matches_fixture(oracle):
     g = json.loads(GOLDEN.read_text())
     e = next(p for p in g["proofs"] if p["n"] == 64)
     proof = oracle.prove_keccak(oracle.keccak_bench_inputs(e["n"], e["seed"]))
+    assert hashlib.sha256(proof).hexdigest() == e["sha256"] and len(proof) == e["size"]
+
+
+# ---- the 3-wide encoder (keccak3.rs): three permutations per 2^17-bit block
+
+def test_wide_witness_rows(oracle):
+    """keccak3.rs:151-300: sub-keccak s of block i holds input 3 i + s
+    (missing ones and padding blocks: the zero state) with state_0 in words
+    64 s..64 s + 24 and state_24 in 64 s + 32..; the shared constant is word
+    192; t fills words 193..1992 and the tail is zero; a & b = z."""
+    n_log, n = 3, 8  # the last block holds two inputs and one zero state
+    st = oracle.keccak_bench_inputs(n, 33)
+    z, a, b = oracle.keccak_witness(st, n_log, width=3)
+    assert z.shape == (8, 2048) and np.array_equal(a & b, z)
+    ones = np.full(25, 2**64 - 1, np.uint64)
+    for i in range(1 << n_log):
+        for s in range(3):
+            k = 3 * i + s
+            s0 = st[k] if k < n else np.zeros(25, np.uint64)
+            assert np.array_equal(z[i, 64 * s:64 * s + 25], s0) and np.array_equal(b[i, 64 * s:64 * s + 25], ones)
+            assert np.array_equal(z[i, 64 * s + 32:64 * s + 57], oracle.keccak_f(s0))
+            assert not z[i, 64 * s + 25:64 * s + 32].any() and not z[i, 64 * s + 57:64 * s + 64].any()
+        assert z[i, 192] == a[i, 192] == b[i, 192] == 1
+        assert not (z[i, 1993:].any() or a[i, 1993:].any() or b[i, 1993:].any())
+
+
+def _parity_checks_wide(oracle, z, a, b, seed):
+    rng = np.random.default_rng(seed)
+    e = rng.integers(0, 2**63, (1 << 17, 2), np.uint64) ^ (rng.integers(0, 2, (1 << 17, 2), np.uint64)
+                                                          << np.uint64(63))
+    bt = oracle.keccak_comb((0, 0), e, width=3)
+    at = oracle.keccak_comb((1, 0), e, width=3) ^ bt
+    zb, ab, bb = _bits(z).astype(bool), _bits(a).astype(bool), _bits(b).astype(bool)
+    ok_a = np.array_equal(np.bitwise_xor.reduce(e[ab], axis=0), np.bitwise_xor.reduce(at[zb], axis=0))
+    ok_b = np.array_equal(np.bitwise_xor.reduce(e[bb], axis=0), np.bitwise_xor.reduce(bt[zb], axis=0))
+    return ok_a and ok_b
+
+
+def test_wide_walker_matches_witness(oracle):
+    """keccak3.rs:430-490: three copies of the recurrence into one comb apply
+    the matrices the 3-wide witness satisfies; a flipped t bit of the third
+    sub-keccak breaks them."""
+    z, a, b = oracle.keccak_witness(oracle.keccak_bench_inputs(5, 9), 3, width=3)
+    for i in (0, 1, 2):
+        assert _parity_checks_wide(oracle, z[i], a[i], b[i], 200 + i), i
+    bit = 12352 + 1600 * (2 * 24 + 7) + 333
+    zz = z[0].copy()
+    zz[bit // 64] ^= np.uint64(1) << np.uint64(bit % 64)
+    assert not _parity_checks_wide(oracle, zz, a[0], b[0], 5)
+
+
+def test_wide_statement_digest_matches_oracle(oracle):
+    import flockgpu
+    for m in (22, 25, 34):
+        assert flockgpu.keccak_statement_digest(m, width=3) == oracle.keccak_digest(m - 17, width=3)
+    assert flockgpu.keccak_statement_digest(25, width=3) != flockgpu.keccak_statement_digest(25)
+
+
+def test_wide_fixtures(oracle):
+    import flockgpu
+    g = json.loads(GOLDEN3.read_text())
+    for m, d in g["digests"].items():
+        assert flockgpu.keccak_statement_digest(int(m), width=3) == bytes.fromhex(d), m
+    e = next(p for p in g["proofs"] if p["n"] == 49)
+    proof = oracle.prove_keccak(oracle.keccak_bench_inputs(e["n"], e["seed"]), width=3)
     assert hashlib.sha256(proof).hexdigest() == e["sha256"] and len(proof) == e["size"]
