@@ -783,6 +783,52 @@ int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const u
   });
 }
 
+int flock_sha256_prove_chain(flock_setup* s, const flock_sha256_compression* comps, size_t n, const uint8_t* domain,
+                             size_t dlen, uint8_t* out, size_t cap, size_t* out_len) {
+  if (!s || !comps || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (s->s->hash != flock::kHashSha256) {
+    s->ctx->err = "not a SHA-256 setup";
+    return FLOCK_ERR_ARG;
+  }
+  if (n != s->n_blocks || n != ((size_t)1 << s->s->n_log)) {
+    s->ctx->err = "a chain fills every slot: expected the setup's n_compressions, a power of two";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(s->ctx, [&] {
+    flock::ChainEnds ends;
+    memcpy(ends.cv0, comps[0].h, sizeof(ends.cv0));
+    flock::sha256_compress(comps[n - 1].h, comps[n - 1].m, ends.cv_last);
+    if (!s->s->records_buf)
+      CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->records_buf), n * sizeof(flock_sha256_compression),
+                         s->s->st));
+    CK(cudaMemcpyAsync(s->s->records_buf, comps, n * sizeof(flock_sha256_compression), cudaMemcpyHostToDevice,
+                       s->s->st));
+    std::string d((const char*)domain, dlen);
+    return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d, false, &ends), out, cap, out_len);
+  });
+}
+
+int flock_sha256_chain_blocks(uint64_t seed, const uint32_t* initial_h, size_t steps, flock_sha256_compression* out) {
+  if (!out && steps) return FLOCK_ERR_ARG;
+  static const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                                 0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+  uint32_t h[8];
+  memcpy(h, initial_h ? initial_h : iv, sizeof(h));
+  uint64_t x = seed;
+  for (size_t i = 0; i < steps; i++) {
+    memcpy(out[i].h, h, 32);
+    for (int w = 0; w < 16; w++) {
+      x += 0x9E3779B97F4A7C15ull;
+      uint64_t z = x;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      out[i].m[w] = (uint32_t)(z ^ (z >> 31));
+    }
+    flock::sha256_compress(out[i].h, out[i].m, h);
+  }
+  return FLOCK_OK;
+}
+
 int flock_verify(flock_setup* s, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen) {
   if (!s || !bytes || (!domain && dlen)) return FLOCK_ERR_ARG;
   return guard(s->ctx, [&] {

@@ -866,7 +866,7 @@ std::vector<uint8_t> encode(const Proof& p) {
     e.o.push_back(4);
     e.o.push_back(p.chain ? 3 : 2);
   }
-  if (p.chain) e.u32(0);  // HashKind::Blake3
+  if (p.chain) e.u32(p.chain_kind);  // HashKind: Blake3 = 0, Sha2 = 1
   e.h(p.root);
   e.u64(p.m);
   e.u64(1);  // log_inv_rate

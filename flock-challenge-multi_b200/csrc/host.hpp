@@ -192,6 +192,7 @@ struct Proof {
   std::vector<f128> ood;
   // hash-chain bundle (flavor 3): the shift argument and public endpoints
   bool chain = false;
+  uint32_t chain_kind = 0;  // the bundle's HashKind (proof_io.rs:51-58): 0 Blake3, 1 Sha2
   std::vector<std::pair<f128, f128>> shift_rounds;
   f128 g_at_point{};
   uint32_t cv0[8] = {}, cv_last[8] = {};

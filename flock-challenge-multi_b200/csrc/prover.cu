@@ -478,8 +478,9 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   const int G = gs * 4;
   const uint32_t n_slots = 1u << n_log;
   mark(0);
-  if (hash != kHashBlake3 && (committed || chain))
-    throw std::runtime_error("batched commits and hash chains are BLAKE3 statements");
+  if (hash != kHashBlake3 && committed) throw std::runtime_error("batched commits are BLAKE3 statements");
+  if (chain && hash != kHashBlake3 && hash != kHashSha256)
+    throw std::runtime_error("hash chains are BLAKE3 or SHA-256 statements");
   if (merkle && (hash != kHashSha256 || n_blocks != n_slots || !merkle->b_bits || merkle->path_log < 0 ||
                  merkle->path_log > n_log))
     throw std::runtime_error("a Merkle path is a SHA-256 statement whose paths fill every slot");
@@ -790,13 +791,14 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   f128 pd_value = mk(0, 0);
   if (chain) {
     P.chain = true;
+    P.chain_kind = hash == kHashSha256 ? 1 : 0;
     memcpy(P.cv0, chain->cv0, sizeof(P.cv0));
     memcpy(P.cv_last, chain->cv_last, sizeof(P.cv_last));
     const size_t N = n_slots;
     const f128 tau_pos = tr.sample_vec(1)[0];
     f128* g = pp[2];
     f128* w = pp[3];
-    chain_fold(z, N, fx(hone(), tau_pos), tau_pos, g, st);
+    chain_fold(z, N, (size_t)1 << (k_log - 7), fx(hone(), tau_pos), tau_pos, g, st);
     const std::vector<f128> tau = tr.sample_vec((size_t)n_log);
     const f128 alpha = tr.sample();
     // W(y, 0) = eq(tau, y - 1) for y >= 1, W(0, 0) = alpha; W(y, 1) = eq(tau, y)
@@ -825,11 +827,13 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       }
     }
     P.g_at_point = pd_value;
-    // round k bound variable n_log - k; variable n_log is s0
-    pd_point.assign(7 + (size_t)n_log, mk(0, 0));
+    // round k bound variable n_log - k; variable n_log is s0; the point is
+    // [tau_pos, s0, 0^(k_log - 9), instance] (k_log - 7 slot coordinates)
+    const size_t off = (size_t)k_log - 7;
+    pd_point.assign(off + (size_t)n_log, mk(0, 0));
     pd_point[0] = tau_pos;
     pd_point[1] = rs[0];
-    for (int k = 1; k <= n_log; k++) pd_point[7 + (size_t)(n_log - k)] = rs[k];
+    for (int k = 1; k <= n_log; k++) pd_point[off + (size_t)(n_log - k)] = rs[k];
   }
 
   // ---- Merkle paths (merkle_path_common.rs:314-430): tau_pos folds each
@@ -986,8 +990,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     const f128 ep[2] = {fx(hone(), tp), tp}, es[2] = {fx(hone(), s0), s0};
     f128 c[4];
     for (int wd = 0; wd < 4; wd++) c[wd] = hmul(gpd, hmul(ep[wd & 1], es[wd >> 1]));
-    eq_table(std::vector<f128>(pd_point.begin() + 7, pd_point.end()), scratch_eq());
-    chain_scatter(pp[1], scratch_eq(), n_slots, c, st);
+    eq_table(std::vector<f128>(pd_point.begin() + (k_log - 7), pd_point.end()), scratch_eq());
+    chain_scatter(pp[1], scratch_eq(), n_slots, (size_t)1 << (k_log - 7), c, st);
   }
   if (merkle) {
     // words w = 0..7 of block i get gpd eq(tau_pos, w & 1) eq(sel, w >> 1 & 1)

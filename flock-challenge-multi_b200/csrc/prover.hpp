@@ -56,6 +56,7 @@ struct ChainEnds {
 // column) for eq = L(z_skip) (x) eq(x_inner) (lincheck.rs:5940-5960).
 struct VerifyStatement {
   int m = 0, k_log = kKLog;
+  int hash = kHashBlake3;                // the statement (a chain bundle names it)
   int fs_fn = kFnBlake3;                 // the transcript's hash
   const MerklePublic* merkle = nullptr;  // a Merkle-path proof's public inputs
   std::array<uint8_t, 32> digest{};

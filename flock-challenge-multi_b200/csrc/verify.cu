@@ -119,7 +119,10 @@ bool decode(const uint8_t* bytes, size_t n, Proof& P, std::string& why, bool mer
   }
   P.merkle = merkle;
   P.chain = !merkle && bytes[6] == 3;
-  if (P.chain && r.u32() != 0) return why = "hash kind is not BLAKE3", false;
+  if (P.chain) {
+    P.chain_kind = r.u32();
+    if (P.chain_kind > 1) return why = "chain hash kind is neither BLAKE3 nor SHA-256", false;
+  }
   P.root = r.h();
   P.m = r.u64();
   if (r.u64() != 1 || r.u64() != 6 || r.u32() != 0) return why = "PCS parameters are not (rate 1/2, batch 2^6, Fast)", false;
@@ -573,6 +576,7 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
   // ---- hash chain: tau_pos, the shift argument from the public endpoints
   std::vector<f128> pd_point;
   if (P.chain) {
+    if (P.chain_kind != (V.hash == kHashSha256 ? 1u : 0u)) return "chain: hash kind of another statement";
     const f128 tp = tr.sample_vec(1)[0];
     const size_t n = (size_t)n_log;
     if (P.shift_rounds.size() != n + 1) return "chain: malformed shift proof";
@@ -597,10 +601,12 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
     const f128 wf = fx(fx(hmul(shift_mle(tau, taup), ops0), hmul(eq_eval(tau.data(), taup.data(), n), s0)),
                        hmul(hmul(al, eq_eval(taup.data(), zero.data(), n)), ops0));
     if (!feq(claim, hmul(wf, P.g_at_point))) return "chain: shift argument";
-    pd_point.assign(7 + n, mk(0, 0));
+    // [tau_pos, s0, 0^(k_log - 9), instance]
+    const size_t off = (size_t)V.k_log - 7;
+    pd_point.assign(off + n, mk(0, 0));
     pd_point[0] = tp;
     pd_point[1] = s0;
-    for (size_t i = 0; i < n; i++) pd_point[7 + i] = taup[i];
+    for (size_t i = 0; i < n; i++) pd_point[off + i] = taup[i];
   }
 
   // ---- Merkle paths: tau_pos, the shift sumcheck from the public leaves
@@ -892,6 +898,7 @@ VerifyStatement device_statement(int m, int hash, const std::array<uint8_t, 32>&
   VerifyStatement V;
   V.m = m;
   V.k_log = hash_k_log(hash);
+  V.hash = hash;
   V.digest = digest;
   const int kk = 1 << V.k_log, pin = statement(hash).z_const;
   V.comb = [=](f128 zskip, const std::vector<f128>& x_inner, f128 alpha, f128 beta) {
@@ -1000,7 +1007,8 @@ std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string
   uint64_t mm = 0;
   for (int k = 0; k < 8; k++) mm |= (uint64_t)bytes[at + k] << (8 * k);
   if (!known_hash(hash)) return "unknown statement hash";
-  if (hash != kHashBlake3 && !merkle && bytes[6] != 2) return "hash chains are BLAKE3 statements";
+  if (hash != kHashBlake3 && hash != kHashSha256 && !merkle && bytes[6] != 2)
+    return "hash chains are BLAKE3 or SHA-256 statements";
   // BLAKE3: 2^8..2^20 compressions; SHA-256: 2^7..2^19; Keccak: 2^6..2^18
   // blocks of one permutation, 2^5..2^17 of three (the same m range)
   if (mm < 22 || mm > 34) return "bundle is for an unsupported statement size";

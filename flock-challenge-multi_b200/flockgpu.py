@@ -43,6 +43,7 @@ EXPORTS = (
     "flock_keccak_bench_inputs", "flock_keccak_statement_digest", "flock_keccak_witness", "flock_keccak_comb",
     "flock_zerocheck_round1_deg4", "flock_bench_round1_deg4", "flock_keccak3_setup_create",
     "flock_keccak3_verify_bundle", "flock_keccak3_statement_digest", "flock_keccak3_witness", "flock_keccak3_comb",
+    "flock_sha256_prove_chain", "flock_sha256_chain_blocks",
 )
 # the hash behind Merkle trees / the transcript (HashKind discriminants)
 HASH = {"sha256": 0, "blake3": 1}
@@ -142,6 +143,8 @@ def load() -> ctypes.CDLL:
         lib.flock_keccak_statement_digest.argtypes = [u32, vp]
         lib.flock_keccak_witness.argtypes = [vp, vp, sz, u32, vp, vp, vp]
         lib.flock_keccak_comb.argtypes = [vp, vp, vp, vp, vp]
+        lib.flock_sha256_prove_chain.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        lib.flock_sha256_chain_blocks.argtypes = [u64, vp, sz, vp]
         lib.flock_sha256_setup_create.argtypes = [vp, sz, i32, i32, ctypes.POINTER(vp)]
         lib.flock_sha256_prove.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_sha256_verify_bundle.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
@@ -251,6 +254,17 @@ def sha256_merkle_inputs(n_log: int, path_log: int = 0, seed: int = None):
     if rc != 0:
         raise FlockError(f"sha256_merkle_inputs: {rc}")
     return comps, b, leaves, root
+
+
+def sha256_chain_blocks(seed: int, steps: int, initial_h=None) -> np.ndarray:
+    """The flock_chain CLI's honest SHA-256 chain, (steps, 24) u32 records
+    (h_in, m) (crates/flock-prover/src/bin/flock_chain.rs:279-316)."""
+    out = np.zeros((steps, 24), np.uint32)
+    h = None if initial_h is None else np.ascontiguousarray(initial_h, np.uint32)
+    rc = load().flock_sha256_chain_blocks(seed, None if h is None else _ptr(h), steps, _ptr(out))
+    if rc:
+        raise FlockError(f"sha256_chain_blocks: {rc}")
+    return out
 
 
 def sha256_compress(h, m) -> np.ndarray:
@@ -785,6 +799,16 @@ class Sha256Prover:
         rc = self.ctx.lib.flock_sha256_prove(self.h, _ptr(comps), comps.shape[0], domain, len(domain),
                                              _ptr(self._buf), self._buf.size, ctypes.byref(n))
         self.ctx._check(rc, "sha256_prove")
+        return self._buf[: n.value].tobytes()
+
+    def prove_chain(self, comps: np.ndarray, domain: bytes = CHAIN_DOMAIN) -> bytes:
+        """prove_chain over (n, 24) u32 compressions that fill the setup
+        (ChainProofBundleLigerito bytes, hash kind Sha2)."""
+        comps = np.ascontiguousarray(comps, np.uint32).reshape(-1, 24)
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_sha256_prove_chain(self.h, _ptr(comps), comps.shape[0], domain, len(domain),
+                                                   _ptr(self._buf), self._buf.size, ctypes.byref(n))
+        self.ctx._check(rc, "sha256_prove_chain")
         return self._buf[: n.value].tobytes()
 
     def prove_merkle(self, comps: np.ndarray, b_bits, path_log: int = 0, domain: bytes = MERKLE_DOMAIN) -> bytes:

@@ -222,6 +222,19 @@ int flock_sha256_prove(flock_setup* s, const flock_sha256_compression* comps, si
  * flock_verify_bundle.  The R1CS bundle does not name its hash, so the
  * statement is chosen by the entry point. */
 int flock_sha256_verify_bundle(flock_ctx* ctx, const uint8_t* bytes, size_t len, const uint8_t* domain, size_t dlen);
+/* Sha256HybridSetup::prove_chain (sha2.rs:1557-1589) + ChainProofBundleLigerito
+ * (hash_kind Sha2) bytes: the n compressions (n = the setup's
+ * n_compressions, a power of two: a chain fills every slot) form a chain
+ * h_in[i + 1] = sha256_compress(h_in[i], m[i]); the public endpoints are
+ * h_in[0] and the last output, the CHAIN_LAYOUT of sha2.rs:1476-1483 (H_in at
+ * byte 0, H_out at byte 32, the BLAKE3 chain's slots).  Verified by
+ * flock_verify on the setup or flock_sha256_verify_bundle. */
+int flock_sha256_prove_chain(flock_setup* s, const flock_sha256_compression* comps, size_t n, const uint8_t* domain,
+                             size_t dlen, uint8_t* out, size_t cap, size_t* out_len);
+/* The flock_chain CLI's honest SHA-256 chain of `steps` compressions
+ * (bin/flock_chain.rs:279-316): h_0 = initial_h or the SHA-256 IV, m_i = 16
+ * SplitMix64(seed) draws (low 32 bits), h_(i+1) = sha256_compress(h_i, m_i). */
+int flock_sha256_chain_blocks(uint64_t seed, const uint32_t* initial_h, size_t steps, flock_sha256_compression* out);
 /* Merkle paths over SHA-256 compressions: Sha256HybridSetup::
  * prove_merkle_paths_ligerito (sha2.rs:1740-1783; path_log = 0 is
  * prove_merkle_path_ligerito, :1662-1697).  2^path_log paths of

@@ -80,6 +80,32 @@ int flockref_prove_chain_blocks(const uint32_t* blocks28, uint32_t log2, const u
   }
 }
 
+// SHA-256 chains: records of 24 u32 (h_in, m), 2^log2 of them
+void flockref_sha256_chain_blocks(uint64_t seed, const uint32_t* initial, size_t steps, uint32_t* out24) {
+  static const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                                 0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+  auto v = sha256_chain_blocks(seed, initial ? initial : iv, steps);
+  memcpy(out24, v.data(), v.size() * sizeof(sha::Compression));
+}
+int flockref_prove_sha256_chain(const uint32_t* blocks24, uint32_t log2, const uint8_t* domain, size_t dlen,
+                                const uint32_t* cv_last, uint8_t* out, size_t cap, size_t* out_len, int* check) {
+  try {
+    std::vector<sha::Compression> blocks((size_t)1 << log2);
+    memcpy(blocks.data(), blocks24, blocks.size() * sizeof(sha::Compression));
+    bool ok = false;
+    ChainBundle cb = prove_sha256_chain(blocks, (int)log2, std::string((const char*)domain, dlen), &ok, cv_last);
+    if (check) *check = ok ? 1 : 0;
+    std::vector<uint8_t> bytes = serialize_chain(cb);
+    *out_len = bytes.size();
+    if (bytes.size() > cap) return 2;
+    memcpy(out, bytes.data(), bytes.size());
+    return 0;
+  } catch (const std::exception& e) {
+    fprintf(stderr, "flockref_prove_sha256_chain: %s\n", e.what());
+    return 1;
+  }
+}
+
 void flockref_f128_mul(const uint64_t* a, const uint64_t* b, uint64_t* out) {
   F128 r = F128(a[0], a[1]) * F128(b[0], b[1]);
   out[0] = r.lo;

@@ -12,7 +12,12 @@
 //    byte 0, out_lo at byte 32, 256-bit slots (region_log 8), so tau_pos has
 //    one coordinate and five slot bits are zero;
 //  * the CLI's honest chain, bin/flock_chain.rs:178-193 (SplitMix64) and
-//    :236-260 (counter 0, block_len 64, flags 0).
+//    :236-260 (counter 0, block_len 64, flags 0);
+//  * the SHA-256 chain, Sha256HybridSetup::prove_chain (r1cs_hashes/sha2.rs:
+//    1557-1589) with CHAIN_LAYOUT (:1476-1483): H_in at byte 0, H_out at byte
+//    32, the same 256-bit slots, in 2^15-bit blocks; the CLI's SHA-256 chain
+//    (bin/flock_chain.rs:279-316: H_0 = the SHA-256 IV, 16 SplitMix64 words
+//    per message); the bundle's hash kind Sha2 (proof_io.rs:51-58).
 #include "flockref.hpp"
 #include <stdexcept>
 
@@ -147,23 +152,18 @@ F128 fold_public_cv(const uint32_t cv[8], F128 tau_pos) {
   return (ONE + tau_pos) * p0 + tau_pos * p1;
 }
 
-ChainBundle prove_chain(const std::vector<Compression>& blocks, int n_log, const std::string& domain,
-                        bool* check, const uint32_t* claimed_cv_last) {
-  const size_t N = (size_t)1 << n_log;
-  if (blocks.size() != N) throw std::runtime_error("prove_chain: the chain must fill 2^n_log slots");
-  ChainBundle cb;
-  memcpy(cb.cv0, blocks[0].cv, 32);
-  compress_cv(blocks[N - 1], cb.cv_last);
-  if (claimed_cv_last) memcpy(cb.cv_last, claimed_cv_last, 32);
-  bool shift_ok = false;
-  CoreHook hook = [&](Challenger& ch, const std::vector<F128>& z) {
+// The chain glue after the core for a 256-bit-slot layout (input words 0, 1
+// and output words 2, 3 of each block of `per` packed words); cb's endpoints
+// are set; `shift_ok` gets the oracle's own check of the shift argument.
+static CoreHook chain_hook(ChainBundle& cb, size_t N, int n_log, size_t per, bool& shift_ok) {
+  return [&cb, N, n_log, per, &shift_ok](Challenger& ch, const std::vector<F128>& z) {
     std::vector<F128> tau_pos = ch.sample_f128_vec(1);
     const F128 e0 = ONE + tau_pos[0], e1 = tau_pos[0];
-    // region fold: words 0, 1 of each block hold cv, words 2, 3 out_lo
+    // region fold: words 0, 1 of each block hold the input cv, words 2, 3 the output
     std::vector<F128> in(N), out(N);
     for (size_t i = 0; i < N; i++) {
-      in[i] = e0 * z[128 * i] + e1 * z[128 * i + 1];
-      out[i] = e0 * z[128 * i + 2] + e1 * z[128 * i + 3];
+      in[i] = e0 * z[per * i] + e1 * z[per * i + 1];
+      out[i] = e0 * z[per * i + 2] + e1 * z[per * i + 3];
     }
     Challenger vch = ch;  // the verifier's transcript from here on
     ChainClaims cl;
@@ -175,12 +175,62 @@ ChainBundle prove_chain(const std::vector<Compression>& blocks, int n_log, const
     DirectClaim dc;
     dc.point.push_back(tau_pos[0]);
     dc.point.push_back(cl.sel0);
-    for (int i = 0; i < 5; i++) dc.point.push_back(ZERO);
+    // 0^(k_log - region_log - 1): the slot bits above the input / output pair
+    for (size_t zb = per; zb > 4; zb >>= 1) dc.point.push_back(ZERO);
     dc.point.insert(dc.point.end(), cl.instance_point.begin(), cl.instance_point.end());
     dc.value = cl.value;
     return std::vector<DirectClaim>{dc};
   };
-  cb.core = prove_with(blocks, n_log, domain, hook);
+}
+
+ChainBundle prove_chain(const std::vector<Compression>& blocks, int n_log, const std::string& domain,
+                        bool* check, const uint32_t* claimed_cv_last) {
+  const size_t N = (size_t)1 << n_log;
+  if (blocks.size() != N) throw std::runtime_error("prove_chain: the chain must fill 2^n_log slots");
+  ChainBundle cb;
+  memcpy(cb.cv0, blocks[0].cv, 32);
+  compress_cv(blocks[N - 1], cb.cv_last);
+  if (claimed_cv_last) memcpy(cb.cv_last, claimed_cv_last, 32);
+  bool shift_ok = false;
+  cb.core = prove_with(blocks, n_log, domain, chain_hook(cb, N, n_log, 128, shift_ok));
+  if (check) *check = shift_ok && last_open_identity_ok();
+  return cb;
+}
+
+std::vector<sha::Compression> sha256_chain_blocks(uint64_t seed, const uint32_t initial[8], size_t steps) {
+  uint64_t s = seed;
+  auto nx = [&]() {
+    s += 0x9E3779B97F4A7C15ull;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  std::vector<sha::Compression> out(steps);
+  uint32_t h[8];
+  memcpy(h, initial, 32);
+  for (size_t i = 0; i < steps; i++) {
+    memcpy(out[i].h, h, 32);
+    for (int w = 0; w < 16; w++) out[i].m[w] = (uint32_t)nx();
+    sha::compress(out[i].h, out[i].m, h);
+  }
+  return out;
+}
+
+ChainBundle prove_sha256_chain(const std::vector<sha::Compression>& blocks, int n_log, const std::string& domain,
+                               bool* check, const uint32_t* claimed_cv_last) {
+  const size_t N = (size_t)1 << n_log;
+  if (blocks.size() != N) throw std::runtime_error("prove_chain: the chain must fill 2^n_log slots");
+  ChainBundle cb;
+  cb.kind = 1;  // HashKind::Sha2
+  memcpy(cb.cv0, blocks[0].h, 32);
+  sha::compress(blocks[N - 1].h, blocks[N - 1].m, cb.cv_last);
+  if (claimed_cv_last) memcpy(cb.cv_last, claimed_cv_last, 32);
+  bool shift_ok = false;
+  std::vector<F128> z, a, b;
+  generate_sha256_witness(blocks, n_log, z, a, b);
+  cb.core = prove_core(sha256_r1cs(n_log), std::move(z), a, b, domain,
+                       chain_hook(cb, N, n_log, (size_t)1 << (15 - 7), shift_ok));
   if (check) *check = shift_ok && last_open_identity_ok();
   return cb;
 }

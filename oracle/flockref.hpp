@@ -391,6 +391,7 @@ struct ChainBundle {
   Bundle core;
   ShiftProof shift;
   uint32_t cv0[8], cv_last[8];
+  uint32_t kind = 0;  // HashKind of the bundle (proof_io.rs:51-58): 0 Blake3, 1 Sha2
 };
 // out_lo of a compression: words 0..7 of the output state
 void compress_cv(const Compression& c, uint32_t out[8]);
@@ -413,6 +414,11 @@ F128 fold_public_cv(const uint32_t cv[8], F128 tau_pos);
 ChainBundle prove_chain(const std::vector<Compression>& blocks, int n_log, const std::string& domain,
                         bool* check = nullptr, const uint32_t* claimed_cv_last = nullptr);
 std::vector<uint8_t> serialize_chain(const ChainBundle& cb);
+// SHA-256 chains (sha2.rs:1557-1589): H_in of step i + 1 = sha256_compress of
+// step i; the CLI's honest chain (bin/flock_chain.rs:279-316)
+std::vector<sha::Compression> sha256_chain_blocks(uint64_t seed, const uint32_t initial[8], size_t steps);
+ChainBundle prove_sha256_chain(const std::vector<sha::Compression>& blocks, int n_log, const std::string& domain,
+                               bool* check = nullptr, const uint32_t* claimed_cv_last = nullptr);
 
 // ---------------------------------------------------------------------------
 // SHA-256 Merkle paths.  crates/flock-prover/src/merkle_path.rs (shift

@@ -747,7 +747,7 @@ std::vector<uint8_t> serialize_merkle(const MerkleBundle& mb) {
 std::vector<uint8_t> serialize_chain(const ChainBundle& cb) {
   W w;
   put_header(w, 3);  // flavor: chain Ligerito
-  w.u32(0);          // HashKind::Blake3
+  w.u32(cb.kind);    // HashKind: Blake3 = 0, Sha2 = 1
   put_core(w, cb.core);
   w.pairs(cb.shift.rounds);
   w.f(cb.shift.g_at_point);

@@ -74,6 +74,13 @@
    holds the same for the 3-wide encoder (keccak3.rs, three permutations per
    2^17-bit block) at n = 49, 100 (partial last block), 6144 and 12288.
 
+12. sha256_chain_proofs.json (--sha256-chain) — SHA-256 hash-chain bundles
+   (Sha256HybridSetup::prove_chain, sha2.rs:1557-1589, hash kind Sha2) of
+   the oracle over the flock_chain CLI's honest SHA-256 chains
+   (bin/flock_chain.rs:279-316, seed n) at n = 128, 1024 and 16384, each
+   recording the oracle's own check: the shift argument verified from the
+   public endpoints and the batched open's claim identity.
+
 Usage (a built oracle; REFERENCE is a checkout of the reference project):
     python tests/golden/make_golden.py --ref REFERENCE [--large]
     python tests/golden/make_golden.py --chain
@@ -82,6 +89,7 @@ Usage (a built oracle; REFERENCE is a checkout of the reference project):
     python tests/golden/make_golden.py --sha256-merkle
     python tests/golden/make_golden.py --default-hashes
     python tests/golden/make_golden.py --keccak
+    python tests/golden/make_golden.py --sha256-chain
     python tests/golden/make_golden.py --gpu-harness VERIFIER --sizes 19:2,20:2 --out FILE
 """
 import hashlib
@@ -281,6 +289,26 @@ def keccak_width_proofs(width, sizes, name, threads) -> None:
         (HERE / name).write_text(json.dumps(out, indent=1))  # after every size
 
 
+SHA256_CHAIN_SIZES = (128, 1024, 16384)
+
+
+def sha256_chain_proofs(threads=8) -> None:
+    import os
+    os.environ["FLOCKREF_THREADS"] = str(threads)
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle_lib
+    orc = oracle_lib.Oracle()
+    out = {"domain": "flock_chain-cli", "proofs": []}
+    for n in SHA256_CHAIN_SIZES:
+        records = orc.sha256_chain_blocks(n, n)
+        data, ok = orc.prove_sha256_chain(records, b"flock_chain-cli")
+        assert ok, n
+        out["proofs"].append({"n": n, "seed": n, "sha256": hashlib.sha256(data).hexdigest(), "size": len(data),
+                              "checked_by": "oracle: shift argument from the public endpoints; "
+                                            "batched-open claim identity"})
+        (HERE / "sha256_chain_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
+
+
 SHA256_MERKLE = ((12, 0), (14, 0), (15, 0), (7, 2), (8, 3))
 
 
@@ -343,6 +371,7 @@ if __name__ == "__main__":
     ap.add_argument("--sha256-merkle", action="store_true")
     ap.add_argument("--default-hashes", action="store_true")
     ap.add_argument("--keccak", action="store_true")
+    ap.add_argument("--sha256-chain", action="store_true")
     ap.add_argument("--gpu-harness", type=Path, metavar="VERIFIER")
     ap.add_argument("--sizes", default="19:2,20:2", help="LOG2:RUNS,... for --gpu-harness")
     ap.add_argument("--out", type=Path, default=HERE / "gpu_verified_proofs.json")
@@ -355,6 +384,8 @@ if __name__ == "__main__":
         sha256_merkle_proofs()
     elif a.keccak:
         keccak_proofs()
+    elif a.sha256_chain:
+        sha256_chain_proofs()
     elif a.default_hashes:
         default_hash_proofs()
     elif a.kernels:

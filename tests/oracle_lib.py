@@ -86,6 +86,9 @@ class Oracle:
         L.flockref_keccak_comb.argtypes = [i32, vp, vp, vp]
         L.flockref_prove_keccak.argtypes = [i32, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_last_open_identity_ok.argtypes = []
+        L.flockref_sha256_chain_blocks.argtypes = [u64, vp, sz, vp]
+        L.flockref_prove_sha256_chain.argtypes = [vp, u32, ctypes.c_char_p, sz, vp, vp, sz, ctypes.POINTER(sz),
+                                                  ctypes.POINTER(ctypes.c_int)]
         L.flockref_round1_deg4.argtypes = [vp, vp, vp, vp, vp, u32, vp, vp, vp]
         L.flockref_time_prove.argtypes = [u32, u64, ctypes.POINTER(sz)]
         L.flockref_time_prove.restype = ctypes.c_double
@@ -273,6 +276,26 @@ class Oracle:
         chk = ctypes.c_int(-1)
         cvl = None if cv_last is None else _p(np.ascontiguousarray(cv_last, np.uint32))
         rc = self.L.flockref_prove_chain_blocks(_p(records), log2, domain, len(domain), cvl, _p(buf), buf.size,
+                                                ctypes.byref(n), ctypes.byref(chk))
+        assert rc == 0, rc
+        return buf[: n.value].tobytes(), chk.value == 1
+
+    def sha256_chain_blocks(self, seed: int, steps: int, initial=None) -> np.ndarray:
+        """(steps, 24) u32 records (h_in, m) of the CLI's honest SHA-256 chain."""
+        out = np.zeros((steps, 24), np.uint32)
+        h = None if initial is None else _p(np.ascontiguousarray(initial, np.uint32))
+        self.L.flockref_sha256_chain_blocks(seed, h, steps, _p(out))
+        return out
+
+    def prove_sha256_chain(self, records: np.ndarray, domain: bytes, cv_last=None) -> tuple:
+        """(SHA-256 chain bundle bytes, check), as prove_chain."""
+        records = np.ascontiguousarray(records, np.uint32)
+        log2 = records.shape[0].bit_length() - 1
+        buf = np.zeros(1 << 21, np.uint8)
+        n = ctypes.c_size_t()
+        chk = ctypes.c_int(-1)
+        cvl = None if cv_last is None else _p(np.ascontiguousarray(cv_last, np.uint32))
+        rc = self.L.flockref_prove_sha256_chain(_p(records), log2, domain, len(domain), cvl, _p(buf), buf.size,
                                                 ctypes.byref(n), ctypes.byref(chk))
         assert rc == 0, rc
         return buf[: n.value].tobytes(), chk.value == 1

@@ -112,3 +112,59 @@ def test_blake3_entry_points_refuse_a_sha256_setup(gpu_ctx):
         assert rc == 1 and "SHA-256" in gpu_ctx.lib.flock_last_error(gpu_ctx.h).decode()
     finally:
         p.close()
+
+
+# ---- SHA-256 hash chains (sha2.rs:1557-1620)
+CHAIN_GOLDEN = json.loads((Path(__file__).resolve().parent / "golden" / "sha256_chain_proofs.json").read_text())
+
+
+def test_chain_matches_oracle(gpu_ctx, oracle):
+    import flockgpu
+    for n in (128, 256):
+        records = flockgpu.sha256_chain_blocks(n + 1, n)
+        p = flockgpu.Sha256Prover(gpu_ctx, n)
+        try:
+            got = p.prove_chain(records)
+            want, ok = oracle.prove_sha256_chain(records, flockgpu.CHAIN_DOMAIN)
+            assert ok and got == want, n
+            assert p.verify(got, flockgpu.CHAIN_DOMAIN) == ""
+            assert gpu_ctx.sha256_verify(got, flockgpu.CHAIN_DOMAIN) == ""
+        finally:
+            p.close()
+
+
+@pytest.mark.parametrize("entry", CHAIN_GOLDEN["proofs"], ids=lambda e: str(e["n"]))
+def test_chain_sizes_match_oracle_fixture(gpu_ctx, entry):
+    import flockgpu
+    p = flockgpu.Sha256Prover(gpu_ctx, entry["n"])
+    try:
+        got = p.prove_chain(flockgpu.sha256_chain_blocks(entry["seed"], entry["n"]))
+        assert hashlib.sha256(got).hexdigest() == entry["sha256"] and len(got) == entry["size"]
+        assert gpu_ctx.sha256_verify(got, flockgpu.CHAIN_DOMAIN) == ""
+    finally:
+        p.close()
+
+
+def test_chain_verify_rejects(gpu_ctx):
+    import flockgpu
+    n = 128
+    records = flockgpu.sha256_chain_blocks(9, n)
+    p = flockgpu.Sha256Prover(gpu_ctx, n)
+    try:
+        good = p.prove_chain(records)
+        # another domain, a flipped proof byte, the BLAKE3 statement
+        assert gpu_ctx.sha256_verify(good, b"another-domain") != ""
+        bad = bytearray(good)
+        bad[len(bad) // 2] ^= 1
+        assert gpu_ctx.sha256_verify(bytes(bad), flockgpu.CHAIN_DOMAIN) != ""
+        assert gpu_ctx.verify(good, flockgpu.CHAIN_DOMAIN) != ""
+        # a wrong public endpoint (the last 256 bools of the bundle are cv_last)
+        wrong = bytearray(good)
+        wrong[-1] ^= 1
+        assert gpu_ctx.sha256_verify(bytes(wrong), flockgpu.CHAIN_DOMAIN) != ""
+        # a broken chain: the prover runs, the verifier refuses the proof
+        broken = records.copy()
+        broken[40, 9] ^= 1
+        assert gpu_ctx.sha256_verify(p.prove_chain(broken), flockgpu.CHAIN_DOMAIN) != ""
+    finally:
+        p.close()
