@@ -18,7 +18,6 @@
 #include <map>
 #include <mutex>
 #include <set>
-#include <thread>
 
 namespace flock {
 
@@ -381,17 +380,6 @@ void Setup::eq_table(const std::vector<f128>& r, f128* dev) {
 void Setup::fetch(const f128* dev, size_t n, f128* host) {
   CK(cudaMemcpyAsync(host, dev, n * sizeof(f128), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  if (yield_gate && yield_left_ms_ > 0 && yield_gate->load(std::memory_order_relaxed) > 0) {
-    // the stream is idle here: hold back this proof's next launches while
-    // small proofs run, within the proof's budget
-    const auto t0 = std::chrono::steady_clock::now();
-    double waited = 0;
-    while (yield_gate->load(std::memory_order_relaxed) > 0 && waited < yield_left_ms_) {
-      std::this_thread::sleep_for(std::chrono::microseconds(20));
-      waited = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    }
-    yield_left_ms_ -= waited;
-  }
 }
 
 uint64_t Setup::grind(Transcript& tr, uint32_t bits) {
@@ -472,7 +460,6 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   P.m = (uint64_t)m;
   P.merkle_fn = merkle_fn;
   pending_.clear();  // (left over only by a proof that threw)
-  yield_left_ms_ = yield_budget_ms;
   stage_off_ = 0;
   const int gs = grid_sms > 0 && grid_sms < sms ? grid_sms : sms;
   const int G = gs * 4;

@@ -2,7 +2,6 @@
 // compressions, the statement (CSC matrices on the device), constant tables
 // and the proof entry point.
 #pragma once
-#include <atomic>
 #include <functional>
 #include <string>
 #include <vector>
@@ -157,11 +156,6 @@ class Setup {
   // serving queue lowers it for large proofs so that their long persistent
   // kernels leave some SMs to small proofs' kernels.
   int grid_sms = 0;
-  // Serving: while *yield_gate > 0 (small proofs running), this proof waits
-  // at its host round trips, up to yield_budget_ms in total per proof, so the
-  // small proofs' kernels get the GPU to themselves (nullptr: never waits)
-  const std::atomic<int>* yield_gate = nullptr;
-  double yield_budget_ms = 0;
   size_t n_words = 0, n_leaves0 = 0;
   cudaStream_t st = nullptr;
   uint32_t* blocks_buf = nullptr;  // device staging for caller-provided compressions
@@ -183,7 +177,6 @@ class Setup {
   };
   static constexpr size_t kStageBytes = (size_t)1 << 21;
   std::vector<PendingOpen> pending_;
-  double yield_left_ms_ = 0;
   size_t stage_off_ = 0;
   H32 root_of(const uint32_t* tree, size_t n_leaves);
   void mark(int phase);

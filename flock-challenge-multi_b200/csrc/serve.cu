@@ -324,17 +324,9 @@ void Server::worker(bool small_only) {
       r.error = e.what();
     }
     if (stop_ && !s) return;
-    const bool small = job.log2 <= kSmallLog2;
-    if (s) {
-      s->grid_sms = n_slots_ >= 3 && !small ? s->sms - kReservedSms : 0;
-      // with an express slot, a large proof steps aside at its round trips
-      // while small proofs run, for up to half its own expected time
-      s->yield_gate = n_slots_ >= 3 && !small ? &small_running_ : nullptr;
-      s->yield_budget_ms = 0.5 * expected_ms(job.log2);
-    }
+    if (s) s->grid_sms = n_slots_ >= 3 && job.log2 > kSmallLog2 ? s->sms - kReservedSms : 0;
     const auto t_run = Clock::now();
     if (s) {
-      if (small) small_running_.fetch_add(1);
       lk.unlock();
       try {
         if (job.has_blocks) {
@@ -356,8 +348,6 @@ void Server::worker(bool small_only) {
         r.status = FLOCK_ERR_INTERNAL;
         r.error = e.what();
       }
-      if (small) small_running_.fetch_sub(1);
-      s->yield_gate = nullptr;
       lk.lock();
       release(std::move(s));
     }

@@ -8,10 +8,8 @@
 // proof, aged by its waiting time (a job that has waited kAging times its own
 // expected run time goes ahead of any fresh job); with 3 or more slots a
 // quarter of the slots (at least one) take only small jobs (at most
-// 2^kSmallLog2 compressions), small jobs' setups run on the
-// highest-priority CUDA stream, and a large proof waits at its host round
-// trips while small proofs run (for at most half its expected time per
-// proof), so that a small proof's kernels meet an idle GPU.  Setups (device buffers + tables for one
+// 2^kSmallLog2 compressions), and small jobs' setups run on the
+// highest-priority CUDA stream.  Setups (device buffers + tables for one
 // size) are cached per size and reused; admission keeps the bytes of all
 // cached setups within the HBM budget, evicting idle setups (the largest
 // first) when a new setup needs room.
@@ -121,7 +119,6 @@ class Server {
   uint64_t next_ticket_ = 1, use_clock_ = 0;
   bool stop_ = false;
   std::atomic<bool> verify_{false};
-  std::atomic<int> small_running_{0};  // small proofs in flight (large ones yield to them)
   int n_slots_ = 0;  // set before the slot threads start (they read it)
   std::vector<std::thread> workers_;
   std::mutex batch_mu_;  // one batch at a time
