@@ -770,11 +770,11 @@ int flock_prove_chain(flock_setup* s, const uint32_t* records, size_t n, const u
   }
   return guard(s->ctx, [&] {
     flock::ChainEnds ends;
-    memcpy(ends.cv0, records, sizeof(ends.cv0));
+    memcpy(ends.in, records, 32);  // 8 u32 words, little endian
     const uint32_t* last = records + 28 * (n - 1);
     uint32_t st16[16];
     flock::b3_compress(last, last + 8, (uint64_t)last[24] | (uint64_t)last[25] << 32, last[26], last[27], st16);
-    memcpy(ends.cv_last, st16, sizeof(ends.cv_last));
+    memcpy(ends.out, st16, 32);
     if (!s->s->records_buf)
       CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->records_buf), n * 28 * sizeof(uint32_t), s->s->st));
     CK(cudaMemcpyAsync(s->s->records_buf, records, n * 28 * sizeof(uint32_t), cudaMemcpyHostToDevice, s->s->st));
@@ -796,8 +796,10 @@ int flock_sha256_prove_chain(flock_setup* s, const flock_sha256_compression* com
   }
   return guard(s->ctx, [&] {
     flock::ChainEnds ends;
-    memcpy(ends.cv0, comps[0].h, sizeof(ends.cv0));
-    flock::sha256_compress(comps[n - 1].h, comps[n - 1].m, ends.cv_last);
+    memcpy(ends.in, comps[0].h, 32);
+    uint32_t h_last[8];
+    flock::sha256_compress(comps[n - 1].h, comps[n - 1].m, h_last);
+    memcpy(ends.out, h_last, 32);
     if (!s->s->records_buf)
       CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->records_buf), n * sizeof(flock_sha256_compression),
                          s->s->st));
@@ -806,6 +808,45 @@ int flock_sha256_prove_chain(flock_setup* s, const flock_sha256_compression* com
     std::string d((const char*)domain, dlen);
     return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d, false, &ends), out, cap, out_len);
   });
+}
+
+int flock_keccak_prove_chain(flock_setup* s, const flock_keccak_state* states, size_t n, const uint8_t* domain,
+                             size_t dlen, uint8_t* out, size_t cap, size_t* out_len) {
+  if (!s || !states || (!domain && dlen)) return FLOCK_ERR_ARG;
+  if (s->s->hash != flock::kHashKeccak) {
+    s->ctx->err = "not a Keccak setup (the 3-wide statement has no chains)";
+    return FLOCK_ERR_ARG;
+  }
+  if (n != s->n_blocks || n != ((size_t)1 << s->s->n_log)) {
+    s->ctx->err = "a chain fills every slot: expected the setup's n_keccaks, a power of two";
+    return FLOCK_ERR_ARG;
+  }
+  return guard(s->ctx, [&] {
+    // endpoints in the slot's physical order: bit z of lane l at 64 l + z
+    // (state_to_phys_bits, keccak.rs:850-857), i.e. the 25 lanes as words
+    flock::ChainEnds ends;
+    memcpy(ends.in, states[0].lanes, 200);
+    uint64_t last[25];
+    memcpy(last, states[n - 1].lanes, 200);
+    flock::keccak_f(last);
+    memcpy(ends.out, last, 200);
+    if (!s->s->records_buf)
+      CK(cudaMallocAsync(reinterpret_cast<void**>(&s->s->records_buf), n * sizeof(flock_keccak_state), s->s->st));
+    CK(cudaMemcpyAsync(s->s->records_buf, states, n * sizeof(flock_keccak_state), cudaMemcpyHostToDevice, s->s->st));
+    std::string d((const char*)domain, dlen);
+    return emit(s->ctx, s->s->prove(nullptr, s->s->records_buf, n, d, false, &ends), out, cap, out_len);
+  });
+}
+
+int flock_keccak_chain_states(const uint64_t* initial, size_t steps, flock_keccak_state* out) {
+  if (!out && steps) return FLOCK_ERR_ARG;
+  uint64_t cur[25] = {};
+  if (initial) memcpy(cur, initial, sizeof(cur));
+  for (size_t i = 0; i < steps; i++) {
+    memcpy(out[i].lanes, cur, sizeof(cur));
+    flock::keccak_f(cur);
+  }
+  return FLOCK_OK;
 }
 
 int flock_sha256_chain_blocks(uint64_t seed, const uint32_t* initial_h, size_t steps, flock_sha256_compression* out) {

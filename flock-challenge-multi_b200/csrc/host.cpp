@@ -907,10 +907,10 @@ std::vector<uint8_t> encode(const Proof& p) {
   e.u64(p.fold_nonces.size());
   for (auto v : p.fold_nonces) e.u64(v);
   if (p.chain) {
-    // Vec<bool>: u64 length, one byte per bit (bit 32 w + b = bit b of word w)
-    for (const uint32_t* cv : {p.cv0, p.cv_last}) {
-      e.u64(256);
-      for (int i = 0; i < 256; i++) e.o.push_back((uint8_t)((cv[i / 32] >> (i % 32)) & 1));
+    // Vec<bool>: u64 length, one byte per bit of the region's physical layout
+    for (const uint64_t* end : {p.end0, p.end_last}) {
+      e.u64((uint64_t)p.end_bits);
+      for (int i = 0; i < p.end_bits; i++) e.o.push_back((uint8_t)((end[i / 64] >> (i % 64)) & 1));
     }
   }
   return e.o;

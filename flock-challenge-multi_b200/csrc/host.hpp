@@ -159,6 +159,17 @@ inline int hash_k_log(int hash) {
 }
 inline bool known_hash(int hash) { return hash >= kHashBlake3 && hash <= kHashKeccak3; }
 inline bool is_keccak(int hash) { return hash == kHashKeccak || hash == kHashKeccak3; }
+// A statement's hash-chain geometry (ChainLayout, chain_common.rs:29-63): the
+// input and output regions are aligned 2^region_log-bit slots at packed words
+// 0 and out_word of each block, holding region_bits real bits
+// (blake3.rs:5160-5167, sha2.rs:1476-1483, keccak.rs:839-846).
+struct ChainGeom {
+  int region_log, out_word, region_bits, kind;  // kind: the bundle's HashKind
+};
+inline ChainGeom chain_geom(int hash) {
+  if (hash == kHashKeccak) return ChainGeom{11, 16, 1600, 2};
+  return ChainGeom{8, 2, 256, hash == kHashSha256 ? 1 : 0};
+}
 // permutations per block of a Keccak statement
 inline int keccak_width(int hash) { return hash == kHashKeccak3 ? 3 : 1; }
 
@@ -192,10 +203,13 @@ struct Proof {
   std::vector<f128> ood;
   // hash-chain bundle (flavor 3): the shift argument and public endpoints
   bool chain = false;
-  uint32_t chain_kind = 0;  // the bundle's HashKind (proof_io.rs:51-58): 0 Blake3, 1 Sha2
+  uint32_t chain_kind = 0;  // the bundle's HashKind (proof_io.rs:51-58): 0 Blake3, 1 Sha2, 2 Keccak
   std::vector<std::pair<f128, f128>> shift_rounds;
   f128 g_at_point{};
-  uint32_t cv0[8] = {}, cv_last[8] = {};
+  // the public endpoints in the region's physical bit order (bit i of the
+  // region = bit i % 64 of word i / 64), end_bits of them
+  uint64_t end0[32] = {}, end_last[32] = {};
+  int end_bits = 256;
   // SHA-256 Merkle-path proof: the shift sumcheck's (q(1), q(w), q(w+1))
   // rounds (g_at_point above); encoded as bincode of (Commitment,
   // MerklePathProofLigerito), without a FLOCK header

@@ -220,8 +220,11 @@ void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size
 // hash chain: region fold of every instance's cv / out_lo words (g = [In | Out],
 // 2 n_inst values) and the packed-direct claim's scatter into b_combined;
 // per: packed words per block (2^(k_log - 7))
-void chain_fold(const f128* z, size_t n_inst, size_t per, f128 e0, f128 e1, f128* g, cudaStream_t s);
-void chain_scatter(f128* bc, const f128* eq_inst, size_t n_inst, size_t per, const f128 c[4], cudaStream_t s);
+// e: the R (<= 16) region weights eq(tau_pos, .); the output region at word out_word
+void chain_fold(const f128* z, size_t n_inst, size_t per, const f128* e, int R, int out_word, f128* g,
+                cudaStream_t s);
+// c: the W (<= 32) word coefficients of the claim
+void chain_scatter(f128* bc, const f128* eq_inst, size_t n_inst, size_t per, const f128* c, int W, cudaStream_t s);
 // Merkle path (2^15-bit blocks): the four slot folds (out: 4 x n_inst), the
 // weight tables ta, tb, one y-round, and the claim's scatter into b_combined
 void mp_fold(const f128* z, size_t n_inst, f128 e0, f128 e1, f128* out, cudaStream_t s);

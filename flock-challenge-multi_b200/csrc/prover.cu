@@ -466,8 +466,8 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   const uint32_t n_slots = 1u << n_log;
   mark(0);
   if (hash != kHashBlake3 && committed) throw std::runtime_error("batched commits are BLAKE3 statements");
-  if (chain && hash != kHashBlake3 && hash != kHashSha256)
-    throw std::runtime_error("hash chains are BLAKE3 or SHA-256 statements");
+  if (chain && hash != kHashBlake3 && hash != kHashSha256 && hash != kHashKeccak)
+    throw std::runtime_error("hash chains are BLAKE3, SHA-256 or Keccak statements");
   if (merkle && (hash != kHashSha256 || n_blocks != n_slots || !merkle->b_bits || merkle->path_log < 0 ||
                  merkle->path_log > n_log))
     throw std::runtime_error("a Merkle path is a SHA-256 statement whose paths fill every slot");
@@ -777,15 +777,18 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   std::vector<f128> pd_point;
   f128 pd_value = mk(0, 0);
   if (chain) {
+    const ChainGeom CG = chain_geom(hash);
     P.chain = true;
-    P.chain_kind = hash == kHashSha256 ? 1 : 0;
-    memcpy(P.cv0, chain->cv0, sizeof(P.cv0));
-    memcpy(P.cv_last, chain->cv_last, sizeof(P.cv_last));
+    P.chain_kind = (uint32_t)CG.kind;
+    P.end_bits = CG.region_bits;
+    memcpy(P.end0, chain->in, sizeof(P.end0));
+    memcpy(P.end_last, chain->out, sizeof(P.end_last));
     const size_t N = n_slots;
-    const f128 tau_pos = tr.sample_vec(1)[0];
+    const std::vector<f128> tau_pos = tr.sample_vec((size_t)CG.region_log - 7);
+    const std::vector<f128> et = heq(tau_pos);  // one weight per packed word of a region
     f128* g = pp[2];
     f128* w = pp[3];
-    chain_fold(z, N, (size_t)1 << (k_log - 7), fx(hone(), tau_pos), tau_pos, g, st);
+    chain_fold(z, N, (size_t)1 << (k_log - 7), et.data(), (int)et.size(), CG.out_word, g, st);
     const std::vector<f128> tau = tr.sample_vec((size_t)n_log);
     const f128 alpha = tr.sample();
     // W(y, 0) = eq(tau, y - 1) for y >= 1, W(0, 0) = alpha; W(y, 1) = eq(tau, y)
@@ -815,11 +818,12 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     }
     P.g_at_point = pd_value;
     // round k bound variable n_log - k; variable n_log is s0; the point is
-    // [tau_pos, s0, 0^(k_log - 9), instance] (k_log - 7 slot coordinates)
-    const size_t off = (size_t)k_log - 7;
+    // [tau_pos, s0, 0^(k_log - region_log - 1), instance] (k_log - 7 slot
+    // coordinates; chain_common.rs:211-231)
+    const size_t off = (size_t)k_log - 7, tl = tau_pos.size();
     pd_point.assign(off + (size_t)n_log, mk(0, 0));
-    pd_point[0] = tau_pos;
-    pd_point[1] = rs[0];
+    for (size_t j = 0; j < tl; j++) pd_point[j] = tau_pos[j];
+    pd_point[tl] = rs[0];
     for (int k = 1; k <= n_log; k++) pd_point[off + (size_t)(n_log - k)] = rs[k];
   }
 
@@ -971,14 +975,17 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
                       gs, st);
   }
   if (chain) {
-    // b_combined += gpd eq(point): words w = 0..3 of block i get
-    // gpd eq(tau_pos, w & 1) eq(s0*, w >> 1) eq(tau', i) (pcs.rs:1236-1248)
-    const f128 tp = pd_point[0], s0 = pd_point[1];
-    const f128 ep[2] = {fx(hone(), tp), tp}, es[2] = {fx(hone(), s0), s0};
-    f128 c[4];
-    for (int wd = 0; wd < 4; wd++) c[wd] = hmul(gpd, hmul(ep[wd & 1], es[wd >> 1]));
+    // b_combined += gpd eq(point): words w < 2R of block i (R packed words
+    // per region) get gpd eq(tau_pos, w mod R) eq(s0*, w / R) eq(tau', i)
+    // (pcs.rs:1236-1248)
+    const int tl = chain_geom(hash).region_log - 7, R = 1 << tl;
+    const std::vector<f128> ep = heq(std::vector<f128>(pd_point.begin(), pd_point.begin() + tl));
+    const f128 s0 = pd_point[(size_t)tl];
+    const f128 es[2] = {fx(hone(), s0), s0};
+    std::vector<f128> c((size_t)2 * R);
+    for (int wd = 0; wd < 2 * R; wd++) c[(size_t)wd] = hmul(gpd, hmul(ep[(size_t)(wd % R)], es[wd / R]));
     eq_table(std::vector<f128>(pd_point.begin() + (k_log - 7), pd_point.end()), scratch_eq());
-    chain_scatter(pp[1], scratch_eq(), n_slots, (size_t)1 << (k_log - 7), c, st);
+    chain_scatter(pp[1], scratch_eq(), n_slots, (size_t)1 << (k_log - 7), c.data(), (int)c.size(), st);
   }
   if (merkle) {
     // words w = 0..7 of block i get gpd eq(tau_pos, w & 1) eq(sel, w >> 1 & 1)

@@ -46,8 +46,10 @@ struct MerklePublic {
 
 // Public endpoints of a hash chain: the input cv of the first compression and
 // the output cv (out_lo) of the last.
+// a chain's public endpoints in the region's physical bit order (bit i = bit
+// i % 64 of word i / 64; a 256-bit cv is its 8 u32 words little endian)
 struct ChainEnds {
-  uint32_t cv0[8], cv_last[8];
+  uint64_t in[32] = {}, out[32] = {};
 };
 
 // What the verifier needs of a statement: its size, digest, and the

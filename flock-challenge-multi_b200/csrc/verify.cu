@@ -93,15 +93,18 @@ struct Rd {
     o.proof = hs();
     return o;
   }
-  bool bits256(uint32_t cv[8]) {
-    if (u64() != 256 || !need(256)) return false;
-    memset(cv, 0, 32);
-    for (int b = 0; b < 256; b++) {
+  // a Vec<bool> of at most 2048 bits into words (bit b = bit b % 64 of word b / 64)
+  bool bools(uint64_t words[32], int& nbits) {
+    const uint64_t len = u64();
+    if (len > 2048 || !need(len)) return false;
+    memset(words, 0, 32 * sizeof(uint64_t));
+    for (uint64_t b = 0; b < len; b++) {
       uint8_t v = p[i + b];
       if (v > 1) return false;
-      cv[b / 32] |= (uint32_t)v << (b % 32);
+      words[b / 64] |= (uint64_t)v << (b % 64);
     }
-    i += 256;
+    i += len;
+    nbits = (int)len;
     return true;
   }
 };
@@ -121,7 +124,7 @@ bool decode(const uint8_t* bytes, size_t n, Proof& P, std::string& why, bool mer
   P.chain = !merkle && bytes[6] == 3;
   if (P.chain) {
     P.chain_kind = r.u32();
-    if (P.chain_kind > 1) return why = "chain hash kind is neither BLAKE3 nor SHA-256", false;
+    if (P.chain_kind > 2) return why = "unknown chain hash kind", false;
   }
   P.root = r.h();
   P.m = r.u64();
@@ -159,7 +162,9 @@ bool decode(const uint8_t* bytes, size_t n, Proof& P, std::string& why, bool mer
   P.grind_nonces = r.u64s();
   P.ood = r.fs();
   P.fold_nonces = r.u64s();
-  if (P.chain && (!r.bits256(P.cv0) || !r.bits256(P.cv_last))) return why = "chain endpoints", false;
+  int last_bits = 0;
+  if (P.chain && (!r.bools(P.end0, P.end_bits) || !r.bools(P.end_last, last_bits) || last_bits != P.end_bits))
+    return why = "chain endpoints", false;
   if (r.bad) return why = "truncated", false;
   if (r.i != n) return why = "trailing bytes", false;
   return true;
@@ -473,8 +478,15 @@ f128 shift_mle(const std::vector<f128>& a, const std::vector<f128>& b) {
   for (size_t j = 0; j < n; j++) acc = fx(acc, hmul(hmul(pre[j], hmul(fx(hone(), a[j]), b[j])), suf[j + 1]));
   return acc;
 }
-// tau_pos-MLE of a public chaining value over its two packed positions
-// (fold_public_phys, chain_common.rs:84-118)
+// tau_pos-MLE of a public region over its packed positions (fold_public_phys,
+// chain_common.rs:84-118): sum_w eq(tau_pos, w) packed word w
+f128 fold_region(const uint64_t words[32], const std::vector<f128>& tau_pos) {
+  const std::vector<f128> et = heq(tau_pos);
+  f128 acc = mk(0, 0);
+  for (size_t w = 0; w < et.size(); w++) acc = fx(acc, hmul(et[w], mk(words[2 * w], words[2 * w + 1])));
+  return acc;
+}
+// a 256-bit public value (8 u32 words) over its two packed positions
 f128 fold_cv(const uint32_t cv[8], f128 tp) {
   const f128 p0 = mk((uint64_t)cv[0] | (uint64_t)cv[1] << 32, (uint64_t)cv[2] | (uint64_t)cv[3] << 32);
   const f128 p1 = mk((uint64_t)cv[4] | (uint64_t)cv[5] << 32, (uint64_t)cv[6] | (uint64_t)cv[7] << 32);
@@ -576,15 +588,17 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
   // ---- hash chain: tau_pos, the shift argument from the public endpoints
   std::vector<f128> pd_point;
   if (P.chain) {
-    if (P.chain_kind != (V.hash == kHashSha256 ? 1u : 0u)) return "chain: hash kind of another statement";
-    const f128 tp = tr.sample_vec(1)[0];
+    const ChainGeom CG = chain_geom(V.hash);
+    if (P.chain_kind != (uint32_t)CG.kind) return "chain: hash kind of another statement";
+    if (P.end_bits != CG.region_bits) return "chain: endpoint length";
+    const std::vector<f128> tpv = tr.sample_vec((size_t)CG.region_log - 7);
     const size_t n = (size_t)n_log;
     if (P.shift_rounds.size() != n + 1) return "chain: malformed shift proof";
     std::vector<f128> tau = tr.sample_vec(n);
     const f128 al = tr.sample();
     f128 tprod = hone();
     for (f128 t : tau) tprod = hmul(tprod, t);
-    f128 claim = fx(hmul(tprod, fold_cv(P.cv_last, tp)), hmul(al, fold_cv(P.cv0, tp)));
+    f128 claim = fx(hmul(tprod, fold_region(P.end_last, tpv)), hmul(al, fold_region(P.end0, tpv)));
     std::vector<f128> rs;
     for (const auto& rd : P.shift_rounds) {
       tr.f128v(rd.first);
@@ -601,11 +615,11 @@ std::string verify_bundle(const uint8_t* bytes, size_t len, const std::string& d
     const f128 wf = fx(fx(hmul(shift_mle(tau, taup), ops0), hmul(eq_eval(tau.data(), taup.data(), n), s0)),
                        hmul(hmul(al, eq_eval(taup.data(), zero.data(), n)), ops0));
     if (!feq(claim, hmul(wf, P.g_at_point))) return "chain: shift argument";
-    // [tau_pos, s0, 0^(k_log - 9), instance]
-    const size_t off = (size_t)V.k_log - 7;
+    // [tau_pos, s0, 0^(k_log - region_log - 1), instance]
+    const size_t off = (size_t)V.k_log - 7, tl = tpv.size();
     pd_point.assign(off + n, mk(0, 0));
-    pd_point[0] = tp;
-    pd_point[1] = s0;
+    for (size_t j = 0; j < tl; j++) pd_point[j] = tpv[j];
+    pd_point[tl] = s0;
     for (size_t i = 0; i < n; i++) pd_point[off + i] = taup[i];
   }
 
@@ -1007,8 +1021,7 @@ std::string Verifier::verify(const uint8_t* bytes, size_t len, const std::string
   uint64_t mm = 0;
   for (int k = 0; k < 8; k++) mm |= (uint64_t)bytes[at + k] << (8 * k);
   if (!known_hash(hash)) return "unknown statement hash";
-  if (hash != kHashBlake3 && hash != kHashSha256 && !merkle && bytes[6] != 2)
-    return "hash chains are BLAKE3 or SHA-256 statements";
+  if (hash == kHashKeccak3 && !merkle && bytes[6] != 2) return "the 3-wide Keccak statement has no chains";
   // BLAKE3: 2^8..2^20 compressions; SHA-256: 2^7..2^19; Keccak: 2^6..2^18
   // blocks of one permutation, 2^5..2^17 of three (the same m range)
   if (mm < 22 || mm > 34) return "bundle is for an unsupported statement size";

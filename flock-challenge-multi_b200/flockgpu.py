@@ -43,7 +43,7 @@ EXPORTS = (
     "flock_keccak_bench_inputs", "flock_keccak_statement_digest", "flock_keccak_witness", "flock_keccak_comb",
     "flock_zerocheck_round1_deg4", "flock_bench_round1_deg4", "flock_keccak3_setup_create",
     "flock_keccak3_verify_bundle", "flock_keccak3_statement_digest", "flock_keccak3_witness", "flock_keccak3_comb",
-    "flock_sha256_prove_chain", "flock_sha256_chain_blocks",
+    "flock_sha256_prove_chain", "flock_sha256_chain_blocks", "flock_keccak_prove_chain", "flock_keccak_chain_states",
 )
 # the hash behind Merkle trees / the transcript (HashKind discriminants)
 HASH = {"sha256": 0, "blake3": 1}
@@ -145,6 +145,8 @@ def load() -> ctypes.CDLL:
         lib.flock_keccak_comb.argtypes = [vp, vp, vp, vp, vp]
         lib.flock_sha256_prove_chain.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_sha256_chain_blocks.argtypes = [u64, vp, sz, vp]
+        lib.flock_keccak_prove_chain.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
+        lib.flock_keccak_chain_states.argtypes = [vp, sz, vp]
         lib.flock_sha256_setup_create.argtypes = [vp, sz, i32, i32, ctypes.POINTER(vp)]
         lib.flock_sha256_prove.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         lib.flock_sha256_verify_bundle.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, sz]
@@ -300,6 +302,17 @@ def keccak_bench_inputs(n: int, seed: int) -> np.ndarray:
     rc = load().flock_keccak_bench_inputs(n, seed, _ptr(out))
     if rc != 0:
         raise FlockError(f"keccak_bench_inputs: {rc}")
+    return out
+
+
+def keccak_chain_states(steps: int, initial=None) -> np.ndarray:
+    """The flock_chain CLI's Keccak chain (bin/flock_chain.rs:319-346):
+    (steps, 25) u64 successive keccak_f states from `initial` (zero state)."""
+    out = np.zeros((steps, 25), np.uint64)
+    init = None if initial is None else np.ascontiguousarray(initial, np.uint64)
+    rc = load().flock_keccak_chain_states(None if init is None else _ptr(init), steps, _ptr(out))
+    if rc:
+        raise FlockError(f"keccak_chain_states: {rc}")
     return out
 
 
@@ -882,6 +895,16 @@ class KeccakProver:
         rc = self.ctx.lib.flock_keccak_prove(self.h, _ptr(states), states.shape[0], domain, len(domain),
                                              _ptr(self._buf), self._buf.size, ctypes.byref(n))
         self.ctx._check(rc, "keccak_prove")
+        return self._buf[: n.value].tobytes()
+
+    def prove_chain(self, states: np.ndarray, domain: bytes = CHAIN_DOMAIN) -> bytes:
+        """prove_chain over (n, 25) u64 states that fill the setup
+        (ChainProofBundleLigerito bytes, hash kind Keccak)."""
+        states = np.ascontiguousarray(states, np.uint64).reshape(-1, 25)
+        n = ctypes.c_size_t()
+        rc = self.ctx.lib.flock_keccak_prove_chain(self.h, _ptr(states), states.shape[0], domain, len(domain),
+                                                   _ptr(self._buf), self._buf.size, ctypes.byref(n))
+        self.ctx._check(rc, "keccak_prove_chain")
         return self._buf[: n.value].tobytes()
 
     def prove_seed(self, seed: int, domain: bytes = DOMAIN) -> bytes:

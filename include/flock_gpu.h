@@ -312,6 +312,19 @@ int flock_keccak_witness(flock_ctx* ctx, const flock_keccak_state* states, size_
  * [const] over the 2^16 rows of a block, on the GPU (e, comb: 2^16 F128 as
  * lo, hi u64 pairs; alpha, beta: one F128). */
 int flock_keccak_comb(flock_ctx* ctx, const uint64_t* e, const uint64_t* alpha, const uint64_t* beta, uint64_t* comb);
+/* KeccakSetup::prove_chain (keccak.rs:1000-1022) + ChainProofBundleLigerito
+ * (hash_kind Keccak) bytes: the n states (n = the setup's n_keccaks, a power
+ * of two: a chain fills every slot) form a chain state[i + 1] =
+ * keccak_f(state[i]); the public endpoints are state[0] and keccak_f of the
+ * last, 1600 bits each in the slot's physical order (state_to_phys_bits,
+ * :850-857).  The chain geometry is CHAIN_LAYOUT (:839-846): state_0 and
+ * state_24 in 2048-bit slots.  Verified by flock_verify on the setup or
+ * flock_keccak_verify_bundle. */
+int flock_keccak_prove_chain(flock_setup* s, const flock_keccak_state* states, size_t n, const uint8_t* domain,
+                             size_t dlen, uint8_t* out, size_t cap, size_t* out_len);
+/* The flock_chain CLI's Keccak chain (bin/flock_chain.rs:319-346): `steps`
+ * successive states from `initial` (25 lanes; NULL: the zero state). */
+int flock_keccak_chain_states(const uint64_t* initial, size_t steps, flock_keccak_state* out);
 /* The 3-wide encoder (crates/flock-prover/src/r1cs_hashes/keccak3.rs): three
  * independent permutations per 2^17-bit block (sub-keccak i: state_0 in slot
  * 2i, state_24 in slot 2i + 1, t[i, r] tight from bit 12352 in the order

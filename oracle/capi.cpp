@@ -80,6 +80,27 @@ int flockref_prove_chain_blocks(const uint32_t* blocks28, uint32_t log2, const u
   }
 }
 
+// Keccak chains: 2^log2 states (25 u64 lanes each); claimed_last: 25 lanes or null
+int flockref_prove_keccak_chain(const uint64_t* states25, uint32_t log2, const uint8_t* domain, size_t dlen,
+                                const uint64_t* claimed_last, uint8_t* out, size_t cap, size_t* out_len,
+                                int* check) {
+  try {
+    std::vector<keccak::State> st((size_t)1 << log2);
+    memcpy(st.data(), states25, st.size() * sizeof(keccak::State));
+    bool ok = false;
+    ChainBundle cb = prove_keccak_chain(st, (int)log2, std::string((const char*)domain, dlen), &ok, claimed_last);
+    if (check) *check = ok ? 1 : 0;
+    std::vector<uint8_t> bytes = serialize_chain(cb);
+    *out_len = bytes.size();
+    if (bytes.size() > cap) return 2;
+    memcpy(out, bytes.data(), bytes.size());
+    return 0;
+  } catch (const std::exception& e) {
+    fprintf(stderr, "flockref_prove_keccak_chain: %s\n", e.what());
+    return 1;
+  }
+}
+
 // SHA-256 chains: records of 24 u32 (h_in, m), 2^log2 of them
 void flockref_sha256_chain_blocks(uint64_t seed, const uint32_t* initial, size_t steps, uint32_t* out24) {
   static const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,

@@ -17,7 +17,13 @@
 //    1557-1589) with CHAIN_LAYOUT (:1476-1483): H_in at byte 0, H_out at byte
 //    32, the same 256-bit slots, in 2^15-bit blocks; the CLI's SHA-256 chain
 //    (bin/flock_chain.rs:279-316: H_0 = the SHA-256 IV, 16 SplitMix64 words
-//    per message); the bundle's hash kind Sha2 (proof_io.rs:51-58).
+//    per message); the bundle's hash kind Sha2 (proof_io.rs:51-58);
+//  * the Keccak chain, KeccakSetup::prove_chain (keccak.rs:1000-1022) with
+//    its CHAIN_LAYOUT (:839-846): state_0 and state_24 in 2048-bit slots
+//    (region_log 11: tau_pos has 4 coordinates, the claim point 4 zero slot
+//    bits), 1600-bit endpoints (state_to_phys_bits :850-857); the CLI's
+//    chain of successive permutations from a start state (flock_chain.rs:
+//    319-366).
 #include "flockref.hpp"
 #include <stdexcept>
 
@@ -146,37 +152,70 @@ bool shift_verify(const ShiftProof& pf, F128 x0_r, F128 xlast_r, size_t n, Chall
   return true;
 }
 
-F128 fold_public_cv(const uint32_t cv[8], F128 tau_pos) {
-  F128 p0((uint64_t)cv[0] | (uint64_t)cv[1] << 32, (uint64_t)cv[2] | (uint64_t)cv[3] << 32);
-  F128 p1((uint64_t)cv[4] | (uint64_t)cv[5] << 32, (uint64_t)cv[6] | (uint64_t)cv[7] << 32);
-  return (ONE + tau_pos) * p0 + tau_pos * p1;
+// physical bits of a 256-bit value of 8 u32 words (cv_to_phys_bits,
+// blake3.rs:5169-5180, sha2.rs:1487-1495): bit 32 w + b = bit b of word w
+static std::vector<uint8_t> phys_of_words(const uint32_t cv[8]) {
+  std::vector<uint8_t> p(256);
+  for (int i = 0; i < 256; i++) p[i] = (uint8_t)((cv[i / 32] >> (i % 32)) & 1);
+  return p;
+}
+// physical bits of a Keccak state: bit z of lane l at 64 l + z (within_lane_contiguous)
+static std::vector<uint8_t> phys_of_lanes(const uint64_t lanes[25]) {
+  std::vector<uint8_t> p(1600);
+  for (int i = 0; i < 1600; i++) p[i] = (uint8_t)((lanes[i / 64] >> (i % 64)) & 1);
+  return p;
 }
 
-// The chain glue after the core for a 256-bit-slot layout (input words 0, 1
-// and output words 2, 3 of each block of `per` packed words); cb's endpoints
-// are set; `shift_ok` gets the oracle's own check of the shift argument.
-static CoreHook chain_hook(ChainBundle& cb, size_t N, int n_log, size_t per, bool& shift_ok) {
-  return [&cb, N, n_log, per, &shift_ok](Challenger& ch, const std::vector<F128>& z) {
-    std::vector<F128> tau_pos = ch.sample_f128_vec(1);
-    const F128 e0 = ONE + tau_pos[0], e1 = tau_pos[0];
-    // region fold: words 0, 1 of each block hold the input cv, words 2, 3 the output
+// fold_public_phys (chain_common.rs:84-118): sum over the region's packed
+// positions of eq(tau_pos, pos) times the 128 physical bits there
+F128 fold_public_phys(const std::vector<uint8_t>& phys, const std::vector<F128>& tau_pos) {
+  const std::vector<F128> eq = build_eq(tau_pos);
+  F128 acc = ZERO;
+  for (size_t pos = 0; pos < eq.size(); pos++) {
+    uint64_t lo = 0, hi = 0;
+    for (int b = 0; b < 128; b++) {
+      const size_t i = pos * 128 + (size_t)b;
+      if (i < phys.size() && phys[i]) (b < 64 ? lo : hi) |= 1ull << (b % 64);
+    }
+    acc += eq[pos] * F128(lo, hi);
+  }
+  return acc;
+}
+
+// The chain glue after the core (prove_chain_ligerito_generic,
+// chain_common.rs:271-346): tau_pos over the region's packed words, the
+// input region at words 0.. and the output region at words out_word.. of each
+// block of `per` packed words; cb's endpoints are set; `shift_ok` gets the
+// oracle's own check of the shift argument.
+static CoreHook chain_hook(ChainBundle& cb, size_t N, int n_log, size_t per, int region_log, size_t out_word,
+                           bool& shift_ok) {
+  return [&cb, N, n_log, per, region_log, out_word, &shift_ok](Challenger& ch, const std::vector<F128>& z) {
+    const std::vector<F128> tau_pos = ch.sample_f128_vec((size_t)region_log - 7);
+    const std::vector<F128> et = build_eq(tau_pos);
     std::vector<F128> in(N), out(N);
     for (size_t i = 0; i < N; i++) {
-      in[i] = e0 * z[per * i] + e1 * z[per * i + 1];
-      out[i] = e0 * z[per * i + 2] + e1 * z[per * i + 3];
+      F128 a = ZERO, b = ZERO;
+      for (size_t w = 0; w < et.size(); w++) {
+        a += et[w] * z[per * i + w];
+        b += et[w] * z[per * i + out_word + w];
+      }
+      in[i] = a;
+      out[i] = b;
     }
     Challenger vch = ch;  // the verifier's transcript from here on
     ChainClaims cl;
     cb.shift = shift_prove(in, out, ch, cl);
     ChainClaims vcl;
-    shift_ok = shift_verify(cb.shift, fold_public_cv(cb.cv0, tau_pos[0]), fold_public_cv(cb.cv_last, tau_pos[0]),
+    shift_ok = shift_verify(cb.shift, fold_public_phys(cb.phys0, tau_pos), fold_public_phys(cb.phys_last, tau_pos),
                             (size_t)n_log, vch, vcl) &&
                vcl.value == cl.value && vcl.sel0 == cl.sel0 && vcl.instance_point == cl.instance_point;
+    // [tau_pos, sel0, 0^(k_log - region_log - 1), instance] (chain_common.rs:211-231)
     DirectClaim dc;
-    dc.point.push_back(tau_pos[0]);
+    dc.point = tau_pos;
     dc.point.push_back(cl.sel0);
-    // 0^(k_log - region_log - 1): the slot bits above the input / output pair
-    for (size_t zb = per; zb > 4; zb >>= 1) dc.point.push_back(ZERO);
+    int k_log = 7;
+    for (size_t p2 = per; p2 > 1; p2 >>= 1) k_log++;
+    for (int i = 0; i < k_log - region_log - 1; i++) dc.point.push_back(ZERO);
     dc.point.insert(dc.point.end(), cl.instance_point.begin(), cl.instance_point.end());
     dc.value = cl.value;
     return std::vector<DirectClaim>{dc};
@@ -188,11 +227,12 @@ ChainBundle prove_chain(const std::vector<Compression>& blocks, int n_log, const
   const size_t N = (size_t)1 << n_log;
   if (blocks.size() != N) throw std::runtime_error("prove_chain: the chain must fill 2^n_log slots");
   ChainBundle cb;
-  memcpy(cb.cv0, blocks[0].cv, 32);
-  compress_cv(blocks[N - 1], cb.cv_last);
-  if (claimed_cv_last) memcpy(cb.cv_last, claimed_cv_last, 32);
+  uint32_t last[8];
+  compress_cv(blocks[N - 1], last);
+  cb.phys0 = phys_of_words(blocks[0].cv);
+  cb.phys_last = phys_of_words(claimed_cv_last ? claimed_cv_last : last);
   bool shift_ok = false;
-  cb.core = prove_with(blocks, n_log, domain, chain_hook(cb, N, n_log, 128, shift_ok));
+  cb.core = prove_with(blocks, n_log, domain, chain_hook(cb, N, n_log, 128, 8, 2, shift_ok));
   if (check) *check = shift_ok && last_open_identity_ok();
   return cb;
 }
@@ -223,14 +263,35 @@ ChainBundle prove_sha256_chain(const std::vector<sha::Compression>& blocks, int 
   if (blocks.size() != N) throw std::runtime_error("prove_chain: the chain must fill 2^n_log slots");
   ChainBundle cb;
   cb.kind = 1;  // HashKind::Sha2
-  memcpy(cb.cv0, blocks[0].h, 32);
-  sha::compress(blocks[N - 1].h, blocks[N - 1].m, cb.cv_last);
-  if (claimed_cv_last) memcpy(cb.cv_last, claimed_cv_last, 32);
+  uint32_t last[8];
+  sha::compress(blocks[N - 1].h, blocks[N - 1].m, last);
+  cb.phys0 = phys_of_words(blocks[0].h);
+  cb.phys_last = phys_of_words(claimed_cv_last ? claimed_cv_last : last);
   bool shift_ok = false;
   std::vector<F128> z, a, b;
   generate_sha256_witness(blocks, n_log, z, a, b);
   cb.core = prove_core(sha256_r1cs(n_log), std::move(z), a, b, domain,
-                       chain_hook(cb, N, n_log, (size_t)1 << (15 - 7), shift_ok));
+                       chain_hook(cb, N, n_log, (size_t)1 << (15 - 7), 8, 2, shift_ok));
+  if (check) *check = shift_ok && last_open_identity_ok();
+  return cb;
+}
+
+ChainBundle prove_keccak_chain(const std::vector<keccak::State>& states, int n_log, const std::string& domain,
+                               bool* check, const uint64_t* claimed_last) {
+  const size_t N = (size_t)1 << n_log;
+  if (states.size() != N) throw std::runtime_error("prove_chain: the chain must fill 2^n_log slots");
+  ChainBundle cb;
+  cb.kind = 2;  // HashKind::Keccak
+  keccak::State last = states[N - 1];
+  keccak::permute(last.lanes);
+  cb.phys0 = phys_of_lanes(states[0].lanes);
+  cb.phys_last = phys_of_lanes(claimed_last ? claimed_last : last.lanes);
+  bool shift_ok = false;
+  const keccak::Layout& L = keccak::single_layout();
+  std::vector<F128> z, a, b;
+  generate_keccak_witness(L, states, n_log, z, a, b);
+  cb.core = prove_core(keccak_r1cs(L, n_log), std::move(z), a, b, domain,
+                       chain_hook(cb, N, n_log, (size_t)1 << (16 - 7), 11, 16, shift_ok));
   if (check) *check = shift_ok && last_open_identity_ok();
   return cb;
 }

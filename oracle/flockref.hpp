@@ -390,8 +390,9 @@ struct ChainClaims { std::vector<F128> instance_point; F128 sel0; F128 value; };
 struct ChainBundle {
   Bundle core;
   ShiftProof shift;
-  uint32_t cv0[8], cv_last[8];
-  uint32_t kind = 0;  // HashKind of the bundle (proof_io.rs:51-58): 0 Blake3, 1 Sha2
+  // the public endpoints in the region's physical bit order (one 0/1 byte per bit)
+  std::vector<uint8_t> phys0, phys_last;
+  uint32_t kind = 0;  // HashKind of the bundle (proof_io.rs:51-58): 0 Blake3, 1 Sha2, 2 Keccak
 };
 // out_lo of a compression: words 0..7 of the output state
 void compress_cv(const Compression& c, uint32_t out[8]);
@@ -419,6 +420,12 @@ std::vector<uint8_t> serialize_chain(const ChainBundle& cb);
 std::vector<sha::Compression> sha256_chain_blocks(uint64_t seed, const uint32_t initial[8], size_t steps);
 ChainBundle prove_sha256_chain(const std::vector<sha::Compression>& blocks, int n_log, const std::string& domain,
                                bool* check = nullptr, const uint32_t* claimed_cv_last = nullptr);
+// Keccak chains (KeccakSetup::prove_chain, keccak.rs:1000-1022, CHAIN_LAYOUT
+// :839-846): state_0 of instance i + 1 = keccak_f(state_0 of instance i);
+// 2048-bit slots, so tau_pos has 4 coordinates; endpoints state_to_phys_bits
+// (:850-857).  claimed_last (25 lanes), when given, replaces the public end.
+ChainBundle prove_keccak_chain(const std::vector<keccak::State>& states, int n_log, const std::string& domain,
+                               bool* check = nullptr, const uint64_t* claimed_last = nullptr);
 
 // ---------------------------------------------------------------------------
 // SHA-256 Merkle paths.  crates/flock-prover/src/merkle_path.rs (shift

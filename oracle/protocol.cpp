@@ -752,9 +752,9 @@ std::vector<uint8_t> serialize_chain(const ChainBundle& cb) {
   w.pairs(cb.shift.rounds);
   w.f(cb.shift.g_at_point);
   put_open(w, cb.core);
-  for (const uint32_t* cv : {cb.cv0, cb.cv_last}) {
-    w.u64(256);
-    for (int i = 0; i < 256; i++) w.u8((uint8_t)((cv[i / 32] >> (i % 32)) & 1));
+  for (const std::vector<uint8_t>* bits : {&cb.phys0, &cb.phys_last}) {
+    w.u64(bits->size());
+    for (uint8_t b : *bits) w.u8(b);
   }
   return w.out;
 }

@@ -80,6 +80,10 @@
    (bin/flock_chain.rs:279-316, seed n) at n = 128, 1024 and 16384, each
    recording the oracle's own check: the shift argument verified from the
    public endpoints and the batched open's claim identity.
+   keccak_chain_proofs.json holds the same for Keccak chains
+   (KeccakSetup::prove_chain, keccak.rs:1000-1022, hash kind Keccak) of
+   successive permutations from the zero state (bin/flock_chain.rs:319-346)
+   at n = 64, 1024 and 8192.
 
 Usage (a built oracle; REFERENCE is a checkout of the reference project):
     python tests/golden/make_golden.py --ref REFERENCE [--large]
@@ -290,6 +294,7 @@ def keccak_width_proofs(width, sizes, name, threads) -> None:
 
 
 SHA256_CHAIN_SIZES = (128, 1024, 16384)
+KECCAK_CHAIN_SIZES = (64, 1024, 8192)
 
 
 def sha256_chain_proofs(threads=8) -> None:
@@ -307,6 +312,15 @@ def sha256_chain_proofs(threads=8) -> None:
                               "checked_by": "oracle: shift argument from the public endpoints; "
                                             "batched-open claim identity"})
         (HERE / "sha256_chain_proofs.json").write_text(json.dumps(out, indent=1))  # after every size
+    kout = {"domain": "flock_chain-cli", "proofs": []}
+    for n in KECCAK_CHAIN_SIZES:
+        data, ok = orc.prove_keccak_chain(orc.keccak_chain_states(n), b"flock_chain-cli")
+        assert ok, n
+        kout["proofs"].append({"n": n, "initial": "zero state", "sha256": hashlib.sha256(data).hexdigest(),
+                               "size": len(data),
+                               "checked_by": "oracle: shift argument from the public endpoints; "
+                                             "batched-open claim identity"})
+        (HERE / "keccak_chain_proofs.json").write_text(json.dumps(kout, indent=1))
 
 
 SHA256_MERKLE = ((12, 0), (14, 0), (15, 0), (7, 2), (8, 3))

@@ -87,6 +87,8 @@ class Oracle:
         L.flockref_prove_keccak.argtypes = [i32, vp, sz, ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz)]
         L.flockref_last_open_identity_ok.argtypes = []
         L.flockref_sha256_chain_blocks.argtypes = [u64, vp, sz, vp]
+        L.flockref_prove_keccak_chain.argtypes = [vp, u32, ctypes.c_char_p, sz, vp, vp, sz, ctypes.POINTER(sz),
+                                                  ctypes.POINTER(ctypes.c_int)]
         L.flockref_prove_sha256_chain.argtypes = [vp, u32, ctypes.c_char_p, sz, vp, vp, sz, ctypes.POINTER(sz),
                                                   ctypes.POINTER(ctypes.c_int)]
         L.flockref_round1_deg4.argtypes = [vp, vp, vp, vp, vp, u32, vp, vp, vp]
@@ -296,6 +298,28 @@ class Oracle:
         chk = ctypes.c_int(-1)
         cvl = None if cv_last is None else _p(np.ascontiguousarray(cv_last, np.uint32))
         rc = self.L.flockref_prove_sha256_chain(_p(records), log2, domain, len(domain), cvl, _p(buf), buf.size,
+                                                ctypes.byref(n), ctypes.byref(chk))
+        assert rc == 0, rc
+        return buf[: n.value].tobytes(), chk.value == 1
+
+    def keccak_chain_states(self, steps: int, initial=None) -> np.ndarray:
+        """(steps, 25) u64: successive keccak_f states from `initial` (zero by default)."""
+        cur = np.zeros(25, np.uint64) if initial is None else np.array(initial, np.uint64)
+        out = np.zeros((steps, 25), np.uint64)
+        for i in range(steps):
+            out[i] = cur
+            cur = self.keccak_f(cur)
+        return out
+
+    def prove_keccak_chain(self, states: np.ndarray, domain: bytes, last=None) -> tuple:
+        """(Keccak chain bundle bytes, check), as prove_chain."""
+        states = np.ascontiguousarray(states, np.uint64).reshape(-1, 25)
+        log2 = states.shape[0].bit_length() - 1
+        buf = np.zeros(1 << 21, np.uint8)
+        n = ctypes.c_size_t()
+        chk = ctypes.c_int(-1)
+        cl = None if last is None else _p(np.ascontiguousarray(last, np.uint64))
+        rc = self.L.flockref_prove_keccak_chain(_p(states), log2, domain, len(domain), cl, _p(buf), buf.size,
                                                 ctypes.byref(n), ctypes.byref(chk))
         assert rc == 0, rc
         return buf[: n.value].tobytes(), chk.value == 1

@@ -203,3 +203,63 @@ def test_wide_large_proof_verifies(gpu_ctx):
         assert gpu_ctx.keccak_verify(bytes(bad), width=3) != ""
     finally:
         p.close()
+
+
+# ---- Keccak hash chains (keccak.rs:1000-1060)
+CHAIN_GOLDEN = json.loads((Path(__file__).resolve().parent / "golden" / "keccak_chain_proofs.json").read_text())
+
+
+def test_chain_matches_oracle(gpu_ctx, oracle):
+    import flockgpu
+    for n, start in ((64, None), (128, flockgpu.keccak_bench_inputs(1, 5)[0])):
+        states = flockgpu.keccak_chain_states(n, start)
+        p = flockgpu.KeccakProver(gpu_ctx, n)
+        try:
+            got = p.prove_chain(states)
+            want, ok = oracle.prove_keccak_chain(states, flockgpu.CHAIN_DOMAIN)
+            assert ok and got == want, n
+            assert p.verify(got, flockgpu.CHAIN_DOMAIN) == ""
+            assert gpu_ctx.keccak_verify(got, flockgpu.CHAIN_DOMAIN) == ""
+        finally:
+            p.close()
+
+
+@pytest.mark.parametrize("entry", CHAIN_GOLDEN["proofs"], ids=lambda e: str(e["n"]))
+def test_chain_sizes_match_oracle_fixture(gpu_ctx, entry):
+    import flockgpu
+    p = flockgpu.KeccakProver(gpu_ctx, entry["n"])
+    try:
+        got = p.prove_chain(flockgpu.keccak_chain_states(entry["n"]))
+        assert hashlib.sha256(got).hexdigest() == entry["sha256"] and len(got) == entry["size"]
+        assert gpu_ctx.keccak_verify(got, flockgpu.CHAIN_DOMAIN) == ""
+    finally:
+        p.close()
+
+
+def test_chain_verify_rejects(gpu_ctx):
+    import flockgpu
+    n = 64
+    states = flockgpu.keccak_chain_states(n)
+    p = flockgpu.KeccakProver(gpu_ctx, n)
+    try:
+        good = p.prove_chain(states)
+        assert gpu_ctx.keccak_verify(good, b"another-domain") != ""
+        bad = bytearray(good)
+        bad[len(bad) // 2] ^= 1
+        assert gpu_ctx.keccak_verify(bytes(bad), flockgpu.CHAIN_DOMAIN) != ""
+        wrong = bytearray(good)
+        wrong[-5] ^= 1  # a bit of the public end state
+        assert gpu_ctx.keccak_verify(bytes(wrong), flockgpu.CHAIN_DOMAIN) != ""
+        broken = states.copy()
+        broken[20, 4] ^= np.uint64(2)
+        assert gpu_ctx.keccak_verify(p.prove_chain(broken), flockgpu.CHAIN_DOMAIN) != ""
+        # another statement's verifier
+        assert gpu_ctx.sha256_verify(good, flockgpu.CHAIN_DOMAIN) != ""
+    finally:
+        p.close()
+    w = flockgpu.KeccakProver(gpu_ctx, 3 * 64, width=3)
+    try:
+        with pytest.raises(flockgpu.FlockError):
+            w.prove_chain(flockgpu.keccak_chain_states(3 * 64))
+    finally:
+        w.close()

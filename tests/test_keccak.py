@@ -208,3 +208,35 @@ def test_wide_fixtures(oracle):
     e = next(p for p in g["proofs"] if p["n"] == 49)
     proof = oracle.prove_keccak(oracle.keccak_bench_inputs(e["n"], e["seed"]), width=3)
     assert hashlib.sha256(proof).hexdigest() == e["sha256"] and len(proof) == e["size"]
+
+
+# ---- Keccak hash chains (keccak.rs:1000-1060 over chain_common.rs)
+CHAIN_GOLDEN = Path(__file__).resolve().parent / "golden" / "keccak_chain_proofs.json"
+
+
+def test_chain_states_match_oracle(oracle):
+    import flockgpu
+    assert np.array_equal(flockgpu.keccak_chain_states(20), oracle.keccak_chain_states(20))
+    s0 = oracle.keccak_bench_inputs(1, 3)[0]
+    assert np.array_equal(flockgpu.keccak_chain_states(5, s0), oracle.keccak_chain_states(5, s0))
+
+
+def test_oracle_chain_checks(oracle):
+    """An honest chain verifies from its public endpoints; a broken link or a
+    wrong endpoint does not; the bundle names HashKind::Keccak and carries
+    1600-bit endpoints."""
+    st = oracle.keccak_chain_states(64)
+    proof, ok = oracle.prove_keccak_chain(st, b"flock_chain-cli")
+    assert ok and proof[7:11] == b"\x02\x00\x00\x00"
+    assert proof[-1608:-1600] == (1600).to_bytes(8, "little")
+    bad = st.copy()
+    bad[33, 7] ^= np.uint64(1 << 40)
+    assert not oracle.prove_keccak_chain(bad, b"flock_chain-cli")[1]
+    assert not oracle.prove_keccak_chain(st, b"flock_chain-cli", last=st[9])[1]
+
+
+def test_oracle_chain_matches_fixture(oracle):
+    g = json.loads(CHAIN_GOLDEN.read_text())
+    e = next(p for p in g["proofs"] if p["n"] == 64)
+    proof, ok = oracle.prove_keccak_chain(oracle.keccak_chain_states(64), b"flock_chain-cli")
+    assert ok and hashlib.sha256(proof).hexdigest() == e["sha256"] and len(proof) == e["size"]
