@@ -589,18 +589,19 @@ def sha256_report(ctx, sizes=(16, 18), steps: int = 5) -> dict:
 KECCAK_SIZES = (6144, 8192, 12288, 24576, 65536)
 
 
-def keccak_report(ctx, sizes=KECCAK_SIZES, steps: int = 5) -> dict:
-    """The Keccak-f[1600] statement (KeccakSetup::prove_fast, r1cs_hashes/
-    keccak.rs, one permutation per 2^16-bit block) at the permutation counts
-    of the reference's benches/keccak3_proof.rs:301-305 and at 2^16, states
-    from that bench's generator.  Device time is the sum of the proof's phase
-    events (states generated on the GPU); e2e goes through flock_keccak_prove
-    from pinned host states (H2D of the states, prove, D2H of the bundle), host
-    clock, medians of `steps`."""
+def keccak_report(ctx, sizes=KECCAK_SIZES, steps: int = 5, widths=(1, 3)) -> dict:
+    """The Keccak-f[1600] statements (KeccakSetup::prove_fast of r1cs_hashes/
+    keccak.rs, one permutation per 2^16-bit block, and of keccak3.rs, three
+    per 2^17-bit block) at the permutation counts of the reference's
+    benches/keccak3_proof.rs:301-305 (the single-vs-3-wide comparison) and at
+    2^16, states from that bench's generator.  Device time is the sum of the
+    proof's phase events (states generated on the GPU); e2e goes through
+    flock_keccak_prove from pinned host states (H2D of the states, prove, D2H
+    of the bundle), host clock, medians of `steps`."""
     import flockgpu
     rows = []
-    for n in sizes:
-        prover = flockgpu.KeccakProver(ctx, n)
+    for n, width in [(n, w) for w in widths for n in sizes]:
+        prover = flockgpu.KeccakProver(ctx, n, width=width)
         states = flockgpu.PinnedArray((n, 25), np.uint64)
         states.array[:] = flockgpu.keccak_bench_inputs(n, flockgpu.keccak_bench_seed(n))
         for _ in range(2):
@@ -614,17 +615,19 @@ def keccak_report(ctx, sizes=KECCAK_SIZES, steps: int = 5) -> dict:
             t0 = time.perf_counter()
             size = len(prover.prove(states.array))
             wall.append(time.perf_counter() - t0)
-        why = ctx.keccak_verify(prover.prove(states.array))
+        why = ctx.keccak_verify(prover.prove(states.array), width=width)
         prover.close()
         if why:
             raise SystemExit(f"keccak_report: proof rejected: {why}")
         d, e = pct(dev, 0.5), pct(wall, 0.5)
-        n_log = max(3, (n - 1).bit_length())
-        rows.append({"n": n, "m": 16 + n_log, "device_ms_median": d, "device_permutations_per_s": n / (d / 1e3),
+        n_log = max(3, (-(-n // width) - 1).bit_length())
+        rows.append({"n": n, "encoder": "keccak.rs" if width == 1 else "keccak3.rs (3-wide)",
+                     "m": (16 if width == 1 else 17) + n_log, "device_ms_median": d,
+                     "device_permutations_per_s": n / (d / 1e3),
                      "e2e_ms_median": e * 1e3, "e2e_permutations_per_s": n / e, "proof_bytes": size,
                      "h2d_bytes_per_proof": n * 200, "phases_ms": {k: round(v, 3) for k, v in ph.items()}})
-    return {"keccak": {"statement": "Keccak-f[1600] permutations, one per 2^16-bit block (keccak.rs)",
-                       "proofs": rows}}
+    return {"keccak": {"statement": "Keccak-f[1600] permutations: one per 2^16-bit block (keccak.rs) and three "
+                                    "per 2^17-bit block (keccak3.rs)", "proofs": rows}}
 
 
 def verify_report(prover, log2: int, reps: int = 3) -> dict:
