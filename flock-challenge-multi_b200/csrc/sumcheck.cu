@@ -197,66 +197,6 @@ __global__ void __launch_bounds__(256) k_lc_zvec(const uint16_t* __restrict__ z,
   for (int p = 0; p < 16; p++) atomic_xor128(zv + col * 4096 + 16 * t + p, acc[p]);
 }
 
-// The same sums from 4-compression subset tables: 16 entries of 16 B each
-// (256 B, two bank rows), so a warp's lookups into one table touch at most 16
-// distinct entries and take about two shared-memory wavefronts, where the
-// 256-entry tables of k_lc_zvec take about eight for 32 random indices.  A
-// thread owns the same 16 positions (one u16 per compression) and does two
-// lookups per position where k_lc_zvec does one.
-constexpr int kZv4Groups = 32;  // 4-compression tables built per barrier pair
-__global__ void __launch_bounds__(256) k_lc_zvec4(const uint16_t* __restrict__ z, const f128* __restrict__ eqo,
-                                                  size_t n_outer, int chunk, int bw, f128* __restrict__ zv) {
-  __shared__ __align__(16) f128 T[kZv4Groups][16];
-  const int col = blockIdx.x;
-  const int t = threadIdx.x;
-  const size_t o0 = (size_t)blockIdx.y * chunk;
-  const size_t o1 = o0 + chunk < n_outer ? o0 + chunk : n_outer;
-  f128 acc[16];
-#pragma unroll
-  for (int p = 0; p < 16; p++) acc[p] = mk(0, 0);
-  for (size_t ob = o0; ob < o1; ob += 4 * kZv4Groups) {
-    __syncthreads();
-    // entry v of table g: XOR of eq(o) over the set bits k of v, o = ob + 4g + k
-    for (int e = t; e < kZv4Groups * 16; e += 256) {
-      const int g = e >> 4, v = e & 15;
-      f128 x = mk(0, 0);
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const size_t o = ob + 4 * g + k;
-        if (((v >> k) & 1) && o < o1) x = fx(x, ldg(eqo + o));
-      }
-      st(&T[g][v], x);
-    }
-    __syncthreads();
-    uint32_t w[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) w[k] = ob + k < o1 ? z[(ob + k) * bw + col * 256 + t] : 0u;
-#pragma unroll 1
-    for (int g = 0; g < kZv4Groups; g++) {
-      const size_t og = ob + 4 * g;
-      if (og >= o1) break;
-      uint32_t wn[4];
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const size_t o = og + 4 + k;
-        wn[k] = (g + 1 < kZv4Groups && o < o1) ? z[o * bw + col * 256 + t] : 0u;
-      }
-      // bits k of nibble p = bit p of compression og + k
-      const uint32_t x01 = w[0] | (w[1] << 16), x23 = w[2] | (w[3] << 16);
-#pragma unroll
-      for (int p = 0; p < 16; p++) {
-        const uint32_t idx = ((x01 >> p) & 1u) | ((x01 >> (15 + p)) & 2u) | ((x23 >> p) & 1u) << 2 |
-                             ((x23 >> (15 + p)) & 2u) << 2;
-        acc[p] = fx(acc[p], ld(&T[g][idx]));
-      }
-#pragma unroll
-      for (int k = 0; k < 4; k++) w[k] = wn[k];
-    }
-  }
-#pragma unroll
-  for (int p = 0; p < 16; p++) atomic_xor128(zv + col * 4096 + 16 * t + p, acc[p]);
-}
-
 // One lincheck round (top binding): with do_fold, fold comb and zv (2 len
 // values each) at r into their first len values; with emit, add the
 // message over the (folded) pairs (i, i + len/2) into out[0..2):
@@ -301,7 +241,7 @@ void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, int k_log, f128* zv
   const int chunk = 1024;  // compressions per CTA (a multiple of 64)
   dim3 grid(1u << (k_log - 12), (unsigned)((n_outer + chunk - 1) / chunk));
   count_launch();
-  k_lc_zvec4<<<grid, 256, 0, s>>>((const uint16_t*)z, eqo, n_outer, chunk, 1 << (k_log - 4), zv);
+  k_lc_zvec<<<grid, 256, 0, s>>>((const uint16_t*)z, eqo, n_outer, chunk, 1 << (k_log - 4), zv);
 }
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s) {
   const int threads = std::max(1, len / 2);
