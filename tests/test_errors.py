@@ -121,3 +121,57 @@ def test_largest_size_deterministic():
         p.close()
     finally:
         ctx.close()
+
+
+def test_statement_entry_points_reject_null_without_a_device():
+    """The SHA-256, Keccak, 3-wide Keccak and degree-4 entry points check
+    their handles and sizes before touching a device."""
+    lib = _lib()
+    vp = ctypes.c_void_p()
+    out = np.zeros(32, np.uint8)
+    for create in (lib.flock_sha256_setup_create, lib.flock_keccak_setup_create, lib.flock_keccak3_setup_create):
+        assert create(None, 256, 1, 0, ctypes.byref(vp)) == ERR_ARG
+    assert lib.flock_keccak_prove(None, None, 64, b"x", 1, None, 0, None) == ERR_ARG
+    assert lib.flock_keccak_prove_chain(None, None, 64, b"x", 1, None, 0, None) == ERR_ARG
+    assert lib.flock_sha256_prove_chain(None, None, 128, b"x", 1, None, 0, None) == ERR_ARG
+    assert lib.flock_keccak_verify_bundle(None, b"FLOCK", 5, b"x", 1) == ERR_ARG
+    assert lib.flock_keccak3_verify_bundle(None, b"FLOCK", 5, b"x", 1) == ERR_ARG
+    assert lib.flock_keccak_chain_states(None, 4, None) == ERR_ARG
+    assert lib.flock_sha256_chain_blocks(1, None, 4, None) == ERR_ARG
+    assert lib.flock_keccak_bench_inputs(4, 1, None) == ERR_ARG
+    # digests: sizes outside the statements' range
+    assert lib.flock_keccak_statement_digest(5, out.ctypes.data) == ERR_ARG
+    assert lib.flock_keccak3_statement_digest(41, out.ctypes.data) == ERR_ARG
+    assert lib.flock_keccak_statement_digest(22, None) == ERR_ARG
+    assert lib.flock_zerocheck_round1_deg4(None, None, None, None, None, None, 8, None, None, None) == ERR_ARG
+    assert lib.flock_bench_round1_deg4(None, 8, 1, 1, None, None, None) == ERR_ARG
+
+
+@pytest.mark.gpu
+def test_statement_setup_sizes(gpu_ctx):
+    """Keccak setups need m = k_log + n_log in 22..34: 33..2^18 permutations
+    (one per block), 49..3 * 2^17 (three per block); the degree-4 round 1
+    takes m in 6..30."""
+    import flockgpu
+    lib, h = gpu_ctx.lib, ctypes.c_void_p()
+    for n in (0, 32, (1 << 18) + 1):
+        assert lib.flock_keccak_setup_create(gpu_ctx.h, n, 1, 0, ctypes.byref(h)) == ERR_ARG, n
+    for n in (0, 48, (3 << 17) + 1):
+        assert lib.flock_keccak3_setup_create(gpu_ctx.h, n, 1, 0, ctypes.byref(h)) == ERR_ARG, n
+    assert lib.flock_keccak_setup_create(gpu_ctx.h, 64, 2, 0, ctypes.byref(h)) == ERR_ARG  # unknown Merkle hash
+    v = np.zeros(8, np.uint64)
+    r = np.zeros((40, 2), np.uint64)
+    pa, pz = np.zeros((192, 2), np.uint64), np.zeros((192, 2), np.uint64)
+    for m in (5, 31):
+        rc = lib.flock_zerocheck_round1_deg4(gpu_ctx.h, *[v.ctypes.data] * 5, m, r.ctypes.data, pa.ctypes.data,
+                                             pz.ctypes.data)
+        assert rc == ERR_ARG, m
+    # a chain must fill its setup: 100 states in a 128-slot setup
+    p = flockgpu.KeccakProver(gpu_ctx, 100)
+    try:
+        with pytest.raises(flockgpu.FlockError):
+            p.prove_chain(flockgpu.keccak_chain_states(100))
+        # the setup still proves
+        assert p.verify(p.prove_seed(3)) == ""
+    finally:
+        p.close()
