@@ -4,11 +4,15 @@
 #include "prover.hpp"
 #include "serve.hpp"
 #include <atomic>
+#include <algorithm>
+#include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 
 struct flock_ctx {
   int device = 0;
+  int sms = 1;  // the device's SM count
   uint64_t budget = 0;
   cudaStream_t st = nullptr;
   std::string err;
@@ -46,6 +50,27 @@ struct flock_challenger {
 std::atomic<uint64_t>& kernel_launch_counter() {
   static std::atomic<uint64_t> n{0};
   return n;
+}
+
+int resident_grid(const void* kernel, int threads, size_t smem, int sms) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, size_t, int>, int> per_sm;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  const auto key = std::make_tuple(kernel, threads, smem, dev);
+  int b = 0;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = per_sm.find(key);
+    if (it != per_sm.end()) b = it->second;
+  }
+  if (!b) {
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem));
+    b = std::max(b, 1);
+    std::lock_guard<std::mutex> g(mu);
+    per_sm[key] = b;
+  }
+  return b * std::max(sms, 1);
 }
 
 namespace {
@@ -122,6 +147,7 @@ int flock_ctx_create(int device, uint64_t hbm_budget_bytes, flock_ctx** out) {
     CK(cudaGetDeviceCount(&n));
     if (device < 0 || device >= n) throw std::runtime_error("no such CUDA device");
     CK(cudaSetDevice(device));
+    CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     return FLOCK_OK;
   });
@@ -1180,7 +1206,7 @@ int flock_sumcheck_round(flock_ctx* c, const uint64_t* f, const uint64_t* b, siz
     CK(cudaMemcpyAsync(df.p, f, n * 16, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(db.p, b, n * 16, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemsetAsync(dout.p, 0, 32, c->st));
-    lig_msg(df.p, db.p, n / 2, dout.p, 148 * 4, c->st);
+    lig_msg(df.p, db.p, n / 2, dout.p, c->sms, c->st);
     CK(cudaMemcpyAsync(msg_out, dout.p, 32, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return FLOCK_OK;
@@ -1379,7 +1405,7 @@ int flock_bench_sumcheck(flock_ctx* c, size_t n, int iters, double* ms) {
     k_fill<<<(unsigned)((2 * n + 255) / 256), 256, 0, c->st>>>((uint64_t*)db.p, 2 * n, 4);
     f128 r = mk(0x1234567890abcdefull, 0x0fedcba987654321ull);
     *ms = time_launches(c->st, iters, [&] {
-      lig_fold_msg(df.p, db.p, fo.p, bo.p, r, n / 4, true, dout.p, 148 * 4, c->st);
+      lig_fold_msg(df.p, db.p, fo.p, bo.p, r, n / 4, true, dout.p, c->sms, c->st);
     });
     return FLOCK_OK;
   });

@@ -37,6 +37,14 @@ struct CudaError : std::runtime_error {
                       std::to_string(__LINE__));                                                \
   } while (0)
 
+// Grid of a grid-stride kernel that runs as exactly one wave on `sms` SMs:
+// the CTAs of `threads` threads and `smem` bytes of dynamic shared memory
+// that fit one SM at once (registers, shared memory, threads), times `sms`.
+// A grid of 4 CTAs per SM for a kernel that fits 3 leaves a second wave of
+// one CTA per SM, which runs with the SM mostly idle.  The occupancy query
+// runs once per (kernel, block shape) and process.
+int resident_grid(const void* kernel, int threads, size_t smem, int sms);
+
 // Makes `device` current for a scope and restores the caller's device after
 // it, so that a library call leaves the calling thread's device as it was.
 struct DeviceScope {
@@ -202,21 +210,22 @@ void build_round1_tables_host(const uint8_t M[64][64], const f128* phi8, void* d
 void zc_round1(const f128* a, const f128* b, const f128* c, const void* tabs, const f128* eqc, size_t n_blocks,
                f128* out, int grid, cudaStream_t s);
 void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag, f128 rho,
-              size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int grid, cudaStream_t s,
+              size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int sms, cudaStream_t s,
               f128* halve_out = nullptr, size_t halve_n = 0);
 void fold_pair_final(const f128* a_in, const f128* b_in, f128 rho, f128* out, cudaStream_t s);
 // k: columns of the block matrices (2^k_log)
 void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_ptr, const uint16_t* bt_row,
              const f128* eq, f128 alpha, f128 beta, int pin, int k, f128* comb, cudaStream_t s);
-void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, int k_log, f128* zv, cudaStream_t s);
+void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, int k_log, f128* zv, int sms, cudaStream_t s);
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s);
 // s_hat_v of the ab claim from the block-folded z (2^k_log values)
 void ring_shat_ab(const f128* zv_pre, const f128* eqt, int k_log, f128* out, cudaStream_t s);
 void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, const f128* ehi1, const f128* L0,
-                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int grid, cudaStream_t s);
-void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int grid, cudaStream_t s);
+                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int sms, cudaStream_t s);
+// sms: the SMs a launch may fill (one wave of resident CTAs on them)
+void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int sms, cudaStream_t s);
 void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size_t n_pairs_out, bool emit, f128* out,
-                  int grid, cudaStream_t s);
+                  int sms, cudaStream_t s);
 // hash chain: region fold of every instance's cv / out_lo words (g = [In | Out],
 // 2 n_inst values) and the packed-direct claim's scatter into b_combined;
 // per: packed words per block (2^(k_log - 7))

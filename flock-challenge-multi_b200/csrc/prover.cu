@@ -632,7 +632,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       nxt_len = etab_len / 2;
     }
     f128* o = next_out(1);
-    zc_round(mode, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, med0 - 9, etab, o, G, st, nxt, nxt_len);
+    zc_round(mode, ain, bin, aout, bout, lag, rho, n_pairs, ns, nm, med0 - 9, etab, o, gs, st, nxt, nxt_len);
     if (nxt) {
       etab = nxt;
       etab_len = nxt_len;
@@ -739,7 +739,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     else lc_comb(at_ptr, at_row, bt_ptr, bt_row, eq_inner, alpha, beta, statement(hash).z_const, kk, comb, st);
     eq_table(x_outer, scratch_eq());
     CK(cudaMemsetAsync(zv, 0, kk * sizeof(f128), st));
-    lc_zvec(z, scratch_eq(), (size_t)1 << (m - k_log), k_log, zv, st);
+    lc_zvec(z, scratch_eq(), (size_t)1 << (m - k_log), k_log, zv, gs, st);
     // pre-sumcheck z_vec: the ab-claim's ring-switch statistic is read from it
     CK(cudaMemcpyAsync(zv_pre, zv, kk * sizeof(f128), cudaMemcpyDeviceToDevice, st));
   }
@@ -1020,13 +1020,13 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     tr.f128v(h_out[1]);
   };
   mo = next_out(1);
-  lig_msg(f, bb, flen / 2, mo, G, st);
+  lig_msg(f, bb, flen / 2, mo, gs, st);
   push_msg();
   auto fold_round = [&](int bits) -> f128 {
     if (bits > 0) P.fold_nonces.push_back(grind(tr, (uint32_t)bits));
     f128 rch = tr.sample();
     mo = next_out(1);
-    lig_fold_msg(f, bb, fo, bo, rch, flen / 4, true, mo, G, st);
+    lig_fold_msg(f, bb, fo, bo, rch, flen / 4, true, mo, gs, st);
     // after the first fold f lives in the ping-pong pair (pp[0], pp[2]) / (pp[1], pp[3])
     if (f == z) { f = fo; fo = pp[0]; }
     else std::swap(f, fo);
@@ -1037,7 +1037,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
   };
   auto introduce = [&](const f128* bnew) {
     mo = next_out(1);
-    lig_msg(f, bnew, flen / 2, mo, G, st);
+    lig_msg(f, bnew, flen / 2, mo, gs, st);
     push_msg();
     f128 be = tr.sample();
     axpy(bb, bnew, be, flen, st);

@@ -76,10 +76,12 @@ void ring_shat_ab(const f128* zv_pre, const f128* eqt, int k_log, f128* out, cud
 }
 
 void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, const f128* ehi1, const f128* L0,
-                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int grid, cudaStream_t s) {
+                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int sms, cudaStream_t s) {
   size_t smem = 2 * kTab4Bytes;
   CK(cudaFuncSetAttribute(k_bcombined_ct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // one wave of resident CTAs: one CTA's table build overlaps the others' lookups
+  const size_t grid = (size_t)resident_grid((const void*)k_bcombined_ct, 512, smem, sms);
   count_launch();
-  k_bcombined_ct<<<(unsigned)std::min<size_t>(n_chunks, (size_t)grid), 512, smem, s>>>(elo0, ehi0, elo1, ehi1, L0, L1,
-                                                                                      lo_bits, n_chunks, out);
+  k_bcombined_ct<<<(unsigned)std::min<size_t>(n_chunks, grid), 512, smem, s>>>(elo0, ehi0, elo1, ehi1, L0, L1,
+                                                                              lo_bits, n_chunks, out);
 }

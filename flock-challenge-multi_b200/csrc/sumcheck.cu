@@ -237,11 +237,16 @@ void lc_comb(const uint32_t* at_ptr, const uint16_t* at_row, const uint32_t* bt_
   count_launch();
   k_lc_comb<<<k * 32 / 256, 256, 0, s>>>(at_ptr, at_row, bt_ptr, bt_row, eq, alpha, beta, pin, k, comb);
 }
-void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, int k_log, f128* zv, cudaStream_t s) {
-  const int chunk = 1024;  // compressions per CTA (a multiple of 64)
-  dim3 grid(1u << (k_log - 12), (unsigned)((n_outer + chunk - 1) / chunk));
+void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, int k_log, f128* zv, int sms, cudaStream_t s) {
+  // compressions per CTA (a multiple of 64), sized so that the columns x
+  // chunks fill one wave of resident CTAs
+  const size_t cols = (size_t)1 << (k_log - 12);
+  const size_t slots = (size_t)resident_grid((const void*)k_lc_zvec, 256, 0, sms);
+  const size_t rows = std::max<size_t>(1, slots / cols);
+  const size_t chunk = std::max<size_t>(64, ((n_outer + rows - 1) / rows + 63) / 64 * 64);
+  dim3 grid((unsigned)cols, (unsigned)((n_outer + chunk - 1) / chunk));
   count_launch();
-  k_lc_zvec<<<grid, 256, 0, s>>>((const uint16_t*)z, eqo, n_outer, chunk, 1 << (k_log - 4), zv);
+  k_lc_zvec<<<grid, 256, 0, s>>>((const uint16_t*)z, eqo, n_outer, (int)chunk, 1 << (k_log - 4), zv);
 }
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s) {
   const int threads = std::max(1, len / 2);
@@ -340,17 +345,21 @@ void sc3_round(const f128* a, const f128* b, const f128* e, f128* ao, f128* bo, 
     k_sc3_round<false><<<grid, 256, 0, s>>>(a, b, e, ao, bo, mk(0, 0), n_pairs, out);
 }
 
-void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int grid, cudaStream_t s) {
+// sms: the SMs the launch may fill (one wave of resident CTAs on them)
+void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int sms, cudaStream_t s) {
+  const int grid = resident_grid((const void*)k_lig_msg, 256, 0, sms);
   count_launch(); k_lig_msg<<<grid, 256, 0, s>>>(f, b, n_pairs, out);
 }
 void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size_t n_pairs_out, bool emit, f128* out,
-                  int grid, cudaStream_t s) {
+                  int sms, cudaStream_t s) {
   count_launch();
   if (n_pairs_out >= (1u << 14)) {
     size_t smem = sizeof(MulTab8);
     CK(cudaFuncSetAttribute(k_lig_fold_msg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = resident_grid((const void*)k_lig_fold_msg<true>, 256, smem, sms);
     k_lig_fold_msg<true><<<grid, 256, smem, s>>>(f, b, fo, bo, r, n_pairs_out, emit, out);
   } else {
+    const int grid = resident_grid((const void*)k_lig_fold_msg<false>, 256, 0, sms);
     k_lig_fold_msg<false><<<grid, 256, 0, s>>>(f, b, fo, bo, r, n_pairs_out, emit, out);
   }
 }

@@ -174,9 +174,10 @@ __global__ void __launch_bounds__(256, 2) k_zc_round(ZcArgs A) {
 // One zerocheck round launch: out[2 js + {0, 1}] ^= (T1, Tinf)(js) for js < 2^ns.
 // mode 0: packed message round, 1: packed fold + message, 2: fold + message.
 // halve_n > 0: also writes halve_out[j] = etab[2j] + etab[2j+1], j < halve_n,
-// the next round's eq table (one launch less per round).
+// the next round's eq table (one launch less per round).  sms: the SMs the
+// launch may fill (one wave of resident CTAs on them).
 void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b_out, const f128* lag, f128 rho,
-              size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int grid, cudaStream_t s,
+              size_t n_pairs, int ns, int nm, int msh, const f128* etab, f128* out, int sms, cudaStream_t s,
               f128* halve_out, size_t halve_n) {
   if (ns < 0 || ns > 2 || nm < 0 || nm > 4 || msh < 0 || (nm > 0 && (((1 << nm) - 1) << msh) >= 64))
     throw CudaError("zc_round: bad eq structure");
@@ -187,16 +188,13 @@ void zc_round(int mode, const f128* a_in, const f128* b_in, f128* a_out, f128* b
   A.halve_out = halve_out; A.halve_n = halve_n;
   const size_t smem = mode == 0 ? 2048 * sizeof(f128) : mode == 1 ? 4096 * sizeof(f128) : sizeof(MulTab8);
   const size_t lanes = (n_pairs + ((size_t)1 << nm) - 1) >> nm;
-  const int g = (int)std::max<size_t>(1, std::min<size_t>((size_t)grid, (lanes + 255) / 256));
+  const void* fn = mode == 0 ? (const void*)k_zc_round<0> : mode == 1 ? (const void*)k_zc_round<1>
+                                                                      : (const void*)k_zc_round<2>;
+  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t full = (size_t)resident_grid(fn, 256, smem, sms);
+  const int g = (int)std::max<size_t>(1, std::min<size_t>(full, (lanes + 255) / 256));
   count_launch();
-  if (mode == 0) {
-    CK(cudaFuncSetAttribute(k_zc_round<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_zc_round<0><<<g, 256, smem, s>>>(A);
-  } else if (mode == 1) {
-    CK(cudaFuncSetAttribute(k_zc_round<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_zc_round<1><<<g, 256, smem, s>>>(A);
-  } else {
-    CK(cudaFuncSetAttribute(k_zc_round<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_zc_round<2><<<g, 256, smem, s>>>(A);
-  }
+  if (mode == 0) k_zc_round<0><<<g, 256, smem, s>>>(A);
+  else if (mode == 1) k_zc_round<1><<<g, 256, smem, s>>>(A);
+  else k_zc_round<2><<<g, 256, smem, s>>>(A);
 }
