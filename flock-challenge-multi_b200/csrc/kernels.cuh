@@ -220,8 +220,11 @@ void lc_zvec(const f128* z, const f128* eqo, size_t n_outer, int k_log, f128* zv
 void lc_round(f128* comb, f128* zv, int len, bool fold, f128 r, bool emit, f128* out, cudaStream_t s);
 // s_hat_v of the ab claim from the block-folded z (2^k_log values)
 void ring_shat_ab(const f128* zv_pre, const f128* eqt, int k_log, f128* out, cudaStream_t s);
+// f, msg (optional): also XOR the first Ligerito message over (f, b_combined)
+// into msg[0..2) (zeroed), the values k_lig_msg gives for the same pairs
 void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, const f128* ehi1, const f128* L0,
-                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int sms, cudaStream_t s);
+                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int sms, cudaStream_t s,
+                       const f128* f = nullptr, f128* msg = nullptr);
 // sms: the SMs a launch may fill (one wave of resident CTAs on them)
 void lig_msg(const f128* f, const f128* b, size_t n_pairs, f128* out, int sms, cudaStream_t s);
 void lig_fold_msg(const f128* f, const f128* b, f128* fo, f128* bo, f128 r, size_t n_pairs_out, bool emit, f128* out,

@@ -938,6 +938,7 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     for (int bb = 0; bb < 128; bb++) c = fx(c, hmul(u[bb], eqdd[k][bb]));
     claim[k] = c;
   }
+  f128* first_msg = nullptr;  // the first Ligerito message, when summed with b_combined
   f128 gam[2] = {tr.sample(), tr.sample()};
   f128 target = fx(hmul(gam[0], claim[0]), hmul(gam[1], claim[1]));
   // the packed-direct claim after the ring-switched ones (pcs.rs:844-872)
@@ -971,8 +972,11 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
       eq_build(xf.data() + 1, lo_bits, hone(), base, st);
       eq_build(xf.data() + 1 + lo_bits, hi_bits, hone(), base + nlo, st);
     }
+    // with no packed-direct claim, b_combined is final here: the first
+    // Ligerito message (over z and b_combined) is summed in the same pass
+    if (!chain && !merkle && lo_bits >= 1) first_msg = next_out(1);
     ring_bcombined_ct(d, d + nlo, d + nlo + nhi, d + 2 * nlo + nhi, bc_tabs, bc_tabs + 4096, lo_bits, nhi, pp[1],
-                      gs, st);
+                      gs, st, first_msg ? z : nullptr, first_msg);
   }
   if (chain) {
     // b_combined += gpd eq(point): words w < 2R of block i (R packed words
@@ -1019,8 +1023,12 @@ std::vector<uint8_t> Setup::prove(const uint64_t* seed, const uint32_t* blocks_d
     tr.f128v(h_out[0]);
     tr.f128v(h_out[1]);
   };
-  mo = next_out(1);
-  lig_msg(f, bb, flen / 2, mo, gs, st);
+  if (first_msg) {
+    mo = first_msg;  // summed with b_combined (no next_out since: the slot is intact)
+  } else {
+    mo = next_out(1);
+    lig_msg(f, bb, flen / 2, mo, gs, st);
+  }
   push_msg();
   auto fold_round = [&](int bits) -> f128 {
     if (bits > 0) P.fold_nonces.push_back(grind(tr, (uint32_t)bits));

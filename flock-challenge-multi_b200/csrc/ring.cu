@@ -70,14 +70,65 @@ __global__ void __launch_bounds__(512) k_bcombined_ct(const f128* __restrict__ e
   }
 }
 
+// The same b_combined, and with it the first Ligerito message over (f, b)
+// (the plain round k_lig_msg computes): msg[0] ^= sum_j f[2j] b[2j],
+// msg[1] ^= sum_j (f[2j] + f[2j+1]) (b[2j] + b[2j+1]).  A thread owns the pair
+// (2j, 2j+1) of a chunk.  The table lookups load the shared-memory pipe and
+// the message's two products per pair the integer multipliers, so one pass
+// keeps both busy where the two kernels each left the other pipe idle, and b
+// is not read back.
+__global__ void __launch_bounds__(256, 3) k_bcombined_msg(const f128* __restrict__ elo0, const f128* __restrict__ ehi0,
+                                                          const f128* __restrict__ elo1, const f128* __restrict__ ehi1,
+                                                          const f128* __restrict__ L0, const f128* __restrict__ L1,
+                                                          int lo_bits, size_t n_chunks, const f128* __restrict__ f,
+                                                          f128* __restrict__ out, f128* __restrict__ msg) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  Tab4* C = reinterpret_cast<Tab4*>(sm);
+  const size_t half = (size_t)1 << (lo_bits - 1);
+  u256 u0 = zero256(), u2 = zero256();
+  for (size_t ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
+    if (threadIdx.x < 64) {
+      const int k = threadIdx.x >> 5, w = threadIdx.x & 31;
+      const f128* L = k ? L1 : L0;
+      const f128 y = mul_x128(ldg((k ? ehi1 : ehi0) + ch), 4 * w);
+      tab4_window(C + k, w, apply_tab(L, y), apply_tab(L, mul_xk(y, 1)), apply_tab(L, mul_xk(y, 2)),
+                  apply_tab(L, mul_xk(y, 3)));
+    }
+    __syncthreads();
+    for (size_t j = threadIdx.x; j < half; j += blockDim.x) {
+      const size_t i = 2 * j, o = (ch << lo_bits) + i;
+      const f128 b0 = fx(tab4_mul(C, ldg(elo0 + i)), tab4_mul(C + 1, ldg(elo1 + i)));
+      const f128 b1 = fx(tab4_mul(C, ldg(elo0 + i + 1)), tab4_mul(C + 1, ldg(elo1 + i + 1)));
+      st(out + o, b0);
+      st(out + o + 1, b1);
+      const f128 f0 = ldg(f + o), f1 = ldg(f + o + 1);
+      acc_wide(u0, mul_wide(f0, b0));
+      acc_wide(u2, mul_wide(fx(f0, f1), fx(b0, b1)));
+    }
+    __syncthreads();  // the next chunk's tables replace these
+  }
+  block_xor_out(reduce(u0), msg);
+  block_xor_out(reduce(u2), msg + 1);
+}
+
 void ring_shat_ab(const f128* zv_pre, const f128* eqt, int k_log, f128* out, cudaStream_t s) {
   count_launch();
   k_shat_from_zvec<<<128, 1 << (k_log - 7), 0, s>>>(zv_pre, eqt, out);
 }
 
 void ring_bcombined_ct(const f128* elo0, const f128* ehi0, const f128* elo1, const f128* ehi1, const f128* L0,
-                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int sms, cudaStream_t s) {
+                       const f128* L1, int lo_bits, size_t n_chunks, f128* out, int sms, cudaStream_t s,
+                       const f128* f, f128* msg) {
   size_t smem = 2 * kTab4Bytes;
+  if (f && msg) {
+    if (lo_bits < 1) throw CudaError("ring_bcombined_ct: the message needs chunks of at least 2 values");
+    CK(cudaFuncSetAttribute(k_bcombined_msg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t grid = (size_t)resident_grid((const void*)k_bcombined_msg, 256, smem, sms);
+    count_launch();
+    k_bcombined_msg<<<(unsigned)std::min<size_t>(n_chunks, grid), 256, smem, s>>>(elo0, ehi0, elo1, ehi1, L0, L1,
+                                                                                 lo_bits, n_chunks, f, out, msg);
+    return;
+  }
   CK(cudaFuncSetAttribute(k_bcombined_ct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // one wave of resident CTAs: one CTA's table build overlaps the others' lookups
   const size_t grid = (size_t)resident_grid((const void*)k_bcombined_ct, 512, smem, sms);
